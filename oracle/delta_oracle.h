@@ -1,0 +1,150 @@
+/*
+ * delta_oracle.h -- CPU restatement (FP64) of the reference's per-timestep contact
+ * pipeline for triangulated particles.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker: tests/, the smoke check
+ * and the CPU-baseline leg of bench.py load it.  The product path (delta_b200) never
+ * links, loads or calls it.
+ *
+ * Every function cites the reference file:line whose arithmetic it follows.  The
+ * library is compiled with -ffp-contract=off so that each a*b+c stays two rounded
+ * operations, as in the reference compiled without FMA contraction.
+ *
+ * Layouts
+ *   pair list  : a[9*ld], b[9*ld]; plane k = 3*vertex + coord, element i = pair i
+ *                (the ispc_bf / ispc_pen pair-list shape, bf.ispc:3, penalty.ispc:154).
+ *   SoA-tri    : x[3*nT], y[3*nT], z[3*nT]; triangle t owns entries 3t..3t+2
+ *                (ParticleRecord _xCoordinates, bf.cpp:47-148).
+ */
+#ifndef DELTA_ORACLE_H
+#define DELTA_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* struct contactpoint, contactpoint.h:42-103 */
+typedef struct {
+  double x[3];
+  double normal[3];
+  double depth;
+  double P[3];
+  double Q[3];
+  int32_t friction;
+  double eps_total;
+  int32_t master;
+  int32_t slave;
+  int32_t penetration;
+  int32_t tri_a;  /* triangle index in A (bookkeeping added here; not in the reference) */
+  int32_t tri_b;  /* triangle index in B */
+} dor_contact;
+
+enum { DOR_BF = 0, DOR_PENALTY = 1, DOR_PENALTY_ITER = 2, DOR_GJK = 3, DOR_HYBRID_PAIR = 4 };
+
+enum {
+  DOR_DRV_BF = 0,               /* bf()                          bf.cpp:47-148          */
+  DOR_DRV_PENALTY = 1,          /* penalty()                     penalty.cpp:133-275    */
+  DOR_DRV_PENALTY_STAT = 2,     /* penaltyStat()                 penalty.cpp:50-110     */
+  DOR_DRV_HYBRID_BATCH = 3,     /* hybridWithPerBatchFallBack    hybrid.cpp:357-487     */
+  DOR_DRV_HYBRID_TRIANGLE = 4,  /* hybridWithPerTriangleFallBack hybrid.cpp:78-200      */
+  DOR_DRV_HYBRID_BATCH_STAT = 5,/* hybridBatchStat               hybrid.cpp:489-628     */
+  DOR_DRV_HYBRID_TRI_STAT = 6,  /* hybridTriangleStat            hybrid.cpp:202-336     */
+  DOR_DRV_GJK = 7               /* gjk(a,3,b,3) per triangle pair, bf() contact rule    */
+};
+
+/* statistics kept by the stat drivers (penalty.cpp:29-48, hybrid.cpp:27-56) */
+typedef struct {
+  int64_t newton_hist[17];
+  int64_t penalty_fails;
+  int64_t batch_fails;
+  int64_t batch_size;
+  double batch_error;
+} dor_stats;
+
+/* ---- per triangle pair ------------------------------------------------------ */
+void dor_bf_solver(const double *xA, const double *yA, const double *zA,
+                   const double *xB, const double *yB, const double *zB, double pq[6]);
+void dor_penalty_solver(const double *xA, const double *yA, const double *zA,
+                        const double *xB, const double *yB, const double *zB,
+                        double max_error, double pq[6], int32_t *failed);
+void dor_penalty_solver_iter(const double *xA, const double *yA, const double *zA,
+                             const double *xB, const double *yB, const double *zB,
+                             double max_error, double pq[6], int32_t *iterations);
+double dor_gjk(const double *a, int32_t na, const double *b, int32_t nb, double p[3], double q[3]);
+
+/* ---- pair list (one triangle pair per element) -------------------------------- */
+/* flags: PENALTY -> failed (0/1); PENALTY_ITER -> iterations; HYBRID_PAIR -> 1 if bf
+ * was used; BF/GJK -> 0.  max_error is the penalty tolerance (reference: (epsA+epsB)/16). */
+void dor_pairs(int32_t method, int64_t n, const double *a, const double *b, int64_t ld,
+               double max_error, double *p, double *q, double *dist, uint8_t *flags,
+               int32_t nthreads);
+
+/* ---- particle-pair drivers ------------------------------------------------------ */
+/* Returns the number of contacts; writes at most cap of them. */
+int64_t dor_detect(int32_t driver,
+                   const double *xA, const double *yA, const double *zA, int32_t nA,
+                   double epsA, int32_t fricA, int32_t idA,
+                   const double *xB, const double *yB, const double *zB, int32_t nB,
+                   double epsB, int32_t fricB, int32_t idB,
+                   dor_contact *out, int64_t cap, dor_stats *stats);
+
+void dor_make_contact(double xPA, double yPA, double zPA, double epsA, int32_t idA,
+                      double xPB, double yPB, double zPB, double epsB, int32_t idB,
+                      int32_t friction, dor_contact *c);
+
+/* ---- forces and dynamics ---------------------------------------------------------- */
+typedef struct { double spring, damper, friction; } dor_material;
+
+void dor_contacts_forces(const dor_contact *c, int64_t nc, double normal_sign,
+                         const double posA[3], const double angA[3], const double linA[3], double massA,
+                         const double posB[3], const double angB[3], const double linB[3], double massB,
+                         const dor_material *mat, double force[3], double torque[3]);
+void dor_expmap(double o1, double o2, double o3, double L[9]);
+void dor_update_rotation(double ang[3], const double ref_ang[3], double rot[9], double step);
+void dor_update_angular(double ref_ang[3], const double rot[9], const double inertia[9],
+                        const double inverse[9], const double torque[3], double step);
+void dor_update_vertex(double *x, double *y, double *z, double rx, double ry, double rz,
+                       const double rot[9], const double pos[3], const double ref_pos[3]);
+
+/* ---- whole time step ---------------------------------------------------------------- */
+typedef struct {
+  int32_t n_bodies;
+  const int64_t *tri_offset;   /* [n_bodies+1] triangle offsets */
+  double *x, *y, *z;           /* spatial SoA-tri vertices, 3 per triangle */
+  const double *rx, *ry, *rz;  /* referential SoA-tri vertices */
+  double *pos;                 /* [3n] spatial centre of mass */
+  const double *ref_pos;       /* [3n] referential centre of mass */
+  double *vel;                 /* [3n] linear velocity */
+  double *ang;                 /* [3n] spatial angular velocity */
+  double *ref_ang;             /* [3n] referential angular velocity */
+  double *rot;                 /* [9n] orientation, column-major as in dynamics.cpp */
+  const double *inertia;       /* [9n] */
+  const double *inverse;       /* [9n] */
+  const double *mass;          /* [n] (obstacles: +inf) */
+  const double *eps;           /* [n] contact halo epsilon */
+  const double *radius;        /* [n] bounding-sphere radius about pos */
+  const uint8_t *friction;     /* [n] */
+  const uint8_t *obstacle;     /* [n] */
+} dor_scene;
+
+typedef struct {
+  double dt;
+  double gravity[3];
+  dor_material mat;
+} dor_step_params;
+
+typedef struct dor_sim dor_sim;
+dor_sim *dor_sim_create(void);
+void dor_sim_destroy(dor_sim *s);
+/* Runs nsteps of the multiscale update order; returns the contact count of the last
+ * detection (the contacts the next step's forces use). */
+int64_t dor_sim_run(dor_sim *s, dor_scene *scene, const dor_step_params *prm, int32_t nsteps,
+                    int64_t *contacts_per_step);
+/* Copies out the contacts currently held (sorted by (master, slave, tri_a, tri_b)). */
+int64_t dor_sim_contacts(const dor_sim *s, dor_contact *out, int64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

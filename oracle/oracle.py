@@ -1,0 +1,216 @@
+"""ctypes bindings for the checker libraries (test infrastructure, not the product).
+
+``Oracle`` wraps ``liboracle.so`` (the C restatement in ``delta_oracle.c``) and
+``Reference`` wraps ``_ref/libdelta_ref*.so`` (the reference's own sources compiled by
+``oracle/Makefile``).  Only tests/, the smoke check and the CPU-baseline leg of bench.py
+import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+BF, PENALTY, PENALTY_ITER, GJK, HYBRID_PAIR = 0, 1, 2, 3, 4
+DRV_BF, DRV_PENALTY, DRV_PENALTY_STAT, DRV_HYBRID_BATCH, DRV_HYBRID_TRIANGLE = 0, 1, 2, 3, 4
+DRV_HYBRID_BATCH_STAT, DRV_HYBRID_TRI_STAT, DRV_GJK = 5, 6, 7
+
+CONTACT_DTYPE = np.dtype(
+    [
+        ("x", "<f8", 3),
+        ("normal", "<f8", 3),
+        ("depth", "<f8"),
+        ("P", "<f8", 3),
+        ("Q", "<f8", 3),
+        ("friction", "<i4"),
+        ("eps_total", "<f8"),
+        ("master", "<i4"),
+        ("slave", "<i4"),
+        ("penetration", "<i4"),
+        ("tri_a", "<i4"),
+        ("tri_b", "<i4"),
+    ],
+    align=True,
+)
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("newton_hist", C.c_int64 * 17),
+        ("penalty_fails", C.c_int64),
+        ("batch_fails", C.c_int64),
+        ("batch_size", C.c_int64),
+        ("batch_error", C.c_double),
+    ]
+
+
+class Material(C.Structure):
+    _fields_ = [("spring", C.c_double), ("damper", C.c_double), ("friction", C.c_double)]
+
+
+class Scene(C.Structure):
+    _fields_ = [
+        ("n_bodies", C.c_int32),
+        ("tri_offset", C.c_void_p),
+        ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p),
+        ("rx", C.c_void_p), ("ry", C.c_void_p), ("rz", C.c_void_p),
+        ("pos", C.c_void_p), ("ref_pos", C.c_void_p),
+        ("vel", C.c_void_p), ("ang", C.c_void_p), ("ref_ang", C.c_void_p),
+        ("rot", C.c_void_p), ("inertia", C.c_void_p), ("inverse", C.c_void_p),
+        ("mass", C.c_void_p), ("eps", C.c_void_p), ("radius", C.c_void_p),
+        ("friction", C.c_void_p), ("obstacle", C.c_void_p),
+    ]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("gravity", C.c_double * 3), ("mat", Material)]
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _build_if_missing(path: Path):
+    if not path.exists():
+        os.system(f"make -s -C {HERE} >/dev/null 2>&1")
+    return path.exists()
+
+
+class _Lib:
+    prefix = ""
+
+    def _sig(self):
+        L, pre = self.lib, self.prefix
+        vp, i32, i64, f8 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        getattr(L, pre + "pairs").argtypes = [i32, i64, vp, vp, i64, f8, vp, vp, vp, vp, i32]
+        getattr(L, pre + "pairs").restype = None
+        getattr(L, pre + "detect").argtypes = [i32, vp, vp, vp, i32, f8, i32, i32, vp, vp, vp, i32, f8, i32, i32,
+                                               vp, i64, vp]
+        getattr(L, pre + "detect").restype = i64
+        for name in ("bf_solver",):
+            getattr(L, pre + name).argtypes = [vp] * 7
+        getattr(L, pre + "penalty_solver").argtypes = [vp] * 6 + [f8, vp, vp]
+        getattr(L, pre + "penalty_solver_iter").argtypes = [vp] * 6 + [f8, vp, vp]
+        getattr(L, pre + "gjk").argtypes = [vp, i32, vp, i32, vp, vp]
+        getattr(L, pre + "gjk").restype = f8
+        getattr(L, pre + "expmap").argtypes = [f8, f8, f8, vp]
+
+    # ---- pair list -------------------------------------------------------------
+    def pairs(self, method, a, b, max_error=0.0, nthreads=0, with_flags=True):
+        """a, b: float64 arrays of shape (9, n) (plane 3*vertex+coord).  Returns p, q, dist, flags."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        n = a.shape[1]
+        p = np.empty((3, n)); q = np.empty((3, n)); d = np.empty(n)
+        fl = np.zeros(n, np.uint8) if with_flags else None
+        getattr(self.lib, self.prefix + "pairs")(method, n, _p(a), _p(b), n, max_error, _p(p), _p(q), _p(d),
+                                                 _p(fl), nthreads)
+        return p, q, d, fl
+
+    # ---- particle pair -----------------------------------------------------------
+    def detect(self, driver, A, nA, epsA, fricA, idA, B, nB, epsB, fricB, idB, cap=None, stats=False):
+        """A, B: (3, 3*nT) float64 SoA-tri coordinates.  Returns (contacts, Stats|None)."""
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        cap = cap if cap is not None else max(1, nA * nB)
+        out = np.zeros(cap, CONTACT_DTYPE)
+        st = Stats() if stats else None
+        n = getattr(self.lib, self.prefix + "detect")(
+            driver, _p(A[0]), _p(A[1]), _p(A[2]), nA, epsA, int(fricA), idA,
+            _p(B[0]), _p(B[1]), _p(B[2]), nB, epsB, int(fricB), idB,
+            _p(out), cap, C.byref(st) if st is not None else None)
+        return out[: min(n, cap)], st
+
+    def expmap(self, o):
+        L = np.empty(9)
+        getattr(self.lib, self.prefix + "expmap")(float(o[0]), float(o[1]), float(o[2]), _p(L))
+        return L
+
+
+class Oracle(_Lib):
+    """The C restatement (liboracle.so)."""
+
+    prefix = "dor_"
+
+    def __init__(self, path: str | os.PathLike | None = None):
+        path = Path(path) if path else HERE / "liboracle.so"
+        if not _build_if_missing(path):
+            raise RuntimeError(f"oracle library missing: {path}")
+        self.lib = C.CDLL(str(path))
+        self._sig()
+        L = self.lib
+        vp, i32, i64, f8 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        L.dor_contacts_forces.argtypes = [vp, i64, f8, vp, vp, vp, f8, vp, vp, vp, f8, vp, vp, vp]
+        L.dor_update_rotation.argtypes = [vp, vp, vp, f8]
+        L.dor_update_angular.argtypes = [vp, vp, vp, vp, vp, f8]
+        L.dor_sim_create.restype = vp
+        L.dor_sim_destroy.argtypes = [vp]
+        L.dor_sim_run.argtypes = [vp, vp, vp, i32, vp]
+        L.dor_sim_run.restype = i64
+        L.dor_sim_contacts.argtypes = [vp, vp, i64]
+        L.dor_sim_contacts.restype = i64
+
+    def contacts_forces(self, contacts, sign, posA, angA, linA, mA, posB, angB, linB, mB, spring, damper, friction):
+        c = np.ascontiguousarray(contacts, CONTACT_DTYPE)
+        F = np.zeros(3); T = np.zeros(3)
+        mat = Material(spring, damper, friction)
+        arr = [np.ascontiguousarray(x, np.float64) for x in (posA, angA, linA, posB, angB, linB)]
+        self.lib.dor_contacts_forces(_p(c), len(c), sign, _p(arr[0]), _p(arr[1]), _p(arr[2]), mA,
+                                     _p(arr[3]), _p(arr[4]), _p(arr[5]), mB, C.byref(mat), _p(F), _p(T))
+        return F, T
+
+    def simulate(self, scene: dict, dt, gravity, spring, damper, friction, nsteps):
+        """Runs nsteps on a copy of `scene` (dict of numpy arrays, see delta_b200.scenarios).
+        Returns (new_scene_dict, contacts_per_step, final_contacts)."""
+        s = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in scene.items()}
+        sc = Scene()
+        sc.n_bodies = s["n_bodies"]
+        for name in ("tri_offset", "x", "y", "z", "rx", "ry", "rz", "pos", "ref_pos", "vel", "ang", "ref_ang",
+                     "rot", "inertia", "inverse", "mass", "eps", "radius", "friction", "obstacle"):
+            setattr(sc, name, s[name].ctypes.data)
+        prm = StepParams(dt, (C.c_double * 3)(*gravity), Material(spring, damper, friction))
+        cps = np.zeros(max(nsteps, 1), np.int64)
+        sim = self.lib.dor_sim_create()
+        try:
+            n = self.lib.dor_sim_run(sim, C.byref(sc), C.byref(prm), nsteps, _p(cps))
+            out = np.zeros(max(n, 1), CONTACT_DTYPE)
+            self.lib.dor_sim_contacts(sim, _p(out), len(out))
+        finally:
+            self.lib.dor_sim_destroy(sim)
+        return s, cps[:nsteps], out[:n]
+
+
+class Reference(_Lib):
+    """The reference's own functions (oracle/_ref), built by oracle/Makefile."""
+
+    prefix = "ref_"
+
+    def __init__(self, flavour: str = "par"):
+        name = "libdelta_ref.so" if flavour == "par" else "libdelta_ref_omp.so"
+        path = HERE / "_ref" / name
+        if not path.exists():
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(str(path))
+        self._sig()
+        L = self.lib
+        vp, i64, f8 = C.c_void_p, C.c_int64, C.c_double
+        L.ref_contacts_forces.argtypes = [vp, i64, vp, vp, vp, f8, vp, vp, vp, f8, vp, vp]
+        L.ref_update_rotation.argtypes = [vp, vp, vp, f8]
+        L.ref_update_angular.argtypes = [vp, vp, vp, vp, vp, f8]
+
+    @staticmethod
+    def available(flavour: str = "par") -> bool:
+        name = "libdelta_ref.so" if flavour == "par" else "libdelta_ref_omp.so"
+        return (HERE / "_ref" / name).exists()
+
+    def contacts_forces(self, contacts, posA, angA, linA, mA, posB, angB, linB, mB):
+        c = np.ascontiguousarray(contacts, CONTACT_DTYPE)
+        F = np.zeros(3); T = np.zeros(3)
+        arr = [np.array(x, np.float64) for x in (posA, angA, linA, posB, angB, linB)]
+        self.lib.ref_contacts_forces(_p(c), len(c), _p(arr[0]), _p(arr[1]), _p(arr[2]), mA,
+                                     _p(arr[3]), _p(arr[4]), _p(arr[5]), mB, _p(F), _p(T))
+        return F, T

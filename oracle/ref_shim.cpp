@@ -1,0 +1,221 @@
+// ref_shim.cpp -- extern "C" entry points over the reference's own hot-path functions.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file together with the
+// reference's sources (delta/contact/..., delta/dynamics/...) where they lie, into
+// oracle/_ref/.  The result pins the C restatement (delta_oracle.c) and serves as the
+// timed CPU baseline.  Nothing in the product path loads it.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "contact/contactpoint.h"
+#include "contact/detection/bf.h"
+#include "contact/detection/gjk.h"
+#include "contact/detection/hybrid.h"
+#include "contact/detection/penalty.h"
+#include "contact/forces/forces.h"
+#include "dynamics/dynamics.h"
+
+#include <thread>
+
+void expmap(iREAL, iREAL, iREAL, iREAL &, iREAL &, iREAL &, iREAL &, iREAL &, iREAL &, iREAL &, iREAL &,
+            iREAL &);
+
+namespace det = delta::contact::detection;
+
+extern "C" {
+
+// Same field order as dor_contact in delta_oracle.h.
+struct ref_contact {
+  double x[3], normal[3], depth, P[3], Q[3];
+  int32_t friction;
+  double eps_total;
+  int32_t master, slave, penetration, tri_a, tri_b;
+};
+
+struct ref_stats {
+  int64_t newton_hist[17];
+  int64_t penalty_fails, batch_fails, batch_size;
+  double batch_error;
+};
+
+void ref_bf_solver(const double *xA, const double *yA, const double *zA, const double *xB, const double *yB,
+                   const double *zB, double pq[6]) {
+  det::bfSolver(xA, yA, zA, xB, yB, zB, pq[0], pq[1], pq[2], pq[3], pq[4], pq[5]);
+}
+
+void ref_penalty_solver(const double *xA, const double *yA, const double *zA, const double *xB,
+                        const double *yB, const double *zB, double max_error, double pq[6], int32_t *failed) {
+  bool f = false;
+  det::penaltySolver(xA, yA, zA, xB, yB, zB, pq[0], pq[1], pq[2], pq[3], pq[4], pq[5], max_error, f);
+  *failed = f ? 1 : 0;
+}
+
+void ref_penalty_solver_iter(const double *xA, const double *yA, const double *zA, const double *xB,
+                             const double *yB, const double *zB, double max_error, double pq[6],
+                             int32_t *iterations) {
+  int it = *iterations;
+  det::penaltySolver(xA, yA, zA, xB, yB, zB, pq[0], pq[1], pq[2], pq[3], pq[4], pq[5], max_error, it);
+  *iterations = it;
+}
+
+double ref_gjk(const double *a, int32_t na, const double *b, int32_t nb, double p[3], double q[3]) {
+  return det::gjk(const_cast<double *>(a), na, const_cast<double *>(b), nb, p, q);
+}
+
+static inline double pq_dist(const double *pq) {
+  return std::sqrt(((pq[3] - pq[0]) * (pq[3] - pq[0])) + ((pq[4] - pq[1]) * (pq[4] - pq[1])) +
+                   ((pq[5] - pq[2]) * (pq[5] - pq[2])));
+}
+
+// Pair list: plane k = 3*vertex + coord, element i.  method: 0 bf, 1 penalty (4 it),
+// 2 penalty (<=16 it), 3 gjk(a,3,b,3), 4 per-pair hybrid (penalty, bf when failed).
+static void pairs_range(int32_t method, int64_t i0, int64_t i1, const double *a, const double *b, int64_t ld,
+                        double max_error, double *p, double *q, double *dist, uint8_t *flags) {
+  for (int64_t i = i0; i < i1; ++i) {
+    double xA[3], yA[3], zA[3], xB[3], yB[3], zB[3], pq[6];
+    for (int v = 0; v < 3; ++v) {
+      xA[v] = a[(3 * v + 0) * ld + i];
+      yA[v] = a[(3 * v + 1) * ld + i];
+      zA[v] = a[(3 * v + 2) * ld + i];
+      xB[v] = b[(3 * v + 0) * ld + i];
+      yB[v] = b[(3 * v + 1) * ld + i];
+      zB[v] = b[(3 * v + 2) * ld + i];
+    }
+    int32_t flag = 0;
+    if (method == 0) {
+      ref_bf_solver(xA, yA, zA, xB, yB, zB, pq);
+    } else if (method == 1) {
+      ref_penalty_solver(xA, yA, zA, xB, yB, zB, max_error, pq, &flag);
+    } else if (method == 2) {
+      ref_penalty_solver_iter(xA, yA, zA, xB, yB, zB, max_error, pq, &flag);
+    } else if (method == 3) {
+      double aa[9], bb[9];
+      for (int v = 0; v < 3; ++v) {
+        aa[3 * v] = xA[v]; aa[3 * v + 1] = yA[v]; aa[3 * v + 2] = zA[v];
+        bb[3 * v] = xB[v]; bb[3 * v + 1] = yB[v]; bb[3 * v + 2] = zB[v];
+      }
+      ref_gjk(aa, 3, bb, 3, pq, pq + 3);
+    } else {
+      ref_penalty_solver(xA, yA, zA, xB, yB, zB, max_error, pq, &flag);
+      if (flag) ref_bf_solver(xA, yA, zA, xB, yB, zB, pq);
+    }
+    for (int k = 0; k < 3; ++k) {
+      p[k * ld + i] = pq[k];
+      q[k * ld + i] = pq[3 + k];
+    }
+    dist[i] = pq_dist(pq);
+    if (flags) flags[i] = (uint8_t)flag;
+  }
+}
+
+// nthreads <= 0 uses every hardware thread; the pairs are split into equal static blocks.
+void ref_pairs(int32_t method, int64_t n, const double *a, const double *b, int64_t ld, double max_error,
+               double *p, double *q, double *dist, uint8_t *flags, int32_t nthreads) {
+  int64_t nt = nthreads > 0 ? nthreads : (int64_t)std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  if (nt > n) nt = n > 0 ? n : 1;
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < nt; ++t)
+    pool.emplace_back(pairs_range, method, n * t / nt, n * (t + 1) / nt, a, b, ld, max_error, p, q, dist, flags);
+  pairs_range(method, 0, n / nt, a, b, ld, max_error, p, q, dist, flags);
+  for (auto &th : pool) th.join();
+}
+
+// Particle-pair drivers.  driver: 0 bf, 1 penalty, 2 penaltyStat, 3 hybridWithPerBatchFallBack,
+// 4 hybridWithPerTriangleFallBack, 5 hybridBatchStat, 6 hybridTriangleStat.
+int64_t ref_detect(int32_t driver, const double *xA, const double *yA, const double *zA, int32_t nA, double epsA,
+                   int32_t fricA, int32_t idA, const double *xB, const double *yB, const double *zB, int32_t nB,
+                   double epsB, int32_t fricB, int32_t idB, ref_contact *out, int64_t cap, ref_stats *stats) {
+  std::vector<delta::contact::contactpoint> r;
+  if (stats) {
+    det::cleanPenaltyStatistics();
+    det::cleanHybridStatistics();
+  }
+  switch (driver) {
+    case 0: r = det::bf(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB); break;
+    case 1: r = det::penalty(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB); break;
+    case 2: r = det::penaltyStat(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB); break;
+    case 3:
+      r = det::hybridWithPerBatchFallBack(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB);
+      break;
+    case 4:
+      r = det::hybridWithPerTriangleFallBack(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB);
+      break;
+    case 5: r = det::hybridBatchStat(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB); break;
+    case 6: r = det::hybridTriangleStat(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB); break;
+    default: return -1;
+  }
+  if (stats) {
+    std::vector<int> h = det::getPenaltyIterationStatistics();
+    for (int i = 0; i < 17 && i < (int)h.size(); ++i) stats->newton_hist[i] = h[i];
+    stats->penalty_fails = det::getPenaltyFails();
+    stats->batch_fails = det::getBatchFails();
+    stats->batch_size = det::getBatchSize();
+    stats->batch_error = det::getBatchError();
+  }
+  const int64_t n = (int64_t)r.size();
+  for (int64_t i = 0; i < n && i < cap; ++i) {
+    const auto &c = r[i];
+    ref_contact &o = out[i];
+    std::memcpy(o.x, c.x, sizeof o.x);
+    std::memcpy(o.normal, c.normal, sizeof o.normal);
+    o.depth = c.depth;
+    std::memcpy(o.P, c.P, sizeof o.P);
+    std::memcpy(o.Q, c.Q, sizeof o.Q);
+    o.friction = c.friction ? 1 : 0;
+    o.eps_total = c.epsilonTotal;
+    o.master = c.master;
+    o.slave = c.slave;
+    o.penetration = c.penetration;
+    o.tri_a = -1;
+    o.tri_b = -1;
+  }
+  return n;
+}
+
+// getContactsForces (mesh path) over nc contacts given as ref_contact records; the
+// spring, damper and friction constants are the ones compiled into forces.cpp.
+void ref_contacts_forces(const ref_contact *cp, int64_t nc, double *posA, double *angA, double *linA, double massA,
+                         double *posB, double *angB, double *linB, double massB, double force[3],
+                         double torque[3]) {
+  std::vector<delta::contact::contactpoint> v((size_t)nc);
+  for (int64_t i = 0; i < nc; ++i) {
+    auto &c = v[i];
+    std::memcpy(c.x, cp[i].x, sizeof c.x);
+    std::memcpy(c.normal, cp[i].normal, sizeof c.normal);
+    c.depth = cp[i].depth;
+    std::memcpy(c.P, cp[i].P, sizeof c.P);
+    std::memcpy(c.Q, cp[i].Q, sizeof c.Q);
+    c.friction = cp[i].friction != 0;
+    c.epsilonTotal = cp[i].eps_total;
+    c.master = cp[i].master;
+    c.slave = cp[i].slave;
+    c.penetration = cp[i].penetration;
+  }
+  double refA[3] = {0, 0, 0}, refB[3] = {0, 0, 0}, refAngA[3] = {0, 0, 0}, refAngB[3] = {0, 0, 0};
+  double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  double RA[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, RB[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  delta::contact::forces::getContactsForces(v, posA, refA, angA, refAngA, linA, massA, I, RA, 0, posB, refB, angB,
+                                            refAngB, linB, massB, I, RB, 0, force, torque, false);
+}
+
+void ref_expmap(double o1, double o2, double o3, double L[9]) {
+  expmap(o1, o2, o3, L[0], L[1], L[2], L[3], L[4], L[5], L[6], L[7], L[8]);
+}
+
+void ref_update_rotation(double ang[3], double ref_ang[3], double rot[9], double step) {
+  delta::dynamics::updateRotationMatrix(ang, ref_ang, rot, step);
+}
+
+void ref_update_angular(double ref_ang[3], double rot[9], double inertia[9], double inverse[9], double torque[3],
+                        double step) {
+  delta::dynamics::updateAngular(ref_ang, rot, inertia, inverse, torque, step);
+}
+
+void ref_update_vertex(double *x, double *y, double *z, double *rx, double *ry, double *rz, double rot[9],
+                       double pos[3], double ref_pos[3]) {
+  delta::dynamics::updateVertices(x, y, z, rx, ry, rz, rot, pos, ref_pos);
+}
+
+}  // extern "C"
