@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 contact narrowphase (one JSON line on rank 0).
+
+Workload: the narrowphase microbenchmark, 2^24 independent triangle pairs (triangle A
+~ U[0,1]^3, B a rotated triangle with edges U(0.05,1) at lognormal(ln 1e-3, 2)
+separation, 10% near-parallel, 5% intersecting), FP64 coordinates resident in HBM.
+A step is one pass of the narrowphase over the 2^24 pairs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Ours: the headline method (default bf_cert: FP32 feature filter + FP64 finishing, whose
+results equal FP64 bfSolver bit for bit) timed with CUDA events; the plain FP64 bf kernel
+is timed beside it on the same pairs.  `e2e` goes through the C ABI's host-buffer entry
+point (delta_pairs_run_host) with pinned host inputs, copies included.
+Reference: the reference's own bfSolver (oracle/_ref, compiled from its sources) over a
+bounded sample of the same pairs on all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "triangle-pair tests/sec and timesteps/sec at 1 B200: learned+FP32 vs plain FP64 at equal contacts"
+BYTES_PER_PAIR = 144 + 56 + 1  # FP64 in (18 doubles) + out (P, Q, dist) + 1 flag byte
+FLOPS_BF = 1214  # algorithmic FP ops of bfSolver per pair (747 add, 439 mul, 13 div, 15 sqrt)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--method", default="bf_cert")
+    ap.add_argument("--pairs-log2", type=int, default=24)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(n):
+    return {
+        "workload": "narrowphase microbenchmark: independent triangle pairs, lognormal(ln 1e-3, 2) separation, "
+                    "10% near-parallel, 5% intersecting, FP64 coordinates",
+        "pairs_per_gpu": n,
+        "l2": "inputs larger than L2 (144 B/pair FP64 in HBM), no flush",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str, n: int):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, scaled to n pairs."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        t = json.loads(p.read_text())[kernel]
+        return float(t["dram_bytes_per_pair"]) * n
+    except (KeyError, ValueError):
+        return None
+
+
+def cpu_reference_rate(a, b, sample: int, min_seconds: float):
+    """The reference's bfSolver (oracle/_ref, or the oracle port when absent) over `sample`
+    pairs on all host threads; repeated until min_seconds.  Returns (pairs/s, cores, kind)."""
+    from oracle.oracle import Oracle, Reference
+
+    cores = os.cpu_count() or 1
+    if Reference.available("omp"):
+        lib, kind = Reference("omp"), "reference"
+    else:
+        lib, kind = Oracle(), "port"
+    a_s = np.ascontiguousarray(a[:, :sample]); b_s = np.ascontiguousarray(b[:, :sample])
+    lib.pairs(0, a_s[:, :1024], b_s[:, :1024], nthreads=cores)  # warm-up
+    done, t0 = 0, time.perf_counter()
+    while True:
+        lib.pairs(0, a_s, b_s, nthreads=cores, with_flags=False)
+        done += sample
+        el = time.perf_counter() - t0
+        if el >= min_seconds:
+            break
+    return done / el, cores, kind
+
+
+def run_reference(args, rank, world):
+    n = 1 << args.pairs_log2
+    if rank != 0:
+        return
+    from delta_b200.scenarios import narrowphase_pairs_chunked
+
+    sample = min(n, 1 << 22)
+    a, b, _, _ = narrowphase_pairs_chunked(sample, seed=args.seed)
+    from oracle.oracle import Oracle, Reference
+
+    cores = os.cpu_count() or 1
+    lib, kind = (Reference("omp"), "reference") if Reference.available("omp") else (Oracle(), "port")
+    for _ in range(args.warmup):
+        lib.pairs(0, a, b, nthreads=cores, with_flags=False)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        lib.pairs(0, a, b, nthreads=cores, with_flags=False)
+    el = time.perf_counter() - t0
+    rate = sample * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {**workload_config(n), "method": "reference bfSolver (FP64, CPU)"},
+        "cpu_baseline": {"value": rate, "unit": "pairs/s", "cores": cores, "kind": kind,
+                         "sample": f"{sample} pairs of the workload per step, bfSolver FP64 on {cores} threads"},
+        "e2e": {"value": rate, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    n = 1 << args.pairs_log2
+    # host-side generation first (spawned pool, before any CUDA initialisation)
+    from delta_b200.scenarios import narrowphase_pairs_chunked
+
+    a_np, b_np, _, _ = narrowphase_pairs_chunked(n, seed=args.seed + 7919 * rank)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from delta_b200.narrowphase import METHODS, Context, pairs_device, pairs_host
+
+    method = METHODS[args.method]
+    stream = torch.cuda.current_stream()
+    ctx = Context(local, stream.cuda_stream)
+    a = torch.from_numpy(a_np).cuda()
+    b = torch.from_numpy(b_np).cuda()
+    out = (torch.empty((3, n), dtype=torch.float64, device="cuda"), torch.empty((3, n), dtype=torch.float64,
+                                                                                device="cuda"),
+           torch.empty(n, dtype=torch.float64, device="cuda"), torch.empty(n, dtype=torch.uint8, device="cuda"))
+    out64 = tuple(torch.empty_like(x) for x in out)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(meth, outs, steps, warmup):
+        for _ in range(warmup):
+            pairs_device(ctx, meth, a, b, out=outs)
+        barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        l0 = ctx.launches
+        ev[0].record(stream)
+        for i in range(steps):
+            pairs_device(ctx, meth, a, b, out=outs)
+            ev[i + 1].record(stream)
+        barrier()
+        per = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+        total = ev[0].elapsed_time(ev[steps])
+        return total, per, ctx.launches - l0
+
+    peak, peak_kind = measured_peak_hbm()
+    with ClockSampler(local) as clk:
+        total_ms, per_ms, launches = timed(method, out, args.steps, args.warmup)
+    # the plain FP64 bf kernel on the same pairs (comparison arm, not the headline)
+    total64_ms, per64_ms, launches64 = timed(0, out64, max(3, args.steps // 2), 2)
+
+    t = torch.tensor([total_ms, total64_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, total64_ms = t.tolist()
+    steps64 = max(3, args.steps // 2)
+    value = world * n * args.steps / (total_ms / 1e3)
+    value64 = world * n * steps64 / (total64_ms / 1e3)
+
+    # parity of the headline method against plain FP64 bf on this rank's pairs
+    torch.cuda.synchronize()
+    diff = ((out[0] != out64[0]).any(0) | (out[1] != out64[1]).any(0) | (out[2] != out64[2])).sum().item()
+    rel = ((out[2] - out64[2]).abs() / out64[2].clamp_min(1e-300)).max().item()
+    mean_evals = out[3].double().mean().item() if method == 5 else None
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        ha = torch.from_numpy(a_np).pin_memory().numpy()
+        hb = torch.from_numpy(b_np).pin_memory().numpy()
+        hp = torch.empty((3, n), dtype=torch.float64).pin_memory().numpy()
+        hq = torch.empty((3, n), dtype=torch.float64).pin_memory().numpy()
+        hd = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        hf = torch.empty(n, dtype=torch.uint8).pin_memory().numpy()
+        pairs_host(ctx, method, ha, hb, out=(hp, hq, hd, hf))  # warm-up (allocates scratch)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            pairs_host(ctx, method, ha, hb, out=(hp, hq, hd, hf))
+        barrier()
+        el = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(el, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * n * args.e2e_steps / el.item(), "unit": "pairs/s",
+               "h2d_bytes_per_step": int(ha.nbytes + hb.nbytes),
+               "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes),
+               "path": "delta_pairs_run_host (C ABI), pinned host buffers, copies in the timed region"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, kind = cpu_reference_rate(a_np, b_np, sample=min(n, 1 << 22), min_seconds=10.0)
+        cpu = {"value": rate, "unit": "pairs/s", "cores": cores, "kind": kind,
+               "sample": f"{min(n, 1 << 22)} pairs of the workload, reference bfSolver FP64, repeated >= 10 s"}
+
+    if rank == 0:
+        kern_ms = float(np.mean(per_ms))
+        achieved = BYTES_PER_PAIR * n / (kern_ms / 1e3) / 1e9
+        kname = f"k_pairs<{args.method}>"
+        traffic = profiled_traffic(args.method, n)
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {**workload_config(n), "method": args.method,
+                       "comparison": "plain FP64 bf kernel on the same pairs"},
+            "fp64_bf": {"value": value64, "unit": "pairs/s", "ms_per_step": total64_ms / steps64},
+            "speedup_vs_fp64_bf": value / value64,
+            "parity_vs_fp64_bf": {"pairs_differing": int(diff), "max_rel_dist_err": rel,
+                                  "mean_fp64_feature_evals": mean_evals},
+            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": BYTES_PER_PAIR * n,
+                         "fp64_equiv_tflops": FLOPS_BF * n / (kern_ms / 1e3) / 1e12},
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,69 @@
+"""ctypes binding of libdelta_b200.so (the C ABI declared in include/delta_b200.h).
+
+The library is required: every compute entry point goes through it and raises when it
+is missing; there is no CPU fallback.  Build it with ``make -C delta_b200``
+(``__graft_entry__.build()`` does this).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libdelta_b200.so"
+HEADER = HERE.parent / "include" / "delta_b200.h"
+
+OK, ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED = range(7)
+STATUS_NAMES = ["OK", "INVALID", "CUDA", "CAPACITY", "TIMEOUT", "NOMEM", "UNSUPPORTED"]
+
+vp, i32, i64, f8 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+
+# argument types of every exported function (restype int = delta_status unless listed)
+SIGNATURES: dict[str, tuple[list, object]] = {
+    "delta_create": ([C.POINTER(vp), C.c_int, vp], C.c_int),
+    "delta_destroy": ([vp], C.c_int),
+    "delta_set_stream": ([vp, vp], C.c_int),
+    "delta_synchronize": ([vp], C.c_int),
+    "delta_last_error": ([], C.c_char_p),
+    "delta_version": ([], C.c_char_p),
+    "delta_launch_count": ([vp], i64),
+    "delta_pairs_run": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp], C.c_int),
+    "delta_pairs_run_host": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp], C.c_int),
+}
+
+
+class DeltaError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"delta_b200: {name}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def header_functions() -> list[str]:
+    """Names of the functions include/delta_b200.h declares."""
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"\b(delta_\w+)\s*\(", text)))
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built (run `make -C {HERE}`); there is no CPU fallback")
+    L = C.CDLL(str(LIB_PATH))
+    for name, (args, res) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(status: int):
+    if status != OK:
+        raise DeltaError(status, lib().delta_last_error().decode(errors="replace"))

@@ -1,0 +1,171 @@
+// capi.cu -- context management and the pair-list entry points of the C ABI.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "internal.h"
+
+namespace delta {
+
+static thread_local std::string g_last_error;
+
+delta_status set_error(delta_status st, const std::string &msg) {
+  g_last_error = msg;
+  return st;
+}
+
+delta_status cuda_error(cudaError_t e, const char *where) {
+  if (e == cudaSuccess) return DELTA_OK;
+  return set_error(e == cudaErrorMemoryAllocation ? DELTA_ERR_NOMEM : DELTA_ERR_CUDA,
+                   std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+delta_status ctx_scratch(delta_ctx *ctx, int slot, size_t bytes, void **out) {
+  delta_buffer &b = ctx->scratch[slot];
+  if (b.bytes < bytes) {
+    if (b.ptr) {
+      cudaError_t e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) return cuda_error(e, "scratch sync");
+      cudaFree(b.ptr);
+      b.ptr = nullptr;
+      b.bytes = 0;
+    }
+    size_t want = bytes + bytes / 4 + 256;
+    cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) return cuda_error(e, "scratch cudaMalloc");
+    b.bytes = want;
+  }
+  *out = b.ptr;
+  return DELTA_OK;
+}
+
+delta_status ctx_pinned(delta_ctx *ctx, size_t bytes, void **out) {
+  if (ctx->pinned_bytes < bytes) {
+    if (ctx->pinned) {
+      cudaError_t e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) return cuda_error(e, "pinned sync");
+      cudaFreeHost(ctx->pinned);
+      ctx->pinned = nullptr;
+      ctx->pinned_bytes = 0;
+    }
+    cudaError_t e = cudaMallocHost(&ctx->pinned, bytes);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMallocHost");
+    ctx->pinned_bytes = bytes;
+  }
+  *out = ctx->pinned;
+  return DELTA_OK;
+}
+
+}  // namespace delta
+
+using namespace delta;
+
+extern "C" {
+
+const char *delta_last_error(void) { return g_last_error.c_str(); }
+const char *delta_version(void) { return "delta_b200 0.1 (sm_100a)"; }
+
+delta_status delta_create(delta_ctx **out, int device, void *stream) {
+  if (!out) return set_error(DELTA_ERR_INVALID, "delta_create: null output");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= n) return set_error(DELTA_ERR_INVALID, "delta_create: bad device");
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+  delta_ctx *c = new delta_ctx();
+  c->device = device;
+  c->stream = (cudaStream_t)stream;
+  *out = c;
+  return DELTA_OK;
+}
+
+delta_status delta_destroy(delta_ctx *ctx) {
+  if (!ctx) return DELTA_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto &b : ctx->scratch)
+    if (b.ptr) cudaFree(b.ptr);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  delete ctx;
+  return DELTA_OK;
+}
+
+delta_status delta_set_stream(delta_ctx *ctx, void *stream) {
+  if (!ctx) return set_error(DELTA_ERR_INVALID, "null context");
+  ctx->stream = (cudaStream_t)stream;
+  return DELTA_OK;
+}
+
+delta_status delta_synchronize(delta_ctx *ctx) {
+  if (!ctx) return set_error(DELTA_ERR_INVALID, "null context");
+  return cuda_error(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+}
+
+int64_t delta_launch_count(const delta_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+static delta_status check_pairs(delta_ctx *ctx, int method, int precision, int64_t n, const void *a, const void *b,
+                                int64_t ld, const void *p, const void *q, const void *dist) {
+  if (!ctx) return set_error(DELTA_ERR_INVALID, "null context");
+  if (method < DELTA_BF || method > DELTA_BF_CERT) return set_error(DELTA_ERR_INVALID, "unknown method");
+  if (precision != DELTA_F64 && precision != DELTA_F32) return set_error(DELTA_ERR_INVALID, "unknown precision");
+  if (n < 0 || ld < n) return set_error(DELTA_ERR_INVALID, "need 0 <= n <= ld");
+  if (n > 0 && (!a || !b || !p || !q || !dist)) return set_error(DELTA_ERR_INVALID, "null buffer");
+  return DELTA_OK;
+}
+
+delta_status delta_pairs_run(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
+                             const double *b, int64_t ld, double max_error, double *p, double *q, double *dist,
+                             uint8_t *flags) {
+  delta_status st = check_pairs(ctx, method, precision, n, a, b, ld, p, q, dist);
+  if (st != DELTA_OK || n == 0) return st;
+  cudaError_t e = launch_pairs(method, precision, ctx->stream, n, a, b, ld, max_error, p, q, dist, flags);
+  if (e != cudaSuccess) return cuda_error(e, "pairs kernel launch");
+  ctx->launches += 1;
+  return DELTA_OK;
+}
+
+delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
+                                  const double *b, int64_t ld, double max_error, double *p, double *q, double *dist,
+                                  uint8_t *flags) {
+  delta_status st = check_pairs(ctx, method, precision, n, a, b, ld, p, q, dist);
+  if (st != DELTA_OK || n == 0) return st;
+  // device layout: a(9n) b(9n) p(3n) q(3n) dist(n) | flags(n)
+  const size_t nd = (size_t)n;
+  void *buf = nullptr, *fbuf = nullptr;
+  if ((st = ctx_scratch(ctx, 0, sizeof(double) * 25 * nd, &buf)) != DELTA_OK) return st;
+  if ((st = ctx_scratch(ctx, 1, nd, &fbuf)) != DELTA_OK) return st;
+  double *da = (double *)buf, *db = da + 9 * nd, *dp = db + 9 * nd, *dq = dp + 3 * nd, *dd = dq + 3 * nd;
+  uint8_t *df = (uint8_t *)fbuf;
+  cudaError_t e = cudaSuccess;
+  if (ld == n) {
+    e = cudaMemcpyAsync(da, a, sizeof(double) * 9 * nd, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, b, sizeof(double) * 9 * nd, cudaMemcpyHostToDevice, ctx->stream);
+  } else {
+    e = cudaMemcpy2DAsync(da, sizeof(double) * nd, a, sizeof(double) * ld, sizeof(double) * nd, 9,
+                          cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(db, sizeof(double) * nd, b, sizeof(double) * ld, sizeof(double) * nd, 9,
+                            cudaMemcpyHostToDevice, ctx->stream);
+  }
+  if (e != cudaSuccess) return cuda_error(e, "pairs H2D");
+  e = launch_pairs(method, precision, ctx->stream, n, da, db, n, max_error, dp, dq, dd, flags ? df : nullptr);
+  if (e != cudaSuccess) return cuda_error(e, "pairs kernel launch");
+  ctx->launches += 1;
+  if (ld == n) {
+    e = cudaMemcpyAsync(p, dp, sizeof(double) * 3 * nd, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q, dq, sizeof(double) * 3 * nd, cudaMemcpyDeviceToHost, ctx->stream);
+  } else {
+    e = cudaMemcpy2DAsync(p, sizeof(double) * ld, dp, sizeof(double) * nd, sizeof(double) * nd, 3,
+                          cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(q, sizeof(double) * ld, dq, sizeof(double) * nd, sizeof(double) * nd, 3,
+                            cudaMemcpyDeviceToHost, ctx->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dist, dd, sizeof(double) * nd, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && flags) e = cudaMemcpyAsync(flags, df, nd, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "pairs D2H");
+  return cuda_error(cudaStreamSynchronize(ctx->stream), "pairs sync");
+}
+
+}  // extern "C"

@@ -1,0 +1,43 @@
+// internal.h -- declarations shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "delta_b200.h"
+
+namespace delta {
+
+constexpr int kNumSMs = 148;  // B200
+
+// Pair-list launcher (pairs.cu).
+cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
+                         int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags);
+
+// Thread-local last-error text (capi.cu).
+delta_status set_error(delta_status st, const std::string &msg);
+delta_status cuda_error(cudaError_t e, const char *where);
+
+}  // namespace delta
+
+// Device buffer owned by a context; grows on demand, never shrinks.
+struct delta_buffer {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct delta_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+  delta_buffer scratch[8];
+  void *pinned = nullptr;
+  size_t pinned_bytes = 0;
+};
+
+namespace delta {
+// Returns a device buffer of at least `bytes` in slot `slot` of the context.
+delta_status ctx_scratch(delta_ctx *ctx, int slot, size_t bytes, void **out);
+delta_status ctx_pinned(delta_ctx *ctx, size_t bytes, void **out);
+}  // namespace delta

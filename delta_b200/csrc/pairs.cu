@@ -1,0 +1,109 @@
+// pairs.cu -- pair-list narrowphase kernels (one thread per triangle pair).
+//
+// Input planes a[9*ld], b[9*ld] (plane 3*vertex+coord), outputs p[3*ld], q[3*ld],
+// dist[n], flags[n].  Every warp reads 18 consecutive 256-byte segments, one per plane,
+// and writes 7 more, so the loads and stores are fully coalesced.  Replaces the
+// per-pair loops of bf()/penalty() (bf.cpp:95-118, penalty.cpp:187-210) and the SIMD
+// pair-list kernels ispc_bf / ispc_pen (bf.ispc:3, penalty.ispc:154).
+#include "internal.h"
+#include "tri_cert.cuh"
+#include "tri_gjk.cuh"
+#include "tri_ref.cuh"
+
+namespace delta {
+
+enum { M_BF = 0, M_PENALTY = 1, M_PENALTY_ITER = 2, M_GJK = 3, M_HYBRID_PAIR = 4, M_BF_CERT = 5 };
+
+template <class R, int M>
+__global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
+                                               int64_t ld, double max_error, double *__restrict__ p,
+                                               double *__restrict__ q, double *__restrict__ dist,
+                                               uint8_t *__restrict__ flags) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double A64[3][3], B64[3][3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        A64[v][k] = __ldg(a + (3 * v + k) * ld + i);
+        B64[v][k] = __ldg(b + (3 * v + k) * ld + i);
+      }
+    double out[6], d;
+    int flag = 0;
+    if constexpr (M == M_BF_CERT) {
+      flag = bf_cert(A64, B64, out);
+      xf64 pq[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) pq[k] = xf64(out[k]);
+      d = pq_distance(pq).v;
+    } else {
+      R A[3][3], B[3][3];
+#pragma unroll
+      for (int v = 0; v < 3; ++v)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          A[v][k] = from_f64<R>(A64[v][k]);
+          B[v][k] = from_f64<R>(B64[v][k]);
+        }
+      R pq[6];
+      const R me = from_f64<R>(max_error);
+      if constexpr (M == M_BF) {
+        bf_solve_ref(A, B, pq);
+      } else if constexpr (M == M_PENALTY) {
+        penalty_ref(A, B, me, false, pq, flag);
+      } else if constexpr (M == M_PENALTY_ITER) {
+        penalty_ref(A, B, me, true, pq, flag);
+      } else if constexpr (M == M_GJK) {
+        gjk_ref(A, B, pq);
+      } else {  // per-pair hybrid: penalty, bf when the pair reports failure
+        penalty_ref(A, B, me, false, pq, flag);
+        if (flag) bf_solve_ref(A, B, pq);
+      }
+#pragma unroll
+      for (int k = 0; k < 6; ++k) out[k] = to_f64(pq[k]);
+      d = to_f64(pq_distance(pq));
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      p[k * ld + i] = out[k];
+      q[k * ld + i] = out[3 + k];
+    }
+    dist[i] = d;
+    if (flags) flags[i] = (uint8_t)flag;
+  }
+}
+
+template <class R, int M>
+static cudaError_t launch_one(cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld, double me,
+                              double *p, double *q, double *dist, uint8_t *flags) {
+  const int threads = 256;
+  int64_t blocks = (n + threads - 1) / threads;
+  const int64_t cap = (int64_t)kNumSMs * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  k_pairs<R, M><<<(unsigned)blocks, threads, 0, s>>>(n, a, b, ld, me, p, q, dist, flags);
+  return cudaGetLastError();
+}
+
+template <class R>
+static cudaError_t launch_prec(int method, cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld,
+                               double me, double *p, double *q, double *dist, uint8_t *flags) {
+  switch (method) {
+    case M_BF: return launch_one<R, M_BF>(s, n, a, b, ld, me, p, q, dist, flags);
+    case M_PENALTY: return launch_one<R, M_PENALTY>(s, n, a, b, ld, me, p, q, dist, flags);
+    case M_PENALTY_ITER: return launch_one<R, M_PENALTY_ITER>(s, n, a, b, ld, me, p, q, dist, flags);
+    case M_GJK: return launch_one<R, M_GJK>(s, n, a, b, ld, me, p, q, dist, flags);
+    case M_HYBRID_PAIR: return launch_one<R, M_HYBRID_PAIR>(s, n, a, b, ld, me, p, q, dist, flags);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
+                         int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags) {
+  if (method == M_BF_CERT) return launch_one<xf64, M_BF_CERT>(s, n, a, b, ld, max_error, p, q, dist, flags);
+  if (precision == 0) return launch_prec<xf64>(method, s, n, a, b, ld, max_error, p, q, dist, flags);
+  return launch_prec<float>(method, s, n, a, b, ld, max_error, p, q, dist, flags);
+}
+
+}  // namespace delta

@@ -1,0 +1,103 @@
+/*
+ * delta_b200.h -- C ABI of the B200 contact pipeline for triangulated particles.
+ *
+ * Plain pointers and sizes only.  Unless a function name ends in _host, every array
+ * argument is a device pointer on the context's device; the caller owns all buffers.
+ * Every call is asynchronous on the context's stream unless stated otherwise, and
+ * returns a delta_status.  delta_last_error() gives a one-line description of the last
+ * failure on the calling thread.
+ *
+ * Layouts
+ *   pair list : a, b hold 9 planes of ld doubles; plane k = 3*vertex + coord, entry i
+ *               is triangle pair i (the SoA pair-list shape of ispc_bf / ispc_pen,
+ *               delta/contact/detection/bf.ispc:3, penalty.ispc:154).
+ *               p, q hold 3 planes of ld doubles (closest points on A and on B).
+ *   SoA-tri   : x, y, z hold 3 entries per triangle; triangle t of body i sits at
+ *               3*(tri_offset[i]+t) .. +2 (ParticleRecord _xCoordinates; the argument
+ *               shape of delta::contact::detection::bf, bf.h:65-81).
+ */
+#ifndef DELTA_B200_H
+#define DELTA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DELTA_OK = 0,
+  DELTA_ERR_INVALID = 1,     /* bad argument (null pointer, negative size, unknown method) */
+  DELTA_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  DELTA_ERR_CAPACITY = 3,    /* an output buffer is too small; the needed size is returned */
+  DELTA_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  DELTA_ERR_NOMEM = 5,       /* device or pinned-host allocation failed */
+  DELTA_ERR_UNSUPPORTED = 6  /* method/precision combination not built */
+} delta_status;
+
+/* Narrowphase methods. */
+typedef enum {
+  DELTA_BF = 0,            /* bfSolver, bf.cpp:217-1178: exact 9 edge-edge + 6 vertex-face */
+  DELTA_PENALTY = 1,       /* penaltySolver(..., MaxError, bool& failed), penalty.cpp:278-432 */
+  DELTA_PENALTY_ITER = 2,  /* penaltySolver(..., maxError, int& iterations), penalty.cpp:434-582 */
+  DELTA_GJK = 3,           /* gjk(a,3,b,3,p,q), gjk.cpp:418-460 */
+  DELTA_HYBRID_PAIR = 4,   /* penalty, bf when it reports failure (per pair) */
+  DELTA_BF_CERT = 5        /* FP32 feature filter + FP64 evaluation of the certified
+                              candidate features; equal to DELTA_BF in FP64 */
+} delta_method;
+
+typedef enum {
+  DELTA_F64 = 0,  /* reference arithmetic in FP64, no FMA contraction */
+  DELTA_F32 = 1   /* the same algorithm in FP32 (the reference's iREAL=float build) */
+} delta_precision;
+
+/* Particle-pair drivers (the functions Collision::collisionDetection switches over,
+ * multiscale/dem/mappings/Collision.cpp:342-645). */
+typedef enum {
+  DELTA_DRV_BF = 0,                /* bf(),                          bf.cpp:47-148      */
+  DELTA_DRV_PENALTY = 1,           /* penalty(),                     penalty.cpp:133-275 */
+  DELTA_DRV_PENALTY_STAT = 2,      /* penaltyStat(),                 penalty.cpp:50-110  */
+  DELTA_DRV_HYBRID_BATCH = 3,      /* hybridWithPerBatchFallBack(),  hybrid.cpp:357-487  */
+  DELTA_DRV_HYBRID_TRIANGLE = 4,   /* hybridWithPerTriangleFallBack, hybrid.cpp:78-200   */
+  DELTA_DRV_HYBRID_BATCH_STAT = 5, /* hybridBatchStat(),             hybrid.cpp:489-628  */
+  DELTA_DRV_HYBRID_TRI_STAT = 6,   /* hybridTriangleStat(),          hybrid.cpp:202-336  */
+  DELTA_DRV_GJK = 7,               /* gjk per triangle pair with bf()'s contact rule     */
+  DELTA_DRV_BF_CERT = 8            /* bf() contact set computed with DELTA_BF_CERT        */
+} delta_driver;
+
+typedef struct delta_ctx delta_ctx;
+
+/* ---- context ---------------------------------------------------------------------- */
+/* stream: a cudaStream_t (NULL = the legacy default stream).  The context owns its
+ * scratch buffers and pinned staging memory. */
+delta_status delta_create(delta_ctx **ctx, int device, void *stream);
+delta_status delta_destroy(delta_ctx *ctx);
+delta_status delta_set_stream(delta_ctx *ctx, void *stream);
+delta_status delta_synchronize(delta_ctx *ctx);
+const char *delta_last_error(void);
+const char *delta_version(void);
+/* Number of kernel launches the library issued on this context so far. */
+int64_t delta_launch_count(const delta_ctx *ctx);
+
+/* ---- pair list -------------------------------------------------------------------- */
+/* Closest points and distance for n independent triangle pairs.  max_error is the
+ * penalty tolerance (the reference passes (epsA+epsB)/16).  flags (may be NULL):
+ * PENALTY -> failed (0/1); PENALTY_ITER -> iterations on early exit, else 0;
+ * HYBRID_PAIR -> 1 where bf ran; BF_CERT -> number of features evaluated in FP64;
+ * BF/GJK -> 0.  Replaces the per-pair loops of bf()/penalty() (bf.cpp:95-118,
+ * penalty.cpp:187-210) and ispc_bf / ispc_pen. */
+delta_status delta_pairs_run(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
+                             const double *b, int64_t ld, double max_error, double *p, double *q,
+                             double *dist, uint8_t *flags);
+
+/* Same with host buffers: copies the inputs to the device, runs, copies the results
+ * back and synchronises.  Large host buffers are staged through pinned memory. */
+delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
+                                  const double *b, int64_t ld, double max_error, double *p, double *q,
+                                  double *dist, uint8_t *flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,124 @@
+"""Pair-list kernels (libdelta_b200.so on the GPU) against the oracle.
+
+FP64 methods reproduce the reference arithmetic and must match bit for bit.  BF_CERT
+(FP32 filter, FP64 finish) must equal FP64 bf bit for bit.  FP32 methods are checked
+against FP64 with the tolerances written in each test.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+METHODS = {"bf": 0, "penalty": 1, "penalty_iter": 2, "gjk": 3, "hybrid": 4}
+MAX_ERR = 1e-3
+
+
+@pytest.fixture(scope="module")
+def workload():
+    from delta_b200.scenarios import narrowphase_pairs
+    from tests.golden.make_golden import edge_case_pairs
+
+    a, b, d, cls = narrowphase_pairs(1 << 16, seed=1234)
+    ea, eb = edge_case_pairs()
+    return np.concatenate([a, ea], 1), np.concatenate([b, eb], 1)
+
+
+def _dev(x):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def _run(ctx, method, a, b, precision=0):
+    from delta_b200.narrowphase import pairs_device
+
+    p, q, d, fl = pairs_device(ctx, method, _dev(a), _dev(b), precision=precision, max_error=MAX_ERR)
+    ctx.synchronize()
+    return p.cpu().numpy(), q.cpu().numpy(), d.cpu().numpy(), fl.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", list(METHODS))
+def test_f64_methods_bit_exact_vs_oracle(ctx, oracle, workload, name):
+    a, b = workload
+    m = METHODS[name]
+    gp, gq, gd, gf = _run(ctx, m, a, b)
+    op, oq, od, of = oracle.pairs(m, a, b, max_error=MAX_ERR)
+    bad = np.flatnonzero((gp != op).any(0) | (gq != oq).any(0) | (gd != od))
+    assert bad.size == 0, f"{bad.size} pairs differ, first {bad[:5]}"
+    assert np.array_equal(gf, of)
+
+
+@pytest.mark.parametrize("name", list(METHODS))
+def test_f64_methods_match_golden(ctx, golden, name):
+    g = golden["pairs"]
+    gp, gq, gd, gf = _run(ctx, METHODS[name], g["a"], g["b"])
+    assert np.array_equal(gp, g[f"{name}_p"]) and np.array_equal(gq, g[f"{name}_q"])
+    assert np.array_equal(gd, g[f"{name}_d"]) and np.array_equal(gf, g[f"{name}_flags"])
+
+
+def test_bf_cert_equals_f64_bf(ctx, oracle, workload):
+    a, b = workload
+    gp, gq, gd, ev = _run(ctx, 5, a, b)
+    op, oq, od, _ = oracle.pairs(0, a, b)
+    bad = np.flatnonzero((gp != op).any(0) | (gq != oq).any(0) | (gd != od))
+    assert bad.size == 0, f"{bad.size} pairs differ, first {bad[:5]}"
+    assert ev.min() >= 1 and ev.max() <= 15
+
+
+def test_f32_bf_close_to_f64(ctx, oracle, workload):
+    """FP32 bfSolver (the reference's iREAL=float build): |d32 - d64| <= 1e-5 * (1 + d64)
+    for every pair (coordinates are O(1))."""
+    a, b = workload
+    _, _, d32, _ = _run(ctx, 0, a, b, precision=1)
+    _, _, d64, _ = oracle.pairs(0, a, b)
+    err = np.abs(d32 - d64)
+    assert np.all(np.isfinite(d32))
+    assert np.all(err <= 1e-5 * (1 + d64)), err.max()
+
+
+def test_f32_penalty_and_gjk_finite(ctx, workload):
+    a, b = workload
+    for m in (1, 2, 3, 4):
+        _, _, d, _ = _run(ctx, m, a, b, precision=1)
+        assert np.isfinite(d).mean() > 0.99
+
+
+def test_host_path_equals_device_path(ctx, workload):
+    from delta_b200.narrowphase import pairs_host
+
+    a, b = workload
+    hp, hq, hd, hf = pairs_host(ctx, 0, a, b, max_error=MAX_ERR)
+    gp, gq, gd, gf = _run(ctx, 0, a, b)
+    assert np.array_equal(hp, gp) and np.array_equal(hq, gq) and np.array_equal(hd, gd)
+
+
+def test_padded_leading_dimension(ctx, oracle, workload):
+    """ld > n: the planes are strided; entries past n are untouched."""
+    import ctypes
+    import torch
+
+    from delta_b200._lib import check, lib
+
+    a, b = workload
+    n, ld = 1000, 1536
+    A = torch.zeros((9, ld), dtype=torch.float64, device="cuda")
+    B = torch.zeros_like(A)
+    A[:, :n] = _dev(a[:, :n]); B[:, :n] = _dev(b[:, :n])
+    P = torch.full((3, ld), 7.0, dtype=torch.float64, device="cuda"); Q = P.clone()
+    D = torch.full((ld,), 7.0, dtype=torch.float64, device="cuda")
+    check(lib().delta_pairs_run(ctx.handle, 0, 0, n, A.data_ptr(), B.data_ptr(), ld, 0.0, P.data_ptr(),
+                                Q.data_ptr(), D.data_ptr(), None))
+    ctx.synchronize()
+    op, oq, od, _ = oracle.pairs(0, a[:, :n], b[:, :n])
+    assert np.array_equal(P[:, :n].cpu().numpy(), op) and np.array_equal(D[:n].cpu().numpy(), od)
+    assert torch.all(P[:, n:] == 7.0) and torch.all(D[n:] == 7.0)
+
+
+def test_empty_and_invalid_arguments(ctx):
+    from delta_b200._lib import DeltaError, check, lib
+
+    check(lib().delta_pairs_run(ctx.handle, 0, 0, 0, None, None, 0, 0.0, None, None, None, None))
+    with pytest.raises(DeltaError, match="INVALID"):
+        check(lib().delta_pairs_run(ctx.handle, 99, 0, 4, None, None, 4, 0.0, None, None, None, None))
+    with pytest.raises(DeltaError, match="INVALID"):
+        check(lib().delta_pairs_run(ctx.handle, 0, 0, 8, None, None, 4, 0.0, None, None, None, None))
