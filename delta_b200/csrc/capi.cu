@@ -168,4 +168,24 @@ delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int
   return cuda_error(cudaStreamSynchronize(ctx->stream), "pairs sync");
 }
 
+delta_status delta_detect(delta_ctx *ctx, int driver, int precision, const delta_meshes *meshes,
+                          const int32_t *pair_a, const int32_t *pair_b, int64_t n_pairs,
+                          const delta_contacts *out, int64_t *n_out, delta_stats *stats) {
+  if (!ctx || !meshes || !out || !n_out) return set_error(DELTA_ERR_INVALID, "delta_detect: null argument");
+  if (driver < DELTA_DRV_BF || driver > DELTA_DRV_BF_CERT) return set_error(DELTA_ERR_INVALID, "unknown driver");
+  if (precision != DELTA_F64 && precision != DELTA_F32) return set_error(DELTA_ERR_INVALID, "unknown precision");
+  if (n_pairs < 0 || out->capacity < 0) return set_error(DELTA_ERR_INVALID, "negative size");
+  *n_out = 0;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (n_pairs == 0) return DELTA_OK;
+  if (!pair_a || !pair_b || !meshes->tri_offset || !meshes->x || !meshes->y || !meshes->z || !meshes->eps ||
+      !meshes->friction || !meshes->id || meshes->n_bodies <= 0)
+    return set_error(DELTA_ERR_INVALID, "delta_detect: incomplete meshes or pairs");
+  if (out->capacity > 0 && (!out->x || !out->normal || !out->P || !out->Q || !out->depth || !out->eps_total ||
+                            !out->master || !out->slave || !out->tri_a || !out->tri_b || !out->penetration ||
+                            !out->friction))
+    return set_error(DELTA_ERR_INVALID, "delta_detect: incomplete contact buffer");
+  return detect_run(ctx, driver, precision, *meshes, pair_a, pair_b, n_pairs, out, n_out, stats);
+}
+
 }  // extern "C"

@@ -1,0 +1,514 @@
+// detect.cu -- particle-pair narrowphase drivers (bf, penalty, hybrids, gjk, stat variants).
+//
+// Work unit: one row = one triangle of body A against all triangles of body B of a
+// candidate pair, processed by one warp (lane l handles B triangles l, l+32, ...).  Rows
+// are handed out by a persistent work queue (an atomic row counter), so candidate pairs
+// of very different sizes share the SMs evenly.  The row-level decisions of the hybrid
+// drivers (hybrid.cpp:151-170, 434-460) and the row minimum of the stat drivers
+// (hybrid.cpp:605-617) are warp reductions.  Contacts are appended with one atomic per
+// warp and a 64-bit key (pair, A triangle, B triangle); a radix sort by key then
+// restores the serial order of the reference drivers, so the output is deterministic.
+#include <cub/cub.cuh>
+
+#include "internal.h"
+#include "tri_cert.cuh"
+#include "tri_gjk.cuh"
+#include "tri_ref.cuh"
+
+namespace delta {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct RawContacts {
+  double *f;        // 14 planes of cap: x(3) normal(3) depth P(3) Q(3) eps_total
+  int32_t *i;       // 4 planes: master slave tri_a tri_b
+  uint8_t *fric;
+  uint64_t *key;
+  int64_t cap;
+  unsigned long long *count;
+};
+
+struct DevStats {
+  unsigned long long hist[17];
+  unsigned long long penalty_fails, batch_fails, batch_size;
+  double batch_error;
+};
+
+struct RowCtx {
+  int64_t k;       // pair index
+  int32_t iA;      // triangle of A (within the body)
+  int64_t tA, tB0; // global triangle indices
+  int32_t nB;
+  double epsA, epsB;
+  int32_t idA, idB;
+  uint8_t fric;
+};
+
+template <class R>
+__device__ __forceinline__ void load_tri(const delta_meshes &m, int64_t t, R T[3][3]) {
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    T[v][0] = from_f64<R>(__ldg(m.x + 3 * t + v));
+    T[v][1] = from_f64<R>(__ldg(m.y + 3 * t + v));
+    T[v][2] = from_f64<R>(__ldg(m.z + 3 * t + v));
+  }
+}
+
+__device__ __forceinline__ void load_tri64(const delta_meshes &m, int64_t t, double T[3][3]) {
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    T[v][0] = __ldg(m.x + 3 * t + v);
+    T[v][1] = __ldg(m.y + 3 * t + v);
+    T[v][2] = __ldg(m.z + 3 * t + v);
+  }
+}
+
+// The per-triangle-pair solver of each driver.  Returns closest points (FP64 values).
+enum Solver { S_BF, S_PENALTY, S_PENALTY_ITER, S_GJK };
+
+template <class R, int S>
+__device__ __forceinline__ void solve(const delta_meshes &m, int64_t tA, int64_t tB, double max_err, double pq[6],
+                                      int &flag) {
+  {
+    R A[3][3], B[3][3], out[6];
+    load_tri<R>(m, tA, A);
+    load_tri<R>(m, tB, B);
+    if constexpr (S == S_BF) bf_solve_ref(A, B, out);
+    else if constexpr (S == S_PENALTY) penalty_ref(A, B, from_f64<R>(max_err), false, out, flag);
+    else if constexpr (S == S_PENALTY_ITER) penalty_ref(A, B, from_f64<R>(max_err), true, out, flag);
+    else gjk_ref(A, B, out);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) pq[k] = to_f64(out[k]);
+  }
+}
+
+// d = |P_B - P_A| (bf.cpp:117) in FP64 reference arithmetic
+__device__ __forceinline__ double pq_dist64(const double pq[6]) {
+  xf64 x[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) x[k] = xf64(pq[k]);
+  return pq_distance(x).v;
+}
+
+// contactpoint(PA, epsA, idA, QB, epsB, idB, friction), contactpoint.cpp:116-155
+__device__ __forceinline__ void write_contact(const RawContacts &rc, int64_t pos, const double pq[6], const RowCtx &r,
+                                              int32_t tb) {
+  const int64_t cap = rc.cap;
+  xf64 P[3] = {xf64(pq[0]), xf64(pq[1]), xf64(pq[2])}, Q[3] = {xf64(pq[3]), xf64(pq[4]), xf64(pq[5])};
+  const xf64 two = xf64(2.0);
+  const xf64 eps_total = xf64(r.epsA) + xf64(r.epsB);
+  const xf64 dist = sqrt_(((Q[0] - P[0]) * (Q[0] - P[0])) + ((Q[1] - P[1]) * (Q[1] - P[1])) +
+                          ((Q[2] - P[2]) * (Q[2] - P[2])));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    rc.f[(0 + k) * cap + pos] = ((P[k] + Q[k]) / two).v;
+    rc.f[(3 + k) * cap + pos] = ((P[k] - Q[k]) / dist).v;
+    rc.f[(7 + k) * cap + pos] = P[k].v;
+    rc.f[(10 + k) * cap + pos] = Q[k].v;
+  }
+  rc.f[6 * cap + pos] = (eps_total - dist).v;
+  rc.f[13 * cap + pos] = eps_total.v;
+  rc.i[0 * cap + pos] = r.idA;
+  rc.i[1 * cap + pos] = r.idB;
+  rc.i[2 * cap + pos] = r.iA;
+  rc.i[3 * cap + pos] = tb;
+  rc.fric[pos] = r.fric;
+  rc.key[pos] = ((uint64_t)r.k << 32) | ((uint64_t)r.iA << 16) | (uint64_t)tb;
+}
+
+// Warp-cooperative append of the lanes with `take` set (their order within the warp is
+// irrelevant: the key sort fixes the final order).
+__device__ __forceinline__ void emit(const RawContacts &rc, bool take, const double pq[6], const RowCtx &r, int32_t tb) {
+  const unsigned mask = __ballot_sync(kFull, take);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(rc.count, (unsigned long long)__popc(mask));
+  base = __shfl_sync(kFull, base, 0);
+  if (take) {
+    const int64_t pos = (int64_t)base + __popc(mask & ((1u << lane) - 1u));
+    if (pos < rc.cap) write_contact(rc, pos, pq, r, tb);
+  }
+}
+
+__device__ __forceinline__ int warp_sum(int v) { return __reduce_add_sync(kFull, v); }
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// Applies `fn(tb, valid)` to the row's B triangles in chunks of 32 (all lanes take part).
+template <class F>
+__device__ __forceinline__ void for_row(int32_t nB, F &&fn) {
+  const int lane = threadIdx.x & 31;
+  for (int32_t base = 0; base < nB; base += 32) {
+    const int32_t tb = base + lane;
+    fn(tb, tb < nB);
+  }
+}
+
+template <class R, int DRV>
+__device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawContacts &rc, DevStats *st,
+                            CertWarpSmem *csm) {
+  const xf64 margin = xf64(r.epsA) + xf64(r.epsB);
+  const double max_err = (margin / xf64(16.0)).v;  // (epsA+epsB)/16, hybrid.cpp:60
+  const double mg = margin.v;
+  double pq[6];
+  int flag = 0;
+  if constexpr (DRV == DELTA_DRV_BF_CERT) {
+    for_row(r.nB, [&](int32_t tb, bool valid) {
+      double A[3][3], B[3][3];
+      load_tri64(m, r.tA, A);
+      load_tri64(m, r.tB0 + (valid ? tb : r.nB - 1), B);
+      bf_cert_warp(A, B, valid, pq, *csm);
+      const bool take = valid && pq_dist64(pq) <= mg;  // bf.cpp:125
+      emit(rc, take, pq, r, tb);
+    });
+  } else if constexpr (DRV == DELTA_DRV_BF || DRV == DELTA_DRV_GJK) {
+    constexpr int S = DRV == DELTA_DRV_BF ? S_BF : S_GJK;
+    for_row(r.nB, [&](int32_t tb, bool valid) {
+      bool take = false;
+      if (valid) {
+        solve<R, S>(m, r.tA, r.tB0 + tb, max_err, pq, flag);
+        take = pq_dist64(pq) <= mg;  // bf.cpp:125
+      }
+      emit(rc, take, pq, r, tb);
+    });
+  } else if constexpr (DRV == DELTA_DRV_PENALTY) {
+    for_row(r.nB, [&](int32_t tb, bool valid) {
+      bool take = false;
+      if (valid) {
+        solve<R, S_PENALTY>(m, r.tA, r.tB0 + tb, max_err, pq, flag);
+        take = pq_dist64(pq) < mg;  // penalty.cpp:217
+      }
+      emit(rc, take, pq, r, tb);
+    });
+  } else if constexpr (DRV == DELTA_DRV_PENALTY_STAT) {
+    for_row(r.nB, [&](int32_t tb, bool valid) {
+      int it = 0;  // penalty.cpp:86
+      bool take = false;
+      if (valid) {
+        solve<R, S_PENALTY_ITER>(m, r.tA, r.tB0 + tb, max_err, pq, it);
+        // penalty.cpp:96 scans coordinate indices below nB: triangles tb with 3*tb < nB
+        take = (3 * tb < r.nB) && pq_dist64(pq) <= mg;
+      }
+#pragma unroll 1
+      for (int h = 0; h < 17; ++h) {
+        const int c = __popc(__ballot_sync(kFull, valid && it == h));
+        if (c && (threadIdx.x & 31) == 0) atomicAdd(&st->hist[h], (unsigned long long)c);
+      }
+      emit(rc, take, pq, r, tb);
+    });
+  } else {
+    // hybrids: penalty over the row, count failures, decide the fallback for the row
+    int fails = 0;
+    for_row(r.nB, [&](int32_t tb, bool valid) {
+      int f = 0;
+      if (valid) solve<R, S_PENALTY>(m, r.tA, r.tB0 + tb, max_err, pq, f);
+      fails += f;
+    });
+    const int counter = warp_sum(fails);
+    bool rerun;
+    const xf64 me = xf64(max_err);
+    if constexpr (DRV == DELTA_DRV_HYBRID_TRIANGLE) {
+      rerun = counter > 0;  // hybrid.cpp:151-156
+    } else if constexpr (DRV == DELTA_DRV_HYBRID_BATCH) {
+      rerun = (xf64((double)counter) * me) > ((me * xf64((double)(3 * (int64_t)r.nB))) / xf64(32.0));  // :434-440
+    } else {
+      rerun = (xf64((double)counter) * me) > ((me * xf64((double)r.nB)) / xf64(32.0));  // :565-573
+      if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&st->batch_size, (unsigned long long)r.nB);
+        atomicAdd(&st->batch_error, max_err);
+        atomicAdd(&st->penalty_fails, (unsigned long long)counter);
+        if (rerun) atomicAdd(&st->batch_fails, 1ull);
+      }
+    }
+    auto final_solve = [&](int32_t tb) {
+      int f = 0;
+      if (rerun) solve<R, S_BF>(m, r.tA, r.tB0 + tb, max_err, pq, f);
+      else solve<R, S_PENALTY>(m, r.tA, r.tB0 + tb, max_err, pq, f);
+    };
+    if constexpr (DRV == DELTA_DRV_HYBRID_BATCH || DRV == DELTA_DRV_HYBRID_TRIANGLE) {
+      for_row(r.nB, [&](int32_t tb, bool valid) {
+        bool take = false;
+        if (valid) {
+          final_solve(tb);
+          take = pq_dist64(pq) < mg;  // hybrid.cpp:176, 466
+        }
+        emit(rc, take, pq, r, tb);
+      });
+    } else {
+      // stat variants keep only the row minimum (hybrid.cpp:319-326, 605-617)
+      double mind = 1E99;
+      for_row(r.nB, [&](int32_t tb, bool valid) {
+        if (valid) {
+          final_solve(tb);
+          mind = fmin(mind, pq_dist64(pq));
+        }
+      });
+      mind = warp_min(mind);
+      for_row(r.nB, [&](int32_t tb, bool valid) {
+        bool take = false;
+        if (valid) {
+          final_solve(tb);
+          const double d = pq_dist64(pq);
+          take = d <= mind && d < mg;
+        }
+        emit(rc, take, pq, r, tb);
+      });
+    }
+  }
+}
+
+template <class R, int DRV>
+__global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *__restrict__ pa,
+                                                const int32_t *__restrict__ pb,
+                                                const int64_t *__restrict__ row_offset, int64_t n_pairs,
+                                                int64_t total_rows, RawContacts rc, DevStats *st,
+                                                unsigned long long *queue) {
+  const int lane = threadIdx.x & 31;
+  __shared__ CertWarpSmem cert_sm[DRV == DELTA_DRV_BF_CERT ? 4 : 1];
+  CertWarpSmem *csm = &cert_sm[DRV == DELTA_DRV_BF_CERT ? (threadIdx.x >> 5) : 0];
+  for (;;) {
+    unsigned long long row = 0;
+    if (lane == 0) row = atomicAdd(queue, 1ull);
+    row = __shfl_sync(kFull, row, 0);
+    if ((int64_t)row >= total_rows) return;
+    // pair k: last k with row_offset[k] <= row
+    int64_t lo = 0, hi = n_pairs;
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (row_offset[mid] <= (int64_t)row) lo = mid;
+      else hi = mid;
+    }
+    RowCtx r;
+    r.k = lo;
+    const int32_t a = pa[lo], b = pb[lo];
+    r.iA = (int32_t)((int64_t)row - row_offset[lo]);
+    r.tA = m.tri_offset[a] + r.iA;
+    r.tB0 = m.tri_offset[b];
+    r.nB = (int32_t)(m.tri_offset[b + 1] - r.tB0);
+    r.epsA = m.eps[a];
+    r.epsB = m.eps[b];
+    r.idA = m.id[a];
+    r.idB = m.id[b];
+    r.fric = (m.friction[a] && m.friction[b]) ? 1 : 0;
+    process_row<R, DRV>(m, r, rc, st, csm);
+  }
+}
+
+__global__ void k_rows_per_pair(const int64_t *tri_offset, const int32_t *pa, int64_t n_pairs, int32_t n_bodies,
+                                int64_t *rows, int *bad) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_pairs) return;
+  const int32_t a = pa[k];
+  if (a < 0 || a >= n_bodies) {
+    atomicExch(bad, 1);
+    rows[k] = 0;
+    return;
+  }
+  rows[k] = tri_offset[a + 1] - tri_offset[a];
+}
+
+__global__ void k_check_pairs(const int64_t *tri_offset, const int32_t *pb, int64_t n_pairs, int32_t n_bodies,
+                              int *bad) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_pairs) return;
+  const int32_t b = pb[k];
+  if (b < 0 || b >= n_bodies) atomicExch(bad, 1);
+}
+
+__global__ void k_max_tris(const int64_t *tri_offset, int32_t n_bodies, int *bad) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_bodies) return;
+  const int64_t n = tri_offset[i + 1] - tri_offset[i];
+  if (n < 0 || n >= 65536) atomicExch(bad, 2);
+}
+
+__global__ void k_iota(int64_t *v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
+}
+
+__global__ void k_gather(RawContacts rc, const int64_t *perm, int64_t n, delta_contacts out) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t s = perm[j], cap = rc.cap, oc = out.capacity;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    out.x[k * oc + j] = rc.f[(0 + k) * cap + s];
+    out.normal[k * oc + j] = rc.f[(3 + k) * cap + s];
+    out.P[k * oc + j] = rc.f[(7 + k) * cap + s];
+    out.Q[k * oc + j] = rc.f[(10 + k) * cap + s];
+  }
+  out.depth[j] = rc.f[6 * cap + s];
+  out.eps_total[j] = rc.f[13 * cap + s];
+  out.master[j] = rc.i[s];
+  out.slave[j] = rc.i[cap + s];
+  out.tri_a[j] = rc.i[2 * cap + s];
+  out.tri_b[j] = rc.i[3 * cap + s];
+  out.penetration[j] = 1;
+  out.friction[j] = rc.fric[s];
+}
+
+template <class R, int DRV>
+cudaError_t launch_detect_t(cudaStream_t s, const delta_meshes &m, const int32_t *pa, const int32_t *pb,
+                            const int64_t *row_offset, int64_t n_pairs, int64_t rows, const RawContacts &rc,
+                            DevStats *st, unsigned long long *queue) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_detect<R, DRV>, 128, 0);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
+  const int64_t need = (rows + 3) / 4;  // 4 warps per block
+  if (blocks > need) blocks = need > 0 ? need : 1;
+  k_detect<R, DRV><<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, row_offset, n_pairs, rows, rc, st, queue);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_detect_prec(int driver, cudaStream_t s, const delta_meshes &m, const int32_t *pa,
+                               const int32_t *pb, const int64_t *ro, int64_t np, int64_t rows,
+                               const RawContacts &rc, DevStats *st, unsigned long long *q) {
+  switch (driver) {
+    case DELTA_DRV_BF: return launch_detect_t<R, DELTA_DRV_BF>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    case DELTA_DRV_PENALTY: return launch_detect_t<R, DELTA_DRV_PENALTY>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    case DELTA_DRV_PENALTY_STAT:
+      return launch_detect_t<R, DELTA_DRV_PENALTY_STAT>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    case DELTA_DRV_HYBRID_BATCH:
+      return launch_detect_t<R, DELTA_DRV_HYBRID_BATCH>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    case DELTA_DRV_HYBRID_TRIANGLE:
+      return launch_detect_t<R, DELTA_DRV_HYBRID_TRIANGLE>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    case DELTA_DRV_HYBRID_BATCH_STAT:
+      return launch_detect_t<R, DELTA_DRV_HYBRID_BATCH_STAT>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    case DELTA_DRV_HYBRID_TRI_STAT:
+      return launch_detect_t<R, DELTA_DRV_HYBRID_TRI_STAT>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    case DELTA_DRV_GJK: return launch_detect_t<R, DELTA_DRV_GJK>(s, m, pa, pb, ro, np, rows, rc, st, q);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+// Scratch slots used here: 2 rows/row_offset, 3 raw contacts, 4 sort buffers, 5 small state.
+delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
+                        const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
+                        delta_stats *stats) {
+  cudaStream_t s = ctx->stream;
+  delta_status st;
+  cudaError_t e;
+  // small device state: [0] bad flag (int), then DevStats, queue counter, contact counter
+  void *small = nullptr;
+  const size_t small_bytes = 256 + sizeof(DevStats) + 64;
+  if ((st = ctx_scratch(ctx, 5, small_bytes, &small)) != DELTA_OK) return st;
+  int *bad = (int *)small;
+  DevStats *dstats = (DevStats *)((char *)small + 256);
+  unsigned long long *queue = (unsigned long long *)((char *)small + 256 + sizeof(DevStats));
+  unsigned long long *count = queue + 1;
+  if ((e = cudaMemsetAsync(small, 0, small_bytes, s)) != cudaSuccess) return cuda_error(e, "detect memset");
+
+  // rows per pair and their exclusive prefix sum
+  void *rbuf = nullptr;
+  if ((st = ctx_scratch(ctx, 2, sizeof(int64_t) * (size_t)(2 * n_pairs + 2), &rbuf)) != DELTA_OK) return st;
+  int64_t *rows = (int64_t *)rbuf, *row_offset = rows + n_pairs + 1;
+  const unsigned g = (unsigned)((n_pairs + 255) / 256);
+  k_rows_per_pair<<<g, 256, 0, s>>>(m.tri_offset, pa, n_pairs, m.n_bodies, rows, bad);
+  k_check_pairs<<<g, 256, 0, s>>>(m.tri_offset, pb, n_pairs, m.n_bodies, bad);
+  k_max_tris<<<(unsigned)((m.n_bodies + 255) / 256), 256, 0, s>>>(m.tri_offset, m.n_bodies, bad);
+  ctx->launches += 3;
+  if ((e = cudaMemsetAsync(rows + n_pairs, 0, sizeof(int64_t), s)) != cudaSuccess) return cuda_error(e, "memset");
+  size_t temp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, rows, row_offset, n_pairs + 1, s);
+  void *temp = nullptr;
+  if ((st = ctx_scratch(ctx, 4, temp_bytes, &temp)) != DELTA_OK) return st;
+  if ((e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, rows, row_offset, n_pairs + 1, s)) != cudaSuccess)
+    return cuda_error(e, "row scan");
+  ctx->launches += 1;
+  int64_t total_rows = 0;
+  int hbad = 0;
+  if ((e = cudaMemcpyAsync(&total_rows, row_offset + n_pairs, sizeof(int64_t), cudaMemcpyDeviceToHost, s)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return cuda_error(e, "detect rows");
+  if (hbad == 1) return set_error(DELTA_ERR_INVALID, "delta_detect: body index out of range");
+  if (hbad == 2) return set_error(DELTA_ERR_INVALID, "delta_detect: a body has 65536 or more triangles");
+
+  // raw contact buffer: at least the caller's capacity; grown and rerun when it overflows
+  int64_t cap = out->capacity > 1024 ? out->capacity : 1024;
+  unsigned long long hcount = 0;
+  RawContacts rc{};
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    void *raw = nullptr;
+    const size_t per = 14 * sizeof(double) + 4 * sizeof(int32_t) + 1 + 2 * sizeof(uint64_t);
+    if ((st = ctx_scratch(ctx, 3, per * (size_t)cap + 64, &raw)) != DELTA_OK) return st;
+    rc.cap = cap;
+    rc.f = (double *)raw;
+    rc.key = (uint64_t *)(rc.f + 14 * cap);
+    rc.i = (int32_t *)(rc.key + 2 * cap);
+    rc.fric = (uint8_t *)(rc.i + 4 * cap);
+    rc.count = count;
+    if ((e = cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
+      return cuda_error(e, "memset");
+    if ((e = cudaMemsetAsync(dstats, 0, sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
+    e = precision == DELTA_F32 && driver != DELTA_DRV_BF_CERT
+            ? launch_detect_prec<float>(driver, s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats, queue)
+            : (driver == DELTA_DRV_BF_CERT
+                   ? launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, n_pairs, total_rows, rc,
+                                                             dstats, queue)
+                   : launch_detect_prec<xf64>(driver, s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats,
+                                              queue));
+    if (e != cudaSuccess) return cuda_error(e, "detect kernel");
+    ctx->launches += 1;
+    if ((e = cudaMemcpyAsync(&hcount, count, sizeof(hcount), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+      return cuda_error(e, "detect count");
+    if ((int64_t)hcount <= cap) break;
+    cap = (int64_t)hcount + hcount / 4;
+  }
+  if (stats) {
+    DevStats h;
+    if ((e = cudaMemcpy(&h, dstats, sizeof h, cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return cuda_error(e, "stats");
+    for (int i = 0; i < 17; ++i) stats->newton_hist[i] = (int64_t)h.hist[i];
+    stats->penalty_fails = (int64_t)h.penalty_fails;
+    stats->batch_fails = (int64_t)h.batch_fails;
+    stats->batch_size = (int64_t)h.batch_size;
+    stats->batch_error = h.batch_error;
+  }
+  const int64_t n = (int64_t)hcount;
+  *n_out = n;
+  if (n == 0) return DELTA_OK;
+  // sort (key, index) and gather into the caller's arrays
+  int64_t *perm_in = nullptr;
+  void *sbuf = nullptr;
+  if ((st = ctx_scratch(ctx, 6, sizeof(int64_t) * 2 * (size_t)n + sizeof(uint64_t) * (size_t)n, &sbuf)) != DELTA_OK)
+    return st;
+  perm_in = (int64_t *)sbuf;
+  int64_t *perm_out = perm_in + n;
+  uint64_t *key_out = (uint64_t *)(perm_out + n);
+  k_iota<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(perm_in, n);
+  ctx->launches += 1;
+  int end_bit = 33;
+  while (end_bit < 64 && ((int64_t)1 << (end_bit - 32)) < n_pairs) ++end_bit;
+  temp_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, rc.key, key_out, perm_in, perm_out, n, 0, end_bit, s);
+  if ((st = ctx_scratch(ctx, 4, temp_bytes, &temp)) != DELTA_OK) return st;
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, rc.key, key_out, perm_in, perm_out, n, 0, end_bit, s)) !=
+      cudaSuccess)
+    return cuda_error(e, "contact sort");
+  ctx->launches += 1;
+  const int64_t wn = n < out->capacity ? n : out->capacity;
+  if (wn > 0) {
+    k_gather<<<(unsigned)((wn + 255) / 256), 256, 0, s>>>(rc, perm_out, wn, *out);
+    ctx->launches += 1;
+  }
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "detect gather");
+  if (n > out->capacity) return set_error(DELTA_ERR_CAPACITY, "delta_detect: contact capacity exceeded");
+  return DELTA_OK;
+}
+
+}  // namespace delta

@@ -15,6 +15,11 @@ constexpr int kNumSMs = 148;  // B200
 cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
                          int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags);
 
+// Particle-pair drivers (detect.cu).
+delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
+                        const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
+                        delta_stats *stats);
+
 // Thread-local last-error text (capi.cu).
 delta_status set_error(delta_status st, const std::string &msg);
 delta_status cuda_error(cudaError_t e, const char *where);

@@ -21,56 +21,74 @@ __global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restri
                                                uint8_t *__restrict__ flags) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    double A64[3][3], B64[3][3];
+    R A[3][3], B[3][3];
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        A64[v][k] = __ldg(a + (3 * v + k) * ld + i);
-        B64[v][k] = __ldg(b + (3 * v + k) * ld + i);
+        A[v][k] = from_f64<R>(__ldg(a + (3 * v + k) * ld + i));
+        B[v][k] = from_f64<R>(__ldg(b + (3 * v + k) * ld + i));
       }
-    double out[6], d;
+    R pq[6];
     int flag = 0;
-    if constexpr (M == M_BF_CERT) {
-      flag = bf_cert(A64, B64, out);
-      xf64 pq[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) pq[k] = xf64(out[k]);
-      d = pq_distance(pq).v;
-    } else {
-      R A[3][3], B[3][3];
-#pragma unroll
-      for (int v = 0; v < 3; ++v)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          A[v][k] = from_f64<R>(A64[v][k]);
-          B[v][k] = from_f64<R>(B64[v][k]);
-        }
-      R pq[6];
-      const R me = from_f64<R>(max_error);
-      if constexpr (M == M_BF) {
-        bf_solve_ref(A, B, pq);
-      } else if constexpr (M == M_PENALTY) {
-        penalty_ref(A, B, me, false, pq, flag);
-      } else if constexpr (M == M_PENALTY_ITER) {
-        penalty_ref(A, B, me, true, pq, flag);
-      } else if constexpr (M == M_GJK) {
-        gjk_ref(A, B, pq);
-      } else {  // per-pair hybrid: penalty, bf when the pair reports failure
-        penalty_ref(A, B, me, false, pq, flag);
-        if (flag) bf_solve_ref(A, B, pq);
-      }
-#pragma unroll
-      for (int k = 0; k < 6; ++k) out[k] = to_f64(pq[k]);
-      d = to_f64(pq_distance(pq));
+    const R me = from_f64<R>(max_error);
+    if constexpr (M == M_BF) {
+      bf_solve_ref(A, B, pq);
+    } else if constexpr (M == M_PENALTY) {
+      penalty_ref(A, B, me, false, pq, flag);
+    } else if constexpr (M == M_PENALTY_ITER) {
+      penalty_ref(A, B, me, true, pq, flag);
+    } else if constexpr (M == M_GJK) {
+      gjk_ref(A, B, pq);
+    } else {  // per-pair hybrid: penalty, bf when the pair reports failure
+      penalty_ref(A, B, me, false, pq, flag);
+      if (flag) bf_solve_ref(A, B, pq);
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      p[k * ld + i] = out[k];
-      q[k * ld + i] = out[3 + k];
+      p[k * ld + i] = to_f64(pq[k]);
+      q[k * ld + i] = to_f64(pq[3 + k]);
     }
-    dist[i] = d;
+    dist[i] = to_f64(pq_distance(pq));
     if (flags) flags[i] = (uint8_t)flag;
+  }
+}
+
+// bf_cert: warps walk the pair list 32 pairs at a time (the certificate's candidate queue
+// is shared by the warp).
+__global__ void __launch_bounds__(256) k_pairs_cert(int64_t n, const double *__restrict__ a,
+                                                    const double *__restrict__ b, int64_t ld,
+                                                    double *__restrict__ p, double *__restrict__ q,
+                                                    double *__restrict__ dist, uint8_t *__restrict__ flags) {
+  __shared__ CertWarpSmem sm[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += nwarps * 32) {
+    const int64_t i = base + lane;
+    const bool valid = i < n;
+    const int64_t ii = valid ? i : n - 1;
+    double A[3][3], B[3][3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        A[v][k] = __ldg(a + (3 * v + k) * ld + ii);
+        B[v][k] = __ldg(b + (3 * v + k) * ld + ii);
+      }
+    double out[6];
+    const int evals = bf_cert_warp(A, B, valid, out, sm[warp]);
+    if (valid) {
+      xf64 pq[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) pq[k] = xf64(out[k]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        p[k * ld + i] = out[k];
+        q[k * ld + i] = out[3 + k];
+      }
+      dist[i] = pq_distance(pq).v;
+      if (flags) flags[i] = (uint8_t)evals;
+    }
   }
 }
 
@@ -101,7 +119,16 @@ static cudaError_t launch_prec(int method, cudaStream_t s, int64_t n, const doub
 
 cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
                          int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags) {
-  if (method == M_BF_CERT) return launch_one<xf64, M_BF_CERT>(s, n, a, b, ld, max_error, p, q, dist, flags);
+  if (method == M_BF_CERT) {
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_cert, 256, 0);
+    if (e != cudaSuccess) return e;
+    int64_t blocks = (n + 255) / 256;
+    const int64_t cap = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1) * 8;
+    if (blocks > cap) blocks = cap;
+    k_pairs_cert<<<(unsigned)(blocks > 0 ? blocks : 1), 256, 0, s>>>(n, a, b, ld, p, q, dist, flags);
+    return cudaGetLastError();
+  }
   if (precision == 0) return launch_prec<xf64>(method, s, n, a, b, ld, max_error, p, q, dist, flags);
   return launch_prec<float>(method, s, n, a, b, ld, max_error, p, q, dist, flags);
 }

@@ -1,0 +1,196 @@
+"""Particle-pair contact detection: the drivers delta::contact::detection::{bf, penalty,
+penaltyStat, hybridWithPerBatchFallBack, hybridWithPerTriangleFallBack, hybridBatchStat,
+hybridTriangleStat, gjk} (delta/contact/detection/*.h) on the GPU.
+
+``detect`` runs one driver over many candidate body pairs at once (the batched form the
+time step uses).  The functions named after the reference drivers take the reference's
+arguments (SoA-tri coordinates of two bodies, triangle counts, epsilon, friction flag,
+particle id) and return the contact list as a numpy structured array with the fields
+of struct contactpoint (contactpoint.h:42-103) plus the two triangle indices.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import DeltaError, ERR_CAPACITY, check, lib
+from .narrowphase import F64, Context
+
+(DRV_BF, DRV_PENALTY, DRV_PENALTY_STAT, DRV_HYBRID_BATCH, DRV_HYBRID_TRIANGLE, DRV_HYBRID_BATCH_STAT,
+ DRV_HYBRID_TRI_STAT, DRV_GJK, DRV_BF_CERT) = range(9)
+
+CONTACT_DTYPE = np.dtype(
+    [("x", "<f8", 3), ("normal", "<f8", 3), ("depth", "<f8"), ("P", "<f8", 3), ("Q", "<f8", 3),
+     ("friction", "<i4"), ("eps_total", "<f8"), ("master", "<i4"), ("slave", "<i4"), ("penetration", "<i4"),
+     ("tri_a", "<i4"), ("tri_b", "<i4")], align=True)
+
+
+class _Meshes(C.Structure):
+    _fields_ = [("n_bodies", C.c_int32), ("tri_offset", C.c_void_p), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("z", C.c_void_p), ("eps", C.c_void_p), ("friction", C.c_void_p), ("id", C.c_void_p)]
+
+
+class _Contacts(C.Structure):
+    _fields_ = [("capacity", C.c_int64), ("x", C.c_void_p), ("normal", C.c_void_p), ("P", C.c_void_p),
+                ("Q", C.c_void_p), ("depth", C.c_void_p), ("eps_total", C.c_void_p), ("master", C.c_void_p),
+                ("slave", C.c_void_p), ("tri_a", C.c_void_p), ("tri_b", C.c_void_p), ("penetration", C.c_void_p),
+                ("friction", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("newton_hist", C.c_int64 * 17), ("penalty_fails", C.c_int64), ("batch_fails", C.c_int64),
+                ("batch_size", C.c_int64), ("batch_error", C.c_double)]
+
+
+class Meshes:
+    """Triangulated bodies on the device in SoA-tri layout."""
+
+    def __init__(self, tri_offset, x, y, z, eps, friction, ids=None, device="cuda"):
+        import torch
+
+        t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).to(device)  # noqa: E731
+        self.tri_offset = t(tri_offset, torch.int64)
+        self.x, self.y, self.z = t(x, torch.float64), t(y, torch.float64), t(z, torch.float64)
+        self.n_bodies = self.tri_offset.numel() - 1
+        self.eps = t(eps, torch.float64)
+        self.friction = t(friction, torch.uint8)
+        self.id = t(ids if ids is not None else np.arange(self.n_bodies), torch.int32)
+
+    @classmethod
+    def from_bodies(cls, bodies, eps, friction, ids=None):
+        """bodies: list of (3, 3*nT) host arrays."""
+        counts = [b.shape[1] // 3 for b in bodies]
+        off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        xyz = np.concatenate(bodies, 1) if bodies else np.zeros((3, 0))
+        return cls(off, xyz[0], xyz[1], xyz[2], eps, friction, ids)
+
+    def struct(self) -> _Meshes:
+        return _Meshes(self.n_bodies, self.tri_offset.data_ptr(), self.x.data_ptr(), self.y.data_ptr(),
+                       self.z.data_ptr(), self.eps.data_ptr(), self.friction.data_ptr(), self.id.data_ptr())
+
+
+class Contacts:
+    """Device contact buffer (SoA) of a given capacity."""
+
+    def __init__(self, capacity: int, device="cuda"):
+        import torch
+
+        cap = max(int(capacity), 1)
+        f8 = dict(dtype=torch.float64, device=device)
+        i4 = dict(dtype=torch.int32, device=device)
+        self.capacity = cap
+        self.x, self.normal = torch.empty((3, cap), **f8), torch.empty((3, cap), **f8)
+        self.P, self.Q = torch.empty((3, cap), **f8), torch.empty((3, cap), **f8)
+        self.depth, self.eps_total = torch.empty(cap, **f8), torch.empty(cap, **f8)
+        self.master, self.slave = torch.empty(cap, **i4), torch.empty(cap, **i4)
+        self.tri_a, self.tri_b = torch.empty(cap, **i4), torch.empty(cap, **i4)
+        self.penetration = torch.empty(cap, **i4)
+        self.friction = torch.empty(cap, dtype=torch.uint8, device=device)
+        self.count = 0
+
+    def struct(self) -> _Contacts:
+        p = lambda t: t.data_ptr()  # noqa: E731
+        return _Contacts(self.capacity, p(self.x), p(self.normal), p(self.P), p(self.Q), p(self.depth),
+                         p(self.eps_total), p(self.master), p(self.slave), p(self.tri_a), p(self.tri_b),
+                         p(self.penetration), p(self.friction))
+
+    def to_numpy(self, n: int | None = None) -> np.ndarray:
+        n = self.count if n is None else n
+        out = np.zeros(n, CONTACT_DTYPE)
+        for name in ("x", "normal", "P", "Q"):
+            out[name] = getattr(self, name)[:, :n].cpu().numpy().T
+        for name in ("depth", "eps_total", "master", "slave", "tri_a", "tri_b", "penetration", "friction"):
+            out[name] = getattr(self, name)[:n].cpu().numpy()
+        return out
+
+
+def detect(ctx: Context, driver: int, meshes: Meshes, pair_a, pair_b, precision=F64, capacity=None,
+           grow=True, stats=False):
+    """Contacts of `driver` over the body pairs (pair_a[k], pair_b[k]), in (pair, A triangle,
+    B triangle) order.  Returns (Contacts, Stats|None).  With grow=True a full buffer is
+    reallocated and the call repeated."""
+    import torch
+
+    pa = torch.as_tensor(np.asarray(pair_a, np.int32) if not torch.is_tensor(pair_a) else pair_a,
+                         dtype=torch.int32).cuda()
+    pb = torch.as_tensor(np.asarray(pair_b, np.int32) if not torch.is_tensor(pair_b) else pair_b,
+                         dtype=torch.int32).cuda()
+    cap = capacity if capacity is not None else 4096
+    while True:
+        out = Contacts(cap)
+        n = C.c_int64(0)
+        st = Stats()
+        status = lib().delta_detect(ctx.handle, int(driver), int(precision), C.byref(meshes.struct()),
+                                    pa.data_ptr(), pb.data_ptr(), pa.numel(), C.byref(out.struct()), C.byref(n),
+                                    C.byref(st))
+        if status == ERR_CAPACITY and grow:
+            cap = int(n.value)
+            continue
+        if status == ERR_CAPACITY:
+            out.count = min(int(n.value), out.capacity)
+            raise DeltaError(status, f"capacity {out.capacity} < {n.value} contacts")
+        check(status)
+        out.count = int(n.value)
+        return out, (st if stats else None)
+
+
+# ---- the reference drivers, one body pair per call ---------------------------------------
+_ctx = None
+
+
+def _default_ctx():
+    global _ctx
+    if _ctx is None:
+        _ctx = Context(0)
+    return _ctx
+
+
+def _one_pair(driver, xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB, precision=F64,
+              ctx=None, stats=False):
+    A = np.stack([np.asarray(xA, float)[:3 * nA], np.asarray(yA, float)[:3 * nA], np.asarray(zA, float)[:3 * nA]])
+    B = np.stack([np.asarray(xB, float)[:3 * nB], np.asarray(yB, float)[:3 * nB], np.asarray(zB, float)[:3 * nB]])
+    m = Meshes.from_bodies([A, B], [epsA, epsB], [int(bool(fricA)), int(bool(fricB))], [idA, idB])
+    out, st = detect(ctx or _default_ctx(), driver, m, [0], [1], precision=precision, stats=True)
+    c = out.to_numpy()
+    return (c, st) if stats else c
+
+
+def bf(*args, **kw):
+    """bf(xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB), bf.h:65-81."""
+    return _one_pair(DRV_BF, *args, **kw)
+
+
+def penalty(*args, **kw):
+    """penalty(...), penalty.h:99-115."""
+    return _one_pair(DRV_PENALTY, *args, **kw)
+
+
+def penaltyStat(*args, **kw):  # noqa: N802 (reference name)
+    """penaltyStat(...), penalty.h:59-74; stats=True also returns the iteration histogram."""
+    return _one_pair(DRV_PENALTY_STAT, *args, **kw)
+
+
+def hybridWithPerBatchFallBack(*args, **kw):  # noqa: N802
+    """hybrid.h:113-128."""
+    return _one_pair(DRV_HYBRID_BATCH, *args, **kw)
+
+
+def hybridWithPerTriangleFallBack(*args, **kw):  # noqa: N802
+    """hybrid.h:76-91 (the A-triangle loop runs over A's triangles)."""
+    return _one_pair(DRV_HYBRID_TRIANGLE, *args, **kw)
+
+
+def hybridBatchStat(*args, **kw):  # noqa: N802
+    """hybrid.h:130-144."""
+    return _one_pair(DRV_HYBRID_BATCH_STAT, *args, **kw)
+
+
+def hybridTriangleStat(*args, **kw):  # noqa: N802
+    """hybrid.h:146-160."""
+    return _one_pair(DRV_HYBRID_TRI_STAT, *args, **kw)
+
+
+def gjk(nA, xA, yA, zA, epsA, fricA, idA, nB, xB, yB, zB, epsB, fricB, idB, **kw):
+    """gjk argument order (gjk.h:32-47); per triangle pair with bf()'s contact rule."""
+    return _one_pair(DRV_GJK, xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB, **kw)

@@ -97,6 +97,51 @@ delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int
                                   const double *b, int64_t ld, double max_error, double *p, double *q,
                                   double *dist, uint8_t *flags);
 
+/* ---- particle pairs ------------------------------------------------------------------ */
+/* Triangulated bodies in SoA-tri layout (device arrays). */
+typedef struct {
+  int32_t n_bodies;
+  const int64_t *tri_offset;  /* [n_bodies+1] first triangle of each body */
+  const double *x, *y, *z;    /* [3*tri_offset[n_bodies]] vertices, 3 per triangle */
+  const double *eps;          /* [n_bodies] contact halo epsilon */
+  const uint8_t *friction;    /* [n_bodies] friction flag */
+  const int32_t *id;          /* [n_bodies] global particle id written to master/slave */
+} delta_meshes;
+
+/* Contacts in SoA (device arrays of `capacity` entries; x, normal, P, Q hold 3 planes of
+ * `capacity`).  One entry per struct contactpoint (contactpoint.h:42-103) plus the
+ * triangle indices that produced it. */
+typedef struct {
+  int64_t capacity;
+  double *x, *normal, *P, *Q;
+  double *depth, *eps_total;
+  int32_t *master, *slave, *tri_a, *tri_b, *penetration;
+  uint8_t *friction;
+} delta_contacts;
+
+/* Statistics of the instrumented drivers (penalty.cpp:29-48, hybrid.cpp:27-56). */
+typedef struct {
+  int64_t newton_hist[17];
+  int64_t penalty_fails;
+  int64_t batch_fails;
+  int64_t batch_size;
+  double batch_error;
+} delta_stats;
+
+/* Runs `driver` on every candidate body pair (pair_a[k], pair_b[k]) (device arrays of
+ * n_pairs) and writes the contacts, ordered by (pair k, A triangle, B triangle) -- the
+ * serial order of the reference drivers.  Each body must have fewer than 65536
+ * triangles.  *n_out (host) receives the contact count; when it exceeds
+ * out->capacity, nothing past the capacity is written and DELTA_ERR_CAPACITY is
+ * returned.  stats (host, may be NULL) is overwritten with this call's statistics.
+ * Synchronises the context's stream.  Drop-in for bf() / penalty() / penaltyStat() /
+ * hybridWith{PerBatch,PerTriangle}FallBack() / hybrid{Batch,Triangle}Stat() called per
+ * candidate pair by Collision::collisionDetection (Collision.cpp:342-645), with the
+ * contact lists of all pairs concatenated. */
+delta_status delta_detect(delta_ctx *ctx, int driver, int precision, const delta_meshes *meshes,
+                          const int32_t *pair_a, const int32_t *pair_b, int64_t n_pairs,
+                          const delta_contacts *out, int64_t *n_out, delta_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif
