@@ -31,6 +31,13 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_pairs_run": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp], C.c_int),
     "delta_pairs_run_host": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp], C.c_int),
     "delta_detect": ([vp, C.c_int, C.c_int, vp, vp, vp, i64, vp, vp, vp], C.c_int),
+    "delta_forces": ([vp, vp, vp, i64, vp, vp, vp, vp], C.c_int),
+    "delta_integrate": ([vp, vp, vp, vp, vp, vp], C.c_int),
+    "delta_broadphase": ([vp, vp, vp, vp, i64, vp], C.c_int),
+    "delta_sim_create": ([vp, vp, C.c_int, vp], C.c_int),
+    "delta_sim_step": ([vp, vp, i32, vp], C.c_int),
+    "delta_sim_contacts": ([vp, vp, vp], C.c_int),
+    "delta_sim_destroy": ([vp], C.c_int),
 }
 
 

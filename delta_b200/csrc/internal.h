@@ -36,7 +36,7 @@ struct delta_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int64_t launches = 0;
-  delta_buffer scratch[8];
+  delta_buffer scratch[16];
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
 };

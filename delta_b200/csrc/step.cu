@@ -1,0 +1,842 @@
+// step.cu -- forces, integration, broadphase and the time-step loop.
+//
+// All physics arithmetic is FP64 written over xf64, i.e. the rounded operations of the
+// reference (forces.cpp, dynamics.cpp, MoveParticles.cpp) in their order, without FMA
+// contraction.  Summations that the reference performs sequentially (contacts of one
+// partner, then partners of one body) are kept sequential per pair / per body; no
+// floating-point atomics are used, so results do not depend on scheduling.
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <vector>
+
+#include "internal.h"
+#include "real.cuh"
+
+namespace delta {
+
+namespace {
+
+using X = xf64;
+
+// ---------------------------------------------------------------------------------------
+// dynamics.cpp
+// ---------------------------------------------------------------------------------------
+
+// expmap, dynamics.cpp:26-102 (Taylor branch below 10 degrees; the off-diagonal term
+// v02 = Omega2*Omega3 of dynamics.cpp:78 is kept as written).
+__device__ __forceinline__ void expmap(X O1, X O2, X O3, X L[9]) {
+  const X v0 = O1 * O1, v1 = O2 * O2, v2 = O3 * O3;
+  X angsq = v0 + v1 + v2, sx, cx;
+  if (angsq < X(3.0461741978671E-02)) {
+    sx = X(1.0) + (X(-1.666666666666667E-1) + (X(8.333333333333333E-3) + (X(-1.984126984126984E-4) +
+         (X(2.755731922398589E-6) + (X(-2.505210838544172E-8) + X(1.605904383682161E-10) * angsq) * angsq) *
+         angsq) * angsq) * angsq) * angsq;
+    cx = X(0.5) + (X(-4.166666666666667E-2) + (X(1.388888888888889E-3) + (X(-2.480158730158730E-5) +
+         (X(2.755731922398589E-7) + (X(-2.087675698786810E-9) + X(1.147074559772972E-11) * angsq) * angsq) *
+         angsq) * angsq) * angsq) * angsq;
+  } else {
+    const X t = angsq;
+    angsq = sqrt_(angsq);
+    const X s = X(sin(angsq.v)), c = X(cos(angsq.v));
+    sx = s / angsq;
+    cx = (X(1.0) - c) / t;
+  }
+  const X v01 = O1 * O2, v02 = O2 * O3, v12 = O2 * O3;
+  const X s0 = sx * O1, s1 = sx * O2, s2 = sx * O3;
+  L[0] = -cx * (v2 + v1);
+  L[1] = cx * v01;
+  L[2] = cx * v02;
+  L[3] = L[1];
+  L[4] = -cx * (v2 + v0);
+  L[5] = cx * v12;
+  L[6] = L[2];
+  L[7] = L[5];
+  L[8] = -cx * (v1 + v0);
+  L[0] += X(1.0);
+  L[1] += s2;
+  L[2] -= s1;
+  L[3] -= s2;
+  L[4] += X(1.0);
+  L[5] += s0;
+  L[6] += s1;
+  L[7] -= s0;
+  L[8] += X(1.0);
+}
+
+struct BodyRef {
+  int32_t n, i;
+  __device__ __forceinline__ int64_t at(int c) const { return (int64_t)c * n + i; }
+};
+
+// updateRotationMatrix, dynamics.cpp:104-138
+__device__ __forceinline__ void update_rotation(const delta_scene &s, BodyRef b, X step) {
+  X W[3], R0[9], DL[9];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) W[k] = X(s.ref_ang[b.at(k)]);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) R0[k] = X(s.rot[b.at(k)]);
+  expmap(step * W[0], step * W[1], step * W[2], DL);
+  X R[9];
+#pragma unroll
+  for (int col = 0; col < 3; ++col)
+#pragma unroll
+    for (int row = 0; row < 3; ++row)
+      R[3 * col + row] = R0[row] * DL[3 * col] + R0[3 + row] * DL[3 * col + 1] + R0[6 + row] * DL[3 * col + 2];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) s.rot[b.at(k)] = R[k].v;
+#pragma unroll
+  for (int row = 0; row < 3; ++row) s.ang[b.at(row)] = (R[row] * W[0] + R[3 + row] * W[1] + R[6 + row] * W[2]).v;
+}
+
+// updateAngular, dynamics.cpp:140-213 (eqs. 13-15)
+__device__ __forceinline__ void update_angular(const delta_scene &s, BodyRef b, const X tq[3], X step) {
+  X W[3], R[9], J[9], Ji[9];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) W[k] = X(s.ref_ang[b.at(k)]);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    R[k] = X(s.rot[b.at(k)]);
+    J[k] = X(s.inertia[b.at(k)]);
+    Ji[k] = X(s.inverse[b.at(k)]);
+  }
+  const X half = X(0.5) * step;
+  X T[3], DL[9], A[3], B[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) T[i] = R[3 * i] * tq[0] + R[3 * i + 1] * tq[1] + R[3 * i + 2] * tq[2];
+  expmap(-half * W[0], -half * W[1], -half * W[2], DL);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) A[i] = J[i] * W[0] + J[3 + i] * W[1] + J[6 + i] * W[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) B[i] = DL[i] * A[0] + DL[3 + i] * A[1] + DL[6 + i] * A[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) B[i] = B[i] + half * T[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) A[i] = Ji[i] * B[0] + Ji[3 + i] * B[1] + Ji[6 + i] * B[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) B[i] = J[i] * A[0] + J[3 + i] * A[1] + J[6 + i] * A[2];
+  T[0] -= A[1] * B[2] - A[2] * B[1];
+  T[1] -= A[2] * B[0] - A[0] * B[2];
+  T[2] -= A[0] * B[1] - A[1] * B[0];
+  T[0] *= step;
+  T[1] *= step;
+  T[2] *= step;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) s.ref_ang[b.at(i)] = (W[i] + Ji[i] * T[0] + Ji[3 + i] * T[1] + Ji[6 + i] * T[2]).v;
+}
+
+// ---------------------------------------------------------------------------------------
+// forces.cpp
+// ---------------------------------------------------------------------------------------
+
+struct ContactView {
+  const double *x, *normal, *depth;
+  const int32_t *master, *slave;
+  const uint8_t *friction;
+  int64_t cap;
+};
+
+// getContactsForces over contacts [c0, c1) of one partner pair, for body `a` (the
+// current particle) against `b`; sign = -1 applies the inverted normal stored for the
+// slave (Collision.cpp:176-184).  Sums into F, T from zero in list order.
+__device__ void pair_forces(const delta_scene &s, const ContactView &cv, int64_t c0, int64_t c1, int32_t a,
+                            int32_t b, bool negate, const delta_step_params &p, X F[3], X Tq[3]) {
+  const int32_t n = s.n_bodies;
+  X posA[3], angA[3], linA[3], posB[3], angB[3], linB[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    posA[k] = X(s.pos[(int64_t)k * n + a]);
+    angA[k] = X(s.ang[(int64_t)k * n + a]);
+    linA[k] = X(s.vel[(int64_t)k * n + a]);
+    posB[k] = X(s.pos[(int64_t)k * n + b]);
+    angB[k] = X(s.ang[(int64_t)k * n + b]);
+    linB[k] = X(s.vel[(int64_t)k * n + b]);
+  }
+  const X massA = X(s.mass[a]), massB = X(s.mass[b]);
+  const X spring = X(p.spring), damper = X(p.damper), mu = X(p.friction);
+  for (int k = 0; k < 3; ++k) {
+    F[k] = X(0.0);
+    Tq[k] = X(0.0);
+  }
+  for (int64_t c = c0; c < c1; ++c) {
+    X x[3], nn[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      x[k] = X(cv.x[k * cv.cap + c]);
+      const X nv = X(cv.normal[k * cv.cap + c]);
+      nn[k] = negate ? X(-1.0) * nv : nv;
+    }
+    const X depth = X(cv.depth[c]);
+    X z[3], vi[3], vj[3], vij[3];
+    for (int k = 0; k < 3; ++k) z[k] = x[k] - posA[k];
+    vi[0] = angA[1] * z[2] - angA[2] * z[1] + linA[0];
+    vi[1] = angA[2] * z[0] - angA[0] * z[2] + linA[1];
+    vi[2] = angA[0] * z[1] - angA[1] * z[0] + linA[2];
+    for (int k = 0; k < 3; ++k) z[k] = x[k] - posB[k];
+    vj[0] = angB[1] * z[2] - angB[2] * z[1] + linB[0];
+    vj[1] = angB[2] * z[0] - angB[0] * z[2] + linB[1];
+    vj[2] = angB[0] * z[1] - angB[1] * z[0] + linB[2];
+    for (int k = 0; k < 3; ++k) vij[k] = vj[k] - vi[k];
+    const X ma = X(1.0) / ((X(1.0) / massA) + (X(1.0) / massB));
+    const X velocity = (vij[0] * nn[0]) + (vij[1] * nn[1]) + (vij[2] * nn[2]);
+    const X damp = damper * X(2.0) * sqrt_(ma * spring) * velocity;
+    const X fmag = spring * depth + damp;
+    X f[3], fr[3] = {X(0.0), X(0.0), X(0.0)};
+    for (int k = 0; k < 3; ++k) f[k] = fmag * nn[k];
+    if (cv.friction[c]) {
+      const X vn = (vi[0] * nn[0]) + (vi[1] * nn[1]) + (vi[2] * nn[2]);
+      for (int k = 0; k < 3; ++k) {
+        const X vt = vi[k] - nn[k] * vn;
+        fr[k] = -vt * mu * fmag;
+      }
+    }
+    for (int k = 0; k < 3; ++k) F[k] += f[k] + fr[k];
+    X arm[3];
+    for (int k = 0; k < 3; ++k) arm[k] = x[k] - posA[k];
+    Tq[0] += arm[1] * (f[2]) - arm[2] * (f[1]);
+    Tq[1] += arm[2] * (f[0]) - arm[0] * (f[2]);
+    Tq[2] += arm[0] * (f[1]) - arm[1] * (f[0]);
+  }
+}
+
+__global__ void k_segment_heads(ContactView cv, int64_t n, uint8_t *head) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  head[c] = (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]) ? 1 : 0;
+}
+
+// One thread per partner pair: both sides' sums, keyed (body << 32 | partner).
+__global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_start, const int64_t *n_seg_p,
+                              int64_t n_contacts, delta_step_params p, uint64_t *key, int64_t *val_idx,
+                              double *entry) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n_seg = *n_seg_p;
+  if (g >= n_seg) return;
+  const int64_t c0 = seg_start[g], c1 = g + 1 < n_seg ? seg_start[g + 1] : n_contacts;
+  const int32_t i = cv.master[c0], j = cv.slave[c0];
+  X F[3], T[3];
+  pair_forces(s, cv, c0, c1, i, j, false, p, F, T);
+  for (int k = 0; k < 3; ++k) {
+    entry[(2 * g) * 6 + k] = F[k].v;
+    entry[(2 * g) * 6 + 3 + k] = T[k].v;
+  }
+  pair_forces(s, cv, c0, c1, j, i, true, p, F, T);
+  for (int k = 0; k < 3; ++k) {
+    entry[(2 * g + 1) * 6 + k] = F[k].v;
+    entry[(2 * g + 1) * 6 + 3 + k] = T[k].v;
+  }
+  key[2 * g] = ((uint64_t)(uint32_t)i << 32) | (uint32_t)j;
+  key[2 * g + 1] = ((uint64_t)(uint32_t)j << 32) | (uint32_t)i;
+  val_idx[2 * g] = 2 * g;
+  val_idx[2 * g + 1] = 2 * g + 1;
+}
+
+// One thread per body: partners in ascending order (entries sorted by key).
+// Entries past the valid ones carry the key ~0 and sort last; they match no body.
+__global__ void k_body_forces(int32_t n_bodies, const uint64_t *skey, const int64_t *sidx, const double *entry,
+                              int64_t ne, double *force, double *torque, uint8_t *has) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_bodies) return;
+  const uint64_t lo_key = (uint64_t)(uint32_t)i << 32;
+  int64_t lo = 0, hi = ne;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (skey[mid] < lo_key) lo = mid + 1;
+    else hi = mid;
+  }
+  X F[3] = {X(0.0), X(0.0), X(0.0)}, T[3] = {X(0.0), X(0.0), X(0.0)};
+  int64_t e = lo;
+  for (; e < ne && (skey[e] >> 32) == (uint64_t)(uint32_t)i; ++e) {
+    const double *v = entry + sidx[e] * 6;
+    for (int k = 0; k < 3; ++k) {
+      F[k] += X(v[k]);
+      T[k] += X(v[3 + k]);
+    }
+  }
+  for (int k = 0; k < 3; ++k) {
+    force[(int64_t)k * n_bodies + i] = F[k].v;
+    torque[(int64_t)k * n_bodies + i] = T[k].v;
+  }
+  has[i] = e > lo ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// integration
+// ---------------------------------------------------------------------------------------
+
+// Collision::touchVertexFirstTime velocity part (Collision.cpp:1105-1115) followed by
+// MoveParticles::moveAllParticlesAssociatedToVertex body part (MoveParticles.cpp:71-94).
+__global__ void k_bodies(delta_scene s, delta_step_params p, const double *force, const double *torque,
+                         const uint8_t *has) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_bodies || s.obstacle[i]) return;
+  const BodyRef b{s.n_bodies, i};
+  const X dt = X(p.dt);
+  if (has[i]) {
+    const X m = X(s.mass[i]);
+    X tq[3];
+    for (int k = 0; k < 3; ++k) {
+      s.vel[b.at(k)] = (X(s.vel[b.at(k)]) + dt * (X(force[b.at(k)]) / m)).v;
+      tq[k] = X(torque[b.at(k)]);
+    }
+    update_angular(s, b, tq, dt);
+  }
+  for (int k = 0; k < 3; ++k) s.vel[b.at(k)] = (X(s.vel[b.at(k)]) + dt * (X(p.gravity[k]))).v;
+  for (int k = 0; k < 3; ++k) s.pos[b.at(k)] = (X(s.pos[b.at(k)]) + dt * X(s.vel[b.at(k)])).v;
+  update_rotation(s, b, dt);
+}
+
+// updateVertices, dynamics.cpp:215-242, one thread per vertex.
+__global__ void k_vertices(delta_scene s, int64_t n_vertices) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n_vertices) return;
+  const int32_t i = s.tri_body[v / 3];
+  if (s.obstacle[i]) return;
+  const int32_t n = s.n_bodies;
+  X R[9], pos[3], rp[3];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) R[k] = X(s.rot[(int64_t)k * n + i]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    pos[k] = X(s.pos[(int64_t)k * n + i]);
+    rp[k] = X(s.ref_pos[(int64_t)k * n + i]);
+  }
+  const X C0 = X(s.rx[v]) - rp[0], C1 = X(s.ry[v]) - rp[1], C2 = X(s.rz[v]) - rp[2];
+  s.x[v] = (pos[0] + (R[0] * C0 + R[3] * C1 + R[6] * C2)).v;
+  s.y[v] = (pos[1] + (R[1] * C0 + R[4] * C1 + R[7] * C2)).v;
+  s.z[v] = (pos[2] + (R[2] * C0 + R[5] * C1 + R[8] * C2)).v;
+}
+
+// ---------------------------------------------------------------------------------------
+// broadphase: uniform grid for moving bodies, bounding boxes for obstacles
+// ---------------------------------------------------------------------------------------
+
+struct Grid {
+  double h;
+  double origin[3];
+};
+
+__device__ __forceinline__ uint64_t cell_key(int64_t cx, int64_t cy, int64_t cz) {
+  const int64_t M = (1 << 21) - 1;
+  cx = cx < 0 ? 0 : (cx > M ? M : cx);
+  cy = cy < 0 ? 0 : (cy > M ? M : cy);
+  cz = cz < 0 ? 0 : (cz > M ? M : cz);
+  return ((uint64_t)cx << 42) | ((uint64_t)cy << 21) | (uint64_t)cz;
+}
+
+__device__ __forceinline__ void cell_of(const delta_scene &s, const Grid &g, int32_t i, int64_t c[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) c[k] = (int64_t)floor((s.pos[(int64_t)k * s.n_bodies + i] - g.origin[k]) / g.h);
+}
+
+__global__ void k_cell_keys(delta_scene s, Grid g, uint64_t *key, int32_t *body) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_bodies) return;
+  int64_t c[3];
+  cell_of(s, g, i, c);
+  key[i] = s.obstacle[i] ? ~0ull : cell_key(c[0], c[1], c[2]);
+  body[i] = i;
+}
+
+__device__ __forceinline__ bool spheres_touch(const delta_scene &s, int32_t i, int32_t j) {
+  const int32_t n = s.n_bodies;
+  double d2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double d = s.pos[(int64_t)k * n + j] - s.pos[(int64_t)k * n + i];
+    d2 += d * d;
+  }
+  const double reach = (s.radius[i] + s.radius[j] + s.eps[i] + s.eps[j]) * (1.0 + 1e-9) + 1e-12;
+  return d2 <= reach * reach;
+}
+
+__device__ __forceinline__ void push_pair(int32_t a, int32_t b, uint64_t *out, unsigned long long *count, int64_t cap) {
+  const unsigned long long pos = atomicAdd(count, 1ull);
+  if ((int64_t)pos < cap) out[pos] = ((uint64_t)(uint32_t)(a < b ? a : b) << 32) | (uint32_t)(a < b ? b : a);
+}
+
+__global__ void k_grid_pairs(delta_scene s, Grid g, const uint64_t *skey, const int32_t *sbody, int32_t n_moving,
+                             uint64_t *out, unsigned long long *count, int64_t cap) {
+  const int32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_moving) return;
+  const int32_t i = sbody[p];
+  int64_t c[3];
+  cell_of(s, g, i, c);
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dz = -1; dz <= 1; ++dz) {
+        const uint64_t k = cell_key(c[0] + dx, c[1] + dy, c[2] + dz);
+        int32_t lo = 0, hi = n_moving;
+        while (lo < hi) {
+          const int32_t mid = (lo + hi) >> 1;
+          if (skey[mid] < k) lo = mid + 1;
+          else hi = mid;
+        }
+        for (int32_t q = lo; q < n_moving && skey[q] == k; ++q) {
+          const int32_t j = sbody[q];
+          if (j > i && spheres_touch(s, i, j)) push_pair(i, j, out, count, cap);
+        }
+      }
+}
+
+// obstacle L (box lo/hi) against every moving body j
+__global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const double *box, int32_t n_obst,
+                                 uint64_t *out, unsigned long long *count, int64_t cap) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n_obst * s.n_bodies) return;
+  const int32_t o = (int32_t)(t / s.n_bodies), j = (int32_t)(t % s.n_bodies);
+  const int32_t L = obst[o];
+  if (s.obstacle[j]) return;
+  double d2 = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    const double c = s.pos[(int64_t)k * s.n_bodies + j];
+    const double lo = box[6 * o + k], hi = box[6 * o + 3 + k];
+    const double d = c < lo ? lo - c : (c > hi ? c - hi : 0.0);
+    d2 += d * d;
+  }
+  const double reach = (s.radius[j] + s.eps[j] + s.eps[L]) * (1.0 + 1e-9) + 1e-12;
+  if (d2 <= reach * reach) push_pair(L, j, out, count, cap);
+}
+
+__global__ void k_unpack_pairs(const uint64_t *k, int64_t n, int32_t *a, int32_t *b) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  a[t] = (int32_t)(k[t] >> 32);
+  b[t] = (int32_t)(k[t] & 0xffffffffu);
+}
+
+__global__ void k_iota32(int32_t *v, int32_t n) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
+}
+
+inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+
+// Buffers owned by a force evaluation (context scratch slots 7..9).
+delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contacts &c, int64_t n_contacts,
+                        const delta_step_params &p, double *force, double *torque, uint8_t *has) {
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  delta_status ds;
+  const int32_t n = s.n_bodies;
+  if (n_contacts == 0) {
+    if ((e = cudaMemsetAsync(force, 0, sizeof(double) * 3 * n, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(torque, 0, sizeof(double) * 3 * n, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(has, 0, (size_t)n, st)) != cudaSuccess)
+      return cuda_error(e, "forces memset");
+    return DELTA_OK;
+  }
+  ContactView cv{c.x, c.normal, c.depth, c.master, c.slave, c.friction, c.capacity};
+  // scratch: head flags, segment starts, segment count, entries (2 per segment)
+  const size_t nc = (size_t)n_contacts;
+  void *buf = nullptr;
+  const size_t bytes = nc * (1 + 8 + 8 * 2 + 8 * 2 + 8 * 2 + 6 * 8 * 2) + 64;
+  if ((ds = ctx_scratch(ctx, 7, bytes, &buf)) != DELTA_OK) return ds;
+  char *b = (char *)buf;
+  int64_t *n_seg = (int64_t *)b; b += 64;
+  int64_t *seg_start = (int64_t *)b; b += 8 * nc;
+  uint64_t *key = (uint64_t *)b; b += 8 * 2 * nc;
+  uint64_t *skey = (uint64_t *)b; b += 8 * 2 * nc;
+  int64_t *idx = (int64_t *)b; b += 8 * 2 * nc;
+  int64_t *sidx = (int64_t *)b; b += 8 * 2 * nc;  // (fits: bytes above counts 8*2 for idx and sidx each)
+  double *entry = (double *)b; b += 6 * 8 * 2 * nc;
+  uint8_t *head = (uint8_t *)b;
+  k_segment_heads<<<blocks_for(n_contacts), 256, 0, st>>>(cv, n_contacts, head);
+  ctx->launches += 1;
+  // segment starts: indices where head == 1
+  size_t tb = 0;
+  cub::CountingInputIterator<int64_t> it(0);
+  cub::DeviceSelect::Flagged(nullptr, tb, it, head, seg_start, n_seg, n_contacts, st);
+  void *temp = nullptr;
+  if ((ds = ctx_scratch(ctx, 8, tb, &temp)) != DELTA_OK) return ds;
+  if ((e = cub::DeviceSelect::Flagged(temp, tb, it, head, seg_start, n_seg, n_contacts, st)) != cudaSuccess)
+    return cuda_error(e, "segment select");
+  ctx->launches += 1;
+  // entries for all potential segments (n_contacts bounds the count; unused keys sort last)
+  if ((e = cudaMemsetAsync(key, 0xff, sizeof(uint64_t) * 2 * nc, st)) != cudaSuccess) return cuda_error(e, "memset");
+  k_pair_forces<<<blocks_for(n_contacts, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, n_contacts, p, key, idx, entry);
+  ctx->launches += 1;
+  tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 64, st);
+  if ((ds = ctx_scratch(ctx, 8, tb, &temp)) != DELTA_OK) return ds;
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 64, st)) !=
+      cudaSuccess)
+    return cuda_error(e, "entry sort");
+  ctx->launches += 1;
+  k_body_forces<<<blocks_for(n), 256, 0, st>>>(n, skey, sidx, entry, (int64_t)(2 * nc), force, torque, has);
+  ctx->launches += 1;
+  return DELTA_OK;
+}
+
+delta_status integrate_run(delta_ctx *ctx, const delta_scene &s, const delta_step_params &p, const double *force,
+                           const double *torque, const uint8_t *has, int64_t n_vertices) {
+  cudaStream_t st = ctx->stream;
+  k_bodies<<<blocks_for(s.n_bodies, 128), 128, 0, st>>>(s, p, force, torque, has);
+  k_vertices<<<blocks_for(n_vertices), 256, 0, st>>>(s, n_vertices);
+  ctx->launches += 2;
+  return cuda_error(cudaGetLastError(), "integrate launch");
+}
+
+// Grid and obstacle boxes of a scene.  Obstacles are static: their boxes are computed
+// once from their current vertices.
+struct BroadphasePlan {
+  Grid g{};
+  int32_t n_obst = 0, n_moving = 0;
+  int32_t *d_obst = nullptr;  // obstacle body indices
+  double *d_box = nullptr;    // [6*n_obst] lo(3) hi(3)
+  void release() {
+    if (d_obst) cudaFree(d_obst);
+    if (d_box) cudaFree(d_box);
+    d_obst = nullptr;
+    d_box = nullptr;
+  }
+};
+
+delta_status broadphase_plan(delta_ctx *ctx, const delta_scene &s, BroadphasePlan &plan) {
+  const int32_t n = s.n_bodies;
+  cudaError_t e;
+  std::vector<double> pos(3 * (size_t)n), rad(n), eps(n);
+  std::vector<uint8_t> obst(n);
+  std::vector<int64_t> off(n + 1);
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess ||
+      (e = cudaMemcpy(pos.data(), s.pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(rad.data(), s.radius, sizeof(double) * n, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(eps.data(), s.eps, sizeof(double) * n, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(obst.data(), s.obstacle, n, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(off.data(), s.tri_offset, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return cuda_error(e, "broadphase plan copy");
+  double reach = 0.0, lo[3] = {1e300, 1e300, 1e300};
+  std::vector<int32_t> ob;
+  for (int32_t i = 0; i < n; ++i) {
+    if (obst[i]) {
+      ob.push_back(i);
+      continue;
+    }
+    reach = std::fmax(reach, rad[i] + eps[i]);
+    for (int k = 0; k < 3; ++k) lo[k] = std::fmin(lo[k], pos[(size_t)k * n + i]);
+  }
+  plan.release();
+  plan.g.h = reach > 0 ? 2.0 * reach * (1.0 + 1e-6) : 1.0;
+  for (int k = 0; k < 3; ++k) plan.g.origin[k] = (lo[k] < 1e299 ? lo[k] : 0.0) - (double)(1 << 20) * plan.g.h;
+  plan.n_obst = (int32_t)ob.size();
+  plan.n_moving = n - plan.n_obst;
+  if (plan.n_obst > 0) {
+    // obstacle boxes from their vertices
+    std::vector<double> box(6 * ob.size());
+    for (size_t o = 0; o < ob.size(); ++o) {
+      const int32_t L = ob[o];
+      const int64_t v0 = 3 * off[L], v1 = 3 * off[L + 1];
+      std::vector<double> xs(v1 - v0), ys(v1 - v0), zs(v1 - v0);
+      if ((e = cudaMemcpy(xs.data(), s.x + v0, sizeof(double) * (v1 - v0), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+          (e = cudaMemcpy(ys.data(), s.y + v0, sizeof(double) * (v1 - v0), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+          (e = cudaMemcpy(zs.data(), s.z + v0, sizeof(double) * (v1 - v0), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_error(e, "obstacle vertices");
+      double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
+      for (size_t q = 0; q < xs.size(); ++q) {
+        const double c[3] = {xs[q], ys[q], zs[q]};
+        for (int k = 0; k < 3; ++k) {
+          bl[k] = std::fmin(bl[k], c[k]);
+          bh[k] = std::fmax(bh[k], c[k]);
+        }
+      }
+      for (int k = 0; k < 3; ++k) {
+        box[6 * o + k] = bl[k];
+        box[6 * o + 3 + k] = bh[k];
+      }
+    }
+    if ((e = cudaMalloc(&plan.d_obst, sizeof(int32_t) * ob.size())) != cudaSuccess ||
+        (e = cudaMalloc(&plan.d_box, sizeof(double) * box.size())) != cudaSuccess ||
+        (e = cudaMemcpy(plan.d_obst, ob.data(), sizeof(int32_t) * ob.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(plan.d_box, box.data(), sizeof(double) * box.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cuda_error(e, "obstacle upload");
+  }
+  return DELTA_OK;
+}
+
+// Scratch slots 10 (cell keys), 11 (pair keys), 12 (sort temp).
+delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const BroadphasePlan &plan, int32_t *pair_a,
+                            int32_t *pair_b, int64_t capacity, int64_t *n_out) {
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  delta_status ds;
+  const int32_t n = s.n_bodies;
+  void *kb = nullptr;
+  if ((ds = ctx_scratch(ctx, 10, (sizeof(uint64_t) * 2 + sizeof(int32_t) * 2) * (size_t)n + 64, &kb)) != DELTA_OK)
+    return ds;
+  uint64_t *key = (uint64_t *)kb, *skey = key + n;
+  int32_t *body = (int32_t *)(skey + n), *sbody = body + n;
+  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body);
+  ctx->launches += 1;
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, body, sbody, n, 0, 64, st);
+  void *temp = nullptr;
+  if ((ds = ctx_scratch(ctx, 12, tb, &temp)) != DELTA_OK) return ds;
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, 64, st)) != cudaSuccess)
+    return cuda_error(e, "cell sort");
+  ctx->launches += 1;
+  int64_t cap = capacity > 4096 ? capacity : 4096;
+  unsigned long long hcount = 0;
+  uint64_t *pk = nullptr;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    void *pb = nullptr;
+    if ((ds = ctx_scratch(ctx, 11, sizeof(uint64_t) * 2 * (size_t)cap + 64, &pb)) != DELTA_OK) return ds;
+    unsigned long long *count = (unsigned long long *)pb;
+    pk = (uint64_t *)pb + 8;
+    if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess) return cuda_error(e, "memset");
+    if (plan.n_moving > 0) {
+      k_grid_pairs<<<blocks_for(plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, pk, count,
+                                                                   cap);
+      ctx->launches += 1;
+    }
+    if (plan.n_obst > 0) {
+      k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
+                                                                            pk, count, cap);
+      ctx->launches += 1;
+    }
+    if ((e = cudaMemcpyAsync(&hcount, count, sizeof(hcount), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return cuda_error(e, "broadphase count");
+    if ((int64_t)hcount <= cap) break;
+    cap = (int64_t)hcount + hcount / 2;
+  }
+  const int64_t np = (int64_t)hcount;
+  *n_out = np;
+  if (np == 0) return DELTA_OK;
+  uint64_t *spk = pk + cap;
+  tb = 0;
+  cub::DeviceRadixSort::SortKeys(nullptr, tb, pk, spk, np, 0, 64, st);
+  if ((ds = ctx_scratch(ctx, 12, tb, &temp)) != DELTA_OK) return ds;
+  if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, np, 0, 64, st)) != cudaSuccess)
+    return cuda_error(e, "pair sort");
+  ctx->launches += 1;
+  const int64_t wn = np < capacity ? np : capacity;
+  if (wn > 0) {
+    k_unpack_pairs<<<blocks_for(wn), 256, 0, st>>>(spk, wn, pair_a, pair_b);
+    ctx->launches += 1;
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "broadphase");
+  if (np > capacity) return set_error(DELTA_ERR_CAPACITY, "delta_broadphase: pair capacity exceeded");
+  return DELTA_OK;
+}
+
+}  // namespace delta
+
+// ---------------------------------------------------------------------------------------
+// simulation object
+// ---------------------------------------------------------------------------------------
+
+struct delta_sim {
+  delta_ctx *ctx = nullptr;
+  delta_scene scene{};
+  int driver = DELTA_DRV_BF;
+  delta::BroadphasePlan plan;
+  int64_t n_tri = 0;
+  int32_t *ids = nullptr;
+  // contacts of the last detection
+  delta_contacts c{};
+  void *c_mem = nullptr;
+  int64_t n_contacts = 0;
+  // pairs and per-body sums
+  int32_t *pa = nullptr, *pb = nullptr;
+  int64_t pair_cap = 0;
+  double *F = nullptr, *T = nullptr;
+  uint8_t *has = nullptr;
+};
+
+namespace delta {
+
+static delta_status alloc_contacts(delta_sim *s, int64_t cap) {
+  if (s->c_mem) cudaFree(s->c_mem);
+  s->c_mem = nullptr;
+  const size_t per = 14 * sizeof(double) + 5 * sizeof(int32_t) + 1;
+  cudaError_t e = cudaMalloc(&s->c_mem, per * (size_t)cap + 256);
+  if (e != cudaSuccess) return cuda_error(e, "contact buffer");
+  double *d = (double *)s->c_mem;
+  s->c.capacity = cap;
+  s->c.x = d;
+  s->c.normal = d + 3 * cap;
+  s->c.P = d + 6 * cap;
+  s->c.Q = d + 9 * cap;
+  s->c.depth = d + 12 * cap;
+  s->c.eps_total = d + 13 * cap;
+  int32_t *ip = (int32_t *)(d + 14 * cap);
+  s->c.master = ip;
+  s->c.slave = ip + cap;
+  s->c.tri_a = ip + 2 * cap;
+  s->c.tri_b = ip + 3 * cap;
+  s->c.penetration = ip + 4 * cap;
+  s->c.friction = (uint8_t *)(ip + 5 * cap);
+  return DELTA_OK;
+}
+
+static delta_status alloc_pairs(delta_sim *s, int64_t cap) {
+  if (s->pa) cudaFree(s->pa);
+  s->pa = nullptr;
+  cudaError_t e = cudaMalloc(&s->pa, sizeof(int32_t) * 2 * (size_t)cap);
+  if (e != cudaSuccess) return cuda_error(e, "pair buffer");
+  s->pb = s->pa + cap;
+  s->pair_cap = cap;
+  return DELTA_OK;
+}
+
+static delta_status sim_detect(delta_sim *s) {
+  delta_status ds;
+  int64_t np = 0;
+  ds = broadphase_run(s->ctx, s->scene, s->plan, s->pa, s->pb, s->pair_cap, &np);
+  if (ds == DELTA_ERR_CAPACITY) {
+    if ((ds = alloc_pairs(s, np + np / 2 + 1024)) != DELTA_OK) return ds;
+    ds = broadphase_run(s->ctx, s->scene, s->plan, s->pa, s->pb, s->pair_cap, &np);
+  }
+  if (ds != DELTA_OK) return ds;
+  delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
+                 s->scene.eps,      s->scene.friction,   s->ids};
+  int64_t nc = 0;
+  if (np == 0) {
+    s->n_contacts = 0;
+    return DELTA_OK;
+  }
+  ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr);
+  if (ds == DELTA_ERR_CAPACITY) {
+    if ((ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;
+    ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr);
+  }
+  if (ds != DELTA_OK) return ds;
+  s->n_contacts = nc;
+  return DELTA_OK;
+}
+
+}  // namespace delta
+
+using namespace delta;
+
+extern "C" {
+
+delta_status delta_forces(delta_ctx *ctx, const delta_scene *scene, const delta_contacts *contacts,
+                          int64_t n_contacts, const delta_step_params *params, double *force, double *torque,
+                          uint8_t *has_contact) {
+  if (!ctx || !scene || !params || !force || !torque || !has_contact || (n_contacts > 0 && !contacts))
+    return set_error(DELTA_ERR_INVALID, "delta_forces: null argument");
+  if (n_contacts < 0 || (contacts && n_contacts > contacts->capacity))
+    return set_error(DELTA_ERR_INVALID, "delta_forces: bad contact count");
+  delta_contacts empty{};
+  return forces_run(ctx, *scene, contacts ? *contacts : empty, n_contacts, *params, force, torque, has_contact);
+}
+
+delta_status delta_integrate(delta_ctx *ctx, const delta_scene *scene, const delta_step_params *params,
+                             const double *force, const double *torque, const uint8_t *has_contact) {
+  if (!ctx || !scene || !params || !force || !torque || !has_contact)
+    return set_error(DELTA_ERR_INVALID, "delta_integrate: null argument");
+  int64_t ntri = 0;
+  cudaError_t e = cudaMemcpyAsync(&ntri, scene->tri_offset + scene->n_bodies, sizeof(int64_t),
+                                  cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "delta_integrate");
+  return integrate_run(ctx, *scene, *params, force, torque, has_contact, 3 * ntri);
+}
+
+delta_status delta_broadphase(delta_ctx *ctx, const delta_scene *scene, int32_t *pair_a, int32_t *pair_b,
+                              int64_t capacity, int64_t *n_out) {
+  if (!ctx || !scene || !n_out || (capacity > 0 && (!pair_a || !pair_b)))
+    return set_error(DELTA_ERR_INVALID, "delta_broadphase: null argument");
+  BroadphasePlan plan;
+  delta_status ds = broadphase_plan(ctx, *scene, plan);
+  if (ds == DELTA_OK) ds = broadphase_run(ctx, *scene, plan, pair_a, pair_b, capacity, n_out);
+  cudaStreamSynchronize(ctx->stream);
+  plan.release();
+  return ds;
+}
+
+delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driver, delta_sim **out) {
+  if (!ctx || !scene || !out) return set_error(DELTA_ERR_INVALID, "delta_sim_create: null argument");
+  if (driver != DELTA_DRV_BF && driver != DELTA_DRV_BF_CERT)
+    return set_error(DELTA_ERR_UNSUPPORTED, "delta_sim_create: the time step runs DELTA_DRV_BF or DELTA_DRV_BF_CERT");
+  delta_sim *s = new delta_sim();
+  s->ctx = ctx;
+  s->scene = *scene;
+  s->driver = driver;
+  const int32_t n = scene->n_bodies;
+  cudaError_t e = cudaMemcpy(&s->n_tri, scene->tri_offset + n, sizeof(int64_t), cudaMemcpyDeviceToHost);
+  delta_status ds = DELTA_OK;
+  if (e != cudaSuccess) ds = cuda_error(e, "sim create");
+  if (ds == DELTA_OK && (e = cudaMalloc(&s->ids, sizeof(int32_t) * n)) != cudaSuccess) ds = cuda_error(e, "ids");
+  if (ds == DELTA_OK && (e = cudaMalloc(&s->F, sizeof(double) * 6 * n + n)) != cudaSuccess) ds = cuda_error(e, "F");
+  if (ds == DELTA_OK) {
+    s->T = s->F + 3 * n;
+    s->has = (uint8_t *)(s->T + 3 * n);
+    k_iota32<<<blocks_for(n), 256, 0, ctx->stream>>>(s->ids, n);
+    ctx->launches += 1;
+    ds = broadphase_plan(ctx, *scene, s->plan);
+  }
+  if (ds == DELTA_OK) ds = alloc_contacts(s, 1 << 16);
+  if (ds == DELTA_OK) ds = alloc_pairs(s, 1 << 14);
+  if (ds != DELTA_OK) {
+    delta_sim_destroy(s);
+    return ds;
+  }
+  *out = s;
+  return DELTA_OK;
+}
+
+delta_status delta_sim_step(delta_sim *s, const delta_step_params *params, int32_t nsteps,
+                            int64_t *contacts_per_step) {
+  if (!s || !params || nsteps < 0) return set_error(DELTA_ERR_INVALID, "delta_sim_step: bad argument");
+  for (int32_t k = 0; k < nsteps; ++k) {
+    delta_status ds = forces_run(s->ctx, s->scene, s->c, s->n_contacts, *params, s->F, s->T, s->has);
+    if (ds != DELTA_OK) return ds;
+    if ((ds = integrate_run(s->ctx, s->scene, *params, s->F, s->T, s->has, 3 * s->n_tri)) != DELTA_OK) return ds;
+    if ((ds = sim_detect(s)) != DELTA_OK) return ds;
+    if (contacts_per_step) contacts_per_step[k] = s->n_contacts;
+  }
+  return DELTA_OK;
+}
+
+delta_status delta_sim_contacts(delta_sim *s, const delta_contacts *out, int64_t *n_out) {
+  if (!s || !out || !n_out) return set_error(DELTA_ERR_INVALID, "delta_sim_contacts: null argument");
+  *n_out = s->n_contacts;
+  const int64_t n = s->n_contacts < out->capacity ? s->n_contacts : out->capacity;
+  cudaStream_t st = s->ctx->stream;
+  const int64_t ic = s->c.capacity, oc = out->capacity;
+  cudaError_t e = cudaSuccess;
+  if (n > 0) {
+    auto cp3 = [&](double *dst, const double *src) {
+      for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+        e = cudaMemcpyAsync(dst + k * oc, src + k * ic, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+    };
+    cp3(out->x, s->c.x);
+    cp3(out->normal, s->c.normal);
+    cp3(out->P, s->c.P);
+    cp3(out->Q, s->c.Q);
+    const void *srcs[] = {s->c.depth, s->c.eps_total, s->c.master, s->c.slave, s->c.tri_a, s->c.tri_b,
+                          s->c.penetration, s->c.friction};
+    void *dsts[] = {out->depth, out->eps_total, out->master, out->slave, out->tri_a, out->tri_b, out->penetration,
+                    out->friction};
+    const size_t sz[] = {8, 8, 4, 4, 4, 4, 4, 1};
+    for (int k = 0; k < 8 && e == cudaSuccess; ++k)
+      e = cudaMemcpyAsync(dsts[k], srcs[k], sz[k] * n, cudaMemcpyDeviceToDevice, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_error(e, "delta_sim_contacts");
+  if (s->n_contacts > out->capacity) return set_error(DELTA_ERR_CAPACITY, "delta_sim_contacts: capacity");
+  return DELTA_OK;
+}
+
+delta_status delta_sim_destroy(delta_sim *s) {
+  if (!s) return DELTA_OK;
+  cudaStreamSynchronize(s->ctx->stream);
+  s->plan.release();
+  if (s->ids) cudaFree(s->ids);
+  if (s->F) cudaFree(s->F);
+  if (s->c_mem) cudaFree(s->c_mem);
+  if (s->pa) cudaFree(s->pa);
+  delete s;
+  return DELTA_OK;
+}
+
+}  // extern "C"

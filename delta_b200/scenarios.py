@@ -254,3 +254,81 @@ def narrowphase_pairs_chunked(n: int, seed: int = 0, chunk: int = 1 << 20, worke
     d = np.concatenate([p[2] for p in parts])
     cls = np.concatenate([p[3] for p in parts])
     return a, b, d, cls
+
+
+# ---------------------------------------------------------------------------------------
+# rigid-body scenes
+# ---------------------------------------------------------------------------------------
+def mass_properties(V, F, density):
+    """Mass, centre of mass and inertia tensor (about the centre) of the solid bounded by
+    the closed, outward-wound mesh (V, F): sum of the signed tetrahedra (origin, a, b, c),
+    each with covariance det * A C0 A^T, C0 = [[2,1,1],[1,2,1],[1,1,2]]/120."""
+    o = V.mean(0)
+    T = V[F] - o  # (nT, 3 vertices, 3)
+    det = np.einsum("ij,ij->i", T[:, 0], np.cross(T[:, 1], T[:, 2]))
+    vol = det.sum() / 6.0
+    mass = density * vol
+    com = o + (det[:, None] * T.sum(1)).sum(0) / (24.0 * vol)
+    C0 = (np.ones((3, 3)) + np.eye(3)) / 120.0
+    Acol = np.transpose(T, (0, 2, 1))  # columns are the vertices
+    cov = density * np.einsum("n,nij,jk,nlk->il", det, Acol, C0, Acol)
+    d = (com - o)[:, None]
+    cov_c = cov - mass * (d @ d.T)
+    inertia = np.trace(cov_c) * np.eye(3) - cov_c
+    return mass, com, inertia
+
+
+def lattice_scene(seed: int = 0, nx: int = 8, ny: int = 4, nz: int = 8, spacing: float = 0.025,
+                  jitter: float = 0.002, radius: float = 0.01, perturb=(0.8, 1.2), n_tri: int = 80,
+                  density: float = 2500.0, eps: float = 1e-4, floor_half: float = 0.5, friction: bool = False):
+    """The small plain-method workload: perturbed sphere meshes on an nx*ny*nz lattice
+    (y vertical) above a floor of two triangles at y = 0 spanning (2*floor_half)^2."""
+    rng = np.random.default_rng(seed)
+    bodies = []
+    base = np.array([-(nx - 1) / 2 * spacing, 1.5 * radius * perturb[1], -(nz - 1) / 2 * spacing])
+    for ix in range(nx):
+        for iy in range(ny):
+            for iz in range(nz):
+                V, F = sphere_mesh(n_tri, rng, radius, perturb)
+                c = base + np.array([ix, iy, iz]) * spacing + rng.uniform(-jitter, jitter, 3)
+                bodies.append((V + c, F))
+    h = floor_half
+    floor_V = np.array([[-h, 0, -h], [h, 0, -h], [h, 0, h], [-h, 0, h]], float)
+    floor_F = np.array([[0, 2, 1], [0, 3, 2]])
+    return build_scene(bodies, obstacles=[(floor_V, floor_F)], density=density, eps=eps, friction=friction)
+
+
+def build_scene(bodies, obstacles=(), density=2500.0, eps=1e-4, friction=False):
+    """Scene dict (AoS per body: pos[3n], rot[9n], ...; SoA-tri vertices) from lists of
+    (V, F) meshes in world coordinates.  Moving bodies first, then obstacles."""
+    all_meshes = [(V, F, False) for V, F in bodies] + [(V, F, True) for V, F in obstacles]
+    n = len(all_meshes)
+    counts = [F.shape[0] for _, F, _ in all_meshes]
+    tri_offset = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    xyz = np.concatenate([V[F].reshape(-1, 3) for V, F, _ in all_meshes])
+    pos = np.zeros((n, 3)); inertia = np.zeros((n, 3, 3)); inverse = np.zeros((n, 3, 3))
+    mass = np.zeros(n); radius = np.zeros(n); obst = np.zeros(n, np.uint8)
+    for i, (V, F, is_obst) in enumerate(all_meshes):
+        if is_obst:
+            c = V.mean(0)
+            pos[i] = c
+            mass[i] = np.inf
+            obst[i] = 1
+        else:
+            m, c, J = mass_properties(V, F, density)
+            pos[i], mass[i], inertia[i] = c, m, J
+            inverse[i] = np.linalg.inv(J)
+        radius[i] = np.linalg.norm(V - pos[i], axis=1).max()
+    tri_body = np.repeat(np.arange(n, dtype=np.int32), counts)
+    rot = np.tile(np.eye(3).reshape(9), n)
+    # 3x3 matrices are stored column-major (dynamics.cpp); J and its inverse are symmetric
+    return {
+        "n_bodies": n, "tri_offset": tri_offset, "tri_body": tri_body,
+        "x": xyz[:, 0].copy(), "y": xyz[:, 1].copy(), "z": xyz[:, 2].copy(),
+        "rx": xyz[:, 0].copy(), "ry": xyz[:, 1].copy(), "rz": xyz[:, 2].copy(),
+        "pos": pos.reshape(-1).copy(), "ref_pos": pos.reshape(-1).copy(),
+        "vel": np.zeros(3 * n), "ang": np.zeros(3 * n), "ref_ang": np.zeros(3 * n), "rot": rot,
+        "inertia": inertia.transpose(0, 2, 1).reshape(-1).copy(), "inverse": inverse.transpose(0, 2, 1).reshape(-1).copy(),
+        "mass": mass, "eps": np.full(n, eps), "radius": radius,
+        "friction": np.full(n, 1 if friction else 0, np.uint8), "obstacle": obst,
+    }

@@ -142,6 +142,75 @@ delta_status delta_detect(delta_ctx *ctx, int driver, int precision, const delta
                           const int32_t *pair_a, const int32_t *pair_b, int64_t n_pairs,
                           const delta_contacts *out, int64_t *n_out, delta_stats *stats);
 
+/* ---- forces, integration, broadphase, time step -------------------------------------- */
+/* Rigid bodies (device arrays).  Per-body vectors are SoA planes: component k of body i
+ * is at [k*n_bodies + i]; rot is the 3x3 orientation stored column-major as in
+ * delta/dynamics/dynamics.cpp (rot[(3*col+row)*n_bodies + i]). */
+typedef struct {
+  int32_t n_bodies;
+  const int64_t *tri_offset;   /* [n_bodies+1] */
+  const int32_t *tri_body;     /* [n_triangles] owner body of each triangle */
+  double *x, *y, *z;           /* spatial vertices, SoA-tri */
+  const double *rx, *ry, *rz;  /* referential vertices, SoA-tri */
+  double *pos;                 /* [3n] spatial centre of mass */
+  const double *ref_pos;       /* [3n] referential centre of mass */
+  double *vel;                 /* [3n] linear velocity */
+  double *ang;                 /* [3n] spatial angular velocity */
+  double *ref_ang;             /* [3n] referential angular velocity */
+  double *rot;                 /* [9n] orientation */
+  const double *inertia;       /* [9n] */
+  const double *inverse;       /* [9n] */
+  const double *mass;          /* [n] (obstacles: +inf) */
+  const double *eps;           /* [n] contact halo epsilon */
+  const double *radius;        /* [n] bounding-sphere radius about pos */
+  const uint8_t *friction;     /* [n] */
+  const uint8_t *obstacle;     /* [n] obstacles never move */
+} delta_scene;
+
+typedef struct {
+  double dt;
+  double gravity[3];  /* added to the velocity as dt*gravity (MoveParticles.cpp:73 uses 9.8 along -y) */
+  double spring;      /* SPRING, forces.cpp:11-14 */
+  double damper;      /* DAMPER */
+  double friction;    /* FRICTION */
+} delta_step_params;
+
+/* Per-body force and torque from contacts sorted by (master, slave, tri_a, tri_b) with
+ * master/slave = body indices: for each body, the contributions of its partners in
+ * ascending partner order, each partner's contacts summed in list order
+ * (Collision::touchVertexFirstTime, Collision.cpp:1060-1101 -> getContactsForces,
+ * forces.cpp:291-396; the slave side uses the inverted normal, Collision.cpp:176-184).
+ * force, torque: [3n] planes; has_contact: [n] (1 where the body has a partner). */
+delta_status delta_forces(delta_ctx *ctx, const delta_scene *scene, const delta_contacts *contacts,
+                          int64_t n_contacts, const delta_step_params *params, double *force,
+                          double *torque, uint8_t *has_contact);
+
+/* v += dt*F/m and updateAngular (dynamics.cpp:140-213) for bodies with a contact
+ * (Collision.cpp:1105-1115), then for every non-obstacle body v += dt*g, x += dt*v,
+ * updateRotationMatrix (dynamics.cpp:104-138) and updateVertices (dynamics.cpp:215-242)
+ * (MoveParticles.cpp:63-112). */
+delta_status delta_integrate(delta_ctx *ctx, const delta_scene *scene, const delta_step_params *params,
+                             const double *force, const double *torque, const uint8_t *has_contact);
+
+/* Candidate body pairs (a < b, not both obstacles) whose bounding spheres, grown by the
+ * two epsilons, overlap; sorted by (a, b).  A superset of the pairs that can hold a
+ * contact (replaces the Peano grid traversal + isSphereOverlayInContact precheck,
+ * Collision.cpp:893-958, sphere.cpp:203-218).  *n_out receives the count; beyond
+ * `capacity` DELTA_ERR_CAPACITY.  Synchronises. */
+delta_status delta_broadphase(delta_ctx *ctx, const delta_scene *scene, int32_t *pair_a, int32_t *pair_b,
+                              int64_t capacity, int64_t *n_out);
+
+/* A simulation: the scene plus the contacts of the last detection.  One step follows
+ * the multiscale order: forces from the previous detection's contacts, velocity and
+ * angular update, move, then broadphase and narrowphase with `driver`. */
+typedef struct delta_sim delta_sim;
+delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driver, delta_sim **out);
+delta_status delta_sim_step(delta_sim *sim, const delta_step_params *params, int32_t nsteps,
+                            int64_t *contacts_per_step /* host [nsteps] or NULL */);
+/* Copies the current contacts into out (device); *n_out gets their number. */
+delta_status delta_sim_contacts(delta_sim *sim, const delta_contacts *out, int64_t *n_out);
+delta_status delta_sim_destroy(delta_sim *sim);
+
 #ifdef __cplusplus
 }
 #endif

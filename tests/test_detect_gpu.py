@@ -53,7 +53,7 @@ def test_drivers_bit_exact_vs_oracle(ctx, oracle, driver):
         o, hist, fails = _oracle_contacts(oracle, driver, bodies, pa, pb, eps_b, fric, ids)
         assert len(g) == len(o) and len(g) > 0
         for f in FIELDS:
-            assert np.array_equal(g[f], o[f]), (driver, f)
+            assert np.array_equal(g[f], o[f], equal_nan=True), (driver, f)
         if driver == 2:
             assert list(st.newton_hist) == list(hist)
         if driver in (5, 6):
@@ -70,7 +70,7 @@ def test_bf_cert_driver_equals_bf(ctx):
         b = detect(ctx, DRV_BF_CERT, m, pa, pb)[0].to_numpy()
         assert len(a) == len(b) and len(a) > 0
         for f in FIELDS:
-            assert np.array_equal(a[f], b[f]), f
+            assert np.array_equal(a[f], b[f], equal_nan=True), f
 
 
 def test_golden_driver_fixture(ctx, golden):
@@ -85,7 +85,7 @@ def test_golden_driver_fixture(ctx, golden):
         ref = g[f"contacts_{d}"]
         assert len(c) == len(ref)
         for f in FIELDS[:10]:
-            assert np.array_equal(c[f], ref[f]), (d, f)
+            assert np.array_equal(c[f], ref[f], equal_nan=True), (d, f)
 
 
 def test_capacity_error_reports_needed_size(ctx):
