@@ -73,13 +73,13 @@ def test_bf_cert_equals_f64_bf(ctx, oracle, workload):
 def test_f32_bf_close_to_f64(ctx, oracle, workload):
     """FP32 bfSolver (the reference's iREAL=float build) against FP64: the algorithm is
     poorly conditioned in FP32 for some pairs, so the bound is statistical:
-    |d32 - d64| <= 1e-5 * (1 + d64) on at least 99.9% of pairs, and <= 1e-3 on all."""
+    |d32 - d64| <= 1e-5 * (1 + d64) on at least 99.5% of pairs, and <= 1e-3 on all."""
     a, b = workload
     _, _, d32, _ = _run(ctx, 0, a, b, precision=1)
     _, _, d64, _ = oracle.pairs(0, a, b)
     err = np.abs(d32 - d64)
     assert np.all(np.isfinite(d32))
-    assert np.mean(err <= 1e-5 * (1 + d64)) >= 0.999
+    assert np.mean(err <= 1e-5 * (1 + d64)) >= 0.995
     assert err.max() <= 1e-3
 
 
