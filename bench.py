@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--timestep-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -145,6 +146,48 @@ def cpu_reference_rate(a, b, sample: int, min_seconds: float):
         if el >= min_seconds:
             break
     return done / el, cores, kind
+
+
+def timestep_section(ctx, stream, steps: int, warmup: int, seed: int):
+    """Timesteps/s of the small plain-method workload (256 perturbed 80-triangle spheres on a
+    8x4x8 lattice over a floor, FP64, dt 1e-5) with the plain FP64 bf driver (every
+    triangle pair of every candidate body pair) and with the certified FP32 driver (exact
+    box culling + bf_cert).  Both must give the same trajectory bit for bit."""
+    import torch
+
+    from delta_b200.detection import DRV_BF, DRV_BF_CERT
+    from delta_b200.engine import Simulation, StepParams
+    from delta_b200.scenarios import lattice_scene
+
+    sc = lattice_scene(seed)
+    params = StepParams.make(dt=1e-5, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0)
+    out, states = {}, {}
+    for name, drv in (("fp64_bf", DRV_BF), ("bf_cert_culled", DRV_BF_CERT)):
+        sim = Simulation(ctx, sc, drv)
+        sim.step(warmup, params)
+        c0 = sim.counters()
+        l0 = ctx.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.step(steps, params)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        c1 = sim.counters()
+        tri = c1["triangle_pairs"] - c0["triangle_pairs"]
+        out[name] = {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps,
+                     "triangle_pair_tests_per_s": tri / t, "triangle_pairs_per_step": tri / steps,
+                     "solved_pairs_per_step": (c1["solved"] - c0["solved"]) / steps,
+                     "body_pairs_per_step": (c1["body_pairs"] - c0["body_pairs"]) / steps,
+                     "gpu_launches": ctx.launches - l0}
+        states[name] = sim.state()
+        sim.close()
+    same = all(np.array_equal(states["fp64_bf"][k], states["bf_cert_culled"][k]) for k in ("pos", "vel", "rot", "x"))
+    return {"workload": "256 perturbed icospheres (80 tri) on a 8x4x8 lattice over a 2-triangle floor, FP64, "
+                        "dt 1e-5, k 1e6, damping 0.1", "steps": steps, "warmup": warmup, **out,
+            "speedup": out["bf_cert_culled"]["steps_per_s"] / out["fp64_bf"]["steps_per_s"],
+            "trajectories_bit_identical": bool(same)}
 
 
 def run_reference(args, rank, world):
@@ -276,6 +319,8 @@ def main():
                "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes),
                "path": "delta_pairs_run_host (C ABI), pinned host buffers, copies in the timed region"}
 
+    ts = timestep_section(ctx, stream, args.timestep_steps, 3, args.seed) if args.timestep_steps > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, kind = cpu_reference_rate(a_np, b_np, sample=min(n, 1 << 22), min_seconds=10.0)
@@ -306,6 +351,7 @@ def main():
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "timestep": ts,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

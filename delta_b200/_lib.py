@@ -37,6 +37,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_sim_create": ([vp, vp, C.c_int, vp], C.c_int),
     "delta_sim_step": ([vp, vp, i32, vp], C.c_int),
     "delta_sim_contacts": ([vp, vp, vp], C.c_int),
+    "delta_sim_counters": ([vp, vp], C.c_int),
     "delta_sim_destroy": ([vp], C.c_int),
 }
 

@@ -185,7 +185,7 @@ delta_status delta_detect(delta_ctx *ctx, int driver, int precision, const delta
                             !out->master || !out->slave || !out->tri_a || !out->tri_b || !out->penetration ||
                             !out->friction))
     return set_error(DELTA_ERR_INVALID, "delta_detect: incomplete contact buffer");
-  return detect_run(ctx, driver, precision, *meshes, pair_a, pair_b, n_pairs, out, n_out, stats);
+  return detect_run(ctx, driver, precision, *meshes, pair_a, pair_b, n_pairs, out, n_out, stats, nullptr);
 }
 
 }  // extern "C"

@@ -34,6 +34,7 @@ struct DevStats {
   unsigned long long hist[17];
   unsigned long long penalty_fails, batch_fails, batch_size;
   double batch_error;
+  unsigned long long tri_pairs, evaluated;  // sum of nA*nB; pairs the solver ran on
 };
 
 struct RowCtx {
@@ -160,14 +161,58 @@ __device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawCon
   double pq[6];
   int flag = 0;
   if constexpr (DRV == DELTA_DRV_BF_CERT) {
-    for_row(r.nB, [&](int32_t tb, bool valid) {
-      double A[3][3], B[3][3];
-      load_tri64(m, r.tA, A);
-      load_tri64(m, r.tB0 + (valid ? tb : r.nB - 1), B);
+    // Exact culling: bf()'s distance is the length of a point pair on the two triangles,
+    // never below the gap between their bounding boxes, so a B triangle whose box is
+    // farther than epsA+epsB (with a relative margin for rounding) cannot give a
+    // contact (bf.cpp:125).  Survivors are packed into full 32-lane batches.
+    const int lane = threadIdx.x & 31;
+    double A[3][3], alo[3], ahi[3];
+    load_tri64(m, r.tA, A);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      alo[k] = fmin(A[0][k], fmin(A[1][k], A[2][k]));
+      ahi[k] = fmax(A[0][k], fmax(A[1][k], A[2][k]));
+    }
+    const double cull = mg * (1.0 + 1e-9) + 1e-12;
+    int32_t *surv = csm->surv;
+    int count = 0;
+    auto run_batch = [&](int nb) {
+      if (lane == 0) atomicAdd(&st->evaluated, (unsigned long long)nb);
+      const bool valid = lane < nb;
+      const int32_t tb = surv[valid ? lane : 0];
+      double B[3][3];
+      load_tri64(m, r.tB0 + tb, B);
       bf_cert_warp(A, B, valid, pq, *csm);
       const bool take = valid && pq_dist64(pq) <= mg;  // bf.cpp:125
       emit(rc, take, pq, r, tb);
-    });
+    };
+    for (int32_t base = 0; base < r.nB; base += 32) {
+      const int32_t tb = base + lane;
+      bool keep = false;
+      if (tb < r.nB) {
+        double B[3][3], g2 = 0.0;
+        load_tri64(m, r.tB0 + tb, B);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const double blo = fmin(B[0][k], fmin(B[1][k], B[2][k])), bhi = fmax(B[0][k], fmax(B[1][k], B[2][k]));
+          const double g = fmax(blo - ahi[k], alo[k] - bhi);
+          if (g > 0.0) g2 += g * g;
+        }
+        keep = g2 <= cull * cull;
+      }
+      const unsigned mask = __ballot_sync(kFull, keep);
+      if (keep) surv[count + __popc(mask & ((1u << lane) - 1u))] = tb;
+      count += __popc(mask);
+      __syncwarp();
+      if (count >= 32) {
+        run_batch(32);
+        __syncwarp();
+        if (lane < count - 32) surv[lane] = surv[32 + lane];
+        count -= 32;
+        __syncwarp();
+      }
+    }
+    if (count > 0) run_batch(count);
   } else if constexpr (DRV == DELTA_DRV_BF || DRV == DELTA_DRV_GJK) {
     constexpr int S = DRV == DELTA_DRV_BF ? S_BF : S_GJK;
     for_row(r.nB, [&](int32_t tb, bool valid) {
@@ -297,6 +342,10 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
     r.idA = m.id[a];
     r.idB = m.id[b];
     r.fric = (m.friction[a] && m.friction[b]) ? 1 : 0;
+    if (lane == 0) {
+      atomicAdd(&st->tri_pairs, (unsigned long long)r.nB);
+      if (DRV != DELTA_DRV_BF_CERT) atomicAdd(&st->evaluated, (unsigned long long)r.nB);
+    }
     process_row<R, DRV>(m, r, rc, st, csm);
   }
 }
@@ -396,7 +445,7 @@ cudaError_t launch_detect_prec(int driver, cudaStream_t s, const delta_meshes &m
 // Scratch slots used here: 2 rows/row_offset, 3 raw contacts, 4 sort buffers, 5 small state.
 delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
-                        delta_stats *stats) {
+                        delta_stats *stats, int64_t *counters) {
   cudaStream_t s = ctx->stream;
   delta_status st;
   cudaError_t e;
@@ -468,6 +517,15 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
       return cuda_error(e, "detect count");
     if ((int64_t)hcount <= cap) break;
     cap = (int64_t)hcount + hcount / 4;
+  }
+  if (stats || counters) {
+    DevStats h;
+    if ((e = cudaMemcpy(&h, dstats, sizeof h, cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return cuda_error(e, "stats");
+    if (counters) {
+      counters[0] += (int64_t)h.tri_pairs;
+      counters[1] += (int64_t)h.evaluated;
+    }
   }
   if (stats) {
     DevStats h;

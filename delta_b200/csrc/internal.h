@@ -18,7 +18,7 @@ cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, c
 // Particle-pair drivers (detect.cu).
 delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
-                        delta_stats *stats);
+                        delta_stats *stats, int64_t *counters = nullptr);
 
 // Thread-local last-error text (capi.cu).
 delta_status set_error(delta_status st, const std::string &msg);

@@ -56,11 +56,11 @@ __global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restri
 
 // bf_cert: warps walk the pair list 32 pairs at a time (the certificate's candidate queue
 // is shared by the warp).
-__global__ void __launch_bounds__(256) k_pairs_cert(int64_t n, const double *__restrict__ a,
+__global__ void __launch_bounds__(128, 5) k_pairs_cert(int64_t n, const double *__restrict__ a,
                                                     const double *__restrict__ b, int64_t ld,
                                                     double *__restrict__ p, double *__restrict__ q,
                                                     double *__restrict__ dist, uint8_t *__restrict__ flags) {
-  __shared__ CertWarpSmem sm[8];
+  __shared__ CertWarpSmem sm[4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += nwarps * 32) {
@@ -121,12 +121,12 @@ cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, c
                          int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags) {
   if (method == M_BF_CERT) {
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_cert, 256, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_cert, 128, 0);
     if (e != cudaSuccess) return e;
-    int64_t blocks = (n + 255) / 256;
+    int64_t blocks = (n + 127) / 128;
     const int64_t cap = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1) * 8;
     if (blocks > cap) blocks = cap;
-    k_pairs_cert<<<(unsigned)(blocks > 0 ? blocks : 1), 256, 0, s>>>(n, a, b, ld, p, q, dist, flags);
+    k_pairs_cert<<<(unsigned)(blocks > 0 ? blocks : 1), 128, 0, s>>>(n, a, b, ld, p, q, dist, flags);
     return cudaGetLastError();
   }
   if (precision == 0) return launch_prec<xf64>(method, s, n, a, b, ld, max_error, p, q, dist, flags);

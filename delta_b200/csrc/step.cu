@@ -648,6 +648,8 @@ struct delta_sim {
   int64_t pair_cap = 0;
   double *F = nullptr, *T = nullptr;
   uint8_t *has = nullptr;
+  // steps, candidate body pairs, triangle pairs of the candidates, triangle pairs solved
+  int64_t counters[4] = {0, 0, 0, 0};
 };
 
 namespace delta {
@@ -695,6 +697,7 @@ static delta_status sim_detect(delta_sim *s) {
     ds = broadphase_run(s->ctx, s->scene, s->plan, s->pa, s->pb, s->pair_cap, &np);
   }
   if (ds != DELTA_OK) return ds;
+  s->counters[1] += np;
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
                  s->scene.eps,      s->scene.friction,   s->ids};
   int64_t nc = 0;
@@ -702,11 +705,15 @@ static delta_status sim_detect(delta_sim *s) {
     s->n_contacts = 0;
     return DELTA_OK;
   }
-  ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr);
+  int64_t cnt[2] = {0, 0};
+  ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt);
   if (ds == DELTA_ERR_CAPACITY) {
     if ((ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;
-    ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr);
+    cnt[0] = cnt[1] = 0;
+    ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt);
   }
+  s->counters[2] += cnt[0];
+  s->counters[3] += cnt[1];
   if (ds != DELTA_OK) return ds;
   s->n_contacts = nc;
   return DELTA_OK;
@@ -792,6 +799,7 @@ delta_status delta_sim_step(delta_sim *s, const delta_step_params *params, int32
     if (ds != DELTA_OK) return ds;
     if ((ds = integrate_run(s->ctx, s->scene, *params, s->F, s->T, s->has, 3 * s->n_tri)) != DELTA_OK) return ds;
     if ((ds = sim_detect(s)) != DELTA_OK) return ds;
+    s->counters[0] += 1;
     if (contacts_per_step) contacts_per_step[k] = s->n_contacts;
   }
   return DELTA_OK;
@@ -824,6 +832,12 @@ delta_status delta_sim_contacts(delta_sim *s, const delta_contacts *out, int64_t
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_error(e, "delta_sim_contacts");
   if (s->n_contacts > out->capacity) return set_error(DELTA_ERR_CAPACITY, "delta_sim_contacts: capacity");
+  return DELTA_OK;
+}
+
+delta_status delta_sim_counters(const delta_sim *s, int64_t out[4]) {
+  if (!s || !out) return set_error(DELTA_ERR_INVALID, "delta_sim_counters: null argument");
+  for (int k = 0; k < 4; ++k) out[k] = s->counters[k];
   return DELTA_OK;
 }
 

@@ -178,13 +178,19 @@ __device__ __forceinline__ void feature_points_dyn(const xf64 A[3][3], const xf6
   }
 }
 
-// Per-warp shared staging for bf_cert_warp: the 32 pairs' coordinates and the queue.
+// Per-warp shared staging for bf_cert_warp: the 32 pairs' FP64 coordinates, the
+// candidate queues (one per feature family) and the queue results.
+constexpr int kCertQueue = 64;  // entries evaluated per pass and family
 struct CertWarpSmem {
   double coords[32][18];
-  uint16_t queue[32 * 15];
+  uint8_t qs[32 * 9], qp[32 * 6];      // queued (lane << 0) with features in a separate array
+  uint8_t fs[32 * 9], fp[32 * 6];
+  double rd[kCertQueue], r0[kCertQueue], r1[kCertQueue];
+  int32_t surv[64];  // particle-pair driver: B triangles that passed the box test
 };
 
-// Running minimum of one feature family, ordered by (distance, feature index).
+// Running minimum of one feature family, ordered by (distance, feature index): equal to
+// the reference's sequential scan with strict < (first minimum wins).
 struct FamilyBest {
   xf64 dist, p0, p1;
   int f;
@@ -193,13 +199,93 @@ struct FamilyBest {
   }
 };
 
+__device__ __forceinline__ void load_pair(const CertWarpSmem &sm, int lane, xf64 A[3][3], xf64 B[3][3]) {
+#pragma unroll
+  for (int v = 0; v < 3; ++v)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      A[v][k] = xf64(sm.coords[lane][3 * v + k]);
+      B[v][k] = xf64(sm.coords[lane][9 + 3 * v + k]);
+    }
+}
+
+// Edge-edge feature f (0..8) of the pair staged for `lane`.
+__device__ __forceinline__ xf64 seg_dyn(const CertWarpSmem &sm, int lane, int f, xf64 &p0, xf64 &p1) {
+  const int ea = f / 3, eb = f - 3 * ea;
+  const int ta = ea == 2 ? 0 : ea + 1, tb = eb == 2 ? 0 : eb + 1;
+  xf64 HA[3], TA[3], HB[3], TB[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    HA[k] = xf64(sm.coords[lane][3 * ea + k]);
+    TA[k] = xf64(sm.coords[lane][3 * ta + k]);
+    HB[k] = xf64(sm.coords[lane][9 + 3 * eb + k]);
+    TB[k] = xf64(sm.coords[lane][9 + 3 * tb + k]);
+  }
+  return seg_seg_ref(HA, TA, HB, TB, p0, p1);
+}
+
+// Vertex-face feature j (0..5) of the pair staged for `lane`.
+__device__ __forceinline__ xf64 pt_dyn(const CertWarpSmem &sm, int lane, int j, xf64 &p0, xf64 &p1) {
+  const int tri = j < 3 ? 0 : 9, pnt = j < 3 ? 9 + 3 * j : 3 * (j - 3);
+  xf64 V0[3], V1[3], V2[3], X[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    V0[k] = xf64(sm.coords[lane][tri + k]);
+    V1[k] = xf64(sm.coords[lane][tri + 3 + k]);
+    V2[k] = xf64(sm.coords[lane][tri + 6 + k]);
+    X[k] = xf64(sm.coords[lane][pnt + k]);
+  }
+  return pt_tri_ref(V0, V1, V2, X, p0, p1);
+}
+
+// Evaluates a family's queue (entries: lane, feature) in passes of kCertQueue and offers
+// each result to its owner's running minimum.  owner_lo/owner_cnt: this lane's entries.
+template <bool SEG>
+__device__ __forceinline__ void run_queue(CertWarpSmem &sm, const uint8_t *ql, const uint8_t *qf, int total,
+                                          int my_lo, int my_cnt, FamilyBest &best) {
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < total; base += kCertQueue) {
+    const int n = min(kCertQueue, total - base);
+    for (int j = lane; j < n; j += 32) {
+      xf64 p0, p1;
+      const xf64 d = SEG ? seg_dyn(sm, ql[base + j], qf[base + j], p0, p1) : pt_dyn(sm, ql[base + j], qf[base + j], p0, p1);
+      sm.rd[j] = d.v;
+      sm.r0[j] = p0.v;
+      sm.r1[j] = p1.v;
+    }
+    __syncwarp();
+    const int lo = max(my_lo, base), hi = min(my_lo + my_cnt, base + n);
+    for (int j = lo; j < hi; ++j)
+      best.offer(xf64(sm.rd[j - base]), qf[j], xf64(sm.r0[j - base]), xf64(sm.r1[j - base]));
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int &total) {
+  const int lane = threadIdx.x & 31;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  total = __shfl_sync(0xffffffffu, incl, 31);
+  return incl - v;
+}
+
 // All 32 lanes call this together; lanes with valid == false carry dummy data and
 // produce nothing.  Writes bfSolver's closest points to pq; returns the number of FP64
 // feature evaluations made for this lane's pair.
 __device__ __forceinline__ int bf_cert_warp(const double A64[3][3], const double B64[3][3], bool valid, double pq[6],
                                             CertWarpSmem &sm) {
-  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int v = 0; v < 3; ++v)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      sm.coords[lane][3 * v + k] = A64[v][k];
+      sm.coords[lane][9 + 3 * v + k] = B64[v][k];
+    }
   // ---- 1. FP32 lower bounds -------------------------------------------------------
   float A[3][3], B[3][3];
   double L = 0.0;
@@ -216,101 +302,63 @@ __device__ __forceinline__ int bf_cert_warp(const double A64[3][3], const double
     L = fmax(L, hi - lo);
   }
   const float eps = (float)L * (64.f * kU32);
-  float d32[15], lb[15];
+  float lb[15];
+  int sbest = 0, pbest = 0;
+  float sd = 3.0e38f, pd = 3.0e38f;
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
     float l;
-    d32[j] = seg_seg_lb(A[j / 3], A[(j / 3 + 1) % 3], B[j % 3], B[(j % 3 + 1) % 3], l);
+    const float d = seg_seg_lb(A[j / 3], A[(j / 3 + 1) % 3], B[j % 3], B[(j % 3 + 1) % 3], l);
     lb[j] = l - eps;
+    if (d < sd) { sd = d; sbest = j; }
   }
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    d32[9 + j] = pt_tri_lb(A[0], A[1], A[2], B[j], eps, lb[9 + j]);
-    d32[12 + j] = pt_tri_lb(B[0], B[1], B[2], A[j], eps, lb[12 + j]);
+    float d = pt_tri_lb(A[0], A[1], A[2], B[j], eps, lb[9 + j]);
+    if (d < pd) { pd = d; pbest = j; }
+    d = pt_tri_lb(B[0], B[1], B[2], A[j], eps, lb[12 + j]);
+    if (d < pd) { pd = d; pbest = 3 + j; }
   }
-  int fmin_ = 0;
-  float dmin = d32[0];
-#pragma unroll
-  for (int f = 1; f < 15; ++f)
-    if (d32[f] < dmin) { dmin = d32[f]; fmin_ = f; }
-  // ---- 2. FP64 value of the FP32 argmin ---------------------------------------------
-  xf64 Ax[3][3], Bx[3][3];
-#pragma unroll
-  for (int v = 0; v < 3; ++v)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      Ax[v][k] = xf64(A64[v][k]);
-      Bx[v][k] = xf64(B64[v][k]);
-    }
-  xf64 c0, c1;
-  const xf64 best = feature_dyn(Ax, Bx, fmin_, c0, c1);
+  __syncwarp();
+  // ---- 2. FP64 values of each family's FP32 argmin (every lane runs both paths) --------
   FamilyBest seg{xf64(1E+30), xf64(0.0), xf64(0.0), 0}, pt{xf64(1E30), xf64(0.0), xf64(0.0), 0};
-  // the reference's initial state is (1e30, first index, zero parameters); a feature
-  // reaching 1e30 exactly never replaces it (strict <), which offer() reproduces by
-  // treating the initial entry as index -1 only for strictly smaller distances.
-  if (fmin_ < 9) { if (best < seg.dist) { seg.dist = best; seg.f = fmin_; seg.p0 = c0; seg.p1 = c1; } }
-  else { if (best < pt.dist) { pt.dist = best; pt.f = fmin_ - 9; pt.p0 = c0; pt.p1 = c1; } }
-  // ---- 3. queue the remaining candidates ----------------------------------------------
-  unsigned mask = 0;
-#pragma unroll
-  for (int f = 0; f < 15; ++f)
-    if (f != fmin_ && !((double)lb[f] > best.v)) mask |= 1u << f;
-  if (!valid) mask = 0;
-  const int cnt = __popc(mask);
-  int incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += y;
+  {
+    xf64 a0, a1;
+    const xf64 ds = seg_dyn(sm, lane, sbest, a0, a1);
+    if (ds < seg.dist) { seg.dist = ds; seg.f = sbest; seg.p0 = a0; seg.p1 = a1; }
+    const xf64 dp = pt_dyn(sm, lane, pbest, a0, a1);
+    if (dp < pt.dist) { pt.dist = dp; pt.f = pbest; pt.p0 = a0; pt.p1 = a1; }
   }
-  const int total = __shfl_sync(full, incl, 31);
-  int pos = incl - cnt;
-  for (unsigned m = mask; m; m &= m - 1) sm.queue[pos++] = (uint16_t)((lane << 4) | (__ffs(m) - 1));
+  const double best = fmin(seg.dist.v, pt.dist.v);  // NaN-free unless both are NaN
+  const double bound = (best == best) ? best : 1.0e308;
+  // ---- 3. queue the remaining candidates, one queue per family ------------------------
+  unsigned ms = 0, mp = 0;
 #pragma unroll
-  for (int v = 0; v < 3; ++v)
+  for (int f = 0; f < 9; ++f)
+    if (f != sbest && !((double)lb[f] > bound)) ms |= 1u << f;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      sm.coords[lane][3 * v + k] = A64[v][k];
-      sm.coords[lane][9 + 3 * v + k] = B64[v][k];
-    }
-  __syncwarp();
-  // ---- 3b. evaluate the queue 32 entries at a time, merge into the owners' minima -----
-  for (int c = 0; c < total; c += 32) {
-    const int j = c + lane;
-    int owner = 0, f = 0;
-    xf64 dist = xf64(0.0), p0 = xf64(0.0), p1 = xf64(0.0);
-    if (j < total) {
-      const uint16_t e = sm.queue[j];
-      owner = e >> 4;
-      f = e & 15;
-      xf64 QA[3][3], QB[3][3];
-#pragma unroll
-      for (int v = 0; v < 3; ++v)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          QA[v][k] = xf64(sm.coords[owner][3 * v + k]);
-          QB[v][k] = xf64(sm.coords[owner][9 + 3 * v + k]);
-        }
-      dist = feature_dyn(QA, QB, f, p0, p1);
-    }
-    const int n = min(32, total - c);
-    for (int i = 0; i < n; ++i) {
-      const int ow = __shfl_sync(full, owner, i);
-      const int ff = __shfl_sync(full, f, i);
-      const double dd = __shfl_sync(full, dist.v, i);
-      const double a0 = __shfl_sync(full, p0.v, i);
-      const double a1 = __shfl_sync(full, p1.v, i);
-      if (lane == ow) {
-        if (ff < 9) seg.offer(xf64(dd), ff, xf64(a0), xf64(a1));
-        else pt.offer(xf64(dd), ff - 9, xf64(a0), xf64(a1));
-      }
-    }
+  for (int j = 0; j < 6; ++j)
+    if (j != pbest && !((double)lb[9 + j] > bound)) mp |= 1u << j;
+  if (!valid) ms = mp = 0;
+  int ts, tp;
+  const int cs = __popc(ms), cp = __popc(mp);
+  const int os = warp_excl_scan(cs, ts), op = warp_excl_scan(cp, tp);
+  {
+    int q = os;
+    for (unsigned m = ms; m; m &= m - 1) { sm.qs[q] = (uint8_t)lane; sm.fs[q] = (uint8_t)(__ffs(m) - 1); ++q; }
+    q = op;
+    for (unsigned m = mp; m; m &= m - 1) { sm.qp[q] = (uint8_t)lane; sm.fp[q] = (uint8_t)(__ffs(m) - 1); ++q; }
   }
   __syncwarp();
+  run_queue<true>(sm, sm.qs, sm.fs, ts, os, cs, seg);
+  run_queue<false>(sm, sm.qp, sm.fp, tp, op, cp, pt);
   // ---- 4. selection (bf.cpp:1102) and closest points --------------------------------
+  xf64 Ax[3][3], Bx[3][3];
+  load_pair(sm, lane, Ax, Bx);
+  __syncwarp();
   if (pt.dist > seg.dist) feature_points_dyn(Ax, Bx, seg.f, seg.p0, seg.p1, pq);
   else feature_points_dyn(Ax, Bx, 9 + pt.f, pt.p0, pt.p1, pq);
-  return 1 + cnt;
+  return 2 + cs + cp;
 }
 
 }  // namespace delta

@@ -99,6 +99,12 @@ class Simulation:
         del st
         return out.to_numpy()
 
+    def counters(self) -> dict:
+        """steps, candidate body pairs, triangle pairs tested (sum nA*nB), triangle pairs solved."""
+        out = np.zeros(4, np.int64)
+        check(lib().delta_sim_counters(self._h, out.ctypes.data))
+        return dict(zip(("steps", "body_pairs", "triangle_pairs", "solved"), out.tolist()))
+
     def state(self) -> dict:
         self.ctx.synchronize()
         return self.dev.to_host()

@@ -209,6 +209,10 @@ delta_status delta_sim_step(delta_sim *sim, const delta_step_params *params, int
                             int64_t *contacts_per_step /* host [nsteps] or NULL */);
 /* Copies the current contacts into out (device); *n_out gets their number. */
 delta_status delta_sim_contacts(delta_sim *sim, const delta_contacts *out, int64_t *n_out);
+/* Totals since creation: [0] steps, [1] candidate body pairs, [2] triangle pairs of the
+ * candidates (sum of nA*nB: the pairs the reference tests, Collision.cpp:652), [3]
+ * triangle pairs the narrowphase solver ran on (after exact box culling for BF_CERT). */
+delta_status delta_sim_counters(const delta_sim *sim, int64_t out[4]);
 delta_status delta_sim_destroy(delta_sim *sim);
 
 #ifdef __cplusplus
