@@ -37,6 +37,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_broadphase": ([vp, vp, vp, vp, i64, vp], C.c_int),
     "delta_sim_create": ([vp, vp, C.c_int, vp], C.c_int),
     "delta_sim_step": ([vp, vp, i32, vp], C.c_int),
+    "delta_sim_step_graph": ([vp, vp, i32, vp], C.c_int),
+    "delta_sim_set_graph_capacity": ([vp, i64, i64], C.c_int),
     "delta_sim_contacts": ([vp, vp, vp], C.c_int),
     "delta_sim_counters": ([vp, vp], C.c_int),
     "delta_sim_destroy": ([vp], C.c_int),

@@ -313,9 +313,10 @@ template <class R, int DRV>
 __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *__restrict__ pa,
                                                 const int32_t *__restrict__ pb,
                                                 const int64_t *__restrict__ row_offset, int64_t n_pairs,
-                                                int64_t total_rows, RawContacts rc, DevStats *st,
+                                                const int64_t *total_rows_p, RawContacts rc, DevStats *st,
                                                 unsigned long long *queue) {
   const int lane = threadIdx.x & 31;
+  const int64_t total_rows = *total_rows_p;
   __shared__ CertWarpSmem cert_sm[DRV == DELTA_DRV_BF_CERT ? 4 : 1];
   CertWarpSmem *csm = &cert_sm[DRV == DELTA_DRV_BF_CERT ? (threadIdx.x >> 5) : 0];
   for (;;) {
@@ -363,6 +364,49 @@ __global__ void k_rows_per_pair(const int64_t *tri_offset, const int32_t *pa, in
   rows[k] = tri_offset[a + 1] - tri_offset[a];
 }
 
+__global__ void k_rows_fixed(const int64_t *tri_offset, const int32_t *pa, int64_t cap, int64_t *rows) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > cap) return;
+  if (k == cap) { rows[k] = 0; return; }
+  const int32_t a = pa[k];
+  rows[k] = a < 0 ? 0 : tri_offset[a + 1] - tri_offset[a];
+}
+
+// Gather for the fixed-capacity path: count and overflow live on the device.
+__global__ void k_gather_fixed(RawContacts rc, const int64_t *perm, delta_contacts out, int64_t *n_out, int *ovf,
+                               int ovf_code, int64_t *count_log) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long cnt = *rc.count;
+  const int64_t n = (int64_t)cnt < out.capacity ? (int64_t)cnt : out.capacity;
+  if (j == 0) {
+    *n_out = n;
+    if (count_log) *count_log = n;
+    if ((int64_t)cnt > out.capacity) atomicCAS(ovf, 0, ovf_code);
+  }
+  if (j >= n) return;
+  const int64_t s = perm[j], cap = rc.cap, oc = out.capacity;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    out.x[k * oc + j] = rc.f[(0 + k) * cap + s];
+    out.normal[k * oc + j] = rc.f[(3 + k) * cap + s];
+    out.P[k * oc + j] = rc.f[(7 + k) * cap + s];
+    out.Q[k * oc + j] = rc.f[(10 + k) * cap + s];
+  }
+  out.depth[j] = rc.f[6 * cap + s];
+  out.eps_total[j] = rc.f[13 * cap + s];
+  out.master[j] = rc.i[s];
+  out.slave[j] = rc.i[cap + s];
+  out.tri_a[j] = rc.i[2 * cap + s];
+  out.tri_b[j] = rc.i[3 * cap + s];
+  out.penetration[j] = 1;
+  out.friction[j] = rc.fric[s];
+}
+
+__global__ void k_accumulate(const DevStats *st, int64_t *counters) {
+  counters[0] += (int64_t)st->tri_pairs;
+  counters[1] += (int64_t)st->evaluated;
+}
+
 __global__ void k_check_pairs(const int64_t *tri_offset, const int32_t *pb, int64_t n_pairs, int32_t n_bodies,
                               int *bad) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -406,15 +450,18 @@ __global__ void k_gather(RawContacts rc, const int64_t *perm, int64_t n, delta_c
 
 template <class R, int DRV>
 cudaError_t launch_detect_t(cudaStream_t s, const delta_meshes &m, const int32_t *pa, const int32_t *pb,
-                            const int64_t *row_offset, int64_t n_pairs, int64_t rows, const RawContacts &rc,
+                            const int64_t *row_offset, int64_t n_pairs, int64_t rows_hint, const RawContacts &rc,
                             DevStats *st, unsigned long long *queue) {
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_detect<R, DRV>, 128, 0);
   if (e != cudaSuccess) return e;
   int64_t blocks = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
-  const int64_t need = (rows + 3) / 4;  // 4 warps per block
-  if (blocks > need) blocks = need > 0 ? need : 1;
-  k_detect<R, DRV><<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, row_offset, n_pairs, rows, rc, st, queue);
+  if (rows_hint >= 0) {
+    const int64_t need = (rows_hint + 3) / 4;  // 4 warps per block
+    if (blocks > need) blocks = need > 0 ? need : 1;
+  }
+  k_detect<R, DRV><<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, row_offset, n_pairs, row_offset + n_pairs, rc, st,
+                                                    queue);
   return cudaGetLastError();
 }
 
@@ -567,6 +614,69 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "detect gather");
   if (n > out->capacity) return set_error(DELTA_ERR_CAPACITY, "delta_detect: contact capacity exceeded");
   return DELTA_OK;
+}
+
+// Fixed-capacity detection for graph capture: pair_cap pairs (entries with a negative
+// body index are empty), raw contact buffer and output of out->capacity entries, counts
+// and overflow on the device.  Scratch (slots 13, 14) must have been sized by
+// detect_fixed_prepare before capture.
+size_t detect_fixed_temp_bytes(int64_t pair_cap, int64_t cap) {
+  size_t a = 0, b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, a, (int64_t *)nullptr, (int64_t *)nullptr, pair_cap + 1);
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, (int64_t *)nullptr,
+                                  (int64_t *)nullptr, cap, 0, 64);
+  return a > b ? a : b;
+}
+
+size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap) {
+  const size_t per = 14 * sizeof(double) + 4 * sizeof(int32_t) + 1 + 2 * sizeof(uint64_t);
+  return 512 + sizeof(DevStats) + sizeof(int64_t) * (size_t)(2 * pair_cap + 2) + per * (size_t)cap +
+         sizeof(int64_t) * 2 * (size_t)cap + 256;
+}
+
+delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
+                              const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
+                              int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
+                              void *temp, size_t temp_bytes) {
+  cudaError_t e;
+  const int64_t cap = out.capacity;
+  char *p = (char *)state;
+  unsigned long long *queue = (unsigned long long *)p;  // [0] queue [1] contact count
+  DevStats *dstats = (DevStats *)(p + 256);
+  p += 512 + sizeof(DevStats);
+  int64_t *rows = (int64_t *)p, *row_offset = rows + pair_cap + 1;
+  p += sizeof(int64_t) * (size_t)(2 * pair_cap + 2);
+  RawContacts rc{};
+  rc.cap = cap;
+  rc.f = (double *)p;
+  rc.key = (uint64_t *)(rc.f + 14 * cap);
+  rc.i = (int32_t *)(rc.key + 2 * cap);
+  rc.fric = (uint8_t *)(rc.i + 4 * cap);
+  rc.count = queue + 1;
+  p += (14 * sizeof(double) + 4 * sizeof(int32_t) + 1 + 2 * sizeof(uint64_t)) * (size_t)cap;
+  p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+  int64_t *perm_in = (int64_t *)p, *perm_out = perm_in + cap;
+  uint64_t *key_out = rc.key + cap;
+  if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
+  if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");
+  k_rows_fixed<<<(unsigned)((pair_cap + 256) / 256), 256, 0, s>>>(m.tri_offset, pa, pair_cap, rows);
+  size_t tb = temp_bytes;
+  if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
+    return cuda_error(e, "row scan");
+  e = driver == DELTA_DRV_BF_CERT
+          ? launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue)
+          : launch_detect_t<xf64, DELTA_DRV_BF>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue);
+  if (e != cudaSuccess) return cuda_error(e, "detect kernel");
+  k_iota<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(perm_in, cap);
+  tb = temp_bytes;
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, rc.key, key_out, perm_in, perm_out, cap, 0, 64, s)) !=
+      cudaSuccess)
+    return cuda_error(e, "contact sort");
+  k_gather_fixed<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, perm_out, out, d_ncontacts, d_ovf, ovf_code,
+                                                               d_count_log);
+  if (d_counters) k_accumulate<<<1, 1, 0, s>>>(dstats, d_counters);
+  ctx->launches += d_counters ? 6 : 5;
+  return cuda_error(cudaGetLastError(), "detect fixed");
 }
 
 }  // namespace delta

@@ -7,7 +7,9 @@
 // floating-point atomics are used, so results do not depend on scheduling.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "internal.h"
@@ -199,6 +201,27 @@ __device__ void pair_forces(const delta_scene &s, const ContactView &cv, int64_t
   }
 }
 
+__global__ void k_segment_heads_fixed(ContactView cv, int64_t cap, const int64_t *n_d, uint8_t *head) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cap) return;
+  const int64_t n = *n_d < cap ? *n_d : cap;
+  head[c] = c < n && (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]) ? 1 : 0;
+}
+
+__global__ void k_flag_overflow(const unsigned long long *count, int64_t cap, int *ovf) {
+  if (*count > (unsigned long long)cap) atomicCAS(ovf, 0, 1);
+}
+
+__global__ void k_step_begin(const int *ovf, int *ovf_snap) { *ovf_snap = *ovf; }
+
+__global__ void k_step_end(const int *ovf_snap, const int64_t *n_contacts, int64_t *log, int64_t log_len,
+                           int64_t *step) {
+  if (*ovf_snap) return;
+  const int64_t k = *step;
+  if (k < log_len) log[k] = *n_contacts;
+  *step = k + 1;
+}
+
 __global__ void k_segment_heads(ContactView cv, int64_t n, uint8_t *head) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -207,10 +230,12 @@ __global__ void k_segment_heads(ContactView cv, int64_t n, uint8_t *head) {
 
 // One thread per partner pair: both sides' sums, keyed (body << 32 | partner).
 __global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_start, const int64_t *n_seg_p,
-                              int64_t n_contacts, delta_step_params p, uint64_t *key, int64_t *val_idx,
-                              double *entry) {
+                              int64_t n_contacts_h, const int64_t *n_contacts_d, delta_step_params p, uint64_t *key,
+                              int64_t *val_idx, double *entry) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n_seg = *n_seg_p;
+  int64_t n_contacts = n_contacts_d ? *n_contacts_d : n_contacts_h;
+  if (n_contacts > cv.cap) n_contacts = cv.cap;
   if (g >= n_seg) return;
   const int64_t c0 = seg_start[g], c1 = g + 1 < n_seg ? seg_start[g + 1] : n_contacts;
   const int32_t i = cv.master[c0], j = cv.slave[c0];
@@ -267,9 +292,10 @@ __global__ void k_body_forces(int32_t n_bodies, const uint64_t *skey, const int6
 // Collision::touchVertexFirstTime velocity part (Collision.cpp:1105-1115) followed by
 // MoveParticles::moveAllParticlesAssociatedToVertex body part (MoveParticles.cpp:71-94).
 __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force, const double *torque,
-                         const uint8_t *has) {
+                         const uint8_t *has, const int *ovf) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n_bodies || s.obstacle[i]) return;
+  if (ovf && *ovf) return;  // graph mode: a capacity overflow froze the state
   const BodyRef b{s.n_bodies, i};
   const X dt = X(p.dt);
   if (has[i]) {
@@ -287,9 +313,10 @@ __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force
 }
 
 // updateVertices, dynamics.cpp:215-242, one thread per vertex.
-__global__ void k_vertices(delta_scene s, int64_t n_vertices) {
+__global__ void k_vertices(delta_scene s, int64_t n_vertices, const int *ovf) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n_vertices) return;
+  if (ovf && *ovf) return;
   const int32_t i = s.tri_body[v / 3];
   if (s.obstacle[i]) return;
   const int32_t n = s.n_bodies;
@@ -460,7 +487,8 @@ delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contac
   ctx->launches += 1;
   // entries for all potential segments (n_contacts bounds the count; unused keys sort last)
   if ((e = cudaMemsetAsync(key, 0xff, sizeof(uint64_t) * 2 * nc, st)) != cudaSuccess) return cuda_error(e, "memset");
-  k_pair_forces<<<blocks_for(n_contacts, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, n_contacts, p, key, idx, entry);
+  k_pair_forces<<<blocks_for(n_contacts, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, n_contacts, nullptr, p, key, idx,
+                                                            entry);
   ctx->launches += 1;
   tb = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 64, st);
@@ -477,8 +505,8 @@ delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contac
 delta_status integrate_run(delta_ctx *ctx, const delta_scene &s, const delta_step_params &p, const double *force,
                            const double *torque, const uint8_t *has, int64_t n_vertices) {
   cudaStream_t st = ctx->stream;
-  k_bodies<<<blocks_for(s.n_bodies, 128), 128, 0, st>>>(s, p, force, torque, has);
-  k_vertices<<<blocks_for(n_vertices), 256, 0, st>>>(s, n_vertices);
+  k_bodies<<<blocks_for(s.n_bodies, 128), 128, 0, st>>>(s, p, force, torque, has, nullptr);
+  k_vertices<<<blocks_for(n_vertices), 256, 0, st>>>(s, n_vertices, nullptr);
   ctx->launches += 2;
   return cuda_error(cudaGetLastError(), "integrate launch");
 }
@@ -626,6 +654,114 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   return DELTA_OK;
 }
 
+
+static int bits_for(int64_t v) {
+  int b = 1;
+  while (b < 31 && ((int64_t)1 << b) <= v) ++b;
+  return b;
+}
+
+// Forces from a fixed-capacity contact buffer with its count on the device.
+size_t forces_fixed_state_bytes(int64_t cap) { return (size_t)cap * (1 + 8 + 16 * 4 + 96) + 512; }
+
+size_t forces_fixed_temp_bytes(int64_t cap, int32_t n_bodies) {
+  size_t a = 0, b = 0;
+  cub::CountingInputIterator<int64_t> it(0);
+  cub::DeviceSelect::Flagged(nullptr, a, it, (uint8_t *)nullptr, (int64_t *)nullptr, (int64_t *)nullptr, cap);
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, (int64_t *)nullptr,
+                                  (int64_t *)nullptr, 2 * cap, 0, 32 + bits_for(n_bodies));
+  return a > b ? a : b;
+}
+
+delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta_contacts &c, const int64_t *d_nc,
+                              const delta_step_params &p, double *force, double *torque, uint8_t *has, void *state,
+                              void *temp, size_t temp_bytes, int &kernels) {
+  cudaError_t e;
+  const int64_t cap = c.capacity;
+  ContactView cv{c.x, c.normal, c.depth, c.master, c.slave, c.friction, cap};
+  char *b = (char *)state;
+  int64_t *n_seg = (int64_t *)b; b += 512;
+  int64_t *seg_start = (int64_t *)b; b += 8 * cap;
+  uint64_t *key = (uint64_t *)b; b += 16 * cap;
+  uint64_t *skey = (uint64_t *)b; b += 16 * cap;
+  int64_t *idx = (int64_t *)b; b += 16 * cap;
+  int64_t *sidx = (int64_t *)b; b += 16 * cap;
+  double *entry = (double *)b; b += 96 * cap;
+  uint8_t *head = (uint8_t *)b;
+  k_segment_heads_fixed<<<blocks_for(cap), 256, 0, st>>>(cv, cap, d_nc, head);
+  size_t tb = temp_bytes;
+  cub::CountingInputIterator<int64_t> it(0);
+  if ((e = cub::DeviceSelect::Flagged(temp, tb, it, head, seg_start, n_seg, cap, st)) != cudaSuccess)
+    return cuda_error(e, "segment select");
+  if ((e = cudaMemsetAsync(key, 0xff, sizeof(uint64_t) * 2 * cap, st)) != cudaSuccess) return cuda_error(e, "memset");
+  k_pair_forces<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, 0, d_nc, p, key, idx, entry);
+  tb = temp_bytes;
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, 2 * cap, 0, 32 + bits_for(s.n_bodies),
+                                           st)) != cudaSuccess)
+    return cuda_error(e, "entry sort");
+  k_body_forces<<<blocks_for(s.n_bodies), 256, 0, st>>>(s.n_bodies, skey, sidx, entry, 2 * cap, force, torque, has);
+  kernels += 5;
+  return cuda_error(cudaGetLastError(), "forces fixed");
+}
+
+// Broadphase into a fixed-capacity pair list (padded with -1), overflow flagged on the device.
+size_t broadphase_fixed_state_bytes(int32_t n, int64_t pair_cap) {
+  return (size_t)n * 24 + 512 + (size_t)pair_cap * 16 + 256;
+}
+
+size_t broadphase_fixed_temp_bytes(int32_t n, int64_t pair_cap) {
+  size_t a = 0, b = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, a, (uint64_t *)nullptr, (uint64_t *)nullptr, (int32_t *)nullptr,
+                                  (int32_t *)nullptr, n, 0, 64);
+  cub::DeviceRadixSort::SortKeys(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, pair_cap, 0,
+                                 32 + bits_for(n));
+  return a > b ? a : b;
+}
+
+delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, int32_t *pair_a,
+                                  int32_t *pair_b, int64_t pair_cap, int *ovf, void *state, void *temp,
+                                  size_t temp_bytes, int &kernels) {
+  cudaError_t e;
+  const int32_t n = s.n_bodies;
+  char *b = (char *)state;
+  uint64_t *key = (uint64_t *)b, *skey = key + n;
+  int32_t *body = (int32_t *)(skey + n), *sbody = body + n;
+  b += (size_t)n * 24;
+  b = (char *)(((uintptr_t)b + 255) & ~(uintptr_t)255);
+  unsigned long long *count = (unsigned long long *)b;
+  uint64_t *pk = (uint64_t *)(b + 256), *spk = pk + pair_cap;
+  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body);
+  size_t tb = temp_bytes;
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, 64, st)) != cudaSuccess)
+    return cuda_error(e, "cell sort");
+  if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess ||
+      (e = cudaMemsetAsync(pk, 0xff, sizeof(uint64_t) * pair_cap, st)) != cudaSuccess)
+    return cuda_error(e, "memset");
+  kernels += 2;
+  if (plan.n_moving > 0) {
+    k_grid_pairs<<<blocks_for(plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, pk, count,
+                                                                 pair_cap);
+    kernels += 1;
+  }
+  if (plan.n_obst > 0) {
+    k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
+                                                                          pk, count, pair_cap);
+    kernels += 1;
+  }
+  tb = temp_bytes;
+  if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, pair_cap, 0, 32 + bits_for(n), st)) != cudaSuccess)
+    return cuda_error(e, "pair sort");
+  k_unpack_pairs<<<blocks_for(pair_cap), 256, 0, st>>>(spk, pair_cap, pair_a, pair_b);
+  k_flag_overflow<<<1, 1, 0, st>>>(count, pair_cap, ovf);
+  kernels += 3;
+  return cuda_error(cudaGetLastError(), "broadphase fixed");
+}
+
+// The raw pair count of the last fixed broadphase (for growing the capacity).
+static unsigned long long *broadphase_fixed_count(void *state, int32_t n) {
+  char *b = (char *)state + (size_t)n * 24;
+  return (unsigned long long *)(((uintptr_t)b + 255) & ~(uintptr_t)255);
+}
 }  // namespace delta
 
 // ---------------------------------------------------------------------------------------
@@ -650,6 +786,25 @@ struct delta_sim {
   uint8_t *has = nullptr;
   // steps, candidate body pairs, triangle pairs of the candidates, triangle pairs solved
   int64_t counters[4] = {0, 0, 0, 0};
+  int64_t graph_pair_cap = 0, graph_contact_cap = 0;  // requested by delta_sim_set_graph_capacity
+  // graph mode: fixed-capacity buffers, device-side counts, the captured step
+  struct Graph {
+    int64_t pair_cap = 0, contact_cap = 0;
+    int32_t *pa = nullptr, *pb = nullptr;
+    void *bp = nullptr, *fs = nullptr, *ds = nullptr, *temp = nullptr, *c_mem = nullptr, *dev = nullptr;
+    size_t temp_bytes = 0;
+    delta_contacts c{};
+    int64_t *d_nc = nullptr, *d_step = nullptr, *d_cnt = nullptr, *d_log = nullptr;
+    int *d_ovf = nullptr, *d_snap = nullptr;
+    int64_t log_len = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    delta_step_params params{};
+    int kernels = 0;
+    bool captured = false;
+  } g;
 };
 
 namespace delta {
@@ -717,6 +872,126 @@ static delta_status sim_detect(delta_sim *s) {
   if (ds != DELTA_OK) return ds;
   s->n_contacts = nc;
   return DELTA_OK;
+}
+
+static void graph_release(delta_sim::Graph &g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  g.exec = nullptr;
+  g.graph = nullptr;
+  g.captured = false;
+  for (void *p : {(void *)g.pa, g.bp, g.fs, g.ds, g.temp, g.c_mem, g.dev})
+    if (p) cudaFree(p);
+  g.pa = g.pb = nullptr;
+  g.bp = g.fs = g.ds = g.temp = g.c_mem = g.dev = nullptr;
+}
+
+// (Re)allocates the fixed buffers for the given capacities (no capture in progress).
+static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_cap, int64_t log_len) {
+  delta_sim::Graph &g = s->g;
+  graph_release(g);
+  const int32_t n = s->scene.n_bodies;
+  g.pair_cap = pair_cap;
+  g.contact_cap = contact_cap;
+  g.log_len = log_len;
+  cudaError_t e;
+  size_t t = detect_fixed_temp_bytes(pair_cap, contact_cap);
+  t = std::max(t, forces_fixed_temp_bytes(contact_cap, n));
+  t = std::max(t, broadphase_fixed_temp_bytes(n, pair_cap));
+  g.temp_bytes = t + 256;
+  const size_t cbytes = (14 * sizeof(double) + 5 * sizeof(int32_t) + 1) * (size_t)contact_cap + 256;
+  if ((e = cudaMalloc(&g.pa, sizeof(int32_t) * 2 * (size_t)pair_cap)) != cudaSuccess ||
+      (e = cudaMalloc(&g.bp, broadphase_fixed_state_bytes(n, pair_cap))) != cudaSuccess ||
+      (e = cudaMalloc(&g.fs, forces_fixed_state_bytes(contact_cap))) != cudaSuccess ||
+      (e = cudaMalloc(&g.ds, detect_fixed_state_bytes(pair_cap, contact_cap))) != cudaSuccess ||
+      (e = cudaMalloc(&g.temp, g.temp_bytes)) != cudaSuccess || (e = cudaMalloc(&g.c_mem, cbytes)) != cudaSuccess ||
+      (e = cudaMalloc(&g.dev, 256 + sizeof(int64_t) * (size_t)log_len)) != cudaSuccess)
+    return cuda_error(e, "graph buffers");
+  g.pb = g.pa + pair_cap;
+  double *d = (double *)g.c_mem;
+  const int64_t cap = contact_cap;
+  g.c = delta_contacts{cap, d, d + 3 * cap, d + 6 * cap, d + 9 * cap, d + 12 * cap, d + 13 * cap,
+                       (int32_t *)(d + 14 * cap), (int32_t *)(d + 14 * cap) + cap,
+                       (int32_t *)(d + 14 * cap) + 2 * cap, (int32_t *)(d + 14 * cap) + 3 * cap,
+                       (int32_t *)(d + 14 * cap) + 4 * cap, (uint8_t *)((int32_t *)(d + 14 * cap) + 5 * cap)};
+  char *v = (char *)g.dev;
+  g.d_nc = (int64_t *)v;
+  g.d_step = (int64_t *)(v + 8);
+  g.d_cnt = (int64_t *)(v + 16);
+  g.d_ovf = (int *)(v + 32);
+  g.d_snap = (int *)(v + 36);
+  g.d_log = (int64_t *)(v + 256);
+  if ((e = cudaMemset(g.dev, 0, 256)) != cudaSuccess) return cuda_error(e, "graph memset");
+  return DELTA_OK;
+}
+
+// Enqueues one fixed-capacity step on g.stream (used under capture).
+static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p) {
+  delta_sim::Graph &g = s->g;
+  cudaStream_t st = g.stream;
+  int k = 0;
+  k_step_begin<<<1, 1, 0, st>>>(g.d_ovf, g.d_snap);
+  delta_status ds = forces_run_fixed(st, s->scene, g.c, g.d_nc, p, s->F, s->T, s->has, g.fs, g.temp, g.temp_bytes, k);
+  if (ds != DELTA_OK) return ds;
+  k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf);
+  k_vertices<<<blocks_for(3 * s->n_tri), 256, 0, st>>>(s->scene, 3 * s->n_tri, g.d_ovf);
+  if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.bp, g.temp, g.temp_bytes,
+                                 k)) != DELTA_OK)
+    return ds;
+  delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
+                 s->scene.eps,      s->scene.friction,   s->ids};
+  const int64_t before = s->ctx->launches;
+  if ((ds = detect_run_fixed(s->ctx, st, s->driver, m, g.pa, g.pb, g.pair_cap, g.c, g.d_nc, g.d_ovf, 1, g.d_cnt,
+                             nullptr, g.ds, g.temp, g.temp_bytes)) != DELTA_OK)
+    return ds;
+  k += (int)(s->ctx->launches - before);
+  s->ctx->launches = before;
+  k_step_end<<<1, 1, 0, st>>>(g.d_snap, g.d_nc, g.d_log, g.log_len, g.d_step);
+  g.kernels = k + 4;
+  return cuda_error(cudaGetLastError(), "graph step");
+}
+
+static delta_status graph_capture(delta_sim *s, const delta_step_params &p) {
+  delta_sim::Graph &g = s->g;
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  g.exec = nullptr;
+  g.graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_error(e, "begin capture");
+  delta_status ds = graph_enqueue_step(s, p);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(g.stream, &graph);
+  if (ds != DELTA_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return ds;
+  }
+  if (e != cudaSuccess) return cuda_error(e, "end capture");
+  g.graph = graph;
+  if ((e = cudaGraphInstantiate(&g.exec, g.graph, 0)) != cudaSuccess) return cuda_error(e, "graph instantiate");
+  g.params = p;
+  g.captured = true;
+  return DELTA_OK;
+}
+
+// Host contact list (sim->c) <-> graph contact buffer.
+static delta_status copy_contacts(const delta_contacts &src, const delta_contacts &dst, int64_t n, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  const int64_t ic = src.capacity, oc = dst.capacity;
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+    e = cudaMemcpyAsync(dst.x + k * oc, src.x + k * ic, 8 * n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst.normal + k * oc, src.normal + k * ic, 8 * n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst.P + k * oc, src.P + k * ic, 8 * n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst.Q + k * oc, src.Q + k * ic, 8 * n, cudaMemcpyDeviceToDevice, st);
+  }
+  const void *srcs[] = {src.depth, src.eps_total, src.master, src.slave, src.tri_a, src.tri_b, src.penetration,
+                        src.friction};
+  void *dsts[] = {dst.depth, dst.eps_total, dst.master, dst.slave, dst.tri_a, dst.tri_b, dst.penetration,
+                  dst.friction};
+  const size_t sz[] = {8, 8, 4, 4, 4, 4, 4, 1};
+  for (int k = 0; k < 8 && e == cudaSuccess; ++k)
+    e = cudaMemcpyAsync(dsts[k], srcs[k], sz[k] * n, cudaMemcpyDeviceToDevice, st);
+  return cuda_error(e, "copy contacts");
 }
 
 }  // namespace delta
@@ -835,6 +1110,114 @@ delta_status delta_sim_contacts(delta_sim *s, const delta_contacts *out, int64_t
   return DELTA_OK;
 }
 
+delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params, int32_t nsteps,
+                                  int64_t *contacts_per_step) {
+  if (!s || !params || nsteps < 0) return set_error(DELTA_ERR_INVALID, "delta_sim_step_graph: bad argument");
+  if (nsteps == 0) return DELTA_OK;
+  delta_sim::Graph &g = s->g;
+  cudaError_t e;
+  delta_status ds;
+  if (!g.stream) {
+    if ((e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_error(e, "graph stream");
+  }
+  int32_t done = 0;
+  if (s->counters[0] == 0) {  // observe one detection before sizing the fixed buffers
+    if ((ds = delta_sim_step(s, params, 1, contacts_per_step)) != DELTA_OK) return ds;
+    done = 1;
+  }
+  int64_t want_pairs = std::max<int64_t>(1024, 2 * std::max<int64_t>(s->counters[1] / std::max<int64_t>(1, s->counters[0]), 1));
+  int64_t want_contacts = std::max<int64_t>(2048, 4 * s->n_contacts);
+  if (s->graph_pair_cap > 0) want_pairs = s->graph_pair_cap;
+  if (s->graph_contact_cap > 0) want_contacts = s->graph_contact_cap;
+  want_contacts = std::max<int64_t>(want_contacts, s->n_contacts);  // the current list must fit
+  s->graph_pair_cap = s->graph_contact_cap = 0;
+  if (!g.pa || g.pair_cap < want_pairs || g.contact_cap < want_contacts || g.log_len < nsteps ||
+      g.pair_cap != want_pairs || g.contact_cap != want_contacts) {
+    if ((ds = graph_alloc(s, std::max(g.pair_cap, want_pairs), std::max(g.contact_cap, want_contacts),
+                          std::max<int64_t>(g.log_len, nsteps))) != DELTA_OK)
+      return ds;
+  }
+  if (memcmp(&g.params, params, sizeof(*params)) != 0) g.captured = false;
+  // hand the current contacts to the graph buffers; ctx stream work must be done first
+  if ((e = cudaEventRecord(g.ev, s->ctx->stream)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(g.stream, g.ev, 0)) != cudaSuccess)
+    return cuda_error(e, "graph order");
+  if ((ds = copy_contacts(s->c, g.c, s->n_contacts, g.stream)) != DELTA_OK) return ds;
+  int64_t hv[2] = {s->n_contacts, 0};
+  if ((e = cudaMemcpyAsync(g.d_nc, &hv[0], 8, cudaMemcpyHostToDevice, g.stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(g.d_step, 0, 8, g.stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(g.d_cnt, 0, 16, g.stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(g.d_ovf, 0, 8, g.stream)) != cudaSuccess || (e = cudaStreamSynchronize(g.stream)) != cudaSuccess)
+    return cuda_error(e, "graph setup");
+  int32_t base = done;  // steps completed before the current batch of launches
+  while (done < nsteps) {
+    if (!g.captured && (ds = graph_capture(s, *params)) != DELTA_OK) return ds;
+    const int32_t batch = nsteps - done;
+    for (int32_t k = 0; k < batch; ++k)
+      if ((e = cudaGraphLaunch(g.exec, g.stream)) != cudaSuccess) return cuda_error(e, "graph launch");
+    s->ctx->launches += (int64_t)g.kernels * batch;
+    int64_t dev_step = 0;
+    int ovf = 0;
+    if ((e = cudaMemcpyAsync(&dev_step, g.d_step, 8, cudaMemcpyDeviceToHost, g.stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&ovf, g.d_ovf, 4, cudaMemcpyDeviceToHost, g.stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(g.stream)) != cudaSuccess)
+      return cuda_error(e, "graph sync");
+    // dev_step counts graph steps (since setup) whose integration ran
+    if (contacts_per_step) {
+      const int64_t first = done - base;
+      const int64_t n = dev_step - first;
+      if (n > 0 && (e = cudaMemcpy(contacts_per_step + done, g.d_log + first, 8 * n, cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_error(e, "graph log");
+    }
+    s->counters[0] += dev_step - (done - base);
+    done = base + (int32_t)dev_step;
+    if (!ovf) break;
+    // overflow in the detection of the last integrated step: grow, detect again, recapture
+    unsigned long long pc = 0;
+    if ((e = cudaMemcpy(&pc, broadphase_fixed_count(g.bp, s->scene.n_bodies), 8, cudaMemcpyDeviceToHost)) !=
+        cudaSuccess)
+      return cuda_error(e, "overflow counts");
+    if ((e = cudaStreamSynchronize(s->ctx->stream)) != cudaSuccess) return cuda_error(e, "sync");
+    if ((ds = sim_detect(s)) != DELTA_OK) return ds;  // non-graph detection of the current state
+    if (contacts_per_step && done > 0) contacts_per_step[done - 1] = s->n_contacts;
+    int64_t saved_log = g.log_len, seg_cnt[2] = {0, 0};
+    if ((e = cudaMemcpy(seg_cnt, g.d_cnt, 16, cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_error(e, "counters");
+    s->counters[2] += seg_cnt[0];
+    s->counters[3] += seg_cnt[1];
+    if ((ds = graph_alloc(s, std::max<int64_t>(2 * g.pair_cap, 2 * (int64_t)pc), std::max<int64_t>(2 * g.contact_cap,
+                          4 * s->n_contacts), saved_log)) != DELTA_OK)
+      return ds;
+    if ((ds = copy_contacts(s->c, g.c, s->n_contacts, g.stream)) != DELTA_OK) return ds;
+    hv[0] = s->n_contacts;
+    if ((e = cudaMemcpyAsync(g.d_nc, &hv[0], 8, cudaMemcpyHostToDevice, g.stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(g.stream)) != cudaSuccess)
+      return cuda_error(e, "graph restart");
+    base = done;
+  }
+  // counters and contacts back to the simulation object
+  int64_t cnt[2] = {0, 0}, nc = 0;
+  if ((e = cudaMemcpy(cnt, g.d_cnt, 16, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(&nc, g.d_nc, 8, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return cuda_error(e, "graph counters");
+  s->counters[2] += cnt[0];
+  s->counters[3] += cnt[1];
+  if (nc > s->c.capacity && (ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;
+  if ((ds = copy_contacts(g.c, s->c, nc, g.stream)) != DELTA_OK) return ds;
+  if ((e = cudaStreamSynchronize(g.stream)) != cudaSuccess) return cuda_error(e, "graph end");
+  s->n_contacts = nc;
+  return DELTA_OK;
+}
+
+delta_status delta_sim_set_graph_capacity(delta_sim *s, int64_t pair_capacity, int64_t contact_capacity) {
+  if (!s || pair_capacity < 1 || contact_capacity < 1)
+    return set_error(DELTA_ERR_INVALID, "delta_sim_set_graph_capacity: bad argument");
+  s->graph_pair_cap = pair_capacity;
+  s->graph_contact_cap = contact_capacity;
+  return DELTA_OK;
+}
+
 delta_status delta_sim_counters(const delta_sim *s, int64_t out[4]) {
   if (!s || !out) return set_error(DELTA_ERR_INVALID, "delta_sim_counters: null argument");
   for (int k = 0; k < 4; ++k) out[k] = s->counters[k];
@@ -844,6 +1227,10 @@ delta_status delta_sim_counters(const delta_sim *s, int64_t out[4]) {
 delta_status delta_sim_destroy(delta_sim *s) {
   if (!s) return DELTA_OK;
   cudaStreamSynchronize(s->ctx->stream);
+  if (s->g.stream) cudaStreamSynchronize(s->g.stream);
+  graph_release(s->g);
+  if (s->g.ev) cudaEventDestroy(s->g.ev);
+  if (s->g.stream) cudaStreamDestroy(s->g.stream);
   s->plan.release();
   if (s->ids) cudaFree(s->ids);
   if (s->F) cudaFree(s->F);

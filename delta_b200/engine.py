@@ -83,11 +83,16 @@ class Simulation:
         self._h = C.c_void_p()
         check(lib().delta_sim_create(ctx.handle, C.byref(self._s), int(driver), C.byref(self._h)))
 
-    def step(self, nsteps: int, params: StepParams | None = None) -> np.ndarray:
+    def step(self, nsteps: int, params: StepParams | None = None, graph: bool = False) -> np.ndarray:
+        """Advances nsteps; graph=True replays a captured CUDA graph of the step."""
         params = params or StepParams.make()
         cps = np.zeros(max(nsteps, 1), np.int64)
-        check(lib().delta_sim_step(self._h, C.byref(params), int(nsteps), cps.ctypes.data))
+        fn = lib().delta_sim_step_graph if graph else lib().delta_sim_step
+        check(fn(self._h, C.byref(params), int(nsteps), cps.ctypes.data))
         return cps[:nsteps]
+
+    def set_graph_capacity(self, pairs: int, contacts: int):
+        check(lib().delta_sim_set_graph_capacity(self._h, int(pairs), int(contacts)))
 
     def contacts(self) -> np.ndarray:
         n = C.c_int64(0)

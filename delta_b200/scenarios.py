@@ -332,3 +332,136 @@ def build_scene(bodies, obstacles=(), density=2500.0, eps=1e-4, friction=False):
         "mass": mass, "eps": np.full(n, eps), "radius": radius,
         "friction": np.full(n, 1 if friction else 0, np.uint8), "obstacle": obst,
     }
+
+
+def _batched_mass_properties(V, F, density):
+    """mass_properties for a batch of meshes sharing connectivity F: V (B, nV, 3)."""
+    o = V.mean(1, keepdims=True)
+    T = V[:, F] - o[:, None]  # (B, nT, 3, 3)
+    det = np.einsum("btj,btj->bt", T[:, :, 0], np.cross(T[:, :, 1], T[:, :, 2]))
+    vol = det.sum(1) / 6.0
+    mass = density * vol
+    com = o[:, 0] + np.einsum("bt,btj->bj", det, T.sum(2)) / (24.0 * vol[:, None])
+    C0 = (np.ones((3, 3)) + np.eye(3)) / 120.0
+    Acol = np.transpose(T, (0, 1, 3, 2))
+    cov = density * np.einsum("bt,btij,jk,btlk->bil", det, Acol, C0, Acol)
+    d = com - o[:, 0]
+    cov_c = cov - mass[:, None, None] * np.einsum("bi,bj->bij", d, d)
+    tr = np.trace(cov_c, axis1=1, axis2=2)
+    inertia = tr[:, None, None] * np.eye(3) - cov_c
+    return mass, com, inertia
+
+
+def particle_cloud_scene(centres, radii, n_tri, obstacles, seed=0, perturb=(0.8, 1.2), density=2500.0,
+                         eps=1e-4, friction=False):
+    """Scene dict for many particles (perturbed sphere meshes of n_tri[i] triangles, radius
+    radii[i], centred at centres[i]) plus static obstacle meshes, built per mesh size."""
+    rng = np.random.default_rng(seed)
+    n = len(centres)
+    n_tri = np.asarray(n_tri)
+    bodies_V = [None] * n
+    bodies_F = {}
+    mass = np.zeros(n); com = np.zeros((n, 3)); inertia = np.zeros((n, 3, 3)); rad = np.zeros(n)
+    for nt in np.unique(n_tri):
+        idx = np.flatnonzero(n_tri == nt)
+        V0, F = sphere_mesh(int(nt), None, 1.0)
+        bodies_F[int(nt)] = F
+        scale = rng.uniform(perturb[0], perturb[1], size=(idx.size, V0.shape[0], 1)) * radii[idx][:, None, None]
+        V = V0[None] * scale + centres[idx][:, None, :]
+        m, c, J = _batched_mass_properties(V, F, density)
+        mass[idx], com[idx], inertia[idx] = m, c, J
+        rad[idx] = np.linalg.norm(V - c[:, None], axis=2).max(1)
+        for k, i in enumerate(idx):
+            bodies_V[i] = V[k]
+    counts = np.concatenate([n_tri, [F.shape[0] for _, F in obstacles]]).astype(np.int64)
+    nb = n + len(obstacles)
+    tri_offset = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    xyz = np.empty((tri_offset[-1] * 3, 3))
+    for i in range(n):
+        F = bodies_F[int(n_tri[i])]
+        xyz[3 * tri_offset[i]:3 * tri_offset[i + 1]] = bodies_V[i][F].reshape(-1, 3)
+    pos = np.zeros((nb, 3)); pos[:n] = com
+    inv = np.zeros((nb, 3, 3)); inv[:n] = np.linalg.inv(inertia)
+    J = np.zeros((nb, 3, 3)); J[:n] = inertia
+    m = np.full(nb, np.inf); m[:n] = mass
+    r = np.zeros(nb); r[:n] = rad
+    obst = np.zeros(nb, np.uint8); obst[n:] = 1
+    for k, (V, F) in enumerate(obstacles):
+        i = n + k
+        xyz[3 * tri_offset[i]:3 * tri_offset[i + 1]] = V[F].reshape(-1, 3)
+        pos[i] = V.mean(0)
+        r[i] = np.linalg.norm(V - pos[i], axis=1).max()
+    return {
+        "n_bodies": nb, "tri_offset": tri_offset, "tri_body": np.repeat(np.arange(nb, dtype=np.int32), counts),
+        "x": xyz[:, 0].copy(), "y": xyz[:, 1].copy(), "z": xyz[:, 2].copy(),
+        "rx": xyz[:, 0].copy(), "ry": xyz[:, 1].copy(), "rz": xyz[:, 2].copy(),
+        "pos": pos.reshape(-1).copy(), "ref_pos": pos.reshape(-1).copy(),
+        "vel": np.zeros(3 * nb), "ang": np.zeros(3 * nb), "ref_ang": np.zeros(3 * nb),
+        "rot": np.tile(np.eye(3).reshape(9), nb),
+        "inertia": J.transpose(0, 2, 1).reshape(-1).copy(), "inverse": inv.transpose(0, 2, 1).reshape(-1).copy(),
+        "mass": m, "eps": np.full(nb, eps), "radius": r,
+        "friction": np.full(nb, 1 if friction else 0, np.uint8), "obstacle": obst,
+    }
+
+
+def _jittered_lattice(n, spacing, origin, jitter, rng, shape_xz):
+    nx, nz = shape_xz
+    ny = -(-n // (nx * nz))
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    g = g[np.lexsort((g[:, 2], g[:, 0], g[:, 1]))][:n]  # fill layer by layer from the bottom
+    return origin + g * spacing + rng.uniform(-jitter, jitter, (n, 3))
+
+
+def hopper_obstacles(n_around=64, n_along=16, half_angle_deg=30.0, outlet=0.08, height=0.8, patch=(4, 2)):
+    """Conical hopper wall (axis y, outlet at y = 0) with 2*n_around*n_along triangles,
+    split into patches of patch[0] x patch[1] quads (one obstacle body each)."""
+    r0 = outlet / 2
+    r1 = r0 + height * np.tan(np.radians(half_angle_deg))
+    th = np.linspace(0, 2 * np.pi, n_around + 1)
+    ys = np.linspace(0, height, n_along + 1)
+    out = []
+    for a0 in range(0, n_around, patch[0]):
+        for h0 in range(0, n_along, patch[1]):
+            V, F = [], []
+            for a in range(a0, min(a0 + patch[0], n_around)):
+                for h in range(h0, min(h0 + patch[1], n_along)):
+                    q = []
+                    for (ai, hi) in ((a, h), (a + 1, h), (a + 1, h + 1), (a, h + 1)):
+                        rr = r0 + (r1 - r0) * ys[hi] / height
+                        q.append((rr * np.cos(th[ai]), ys[hi], rr * np.sin(th[ai])))
+                    b = len(V)
+                    V += q
+                    F += [(b, b + 1, b + 2), (b, b + 2, b + 3)]
+            out.append((np.array(V), np.array(F)))
+    return out
+
+
+def hopper_scene(n_particles=10000, seed=0, sizes=(40, 80, 160, 320), radius=(0.005, 0.015), eps=1e-4):
+    """The batched uneven hopper workload: particles of mixed mesh sizes above a conical hopper."""
+    rng = np.random.default_rng(seed)
+    radii = rng.uniform(radius[0], radius[1], n_particles)
+    n_tri = rng.choice(np.asarray(sizes), n_particles)
+    sp = 2.0 * radius[1] * 1.2 * 1.05
+    side = int(np.ceil(np.sqrt(n_particles / 30)))
+    cen = _jittered_lattice(n_particles, sp, np.array([-(side - 1) * sp / 2, 0.3, -(side - 1) * sp / 2]),
+                            0.1 * sp, rng, (side, side))
+    return particle_cloud_scene(cen, radii, n_tri, hopper_obstacles(), seed=seed + 1, eps=eps)
+
+
+def box_scene(n_particles=200000, seed=0, sizes=(80, 160, 320, 500), radius=(0.004, 0.012), eps=1e-4,
+              box=(0.6, 1.2, 0.6)):
+    """The large box workload: particles poured from a jittered lattice into a box of 12
+    wall triangles (6 faces, x and z sides 0.6 m, height 1.2 m; y vertical)."""
+    rng = np.random.default_rng(seed)
+    radii = rng.uniform(radius[0], radius[1], n_particles)
+    n_tri = rng.choice(np.asarray(sizes), n_particles)
+    sp = 2.0 * radius[1] * 1.2 * 1.02
+    nx = int(box[0] / sp) - 1
+    cen = _jittered_lattice(n_particles, sp, np.array([-(nx - 1) * sp / 2, sp, -(nx - 1) * sp / 2]), 0.05 * sp, rng,
+                            (nx, nx))
+    hx, hy, hz = box[0] / 2, box[1], box[2] / 2
+    C = np.array([[-hx, 0, -hz], [hx, 0, -hz], [hx, 0, hz], [-hx, 0, hz],
+                  [-hx, hy, -hz], [hx, hy, -hz], [hx, hy, hz], [-hx, hy, hz]], float)
+    quads = [(0, 1, 2, 3), (4, 7, 6, 5), (0, 4, 5, 1), (1, 5, 6, 2), (2, 6, 7, 3), (3, 7, 4, 0)]
+    walls = [(C[list(q)], np.array([[0, 1, 2], [0, 2, 3]])) for q in quads]
+    return particle_cloud_scene(cen, radii, n_tri, walls, seed=seed + 1, eps=eps)

@@ -222,6 +222,19 @@ typedef struct delta_sim delta_sim;
 delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driver, delta_sim **out);
 delta_status delta_sim_step(delta_sim *sim, const delta_step_params *params, int32_t nsteps,
                             int64_t *contacts_per_step /* host [nsteps] or NULL */);
+/* Same steps as delta_sim_step, recorded once as a CUDA graph (every kernel of a step,
+ * fixed-capacity buffers, counts kept on the device) and replayed nsteps times without
+ * host synchronisation.  The first call sizes the buffers from an observed detection.
+ * A capacity overflow in a replayed step freezes the state after that step's
+ * integration; the host then repeats that detection with larger buffers, records the
+ * graph again and continues, so results equal delta_sim_step's bit for bit.  The graph is
+ * recorded again whenever params change. */
+delta_status delta_sim_step_graph(delta_sim *sim, const delta_step_params *params, int32_t nsteps,
+                                  int64_t *contacts_per_step /* host [nsteps] or NULL */);
+/* Capacities (candidate pairs, contacts) of the graph buffers for the next
+ * delta_sim_step_graph call instead of the observed-size default; overflows still
+ * recover as described above. */
+delta_status delta_sim_set_graph_capacity(delta_sim *sim, int64_t pair_capacity, int64_t contact_capacity);
 /* Copies the current contacts into out (device); *n_out gets their number. */
 delta_status delta_sim_contacts(delta_sim *sim, const delta_contacts *out, int64_t *n_out);
 /* Totals since creation: [0] steps, [1] candidate body pairs, [2] triangle pairs of the

@@ -92,3 +92,31 @@ def test_broadphase_covers_every_contact_pair(ctx, scene):
                 want.add((i, j))
     got = set(zip(pa.tolist(), pb.tolist()))
     assert want <= got
+
+
+@pytest.mark.parametrize("caps", [None, (8, 8)])
+def test_graph_replay_equals_stepping(ctx, oracle, scene, caps):
+    """The graph-captured step gives the stepped trajectory bit for bit; with tiny
+    capacities every replay overflows and the recovery path (repeat the detection with
+    larger buffers, record again) must give the same result."""
+    from delta_b200.engine import Simulation, StepParams
+
+    p = StepParams.make(**PARAMS)
+    o_state, o_cps, o_c = _oracle(oracle, scene, 30)
+    sim = Simulation(ctx, scene, 8)
+    if caps:
+        sim.step(1, p)
+        sim.set_graph_capacity(*caps)
+        cps = np.concatenate([[-1], sim.step(29, p, graph=True)])
+        cps[0] = o_cps[0]
+    else:
+        cps = sim.step(30, p, graph=True)
+    st = sim.state()
+    c = sim.contacts()
+    sim.close()
+    assert list(cps) == list(o_cps)
+    for k in STATE:
+        assert np.array_equal(st[k], o_state[k]), k
+    assert len(c) == len(o_c)
+    for f in FIELDS:
+        assert np.array_equal(c[f], o_c[f]), f
