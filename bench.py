@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--timestep-steps", type=int, default=200)
+    ap.add_argument("--hopper-steps", type=int, default=50)
     return ap.parse_args()
 
 
@@ -148,45 +149,50 @@ def cpu_reference_rate(a, b, sample: int, min_seconds: float):
     return done / el, cores, kind
 
 
-def timestep_section(ctx, stream, steps: int, warmup: int, seed: int):
-    """Timesteps/s of the small plain-method workload (256 perturbed 80-triangle spheres on a
-    8x4x8 lattice over a floor, FP64, dt 1e-5) with the plain FP64 bf driver (every
-    triangle pair of every candidate body pair) and with the certified FP32 driver (exact
-    box culling + bf_cert).  Both must give the same trajectory bit for bit."""
+def _time_sim(ctx, stream, sim, steps, params, graph):
     import torch
 
-    from delta_b200.detection import DRV_BF, DRV_BF_CERT
-    from delta_b200.engine import Simulation, StepParams
-    from delta_b200.scenarios import lattice_scene
+    c0 = sim.counters()
+    l0 = ctx.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    sim.step(steps, params, graph=graph)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    # graph replays run on the simulation's own stream: the wall clock brackets them
+    t = wall if graph else e0.elapsed_time(e1) / 1e3
+    c1 = sim.counters()
+    tri = c1["triangle_pairs"] - c0["triangle_pairs"]
+    return {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps, "triangle_pair_tests_per_s": tri / t,
+            "triangle_pairs_per_step": tri / steps, "solved_pairs_per_step": (c1["solved"] - c0["solved"]) / steps,
+            "body_pairs_per_step": (c1["body_pairs"] - c0["body_pairs"]) / steps,
+            "gpu_launches": ctx.launches - l0, "timer": "wall clock around synchronised replays" if graph else
+            "CUDA events"}
 
-    sc = lattice_scene(seed)
-    params = StepParams.make(dt=1e-5, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0)
+
+def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, params):
+    """Timesteps/s of a scene with the plain FP64 bf driver (every triangle pair of every
+    candidate body pair, as the reference) and with the certified FP32 driver (exact box
+    culling + bf_cert), stepped and replayed as a CUDA graph.  All three must give the same
+    trajectory bit for bit."""
+    from delta_b200.detection import DRV_BF, DRV_BF_CERT
+    from delta_b200.engine import Simulation
+
     out, states = {}, {}
-    for name, drv in (("fp64_bf", DRV_BF), ("bf_cert_culled", DRV_BF_CERT)):
-        sim = Simulation(ctx, sc, drv)
-        sim.step(warmup, params)
-        c0 = sim.counters()
-        l0 = ctx.launches
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        sim.step(steps, params)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        t = e0.elapsed_time(e1) / 1e3
-        c1 = sim.counters()
-        tri = c1["triangle_pairs"] - c0["triangle_pairs"]
-        out[name] = {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps,
-                     "triangle_pair_tests_per_s": tri / t, "triangle_pairs_per_step": tri / steps,
-                     "solved_pairs_per_step": (c1["solved"] - c0["solved"]) / steps,
-                     "body_pairs_per_step": (c1["body_pairs"] - c0["body_pairs"]) / steps,
-                     "gpu_launches": ctx.launches - l0}
+    for name, drv, graph in (("fp64_bf", DRV_BF, False), ("bf_cert_culled", DRV_BF_CERT, False),
+                             ("bf_cert_culled_graph", DRV_BF_CERT, True)):
+        sim = Simulation(ctx, scene, drv)
+        sim.step(warmup, params, graph=graph)
+        out[name] = _time_sim(ctx, stream, sim, steps, params, graph)
         states[name] = sim.state()
         sim.close()
-    same = all(np.array_equal(states["fp64_bf"][k], states["bf_cert_culled"][k]) for k in ("pos", "vel", "rot", "x"))
-    return {"workload": "256 perturbed icospheres (80 tri) on a 8x4x8 lattice over a 2-triangle floor, FP64, "
-                        "dt 1e-5, k 1e6, damping 0.1", "steps": steps, "warmup": warmup, **out,
-            "speedup": out["bf_cert_culled"]["steps_per_s"] / out["fp64_bf"]["steps_per_s"],
+    ref = states["fp64_bf"]
+    same = all(np.array_equal(ref[k], st[k]) for st in states.values() for k in ("pos", "vel", "rot", "x"))
+    return {"workload": workload, "steps": steps, "warmup": warmup, **out,
+            "speedup": out["bf_cert_culled_graph"]["steps_per_s"] / out["fp64_bf"]["steps_per_s"],
             "trajectories_bit_identical": bool(same)}
 
 
@@ -319,7 +325,22 @@ def main():
                "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes),
                "path": "delta_pairs_run_host (C ABI), pinned host buffers, copies in the timed region"}
 
-    ts = timestep_section(ctx, stream, args.timestep_steps, 3, args.seed) if args.timestep_steps > 0 else None
+    ts = hop = None
+    if args.timestep_steps > 0:
+        from delta_b200.engine import StepParams
+        from delta_b200.scenarios import hopper_scene, lattice_scene
+
+        ts = timestep_section(
+            ctx, stream, lattice_scene(args.seed),
+            "256 perturbed icospheres (80 tri) on a 8x4x8 lattice over a 2-triangle floor, FP64, dt 1e-5, k 1e6, "
+            "damping 0.1", args.timestep_steps, 3,
+            StepParams.make(dt=1e-5, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0))
+        if args.hopper_steps > 0:
+            hop = timestep_section(
+                ctx, stream, hopper_scene(10000, seed=args.seed),
+                "10,000 perturbed spheres of {40,80,160,320} triangles (r 5-15 mm) over a conical hopper of 2,048 "
+                "wall triangles (30 deg, 8 cm outlet), FP64, dt 5e-6", args.hopper_steps, 3,
+                StepParams.make(dt=5e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -352,6 +373,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "timestep": ts,
+            "timestep_hopper": hop,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -342,9 +342,11 @@ def _batched_mass_properties(V, F, density):
     vol = det.sum(1) / 6.0
     mass = density * vol
     com = o[:, 0] + np.einsum("bt,btj->bj", det, T.sum(2)) / (24.0 * vol[:, None])
-    C0 = (np.ones((3, 3)) + np.eye(3)) / 120.0
-    Acol = np.transpose(T, (0, 1, 3, 2))
-    cov = density * np.einsum("bt,btij,jk,btlk->bil", det, Acol, C0, Acol)
+    # sum over tetrahedra of det * A C0 A^T with C0 = (I + 1 1^T)/120, i.e.
+    # det/120 * (sum_v v v^T + s s^T), s = sum of the three vertices
+    ssum = T.sum(2)
+    cov = density / 120.0 * (np.einsum("bt,btvi,btvj->bij", det, T, T, optimize=True) +
+                             np.einsum("bt,bti,btj->bij", det, ssum, ssum, optimize=True))
     d = com - o[:, 0]
     cov_c = cov - mass[:, None, None] * np.einsum("bi,bj->bij", d, d)
     tr = np.trace(cov_c, axis1=1, axis2=2)
@@ -359,27 +361,23 @@ def particle_cloud_scene(centres, radii, n_tri, obstacles, seed=0, perturb=(0.8,
     rng = np.random.default_rng(seed)
     n = len(centres)
     n_tri = np.asarray(n_tri)
-    bodies_V = [None] * n
-    bodies_F = {}
-    mass = np.zeros(n); com = np.zeros((n, 3)); inertia = np.zeros((n, 3, 3)); rad = np.zeros(n)
-    for nt in np.unique(n_tri):
-        idx = np.flatnonzero(n_tri == nt)
-        V0, F = sphere_mesh(int(nt), None, 1.0)
-        bodies_F[int(nt)] = F
-        scale = rng.uniform(perturb[0], perturb[1], size=(idx.size, V0.shape[0], 1)) * radii[idx][:, None, None]
-        V = V0[None] * scale + centres[idx][:, None, :]
-        m, c, J = _batched_mass_properties(V, F, density)
-        mass[idx], com[idx], inertia[idx] = m, c, J
-        rad[idx] = np.linalg.norm(V - c[:, None], axis=2).max(1)
-        for k, i in enumerate(idx):
-            bodies_V[i] = V[k]
     counts = np.concatenate([n_tri, [F.shape[0] for _, F in obstacles]]).astype(np.int64)
     nb = n + len(obstacles)
     tri_offset = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
     xyz = np.empty((tri_offset[-1] * 3, 3))
-    for i in range(n):
-        F = bodies_F[int(n_tri[i])]
-        xyz[3 * tri_offset[i]:3 * tri_offset[i + 1]] = bodies_V[i][F].reshape(-1, 3)
+    mass = np.zeros(n); com = np.zeros((n, 3)); inertia = np.zeros((n, 3, 3)); rad = np.zeros(n)
+    for nt in np.unique(n_tri):
+        idx = np.flatnonzero(n_tri == nt)
+        V0, F = sphere_mesh(int(nt), None, 1.0)
+        for lo in range(0, idx.size, 20000):  # bounded temporaries
+            sub = idx[lo:lo + 20000]
+            scale = rng.uniform(perturb[0], perturb[1], size=(sub.size, V0.shape[0], 1)) * radii[sub][:, None, None]
+            V = V0[None] * scale + centres[sub][:, None, :]
+            m, c, J = _batched_mass_properties(V, F, density)
+            mass[sub], com[sub], inertia[sub] = m, c, J
+            rad[sub] = np.linalg.norm(V - c[:, None], axis=2).max(1)
+            vidx = (3 * tri_offset[sub])[:, None] + np.arange(3 * int(nt))[None]
+            xyz[vidx.reshape(-1)] = V[:, F].reshape(-1, 3)
     pos = np.zeros((nb, 3)); pos[:n] = com
     inv = np.zeros((nb, 3, 3)); inv[:n] = np.linalg.inv(inertia)
     J = np.zeros((nb, 3, 3)); J[:n] = inertia
