@@ -28,6 +28,10 @@ struct RawContacts {
   uint64_t *key;
   int64_t cap;
   unsigned long long *count;
+  // certified driver: triangle pairs that survive the box test, as keys (pair, A tri, B tri)
+  uint64_t *sv;
+  int64_t sv_cap;
+  unsigned long long *sv_count;
 };
 
 struct DevStats {
@@ -174,20 +178,9 @@ __device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawCon
       ahi[k] = fmax(A[0][k], fmax(A[1][k], A[2][k]));
     }
     const double cull = mg * (1.0 + 1e-9) + 1e-12;
-    int32_t *surv = csm->surv;
-    int count = 0;
-    auto run_batch = [&](int nb) {
-      if (lane == 0) atomicAdd(&st->evaluated, (unsigned long long)nb);
-      const bool valid = lane < nb;
-      const int32_t tb = surv[valid ? lane : 0];
-      double B[3][3];
-      load_tri64(m, r.tB0 + tb, B);
-      bf_cert_warp(A, B, valid, pq, *csm);
-      const bool take = valid && pq_dist64(pq) <= mg;  // bf.cpp:125
-      emit(rc, take, pq, r, tb);
-    };
+    const int lane_ = lane;
     for (int32_t base = 0; base < r.nB; base += 32) {
-      const int32_t tb = base + lane;
+      const int32_t tb = base + lane_;
       bool keep = false;
       if (tb < r.nB) {
         double B[3][3], g2 = 0.0;
@@ -201,18 +194,17 @@ __device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawCon
         keep = g2 <= cull * cull;
       }
       const unsigned mask = __ballot_sync(kFull, keep);
-      if (keep) surv[count + __popc(mask & ((1u << lane) - 1u))] = tb;
-      count += __popc(mask);
-      __syncwarp();
-      if (count >= 32) {
-        run_batch(32);
-        __syncwarp();
-        if (lane < count - 32) surv[lane] = surv[32 + lane];
-        count -= 32;
-        __syncwarp();
+      if (!mask) continue;
+      unsigned long long sbase = 0;
+      if (lane_ == 0) sbase = atomicAdd(rc.sv_count, (unsigned long long)__popc(mask));
+      sbase = __shfl_sync(kFull, sbase, 0);
+      if (keep) {
+        const int64_t pos = (int64_t)sbase + __popc(mask & ((1u << lane_) - 1u));
+        if (pos < rc.sv_cap) rc.sv[pos] = ((uint64_t)r.k << 32) | ((uint64_t)r.iA << 16) | (uint64_t)tb;
       }
     }
-    if (count > 0) run_batch(count);
+    (void)csm;
+    (void)pq;
   } else if constexpr (DRV == DELTA_DRV_BF || DRV == DELTA_DRV_GJK) {
     constexpr int S = DRV == DELTA_DRV_BF ? S_BF : S_GJK;
     for_row(r.nB, [&](int32_t tb, bool valid) {
@@ -349,6 +341,48 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
     }
     process_row<R, DRV>(m, r, rc, st, csm);
   }
+}
+
+// Certified bf over the survivors of the box test, 32 per warp (any mix of pairs).
+__global__ void __launch_bounds__(128) k_cert_survivors(delta_meshes m, const int32_t *__restrict__ pa,
+                                                        const int32_t *__restrict__ pb, RawContacts rc,
+                                                        DevStats *st) {
+  __shared__ CertWarpSmem sm[4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned long long cnt = *rc.sv_count;
+  const int64_t n = (int64_t)cnt < rc.sv_cap ? (int64_t)cnt : rc.sv_cap;
+  if (n == 0) return;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += nwarps * 32) {
+    const int64_t i = base + lane;
+    const bool valid = i < n;
+    const uint64_t key = rc.sv[valid ? i : n - 1];
+    RowCtx r;
+    r.k = (int64_t)(key >> 32);
+    r.iA = (int32_t)((key >> 16) & 0xffff);
+    const int32_t tb = (int32_t)(key & 0xffff);
+    const int32_t a = pa[r.k], b = pb[r.k];
+    r.tA = m.tri_offset[a] + r.iA;
+    r.tB0 = m.tri_offset[b];
+    r.epsA = m.eps[a];
+    r.epsB = m.eps[b];
+    r.idA = m.id[a];
+    r.idB = m.id[b];
+    r.fric = (m.friction[a] && m.friction[b]) ? 1 : 0;
+    double A[3][3], B[3][3], pq[6];
+    load_tri64(m, r.tA, A);
+    load_tri64(m, r.tB0 + tb, B);
+    bf_cert_warp(A, B, valid, pq, sm[warp]);
+    const double mg = (xf64(r.epsA) + xf64(r.epsB)).v;
+    const bool take = valid && pq_dist64(pq) <= mg;  // bf.cpp:125
+    emit(rc, take, pq, r, tb);
+  }
+}
+
+__global__ void k_sv_evaluated(const unsigned long long *sv_count, int64_t sv_cap, DevStats *st, int *ovf) {
+  const unsigned long long c = *sv_count;
+  st->evaluated += c;
+  if (ovf && c > (unsigned long long)sv_cap) atomicCAS(ovf, 0, 1);
 }
 
 __global__ void k_rows_per_pair(const int64_t *tri_offset, const int32_t *pa, int64_t n_pairs, int32_t n_bodies,
@@ -504,6 +538,7 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   DevStats *dstats = (DevStats *)((char *)small + 256);
   unsigned long long *queue = (unsigned long long *)((char *)small + 256 + sizeof(DevStats));
   unsigned long long *count = queue + 1;
+  unsigned long long *sv_count = queue + 2;
   if ((e = cudaMemsetAsync(small, 0, small_bytes, s)) != cudaSuccess) return cuda_error(e, "detect memset");
 
   // rows per pair and their exclusive prefix sum
@@ -547,18 +582,54 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
     rc.i = (int32_t *)(rc.key + 2 * cap);
     rc.fric = (uint8_t *)(rc.i + 4 * cap);
     rc.count = count;
-    if ((e = cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
+    rc.sv_count = sv_count;
+    if ((e = cudaMemsetAsync(queue, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess)
       return cuda_error(e, "memset");
     if ((e = cudaMemsetAsync(dstats, 0, sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
-    e = precision == DELTA_F32 && driver != DELTA_DRV_BF_CERT
+    if (driver == DELTA_DRV_BF_CERT) {
+      // phase 1: box culling into the survivor list (grown and repeated on overflow);
+      // phase 2: certified bf over the survivors, full warps across pairs
+      int64_t sv_cap = 8 * cap > (1 << 16) ? 8 * cap : (1 << 16);
+      unsigned long long hsv = 0;
+      for (int sv_attempt = 0; sv_attempt < 2; ++sv_attempt) {
+        void *svb = nullptr;
+        if ((st = ctx_scratch(ctx, 9, sizeof(uint64_t) * (size_t)sv_cap, &svb)) != DELTA_OK) return st;
+        rc.sv = (uint64_t *)svb;
+        rc.sv_cap = sv_cap;
+        if ((e = cudaMemsetAsync(queue, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess)
+          return cuda_error(e, "memset");
+        if ((e = launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats,
+                                                         queue)) != cudaSuccess)
+          return cuda_error(e, "cull kernel");
+        ctx->launches += 1;
+        if ((e = cudaMemcpyAsync(&hsv, sv_count, sizeof(hsv), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+          return cuda_error(e, "survivor count");
+        if ((int64_t)hsv <= sv_cap) break;
+        sv_cap = (int64_t)hsv + hsv / 4;
+      }
+      int per_sm = 0;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0)) != cudaSuccess)
+        return cuda_error(e, "occupancy");
+      int64_t blocks = ((int64_t)hsv + 127) / 128;
+      const int64_t mx = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
+      if (blocks > mx) blocks = mx;
+      if (blocks < 1) blocks = 1;
+      k_cert_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc, dstats);
+      k_sv_evaluated<<<1, 1, 0, s>>>(sv_count, rc.sv_cap, dstats, nullptr);
+      ctx->launches += 2;
+      e = cudaGetLastError();
+    } else {
+      e = precision == DELTA_F32
             ? launch_detect_prec<float>(driver, s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats, queue)
             : (driver == DELTA_DRV_BF_CERT
                    ? launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, n_pairs, total_rows, rc,
                                                              dstats, queue)
                    : launch_detect_prec<xf64>(driver, s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats,
                                               queue));
+      ctx->launches += 1;
+    }
     if (e != cudaSuccess) return cuda_error(e, "detect kernel");
-    ctx->launches += 1;
     if ((e = cudaMemcpyAsync(&hcount, count, sizeof(hcount), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
       return cuda_error(e, "detect count");
@@ -628,10 +699,12 @@ size_t detect_fixed_temp_bytes(int64_t pair_cap, int64_t cap) {
   return a > b ? a : b;
 }
 
+static int64_t fixed_sv_cap(int64_t cap) { return 32 * cap > (1 << 16) ? 32 * cap : (1 << 16); }
+
 size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap) {
   const size_t per = 14 * sizeof(double) + 4 * sizeof(int32_t) + 1 + 2 * sizeof(uint64_t);
   return 512 + sizeof(DevStats) + sizeof(int64_t) * (size_t)(2 * pair_cap + 2) + per * (size_t)cap +
-         sizeof(int64_t) * 2 * (size_t)cap + 256;
+         sizeof(int64_t) * 2 * (size_t)cap + 256 + sizeof(uint64_t) * (size_t)fixed_sv_cap(cap) + 256;
 }
 
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
@@ -657,15 +730,29 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
   int64_t *perm_in = (int64_t *)p, *perm_out = perm_in + cap;
   uint64_t *key_out = rc.key + cap;
+  p += sizeof(int64_t) * 2 * (size_t)cap;
+  p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+  rc.sv = (uint64_t *)p;
+  rc.sv_cap = fixed_sv_cap(cap);
+  rc.sv_count = queue + 2;
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
   if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");
   k_rows_fixed<<<(unsigned)((pair_cap + 256) / 256), 256, 0, s>>>(m.tri_offset, pa, pair_cap, rows);
   size_t tb = temp_bytes;
   if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
     return cuda_error(e, "row scan");
-  e = driver == DELTA_DRV_BF_CERT
-          ? launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue)
-          : launch_detect_t<xf64, DELTA_DRV_BF>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue);
+  if (driver == DELTA_DRV_BF_CERT) {
+    e = launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue);
+    if (e != cudaSuccess) return cuda_error(e, "cull kernel");
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0)) != cudaSuccess)
+      return cuda_error(e, "occupancy");
+    k_cert_survivors<<<(unsigned)(kNumSMs * (per_sm > 0 ? per_sm : 1)), 128, 0, s>>>(m, pa, pb, rc, dstats);
+    k_sv_evaluated<<<1, 1, 0, s>>>(rc.sv_count, rc.sv_cap, dstats, d_ovf);
+    ctx->launches += 2;
+  } else {
+    e = launch_detect_t<xf64, DELTA_DRV_BF>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue);
+  }
   if (e != cudaSuccess) return cuda_error(e, "detect kernel");
   k_iota<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(perm_in, cap);
   tb = temp_bytes;
