@@ -282,6 +282,11 @@ def main():
         total = ev[0].elapsed_time(ev[steps])
         return total, per, ctx.launches - l0
 
+    # launch shapes chosen by the autotuner on this rank's pairs (headline and comparison)
+    from delta_b200.narrowphase import autotune
+
+    tuned = {args.method: autotune(ctx, method, a, b, out=out), "bf": autotune(ctx, 0, a, b, out=out64)}
+
     peak, peak_kind = measured_peak_hbm()
     with ClockSampler(local) as clk:
         total_ms, per_ms, launches = timed(method, out, args.steps, args.warmup)
@@ -360,6 +365,7 @@ def main():
             "config": {**workload_config(n), "method": args.method,
                        "comparison": "plain FP64 bf kernel on the same pairs"},
             "fp64_bf": {"value": value64, "unit": "pairs/s", "ms_per_step": total64_ms / steps64},
+            "autotuned_launch": tuned,
             "speedup_vs_fp64_bf": value / value64,
             "parity_vs_fp64_bf": {"pairs_differing": int(diff), "max_rel_dist_err": rel,
                                   "mean_fp64_feature_evals": mean_evals},

@@ -30,6 +30,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_launch_count": ([vp], i64),
     "delta_pairs_run": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp], C.c_int),
     "delta_pairs_run_host": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp], C.c_int),
+    "delta_set_pair_launch": ([vp, C.c_int, C.c_int, i32, i32], C.c_int),
+    "delta_autotune_pairs": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "delta_pairs_run_host_noalloc": ([vp, C.c_int, C.c_int, i64, vp, vp, i64, f8, vp, vp, vp, vp], C.c_int),
     "delta_detect": ([vp, C.c_int, C.c_int, vp, vp, vp, i64, vp, vp, vp], C.c_int),
     "delta_forces": ([vp, vp, vp, i64, vp, vp, vp, vp], C.c_int),

@@ -2,6 +2,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "internal.h"
 
@@ -104,6 +105,10 @@ delta_status delta_synchronize(delta_ctx *ctx) {
 
 int64_t delta_launch_count(const delta_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
+static PairLaunch ctx_pair_launch(const delta_ctx *ctx, int method, int precision) {
+  return ctx->pair_launch_set[method][precision] ? ctx->pair_launch[method][precision] : default_pair_launch(method);
+}
+
 static delta_status check_pairs(delta_ctx *ctx, int method, int precision, int64_t n, const void *a, const void *b,
                                 int64_t ld, const void *p, const void *q, const void *dist) {
   if (!ctx) return set_error(DELTA_ERR_INVALID, "null context");
@@ -119,9 +124,69 @@ delta_status delta_pairs_run(delta_ctx *ctx, int method, int precision, int64_t 
                              uint8_t *flags) {
   delta_status st = check_pairs(ctx, method, precision, n, a, b, ld, p, q, dist);
   if (st != DELTA_OK || n == 0) return st;
-  cudaError_t e = launch_pairs(method, precision, ctx->stream, n, a, b, ld, max_error, p, q, dist, flags);
+  cudaError_t e = launch_pairs_cfg(method, precision, ctx->stream, n, a, b, ld, max_error, p, q, dist, flags,
+                                   ctx_pair_launch(ctx, method, precision));
   if (e != cudaSuccess) return cuda_error(e, "pairs kernel launch");
   ctx->launches += 1;
+  return DELTA_OK;
+}
+
+delta_status delta_set_pair_launch(delta_ctx *ctx, int method, int precision, int32_t threads,
+                                   int32_t blocks_per_sm) {
+  if (!ctx || method < DELTA_BF || method > DELTA_BF_CERT || (precision != 0 && precision != 1))
+    return set_error(DELTA_ERR_INVALID, "delta_set_pair_launch: bad method/precision");
+  if (!(threads == 64 || threads == 128 || threads == 256) || blocks_per_sm < 1 ||
+      (method == DELTA_BF_CERT && threads == 256))
+    return set_error(DELTA_ERR_INVALID, "delta_set_pair_launch: unsupported launch shape");
+  ctx->pair_launch[method][precision] = PairLaunch{threads, blocks_per_sm};
+  ctx->pair_launch_set[method][precision] = true;
+  return DELTA_OK;
+}
+
+delta_status delta_autotune_pairs(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
+                                  const double *b, int64_t ld, double max_error, double *p, double *q, double *dist,
+                                  uint8_t *flags, int32_t *threads_out, int32_t *blocks_per_sm_out, float *ms_out) {
+  delta_status st = check_pairs(ctx, method, precision, n, a, b, ld, p, q, dist);
+  if (st != DELTA_OK) return st;
+  if (n == 0) return set_error(DELTA_ERR_INVALID, "delta_autotune_pairs: empty sample");
+  std::vector<PairLaunch> cand;
+  if (method == DELTA_BF_CERT) {
+    for (int t : {64, 128})
+      for (int b : {2, 4, 8, 16}) cand.push_back(PairLaunch{t, b});
+  } else {
+    for (int t : {64, 128, 256})
+      for (int b : {4, 8, 16, 32}) cand.push_back(PairLaunch{t, b});
+  }
+  cudaEvent_t e0, e1;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) return cuda_error(e, "autotune events");
+  float best = 1e30f;
+  PairLaunch bestc = default_pair_launch(method);
+  for (const PairLaunch &c : cand) {
+    e = launch_pairs_cfg(method, precision, ctx->stream, n, a, b, ld, max_error, p, q, dist, flags, c);  // warm-up
+    if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+      e = launch_pairs_cfg(method, precision, ctx->stream, n, a, b, ld, max_error, p, q, dist, flags, c);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) break;
+    ctx->launches += 4;
+    if (ms / 3 < best) {
+      best = ms / 3;
+      bestc = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_error(e, "autotune");
+  ctx->pair_launch[method][precision] = bestc;
+  ctx->pair_launch_set[method][precision] = true;
+  if (threads_out) *threads_out = bestc.threads;
+  if (blocks_per_sm_out) *blocks_per_sm_out = bestc.blocks_per_sm;
+  if (ms_out) *ms_out = best;
   return DELTA_OK;
 }
 
@@ -149,7 +214,8 @@ delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int
                             cudaMemcpyHostToDevice, ctx->stream);
   }
   if (e != cudaSuccess) return cuda_error(e, "pairs H2D");
-  e = launch_pairs(method, precision, ctx->stream, n, da, db, n, max_error, dp, dq, dd, flags ? df : nullptr);
+  e = launch_pairs_cfg(method, precision, ctx->stream, n, da, db, n, max_error, dp, dq, dd, flags ? df : nullptr,
+                       ctx_pair_launch(ctx, method, precision));
   if (e != cudaSuccess) return cuda_error(e, "pairs kernel launch");
   ctx->launches += 1;
   if (ld == n) {

@@ -11,7 +11,25 @@ namespace delta {
 
 constexpr int kNumSMs = 148;  // B200
 
-// Pair-list launcher (pairs.cu).
+// Launch shape of a pair-list kernel: threads per block (64, 128, 256) and the grid
+// cap in blocks per SM (cert: in units of the occupancy limit).
+struct PairLaunch {
+  int threads = 256;
+  int blocks_per_sm = 32;
+};
+inline PairLaunch default_pair_launch(int method) {
+  PairLaunch c;
+  if (method == 5) {
+    c.threads = 128;
+    c.blocks_per_sm = 8;
+  }
+  return c;
+}
+cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
+                             int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags,
+                             PairLaunch cfg);
+
+// Pair-list launcher (pairs.cu), default launch shape.
 cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
                          int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags);
 
@@ -44,6 +62,9 @@ struct delta_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int64_t launches = 0;
+  // launch shapes of the pair kernels [method][precision], set by autotuning
+  delta::PairLaunch pair_launch[6][2];
+  bool pair_launch_set[6][2] = {};
   delta_buffer scratch[16];
   void *pinned = nullptr;
   size_t pinned_bytes = 0;

@@ -56,11 +56,12 @@ __global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restri
 
 // bf_cert: warps walk the pair list 32 pairs at a time (the certificate's candidate queue
 // is shared by the warp).
-__global__ void __launch_bounds__(128, 5) k_pairs_cert(int64_t n, const double *__restrict__ a,
-                                                    const double *__restrict__ b, int64_t ld,
-                                                    double *__restrict__ p, double *__restrict__ q,
-                                                    double *__restrict__ dist, uint8_t *__restrict__ flags) {
-  __shared__ CertWarpSmem sm[4];
+template <int W>
+__global__ void __launch_bounds__(32 * W) k_pairs_cert(int64_t n, const double *__restrict__ a,
+                                                       const double *__restrict__ b, int64_t ld,
+                                                       double *__restrict__ p, double *__restrict__ q,
+                                                       double *__restrict__ dist, uint8_t *__restrict__ flags) {
+  __shared__ CertWarpSmem sm[W];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += nwarps * 32) {
@@ -94,10 +95,10 @@ __global__ void __launch_bounds__(128, 5) k_pairs_cert(int64_t n, const double *
 
 template <class R, int M>
 static cudaError_t launch_one(cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld, double me,
-                              double *p, double *q, double *dist, uint8_t *flags) {
-  const int threads = 256;
+                              double *p, double *q, double *dist, uint8_t *flags, PairLaunch cfg) {
+  const int threads = cfg.threads == 64 || cfg.threads == 128 ? cfg.threads : 256;
   int64_t blocks = (n + threads - 1) / threads;
-  const int64_t cap = (int64_t)kNumSMs * 32;
+  const int64_t cap = (int64_t)kNumSMs * (cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 32);
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   k_pairs<R, M><<<(unsigned)blocks, threads, 0, s>>>(n, a, b, ld, me, p, q, dist, flags);
@@ -106,31 +107,45 @@ static cudaError_t launch_one(cudaStream_t s, int64_t n, const double *a, const 
 
 template <class R>
 static cudaError_t launch_prec(int method, cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld,
-                               double me, double *p, double *q, double *dist, uint8_t *flags) {
+                               double me, double *p, double *q, double *dist, uint8_t *flags, PairLaunch cfg) {
   switch (method) {
-    case M_BF: return launch_one<R, M_BF>(s, n, a, b, ld, me, p, q, dist, flags);
-    case M_PENALTY: return launch_one<R, M_PENALTY>(s, n, a, b, ld, me, p, q, dist, flags);
-    case M_PENALTY_ITER: return launch_one<R, M_PENALTY_ITER>(s, n, a, b, ld, me, p, q, dist, flags);
-    case M_GJK: return launch_one<R, M_GJK>(s, n, a, b, ld, me, p, q, dist, flags);
-    case M_HYBRID_PAIR: return launch_one<R, M_HYBRID_PAIR>(s, n, a, b, ld, me, p, q, dist, flags);
+    case M_BF: return launch_one<R, M_BF>(s, n, a, b, ld, me, p, q, dist, flags, cfg);
+    case M_PENALTY: return launch_one<R, M_PENALTY>(s, n, a, b, ld, me, p, q, dist, flags, cfg);
+    case M_PENALTY_ITER: return launch_one<R, M_PENALTY_ITER>(s, n, a, b, ld, me, p, q, dist, flags, cfg);
+    case M_GJK: return launch_one<R, M_GJK>(s, n, a, b, ld, me, p, q, dist, flags, cfg);
+    case M_HYBRID_PAIR: return launch_one<R, M_HYBRID_PAIR>(s, n, a, b, ld, me, p, q, dist, flags, cfg);
     default: return cudaErrorInvalidValue;
   }
 }
 
+template <int W>
+static cudaError_t launch_cert(cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld, double *p,
+                               double *q, double *dist, uint8_t *flags, PairLaunch cfg) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_cert<W>, 32 * W, 0);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = (n + 32 * W - 1) / (32 * W);
+  const int64_t per = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 8;
+  const int64_t cap = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1) * per;
+  if (blocks > cap) blocks = cap;
+  k_pairs_cert<W><<<(unsigned)(blocks > 0 ? blocks : 1), 32 * W, 0, s>>>(n, a, b, ld, p, q, dist, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
+                             int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags,
+                             PairLaunch cfg) {
+  if (method == M_BF_CERT) {
+    if (cfg.threads == 64) return launch_cert<2>(s, n, a, b, ld, p, q, dist, flags, cfg);
+    return launch_cert<4>(s, n, a, b, ld, p, q, dist, flags, cfg);
+  }
+  if (precision == 0) return launch_prec<xf64>(method, s, n, a, b, ld, max_error, p, q, dist, flags, cfg);
+  return launch_prec<float>(method, s, n, a, b, ld, max_error, p, q, dist, flags, cfg);
+}
+
 cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
                          int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags) {
-  if (method == M_BF_CERT) {
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_cert, 128, 0);
-    if (e != cudaSuccess) return e;
-    int64_t blocks = (n + 127) / 128;
-    const int64_t cap = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1) * 8;
-    if (blocks > cap) blocks = cap;
-    k_pairs_cert<<<(unsigned)(blocks > 0 ? blocks : 1), 128, 0, s>>>(n, a, b, ld, p, q, dist, flags);
-    return cudaGetLastError();
-  }
-  if (precision == 0) return launch_prec<xf64>(method, s, n, a, b, ld, max_error, p, q, dist, flags);
-  return launch_prec<float>(method, s, n, a, b, ld, max_error, p, q, dist, flags);
+  return launch_pairs_cfg(method, precision, s, n, a, b, ld, max_error, p, q, dist, flags, default_pair_launch(method));
 }
 
 }  // namespace delta

@@ -109,3 +109,25 @@ def pairs_host(ctx: Context, method, a: np.ndarray, b: np.ndarray, out=None, pre
     check(lib().delta_pairs_run_host(ctx.handle, _method(method), int(precision), n, ptr(a), ptr(b), n,
                                      float(max_error), ptr(p), ptr(q), ptr(d), ptr(fl)))
     return p, q, d, fl
+
+
+def autotune(ctx: Context, method, a, b, precision=F64, max_error=0.0, out=None):
+    """Times the candidate launch shapes of `method` on CUDA tensors a, b (9, n) and keeps
+    the fastest on `ctx`.  Returns {"threads", "blocks_per_sm", "ms"}."""
+    import torch
+
+    n = a.shape[1]
+    if out is None:
+        out = (torch.empty((3, n), dtype=torch.float64, device=a.device),
+               torch.empty((3, n), dtype=torch.float64, device=a.device),
+               torch.empty(n, dtype=torch.float64, device=a.device), torch.empty(n, dtype=torch.uint8, device=a.device))
+    p, q, d, fl = out
+    t = C.c_int32(0); bps = C.c_int32(0); ms = C.c_float(0)
+    check(lib().delta_autotune_pairs(ctx.handle, _method(method), int(precision), n, a.data_ptr(), b.data_ptr(), n,
+                                     float(max_error), p.data_ptr(), q.data_ptr(), d.data_ptr(), fl.data_ptr(),
+                                     C.byref(t), C.byref(bps), C.byref(ms)))
+    return {"threads": t.value, "blocks_per_sm": bps.value, "ms": ms.value}
+
+
+def set_launch(ctx: Context, method, precision, threads: int, blocks_per_sm: int):
+    check(lib().delta_set_pair_launch(ctx.handle, _method(method), int(precision), int(threads), int(blocks_per_sm)))

@@ -97,6 +97,23 @@ delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int
                                   const double *b, int64_t ld, double max_error, double *p, double *q,
                                   double *dist, uint8_t *flags);
 
+/* Launch shape of the pair kernel of (method, precision) on this context: threads per
+ * block (64, 128 or 256; the certified kernel takes 64 or 128) and the grid cap in
+ * blocks per SM.  No counterpart in the reference (its SIMD width and OpenMP schedule are
+ * compile-time, bf.cpp:93-102). */
+delta_status delta_set_pair_launch(delta_ctx *ctx, int method, int precision, int32_t threads,
+                                   int32_t blocks_per_sm);
+
+/* Autotuner: runs the pair kernel of (method, precision) over the given pairs (device
+ * buffers, as delta_pairs_run) with each candidate launch shape, times them with CUDA
+ * events, and keeps the fastest for this context.  Writes the choice and its time per
+ * launch.  Synchronises.  (The reference's counterpart is the Peano grain-size oracle,
+ * multiscale/sharedmemoryoracles.) */
+delta_status delta_autotune_pairs(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
+                                  const double *b, int64_t ld, double max_error, double *p, double *q,
+                                  double *dist, uint8_t *flags, int32_t *threads_out, int32_t *blocks_per_sm_out,
+                                  float *ms_out);
+
 /* No counterpart in the reference.  delta_pairs_run_host for callers that must not let
  * the library allocate device memory (a host whose own pool owns the GPU memory, work
  * recorded by stream capture, allocation-free loops).  Inputs and outputs are staged in

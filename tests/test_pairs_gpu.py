@@ -129,3 +129,20 @@ def test_empty_and_invalid_arguments(ctx):
         check(lib().delta_pairs_run(ctx.handle, 99, 0, 4, None, None, 4, 0.0, None, None, None, None))
     with pytest.raises(DeltaError, match="INVALID"):
         check(lib().delta_pairs_run(ctx.handle, 0, 0, 8, None, None, 4, 0.0, None, None, None, None))
+
+
+def test_autotuned_launch_keeps_results(ctx, oracle, workload):
+    """The autotuner picks a launch shape; results stay bit-exact with every shape."""
+    from delta_b200.narrowphase import autotune, set_launch
+
+    a, b = workload
+    for m in (0, 5):
+        cfg = autotune(ctx, m, _dev(a), _dev(b))
+        assert cfg["threads"] in (64, 128, 256) and cfg["blocks_per_sm"] >= 1 and cfg["ms"] > 0
+        gp, gq, gd, _ = _run(ctx, m, a, b)
+        op, oq, od, _ = oracle.pairs(0, a, b)
+        assert not (_differ(gp, op) | _differ(gq, oq) | _differ(gd[None], od[None])).any()
+    set_launch(ctx, 0, 0, 64, 4)
+    gp, _, gd, _ = _run(ctx, 0, a, b)
+    assert not _differ(gd[None], od[None]).any()
+    set_launch(ctx, 0, 0, 256, 32)
