@@ -44,6 +44,19 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_sim_contacts": ([vp, vp, vp], C.c_int),
     "delta_sim_counters": ([vp, vp], C.c_int),
     "delta_sim_destroy": ([vp], C.c_int),
+    "delta_mlp_layout": ([vp], C.c_int),
+    "delta_mlp_infer": ([vp, i64, vp, vp, i64, vp, vp, vp], C.c_int),
+    "delta_mlp_features": ([vp, i64, vp, vp, i64, vp, vp, vp, vp, vp], C.c_int),
+    "delta_gemm_bf16": ([vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int,
+                         C.c_int, C.c_int], C.c_int),
+    "delta_mlp_bias_act": ([vp, i64, C.c_int, vp, vp, vp, C.c_int], C.c_int),
+    "delta_mlp_mse": ([vp, i64, vp, vp, vp, C.c_float, vp, vp], C.c_int),
+    "delta_mlp_act_grad": ([vp, i64, C.c_int, vp, vp, vp], C.c_int),
+    "delta_mlp_colsum": ([vp, i64, C.c_int, vp, vp], C.c_int),
+    "delta_adam": ([vp, i64, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, i64, vp], C.c_int),
+    "delta_to_bf16": ([vp, i64, vp, vp], C.c_int),
+    "delta_penalty_warm": ([vp, i64, vp, vp, i64, vp, f8, vp, vp, vp, vp], C.c_int),
+    "delta_learned_refine": ([vp, i64, vp, vp, i64, vp, i32, f8, vp, vp, vp, vp], C.c_int),
 }
 
 

@@ -1,0 +1,708 @@
+// mlp.cu -- the learned warm start: canonical pair features, a BF16 tensor-core GEMM,
+// the MLP's elementwise steps, Adam, and the penalty solver started from a prediction.
+//
+// The network maps a canonicalised triangle pair (18 coordinates) to the four barycentric
+// weights (x0, x1 of P on A; x2, x3 of Q on B) that penaltySolver iterates on
+// (penalty.cpp:353-356 starts them at 0.33).  Labels come from the FP64 bfSolver result.
+// Matrices are row-major; GEMMs are C = op(A) op(B) in BF16 with FP32 accumulation on
+// the tensor cores (mma.sync m16n8k16).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "internal.h"
+#include "tri_ref.cuh"
+
+namespace delta {
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// canonical features and labels
+// ---------------------------------------------------------------------------------------
+
+// Frame of triangle A: origin at its centroid, x along A1-A0, z along its normal, unit
+// scale = its longest edge.  Features: the 6 vertices in that frame (18 values).  FP64
+// with every operation rounded once (xf64), so the features are reproducible bit for bit;
+// ok is false for a degenerate A.
+__device__ __forceinline__ void canon_pair(const double *__restrict__ a, const double *__restrict__ b, int64_t ld,
+                                           int64_t i, xf64 A[3][3], xf64 B[3][3], float f[18], bool &ok) {
+  for (int v = 0; v < 3; ++v)
+    for (int k = 0; k < 3; ++k) {
+      A[v][k] = xf64(a[(3 * v + k) * ld + i]);
+      B[v][k] = xf64(b[(3 * v + k) * ld + i]);
+    }
+  xf64 c[3], E0[3], E1[3], E2[3], E3[3], nr[3];
+  for (int k = 0; k < 3; ++k) {
+    c[k] = ((A[0][k] + A[1][k]) + A[2][k]) / xf64(3.0);
+    E0[k] = A[1][k] - A[0][k];
+    E1[k] = A[2][k] - A[0][k];
+    E2[k] = A[2][k] - A[1][k];
+    E3[k] = A[0][k] - A[2][k];
+  }
+  nr[0] = E0[1] * E1[2] - E0[2] * E1[1];
+  nr[1] = E0[2] * E1[0] - E0[0] * E1[2];
+  nr[2] = E0[0] * E1[1] - E0[1] * E1[0];
+  const xf64 l0 = sqrt_(dot3(E0, E0)), l1 = sqrt_(dot3(E2, E2)), l2 = sqrt_(dot3(E3, E3));
+  const xf64 ln = sqrt_(dot3(nr, nr));
+  xf64 emax = l0;
+  if (l1 > emax) emax = l1;
+  if (l2 > emax) emax = l2;
+  ok = l0 > xf64(0.0) && ln > xf64(0.0);
+  xf64 e1[3], e3[3], e2[3];
+  for (int k = 0; k < 3; ++k) {
+    e1[k] = ok ? E0[k] / l0 : xf64(0.0);
+    e3[k] = ok ? nr[k] / ln : xf64(0.0);
+  }
+  e2[0] = e3[1] * e1[2] - e3[2] * e1[1];
+  e2[1] = e3[2] * e1[0] - e3[0] * e1[2];
+  e2[2] = e3[0] * e1[1] - e3[1] * e1[0];
+  const xf64 s = ok ? xf64(1.0) / emax : xf64(0.0);
+  for (int v = 0; v < 6; ++v) {
+    const xf64 *X = v < 3 ? A[v] : B[v - 3];
+    const xf64 d[3] = {X[0] - c[0], X[1] - c[1], X[2] - c[2]};
+    f[3 * v + 0] = (float)(s * dot3(d, e1)).v;
+    f[3 * v + 1] = (float)(s * dot3(d, e2)).v;
+    f[3 * v + 2] = (float)(s * dot3(d, e3)).v;
+  }
+}
+
+// Features (rows of 32 BF16, 18 used) and, when P, Q are given, the targets: barycentric
+// weights of P on A and Q on B from the 2x2 normal equations; rows with a degenerate
+// triangle are marked invalid.
+__global__ void k_canon(int64_t n, const double *__restrict__ a, const double *__restrict__ b, int64_t ld,
+                        const double *__restrict__ p, const double *__restrict__ q, __nv_bfloat16 *feat,
+                        float *target, uint8_t *valid) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  xf64 A[3][3], B[3][3];
+  float f[18];
+  bool ok;
+  canon_pair(a, b, ld, i, A, B, f, ok);
+  __nv_bfloat16 *row = feat + 32 * i;
+  for (int k = 0; k < 18; ++k) row[k] = __float2bfloat16(f[k]);
+  for (int k = 18; k < 32; ++k) row[k] = __float2bfloat16(0.f);
+  if (p && q) {
+    // P = A0 + x0 (A1-A0) + x1 (A2-A0); Q = B0 + x2 (B1-B0) + x3 (B2-B0)
+    xf64 x[4];
+    for (int t = 0; t < 2; ++t) {
+      const xf64(*T)[3] = t == 0 ? A : B;
+      const double *src = t == 0 ? p : q;
+      xf64 U[3], V[3], W[3];
+      for (int k = 0; k < 3; ++k) {
+        U[k] = T[1][k] - T[0][k];
+        V[k] = T[2][k] - T[0][k];
+        W[k] = xf64(src[k * ld + i]) - T[0][k];
+      }
+      const xf64 uu = dot3(U, U), uv = dot3(U, V), vv = dot3(V, V), wu = dot3(W, U), wv = dot3(W, V);
+      const xf64 det = uu * vv - uv * uv;
+      if (!(det > xf64(1e-12) * uu * vv)) ok = false;
+      x[2 * t] = (wu * vv - wv * uv) / det;
+      x[2 * t + 1] = (wv * uu - wu * uv) / det;
+    }
+    for (int k = 0; k < 4; ++k) target[4 * i + k] = ok ? (float)x[k].v : 0.f;
+  }
+  if (valid) valid[i] = ok ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// BF16 GEMM on the tensor cores: C[M,N] (+)= op(A)[M,K] op(B)[K,N], FP32 accumulate.
+// A is stored [M,K] (trans_a = 0) or [K,M]; B is stored [K,N] (trans_b = 0) or [N,K].
+// CTA tile 64x64x32, 4 warps of 32x32, split-K over gridDim.z with FP32 atomics.
+// ---------------------------------------------------------------------------------------
+constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
+
+__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bfloat16 *__restrict__ A, int lda,
+                                              int trans_a, const __nv_bfloat16 *__restrict__ B, int ldb, int trans_b,
+                                              float *__restrict__ Cm, int ldc, int accumulate, int k_per_split) {
+  __shared__ __align__(16) __nv_bfloat16 As[BM][BK + PAD];  // [m][k]
+  __shared__ __align__(16) __nv_bfloat16 Bs[BN][BK + PAD];  // [n][k]
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int kb = blockIdx.z * k_per_split, ke = min(K, kb + k_per_split);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int g = lane >> 2, t = lane & 3;
+  float acc[2][4][4] = {};
+  const __nv_bfloat16 zero = __float2bfloat16(0.f);
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    for (int e = tid; e < BM * BK; e += 128) {
+      const int r = e / BK, c = e % BK, m = m0 + r, k = k0 + c;
+      __nv_bfloat16 v = zero;
+      if (m < M && k < ke) v = trans_a ? A[(int64_t)k * lda + m] : A[(int64_t)m * lda + k];
+      As[r][c] = v;
+    }
+    for (int e = tid; e < BN * BK; e += 128) {
+      const int r = e / BK, c = e % BK, nn = n0 + r, k = k0 + c;
+      __nv_bfloat16 v = zero;
+      if (nn < N && k < ke) v = trans_b ? B[(int64_t)nn * ldb + k] : B[(int64_t)k * ldb + nn];
+      Bs[r][c] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+      uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        const int r = wm + mi * 16 + g;
+        af[mi][0] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * t]);
+        af[mi][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * t]);
+        af[mi][2] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * t + 8]);
+        af[mi][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int cidx = wn + ni * 8 + g;
+        bfr[ni][0] = *reinterpret_cast<const uint32_t *>(&Bs[cidx][kk + 2 * t]);
+        bfr[ni][1] = *reinterpret_cast<const uint32_t *>(&Bs[cidx][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], af[mi], bfr[ni]);
+    }
+    __syncthreads();
+  }
+  const bool atomic = gridDim.z > 1 || accumulate;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const int m = m0 + wm + mi * 16 + g + (h >= 2 ? 8 : 0);
+        const int nn = n0 + wn + ni * 8 + 2 * t + (h & 1);
+        if (m < M && nn < N) {
+          float *dst = Cm + (int64_t)m * ldc + nn;
+          if (atomic) atomicAdd(dst, acc[mi][ni][h]);
+          else *dst = acc[mi][ni][h];
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------------------
+// elementwise steps
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ float gelu(float x) {
+  const float k = 0.7978845608028654f;  // sqrt(2/pi), tanh form of GELU
+  return 0.5f * x * (1.f + tanhf(k * (x + 0.044715f * x * x * x)));
+}
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float k = 0.7978845608028654f;
+  const float u = k * (x + 0.044715f * x * x * x);
+  const float th = tanhf(u);
+  return 0.5f * (1.f + th) + 0.5f * x * (1.f - th * th) * k * (1.f + 3.f * 0.044715f * x * x);
+}
+
+// Z[M,N] += bias; H = bf16(gelu(Z)) (or bf16(Z) when act == 0); Z keeps the pre-activation.
+__global__ void k_bias_act(int64_t M, int N, float *Z, const float *bias, __nv_bfloat16 *H, int act) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M * N) return;
+  const float z = Z[e] + bias[e % N];
+  Z[e] = z;
+  if (H) H[e] = __float2bfloat16(act ? gelu(z) : z);
+}
+
+// MSE over valid rows: dY = 2 (Y - T) / n_valid (bf16), loss accumulated into *loss.
+__global__ void k_mse(int64_t M, const float *Y, const float *T, const uint8_t *valid, float inv_n,
+                      __nv_bfloat16 *dY, float *loss) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.f;
+  if (e < M * 4) {
+    const bool v = valid[e / 4] != 0;
+    const float d = v ? Y[e] - T[e] : 0.f;
+    dY[e] = __float2bfloat16(2.f * d * inv_n);
+    l = d * d * inv_n;
+  }
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+  if ((threadIdx.x & 31) == 0 && l != 0.f) atomicAdd(loss, l);
+}
+
+// dZ = bf16(dH * gelu'(Z))
+__global__ void k_act_grad(int64_t M, int N, const float *dH, const float *Z, __nv_bfloat16 *dZ) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M * N) return;
+  dZ[e] = __float2bfloat16(dH[e] * gelu_grad(Z[e]));
+}
+
+// db[n] += sum over rows of dZ[:, n]
+__global__ void k_colsum(int64_t M, int N, const __nv_bfloat16 *dZ, float *db) {
+  const int n = blockIdx.x;
+  float s = 0.f;
+  for (int64_t m = threadIdx.x + (int64_t)blockIdx.y * blockDim.x; m < M; m += (int64_t)blockDim.x * gridDim.y)
+    s += __bfloat162float(dZ[m * N + n]);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ float part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+    atomicAdd(&db[n], t);
+  }
+}
+
+// Adam (Kingma & Ba 2015) on FP32 master weights; refreshes the BF16 copy.
+__global__ void k_adam(int64_t n, float *w, const float *g, float *m, float *v, float lr, float b1, float b2,
+                       float eps, float c1, float c2, __nv_bfloat16 *wb) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16(wi);
+}
+
+__global__ void k_f32_to_bf16(int64_t n, const float *x, __nv_bfloat16 *y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = __float2bfloat16(x[i]);
+}
+
+// ---------------------------------------------------------------------------------------
+// fused inference: features -> 4 layers -> x0, one kernel.  Weights stay in shared memory
+// for the CTA's lifetime; each warp owns 16 pairs and keeps its activations in its own
+// shared rows, so layers need no block barrier.  The MMAs run in the same order as
+// k_gemm's, so the output equals the layer-by-layer path bit for bit.
+// ---------------------------------------------------------------------------------------
+constexpr int kIn = 32, kHid = 128, kOut = 4;
+constexpr int64_t kOffW1 = 0, kOffB1 = kOffW1 + kHid * kIn, kOffW2 = kOffB1 + kHid, kOffB2 = kOffW2 + kHid * kHid,
+                  kOffW3 = kOffB2 + kHid, kOffB3 = kOffW3 + kHid * kHid, kOffW4 = kOffB3 + kHid,
+                  kOffB4 = kOffW4 + kOut * kHid, kNumParams = (kOffB4 + kOut + 7) / 8 * 8;
+constexpr int kIP = kIn + 8, kHP = kHid + 8;  // padded row pitches (bf16): conflict-free fragments
+constexpr int kInferWarps = 4;
+
+struct InferSmem {
+  __nv_bfloat16 w1[kHid][kIP];
+  __nv_bfloat16 w2[kHid][kHP];
+  __nv_bfloat16 w3[kHid][kHP];
+  __nv_bfloat16 w4[8][kHP];  // rows 4..7 zero
+  float bias[3 * kHid + 8];
+  __nv_bfloat16 h[kInferWarps][16][kHP];
+};
+
+// acc[NT][4] = H[16][16*KS] . W^T for W rows 0..8*NT-1 (row pitch wp), fragments as k_gemm.
+template <int KS, int NT>
+__device__ __forceinline__ void warp_mma_rows(const __nv_bfloat16 (*H)[kHP], const __nv_bfloat16 *W, int wp,
+                                              float acc[NT][4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks) {
+    const int kk = 16 * ks;
+    uint32_t af[4];
+    af[0] = *reinterpret_cast<const uint32_t *>(&H[g][kk + 2 * t]);
+    af[1] = *reinterpret_cast<const uint32_t *>(&H[g + 8][kk + 2 * t]);
+    af[2] = *reinterpret_cast<const uint32_t *>(&H[g][kk + 2 * t + 8]);
+    af[3] = *reinterpret_cast<const uint32_t *>(&H[g + 8][kk + 2 * t + 8]);
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      uint32_t bf[2];
+      const __nv_bfloat16 *wr = W + (8 * nt + g) * wp + kk + 2 * t;
+      bf[0] = *reinterpret_cast<const uint32_t *>(wr);
+      bf[1] = *reinterpret_cast<const uint32_t *>(wr + 8);
+      mma_bf16(acc[nt], af, bf);
+    }
+  }
+}
+
+// H[16][128] = bf16(GELU(acc + bias)) in place (after every lane has read H).
+__device__ __forceinline__ void warp_store_gelu(__nv_bfloat16 (*H)[kHP], const float acc[16][4], const float *bias) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  __syncwarp();
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    const int col = 8 * nt + 2 * t;
+    const float b0 = bias[col], b1 = bias[col + 1];
+    *reinterpret_cast<__nv_bfloat162 *>(&H[g][col]) =
+        __halves2bfloat162(__float2bfloat16(gelu(acc[nt][0] + b0)), __float2bfloat16(gelu(acc[nt][1] + b1)));
+    *reinterpret_cast<__nv_bfloat162 *>(&H[g + 8][col]) =
+        __halves2bfloat162(__float2bfloat16(gelu(acc[nt][2] + b0)), __float2bfloat16(gelu(acc[nt][3] + b1)));
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(32 * kInferWarps, 2)
+    k_mlp_infer(int64_t n, const double *__restrict__ a, const double *__restrict__ b, int64_t ld,
+                const float *__restrict__ params, const __nv_bfloat16 *__restrict__ wb, float *__restrict__ x0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  InferSmem &sm = *reinterpret_cast<InferSmem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // weights (BF16) and biases (FP32) into shared memory, once per CTA
+  for (int e = tid; e < kHid * (kIn / 2); e += blockDim.x) {
+    const int r = e / (kIn / 2), c = 2 * (e % (kIn / 2));
+    *reinterpret_cast<uint32_t *>(&sm.w1[r][c]) = *reinterpret_cast<const uint32_t *>(wb + kOffW1 + r * kIn + c);
+  }
+  for (int e = tid; e < kHid * (kHid / 2); e += blockDim.x) {
+    const int r = e / (kHid / 2), c = 2 * (e % (kHid / 2));
+    *reinterpret_cast<uint32_t *>(&sm.w2[r][c]) = *reinterpret_cast<const uint32_t *>(wb + kOffW2 + r * kHid + c);
+    *reinterpret_cast<uint32_t *>(&sm.w3[r][c]) = *reinterpret_cast<const uint32_t *>(wb + kOffW3 + r * kHid + c);
+  }
+  for (int e = tid; e < 8 * (kHid / 2); e += blockDim.x) {
+    const int r = e / (kHid / 2), c = 2 * (e % (kHid / 2));
+    *reinterpret_cast<uint32_t *>(&sm.w4[r][c]) =
+        r < kOut ? *reinterpret_cast<const uint32_t *>(wb + kOffW4 + r * kHid + c) : 0u;
+  }
+  for (int e = tid; e < kHid; e += blockDim.x) {
+    sm.bias[e] = params[kOffB1 + e];
+    sm.bias[kHid + e] = params[kOffB2 + e];
+    sm.bias[2 * kHid + e] = params[kOffB3 + e];
+  }
+  if (tid < 8) sm.bias[3 * kHid + tid] = tid < kOut ? params[kOffB4 + tid] : 0.f;
+  __syncthreads();
+
+  __nv_bfloat16(*H)[kHP] = sm.h[warp];
+  const int64_t tiles = (n + 15) / 16;
+  for (int64_t tile = (int64_t)blockIdx.x * kInferWarps + warp; tile < tiles;
+       tile += (int64_t)gridDim.x * kInferWarps) {
+    const int64_t row0 = tile * 16;
+    if (lane < 16) {
+      const int64_t i = row0 + lane;
+      float f[18];
+      if (i < n) {
+        xf64 A[3][3], B[3][3];
+        bool ok;
+        canon_pair(a, b, ld, i, A, B, f, ok);
+      } else {
+        for (int k = 0; k < 18; ++k) f[k] = 0.f;
+      }
+      for (int k = 0; k < 18; k += 2)
+        *reinterpret_cast<__nv_bfloat162 *>(&H[lane][k]) =
+            __halves2bfloat162(__float2bfloat16(f[k]), __float2bfloat16(f[k + 1]));
+      for (int k = 18; k < kIn; k += 2)
+        *reinterpret_cast<__nv_bfloat162 *>(&H[lane][k]) = __halves2bfloat162(__float2bfloat16(0.f), __float2bfloat16(0.f));
+    }
+    __syncwarp();
+    float acc[16][4];
+    warp_mma_rows<kIn / 16, 16>(H, &sm.w1[0][0], kIP, acc);
+    warp_store_gelu(H, acc, sm.bias);
+    warp_mma_rows<kHid / 16, 16>(H, &sm.w2[0][0], kHP, acc);
+    warp_store_gelu(H, acc, sm.bias + kHid);
+    warp_mma_rows<kHid / 16, 16>(H, &sm.w3[0][0], kHP, acc);
+    warp_store_gelu(H, acc, sm.bias + 2 * kHid);
+    float out[1][4];
+    warp_mma_rows<kHid / 16, 1>(H, &sm.w4[0][0], kHP, out);
+    const int g = lane >> 2, t = lane & 3;
+    if (t < 2) {
+      const float b0 = sm.bias[3 * kHid + 2 * t], b1 = sm.bias[3 * kHid + 2 * t + 1];
+      if (row0 + g < n)
+        *reinterpret_cast<float2 *>(x0 + 4 * (row0 + g) + 2 * t) = make_float2(out[0][0] + b0, out[0][1] + b1);
+      if (row0 + g + 8 < n)
+        *reinterpret_cast<float2 *>(x0 + 4 * (row0 + g + 8) + 2 * t) = make_float2(out[0][2] + b0, out[0][3] + b1);
+    }
+    __syncwarp();
+  }
+}
+
+// penaltySolver (penalty.cpp:434-582, adaptive, FP64 reference arithmetic) started from
+// x0 (4 floats per pair) instead of 0.33; iterations written to iters.
+__global__ void k_penalty_warm(int64_t n, const double *a, const double *b, int64_t ld, const float *x0,
+                               double max_error, double *p, double *q, double *dist, uint8_t *iters) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  xf64 A[3][3], B[3][3], pq[6];
+  for (int v = 0; v < 3; ++v)
+    for (int k = 0; k < 3; ++k) {
+      A[v][k] = xf64(a[(3 * v + k) * ld + i]);
+      B[v][k] = xf64(b[(3 * v + k) * ld + i]);
+    }
+  xf64 start[4];
+  for (int k = 0; k < 4; ++k) start[k] = x0 ? xf64((double)x0[4 * i + k]) : xf64(0.33);
+  int it = 16;  // 16: did not meet the tolerance within MaxNumberOfNewtonIterations
+  penalty_ref_from(A, B, xf64(max_error), true, pq, it, start);
+  for (int k = 0; k < 3; ++k) {
+    p[k * ld + i] = pq[k].v;
+    q[k * ld + i] = pq[3 + k].v;
+  }
+  dist[i] = pq_distance(pq).v;
+  iters[i] = (uint8_t)it;
+}
+
+// Closest point of triangle (V0, V0+E0, V0+E1) to X: barycentric (s, t) by Eberly's region
+// classification (FP32; any feasible answer is acceptable here, the certificate decides).
+__device__ __forceinline__ void closest_on_tri(const float *V0, const float *E0, const float *E1, const float *X,
+                                               float &s, float &t) {
+  float D[3];
+  for (int k = 0; k < 3; ++k) D[k] = V0[k] - X[k];
+  const float a = dot3(E0, E0), b = dot3(E0, E1), c = dot3(E1, E1), d = dot3(E0, D), e = dot3(E1, D);
+  const float det = fmaxf(a * c - b * b, 1e-30f);
+  s = b * e - c * d;
+  t = b * d - a * e;
+  if (s + t <= det) {
+    if (s < 0.f) {
+      if (t < 0.f) {
+        if (d < 0.f) { t = 0.f; s = fminf(fmaxf(-d / a, 0.f), 1.f); }
+        else { s = 0.f; t = fminf(fmaxf(-e / c, 0.f), 1.f); }
+      } else { s = 0.f; t = fminf(fmaxf(-e / c, 0.f), 1.f); }
+    } else if (t < 0.f) { t = 0.f; s = fminf(fmaxf(-d / a, 0.f), 1.f); }
+    else { s /= det; t /= det; }
+  } else {
+    if (s < 0.f) {
+      const float tmp0 = b + d, tmp1 = c + e;
+      if (tmp1 > tmp0) { s = fminf((tmp1 - tmp0) / fmaxf(a - 2.f * b + c, 1e-30f), 1.f); t = 1.f - s; }
+      else { s = 0.f; t = fminf(fmaxf(-e / c, 0.f), 1.f); }
+    } else if (t < 0.f) {
+      const float tmp0 = b + e, tmp1 = a + d;
+      if (tmp1 > tmp0) { t = fminf((tmp1 - tmp0) / fmaxf(a - 2.f * b + c, 1e-30f), 1.f); s = 1.f - t; }
+      else { t = 0.f; s = fminf(fmaxf(-d / a, 0.f), 1.f); }
+    } else {
+      const float numer = c + e - b - d;
+      s = numer <= 0.f ? 0.f : fminf(numer / fmaxf(a - 2.f * b + c, 1e-30f), 1.f);
+      t = 1.f - s;
+    }
+  }
+}
+
+// Learned hybrid solver for one pair.  From the warm start x0 (barycentric weights of P
+// on A and Q on B; centroids when x0 is null), `sweeps` FP32 alternating projections
+// (Q <- closest point of B to P, P <- closest point of A to Q) locate the closest points
+// roughly.  Three bfSolver features are read off them: B's vertex nearest Q against face
+// A, A's vertex nearest P against face B, and the edge pair nearest (P, Q).  They are
+// evaluated in FP64 with the reference arithmetic (bf.cpp:586-697, 920-1090) and chosen
+// between by bfSolver's rule (bf.cpp:1102), so an identified feature gives bfSolver's
+// points bit for bit.  FP64 certificate: with r = P - Q, every plane normal to r bounds
+// the distance below by min_i r.A_i/|r| - max_j r.B_j/|r|; the result is certified when
+// |r| minus that bound (plus a rounding slack) is at most rel_tol |r|.  Intersecting
+// triangles have no separating plane and are never certified.
+__global__ void k_learned_refine(int64_t n, const double *a, const double *b, int64_t ld, const float *x0,
+                                 int sweeps, double rel_tol, double *p, double *q, double *dist, uint8_t *flags) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  xf64 A[3][3], B[3][3];
+  double scale = 0.0;
+  for (int v = 0; v < 3; ++v)
+    for (int k = 0; k < 3; ++k) {
+      A[v][k] = xf64(a[(3 * v + k) * ld + i]);
+      B[v][k] = xf64(b[(3 * v + k) * ld + i]);
+      scale = fmax(scale, fmax(fabs(A[v][k].v), fabs(B[v][k].v)));
+    }
+  float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
+  if (x0) {
+    const float4 x = reinterpret_cast<const float4 *>(x0)[i];
+    // project the prediction into the parameter triangles
+    s = fmaxf(x.x, 0.f); t = fmaxf(x.y, 0.f); u = fmaxf(x.z, 0.f); w = fmaxf(x.w, 0.f);
+    const float st = s + t, uw = u + w;
+    if (st > 1.f) { s /= st; t /= st; }
+    if (uw > 1.f) { u /= uw; w /= uw; }
+  }
+  if (sweeps > 0) {
+    float A0[3], EA0[3], EA1[3], B0[3], EB0[3], EB1[3];
+    for (int k = 0; k < 3; ++k) {
+      A0[k] = 0.f;
+      EA0[k] = (float)(A[1][k].v - A[0][k].v);
+      EA1[k] = (float)(A[2][k].v - A[0][k].v);
+      B0[k] = (float)(B[0][k].v - A[0][k].v);
+      EB0[k] = (float)(B[1][k].v - B[0][k].v);
+      EB1[k] = (float)(B[2][k].v - B[0][k].v);
+    }
+    for (int it = 0; it < sweeps; ++it) {
+      float P[3];
+      for (int k = 0; k < 3; ++k) P[k] = A0[k] + s * EA0[k] + t * EA1[k];
+      closest_on_tri(B0, EB0, EB1, P, u, w);
+      float Q[3];
+      for (int k = 0; k < 3; ++k) Q[k] = B0[k] + u * EB0[k] + w * EB1[k];
+      closest_on_tri(A0, EA0, EA1, Q, s, t);
+    }
+  }
+  // features read off the barycentric weights lA = (1-s-t, s, t), lB = (1-u-w, u, w)
+  const float lA[3] = {1.f - s - t, s, t}, lB[3] = {1.f - u - w, u, w};
+  int iA = 0, jB = 0, kA = 0, kB = 0;
+  for (int v = 1; v < 3; ++v) {
+    if (lA[v] > lA[iA]) iA = v;
+    if (lB[v] > lB[jB]) jB = v;
+    if (lA[v] < lA[kA]) kA = v;
+    if (lB[v] < lB[kB]) kB = v;
+  }
+  // bf's vertex-face features: 9 + j is B's vertex j on face A, 12 + j A's vertex j on
+  // face B; edge-edge 3 ea + eb joins vertices ea, ea+1 (the edge opposite vertex ea+2).
+  const int fB = 9 + jB, fA = 12 + iA, fE = 3 * ((kA + 1) % 3) + (kB + 1) % 3;
+  xf64 s1, t1, s2, t2, sc, tc;
+  const xf64 d1 = feature_ref(A, B, fB, s1, t1);
+  const xf64 d2 = feature_ref(A, B, fA, s2, t2);
+  const xf64 de = feature_ref(A, B, fE, sc, tc);
+  xf64 pq[6];
+  // first minimum in feature order within the vertex-face family; the edge pair only
+  // when strictly closer
+  const bool second = d2 < d1;
+  const xf64 dpt = second ? d2 : d1;
+  if (dpt > de) seg_seg_points(A, B, fE, sc, tc, pq);
+  else if (second) pt_tri_points(A, B, fA - 9, s2, t2, pq);
+  else pt_tri_points(A, B, fB - 9, s1, t1, pq);
+  const double d = pq_distance(pq).v;
+  bool ok = false;
+  if (d > 0) {
+    const double r[3] = {pq[0].v - pq[3].v, pq[1].v - pq[4].v, pq[2].v - pq[5].v};
+    double amin = 1e300, bmax = -1e300;
+    for (int v = 0; v < 3; ++v) {
+      amin = fmin(amin, (A[v][0].v * r[0] + A[v][1].v * r[1] + A[v][2].v * r[2]) / d);
+      bmax = fmax(bmax, (B[v][0].v * r[0] + B[v][1].v * r[1] + B[v][2].v * r[2]) / d);
+    }
+    ok = d - (amin - bmax) + 1e-14 * scale <= rel_tol * d;
+  }
+  for (int k = 0; k < 3; ++k) {
+    p[k * ld + i] = pq[k].v;
+    q[k * ld + i] = pq[3 + k].v;
+  }
+  dist[i] = d;
+  flags[i] = ok ? 1 : 0;
+}
+
+inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
+
+}  // namespace
+
+}  // namespace delta
+
+using namespace delta;
+
+extern "C" {
+
+delta_status delta_mlp_features(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                const double *p, const double *q, void *features_bf16, float *targets,
+                                uint8_t *valid) {
+  if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !features_bf16)) || ((p == nullptr) != (q == nullptr)) ||
+      (p && !targets))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_features: bad argument");
+  if (n == 0) return DELTA_OK;
+  k_canon<<<nblk(n), 256, 0, ctx->stream>>>(n, a, b, ld, p, q, (__nv_bfloat16 *)features_bf16, targets, valid);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_mlp_features");
+}
+
+delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A, int lda, int trans_a,
+                             const void *B, int ldb, int trans_b, float *C, int ldc, int accumulate, int split_k) {
+  if (!ctx || M < 0 || N < 0 || K < 0 || !A || !B || !C || split_k < 1)
+    return set_error(DELTA_ERR_INVALID, "delta_gemm_bf16: bad argument");
+  if (M == 0 || N == 0) return DELTA_OK;
+  cudaError_t e = cudaSuccess;
+  if (!accumulate && (split_k > 1)) e = cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * ldc, ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "gemm memset");
+  int per = (K + split_k - 1) / split_k;
+  per = (per + BK - 1) / BK * BK;
+  const int splits = per > 0 ? (K + per - 1) / per : 1;
+  dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, splits > 0 ? splits : 1);
+  k_gemm<<<grid, 128, 0, ctx->stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, trans_a, (const __nv_bfloat16 *)B,
+                                        ldb, trans_b, C, ldc, accumulate, per > 0 ? per : BK);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_gemm_bf16");
+}
+
+delta_status delta_mlp_bias_act(delta_ctx *ctx, int64_t M, int N, float *Z, const float *bias, void *H_bf16,
+                                int gelu_on) {
+  if (!ctx || !Z || !bias || M < 0 || N <= 0) return set_error(DELTA_ERR_INVALID, "delta_mlp_bias_act");
+  if (M == 0) return DELTA_OK;
+  k_bias_act<<<nblk(M * N), 256, 0, ctx->stream>>>(M, N, Z, bias, (__nv_bfloat16 *)H_bf16, gelu_on);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_mlp_bias_act");
+}
+
+delta_status delta_mlp_mse(delta_ctx *ctx, int64_t M, const float *Y, const float *T, const uint8_t *valid,
+                           float inv_n, void *dY_bf16, float *loss) {
+  if (!ctx || !Y || !T || !valid || !dY_bf16 || !loss) return set_error(DELTA_ERR_INVALID, "delta_mlp_mse");
+  if (M == 0) return DELTA_OK;
+  k_mse<<<nblk(M * 4), 256, 0, ctx->stream>>>(M, Y, T, valid, inv_n, (__nv_bfloat16 *)dY_bf16, loss);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_mlp_mse");
+}
+
+delta_status delta_mlp_act_grad(delta_ctx *ctx, int64_t M, int N, const float *dH, const float *Z, void *dZ_bf16) {
+  if (!ctx || !dH || !Z || !dZ_bf16) return set_error(DELTA_ERR_INVALID, "delta_mlp_act_grad");
+  if (M == 0) return DELTA_OK;
+  k_act_grad<<<nblk(M * N), 256, 0, ctx->stream>>>(M, N, dH, Z, (__nv_bfloat16 *)dZ_bf16);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_mlp_act_grad");
+}
+
+delta_status delta_mlp_colsum(delta_ctx *ctx, int64_t M, int N, const void *dZ_bf16, float *db) {
+  if (!ctx || !dZ_bf16 || !db) return set_error(DELTA_ERR_INVALID, "delta_mlp_colsum");
+  if (M == 0) return DELTA_OK;
+  const int ys = (int)std::min<int64_t>(64, (M + 255) / 256);
+  k_colsum<<<dim3(N, ys > 0 ? ys : 1), 256, 0, ctx->stream>>>(M, N, (const __nv_bfloat16 *)dZ_bf16, db);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_mlp_colsum");
+}
+
+delta_status delta_adam(delta_ctx *ctx, int64_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
+                        float b2, float eps, int64_t step, void *w_bf16) {
+  if (!ctx || !w || !g || !m || !v || step < 1) return set_error(DELTA_ERR_INVALID, "delta_adam");
+  if (n == 0) return DELTA_OK;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<nblk(n), 256, 0, ctx->stream>>>(n, w, g, m, v, lr, b1, b2, eps, c1, c2, (__nv_bfloat16 *)w_bf16);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_adam");
+}
+
+delta_status delta_to_bf16(delta_ctx *ctx, int64_t n, const float *x, void *y_bf16) {
+  if (!ctx || (n > 0 && (!x || !y_bf16))) return set_error(DELTA_ERR_INVALID, "delta_to_bf16");
+  if (n == 0) return DELTA_OK;
+  k_f32_to_bf16<<<nblk(n), 256, 0, ctx->stream>>>(n, x, (__nv_bfloat16 *)y_bf16);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_to_bf16");
+}
+
+delta_status delta_mlp_layout(int64_t offsets[9]) {
+  if (!offsets) return set_error(DELTA_ERR_INVALID, "delta_mlp_layout: null");
+  const int64_t o[9] = {kOffW1, kOffB1, kOffW2, kOffB2, kOffW3, kOffB3, kOffW4, kOffB4, kNumParams};
+  for (int k = 0; k < 9; ++k) offsets[k] = o[k];
+  return DELTA_OK;
+}
+
+delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                             const float *params, const void *params_bf16, float *x0) {
+  if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !params || !params_bf16 || !x0)))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer: bad argument");
+  if ((reinterpret_cast<uintptr_t>(params_bf16) & 3) || (reinterpret_cast<uintptr_t>(x0) & 7))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer: params_bf16 must be 4-byte and x0 8-byte aligned");
+  if (n == 0) return DELTA_OK;
+  static thread_local int configured_device = -1;
+  cudaError_t e = cudaSuccess;
+  if (configured_device != ctx->device) {
+    e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
+    if (e != cudaSuccess) return cuda_error(e, "delta_mlp_infer: shared memory attribute");
+    configured_device = ctx->device;
+  }
+  const int64_t tiles = (n + 15) / 16;
+  const int64_t want = (tiles + kInferWarps - 1) / kInferWarps;
+  const unsigned grid = (unsigned)std::min<int64_t>(want, 2 * kNumSMs);
+  k_mlp_infer<<<grid, 32 * kInferWarps, sizeof(InferSmem), ctx->stream>>>(n, a, b, ld, params,
+                                                                          (const __nv_bfloat16 *)params_bf16, x0);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_mlp_infer");
+}
+
+delta_status delta_penalty_warm(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                const float *x0, double max_error, double *p, double *q, double *dist,
+                                uint8_t *iterations) {
+  if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !p || !q || !dist || !iterations)))
+    return set_error(DELTA_ERR_INVALID, "delta_penalty_warm: bad argument");
+  if (n == 0) return DELTA_OK;
+  k_penalty_warm<<<nblk(n, 128), 128, 0, ctx->stream>>>(n, a, b, ld, x0, max_error, p, q, dist, iterations);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_penalty_warm");
+}
+
+delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                  const float *x0, int32_t sweeps, double rel_tol, double *p, double *q, double *dist,
+                                  uint8_t *certified) {
+  if (!ctx || n < 0 || ld < n || sweeps < 0 || (n > 0 && (!a || !b || !p || !q || !dist || !certified)))
+    return set_error(DELTA_ERR_INVALID, "delta_learned_refine: bad argument");
+  if (reinterpret_cast<uintptr_t>(x0) & 15)
+    return set_error(DELTA_ERR_INVALID, "delta_learned_refine: x0 must be 16-byte aligned");
+  if (n == 0) return DELTA_OK;
+  k_learned_refine<<<nblk(n, 128), 128, 0, ctx->stream>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, certified);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_learned_refine");
+}
+
+}  // extern "C"

@@ -230,8 +230,8 @@ __device__ __forceinline__ void bf_solve_ref(const R A[3][3], const R B[3][3], R
 // the last step) and penalty.cpp:434-582 (adaptive = true: at most 16 iterations,
 // flag = iteration index of the early exit, unchanged otherwise).
 template <class R>
-__device__ __forceinline__ void penalty_ref(const R A[3][3], const R B[3][3], R max_error, bool adaptive, R pq[6],
-                                            int &flag) {
+__device__ __forceinline__ void penalty_ref_from(const R A[3][3], const R B[3][3], R max_error, bool adaptive,
+                                                 R pq[6], int &flag, const R *start) {
   R BA[3], CA[3], ED[3], FD[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -261,7 +261,13 @@ __device__ __forceinline__ void penalty_ref(const R A[3][3], const R B[3][3], R 
   R delta = (h[0] + h[5] + h[10] + h[15]) * R(1E-2);
   const R lambda = sqrt_(R(0.0125) * (h[0] + h[5] + h[10] + h[15]));
   const R r = lambda * R(1E5);
-  R x[4] = {R(0.33), R(0.33), R(0.33), R(0.33)};
+  R x[4] = {R(0.33), R(0.33), R(0.33), R(0.33)};  // initial guess, penalty.cpp:353-356
+  if (start) {
+    x[0] = start[0];
+    x[1] = start[1];
+    x[2] = start[2];
+    x[3] = start[3];
+  }
   const int n_iter = adaptive ? 16 : 4;
   if (!adaptive) flag = 0;
   for (int i = 0; i < n_iter; ++i) {
@@ -317,6 +323,12 @@ __device__ __forceinline__ void penalty_ref(const R A[3][3], const R B[3][3], R 
     pq[k] = A[0][k] + (BA[k] * x[0]) + (CA[k] * x[1]);
     pq[3 + k] = B[0][k] + (ED[k] * x[2]) + (FD[k] * x[3]);
   }
+}
+
+template <class R>
+__device__ __forceinline__ void penalty_ref(const R A[3][3], const R B[3][3], R max_error, bool adaptive, R pq[6],
+                                            int &flag) {
+  penalty_ref_from<R>(A, B, max_error, adaptive, pq, flag, nullptr);
 }
 
 // d = |P_B - P_A| as the drivers compute it (bf.cpp:117).

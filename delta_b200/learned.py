@@ -1,0 +1,270 @@
+"""Learned warm start for the triangle-pair narrowphase.
+
+A small MLP maps a canonicalised triangle pair (triangle A's frame, unit = its longest
+edge: 18 coordinates) to the barycentric weights of the closest points, the four
+parameters penaltySolver iterates on and starts at 0.33 (penalty.cpp:353-356).  It is
+trained on the GPU with the library's own kernels (BF16 tensor-core GEMMs, GELU,
+MSE, Adam in libdelta_b200.so); torch only holds the device memory.  Labels are the
+FP64 bfSolver closest points (bf.cpp:217-1178) of the same pairs.
+
+The learned solver (`learned_pairs`) starts from the prediction, identifies the
+closest features, evaluates them in FP64 with the reference arithmetic, certifies the
+distance with a separating plane, and sends every uncertified pair to DELTA_BF_CERT,
+which is exact; the brute force is both the fallback and the error judge.  There is no
+counterpart of this module in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from ._lib import check, lib
+from .narrowphase import BF, BF_CERT, F64, Context, pairs_device
+
+IN, HIDDEN, OUT, FEATURES = 32, 128, 4, 18
+LAYERS = ((IN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, OUT))  # (fan_in, fan_out)
+
+
+def layout() -> dict:
+    """Flat parameter layout from the library: offsets of W1, b1, ..., W4, b4 and the total."""
+    off = (C.c_int64 * 9)()
+    check(lib().delta_mlp_layout(off))
+    names = ("W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4", "total")
+    return dict(zip(names, [int(x) for x in off]))
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """FP32 initial parameters in the flat layout: U(-1/sqrt(fan_in), 1/sqrt(fan_in)) for
+    weights and biases (fan_in of layer 1 = the 18 used features; its padding columns 0)."""
+    L = layout()
+    rng = np.random.default_rng(seed)
+    w = np.zeros(L["total"], np.float32)
+    for l, (fi, fo) in enumerate(LAYERS, start=1):
+        used = FEATURES if l == 1 else fi
+        bound = 1.0 / math.sqrt(used)
+        W = np.zeros((fo, fi), np.float32)
+        W[:, :used] = rng.uniform(-bound, bound, (fo, used))
+        w[L[f"W{l}"]:L[f"W{l}"] + fo * fi] = W.ravel()
+        w[L[f"b{l}"]:L[f"b{l}"] + fo] = rng.uniform(-bound, bound, fo)
+    return w
+
+
+class WarmStartMLP:
+    """18 -> 128 -> 128 -> 128 -> 4 with GELU, BF16 weights/activations, FP32 master
+    weights and Adam moments, on one context's device."""
+
+    def __init__(self, ctx: Context, seed: int = 0, params: np.ndarray | None = None):
+        import torch
+
+        self.ctx = ctx
+        self.L = layout()
+        self.dev = torch.device("cuda", ctx.device)
+        host = init_params(seed) if params is None else np.asarray(params, np.float32)
+        if host.shape != (self.L["total"],):
+            raise ValueError(f"params must have {self.L['total']} entries")
+        self.params = torch.from_numpy(host.copy()).to(self.dev)
+        self.params_bf16 = torch.empty(self.L["total"], dtype=torch.bfloat16, device=self.dev)
+        self.grads = torch.zeros_like(self.params)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.steps = 0
+        self._ws_rows = 0
+        self._refresh_bf16()
+
+    # -- parameter views ---------------------------------------------------------------
+    def _view(self, t, name, shape):
+        o = self.L[name]
+        return t[o:o + int(np.prod(shape))].view(*shape)
+
+    def weight(self, l, bf16=True):
+        fi, fo = LAYERS[l - 1]
+        return self._view(self.params_bf16 if bf16 else self.params, f"W{l}", (fo, fi))
+
+    def bias(self, l):
+        return self._view(self.params, f"b{l}", (LAYERS[l - 1][1],))
+
+    def grad(self, name):
+        l = int(name[1])
+        fi, fo = LAYERS[l - 1]
+        return self._view(self.grads, name, (fo, fi) if name[0] == "W" else (fo,))
+
+    def _refresh_bf16(self):
+        check(lib().delta_to_bf16(self.ctx.handle, self.L["total"], self.params.data_ptr(),
+                                  self.params_bf16.data_ptr()))
+
+    def state_dict(self) -> dict:
+        return {"params": self.params.cpu().numpy(), "steps": self.steps}
+
+    # -- workspace ---------------------------------------------------------------------
+    def _workspace(self, M):
+        import torch
+
+        if self._ws_rows >= M:
+            return
+        f32 = dict(dtype=torch.float32, device=self.dev)
+        b16 = dict(dtype=torch.bfloat16, device=self.dev)
+        self.Z = [torch.empty((M, HIDDEN), **f32) for _ in range(3)]
+        self.H = [torch.empty((M, HIDDEN), **b16) for _ in range(3)]
+        self.Y = torch.empty((M, OUT), **f32)
+        self.dY = torch.empty((M, OUT), **b16)
+        self.dH = torch.empty((M, HIDDEN), **f32)
+        self.dZ = torch.empty((M, HIDDEN), **b16)
+        self.loss = torch.zeros(1, **f32)
+        self._ws_rows = M
+
+    # -- kernels -----------------------------------------------------------------------
+    def _gemm(self, M, N, K, A, lda, ta, B, ldb, tb, Cm, ldc, acc=0, split=1):
+        check(lib().delta_gemm_bf16(self.ctx.handle, M, N, K, A.data_ptr(), lda, ta, B.data_ptr(), ldb, tb,
+                                    Cm.data_ptr(), ldc, acc, split))
+
+    def forward(self, X):
+        """Layer by layer on X (M, 32) BF16; returns Y (M, 4) FP32 (a workspace view)."""
+        M = X.shape[0]
+        self._workspace(M)
+        h = X
+        for l in range(1, 4):
+            fi = LAYERS[l - 1][0]
+            Z, H = self.Z[l - 1][:M], self.H[l - 1][:M]
+            self._gemm(M, HIDDEN, fi, h, fi, 0, self.weight(l), fi, 1, Z, HIDDEN)
+            check(lib().delta_mlp_bias_act(self.ctx.handle, M, HIDDEN, Z.data_ptr(), self.bias(l).data_ptr(),
+                                           H.data_ptr(), 1))
+            h = H
+        Y = self.Y[:M]
+        self._gemm(M, OUT, HIDDEN, h, HIDDEN, 0, self.weight(4), HIDDEN, 1, Y, OUT)
+        check(lib().delta_mlp_bias_act(self.ctx.handle, M, OUT, Y.data_ptr(), self.bias(4).data_ptr(), None, 0))
+        return Y
+
+    def backward(self, X, T, valid, n_valid: int):
+        """Gradients of the MSE over valid rows into self.grads (after forward(X))."""
+        M = X.shape[0]
+        split = max(1, min(128, M // 1024))
+        self.grads.zero_()
+        self.loss.zero_()
+        h = lib()
+        dY = self.dY[:M]
+        check(h.delta_mlp_mse(self.ctx.handle, M, self.Y[:M].data_ptr(), T.data_ptr(), valid.data_ptr(),
+                              1.0 / max(n_valid, 1), dY.data_ptr(), self.loss.data_ptr()))
+        d, width = dY, OUT
+        for l in range(4, 0, -1):
+            fi, fo = LAYERS[l - 1]
+            prev = X if l == 1 else self.H[l - 2][:M]
+            # dW[fo, fi] = d^T prev ; db = column sums of d
+            self._gemm(fo, fi, M, d, width, 1, prev, fi, 0, self.grad(f"W{l}"), fi, 1, split)
+            check(h.delta_mlp_colsum(self.ctx.handle, M, fo, d.data_ptr(), self.grad(f"b{l}").data_ptr()))
+            if l == 1:
+                break
+            dH = self.dH[:M]
+            self._gemm(M, fi, fo, d, width, 0, self.weight(l), fi, 0, dH, fi)
+            dZ = self.dZ[:M]
+            check(h.delta_mlp_act_grad(self.ctx.handle, M, fi, dH.data_ptr(), self.Z[l - 2][:M].data_ptr(),
+                                       dZ.data_ptr()))
+            d, width = dZ, fi
+
+    def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        self.steps += 1
+        check(lib().delta_adam(self.ctx.handle, self.L["total"], self.params.data_ptr(), self.grads.data_ptr(),
+                               self.m.data_ptr(), self.v.data_ptr(), lr, b1, b2, eps, self.steps,
+                               self.params_bf16.data_ptr()))
+
+    def train_step(self, X, T, valid, n_valid: int, lr=1e-3):
+        self.forward(X)
+        self.backward(X, T, valid, n_valid)
+        self.adam(lr)
+
+    # -- inference ---------------------------------------------------------------------
+    def predict(self, a, b, out=None):
+        """x0 (n, 4) FP32 for pair-list tensors a, b (9, n) on the device: one fused kernel."""
+        import torch
+
+        n = a.shape[1]
+        x0 = out if out is not None else torch.empty((n, OUT), dtype=torch.float32, device=a.device)
+        check(lib().delta_mlp_infer(self.ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0),
+                                    self.params.data_ptr(), self.params_bf16.data_ptr(), x0.data_ptr()))
+        return x0
+
+
+def features(ctx: Context, a, b, p=None, q=None):
+    """(X (n, 32) BF16, T (n, 4) FP32 or None, valid (n,) uint8) for pair-list tensors."""
+    import torch
+
+    n = a.shape[1]
+    X = torch.empty((n, IN), dtype=torch.bfloat16, device=a.device)
+    T = torch.empty((n, OUT), dtype=torch.float32, device=a.device) if p is not None else None
+    valid = torch.empty(n, dtype=torch.uint8, device=a.device)
+    check(lib().delta_mlp_features(ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0),
+                                   None if p is None else p.data_ptr(), None if q is None else q.data_ptr(),
+                                   X.data_ptr(), None if T is None else T.data_ptr(), valid.data_ptr()))
+    return X, T, valid
+
+
+def labelled(ctx: Context, a, b):
+    """Training rows for pair-list tensors a, b: features, bfSolver targets, valid flags."""
+    p, q, _, _ = pairs_device(ctx, BF, a, b, precision=F64, with_flags=False)
+    return features(ctx, a, b, p, q)
+
+
+def train(model: WarmStartMLP, X, T, valid, epochs: int = 1, batch: int = 65536, lr: float = 1e-3,
+          seed: int = 0, log=None) -> list[float]:
+    """Adam over shuffled mini-batches; returns the mean loss of each epoch."""
+    import torch
+
+    n = X.shape[0]
+    gen = torch.Generator(device=X.device)
+    gen.manual_seed(seed)
+    losses = []
+    nb = n // batch
+    if nb == 0:
+        raise ValueError("fewer rows than one batch")
+    for ep in range(epochs):
+        perm = torch.randperm(n, device=X.device, generator=gen)[: nb * batch].view(nb, batch)
+        vb = valid[perm].view(nb, batch)
+        counts = vb.sum(1, dtype=torch.int64).cpu().tolist()
+        total = torch.zeros(1, dtype=torch.float32, device=X.device)
+        for k in range(nb):
+            idx = perm[k]
+            model.train_step(X[idx], T[idx], vb[k].contiguous(), counts[k], lr)
+            total += model.loss
+        losses.append(float(total.item()) / nb)
+        if log:
+            log(f"epoch {ep}: loss {losses[-1]:.6g}")
+    return losses
+
+
+def refine(ctx: Context, a, b, x0=None, sweeps: int = 2, rel_tol: float = 1e-6, out=None):
+    """delta_learned_refine: (p, q, dist, certified) for pair-list tensors a, b."""
+    import torch
+
+    n = a.shape[1]
+    if out is None:
+        p = torch.empty((3, n), dtype=torch.float64, device=a.device)
+        q = torch.empty_like(p)
+        d = torch.empty(n, dtype=torch.float64, device=a.device)
+        cert = torch.empty(n, dtype=torch.uint8, device=a.device)
+    else:
+        p, q, d, cert = out
+    check(lib().delta_learned_refine(ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0),
+                                     None if x0 is None else x0.data_ptr(), int(sweeps), float(rel_tol),
+                                     p.data_ptr(), q.data_ptr(), d.data_ptr(), cert.data_ptr()))
+    return p, q, d, cert
+
+
+def learned_pairs(ctx: Context, model: WarmStartMLP | None, a, b, sweeps: int = 2, rel_tol: float = 1e-6):
+    """The learned hybrid over pair-list tensors a, b (9, n) float64 on the device.
+
+    model None runs the same solver from the centroids (the method without the network).
+    Returns (p, q, dist, certified): certified pairs carry a distance within rel_tol of
+    the exact one; every other pair is solved by DELTA_BF_CERT and equals bfSolver bit
+    for bit.
+    """
+    x0 = model.predict(a, b) if model is not None else None
+    p, q, d, cert = refine(ctx, a, b, x0, sweeps, rel_tol)
+    idx = (cert == 0).nonzero().squeeze(1)
+    if idx.numel():
+        sp, sq, sd, _ = pairs_device(ctx, BF_CERT, a[:, idx].contiguous(), b[:, idx].contiguous(), precision=F64,
+                                     with_flags=False)
+        p[:, idx] = sp
+        q[:, idx] = sq
+        d[idx] = sd
+    return p, q, d, cert

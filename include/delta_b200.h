@@ -260,6 +260,73 @@ delta_status delta_sim_contacts(delta_sim *sim, const delta_contacts *out, int64
 delta_status delta_sim_counters(const delta_sim *sim, int64_t out[4]);
 delta_status delta_sim_destroy(delta_sim *sim);
 
+/* ---- learned warm start ----------------------------------------------------------------
+ * No counterpart in the reference.  A small MLP (18 -> 128 -> 128 -> 128 -> 4, GELU, BF16
+ * weights and activations, FP32 accumulation) maps a canonicalised triangle pair to the
+ * four barycentric weights that penaltySolver iterates on (x0, x1: P = A0 + x0 (A1-A0) +
+ * x1 (A2-A0); x2, x3: Q on B likewise), which the reference starts at 0.33
+ * (penalty.cpp:353-356).  These entry points are the network's training and inference
+ * steps; row-major matrices, BF16 arrays passed as void* (2 bytes per element). */
+
+/* Offsets (in elements) of W1 [128][32], b1, W2 [128][128], b2, W3, b3, W4 [4][128], b4 in
+ * the flat parameter array, and [8] its length.  The FP32 master copy and the BF16 copy
+ * share this layout; W1's columns 18..31 multiply zero features. */
+delta_status delta_mlp_layout(int64_t offsets[9]);
+/* Inference in one kernel: features, the four layers and x0 [n][4] (FP32).  params is the
+ * FP32 array (biases are read from it), params_bf16 the BF16 copy (weights); x0 8-byte
+ * aligned.  Equal bit for bit to delta_mlp_features + delta_gemm_bf16 + delta_mlp_bias_act
+ * layer by layer. */
+delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                             const float *params, const void *params_bf16, float *x0);
+/* Canonical features: triangle A's frame (origin at its centroid, x along A1-A0, z along
+ * its normal, unit = its longest edge), the six vertices in that frame as 18 BF16 values
+ * padded with zeros to rows of 32 (features_bf16 [n][32]).  With p, q (closest points,
+ * pair-list planes) also the targets [n][4] (barycentric weights of p on A and q on B).
+ * valid [n] (optional) is 0 for pairs with a degenerate triangle. */
+delta_status delta_mlp_features(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                const double *p, const double *q, void *features_bf16, float *targets,
+                                uint8_t *valid);
+/* C[M][N] (+)= op(A) op(B): A is [M][K] (trans_a 0) or [K][M]; B is [K][N] (trans_b 0)
+ * or [N][K]; BF16 operands on the tensor cores, FP32 C.  split_k > 1 splits K across
+ * CTAs and accumulates with atomics (C is zeroed first unless accumulate). */
+delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A, int lda, int trans_a,
+                             const void *B, int ldb, int trans_b, float *C, int ldc, int accumulate, int split_k);
+/* Z[M][N] += bias; H_bf16 (optional) = bf16(GELU(Z)) (tanh form) or bf16(Z) when gelu_on is 0. */
+delta_status delta_mlp_bias_act(delta_ctx *ctx, int64_t M, int N, float *Z, const float *bias, void *H_bf16,
+                                int gelu_on);
+/* Mean-squared error over rows with valid != 0: dY_bf16 [M][4] = 2 (Y-T) inv_n, and
+ * *loss += sum (Y-T)^2 inv_n (inv_n = 1 / number of valid rows). */
+delta_status delta_mlp_mse(delta_ctx *ctx, int64_t M, const float *Y, const float *T, const uint8_t *valid,
+                           float inv_n, void *dY_bf16, float *loss);
+/* dZ_bf16 = bf16(dH * GELU'(Z)). */
+delta_status delta_mlp_act_grad(delta_ctx *ctx, int64_t M, int N, const float *dH, const float *Z, void *dZ_bf16);
+/* db[N] += column sums of dZ_bf16 [M][N]. */
+delta_status delta_mlp_colsum(delta_ctx *ctx, int64_t M, int N, const void *dZ_bf16, float *db);
+/* One Adam step (bias-corrected, step >= 1) on FP32 master weights w with moments m, v;
+ * w_bf16 (optional) receives the BF16 copy. */
+delta_status delta_adam(delta_ctx *ctx, int64_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
+                        float b2, float eps, int64_t step, void *w_bf16);
+delta_status delta_to_bf16(delta_ctx *ctx, int64_t n, const float *x, void *y_bf16);
+/* penaltySolver(..., maxError, int& iterations) (penalty.cpp:434-582, FP64 reference
+ * arithmetic) started from x0 [n][4] instead of 0.33 (x0 NULL: 0.33).  iterations [n]
+ * gets the iteration count, 16 when the step-size test never passed. */
+delta_status delta_penalty_warm(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                const float *x0, double max_error, double *p, double *q, double *dist,
+                                uint8_t *iterations);
+/* The learned solver.  From x0 [n][4] (16-byte aligned; NULL: the centroids), `sweeps`
+ * FP32 alternating closest-point projections between the triangles; the closest points
+ * found name three bfSolver features (B's nearest vertex against face A, A's nearest
+ * vertex against face B, the nearest edge pair), which are evaluated in FP64 with the
+ * reference arithmetic and chosen between by bfSolver's rule (bf.cpp:1102): p, q, dist.
+ * Then an FP64 separating-plane certificate: with r = p - q, every plane normal to r
+ * bounds the distance below by min_i r.A_i/|r| - max_j r.B_j/|r|; certified [n] is 1 when
+ * |r| exceeds that bound by at most rel_tol |r|, so dist is within rel_tol of the true
+ * distance.  Intersecting triangles are never certified; uncertified pairs are for
+ * DELTA_BF_CERT. */
+delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                  const float *x0, int32_t sweeps, double rel_tol, double *p, double *q, double *dist,
+                                  uint8_t *certified);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,206 @@
+"""The learned warm start on the GPU: its kernels against the CPU oracle
+(oracle/mlp_oracle.py) and torch's FP32 matmul, training with the library's own
+forward/backward kernels, what the trained network gains over the same solver without
+it, and the learned solver's results against FP64 bfSolver.
+
+Tolerances: BF16 tensor-core GEMM vs torch FP32 matmul of the same BF16 operands:
+relative Frobenius error <= 1e-5.  Forward/backward vs the oracle with the BF16
+roundings mirrored: relative Frobenius error <= 2e-2 per tensor (what remains is FP32
+versus FP64 accumulation and rare one-step BF16 rounding flips that follow from it).
+Learned solver vs FP64 bfSolver: relative distance error <= 1e-6 on every pair.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(x):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def _rel(x, y):
+    x = np.asarray(x, np.float64)
+    y = np.asarray(y, np.float64)
+    return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def pairs():
+    from delta_b200.scenarios import narrowphase_pairs
+
+    a, b, _, _ = narrowphase_pairs(1 << 16, seed=77)
+    return a, b
+
+
+def test_layout_matches_oracle():
+    from delta_b200.learned import layout
+
+    from oracle import mlp_oracle as mo
+
+    assert layout() == mo.layout()
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("split,acc", [(1, 0), (4, 0), (1, 1), (3, 1)])
+def test_gemm_bf16_vs_torch(ctx, ta, tb, split, acc):
+    import torch
+
+    from delta_b200._lib import check, lib
+
+    g = torch.Generator(device="cuda").manual_seed(ta * 7 + tb * 3 + split)
+    M, N, K = 200, 72, 300
+    A = torch.randn((K, M) if ta else (M, K), generator=g, device="cuda").to(torch.bfloat16)
+    B = torch.randn((N, K) if tb else (K, N), generator=g, device="cuda").to(torch.bfloat16)
+    C0 = torch.randn((M, N), generator=g, device="cuda")
+    Cm = C0.clone()
+    check(lib().delta_gemm_bf16(ctx.handle, M, N, K, A.data_ptr(), A.shape[1], ta, B.data_ptr(), B.shape[1], tb,
+                                Cm.data_ptr(), N, acc, split))
+    ctx.synchronize()
+    Af = A.float().T if ta else A.float()
+    Bf = B.float().T if tb else B.float()
+    ref = Af @ Bf + (C0 if acc else 0)
+    assert _rel(Cm.cpu(), ref.cpu()) <= 1e-5
+
+
+def test_features_bit_exact_vs_oracle(ctx, pairs):
+    from delta_b200.learned import features
+    from delta_b200.narrowphase import pairs_device
+
+    from oracle import mlp_oracle as mo
+
+    a, b = pairs
+    da, db = _dev(a), _dev(b)
+    p, q, _, _ = pairs_device(ctx, 0, da, db)
+    X, T, valid = features(ctx, da, db, p, q)
+    ctx.synchronize()
+    f, To, ok = mo.canon(a, b, p.cpu().numpy(), q.cpu().numpy())
+    assert np.array_equal(X.float().cpu().numpy().astype(np.float64), f)
+    assert np.array_equal(valid.cpu().numpy().astype(bool), ok)
+    assert np.array_equal(T.cpu().numpy(), To)
+
+
+def test_forward_backward_vs_oracle(ctx, pairs):
+    import torch
+
+    from delta_b200.learned import WarmStartMLP, labelled
+
+    from oracle import mlp_oracle as mo
+
+    a, b = pairs
+    M = 4096
+    da, db = _dev(a[:, :M]), _dev(b[:, :M])
+    X, T, valid = labelled(ctx, da, db)
+    model = WarmStartMLP(ctx, seed=3)
+    nv = int(valid.sum().item())
+    Y = model.forward(X).clone()
+    model.backward(X, T, valid, nv)
+    ctx.synchronize()
+    P = mo.unpack(model.params.cpu().numpy().astype(np.float64))
+    cache = mo.forward(X.float().cpu().numpy(), P)
+    loss, g = mo.backward(cache, P, T.cpu().numpy().astype(np.float64), valid.cpu().numpy().astype(bool))
+    assert _rel(Y.cpu().numpy(), cache["Y"]) <= 2e-2
+    assert abs(float(model.loss.item()) - loss) <= 2e-2 * loss
+    for name in ("W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4"):
+        assert _rel(model.grad(name).cpu().numpy(), g[name]) <= 2e-2, name
+    # and the Adam step against the oracle's
+    w0 = model.params.cpu().numpy().astype(np.float64)
+    gr = model.grads.cpu().numpy().astype(np.float64)
+    model.adam(lr=1e-3)
+    ctx.synchronize()
+    w1, _, _ = mo.adam(w0, gr, np.zeros_like(w0), np.zeros_like(w0), 1)
+    assert np.max(np.abs(model.params.cpu().numpy() - w1)) <= 1e-6
+    assert torch.equal(model.params_bf16, model.params.to(torch.bfloat16))
+
+
+def test_fused_inference_equals_layer_path(ctx, pairs):
+    from delta_b200.learned import WarmStartMLP, features
+
+    a, b = pairs
+    n = 5000  # not a multiple of the 16-row tile
+    da, db = _dev(a[:, :n]), _dev(b[:, :n])
+    model = WarmStartMLP(ctx, seed=4)
+    x0 = model.predict(da, db)
+    X, _, _ = features(ctx, da, db)
+    Y = model.forward(X)
+    ctx.synchronize()
+    assert np.array_equal(x0.cpu().numpy(), Y.cpu().numpy())
+
+
+@pytest.fixture(scope="module")
+def trained(ctx):
+    """A network trained on 2^19 fresh pairs for 6 epochs with the library's kernels."""
+    from delta_b200.learned import WarmStartMLP, labelled, train
+    from delta_b200.scenarios import narrowphase_pairs
+
+    a, b, _, _ = narrowphase_pairs(1 << 19, seed=2024)
+    X, T, valid = labelled(ctx, _dev(a), _dev(b))
+    model = WarmStartMLP(ctx, seed=0)
+    losses = train(model, X, T, valid, epochs=6, batch=8192, lr=2e-3, seed=1)
+    return model, losses
+
+
+def test_training_reduces_loss(trained):
+    _, losses = trained
+    assert losses[-1] < 0.5 * losses[0], losses
+    assert all(np.isfinite(losses))
+
+
+def test_trained_network_beats_centroid_start(ctx, trained, pairs):
+    """What the network gains: the reference penalty iteration (penalty.cpp:434-582)
+    converges in fewer iterations from the prediction than from 0.33, and the learned
+    solver certifies more pairs without the fallback than from the centroids."""
+    import torch
+
+    from delta_b200._lib import check, lib
+    from delta_b200.learned import refine
+
+    model, _ = trained
+    a, b = pairs
+    da, db = _dev(a), _dev(b)
+    n = a.shape[1]
+    x0 = model.predict(da, db)
+    it = {}
+    for name, start in (("net", x0), ("plain", None)):
+        p = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        q, d = torch.empty_like(p), torch.empty(n, dtype=torch.float64, device="cuda")
+        iters = torch.empty(n, dtype=torch.uint8, device="cuda")
+        check(lib().delta_penalty_warm(ctx.handle, n, da.data_ptr(), db.data_ptr(), n,
+                                       None if start is None else start.data_ptr(), 1e-6, p.data_ptr(),
+                                       q.data_ptr(), d.data_ptr(), iters.data_ptr()))
+        it[name] = iters.float().mean().item()
+    assert it["net"] < it["plain"], it
+    for sweeps in (0, 1):
+        c_net = refine(ctx, da, db, x0, sweeps)[3].float().mean().item()
+        c_plain = refine(ctx, da, db, None, sweeps)[3].float().mean().item()
+        assert c_net > c_plain, (sweeps, c_net, c_plain)
+
+
+@pytest.mark.parametrize("use_net", [True, False])
+def test_learned_solver_vs_fp64_bf(ctx, trained, oracle, pairs, use_net):
+    """Every pair within 1e-6 relative distance of FP64 bfSolver; uncertified pairs
+    (fallback) bit-exact; contact sets equal outside the 1e-6 band of the threshold."""
+    from delta_b200.learned import learned_pairs
+
+    from tests.golden.make_golden import edge_case_pairs
+
+    model = trained[0] if use_net else None
+    ea, eb = edge_case_pairs()
+    a = np.concatenate([pairs[0], ea], 1)
+    b = np.concatenate([pairs[1], eb], 1)
+    p, q, d, cert = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=2)
+    ctx.synchronize()
+    p, q, d, cert = p.cpu().numpy(), q.cpu().numpy(), d.cpu().numpy(), cert.cpu().numpy()
+    op, oq, od, _ = oracle.pairs(0, a, b)
+    fin = np.isfinite(od)
+    rel = np.abs(d - od)[fin] / np.maximum(od[fin], 1e-300)
+    assert rel.max() <= 1e-6, rel.max()
+    fb = cert == 0
+    assert np.array_equal(d[fb], od[fb], equal_nan=True)
+    assert np.array_equal(p[:, fb], op[:, fb], equal_nan=True)
+    assert cert.mean() > 0.5
+    for thr in (1e-4, 1e-3, 1e-2):
+        band = np.abs(od - thr) <= 1e-6 * thr
+        assert np.array_equal((d <= thr)[~band], (od <= thr)[~band])
