@@ -57,6 +57,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_to_bf16": ([vp, i64, vp, vp], C.c_int),
     "delta_penalty_warm": ([vp, i64, vp, vp, i64, vp, f8, vp, vp, vp, vp], C.c_int),
     "delta_learned_refine": ([vp, i64, vp, vp, i64, vp, i32, f8, vp, vp, vp, vp], C.c_int),
+    "delta_pairs_run_learned": ([vp, i64, vp, vp, i64, vp, vp, i32, f8, vp, vp, vp, vp, vp], C.c_int),
 }
 
 

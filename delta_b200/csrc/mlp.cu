@@ -21,6 +21,11 @@ namespace {
 // canonical features and labels
 // ---------------------------------------------------------------------------------------
 
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __halves2bfloat162(__float2bfloat16(lo), __float2bfloat16(hi));
+  return *reinterpret_cast<const uint32_t *>(&v);
+}
+
 // Frame of triangle A: origin at its centroid, x along A1-A0, z along its normal, unit
 // scale = its longest edge.  Features: the 6 vertices in that frame (18 values).  FP64
 // with every operation rounded once (xf64), so the features are reproducible bit for bit;
@@ -79,9 +84,12 @@ __global__ void k_canon(int64_t n, const double *__restrict__ a, const double *_
   float f[18];
   bool ok;
   canon_pair(a, b, ld, i, A, B, f, ok);
-  __nv_bfloat16 *row = feat + 32 * i;
-  for (int k = 0; k < 18; ++k) row[k] = __float2bfloat16(f[k]);
-  for (int k = 18; k < 32; ++k) row[k] = __float2bfloat16(0.f);
+  // the 64-byte row as four 16-byte stores
+  uint32_t w[16];
+  for (int k = 0; k < 9; ++k) w[k] = pack_bf16(f[2 * k], f[2 * k + 1]);
+  for (int k = 9; k < 16; ++k) w[k] = 0u;
+  uint4 *row = reinterpret_cast<uint4 *>(feat + 32 * i);
+  for (int k = 0; k < 4; ++k) row[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
   if (p && q) {
     // P = A0 + x0 (A1-A0) + x1 (A2-A0); Q = B0 + x2 (B1-B0) + x3 (B2-B0)
     xf64 x[4];
@@ -100,7 +108,8 @@ __global__ void k_canon(int64_t n, const double *__restrict__ a, const double *_
       x[2 * t] = (wu * vv - wv * uv) / det;
       x[2 * t + 1] = (wv * uu - wu * uv) / det;
     }
-    for (int k = 0; k < 4; ++k) target[4 * i + k] = ok ? (float)x[k].v : 0.f;
+    reinterpret_cast<float4 *>(target)[i] = ok ? make_float4((float)x[0].v, (float)x[1].v, (float)x[2].v, (float)x[3].v)
+                                               : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   if (valid) valid[i] = ok ? 1 : 0;
 }
@@ -190,15 +199,24 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
 // ---------------------------------------------------------------------------------------
 // elementwise steps
 // ---------------------------------------------------------------------------------------
+// GELU, tanh form (Hendrycks & Gimpel 2016), with the hardware tanh (tanh.approx.f32,
+// relative error about 2^-11, below the BF16 rounding that follows).
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float kGeluK = 0.7978845608028654f;  // sqrt(2/pi)
+constexpr float kGeluC = 0.044715f;
 __device__ __forceinline__ float gelu(float x) {
-  const float k = 0.7978845608028654f;  // sqrt(2/pi), tanh form of GELU
-  return 0.5f * x * (1.f + tanhf(k * (x + 0.044715f * x * x * x)));
+  const float u = x * fmaf(kGeluC * kGeluK, x * x, kGeluK);
+  const float h = 0.5f * x;
+  return fmaf(h, tanh_hw(u), h);
 }
 __device__ __forceinline__ float gelu_grad(float x) {
-  const float k = 0.7978845608028654f;
-  const float u = k * (x + 0.044715f * x * x * x);
-  const float th = tanhf(u);
-  return 0.5f * (1.f + th) + 0.5f * x * (1.f - th * th) * k * (1.f + 3.f * 0.044715f * x * x);
+  const float x2 = x * x;
+  const float th = tanh_hw(x * fmaf(kGeluC * kGeluK, x2, kGeluK));
+  return 0.5f * (1.f + th) + 0.5f * x * (1.f - th * th) * kGeluK * fmaf(3.f * kGeluC, x2, 1.f);
 }
 
 // Z[M,N] += bias; H = bf16(gelu(Z)) (or bf16(Z) when act == 0); Z keeps the pre-activation.
@@ -270,17 +288,19 @@ __global__ void k_f32_to_bf16(int64_t n, const float *x, __nv_bfloat16 *y) {
 }
 
 // ---------------------------------------------------------------------------------------
-// fused inference: features -> 4 layers -> x0, one kernel.  Weights stay in shared memory
-// for the CTA's lifetime; each warp owns 16 pairs and keeps its activations in its own
-// shared rows, so layers need no block barrier.  The MMAs run in the same order as
-// k_gemm's, so the output equals the layer-by-layer path bit for bit.
+// fused inference: the four layers on rows of canonical features, one kernel.  Weights
+// stay in shared memory for the CTA's lifetime; each warp owns 16 pairs at a time and
+// keeps their activations in registers: the FP32 accumulator fragment of one layer
+// (m16n8 tiles) is, packed to BF16 pairs, exactly the A fragment (m16k16) of the next.
+// The MMAs run in the same order as k_gemm's and the epilogue is k_bias_act's, so the
+// output equals the layer-by-layer path bit for bit.
 // ---------------------------------------------------------------------------------------
 constexpr int kIn = 32, kHid = 128, kOut = 4;
 constexpr int64_t kOffW1 = 0, kOffB1 = kOffW1 + kHid * kIn, kOffW2 = kOffB1 + kHid, kOffB2 = kOffW2 + kHid * kHid,
                   kOffW3 = kOffB2 + kHid, kOffB3 = kOffW3 + kHid * kHid, kOffW4 = kOffB3 + kHid,
                   kOffB4 = kOffW4 + kOut * kHid, kNumParams = (kOffB4 + kOut + 7) / 8 * 8;
-constexpr int kIP = kIn + 8, kHP = kHid + 8;  // padded row pitches (bf16): conflict-free fragments
-constexpr int kInferWarps = 4;
+constexpr int kIP = kIn + 8, kHP = kHid + 8;  // padded row pitches (bf16): conflict-free ldmatrix
+constexpr int kInferWarps = 8;
 
 struct InferSmem {
   __nv_bfloat16 w1[kHid][kIP];
@@ -288,54 +308,70 @@ struct InferSmem {
   __nv_bfloat16 w3[kHid][kHP];
   __nv_bfloat16 w4[8][kHP];  // rows 4..7 zero
   float bias[3 * kHid + 8];
-  __nv_bfloat16 h[kInferWarps][16][kHP];
 };
 
-// acc[NT][4] = H[16][16*KS] . W^T for W rows 0..8*NT-1 (row pitch wp), fragments as k_gemm.
+__device__ __forceinline__ void ldmatrix_x4(uint32_t r[4], const void *row_addr) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(row_addr);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(s));
+}
+__device__ __forceinline__ void ldmatrix_x2(uint32_t r[2], const void *row_addr) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(row_addr);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r[0]), "=r"(r[1]) : "r"(s));
+}
+
+// acc[NT][4] = H . W^T for 16 rows: H as A fragments a[KS][4] in registers, W rows
+// 0..8*NT-1 (row pitch wp) in shared memory, B fragments by ldmatrix (row addresses
+// 16-byte aligned: pitches of 80 and 272 bytes, column offsets of 16 bytes).
 template <int KS, int NT>
-__device__ __forceinline__ void warp_mma_rows(const __nv_bfloat16 (*H)[kHP], const __nv_bfloat16 *W, int wp,
-                                              float acc[NT][4]) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+__device__ __forceinline__ void warp_layer(const uint32_t a[KS][4], const __nv_bfloat16 *W, int wp,
+                                           float acc[NT][4]) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  // B is stored [n][k]: lanes 0-7 address rows n0..n0+7 at k, 8-15 the same rows at k+8,
+  // 16-23 rows n0+8.. at k, 24-31 those at k+8
+  const __nv_bfloat16 *brow = W + ((lane & 7) + ((lane >> 4) << 3)) * wp + ((lane >> 3) & 1) * 8;
 #pragma unroll
   for (int ks = 0; ks < KS; ++ks) {
     const int kk = 16 * ks;
-    uint32_t af[4];
-    af[0] = *reinterpret_cast<const uint32_t *>(&H[g][kk + 2 * t]);
-    af[1] = *reinterpret_cast<const uint32_t *>(&H[g + 8][kk + 2 * t]);
-    af[2] = *reinterpret_cast<const uint32_t *>(&H[g][kk + 2 * t + 8]);
-    af[3] = *reinterpret_cast<const uint32_t *>(&H[g + 8][kk + 2 * t + 8]);
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
+    if constexpr (NT == 1) {
       uint32_t bf[2];
-      const __nv_bfloat16 *wr = W + (8 * nt + g) * wp + kk + 2 * t;
-      bf[0] = *reinterpret_cast<const uint32_t *>(wr);
-      bf[1] = *reinterpret_cast<const uint32_t *>(wr + 8);
-      mma_bf16(acc[nt], af, bf);
+      ldmatrix_x2(bf, brow + kk);
+      mma_bf16(acc[0], a[ks], bf);
+    } else {
+#pragma unroll
+      for (int nt = 0; nt < NT; nt += 2) {
+        uint32_t r[4];
+        ldmatrix_x4(r, brow + 8 * nt * wp + kk);
+        const uint32_t b0[2] = {r[0], r[1]}, b1[2] = {r[2], r[3]};
+        mma_bf16(acc[nt], a[ks], b0);
+        mma_bf16(acc[nt + 1], a[ks], b1);
+      }
     }
   }
 }
 
-// H[16][128] = bf16(GELU(acc + bias)) in place (after every lane has read H).
-__device__ __forceinline__ void warp_store_gelu(__nv_bfloat16 (*H)[kHP], const float acc[16][4], const float *bias) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  __syncwarp();
+// GELU(acc + bias) packed to BF16 as the next layer's A fragments: k-tile kt takes output
+// n-tiles 2kt (k 0..7) and 2kt+1 (k 8..15); rows g (regs 0, 2) and g+8 (regs 1, 3).
+__device__ __forceinline__ void warp_gelu_to_a(const float acc[16][4], const float *bias, uint32_t a[8][4]) {
+  const int t = threadIdx.x & 3;
 #pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    const int col = 8 * nt + 2 * t;
-    const float b0 = bias[col], b1 = bias[col + 1];
-    *reinterpret_cast<__nv_bfloat162 *>(&H[g][col]) =
-        __halves2bfloat162(__float2bfloat16(gelu(acc[nt][0] + b0)), __float2bfloat16(gelu(acc[nt][1] + b1)));
-    *reinterpret_cast<__nv_bfloat162 *>(&H[g + 8][col]) =
-        __halves2bfloat162(__float2bfloat16(gelu(acc[nt][2] + b0)), __float2bfloat16(gelu(acc[nt][3] + b1)));
+  for (int kt = 0; kt < 8; ++kt) {
+#pragma unroll
+    for (int hlf = 0; hlf < 2; ++hlf) {
+      const int nt = 2 * kt + hlf, col = 8 * nt + 2 * t;
+      const float b0 = bias[col], b1 = bias[col + 1];
+      a[kt][2 * hlf] = pack_bf16(gelu(acc[nt][0] + b0), gelu(acc[nt][1] + b1));
+      a[kt][2 * hlf + 1] = pack_bf16(gelu(acc[nt][2] + b0), gelu(acc[nt][3] + b1));
+    }
   }
-  __syncwarp();
 }
 
 __global__ void __launch_bounds__(32 * kInferWarps, 2)
-    k_mlp_infer(int64_t n, const double *__restrict__ a, const double *__restrict__ b, int64_t ld,
-                const float *__restrict__ params, const __nv_bfloat16 *__restrict__ wb, float *__restrict__ x0) {
+    k_mlp_infer(int64_t n, const __nv_bfloat16 *__restrict__ feat, const float *__restrict__ params,
+                const __nv_bfloat16 *__restrict__ wb, float *__restrict__ x0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   InferSmem &sm = *reinterpret_cast<InferSmem *>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -362,38 +398,35 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2)
   if (tid < 8) sm.bias[3 * kHid + tid] = tid < kOut ? params[kOffB4 + tid] : 0.f;
   __syncthreads();
 
-  __nv_bfloat16(*H)[kHP] = sm.h[warp];
+  const int g = lane >> 2, t = lane & 3;
   const int64_t tiles = (n + 15) / 16;
   for (int64_t tile = (int64_t)blockIdx.x * kInferWarps + warp; tile < tiles;
        tile += (int64_t)gridDim.x * kInferWarps) {
     const int64_t row0 = tile * 16;
-    if (lane < 16) {
-      const int64_t i = row0 + lane;
-      float f[18];
-      if (i < n) {
-        xf64 A[3][3], B[3][3];
-        bool ok;
-        canon_pair(a, b, ld, i, A, B, f, ok);
-      } else {
-        for (int k = 0; k < 18; ++k) f[k] = 0.f;
+    // layer-1 A fragments straight from the feature rows (32 BF16 = 16 words per row)
+    uint32_t a1[2][4];
+    {
+      const int64_t r0 = row0 + g, r1 = row0 + g + 8;
+      const uint32_t *f0 = reinterpret_cast<const uint32_t *>(feat + 32 * (r0 < n ? r0 : n - 1));
+      const uint32_t *f1 = reinterpret_cast<const uint32_t *>(feat + 32 * (r1 < n ? r1 : n - 1));
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks) {
+        a1[ks][0] = __ldg(f0 + 8 * ks + t);
+        a1[ks][1] = __ldg(f1 + 8 * ks + t);
+        a1[ks][2] = __ldg(f0 + 8 * ks + 4 + t);
+        a1[ks][3] = __ldg(f1 + 8 * ks + 4 + t);
       }
-      for (int k = 0; k < 18; k += 2)
-        *reinterpret_cast<__nv_bfloat162 *>(&H[lane][k]) =
-            __halves2bfloat162(__float2bfloat16(f[k]), __float2bfloat16(f[k + 1]));
-      for (int k = 18; k < kIn; k += 2)
-        *reinterpret_cast<__nv_bfloat162 *>(&H[lane][k]) = __halves2bfloat162(__float2bfloat16(0.f), __float2bfloat16(0.f));
     }
-    __syncwarp();
     float acc[16][4];
-    warp_mma_rows<kIn / 16, 16>(H, &sm.w1[0][0], kIP, acc);
-    warp_store_gelu(H, acc, sm.bias);
-    warp_mma_rows<kHid / 16, 16>(H, &sm.w2[0][0], kHP, acc);
-    warp_store_gelu(H, acc, sm.bias + kHid);
-    warp_mma_rows<kHid / 16, 16>(H, &sm.w3[0][0], kHP, acc);
-    warp_store_gelu(H, acc, sm.bias + 2 * kHid);
+    uint32_t h[8][4];
+    warp_layer<2, 16>(a1, &sm.w1[0][0], kIP, acc);
+    warp_gelu_to_a(acc, sm.bias, h);
+    warp_layer<8, 16>(h, &sm.w2[0][0], kHP, acc);
+    warp_gelu_to_a(acc, sm.bias + kHid, h);
+    warp_layer<8, 16>(h, &sm.w3[0][0], kHP, acc);
+    warp_gelu_to_a(acc, sm.bias + 2 * kHid, h);
     float out[1][4];
-    warp_mma_rows<kHid / 16, 1>(H, &sm.w4[0][0], kHP, out);
-    const int g = lane >> 2, t = lane & 3;
+    warp_layer<8, 1>(h, &sm.w4[0][0], kHP, out);
     if (t < 2) {
       const float b0 = sm.bias[3 * kHid + 2 * t], b1 = sm.bias[3 * kHid + 2 * t + 1];
       if (row0 + g < n)
@@ -401,7 +434,6 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2)
       if (row0 + g + 8 < n)
         *reinterpret_cast<float2 *>(x0 + 4 * (row0 + g + 8) + 2 * t) = make_float2(out[0][2] + b0, out[0][3] + b1);
     }
-    __syncwarp();
   }
 }
 
@@ -464,32 +496,66 @@ __device__ __forceinline__ void closest_on_tri(const float *V0, const float *E0,
   }
 }
 
-// Learned hybrid solver for one pair.  From the warm start x0 (barycentric weights of P
-// on A and Q on B; centroids when x0 is null), `sweeps` FP32 alternating projections
-// (Q <- closest point of B to P, P <- closest point of A to Q) locate the closest points
-// roughly.  Three bfSolver features are read off them: B's vertex nearest Q against face
-// A, A's vertex nearest P against face B, and the edge pair nearest (P, Q).  They are
-// evaluated in FP64 with the reference arithmetic (bf.cpp:586-697, 920-1090) and chosen
-// between by bfSolver's rule (bf.cpp:1102), so an identified feature gives bfSolver's
-// points bit for bit.  FP64 certificate: with r = P - Q, every plane normal to r bounds
-// the distance below by min_i r.A_i/|r| - max_j r.B_j/|r|; the result is certified when
-// |r| minus that bound (plus a rounding slack) is at most rel_tol |r|.  Intersecting
-// triangles have no separating plane and are never certified.
-__global__ void k_learned_refine(int64_t n, const double *a, const double *b, int64_t ld, const float *x0,
-                                 int sweeps, double rel_tol, double *p, double *q, double *dist, uint8_t *flags) {
+// First index of the largest / smallest of three values.
+__device__ __forceinline__ int argmax3(float x0, float x1, float x2) {
+  const int i = x1 > x0 ? 1 : 0;
+  return x2 > (i ? x1 : x0) ? 2 : i;
+}
+__device__ __forceinline__ int argmin3(float x0, float x1, float x2) {
+  const int i = x1 < x0 ? 1 : 0;
+  return x2 < (i ? x1 : x0) ? 2 : i;
+}
+
+// Vertex j (0..2) of T, by selects (no dynamically indexed register array).
+template <class R>
+__device__ __forceinline__ void pick_vertex(const R T[3][3], int j, R out[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) out[k] = j == 0 ? T[0][k] : (j == 1 ? T[1][k] : T[2][k]);
+}
+
+// Learned hybrid solver, one pair per thread.  From the warm start x0 (barycentric
+// weights of P on A and Q on B; centroids when x0 is null), `sweeps` FP32 alternating
+// projections (Q <- closest point of B to P, P <- closest point of A to Q) locate the
+// closest points roughly.  Three bfSolver features are read off them: B's vertex nearest
+// Q against face A, A's vertex nearest P against face B, and the edge pair nearest
+// (P, Q).  The one bfSolver's rule (bf.cpp:1102: vertex-face family first, first minimum
+// in feature order, the edge pair only when strictly closer) picks on FP32 distances is
+// evaluated in FP64 with the reference arithmetic (bf.cpp:586-697 or 920-1090), so a
+// pair whose closest feature was found gets bfSolver's points bit for bit.
+// FP64 certificate: with r = P - Q, every plane normal to r bounds the distance below by
+// (min_i r.A_i - max_j r.B_j)/|r|; the result is certified when
+// |r|^2 - (min_i r.A_i - max_j r.B_j) + slack |r| <= rel_tol |r|^2, i.e. the distance is
+// within rel_tol of the true one; slack = 1e-14 max|coordinate| covers the rounding of the
+// dot products.  Intersecting triangles have no separating plane and are never certified.
+// With `list`, uncertified pairs are appended to list[*count] (warp-aggregated) and their
+// outputs left for the exact solver; flags then read 1 (certified) or 2 (listed).
+__global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double *__restrict__ a,
+                                                        const double *__restrict__ b, int64_t ld,
+                                                        const float *__restrict__ x0, int sweeps, double rel_tol,
+                                                        double *__restrict__ p, double *__restrict__ q,
+                                                        double *__restrict__ dist, uint8_t *__restrict__ flags,
+                                                        uint32_t *__restrict__ list, uint32_t *__restrict__ count) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const bool valid = i < n;
+  const int64_t ii = valid ? i : n - 1;
   xf64 A[3][3], B[3][3];
+  float Af[3][3], Bf[3][3];
   double scale = 0.0;
   for (int v = 0; v < 3; ++v)
     for (int k = 0; k < 3; ++k) {
-      A[v][k] = xf64(a[(3 * v + k) * ld + i]);
-      B[v][k] = xf64(b[(3 * v + k) * ld + i]);
+      A[v][k] = xf64(__ldg(a + (3 * v + k) * ld + ii));
+      B[v][k] = xf64(__ldg(b + (3 * v + k) * ld + ii));
       scale = fmax(scale, fmax(fabs(A[v][k].v), fabs(B[v][k].v)));
+    }
+  // FP32 copies relative to A0 (the distance is translation invariant)
+  for (int v = 0; v < 3; ++v)
+    for (int k = 0; k < 3; ++k) {
+      Af[v][k] = (float)(A[v][k].v - A[0][k].v);
+      Bf[v][k] = (float)(B[v][k].v - A[0][k].v);
     }
   float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
   if (x0) {
-    const float4 x = reinterpret_cast<const float4 *>(x0)[i];
+    const float4 x = reinterpret_cast<const float4 *>(x0)[ii];
     // project the prediction into the parameter triangles
     s = fmaxf(x.x, 0.f); t = fmaxf(x.y, 0.f); u = fmaxf(x.z, 0.f); w = fmaxf(x.w, 0.f);
     const float st = s + t, uw = u + w;
@@ -497,65 +563,98 @@ __global__ void k_learned_refine(int64_t n, const double *a, const double *b, in
     if (uw > 1.f) { u /= uw; w /= uw; }
   }
   if (sweeps > 0) {
-    float A0[3], EA0[3], EA1[3], B0[3], EB0[3], EB1[3];
+    float EA0[3], EA1[3], EB0[3], EB1[3];
     for (int k = 0; k < 3; ++k) {
-      A0[k] = 0.f;
-      EA0[k] = (float)(A[1][k].v - A[0][k].v);
-      EA1[k] = (float)(A[2][k].v - A[0][k].v);
-      B0[k] = (float)(B[0][k].v - A[0][k].v);
-      EB0[k] = (float)(B[1][k].v - B[0][k].v);
-      EB1[k] = (float)(B[2][k].v - B[0][k].v);
+      EA0[k] = Af[1][k] - Af[0][k];
+      EA1[k] = Af[2][k] - Af[0][k];
+      EB0[k] = Bf[1][k] - Bf[0][k];
+      EB1[k] = Bf[2][k] - Bf[0][k];
     }
     for (int it = 0; it < sweeps; ++it) {
       float P[3];
-      for (int k = 0; k < 3; ++k) P[k] = A0[k] + s * EA0[k] + t * EA1[k];
-      closest_on_tri(B0, EB0, EB1, P, u, w);
+      for (int k = 0; k < 3; ++k) P[k] = Af[0][k] + s * EA0[k] + t * EA1[k];
+      closest_on_tri(Bf[0], EB0, EB1, P, u, w);
       float Q[3];
-      for (int k = 0; k < 3; ++k) Q[k] = B0[k] + u * EB0[k] + w * EB1[k];
-      closest_on_tri(A0, EA0, EA1, Q, s, t);
+      for (int k = 0; k < 3; ++k) Q[k] = Bf[0][k] + u * EB0[k] + w * EB1[k];
+      closest_on_tri(Af[0], EA0, EA1, Q, s, t);
     }
   }
   // features read off the barycentric weights lA = (1-s-t, s, t), lB = (1-u-w, u, w)
-  const float lA[3] = {1.f - s - t, s, t}, lB[3] = {1.f - u - w, u, w};
-  int iA = 0, jB = 0, kA = 0, kB = 0;
-  for (int v = 1; v < 3; ++v) {
-    if (lA[v] > lA[iA]) iA = v;
-    if (lB[v] > lB[jB]) jB = v;
-    if (lA[v] < lA[kA]) kA = v;
-    if (lB[v] < lB[kB]) kB = v;
-  }
-  // bf's vertex-face features: 9 + j is B's vertex j on face A, 12 + j A's vertex j on
-  // face B; edge-edge 3 ea + eb joins vertices ea, ea+1 (the edge opposite vertex ea+2).
-  const int fB = 9 + jB, fA = 12 + iA, fE = 3 * ((kA + 1) % 3) + (kB + 1) % 3;
-  xf64 s1, t1, s2, t2, sc, tc;
-  const xf64 d1 = feature_ref(A, B, fB, s1, t1);
-  const xf64 d2 = feature_ref(A, B, fA, s2, t2);
-  const xf64 de = feature_ref(A, B, fE, sc, tc);
+  const int iA = argmax3(1.f - s - t, s, t), jB = argmax3(1.f - u - w, u, w);
+  const int kA = argmin3(1.f - s - t, s, t), kB = argmin3(1.f - u - w, u, w);
+  // bf's vertex-face features: B's vertex jB on face A (feature 9 + jB), A's vertex iA
+  // on face B (12 + iA); edge-edge feature 3 ea + eb joins vertices ea, ea+1 (the edge
+  // opposite vertex ea+2).  Operands are selected, not indexed, so all lanes run the
+  // same code whichever features they picked.
+  const int ea = (kA + 1) % 3, eb = (kB + 1) % 3;
+  float X1[3], X2[3], HA[3], TA[3], HB[3], TB[3], f0, f1;
+  pick_vertex(Bf, jB, X1);
+  pick_vertex(Af, iA, X2);
+  pick_vertex(Af, ea, HA);
+  pick_vertex(Af, (ea + 1) % 3, TA);
+  pick_vertex(Bf, eb, HB);
+  pick_vertex(Bf, (eb + 1) % 3, TB);
+  const float d1 = pt_tri_ref(Af[0], Af[1], Af[2], X1, f0, f1);
+  const float d2 = pt_tri_ref(Bf[0], Bf[1], Bf[2], X2, f0, f1);
+  const float de = seg_seg_ref(HA, TA, HB, TB, f0, f1);
+  const bool edge = (d2 < d1 ? d2 : d1) > de, faceB = d2 < d1;
   xf64 pq[6];
-  // first minimum in feature order within the vertex-face family; the edge pair only
-  // when strictly closer
-  const bool second = d2 < d1;
-  const xf64 dpt = second ? d2 : d1;
-  if (dpt > de) seg_seg_points(A, B, fE, sc, tc, pq);
-  else if (second) pt_tri_points(A, B, fA - 9, s2, t2, pq);
-  else pt_tri_points(A, B, fB - 9, s1, t1, pq);
+  if (edge) {
+    xf64 HA[3], TA[3], HB[3], TB[3], sc, tc;
+    pick_vertex(A, ea, HA);
+    pick_vertex(A, (ea + 1) % 3, TA);
+    pick_vertex(B, eb, HB);
+    pick_vertex(B, (eb + 1) % 3, TB);
+    seg_seg_ref(HA, TA, HB, TB, sc, tc);
+    for (int k = 0; k < 3; ++k) {  // bf.cpp:715-879 (seg_seg_points)
+      pq[k] = TA[k] + ((HA[k] - TA[k]) * sc);
+      pq[3 + k] = TB[k] + ((HB[k] - TB[k]) * tc);
+    }
+  } else {
+    xf64 T[3][3], X[3], sf, tf;
+    for (int v = 0; v < 3; ++v)
+      for (int k = 0; k < 3; ++k) T[v][k] = faceB ? B[v][k] : A[v][k];
+    if (faceB) pick_vertex(A, iA, X);
+    else pick_vertex(B, jB, X);
+    pt_tri_ref(T[0], T[1], T[2], X, sf, tf);
+    for (int k = 0; k < 3; ++k) {  // bf.cpp:1104-1177 (pt_tri_points)
+      const xf64 face = T[0][k] + ((T[2][k] - T[0][k]) * tf) + ((T[1][k] - T[0][k]) * sf);
+      pq[k] = faceB ? X[k] : face;
+      pq[3 + k] = faceB ? face : X[k];
+    }
+  }
   const double d = pq_distance(pq).v;
   bool ok = false;
   if (d > 0) {
     const double r[3] = {pq[0].v - pq[3].v, pq[1].v - pq[4].v, pq[2].v - pq[5].v};
     double amin = 1e300, bmax = -1e300;
     for (int v = 0; v < 3; ++v) {
-      amin = fmin(amin, (A[v][0].v * r[0] + A[v][1].v * r[1] + A[v][2].v * r[2]) / d);
-      bmax = fmax(bmax, (B[v][0].v * r[0] + B[v][1].v * r[1] + B[v][2].v * r[2]) / d);
+      amin = fmin(amin, A[v][0].v * r[0] + A[v][1].v * r[1] + A[v][2].v * r[2]);
+      bmax = fmax(bmax, B[v][0].v * r[0] + B[v][1].v * r[1] + B[v][2].v * r[2]);
     }
-    ok = d - (amin - bmax) + 1e-14 * scale <= rel_tol * d;
+    const double d2r = d * d;
+    ok = d2r - (amin - bmax) + 1e-14 * scale * d <= rel_tol * d2r;
   }
-  for (int k = 0; k < 3; ++k) {
-    p[k * ld + i] = pq[k].v;
-    q[k * ld + i] = pq[3 + k].v;
+  if (list) {
+    const bool need = valid && !ok;
+    const unsigned ballot = __ballot_sync(0xffffffffu, need);
+    const int lane = threadIdx.x & 31;
+    unsigned base = 0;
+    if (ballot) {
+      if (lane == 0) base = atomicAdd(count, (unsigned)__popc(ballot));
+      base = __shfl_sync(0xffffffffu, base, 0);
+    }
+    if (need) list[base + __popc(ballot & ((1u << lane) - 1u))] = (uint32_t)i;
   }
-  dist[i] = d;
-  flags[i] = ok ? 1 : 0;
+  if (!valid) return;
+  if (ok || !list) {
+    for (int k = 0; k < 3; ++k) {
+      p[k * ld + i] = pq[k].v;
+      q[k * ld + i] = pq[3 + k].v;
+    }
+    dist[i] = d;
+  }
+  if (flags) flags[i] = list ? (ok ? 1 : 2) : (ok ? 1 : 0);
 }
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
@@ -574,6 +673,8 @@ delta_status delta_mlp_features(delta_ctx *ctx, int64_t n, const double *a, cons
   if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !features_bf16)) || ((p == nullptr) != (q == nullptr)) ||
       (p && !targets))
     return set_error(DELTA_ERR_INVALID, "delta_mlp_features: bad argument");
+  if ((reinterpret_cast<uintptr_t>(features_bf16) & 15) || (reinterpret_cast<uintptr_t>(targets) & 15))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_features: features and targets must be 16-byte aligned");
   if (n == 0) return DELTA_OK;
   k_canon<<<nblk(n), 256, 0, ctx->stream>>>(n, a, b, ld, p, q, (__nv_bfloat16 *)features_bf16, targets, valid);
   ctx->launches += 1;
@@ -665,8 +766,15 @@ delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const d
   if ((reinterpret_cast<uintptr_t>(params_bf16) & 3) || (reinterpret_cast<uintptr_t>(x0) & 7))
     return set_error(DELTA_ERR_INVALID, "delta_mlp_infer: params_bf16 must be 4-byte and x0 8-byte aligned");
   if (n == 0) return DELTA_OK;
+  void *fbuf;
+  delta_status st = ctx_scratch(ctx, 15, sizeof(__nv_bfloat16) * 32 * (size_t)n, &fbuf);
+  if (st != DELTA_OK) return st;
+  __nv_bfloat16 *feat = static_cast<__nv_bfloat16 *>(fbuf);
+  k_canon<<<nblk(n), 256, 0, ctx->stream>>>(n, a, b, ld, nullptr, nullptr, feat, nullptr, nullptr);
+  ctx->launches += 1;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "delta_mlp_infer: features");
   static thread_local int configured_device = -1;
-  cudaError_t e = cudaSuccess;
   if (configured_device != ctx->device) {
     e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
     if (e != cudaSuccess) return cuda_error(e, "delta_mlp_infer: shared memory attribute");
@@ -675,7 +783,7 @@ delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const d
   const int64_t tiles = (n + 15) / 16;
   const int64_t want = (tiles + kInferWarps - 1) / kInferWarps;
   const unsigned grid = (unsigned)std::min<int64_t>(want, 2 * kNumSMs);
-  k_mlp_infer<<<grid, 32 * kInferWarps, sizeof(InferSmem), ctx->stream>>>(n, a, b, ld, params,
+  k_mlp_infer<<<grid, 32 * kInferWarps, sizeof(InferSmem), ctx->stream>>>(n, feat, params,
                                                                           (const __nv_bfloat16 *)params_bf16, x0);
   ctx->launches += 1;
   return cuda_error(cudaGetLastError(), "delta_mlp_infer");
@@ -700,9 +808,52 @@ delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, co
   if (reinterpret_cast<uintptr_t>(x0) & 15)
     return set_error(DELTA_ERR_INVALID, "delta_learned_refine: x0 must be 16-byte aligned");
   if (n == 0) return DELTA_OK;
-  k_learned_refine<<<nblk(n, 128), 128, 0, ctx->stream>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, certified);
+  k_learned_refine<<<nblk(n, 128), 128, 0, ctx->stream>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, certified,
+                                                          nullptr, nullptr);
   ctx->launches += 1;
   return cuda_error(cudaGetLastError(), "delta_learned_refine");
+}
+
+delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                     const float *params, const void *params_bf16, int32_t sweeps, double rel_tol,
+                                     double *p, double *q, double *dist, uint8_t *flags, int64_t *n_fallback) {
+  if (!ctx || n < 0 || ld < n || sweeps < 0 || n > (int64_t)UINT32_MAX ||
+      (n > 0 && (!a || !b || !p || !q || !dist)) || ((params == nullptr) != (params_bf16 == nullptr)))
+    return set_error(DELTA_ERR_INVALID, "delta_pairs_run_learned: bad argument");
+  if (n_fallback) *n_fallback = 0;
+  if (n == 0) return DELTA_OK;
+  delta_status st;
+  float *x0 = nullptr;
+  if (params) {
+    void *buf;
+    if ((st = ctx_scratch(ctx, 13, sizeof(float) * 4 * (size_t)n, &buf)) != DELTA_OK) return st;
+    x0 = static_cast<float *>(buf);
+    if ((st = delta_mlp_infer(ctx, n, a, b, ld, params, params_bf16, x0)) != DELTA_OK) return st;
+  }
+  void *lbuf;
+  if ((st = ctx_scratch(ctx, 14, 256 + sizeof(uint32_t) * (size_t)n, &lbuf)) != DELTA_OK) return st;
+  uint32_t *count = static_cast<uint32_t *>(lbuf);
+  uint32_t *list = reinterpret_cast<uint32_t *>(static_cast<char *>(lbuf) + 256);
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: memset");
+  k_learned_refine<<<nblk(n, 128), 128, 0, ctx->stream>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list,
+                                                          count);
+  ctx->launches += 1;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: refine");
+  const PairLaunch cfg = ctx->pair_launch_set[DELTA_BF_CERT][0] ? ctx->pair_launch[DELTA_BF_CERT][0]
+                                                                : default_pair_launch(DELTA_BF_CERT);
+  e = launch_cert_indexed(ctx->stream, count, n, list, a, b, ld, p, q, dist, cfg);
+  ctx->launches += 1;
+  if (e != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: exact fallback");
+  if (n_fallback) {
+    void *pin;
+    if ((st = ctx_pinned(ctx, sizeof(uint32_t), &pin)) != DELTA_OK) return st;
+    if ((e = cudaMemcpyAsync(pin, count, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+      return cuda_error(e, "delta_pairs_run_learned: count");
+    *n_fallback = *static_cast<uint32_t *>(pin);
+  }
+  return DELTA_OK;
 }
 
 }  // extern "C"

@@ -93,6 +93,47 @@ __global__ void __launch_bounds__(32 * W) k_pairs_cert(int64_t n, const double *
   }
 }
 
+// The certified kernel over an index list: pairs idx[0 .. *count) of the pair list (the
+// count is read on the device, so the list can be built by an earlier kernel on the
+// stream without a host round trip).
+template <int W>
+__global__ void __launch_bounds__(32 * W) k_pairs_cert_indexed(const uint32_t *__restrict__ count,
+                                                               const uint32_t *__restrict__ idx,
+                                                               const double *__restrict__ a,
+                                                               const double *__restrict__ b, int64_t ld,
+                                                               double *__restrict__ p, double *__restrict__ q,
+                                                               double *__restrict__ dist) {
+  __shared__ CertWarpSmem sm[W];
+  const int64_t n = *count;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += nwarps * 32) {
+    const bool valid = base + lane < n;
+    const int64_t i = idx[valid ? base + lane : n - 1];
+    double A[3][3], B[3][3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        A[v][k] = __ldg(a + (3 * v + k) * ld + i);
+        B[v][k] = __ldg(b + (3 * v + k) * ld + i);
+      }
+    double out[6];
+    bf_cert_warp(A, B, valid, out, sm[warp]);
+    if (valid) {
+      xf64 pq[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) pq[k] = xf64(out[k]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        p[k * ld + i] = out[k];
+        q[k * ld + i] = out[3 + k];
+      }
+      dist[i] = pq_distance(pq).v;
+    }
+  }
+}
+
 template <class R, int M>
 static cudaError_t launch_one(cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld, double me,
                               double *p, double *q, double *dist, uint8_t *flags, PairLaunch cfg) {
@@ -141,6 +182,20 @@ cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t 
   }
   if (precision == 0) return launch_prec<xf64>(method, s, n, a, b, ld, max_error, p, q, dist, flags, cfg);
   return launch_prec<float>(method, s, n, a, b, ld, max_error, p, q, dist, flags, cfg);
+}
+
+cudaError_t launch_cert_indexed(cudaStream_t s, const uint32_t *count, int64_t max_count, const uint32_t *idx,
+                                const double *a, const double *b, int64_t ld, double *p, double *q, double *dist,
+                                PairLaunch cfg) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_cert_indexed<4>, 128, 0);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = (max_count + 127) / 128;
+  const int64_t per = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 8;
+  const int64_t cap = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1) * per;
+  if (blocks > cap) blocks = cap;
+  k_pairs_cert_indexed<4><<<(unsigned)(blocks > 0 ? blocks : 1), 128, 0, s>>>(count, idx, a, b, ld, p, q, dist);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,

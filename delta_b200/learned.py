@@ -21,10 +21,17 @@ import math
 import numpy as np
 
 from ._lib import check, lib
-from .narrowphase import BF, BF_CERT, F64, Context, pairs_device
+from .narrowphase import BF, F64, Context, pairs_device
 
 IN, HIDDEN, OUT, FEATURES = 32, 128, 4, 18
 LAYERS = ((IN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, OUT))  # (fan_in, fan_out)
+
+
+def default_weights():
+    """Path of the checkpoint shipped with the package (trained by train_warmstart)."""
+    from pathlib import Path
+
+    return Path(__file__).resolve().parent / "weights" / "warmstart_mlp.npz"
 
 
 def layout() -> dict:
@@ -96,6 +103,15 @@ class WarmStartMLP:
 
     def state_dict(self) -> dict:
         return {"params": self.params.cpu().numpy(), "steps": self.steps}
+
+    @classmethod
+    def load(cls, ctx: Context, path=None) -> "WarmStartMLP":
+        """A network from a checkpoint written by train_warmstart (default: the bundled one)."""
+        from pathlib import Path
+
+        p = Path(path) if path is not None else default_weights()
+        with np.load(p) as z:
+            return cls(ctx, params=z["params"])
 
     # -- workspace ---------------------------------------------------------------------
     def _workspace(self, M):
@@ -250,21 +266,31 @@ def refine(ctx: Context, a, b, x0=None, sweeps: int = 2, rel_tol: float = 1e-6, 
     return p, q, d, cert
 
 
-def learned_pairs(ctx: Context, model: WarmStartMLP | None, a, b, sweeps: int = 2, rel_tol: float = 1e-6):
-    """The learned hybrid over pair-list tensors a, b (9, n) float64 on the device.
+def learned_pairs(ctx: Context, model: WarmStartMLP | None, a, b, sweeps: int = 2, rel_tol: float = 1e-6,
+                  out=None, count_fallback: bool = False):
+    """The learned hybrid (delta_pairs_run_learned) over pair-list tensors a, b (9, n)
+    float64 on the device.
 
     model None runs the same solver from the centroids (the method without the network).
-    Returns (p, q, dist, certified): certified pairs carry a distance within rel_tol of
-    the exact one; every other pair is solved by DELTA_BF_CERT and equals bfSolver bit
-    for bit.
+    Returns (p, q, dist, flags[, n_fallback]): flags 1 = certified, the distance within
+    rel_tol of the exact one; 2 = solved by DELTA_BF_CERT, equal to bfSolver bit for bit.
     """
-    x0 = model.predict(a, b) if model is not None else None
-    p, q, d, cert = refine(ctx, a, b, x0, sweeps, rel_tol)
-    idx = (cert == 0).nonzero().squeeze(1)
-    if idx.numel():
-        sp, sq, sd, _ = pairs_device(ctx, BF_CERT, a[:, idx].contiguous(), b[:, idx].contiguous(), precision=F64,
-                                     with_flags=False)
-        p[:, idx] = sp
-        q[:, idx] = sq
-        d[idx] = sd
-    return p, q, d, cert
+    import torch
+
+    n = a.shape[1]
+    if out is None:
+        p = torch.empty((3, n), dtype=torch.float64, device=a.device)
+        q = torch.empty_like(p)
+        d = torch.empty(n, dtype=torch.float64, device=a.device)
+        fl = torch.empty(n, dtype=torch.uint8, device=a.device)
+    else:
+        p, q, d, fl = out
+    nf = C.c_int64(0)
+    check(lib().delta_pairs_run_learned(
+        ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0),
+        None if model is None else model.params.data_ptr(), None if model is None else model.params_bf16.data_ptr(),
+        int(sweeps), float(rel_tol), p.data_ptr(), q.data_ptr(), d.data_ptr(),
+        None if fl is None else fl.data_ptr(), C.byref(nf) if count_fallback else None))
+    if count_fallback:
+        return p, q, d, fl, int(nf.value)
+    return p, q, d, fl

@@ -282,6 +282,7 @@ delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const d
  * its normal, unit = its longest edge), the six vertices in that frame as 18 BF16 values
  * padded with zeros to rows of 32 (features_bf16 [n][32]).  With p, q (closest points,
  * pair-list planes) also the targets [n][4] (barycentric weights of p on A and q on B).
+ * features_bf16 and targets 16-byte aligned.
  * valid [n] (optional) is 0 for pairs with a degenerate triangle. */
 delta_status delta_mlp_features(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                                 const double *p, const double *q, void *features_bf16, float *targets,
@@ -326,6 +327,16 @@ delta_status delta_penalty_warm(delta_ctx *ctx, int64_t n, const double *a, cons
 delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                                   const float *x0, int32_t sweeps, double rel_tol, double *p, double *q, double *dist,
                                   uint8_t *certified);
+/* The learned hybrid narrowphase over a pair list (n < 2^32): delta_mlp_infer (skipped
+ * when params and params_bf16 are NULL: the same solver from the centroids), then
+ * delta_learned_refine, which lists the uncertified pairs on the device, then
+ * DELTA_BF_CERT over that list.  Every distance is within rel_tol of FP64 bfSolver's and
+ * every listed pair equals bfSolver bit for bit.  flags [n] (optional): 1 certified,
+ * 2 solved exactly.  n_fallback (host, optional) receives the number of listed pairs and
+ * makes the call synchronise; otherwise asynchronous. */
+delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                     const float *params, const void *params_bf16, int32_t sweeps, double rel_tol,
+                                     double *p, double *q, double *dist, uint8_t *flags, int64_t *n_fallback);
 
 #ifdef __cplusplus
 }

@@ -190,17 +190,19 @@ def test_learned_solver_vs_fp64_bf(ctx, trained, oracle, pairs, use_net):
     ea, eb = edge_case_pairs()
     a = np.concatenate([pairs[0], ea], 1)
     b = np.concatenate([pairs[1], eb], 1)
-    p, q, d, cert = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=2)
+    p, q, d, flags, nfb = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=2, count_fallback=True)
     ctx.synchronize()
-    p, q, d, cert = p.cpu().numpy(), q.cpu().numpy(), d.cpu().numpy(), cert.cpu().numpy()
+    p, q, d, flags = p.cpu().numpy(), q.cpu().numpy(), d.cpu().numpy(), flags.cpu().numpy()
+    assert set(np.unique(flags)) <= {1, 2} and nfb == int((flags == 2).sum())
     op, oq, od, _ = oracle.pairs(0, a, b)
     fin = np.isfinite(od)
     rel = np.abs(d - od)[fin] / np.maximum(od[fin], 1e-300)
     assert rel.max() <= 1e-6, rel.max()
-    fb = cert == 0
+    fb = flags == 2
     assert np.array_equal(d[fb], od[fb], equal_nan=True)
     assert np.array_equal(p[:, fb], op[:, fb], equal_nan=True)
-    assert cert.mean() > 0.5
+    assert np.array_equal(q[:, fb], oq[:, fb], equal_nan=True)
+    assert (flags == 1).mean() > 0.5
     for thr in (1e-4, 1e-3, 1e-2):
         band = np.abs(od - thr) <= 1e-6 * thr
         assert np.array_equal((d <= thr)[~band], (od <= thr)[~band])
