@@ -8,10 +8,14 @@ A step is one pass of the narrowphase over the 2^24 pairs.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Ours: the headline method (default bf_cert: FP32 feature filter + FP64 finishing, whose
-results equal FP64 bfSolver bit for bit) timed with CUDA events; the plain FP64 bf kernel
-is timed beside it on the same pairs.  `e2e` goes through the C ABI's host-buffer entry
-point (delta_pairs_run_host) with pinned host inputs, copies included.
+Ours: the headline method timed with CUDA events.  Default: the learned hybrid
+(delta_pairs_run_learned: optional MLP warm start, FP32 projections, one FP64 feature,
+FP64 separating-plane certificate at 1e-6, exact DELTA_BF_CERT for every uncertified pair)
+in the configuration its autotuner times fastest (network on or off, projection sweeps);
+the network-on and network-off arms, bf_cert and the plain FP64 bf kernel are timed beside
+it on the same pairs.  `e2e` goes through the C ABI's host-buffer entry point
+(delta_pairs_run_learned_host, or delta_pairs_run_host for a pair method) with pinned host
+inputs, copies included.
 Reference: the reference's own bfSolver (oracle/_ref, compiled from its sources) over a
 bounded sample of the same pairs on all host threads.
 """
@@ -42,7 +46,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--method", default="bf_cert")
+    ap.add_argument("--method", default="learned",
+                    help="learned (the learned hybrid, configuration autotuned) or a pair method: bf_cert, bf, ...")
+    ap.add_argument("--weights", default=None, help="warm-start checkpoint (default: the bundled one)")
     ap.add_argument("--pairs-log2", type=int, default=24)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=5)
@@ -250,62 +256,149 @@ def main():
         from datetime import timedelta
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    from delta_b200.narrowphase import METHODS, Context, pairs_device, pairs_host
+    from delta_b200.narrowphase import METHODS, Context, autotune, pairs_device, pairs_host
 
-    method = METHODS[args.method]
     stream = torch.cuda.current_stream()
     ctx = Context(local, stream.cuda_stream)
     a = torch.from_numpy(a_np).cuda()
     b = torch.from_numpy(b_np).cuda()
-    out = (torch.empty((3, n), dtype=torch.float64, device="cuda"), torch.empty((3, n), dtype=torch.float64,
-                                                                                device="cuda"),
-           torch.empty(n, dtype=torch.float64, device="cuda"), torch.empty(n, dtype=torch.uint8, device="cuda"))
-    out64 = tuple(torch.empty_like(x) for x in out)
+
+    def new_out():
+        return (torch.empty((3, n), dtype=torch.float64, device="cuda"),
+                torch.empty((3, n), dtype=torch.float64, device="cuda"),
+                torch.empty(n, dtype=torch.float64, device="cuda"), torch.empty(n, dtype=torch.uint8, device="cuda"))
+
+    out, out64 = new_out(), new_out()
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed(meth, outs, steps, warmup):
+    def timed(run, outs, steps, warmup):
         for _ in range(warmup):
-            pairs_device(ctx, meth, a, b, out=outs)
+            run(outs)
         barrier()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
         l0 = ctx.launches
         ev[0].record(stream)
         for i in range(steps):
-            pairs_device(ctx, meth, a, b, out=outs)
+            run(outs)
             ev[i + 1].record(stream)
         barrier()
         per = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
-        total = ev[0].elapsed_time(ev[steps])
-        return total, per, ctx.launches - l0
+        return ev[0].elapsed_time(ev[steps]), per, ctx.launches - l0
 
-    # launch shapes chosen by the autotuner on this rank's pairs (headline and comparison)
-    from delta_b200.narrowphase import autotune
+    def max_ranks(vals):
+        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.tolist()
 
-    tuned = {args.method: autotune(ctx, method, a, b, out=out), "bf": autotune(ctx, 0, a, b, out=out64)}
+    def pair_run(m):
+        return lambda outs: pairs_device(ctx, m, a, b, out=outs)
+
+    # launch shapes of the pair kernels chosen by the autotuner on this rank's pairs
+    tuned = {"bf_cert": autotune(ctx, METHODS["bf_cert"], a, b, out=out),
+             "bf": autotune(ctx, METHODS["bf"], a, b, out=out64)}
+    learned_info = None
+    if args.method == "learned":
+        from delta_b200.learned import WarmStartMLP, default_weights, learned_pairs, learned_pairs_host, refine, tune
+
+        model = WarmStartMLP.load(ctx, args.weights)
+        tuning = tune(ctx, model, a, b)
+        best = tuning[0]
+        use_model = model if best["network"] else None
+        sweeps, feats = best["sweeps"], best["features"]
+
+        def headline(outs):
+            return learned_pairs(ctx, use_model, a, b, sweeps, out=outs, features=feats)
+    else:
+        headline = pair_run(METHODS[args.method])
 
     peak, peak_kind = measured_peak_hbm()
     with ClockSampler(local) as clk:
-        total_ms, per_ms, launches = timed(method, out, args.steps, args.warmup)
+        total_ms, per_ms, launches = timed(headline, out, args.steps, args.warmup)
     # the plain FP64 bf kernel on the same pairs (comparison arm, not the headline)
-    total64_ms, per64_ms, launches64 = timed(0, out64, max(3, args.steps // 2), 2)
-
-    t = torch.tensor([total_ms, total64_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, total64_ms = t.tolist()
     steps64 = max(3, args.steps // 2)
+    total64_ms, per64_ms, _ = timed(pair_run(METHODS["bf"]), out64, steps64, 2)
+    total_ms, total64_ms = max_ranks([total_ms, total64_ms])
     value = world * n * args.steps / (total_ms / 1e3)
     value64 = world * n * steps64 / (total64_ms / 1e3)
 
-    # parity of the headline method against plain FP64 bf on this rank's pairs
+    # parity of the headline against plain FP64 bf on this rank's pairs
     torch.cuda.synchronize()
-    diff = ((out[0] != out64[0]).any(0) | (out[1] != out64[1]).any(0) | (out[2] != out64[2])).sum().item()
-    rel = ((out[2] - out64[2]).abs() / out64[2].clamp_min(1e-300)).max().item()
-    mean_evals = out[3].double().mean().item() if method == 5 else None
+    d, d64 = out[2], out64[2]
+    fin = torch.isfinite(d64)
+    rel = ((d - d64).abs() / d64.clamp_min(1e-300))[fin].max().item()
+    same = ((out[0] == out64[0]).all(0) & (out[1] == out64[1]).all(0) & ((d == d64) | (d.isnan() & d64.isnan())))
+    contacts = {}
+    for thr in (1e-4, 1e-3, 1e-2):
+        outside = (d64 - thr).abs() > 1e-6 * thr
+        contacts[f"{thr:g}"] = {"fp64_contacts": int((d64 <= thr).sum().item()),
+                                "mismatches_outside_band": int((((d <= thr) != (d64 <= thr)) & outside).sum().item()),
+                                "pairs_in_band": int((~outside).sum().item())}
+    parity = {"pairs_bit_identical_fraction": same.double().mean().item(), "max_rel_dist_err": rel,
+              "rel_tol": 1e-6 if args.method == "learned" else 0.0,
+              "contact_sets_at_threshold": contacts,
+              "band": "|d_fp64 - threshold| <= 1e-6 threshold"}
+
+    if args.method == "learned":
+        # comparison arms on the same pairs and the same timing protocol
+        arms = {}
+        best_on = next(r for r in tuning if r["network"])
+        best_off = next(r for r in tuning if not r["network"])
+        k = max(3, args.steps // 2)
+        arm_out = new_out()
+        for name, run in (
+                ("bf_cert", pair_run(METHODS["bf_cert"])),
+                ("learned_network_on", lambda o: learned_pairs(ctx, model, a, b, best_on["sweeps"], out=o,
+                                                               features=best_on["features"])),
+                ("learned_network_off", lambda o: learned_pairs(ctx, None, a, b, best_off["sweeps"], out=o,
+                                                                features=best_off["features"]))):
+            t_ms, _, _ = timed(run, arm_out, k, 2)
+            (t_ms,) = max_ranks([t_ms])
+            arms[name] = {"value": world * n * k / (t_ms / 1e3), "unit": "pairs/s", "ms_per_step": t_ms / k}
+        for arm, r in (("learned_network_on", best_on), ("learned_network_off", best_off)):
+            arms[arm].update(sweeps=r["sweeps"], features=r["features"], certified_fraction=r["certified_fraction"])
+        # per-kernel breakdown of the headline configuration
+        x0 = model.predict(a, b) if use_model is not None else None
+        ref_out = new_out()
+
+        def ev_time(fn, reps=max(3, args.steps // 2)):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        refine_ms = ev_time(lambda: refine(ctx, a, b, x0, sweeps, out=ref_out, features=feats))
+        infer_ms = ev_time(lambda: model.predict(a, b, out=x0)) if use_model is not None else 0.0
+        head_ms = total_ms / args.steps
+        ckpt = json.loads(default_weights().with_suffix(".json").read_text()) if args.weights is None else None
+        learned_info = {
+            "config": {"network": bool(best["network"]), "sweeps": sweeps, "features": feats,
+                       "certified_fraction": best["certified_fraction"],
+                       "chosen_by": "delta_b200.learned.tune: CUDA-event timing of every (network, sweeps, features)"},
+            "tuning": tuning,
+            "arms": arms,
+            "breakdown_ms": {"mlp_inference": infer_ms, "refine_and_certify": refine_ms,
+                             "exact_fallback_and_list": max(head_ms - refine_ms - infer_ms, 0.0)},
+            "network_gain_certified_fraction": {
+                f"sweeps{r['sweeps']}_features{r['features']}": {
+                    "network": r["certified_fraction"],
+                    "plain": next(x["certified_fraction"] for x in tuning if not x["network"] and
+                                  x["sweeps"] == r["sweeps"] and x["features"] == r["features"])}
+                for r in tuning if r["network"]},
+            "checkpoint": None if ckpt is None else {
+                "training_pairs": ckpt["training_pairs"], "epochs": ckpt["epochs"], "batch": ckpt["batch"],
+                "lr": ckpt["lr"], "train_samples_per_second": ckpt["train_samples_per_second"],
+                "eval_loss": ckpt["evaluation"]["loss"], "device": ckpt["device"]},
+        }
 
     # end to end through the C ABI with pinned host buffers
     e2e = None
@@ -316,19 +409,24 @@ def main():
         hq = torch.empty((3, n), dtype=torch.float64).pin_memory().numpy()
         hd = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
         hf = torch.empty(n, dtype=torch.uint8).pin_memory().numpy()
-        pairs_host(ctx, method, ha, hb, out=(hp, hq, hd, hf))  # warm-up (allocates scratch)
+        if args.method == "learned":
+            def host_run():
+                learned_pairs_host(ctx, use_model, ha, hb, sweeps, out=(hp, hq, hd, hf), features=feats)
+            path = "delta_pairs_run_learned_host (C ABI), pinned host buffers, copies in the timed region"
+        else:
+            def host_run():
+                pairs_host(ctx, METHODS[args.method], ha, hb, out=(hp, hq, hd, hf))
+            path = "delta_pairs_run_host (C ABI), pinned host buffers, copies in the timed region"
+        host_run()  # warm-up (allocates scratch)
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            pairs_host(ctx, method, ha, hb, out=(hp, hq, hd, hf))
+            host_run()
         barrier()
-        el = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(el, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * n * args.e2e_steps / el.item(), "unit": "pairs/s",
+        (el,) = max_ranks([time.perf_counter() - t0])
+        e2e = {"value": world * n * args.e2e_steps / el, "unit": "pairs/s",
                "h2d_bytes_per_step": int(ha.nbytes + hb.nbytes),
-               "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes),
-               "path": "delta_pairs_run_host (C ABI), pinned host buffers, copies in the timed region"}
+               "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes), "path": path}
 
     ts = hop = None
     if args.timestep_steps > 0:
@@ -354,10 +452,18 @@ def main():
                "sample": f"{min(n, 1 << 22)} pairs of the workload, reference bfSolver FP64, repeated >= 10 s"}
 
     if rank == 0:
-        kern_ms = float(np.mean(per_ms))
-        achieved = BYTES_PER_PAIR * n / (kern_ms / 1e3) / 1e9
-        kname = f"k_pairs<{args.method}>"
-        traffic = profiled_traffic(args.method, n)
+        if args.method == "learned":
+            # dominant kernel of the headline: the refine/certify kernel (or the MLP when on)
+            kname = "k_learned_refine"
+            bpp = BYTES_PER_PAIR + (16 if use_model is not None else 0)
+            kern_ms = learned_info["breakdown_ms"]["refine_and_certify"]
+            traffic = profiled_traffic("learned_refine", n)
+        else:
+            kname = f"k_pairs<{args.method}>"
+            bpp = BYTES_PER_PAIR
+            kern_ms = float(np.mean(per_ms))
+            traffic = profiled_traffic(args.method, n)
+        achieved = bpp * n / (kern_ms / 1e3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -367,13 +473,11 @@ def main():
             "fp64_bf": {"value": value64, "unit": "pairs/s", "ms_per_step": total64_ms / steps64},
             "autotuned_launch": tuned,
             "speedup_vs_fp64_bf": value / value64,
-            "parity_vs_fp64_bf": {"pairs_differing": int(diff), "max_rel_dist_err": rel,
-                                  "mean_fp64_feature_evals": mean_evals},
+            "parity_vs_fp64_bf": parity,
+            "learned": learned_info,
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic,
-                         "algorithmic_bytes_per_launch": BYTES_PER_PAIR * n,
-                         "fp64_equiv_tflops": FLOPS_BF * n / (kern_ms / 1e3) / 1e12},
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": bpp * n, "kernel_ms": kern_ms},
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "e2e": e2e,

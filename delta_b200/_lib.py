@@ -56,8 +56,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_adam": ([vp, i64, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, i64, vp], C.c_int),
     "delta_to_bf16": ([vp, i64, vp, vp], C.c_int),
     "delta_penalty_warm": ([vp, i64, vp, vp, i64, vp, f8, vp, vp, vp, vp], C.c_int),
-    "delta_learned_refine": ([vp, i64, vp, vp, i64, vp, i32, f8, vp, vp, vp, vp], C.c_int),
-    "delta_pairs_run_learned": ([vp, i64, vp, vp, i64, vp, vp, i32, f8, vp, vp, vp, vp, vp], C.c_int),
+    "delta_learned_refine": ([vp, i64, vp, vp, i64, vp, i32, i32, f8, vp, vp, vp, vp], C.c_int),
+    "delta_pairs_run_learned": ([vp, i64, vp, vp, i64, vp, vp, i32, i32, f8, vp, vp, vp, vp, vp], C.c_int),
+    "delta_pairs_run_learned_host": ([vp, i64, vp, vp, i64, vp, vp, i32, i32, f8, vp, vp, vp, vp, vp], C.c_int),
 }
 
 

@@ -123,19 +123,24 @@ __device__ __forceinline__ void write_contact(const RawContacts &rc, int64_t pos
   rc.key[pos] = ((uint64_t)r.k << 32) | ((uint64_t)r.iA << 16) | (uint64_t)tb;
 }
 
-// Warp-cooperative append of the lanes with `take` set (their order within the warp is
-// irrelevant: the key sort fixes the final order).
-__device__ __forceinline__ void emit(const RawContacts &rc, bool take, const double pq[6], const RowCtx &r, int32_t tb) {
-  const unsigned mask = __ballot_sync(kFull, take);
-  if (!mask) return;
-  const int lane = threadIdx.x & 31;
+// Slot for the calling lane in an append buffer: one atomic per group of lanes that
+// arrive together (__activemask), whatever the warp's convergence after the
+// data-dependent solver branches before the call.
+__device__ __forceinline__ int64_t agg_slot(unsigned long long *count) {
+  const unsigned grp = __activemask();
+  const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
   unsigned long long base = 0;
-  if (lane == 0) base = atomicAdd(rc.count, (unsigned long long)__popc(mask));
-  base = __shfl_sync(kFull, base, 0);
-  if (take) {
-    const int64_t pos = (int64_t)base + __popc(mask & ((1u << lane) - 1u));
-    if (pos < rc.cap) write_contact(rc, pos, pq, r, tb);
-  }
+  if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(grp));
+  base = __shfl_sync(grp, base, leader);
+  return (int64_t)base + __popc(grp & ((1u << lane) - 1u));
+}
+
+// Append of the lanes with `take` set (their order is irrelevant: the key sort fixes the
+// final order).
+__device__ __forceinline__ void emit(const RawContacts &rc, bool take, const double pq[6], const RowCtx &r, int32_t tb) {
+  if (!take) return;
+  const int64_t pos = agg_slot(rc.count);
+  if (pos < rc.cap) write_contact(rc, pos, pq, r, tb);
 }
 
 __device__ __forceinline__ int warp_sum(int v) { return __reduce_add_sync(kFull, v); }
@@ -193,13 +198,8 @@ __device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawCon
         }
         keep = g2 <= cull * cull;
       }
-      const unsigned mask = __ballot_sync(kFull, keep);
-      if (!mask) continue;
-      unsigned long long sbase = 0;
-      if (lane_ == 0) sbase = atomicAdd(rc.sv_count, (unsigned long long)__popc(mask));
-      sbase = __shfl_sync(kFull, sbase, 0);
       if (keep) {
-        const int64_t pos = (int64_t)sbase + __popc(mask & ((1u << lane_) - 1u));
+        const int64_t pos = agg_slot(rc.sv_count);
         if (pos < rc.sv_cap) rc.sv[pos] = ((uint64_t)r.k << 32) | ((uint64_t)r.iA << 16) | (uint64_t)tb;
       }
     }
@@ -233,11 +233,7 @@ __device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawCon
         // penalty.cpp:96 scans coordinate indices below nB: triangles tb with 3*tb < nB
         take = (3 * tb < r.nB) && pq_dist64(pq) <= mg;
       }
-#pragma unroll 1
-      for (int h = 0; h < 17; ++h) {
-        const int c = __popc(__ballot_sync(kFull, valid && it == h));
-        if (c && (threadIdx.x & 31) == 0) atomicAdd(&st->hist[h], (unsigned long long)c);
-      }
+      if (valid && it >= 0 && it < 17) atomicAdd(&st->hist[it], 1ull);
       emit(rc, take, pq, r, tb);
     });
   } else {

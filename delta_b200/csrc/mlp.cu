@@ -516,10 +516,12 @@ __device__ __forceinline__ void pick_vertex(const R T[3][3], int j, R out[3]) {
 // Learned hybrid solver, one pair per thread.  From the warm start x0 (barycentric
 // weights of P on A and Q on B; centroids when x0 is null), `sweeps` FP32 alternating
 // projections (Q <- closest point of B to P, P <- closest point of A to Q) locate the
-// closest points roughly.  Three bfSolver features are read off them: B's vertex nearest
-// Q against face A, A's vertex nearest P against face B, and the edge pair nearest
-// (P, Q).  The one bfSolver's rule (bf.cpp:1102: vertex-face family first, first minimum
-// in feature order, the edge pair only when strictly closer) picks on FP32 distances is
+// closest points roughly.  CAND bfSolver features are then evaluated in FP32: 3 = read off
+// the projections (B's vertex nearest Q against face A, A's vertex nearest P against face
+// B, the edge pair nearest (P, Q)); 7 = all six vertex-face features and that edge pair;
+// 11 = all six vertex-face features and the six edge pairs that contain A's or B's
+// nearest edge; 15 = all features.  The one bfSolver's rule (bf.cpp:1102: first minimum in feature order
+// within each family, the edge pair only when strictly closer) picks on FP32 distances is
 // evaluated in FP64 with the reference arithmetic (bf.cpp:586-697 or 920-1090), so a
 // pair whose closest feature was found gets bfSolver's points bit for bit.
 // FP64 certificate: with r = P - Q, every plane normal to r bounds the distance below by
@@ -527,8 +529,10 @@ __device__ __forceinline__ void pick_vertex(const R T[3][3], int j, R out[3]) {
 // |r|^2 - (min_i r.A_i - max_j r.B_j) + slack |r| <= rel_tol |r|^2, i.e. the distance is
 // within rel_tol of the true one; slack = 1e-14 max|coordinate| covers the rounding of the
 // dot products.  Intersecting triangles have no separating plane and are never certified.
-// With `list`, uncertified pairs are appended to list[*count] (warp-aggregated) and their
+// With `list`, uncertified pairs are appended to list[*count] (aggregated over the lanes
+// that reach the append together) and their
 // outputs left for the exact solver; flags then read 1 (certified) or 2 (listed).
+template <int CAND>
 __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double *__restrict__ a,
                                                         const double *__restrict__ b, int64_t ld,
                                                         const float *__restrict__ x0, int sweeps, double rel_tol,
@@ -586,18 +590,63 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
   // on face B (12 + iA); edge-edge feature 3 ea + eb joins vertices ea, ea+1 (the edge
   // opposite vertex ea+2).  Operands are selected, not indexed, so all lanes run the
   // same code whichever features they picked.
-  const int ea = (kA + 1) % 3, eb = (kB + 1) % 3;
-  float X1[3], X2[3], HA[3], TA[3], HB[3], TB[3], f0, f1;
-  pick_vertex(Bf, jB, X1);
-  pick_vertex(Af, iA, X2);
-  pick_vertex(Af, ea, HA);
-  pick_vertex(Af, (ea + 1) % 3, TA);
-  pick_vertex(Bf, eb, HB);
-  pick_vertex(Bf, (eb + 1) % 3, TB);
-  const float d1 = pt_tri_ref(Af[0], Af[1], Af[2], X1, f0, f1);
-  const float d2 = pt_tri_ref(Bf[0], Bf[1], Bf[2], X2, f0, f1);
-  const float de = seg_seg_ref(HA, TA, HB, TB, f0, f1);
-  const bool edge = (d2 < d1 ? d2 : d1) > de, faceB = d2 < d1;
+  int ea = (kA + 1) % 3, eb = (kB + 1) % 3;
+  float HA[3], TA[3], HB[3], TB[3], f0, f1;
+  bool faceB;  // chosen vertex-face feature: A's vertex vtx on face B, else B's vertex vtx on face A
+  int vtx;
+  float dpt, de;
+  if constexpr (CAND == 3) {
+    float X1[3], X2[3];
+    pick_vertex(Bf, jB, X1);
+    pick_vertex(Af, iA, X2);
+    const float d1 = pt_tri_ref(Af[0], Af[1], Af[2], X1, f0, f1);
+    const float d2 = pt_tri_ref(Bf[0], Bf[1], Bf[2], X2, f0, f1);
+    faceB = d2 < d1;
+    vtx = faceB ? iA : jB;
+    dpt = faceB ? d2 : d1;
+  } else {
+    // all six vertex-face features in bfSolver's order, first minimum kept
+    dpt = 1e30f;
+    faceB = false;
+    vtx = 0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const float dj = j < 3 ? pt_tri_ref(Af[0], Af[1], Af[2], Bf[j], f0, f1)
+                             : pt_tri_ref(Bf[0], Bf[1], Bf[2], Af[j - 3], f0, f1);
+      if (dj < dpt) { dpt = dj; faceB = j >= 3; vtx = j % 3; }
+    }
+  }
+  if constexpr (CAND == 15) {
+    // all nine edge pairs, first minimum kept
+    de = 1e30f;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const float dj = seg_seg_ref(Af[j / 3], Af[(j / 3 + 1) % 3], Bf[j % 3], Bf[(j % 3 + 1) % 3], f0, f1);
+      if (dj < de) { de = dj; ea = j / 3; eb = j % 3; }
+    }
+  } else if constexpr (CAND == 11) {
+    // the edge pairs that contain A's nearest edge or B's nearest edge; the minimum in
+    // feature order (distance, then index 3 ea + eb)
+    const int ean = ea, ebn = eb;
+    de = 1e30f;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const int xa = j < 3 ? ean : j - 3, xb = j < 3 ? j : ebn;
+      pick_vertex(Af, xa, HA);
+      pick_vertex(Af, (xa + 1) % 3, TA);
+      pick_vertex(Bf, xb, HB);
+      pick_vertex(Bf, (xb + 1) % 3, TB);
+      const float dj = seg_seg_ref(HA, TA, HB, TB, f0, f1);
+      if (dj < de || (dj == de && 3 * xa + xb < 3 * ea + eb)) { de = dj; ea = xa; eb = xb; }
+    }
+  } else {
+    pick_vertex(Af, ea, HA);
+    pick_vertex(Af, (ea + 1) % 3, TA);
+    pick_vertex(Bf, eb, HB);
+    pick_vertex(Bf, (eb + 1) % 3, TB);
+    de = seg_seg_ref(HA, TA, HB, TB, f0, f1);
+  }
+  const bool edge = dpt > de;
   xf64 pq[6];
   if (edge) {
     xf64 HA[3], TA[3], HB[3], TB[3], sc, tc;
@@ -614,8 +663,8 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
     xf64 T[3][3], X[3], sf, tf;
     for (int v = 0; v < 3; ++v)
       for (int k = 0; k < 3; ++k) T[v][k] = faceB ? B[v][k] : A[v][k];
-    if (faceB) pick_vertex(A, iA, X);
-    else pick_vertex(B, jB, X);
+    if (faceB) pick_vertex(A, vtx, X);
+    else pick_vertex(B, vtx, X);
     pt_tri_ref(T[0], T[1], T[2], X, sf, tf);
     for (int k = 0; k < 3; ++k) {  // bf.cpp:1104-1177 (pt_tri_points)
       const xf64 face = T[0][k] + ((T[2][k] - T[0][k]) * tf) + ((T[1][k] - T[0][k]) * sf);
@@ -635,18 +684,17 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
     const double d2r = d * d;
     ok = d2r - (amin - bmax) + 1e-14 * scale * d <= rel_tol * d2r;
   }
-  if (list) {
-    const bool need = valid && !ok;
-    const unsigned ballot = __ballot_sync(0xffffffffu, need);
-    const int lane = threadIdx.x & 31;
-    unsigned base = 0;
-    if (ballot) {
-      if (lane == 0) base = atomicAdd(count, (unsigned)__popc(ballot));
-      base = __shfl_sync(0xffffffffu, base, 0);
-    }
-    if (need) list[base + __popc(ballot & ((1u << lane) - 1u))] = (uint32_t)i;
-  }
   if (!valid) return;
+  if (list && !ok) {
+    // append, aggregated over the lanes that arrive here together (whatever the warp's
+    // convergence after the data-dependent branches above)
+    const unsigned grp = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    list[base + __popc(grp & ((1u << lane) - 1u))] = (uint32_t)i;
+  }
   if (ok || !list) {
     for (int k = 0; k < 3; ++k) {
       p[k * ld + i] = pq[k].v;
@@ -658,6 +706,16 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
 }
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
+
+void launch_refine(int features, cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld,
+                   const float *x0, int sweeps, double rel_tol, double *p, double *q, double *dist, uint8_t *flags,
+                   uint32_t *list, uint32_t *count) {
+  const unsigned g = nblk(n, 128);
+  if (features == 11) k_learned_refine<11><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+  else if (features == 15) k_learned_refine<15><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+  else if (features == 7) k_learned_refine<7><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+  else k_learned_refine<3><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+}
 
 }  // namespace
 
@@ -801,23 +859,25 @@ delta_status delta_penalty_warm(delta_ctx *ctx, int64_t n, const double *a, cons
 }
 
 delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
-                                  const float *x0, int32_t sweeps, double rel_tol, double *p, double *q, double *dist,
-                                  uint8_t *certified) {
-  if (!ctx || n < 0 || ld < n || sweeps < 0 || (n > 0 && (!a || !b || !p || !q || !dist || !certified)))
+                                  const float *x0, int32_t sweeps, int32_t features, double rel_tol, double *p,
+                                  double *q, double *dist, uint8_t *certified) {
+  if (!ctx || n < 0 || ld < n || sweeps < 0 || (features != 3 && features != 7 && features != 11 && features != 15) ||
+      (n > 0 && (!a || !b || !p || !q || !dist || !certified)))
     return set_error(DELTA_ERR_INVALID, "delta_learned_refine: bad argument");
   if (reinterpret_cast<uintptr_t>(x0) & 15)
     return set_error(DELTA_ERR_INVALID, "delta_learned_refine: x0 must be 16-byte aligned");
   if (n == 0) return DELTA_OK;
-  k_learned_refine<<<nblk(n, 128), 128, 0, ctx->stream>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, certified,
-                                                          nullptr, nullptr);
+  launch_refine(features, ctx->stream, n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, certified, nullptr, nullptr);
   ctx->launches += 1;
   return cuda_error(cudaGetLastError(), "delta_learned_refine");
 }
 
 delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
-                                     const float *params, const void *params_bf16, int32_t sweeps, double rel_tol,
-                                     double *p, double *q, double *dist, uint8_t *flags, int64_t *n_fallback) {
+                                     const float *params, const void *params_bf16, int32_t sweeps, int32_t features,
+                                     double rel_tol, double *p, double *q, double *dist, uint8_t *flags,
+                                     int64_t *n_fallback) {
   if (!ctx || n < 0 || ld < n || sweeps < 0 || n > (int64_t)UINT32_MAX ||
+      (features != 3 && features != 7 && features != 11 && features != 15) ||
       (n > 0 && (!a || !b || !p || !q || !dist)) || ((params == nullptr) != (params_bf16 == nullptr)))
     return set_error(DELTA_ERR_INVALID, "delta_pairs_run_learned: bad argument");
   if (n_fallback) *n_fallback = 0;
@@ -836,8 +896,7 @@ delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a,
   uint32_t *list = reinterpret_cast<uint32_t *>(static_cast<char *>(lbuf) + 256);
   cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), ctx->stream);
   if (e != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: memset");
-  k_learned_refine<<<nblk(n, 128), 128, 0, ctx->stream>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list,
-                                                          count);
+  launch_refine(features, ctx->stream, n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
   ctx->launches += 1;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: refine");
   const PairLaunch cfg = ctx->pair_launch_set[DELTA_BF_CERT][0] ? ctx->pair_launch[DELTA_BF_CERT][0]
@@ -854,6 +913,37 @@ delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a,
     *n_fallback = *static_cast<uint32_t *>(pin);
   }
   return DELTA_OK;
+}
+
+delta_status delta_pairs_run_learned_host(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                          const float *params, const void *params_bf16, int32_t sweeps,
+                                          int32_t features, double rel_tol, double *p, double *q, double *dist,
+                                          uint8_t *flags, int64_t *n_fallback) {
+  if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !p || !q || !dist)))
+    return set_error(DELTA_ERR_INVALID, "delta_pairs_run_learned_host: bad argument");
+  if (n_fallback) *n_fallback = 0;
+  if (n == 0) return DELTA_OK;
+  // device staging: a(9n) b(9n) p(3n) q(3n) dist(n) | flags(n)
+  const size_t nd = (size_t)n;
+  void *buf = nullptr, *fbuf = nullptr;
+  delta_status st;
+  if ((st = ctx_scratch(ctx, 0, sizeof(double) * 25 * nd, &buf)) != DELTA_OK) return st;
+  if ((st = ctx_scratch(ctx, 1, nd, &fbuf)) != DELTA_OK) return st;
+  double *da = (double *)buf, *db = da + 9 * nd, *dp = db + 9 * nd, *dq = dp + 3 * nd, *dd = dq + 3 * nd;
+  uint8_t *df = (uint8_t *)fbuf;
+  const size_t row = sizeof(double) * nd, pitch = sizeof(double) * (size_t)ld;
+  cudaError_t e = cudaMemcpy2DAsync(da, row, a, pitch, row, 9, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpy2DAsync(db, row, b, pitch, row, 9, cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "learned H2D");
+  if ((st = delta_pairs_run_learned(ctx, n, da, db, n, params, params_bf16, sweeps, features, rel_tol, dp, dq, dd,
+                                    flags ? df : nullptr, n_fallback)) != DELTA_OK)
+    return st;
+  e = cudaMemcpy2DAsync(p, pitch, dp, row, row, 3, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpy2DAsync(q, pitch, dq, row, row, 3, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dist, dd, row, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && flags) e = cudaMemcpyAsync(flags, df, nd, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "learned D2H");
+  return cuda_error(cudaStreamSynchronize(ctx->stream), "learned sync");
 }
 
 }  // extern "C"

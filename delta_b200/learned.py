@@ -248,7 +248,7 @@ def train(model: WarmStartMLP, X, T, valid, epochs: int = 1, batch: int = 65536,
     return losses
 
 
-def refine(ctx: Context, a, b, x0=None, sweeps: int = 2, rel_tol: float = 1e-6, out=None):
+def refine(ctx: Context, a, b, x0=None, sweeps: int = 2, rel_tol: float = 1e-6, out=None, features: int = 3):
     """delta_learned_refine: (p, q, dist, certified) for pair-list tensors a, b."""
     import torch
 
@@ -261,13 +261,13 @@ def refine(ctx: Context, a, b, x0=None, sweeps: int = 2, rel_tol: float = 1e-6, 
     else:
         p, q, d, cert = out
     check(lib().delta_learned_refine(ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0),
-                                     None if x0 is None else x0.data_ptr(), int(sweeps), float(rel_tol),
+                                     None if x0 is None else x0.data_ptr(), int(sweeps), int(features), float(rel_tol),
                                      p.data_ptr(), q.data_ptr(), d.data_ptr(), cert.data_ptr()))
     return p, q, d, cert
 
 
 def learned_pairs(ctx: Context, model: WarmStartMLP | None, a, b, sweeps: int = 2, rel_tol: float = 1e-6,
-                  out=None, count_fallback: bool = False):
+                  out=None, count_fallback: bool = False, features: int = 3):
     """The learned hybrid (delta_pairs_run_learned) over pair-list tensors a, b (9, n)
     float64 on the device.
 
@@ -289,8 +289,59 @@ def learned_pairs(ctx: Context, model: WarmStartMLP | None, a, b, sweeps: int = 
     check(lib().delta_pairs_run_learned(
         ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0),
         None if model is None else model.params.data_ptr(), None if model is None else model.params_bf16.data_ptr(),
-        int(sweeps), float(rel_tol), p.data_ptr(), q.data_ptr(), d.data_ptr(),
+        int(sweeps), int(features), float(rel_tol), p.data_ptr(), q.data_ptr(), d.data_ptr(),
         None if fl is None else fl.data_ptr(), C.byref(nf) if count_fallback else None))
     if count_fallback:
         return p, q, d, fl, int(nf.value)
     return p, q, d, fl
+
+
+def learned_pairs_host(ctx: Context, model: WarmStartMLP | None, a: np.ndarray, b: np.ndarray, sweeps: int = 1,
+                       rel_tol: float = 1e-6, out=None, features: int = 3):
+    """learned_pairs with host arrays (9, n) in and (p, q, dist, flags, n_fallback) out
+    (delta_pairs_run_learned_host: copies to and from the device inside; synchronous)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    if a.shape != b.shape or a.shape[0] != 9:
+        raise ValueError("a, b must have shape (9, n)")
+    n = a.shape[1]
+    if out is None:
+        p, q, d, fl = np.empty((3, n)), np.empty((3, n)), np.empty(n), np.empty(n, np.uint8)
+    else:
+        p, q, d, fl = out
+    nf = C.c_int64(0)
+    check(lib().delta_pairs_run_learned_host(
+        ctx.handle, n, a.ctypes.data, b.ctypes.data, n, None if model is None else model.params.data_ptr(),
+        None if model is None else model.params_bf16.data_ptr(), int(sweeps), int(features), float(rel_tol),
+        p.ctypes.data,
+        q.ctypes.data, d.ctypes.data, None if fl is None else fl.ctypes.data, C.byref(nf)))
+    return p, q, d, fl, int(nf.value)
+
+
+def tune(ctx: Context, model: WarmStartMLP | None, a, b, sweeps=(0, 1, 2), features=(3, 7, 11, 15), reps: int = 3):
+    """The learned solver's autotuner: times delta_pairs_run_learned on device pairs a, b
+    for each (network on/off, sweeps, candidate features) with CUDA events and returns the
+    configurations sorted fastest first ({"network", "sweeps", "features", "ms",
+    "certified_fraction"})."""
+    import torch
+
+    n = a.shape[1]
+    out = (torch.empty((3, n), dtype=torch.float64, device=a.device), torch.empty((3, n), dtype=torch.float64,
+                                                                                  device=a.device),
+           torch.empty(n, dtype=torch.float64, device=a.device), torch.empty(n, dtype=torch.uint8, device=a.device))
+    stream = torch.cuda.current_stream(a.device)
+    res = []
+    for net in ((True, False) if model is not None else (False,)):
+        for s in sweeps:
+            for f in features:
+                m = model if net else None
+                nf = learned_pairs(ctx, m, a, b, s, out=out, count_fallback=True, features=f)[4]
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    learned_pairs(ctx, m, a, b, s, out=out, features=f)
+                e1.record(stream)
+                e1.synchronize()
+                res.append({"network": net, "sweeps": s, "features": f, "ms": e0.elapsed_time(e1) / reps,
+                            "certified_fraction": 1.0 - nf / n})
+    return sorted(res, key=lambda r: r["ms"])

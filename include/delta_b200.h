@@ -315,18 +315,21 @@ delta_status delta_penalty_warm(delta_ctx *ctx, int64_t n, const double *a, cons
                                 const float *x0, double max_error, double *p, double *q, double *dist,
                                 uint8_t *iterations);
 /* The learned solver.  From x0 [n][4] (16-byte aligned; NULL: the centroids), `sweeps`
- * FP32 alternating closest-point projections between the triangles; the closest points
- * found name three bfSolver features (B's nearest vertex against face A, A's nearest
- * vertex against face B, the nearest edge pair), which are evaluated in FP64 with the
- * reference arithmetic and chosen between by bfSolver's rule (bf.cpp:1102): p, q, dist.
+ * FP32 alternating closest-point projections between the triangles; then `features`
+ * bfSolver features are evaluated in FP32: 3 = those the projections name (B's nearest
+ * vertex against face A, A's nearest vertex against face B, the nearest edge pair), 7 = all
+ * six vertex-face features and that edge pair, 11 = all six vertex-face features and the
+ * six edge pairs containing A's or B's nearest edge, 15 = all.  The one bfSolver's rule
+ * (bf.cpp:1102) picks among them is evaluated in FP64 with the reference arithmetic: p, q,
+ * dist.
  * Then an FP64 separating-plane certificate: with r = p - q, every plane normal to r
  * bounds the distance below by min_i r.A_i/|r| - max_j r.B_j/|r|; certified [n] is 1 when
  * |r| exceeds that bound by at most rel_tol |r|, so dist is within rel_tol of the true
  * distance.  Intersecting triangles are never certified; uncertified pairs are for
  * DELTA_BF_CERT. */
 delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
-                                  const float *x0, int32_t sweeps, double rel_tol, double *p, double *q, double *dist,
-                                  uint8_t *certified);
+                                  const float *x0, int32_t sweeps, int32_t features, double rel_tol, double *p,
+                                  double *q, double *dist, uint8_t *certified);
 /* The learned hybrid narrowphase over a pair list (n < 2^32): delta_mlp_infer (skipped
  * when params and params_bf16 are NULL: the same solver from the centroids), then
  * delta_learned_refine, which lists the uncertified pairs on the device, then
@@ -335,8 +338,16 @@ delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, co
  * 2 solved exactly.  n_fallback (host, optional) receives the number of listed pairs and
  * makes the call synchronise; otherwise asynchronous. */
 delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
-                                     const float *params, const void *params_bf16, int32_t sweeps, double rel_tol,
-                                     double *p, double *q, double *dist, uint8_t *flags, int64_t *n_fallback);
+                                     const float *params, const void *params_bf16, int32_t sweeps, int32_t features,
+                                     double rel_tol, double *p, double *q, double *dist, uint8_t *flags,
+                                     int64_t *n_fallback);
+/* Same with host pair buffers (a, b, p, q, dist, flags; row pitch ld): copies in, runs,
+ * copies out and synchronises.  params / params_bf16 stay device pointers (the network
+ * is loaded once). */
+delta_status delta_pairs_run_learned_host(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                          const float *params, const void *params_bf16, int32_t sweeps,
+                                          int32_t features, double rel_tol, double *p, double *q, double *dist,
+                                          uint8_t *flags, int64_t *n_fallback);
 
 #ifdef __cplusplus
 }

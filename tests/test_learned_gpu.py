@@ -178,8 +178,9 @@ def test_trained_network_beats_centroid_start(ctx, trained, pairs):
         assert c_net > c_plain, (sweeps, c_net, c_plain)
 
 
+@pytest.mark.parametrize("features", [3, 7, 11, 15])
 @pytest.mark.parametrize("use_net", [True, False])
-def test_learned_solver_vs_fp64_bf(ctx, trained, oracle, pairs, use_net):
+def test_learned_solver_vs_fp64_bf(ctx, trained, oracle, pairs, use_net, features):
     """Every pair within 1e-6 relative distance of FP64 bfSolver; uncertified pairs
     (fallback) bit-exact; contact sets equal outside the 1e-6 band of the threshold."""
     from delta_b200.learned import learned_pairs
@@ -190,7 +191,8 @@ def test_learned_solver_vs_fp64_bf(ctx, trained, oracle, pairs, use_net):
     ea, eb = edge_case_pairs()
     a = np.concatenate([pairs[0], ea], 1)
     b = np.concatenate([pairs[1], eb], 1)
-    p, q, d, flags, nfb = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=2, count_fallback=True)
+    p, q, d, flags, nfb = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=2, count_fallback=True,
+                                        features=features)
     ctx.synchronize()
     p, q, d, flags = p.cpu().numpy(), q.cpu().numpy(), d.cpu().numpy(), flags.cpu().numpy()
     assert set(np.unique(flags)) <= {1, 2} and nfb == int((flags == 2).sum())
@@ -206,3 +208,27 @@ def test_learned_solver_vs_fp64_bf(ctx, trained, oracle, pairs, use_net):
     for thr in (1e-4, 1e-3, 1e-2):
         band = np.abs(od - thr) <= 1e-6 * thr
         assert np.array_equal((d <= thr)[~band], (od <= thr)[~band])
+
+
+def test_learned_host_entry_equals_device_entry(ctx, trained, pairs):
+    """delta_pairs_run_learned_host gives the device entry point's results bit for bit."""
+    from delta_b200.learned import learned_pairs, learned_pairs_host
+
+    a, b = pairs[0][:, :20000], pairs[1][:, :20000]
+    model = trained[0]
+    p, q, d, fl, nf = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=1, count_fallback=True, features=7)
+    hp, hq, hd, hfl, hnf = learned_pairs_host(ctx, model, a, b, sweeps=1, features=7)
+    assert nf == hnf
+    assert np.array_equal(p.cpu().numpy(), hp) and np.array_equal(q.cpu().numpy(), hq)
+    assert np.array_equal(d.cpu().numpy(), hd) and np.array_equal(fl.cpu().numpy(), hfl)
+
+
+def test_learned_rejects_bad_arguments(ctx, pairs):
+    from delta_b200._lib import DeltaError
+    from delta_b200.learned import learned_pairs
+
+    a, b = _dev(pairs[0][:, :100]), _dev(pairs[1][:, :100])
+    with pytest.raises(DeltaError):
+        learned_pairs(ctx, None, a, b, sweeps=1, features=5)
+    with pytest.raises(DeltaError):
+        learned_pairs(ctx, None, a, b, sweeps=-1)
