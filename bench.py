@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--method", default="learned",
                     help="learned (the learned hybrid, configuration autotuned) or a pair method: bf_cert, bf, ...")
     ap.add_argument("--weights", default=None, help="warm-start checkpoint (default: the bundled one)")
+    ap.add_argument("--learned-config", default="auto",
+                    help="auto (autotuned) or network:sweeps:features, e.g. off:1:3, to pin the learned hybrid's "
+                         "setting (no tuning, no comparison arms)")
     ap.add_argument("--pairs-log2", type=int, default=24)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=5)
@@ -306,8 +309,14 @@ def main():
         from delta_b200.learned import WarmStartMLP, default_weights, learned_pairs, learned_pairs_host, refine, tune
 
         model = WarmStartMLP.load(ctx, args.weights)
-        tuning = tune(ctx, model, a, b)
-        best = tuning[0]
+        if args.learned_config == "auto":
+            tuning = tune(ctx, model, a, b)
+            best = tuning[0]
+        else:
+            net_s, sw_s, f_s = args.learned_config.split(":")
+            best = {"network": net_s == "on", "sweeps": int(sw_s), "features": int(f_s),
+                    "certified_fraction": None}
+            tuning = [best]
         use_model = model if best["network"] else None
         sweeps, feats = best["sweeps"], best["features"]
 
@@ -346,21 +355,24 @@ def main():
     if args.method == "learned":
         # comparison arms on the same pairs and the same timing protocol
         arms = {}
-        best_on = next(r for r in tuning if r["network"])
-        best_off = next(r for r in tuning if not r["network"])
+        best_on = next((r for r in tuning if r["network"]), None)
+        best_off = next((r for r in tuning if not r["network"]), None)
         k = max(3, args.steps // 2)
         arm_out = new_out()
-        for name, run in (
-                ("bf_cert", pair_run(METHODS["bf_cert"])),
+        arm_runs = [("bf_cert", pair_run(METHODS["bf_cert"]), None)]
+        if args.learned_config == "auto":
+            arm_runs += [
                 ("learned_network_on", lambda o: learned_pairs(ctx, model, a, b, best_on["sweeps"], out=o,
-                                                               features=best_on["features"])),
+                                                               features=best_on["features"]), best_on),
                 ("learned_network_off", lambda o: learned_pairs(ctx, None, a, b, best_off["sweeps"], out=o,
-                                                                features=best_off["features"]))):
+                                                                features=best_off["features"]), best_off)]
+        for name, run, r in arm_runs:
             t_ms, _, _ = timed(run, arm_out, k, 2)
             (t_ms,) = max_ranks([t_ms])
             arms[name] = {"value": world * n * k / (t_ms / 1e3), "unit": "pairs/s", "ms_per_step": t_ms / k}
-        for arm, r in (("learned_network_on", best_on), ("learned_network_off", best_off)):
-            arms[arm].update(sweeps=r["sweeps"], features=r["features"], certified_fraction=r["certified_fraction"])
+            if r is not None:
+                arms[name].update(sweeps=r["sweeps"], features=r["features"],
+                                  certified_fraction=r["certified_fraction"])
         # per-kernel breakdown of the headline configuration
         x0 = model.predict(a, b) if use_model is not None else None
         ref_out = new_out()
@@ -391,8 +403,8 @@ def main():
             "network_gain_certified_fraction": {
                 f"sweeps{r['sweeps']}_features{r['features']}": {
                     "network": r["certified_fraction"],
-                    "plain": next(x["certified_fraction"] for x in tuning if not x["network"] and
-                                  x["sweeps"] == r["sweeps"] and x["features"] == r["features"])}
+                    "plain": next((x["certified_fraction"] for x in tuning if not x["network"] and
+                                   x["sweeps"] == r["sweeps"] and x["features"] == r["features"]), None)}
                 for r in tuning if r["network"]},
             "checkpoint": None if ckpt is None else {
                 "training_pairs": ckpt["training_pairs"], "epochs": ckpt["epochs"], "batch": ckpt["batch"],
