@@ -46,6 +46,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_sim_destroy": ([vp], C.c_int),
     "delta_mlp_layout": ([vp], C.c_int),
     "delta_mlp_infer": ([vp, i64, vp, vp, i64, vp, vp, vp], C.c_int),
+    "delta_mlp_infer_tcgen05": ([vp, i64, vp, vp, i64, vp, vp, vp], C.c_int),
+    "delta_mlp_set_engine": ([vp, C.c_int], C.c_int),
     "delta_mlp_features": ([vp, i64, vp, vp, i64, vp, vp, vp, vp, vp], C.c_int),
     "delta_gemm_bf16": ([vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int,
                          C.c_int, C.c_int], C.c_int),

@@ -69,7 +69,8 @@ struct delta_ctx {
   // launch shapes of the pair kernels [method][precision], set by autotuning
   delta::PairLaunch pair_launch[6][2];
   bool pair_launch_set[6][2] = {};
-  delta_buffer scratch[16];
+  delta_buffer scratch[24];
+  int mlp_engine = DELTA_MLP_TCGEN05;  // network engine of the learned hybrid
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
 };

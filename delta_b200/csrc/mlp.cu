@@ -437,6 +437,244 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2)
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// fused inference on the 5th-generation tensor cores (tcgen05, accumulators in TMEM).
+// One CTA = 8 warps = 256 threads works on tiles of 128 pairs: pair r of the tile is row r
+// of every layer's M=128 MMA and TMEM lane r of its accumulator; warps w and w+4 both read
+// lanes 32(w%4)..32(w%4)+31 (the TMEM lanes a warp may access), w < 4 columns 0..63 and
+// w >= 4 columns 64..127.  Two CTAs fit on an SM, so one's MMAs overlap the other's
+// epilogue.
+// Operands live in shared memory in the canonical K-major layout without swizzle:
+// element (r, k) of a [rows][K] BF16 matrix sits at (r/8)*SBO + (k/8)*128 + (r%8)*16 +
+// (k%8)*2 bytes (8x8 core matrices of 128 bytes; LBO = 128 between K neighbours, SBO =
+// 16*K between row groups).  One thread issues the MMAs of a layer (K/16 of them,
+// 128x128x16 or 128x16x16), commits them to an mbarrier, and every thread then reads its
+// row of the accumulator with tcgen05.ld, adds the bias, applies GELU and writes the BF16
+// row back as the next layer's A operand.  Waits on the mbarrier are bounded: on time-out
+// the kernel records it in *err, stops, and frees its TMEM.
+// ---------------------------------------------------------------------------------------
+constexpr int kTcRows = 128;          // pairs per tile = MMA M
+constexpr uint32_t kTmemCols = 128;   // FP32 accumulator columns (N of the hidden layers)
+constexpr int kTcW4Rows = 16;         // W4 padded to N = 16
+constexpr uint32_t kTcSpin = 1u << 22;  // mbarrier polls before giving up
+
+struct TcSmem {
+  __nv_bfloat16 w1[kHid * kIn];         // 8 KB   (N=128, K=32)
+  __nv_bfloat16 w2[kHid * kHid];        // 32 KB  (N=128, K=128)
+  __nv_bfloat16 w3[kHid * kHid];        // 32 KB
+  __nv_bfloat16 w4[kTcW4Rows * kHid];   // 4 KB   (N=16, K=128; rows 4..15 zero)
+  __nv_bfloat16 ah[kTcRows * kHid];     // 32 KB  A operand: layer-1 input (K=32) or hidden (K=128)
+  float bias[3 * kHid + kTcW4Rows];
+  uint64_t mbar;
+  uint32_t tmem_base;
+  int abort;
+};
+
+// byte offset of the 16-byte chunk (row r, k-chunk kc) in a canonical K-major tile
+__device__ __forceinline__ uint32_t tc_chunk(int r, int kc, int K) {
+  return (uint32_t)((r >> 3) * (16 * K) + kc * 128 + (r & 7) * 16);
+}
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t smem_addr, uint32_t sbo) {
+  // start address >> 4 [0,14), LBO >> 4 [16,30) = 128 B, SBO >> 4 [32,46), version 1 at
+  // bit 46, base offset 0, no swizzle
+  return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: F32 accumulator, BF16 A and B, both K-major, M x N
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *mbar) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(mbar);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(a) : "memory");
+}
+
+// bounded wait for the mbarrier phase with parity `phase`; false on time-out
+__device__ __forceinline__ bool tc_wait(uint64_t *mbar, uint32_t phase) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(mbar);
+  for (uint32_t it = 0; it < kTcSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 32 consecutive FP32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float v[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// copy a row-major [rows][K] BF16 matrix (global, 16-byte aligned rows) into the canonical
+// layout; rows at or beyond `valid_rows` are zero
+__device__ __forceinline__ void tc_stage(__nv_bfloat16 *dst, const __nv_bfloat16 *src, int rows, int valid_rows,
+                                         int K) {
+  const int chunks = K / 8;
+  for (int e = threadIdx.x; e < rows * chunks; e += blockDim.x) {
+    const int r = e / chunks, kc = e % chunks;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (r < valid_rows) v = __ldg(reinterpret_cast<const uint4 *>(src + (size_t)r * K + kc * 8));
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(dst) + tc_chunk(r, kc, K)) = v;
+  }
+}
+
+// one layer: the elected thread issues K/16 MMAs into TMEM and commits; everyone waits.
+// Returns false (and sets the CTA's abort flag) when the wait timed out.
+__device__ __forceinline__ bool tc_layer(TcSmem &sm, const __nv_bfloat16 *A, const __nv_bfloat16 *W, int K, int N,
+                                         uint32_t &phase) {
+  // make the generic-proxy stores of A visible to the tensor cores, then synchronise
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (threadIdx.x == 0) {
+    const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(A), w0 = (uint32_t)__cvta_generic_to_shared(W);
+    const uint32_t idesc = tc_idesc(kTcRows, N);
+    for (int s = 0; s < K / 16; ++s)
+      tc_mma(sm.tmem_base, tc_desc(a0 + 256u * s, 16u * K), tc_desc(w0 + 256u * s, 16u * K), idesc, s > 0 ? 1u : 0u);
+    tc_commit(&sm.mbar);
+    if (!tc_wait(&sm.mbar, phase)) sm.abort = 1;
+  }
+  __syncthreads();
+  phase ^= 1u;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  return sm.abort == 0;
+}
+
+constexpr int kTcThreads = 2 * kTcRows;
+
+__global__ void __launch_bounds__(kTcThreads, 2)
+    k_mlp_infer_tc(int64_t n, const __nv_bfloat16 *__restrict__ feat, const float *__restrict__ params,
+                   const __nv_bfloat16 *__restrict__ wb, float *__restrict__ x0, int *__restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  tc_stage(sm.w1, wb + kOffW1, kHid, kHid, kIn);
+  tc_stage(sm.w2, wb + kOffW2, kHid, kHid, kHid);
+  tc_stage(sm.w3, wb + kOffW3, kHid, kHid, kHid);
+  tc_stage(sm.w4, wb + kOffW4, kTcW4Rows, kOut, kHid);
+  for (int e = tid; e < kHid; e += blockDim.x) {
+    sm.bias[e] = params[kOffB1 + e];
+    sm.bias[kHid + e] = params[kOffB2 + e];
+    sm.bias[2 * kHid + e] = params[kOffB3 + e];
+  }
+  if (tid < kTcW4Rows) sm.bias[3 * kHid + tid] = tid < kOut ? params[kOffB4 + tid] : 0.f;
+  if (tid == 0) {
+    sm.abort = 0;
+    const unsigned a = (unsigned)__cvta_generic_to_shared(&sm.mbar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(&sm.tmem_base);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const int r = tid & (kTcRows - 1), half = tid >> 7;  // row of the tile, column half
+  // this thread's TMEM lane (row) in bits 16..31 of the address, column in bits 0..15
+  const uint32_t tlane = sm.tmem_base + ((uint32_t)((warp & 3) * 32) << 16);
+  uint32_t phase = 0;
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t row = tile * kTcRows + r;
+    // layer-1 input: two of the row's four 16-byte feature chunks per thread
+    {
+      const uint4 *src = reinterpret_cast<const uint4 *>(feat + 32 * (row < n ? row : n - 1));
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int kc = 2 * half + q;
+        *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(sm.ah) + tc_chunk(r, kc, kIn)) = __ldg(src + kc);
+      }
+    }
+    int K = kIn;
+    const __nv_bfloat16 *Ws[3] = {sm.w1, sm.w2, sm.w3};
+    bool ok = true;
+    for (int l = 0; l < 3; ++l) {
+      ok = tc_layer(sm, sm.ah, Ws[l], K, kHid, phase);
+      if (!ok) break;
+      // bias + GELU of this thread's 64 columns of its row, into the hidden A tile
+#pragma unroll 1
+      for (int c = 64 * half; c < 64 * half + 64; c += 32) {
+        float v[32];
+        tc_ld32(tlane + (uint32_t)c, v);
+        uint32_t w[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+          w[k] = pack_bf16(gelu(v[2 * k] + sm.bias[l * kHid + c + 2 * k]),
+                           gelu(v[2 * k + 1] + sm.bias[l * kHid + c + 2 * k + 1]));
+        char *dst = reinterpret_cast<char *>(sm.ah);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4 *>(dst + tc_chunk(r, c / 8 + q, kHid)) =
+              make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+      }
+      K = kHid;
+    }
+    if (!ok) break;
+    if (!tc_layer(sm, sm.ah, sm.w4, kHid, kTcW4Rows, phase)) break;
+    if (half == 0) {
+      float v[16];
+      tc_ld16(tlane, v);
+      if (row < n)
+        *reinterpret_cast<float4 *>(x0 + 4 * row) =
+            make_float4(v[0] + sm.bias[3 * kHid], v[1] + sm.bias[3 * kHid + 1], v[2] + sm.bias[3 * kHid + 2],
+                        v[3] + sm.bias[3 * kHid + 3]);
+    }
+  }
+  if (sm.abort && tid == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem_base), "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
 // penaltySolver (penalty.cpp:434-582, adaptive, FP64 reference arithmetic) started from
 // x0 (4 floats per pair) instead of 0.33; iterations written to iters.
 __global__ void k_penalty_warm(int64_t n, const double *a, const double *b, int64_t ld, const float *x0,
@@ -707,6 +945,67 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
 
+// Features into scratch, then the network on `engine`; with the tcgen05 engine *err_out
+// receives the device time-out flag (zeroed here, set by the kernel).
+delta_status mlp_infer_launch(delta_ctx *ctx, int engine, int64_t n, const double *a, const double *b, int64_t ld,
+                              const float *params, const void *params_bf16, float *x0, int **err_out) {
+  void *fbuf;
+  delta_status st = ctx_scratch(ctx, 15, sizeof(__nv_bfloat16) * 32 * (size_t)n, &fbuf);
+  if (st != DELTA_OK) return st;
+  __nv_bfloat16 *feat = static_cast<__nv_bfloat16 *>(fbuf);
+  k_canon<<<nblk(n), 256, 0, ctx->stream>>>(n, a, b, ld, nullptr, nullptr, feat, nullptr, nullptr);
+  ctx->launches += 1;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "mlp features");
+  const __nv_bfloat16 *wb = static_cast<const __nv_bfloat16 *>(params_bf16);
+  if (engine == DELTA_MLP_TCGEN05) {
+    void *ebuf;
+    if ((st = ctx_scratch(ctx, 16, sizeof(int), &ebuf)) != DELTA_OK) return st;
+    int *err = static_cast<int *>(ebuf);
+    if ((e = cudaMemsetAsync(err, 0, sizeof(int), ctx->stream)) != cudaSuccess) return cuda_error(e, "mlp flag");
+    static thread_local int configured_device = -1;
+    if (configured_device != ctx->device) {
+      e = cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem));
+      if (e != cudaSuccess) return cuda_error(e, "mlp tcgen05: shared memory attribute");
+      configured_device = ctx->device;
+    }
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    const unsigned grid = (unsigned)std::min<int64_t>(tiles, 2 * kNumSMs);
+    k_mlp_infer_tc<<<grid, kTcThreads, sizeof(TcSmem), ctx->stream>>>(n, feat, params, wb, x0, err);
+    if (err_out) *err_out = err;
+  } else {
+    static thread_local int configured_device = -1;
+    if (configured_device != ctx->device) {
+      e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
+      if (e != cudaSuccess) return cuda_error(e, "mlp mma: shared memory attribute");
+      configured_device = ctx->device;
+    }
+    const int64_t tiles = (n + 15) / 16;
+    const int64_t want = (tiles + kInferWarps - 1) / kInferWarps;
+    const unsigned grid = (unsigned)std::min<int64_t>(want, 2 * kNumSMs);
+    k_mlp_infer<<<grid, 32 * kInferWarps, sizeof(InferSmem), ctx->stream>>>(n, feat, params, wb, x0);
+    if (err_out) *err_out = nullptr;
+  }
+  ctx->launches += 1;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "mlp network");
+  return DELTA_OK;
+}
+
+// Synchronises and reports the tcgen05 kernel's time-out flag (err may be null).
+delta_status mlp_check_error(delta_ctx *ctx, const int *err) {
+  if (!err) return DELTA_OK;
+  void *pin;
+  delta_status st = ctx_pinned(ctx, sizeof(int), &pin);
+  if (st != DELTA_OK) return st;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(pin, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_error(e, "mlp status");
+  if (*static_cast<int *>(pin))
+    return set_error(DELTA_ERR_TIMEOUT, "tcgen05 inference: bounded wait for the tensor cores gave up");
+  return DELTA_OK;
+}
+
 void launch_refine(int features, cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld,
                    const float *x0, int sweeps, double rel_tol, double *p, double *q, double *dist, uint8_t *flags,
                    uint32_t *list, uint32_t *count) {
@@ -817,34 +1116,34 @@ delta_status delta_mlp_layout(int64_t offsets[9]) {
   return DELTA_OK;
 }
 
+delta_status delta_mlp_set_engine(delta_ctx *ctx, int engine) {
+  if (!ctx || (engine != DELTA_MLP_TCGEN05 && engine != DELTA_MLP_MMA_SYNC))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_set_engine: unknown engine");
+  ctx->mlp_engine = engine;
+  return DELTA_OK;
+}
+
 delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                              const float *params, const void *params_bf16, float *x0) {
   if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !params || !params_bf16 || !x0)))
     return set_error(DELTA_ERR_INVALID, "delta_mlp_infer: bad argument");
-  if ((reinterpret_cast<uintptr_t>(params_bf16) & 3) || (reinterpret_cast<uintptr_t>(x0) & 7))
-    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer: params_bf16 must be 4-byte and x0 8-byte aligned");
+  if ((reinterpret_cast<uintptr_t>(params_bf16) & 15) || (reinterpret_cast<uintptr_t>(x0) & 15))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer: params_bf16 and x0 must be 16-byte aligned");
   if (n == 0) return DELTA_OK;
-  void *fbuf;
-  delta_status st = ctx_scratch(ctx, 15, sizeof(__nv_bfloat16) * 32 * (size_t)n, &fbuf);
+  return mlp_infer_launch(ctx, DELTA_MLP_MMA_SYNC, n, a, b, ld, params, params_bf16, x0, nullptr);
+}
+
+delta_status delta_mlp_infer_tcgen05(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                     const float *params, const void *params_bf16, float *x0) {
+  if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !params || !params_bf16 || !x0)))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer_tcgen05: bad argument");
+  if ((reinterpret_cast<uintptr_t>(params_bf16) & 15) || (reinterpret_cast<uintptr_t>(x0) & 15))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer_tcgen05: params_bf16 and x0 must be 16-byte aligned");
+  if (n == 0) return DELTA_OK;
+  int *err = nullptr;
+  delta_status st = mlp_infer_launch(ctx, DELTA_MLP_TCGEN05, n, a, b, ld, params, params_bf16, x0, &err);
   if (st != DELTA_OK) return st;
-  __nv_bfloat16 *feat = static_cast<__nv_bfloat16 *>(fbuf);
-  k_canon<<<nblk(n), 256, 0, ctx->stream>>>(n, a, b, ld, nullptr, nullptr, feat, nullptr, nullptr);
-  ctx->launches += 1;
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_error(e, "delta_mlp_infer: features");
-  static thread_local int configured_device = -1;
-  if (configured_device != ctx->device) {
-    e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
-    if (e != cudaSuccess) return cuda_error(e, "delta_mlp_infer: shared memory attribute");
-    configured_device = ctx->device;
-  }
-  const int64_t tiles = (n + 15) / 16;
-  const int64_t want = (tiles + kInferWarps - 1) / kInferWarps;
-  const unsigned grid = (unsigned)std::min<int64_t>(want, 2 * kNumSMs);
-  k_mlp_infer<<<grid, 32 * kInferWarps, sizeof(InferSmem), ctx->stream>>>(n, feat, params,
-                                                                          (const __nv_bfloat16 *)params_bf16, x0);
-  ctx->launches += 1;
-  return cuda_error(cudaGetLastError(), "delta_mlp_infer");
+  return mlp_check_error(ctx, err);
 }
 
 delta_status delta_penalty_warm(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
@@ -884,11 +1183,15 @@ delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a,
   if (n == 0) return DELTA_OK;
   delta_status st;
   float *x0 = nullptr;
+  int *mlp_err = nullptr;
   if (params) {
     void *buf;
     if ((st = ctx_scratch(ctx, 13, sizeof(float) * 4 * (size_t)n, &buf)) != DELTA_OK) return st;
     x0 = static_cast<float *>(buf);
-    if ((st = delta_mlp_infer(ctx, n, a, b, ld, params, params_bf16, x0)) != DELTA_OK) return st;
+    if ((reinterpret_cast<uintptr_t>(params_bf16) & 15))
+      return set_error(DELTA_ERR_INVALID, "delta_pairs_run_learned: params_bf16 must be 16-byte aligned");
+    if ((st = mlp_infer_launch(ctx, ctx->mlp_engine, n, a, b, ld, params, params_bf16, x0, &mlp_err)) != DELTA_OK)
+      return st;
   }
   void *lbuf;
   if ((st = ctx_scratch(ctx, 14, 256 + sizeof(uint32_t) * (size_t)n, &lbuf)) != DELTA_OK) return st;
@@ -911,6 +1214,9 @@ delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a,
         (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
       return cuda_error(e, "delta_pairs_run_learned: count");
     *n_fallback = *static_cast<uint32_t *>(pin);
+    // the warm start only steers the search (every result is certified or exact), but a
+    // tensor-core time-out is still reported
+    return mlp_check_error(ctx, mlp_err);
   }
   return DELTA_OK;
 }

@@ -190,15 +190,26 @@ class WarmStartMLP:
         self.adam(lr)
 
     # -- inference ---------------------------------------------------------------------
-    def predict(self, a, b, out=None):
-        """x0 (n, 4) FP32 for pair-list tensors a, b (9, n) on the device: one fused kernel."""
+    def predict(self, a, b, out=None, engine: str = "mma"):
+        """x0 (n, 4) FP32 for pair-list tensors a, b (9, n) on the device: the features
+        kernel and one fused network kernel, on the mma.sync tensor-core path ("mma") or
+        the tcgen05/TMEM path ("tcgen05", synchronous)."""
         import torch
 
         n = a.shape[1]
         x0 = out if out is not None else torch.empty((n, OUT), dtype=torch.float32, device=a.device)
-        check(lib().delta_mlp_infer(self.ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0),
-                                    self.params.data_ptr(), self.params_bf16.data_ptr(), x0.data_ptr()))
+        fn = lib().delta_mlp_infer_tcgen05 if engine == "tcgen05" else lib().delta_mlp_infer
+        check(fn(self.ctx.handle, n, a.data_ptr(), b.data_ptr(), a.stride(0), self.params.data_ptr(),
+                 self.params_bf16.data_ptr(), x0.data_ptr()))
         return x0
+
+
+ENGINES = {"tcgen05": 0, "mma": 1}
+
+
+def set_engine(ctx: Context, engine: str):
+    """Network engine of the learned hybrid on this context: "tcgen05" (default) or "mma"."""
+    check(lib().delta_mlp_set_engine(ctx.handle, ENGINES[engine]))
 
 
 def features(ctx: Context, a, b, p=None, q=None):

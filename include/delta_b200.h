@@ -272,12 +272,25 @@ delta_status delta_sim_destroy(delta_sim *sim);
  * the flat parameter array, and [8] its length.  The FP32 master copy and the BF16 copy
  * share this layout; W1's columns 18..31 multiply zero features. */
 delta_status delta_mlp_layout(int64_t offsets[9]);
-/* Inference in one kernel: features, the four layers and x0 [n][4] (FP32).  params is the
- * FP32 array (biases are read from it), params_bf16 the BF16 copy (weights); x0 8-byte
- * aligned.  Equal bit for bit to delta_mlp_features + delta_gemm_bf16 + delta_mlp_bias_act
- * layer by layer. */
+/* Inference: the features kernel, then the four layers in one kernel on the mma.sync
+ * path, into x0 [n][4] (FP32).  params is the FP32 array (biases are read from it),
+ * params_bf16 the BF16 copy (weights); both x0 and params_bf16 16-byte aligned.  Equal bit
+ * for bit to delta_mlp_features + delta_gemm_bf16 + delta_mlp_bias_act layer by layer. */
 delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                              const float *params, const void *params_bf16, float *x0);
+/* Network engines of the learned hybrid (delta_pairs_run_learned): the 5th-generation
+ * tensor cores (tcgen05 MMAs, TMEM accumulators; the default) or the warp-level
+ * mma.sync path. */
+#define DELTA_MLP_TCGEN05 0
+#define DELTA_MLP_MMA_SYNC 1
+delta_status delta_mlp_set_engine(delta_ctx *ctx, int engine);
+/* delta_mlp_infer on the 5th-generation tensor cores (tcgen05 MMAs with TMEM
+ * accumulators): same network and features, FP32 accumulation in a different order, so
+ * x0 agrees with delta_mlp_infer to BF16 rounding rather than bit for bit.  params_bf16 and
+ * x0 16-byte aligned.  Synchronises; DELTA_ERR_TIMEOUT if a bounded wait for the tensor
+ * cores gave up (x0 is then incomplete). */
+delta_status delta_mlp_infer_tcgen05(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                                     const float *params, const void *params_bf16, float *x0);
 /* Canonical features: triangle A's frame (origin at its centroid, x along A1-A0, z along
  * its normal, unit = its longest edge), the six vertices in that frame as 18 BF16 values
  * padded with zeros to rows of 32 (features_bf16 [n][32]).  With p, q (closest points,
@@ -336,7 +349,9 @@ delta_status delta_learned_refine(delta_ctx *ctx, int64_t n, const double *a, co
  * DELTA_BF_CERT over that list.  Every distance is within rel_tol of FP64 bfSolver's and
  * every listed pair equals bfSolver bit for bit.  flags [n] (optional): 1 certified,
  * 2 solved exactly.  n_fallback (host, optional) receives the number of listed pairs and
- * makes the call synchronise; otherwise asynchronous. */
+ * makes the call synchronise (and report a tensor-core time-out of the network as
+ * DELTA_ERR_TIMEOUT); otherwise asynchronous.  The network runs on the context's engine
+ * (delta_mlp_set_engine). */
 delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                                      const float *params, const void *params_bf16, int32_t sweeps, int32_t features,
                                      double rel_tol, double *p, double *q, double *dist, uint8_t *flags,

@@ -129,6 +129,28 @@ def test_fused_inference_equals_layer_path(ctx, pairs):
     assert np.array_equal(x0.cpu().numpy(), Y.cpu().numpy())
 
 
+def test_tcgen05_inference_matches_mma_path_and_oracle(ctx, pairs):
+    """The tcgen05/TMEM inference kernel against the mma.sync kernel (same network, other
+    accumulation order: equal to BF16 rounding) and against the oracle's forward."""
+    from delta_b200.learned import WarmStartMLP, features
+
+    from oracle import mlp_oracle as mo
+
+    a, b = pairs
+    n = 40000  # several 128-pair tiles per CTA, last tile partial
+    da, db = _dev(a[:, :n]), _dev(b[:, :n])
+    model = WarmStartMLP.load(ctx)
+    x_mma = model.predict(da, db).cpu().numpy()
+    x_tc = model.predict(da, db, engine="tcgen05").cpu().numpy()
+    assert np.all(np.isfinite(x_tc))
+    assert _rel(x_tc, x_mma) <= 1e-2
+    assert np.max(np.abs(x_tc - x_mma)) <= 5e-2
+    X, _, _ = features(ctx, da[:, :4096].contiguous(), db[:, :4096].contiguous())
+    P = mo.unpack(model.params.cpu().numpy().astype(np.float64))
+    ref = mo.forward(X.float().cpu().numpy(), P)["Y"]
+    assert _rel(x_tc[:4096], ref) <= 2e-2
+
+
 @pytest.fixture(scope="module")
 def trained(ctx):
     """A network trained on 2^19 fresh pairs for 6 epochs with the library's kernels."""
@@ -208,6 +230,27 @@ def test_learned_solver_vs_fp64_bf(ctx, trained, oracle, pairs, use_net, feature
     for thr in (1e-4, 1e-3, 1e-2):
         band = np.abs(od - thr) <= 1e-6 * thr
         assert np.array_equal((d <= thr)[~band], (od <= thr)[~band])
+
+
+@pytest.mark.parametrize("engine", ["tcgen05", "mma"])
+def test_learned_pipeline_engines(ctx, oracle, pairs, engine):
+    """The bundled network on either tensor-core engine inside delta_pairs_run_learned:
+    within 1e-6 of FP64 bfSolver, fallback bit-exact, no time-out."""
+    from delta_b200.learned import WarmStartMLP, learned_pairs, set_engine
+
+    a, b = pairs[0][:, :30000], pairs[1][:, :30000]
+    model = WarmStartMLP.load(ctx)
+    set_engine(ctx, engine)
+    try:
+        p, q, d, fl, nf = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=0, count_fallback=True)
+    finally:
+        set_engine(ctx, "tcgen05")
+    d, fl = d.cpu().numpy(), fl.cpu().numpy()
+    _, _, od, _ = oracle.pairs(0, a, b)
+    fin = np.isfinite(od)
+    assert np.all(np.abs(d - od)[fin] <= 1e-6 * od[fin])
+    assert np.array_equal(d[fl == 2], od[fl == 2], equal_nan=True)
+    assert (fl == 1).mean() > 0.8  # the trained network's start certifies most pairs without sweeps
 
 
 def test_learned_host_entry_equals_device_entry(ctx, trained, pairs):
