@@ -43,7 +43,7 @@ FLOPS_BF = 1214  # algorithmic FP ops of bfSolver per pair (747 add, 439 mul, 13
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--method", default="learned",
@@ -84,9 +84,15 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the sampler is running once its first line is in; samples before the timed
+            # region starts are dropped
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 5.0:
+                time.sleep(0.01)
+            self.rows.clear()
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
