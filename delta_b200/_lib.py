@@ -44,6 +44,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_sim_contacts": ([vp, vp, vp], C.c_int),
     "delta_sim_counters": ([vp, vp], C.c_int),
     "delta_sim_destroy": ([vp], C.c_int),
+    "delta_filter_new_contacts": ([vp, vp, i64, f8, vp], C.c_int),
+    "delta_filter_old_contacts": ([vp, vp, i64, vp, i64, f8, vp], C.c_int),
     "delta_mlp_layout": ([vp], C.c_int),
     "delta_mlp_infer": ([vp, i64, vp, vp, i64, vp, vp, vp], C.c_int),
     "delta_mlp_infer_tcgen05": ([vp, i64, vp, vp, i64, vp, vp, vp], C.c_int),

@@ -95,6 +95,19 @@ class Contacts:
                          p(self.eps_total), p(self.master), p(self.slave), p(self.tri_a), p(self.tri_b),
                          p(self.penetration), p(self.friction))
 
+    def select(self, mask, n: int | None = None) -> "Contacts":
+        """A new buffer with the first n contacts where mask (device, bool/uint8) is set."""
+        n = self.count if n is None else n
+        m = mask[:n].bool()
+        k = int(m.sum().item())
+        out = Contacts(k, device=self.x.device)
+        for name in ("x", "normal", "P", "Q"):
+            getattr(out, name)[:, :k] = getattr(self, name)[:, :n][:, m]
+        for name in ("depth", "eps_total", "master", "slave", "tri_a", "tri_b", "penetration", "friction"):
+            getattr(out, name)[:k] = getattr(self, name)[:n][m]
+        out.count = k
+        return out
+
     def to_numpy(self, n: int | None = None) -> np.ndarray:
         n = self.count if n is None else n
         out = np.zeros(n, CONTACT_DTYPE)
@@ -194,3 +207,33 @@ def hybridTriangleStat(*args, **kw):  # noqa: N802
 def gjk(nA, xA, yA, zA, epsA, fricA, idA, nB, xB, yB, zB, epsB, fricB, idB, **kw):
     """gjk argument order (gjk.h:32-47); per triangle pair with bf()'s contact rule."""
     return _one_pair(DRV_GJK, xA, yA, zA, nA, epsA, fricA, idA, xB, yB, zB, nB, epsB, fricB, idB, **kw)
+
+
+def filter_new_mask(ctx: Context, contacts: Contacts, n: int | None = None, eps: float = 1e-4):
+    """keep flags (device uint8) of filterNewContacts (filter.cpp:80-101) per particle pair."""
+    import torch
+
+    n = contacts.count if n is None else n
+    keep = torch.empty(max(n, 1), dtype=torch.uint8, device=contacts.x.device)
+    check(lib().delta_filter_new_contacts(ctx.handle, C.byref(contacts.struct()), n, float(eps), keep.data_ptr()))
+    return keep[:n]
+
+
+def filter_old_mask(ctx: Context, stored: Contacts, fresh: Contacts, eps: float = 1e-4):
+    """keep flags (device uint8) of filterOldContacts (filter.cpp:3-78) for fresh vs stored."""
+    import torch
+
+    keep = torch.empty(max(fresh.count, 1), dtype=torch.uint8, device=fresh.x.device)
+    check(lib().delta_filter_old_contacts(ctx.handle, C.byref(stored.struct()), stored.count,
+                                          C.byref(fresh.struct()), fresh.count, float(eps), keep.data_ptr()))
+    return keep[:fresh.count]
+
+
+def filterNewContacts(ctx: Context, contacts: Contacts, eps: float = 1e-4) -> Contacts:  # noqa: N802
+    """delta::contact::filterNewContacts over every particle pair's contacts."""
+    return contacts.select(filter_new_mask(ctx, contacts, eps=eps))
+
+
+def filterOldContacts(ctx: Context, stored: Contacts, fresh: Contacts, eps: float = 1e-4) -> Contacts:  # noqa: N802
+    """delta::contact::filterOldContacts: the fresh contacts not near a stored one of their pair."""
+    return fresh.select(filter_old_mask(ctx, stored, fresh, eps=eps))

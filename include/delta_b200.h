@@ -260,6 +260,21 @@ delta_status delta_sim_contacts(delta_sim *sim, const delta_contacts *out, int64
 delta_status delta_sim_counters(const delta_sim *sim, int64_t out[4]);
 delta_status delta_sim_destroy(delta_sim *sim);
 
+/* ---- contact de-duplication ----------------------------------------------------------
+ * filter.cpp (the reference defines these; its time step does not call them).  A run is a
+ * maximal sequence of contacts with equal (master, slave), i.e. one particle pair's
+ * contacts as delta_detect returns them.  keep [n] receives 1 for the contacts that stay.
+ * eps is the reference's 0.0001 unless given otherwise; two contacts are near when
+ * |x_a - x_b| < eps on every coordinate (FP64). */
+/* filterNewContacts (filter.cpp:80-101) on every run: a contact stays unless an earlier
+ * contact of its run that stayed is near it. */
+delta_status delta_filter_new_contacts(delta_ctx *ctx, const delta_contacts *contacts, int64_t n, double eps,
+                                       uint8_t *keep);
+/* filterOldContacts (filter.cpp:3-78, all three overloads): a new contact stays unless a
+ * stored contact of the same (master, slave) is near it.  Any order of either list. */
+delta_status delta_filter_old_contacts(delta_ctx *ctx, const delta_contacts *stored, int64_t n_stored,
+                                       const delta_contacts *fresh, int64_t n_fresh, double eps, uint8_t *keep);
+
 /* ---- learned warm start ----------------------------------------------------------------
  * No counterpart in the reference.  A small MLP (18 -> 128 -> 128 -> 128 -> 4, GELU, BF16
  * weights and activations, FP32 accumulation) maps a canonicalised triangle pair to the

@@ -936,3 +936,39 @@ int64_t dor_sim_contacts(const dor_sim *s, dor_contact *out, int64_t cap) {
   if (n > 0) memcpy(out, s->c, sizeof(dor_contact) * (size_t)n);
   return s->n;
 }
+
+/* ---- contact de-duplication: filter.cpp --------------------------------------------- */
+
+static int dor_near(const double *x, int64_t ld, int64_t i, const double *y, int64_t ldy, int64_t j, double eps) {
+  /* filter.cpp:16-21 / 92-97: the three coordinate differences, each |.| < eps */
+  return fabs(x[i] - y[j]) < eps && fabs(x[ld + i] - y[ldy + j]) < eps &&
+         fabs(x[2 * ld + i] - y[2 * ldy + j]) < eps;
+}
+
+void dor_filter_new(int64_t n, const double *x, int64_t ld, const int32_t *master, const int32_t *slave,
+                    double eps, uint8_t *keep) {
+  int64_t s = 0;
+  while (s < n) {
+    int64_t e = s + 1;
+    while (e < n && master[e] == master[s] && slave[e] == slave[s]) ++e;
+    /* filter.cpp:80-101: a contact survives unless a survivor before it is near */
+    for (int64_t i = s; i < e; ++i) {
+      int hit = 0;
+      for (int64_t j = s; j < i && !hit; ++j)
+        if (keep[j] && dor_near(x, ld, i, x, ld, j, eps)) hit = 1;
+      keep[i] = hit ? 0 : 1;
+    }
+    s = e;
+  }
+}
+
+void dor_filter_old(int64_t ns, const double *xs, int64_t lds, const int32_t *ms, const int32_t *ss, int64_t nn,
+                    const double *xn, int64_t ldn, const int32_t *mn, const int32_t *sn, double eps,
+                    uint8_t *keep) {
+  for (int64_t i = 0; i < nn; ++i) {
+    int hit = 0;
+    for (int64_t j = 0; j < ns && !hit; ++j)
+      if (ms[j] == mn[i] && ss[j] == sn[i] && dor_near(xn, ldn, i, xs, lds, j, eps)) hit = 1;
+    keep[i] = hit ? 0 : 1;
+  }
+}

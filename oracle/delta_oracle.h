@@ -144,6 +144,18 @@ int64_t dor_sim_run(dor_sim *s, dor_scene *scene, const dor_step_params *prm, in
 /* Copies out the contacts currently held (sorted by (master, slave, tri_a, tri_b)). */
 int64_t dor_sim_contacts(const dor_sim *s, dor_contact *out, int64_t cap);
 
+/* Contact de-duplication (filter.cpp).  Contacts are given by their points x as 3 planes
+ * of ld doubles and their (master, slave) ids; a segment is a maximal run of equal
+ * (master, slave).  filterNewContacts (filter.cpp:80-101) within each segment, in order:
+ * keep[i] = 1 unless an earlier kept contact of the segment lies within eps on every
+ * coordinate (|dx| < eps).  filterOldContacts (filter.cpp:3-78, all three overloads):
+ * keep[i] = 0 when any stored contact with the same (master, slave) lies within eps. */
+void dor_filter_new(int64_t n, const double *x, int64_t ld, const int32_t *master, const int32_t *slave,
+                    double eps, uint8_t *keep);
+void dor_filter_old(int64_t ns, const double *xs, int64_t lds, const int32_t *ms, const int32_t *ss, int64_t nn,
+                    const double *xn, int64_t ldn, const int32_t *mn, const int32_t *sn, double eps,
+                    uint8_t *keep);
+
 #ifdef __cplusplus
 }
 #endif

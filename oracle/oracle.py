@@ -153,6 +153,26 @@ class Oracle(_Lib):
         L.dor_sim_run.restype = i64
         L.dor_sim_contacts.argtypes = [vp, vp, i64]
         L.dor_sim_contacts.restype = i64
+        L.dor_filter_new.argtypes = [i64, vp, i64, vp, vp, f8, vp]
+        L.dor_filter_old.argtypes = [i64, vp, i64, vp, vp, i64, vp, i64, vp, vp, f8, vp]
+
+    def filter_new(self, x, master, slave, eps=1e-4):
+        """keep flags of filterNewContacts per (master, slave) segment; x is (3, n)."""
+        x = np.ascontiguousarray(x, np.float64)
+        m = np.ascontiguousarray(master, np.int32); s = np.ascontiguousarray(slave, np.int32)
+        n = x.shape[1]
+        keep = np.zeros(n, np.uint8)
+        self.lib.dor_filter_new(n, _p(x), n, _p(m), _p(s), eps, _p(keep))
+        return keep
+
+    def filter_old(self, xs, ms, ss, xn, mn, sn, eps=1e-4):
+        """keep flags of filterOldContacts for the new contacts xn against stored xs."""
+        xs = np.ascontiguousarray(xs, np.float64); xn = np.ascontiguousarray(xn, np.float64)
+        a = [np.ascontiguousarray(v, np.int32) for v in (ms, ss, mn, sn)]
+        keep = np.zeros(xn.shape[1], np.uint8)
+        self.lib.dor_filter_old(xs.shape[1], _p(xs), xs.shape[1], _p(a[0]), _p(a[1]), xn.shape[1], _p(xn),
+                                xn.shape[1], _p(a[2]), _p(a[3]), eps, _p(keep))
+        return keep
 
     def contacts_forces(self, contacts, sign, posA, angA, linA, mA, posB, angB, linB, mB, spring, damper, friction):
         c = np.ascontiguousarray(contacts, CONTACT_DTYPE)
@@ -201,6 +221,24 @@ class Reference(_Lib):
         L.ref_contacts_forces.argtypes = [vp, i64, vp, vp, vp, f8, vp, vp, vp, f8, vp, vp]
         L.ref_update_rotation.argtypes = [vp, vp, vp, f8]
         L.ref_update_angular.argtypes = [vp, vp, vp, vp, vp, f8]
+        L.ref_filter_new.argtypes = [i64, vp, i64, vp]
+        L.ref_filter_new.restype = i64
+        L.ref_filter_old.argtypes = [i64, vp, i64, i64, vp, i64, vp]
+        L.ref_filter_old.restype = i64
+
+    def filter_new(self, x):
+        """keep flags of the reference's filterNewContacts over one contact list x (3, n)."""
+        x = np.ascontiguousarray(x, np.float64)
+        keep = np.zeros(x.shape[1], np.uint8)
+        self.lib.ref_filter_new(x.shape[1], _p(x), x.shape[1], _p(keep))
+        return keep
+
+    def filter_old(self, xs, xn):
+        """keep flags of the reference's filterOldContacts(stored xs, new xn)."""
+        xs = np.ascontiguousarray(xs, np.float64); xn = np.ascontiguousarray(xn, np.float64)
+        keep = np.zeros(xn.shape[1], np.uint8)
+        self.lib.ref_filter_old(xs.shape[1], _p(xs), xs.shape[1], xn.shape[1], _p(xn), xn.shape[1], _p(keep))
+        return keep
 
     @staticmethod
     def available(flavour: str = "par") -> bool:

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "contact/contactpoint.h"
+#include "contact/filter.h"
 #include "contact/detection/bf.h"
 #include "contact/detection/gjk.h"
 #include "contact/detection/hybrid.h"
@@ -216,6 +217,35 @@ void ref_update_angular(double ref_ang[3], double rot[9], double inertia[9], dou
 void ref_update_vertex(double *x, double *y, double *z, double *rx, double *ry, double *rz, double rot[9],
                        double pos[3], double ref_pos[3]) {
   delta::dynamics::updateVertices(x, y, z, rx, ry, rz, rot, pos, ref_pos);
+}
+
+// filterNewContacts / filterOldContacts on one contact list each (x as 3 planes of ld
+// doubles).  The contacts carry their index in `master`, so the survivors name themselves:
+// keep[i] = 1 for every contact the reference function keeps.  Returns the survivors.
+static std::vector<delta::contact::contactpoint> as_contacts(int64_t n, const double *x, int64_t ld) {
+  std::vector<delta::contact::contactpoint> v(n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) v[i].x[k] = x[k * ld + i];
+    v[i].master = (int)i;
+  }
+  return v;
+}
+
+int64_t ref_filter_new(int64_t n, const double *x, int64_t ld, uint8_t *keep) {
+  std::vector<delta::contact::contactpoint> v = as_contacts(n, x, ld);
+  delta::contact::filterNewContacts(v);
+  std::memset(keep, 0, (size_t)n);
+  for (const auto &c : v) keep[c.master] = 1;
+  return (int64_t)v.size();
+}
+
+int64_t ref_filter_old(int64_t ns, const double *xs, int64_t lds, int64_t nn, const double *xn, int64_t ldn,
+                       uint8_t *keep) {
+  std::vector<delta::contact::contactpoint> stored = as_contacts(ns, xs, lds), fresh = as_contacts(nn, xn, ldn);
+  delta::contact::filterOldContacts(stored, fresh);
+  std::memset(keep, 0, (size_t)nn);
+  for (const auto &c : fresh) keep[c.master] = 1;
+  return (int64_t)fresh.size();
 }
 
 }  // extern "C"
