@@ -44,6 +44,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_sim_contacts": ([vp, vp, vp], C.c_int),
     "delta_sim_counters": ([vp, vp], C.c_int),
     "delta_sim_destroy": ([vp], C.c_int),
+    "delta_sphere_contacts": ([vp, vp, vp, vp, i64, vp, vp], C.c_int),
+    "delta_sphere_mesh_contacts": ([vp, vp, vp, vp, vp, i64, C.c_int, vp, vp], C.c_int),
+    "delta_sphere_overlap": ([vp, vp, i64, vp, vp, vp, i64, vp], C.c_int),
     "delta_filter_new_contacts": ([vp, vp, i64, f8, vp], C.c_int),
     "delta_filter_old_contacts": ([vp, vp, i64, vp, i64, f8, vp], C.c_int),
     "delta_mlp_layout": ([vp], C.c_int),

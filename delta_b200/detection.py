@@ -237,3 +237,90 @@ def filterNewContacts(ctx: Context, contacts: Contacts, eps: float = 1e-4) -> Co
 def filterOldContacts(ctx: Context, stored: Contacts, fresh: Contacts, eps: float = 1e-4) -> Contacts:  # noqa: N802
     """delta::contact::filterOldContacts: the fresh contacts not near a stored one of their pair."""
     return fresh.select(filter_old_mask(ctx, stored, fresh, eps=eps))
+
+
+# ---- sphere model (sphere.cpp) ----------------------------------------------------------
+class _Spheres(C.Structure):
+    _fields_ = [("n", C.c_int64), ("centre", C.c_void_p), ("diameter", C.c_void_p), ("eps", C.c_void_p),
+                ("friction", C.c_void_p), ("id", C.c_void_p)]
+
+
+class Spheres:
+    """Spherical particles on the device: centres (3, n), diameters, halo eps, friction, ids."""
+
+    def __init__(self, centre, diameter, eps, friction, ids=None, device="cuda"):
+        import torch
+
+        t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).to(device)  # noqa: E731
+        self.centre = t(centre, torch.float64)
+        self.n = self.centre.shape[1]
+        self.diameter = t(diameter, torch.float64)
+        self.eps = t(eps, torch.float64)
+        self.friction = t(friction, torch.uint8)
+        self.id = t(ids if ids is not None else np.arange(self.n), torch.int32)
+
+    def struct(self) -> _Spheres:
+        return _Spheres(self.n, self.centre.data_ptr(), self.diameter.data_ptr(), self.eps.data_ptr(),
+                        self.friction.data_ptr(), self.id.data_ptr())
+
+
+def _pairs_dev(a):
+    import torch
+
+    return torch.as_tensor(np.asarray(a, np.int32) if not torch.is_tensor(a) else a, dtype=torch.int32).cuda()
+
+
+def _grow(call, capacity):
+    cap = capacity
+    while True:
+        out = Contacts(cap)
+        n = C.c_int64(0)
+        status = call(out, n)
+        if status == ERR_CAPACITY:
+            cap = int(n.value)
+            continue
+        check(status)
+        out.count = int(n.value)
+        return out
+
+
+def sphere(ctx: Context, spheres: Spheres, pair_a, pair_b, capacity: int = 1024) -> Contacts:
+    """delta::contact::detection::sphere (sphere.cpp:29-77) over sphere pairs, in pair order."""
+    pa, pb = _pairs_dev(pair_a), _pairs_dev(pair_b)
+    return _grow(lambda out, n: lib().delta_sphere_contacts(ctx.handle, C.byref(spheres.struct()), pa.data_ptr(),
+                                                            pb.data_ptr(), pa.numel(), C.byref(out.struct()),
+                                                            C.byref(n)), capacity)
+
+
+def _sphere_mesh(ctx, spheres, meshes, sphere_idx, body_idx, sphere_is_b, capacity):
+    ps, pm = _pairs_dev(sphere_idx), _pairs_dev(body_idx)
+    return _grow(lambda out, n: lib().delta_sphere_mesh_contacts(
+        ctx.handle, C.byref(spheres.struct()), C.byref(meshes.struct()), ps.data_ptr(), pm.data_ptr(), ps.numel(),
+        int(sphere_is_b), C.byref(out.struct()), C.byref(n)), capacity)
+
+
+def sphereWithBarrierAB(ctx: Context, spheres: Spheres, meshes: Meshes, sphere_idx, body_idx,  # noqa: N802
+                        capacity: int = 4096) -> Contacts:
+    """sphere.cpp:79-140: sphere A against the triangles of mesh B, in (pair, triangle) order."""
+    return _sphere_mesh(ctx, spheres, meshes, sphere_idx, body_idx, 0, capacity)
+
+
+def sphereWithBarrierBA(ctx: Context, spheres: Spheres, meshes: Meshes, sphere_idx, body_idx,  # noqa: N802
+                        capacity: int = 4096) -> Contacts:
+    """sphere.cpp:142-201: sphere B against the triangles of mesh A (mesh point first)."""
+    return _sphere_mesh(ctx, spheres, meshes, sphere_idx, body_idx, 1, capacity)
+
+
+def isSphereOverlayInContact(ctx: Context, centre, radius, pair_a, pair_b):  # noqa: N802
+    """sphere.cpp:203-218 for each pair: |cA - cB| <= rA + rB (device uint8 flags)."""
+    import torch
+
+    c = torch.as_tensor(np.ascontiguousarray(centre) if not torch.is_tensor(centre) else centre,
+                        dtype=torch.float64).cuda().contiguous()
+    r = torch.as_tensor(np.ascontiguousarray(radius) if not torch.is_tensor(radius) else radius,
+                        dtype=torch.float64).cuda().contiguous()
+    pa, pb = _pairs_dev(pair_a), _pairs_dev(pair_b)
+    out = torch.empty(max(pa.numel(), 1), dtype=torch.uint8, device="cuda")
+    check(lib().delta_sphere_overlap(ctx.handle, c.data_ptr(), c.shape[1], r.data_ptr(), pa.data_ptr(),
+                                     pb.data_ptr(), pa.numel(), out.data_ptr()))
+    return out[:pa.numel()]

@@ -260,6 +260,38 @@ delta_status delta_sim_contacts(delta_sim *sim, const delta_contacts *out, int64
 delta_status delta_sim_counters(const delta_sim *sim, int64_t out[4]);
 delta_status delta_sim_destroy(delta_sim *sim);
 
+/* ---- sphere model ----------------------------------------------------------------------
+ * sphere.cpp / point.cpp: particles as spheres (the reference's cheap baseline and halo
+ * precheck).  Contacts use the same record as the mesh path (contactpoint.cpp:116-155),
+ * tri_a = -1, tri_b = the mesh triangle (or -1); they equal the reference's bit for bit.
+ * The forces of sphere contacts are delta_forces' with the sphere constants (springSphere,
+ * forces.cpp:227-253, is spring's formula with SSPRING and SDAMPER; the sphere friction
+ * uses SFRICTIONGOLD). */
+typedef struct {
+  int64_t n;
+  const double *centre;     /* [3][n] planes x, y, z */
+  const double *diameter;   /* [n] (the reference passes diameters) */
+  const double *eps;        /* [n] */
+  const uint8_t *friction;  /* [n] */
+  const int32_t *id;        /* [n] global particle id written to master/slave */
+} delta_spheres;
+/* sphere() (sphere.cpp:29-77) for the sphere pairs (pair_a[k], pair_b[k]): at most one
+ * contact per pair, written in pair order.  *n_out = the number of contacts; beyond
+ * out->capacity DELTA_ERR_CAPACITY.  Synchronises. */
+delta_status delta_sphere_contacts(delta_ctx *ctx, const delta_spheres *spheres, const int32_t *pair_a,
+                                   const int32_t *pair_b, int64_t n_pairs, const delta_contacts *out,
+                                   int64_t *n_out);
+/* sphereWithBarrierAB (sphere_is_b = 0: sphere.cpp:79-140) or sphereWithBarrierBA
+ * (sphere_is_b = 1: sphere.cpp:142-201) for (sphere[k], mesh body[k]): one contact per
+ * triangle of the body within the halo, in (pair, triangle) order.  Synchronises. */
+delta_status delta_sphere_mesh_contacts(delta_ctx *ctx, const delta_spheres *spheres, const delta_meshes *meshes,
+                                        const int32_t *sphere, const int32_t *body, int64_t n_pairs,
+                                        int sphere_is_b, const delta_contacts *out, int64_t *n_out);
+/* isSphereOverlayInContact (sphere.cpp:203-218) for each pair: centre [3][ld], radius [n]
+ * (the values the caller passes as radii); overlap [n_pairs] = 1 when |cA - cB| <= rA + rB. */
+delta_status delta_sphere_overlap(delta_ctx *ctx, const double *centre, int64_t ld, const double *radius,
+                                  const int32_t *pair_a, const int32_t *pair_b, int64_t n_pairs, uint8_t *overlap);
+
 /* ---- contact de-duplication ----------------------------------------------------------
  * filter.cpp (the reference defines these; its time step does not call them).  A run is a
  * maximal sequence of contacts with equal (master, slave), i.e. one particle pair's

@@ -972,3 +972,150 @@ void dor_filter_old(int64_t ns, const double *xs, int64_t lds, const int32_t *ms
     keep[i] = hit ? 0 : 1;
   }
 }
+
+/* ---- sphere model: point.cpp, sphere.cpp --------------------------------------------- */
+
+#define DOR_DOT(a, b) ((a)[0] * (b)[0] + (a)[1] * (b)[1] + (a)[2] * (b)[2])
+
+double dor_pt(const double TP1[3], const double TP2[3], const double TP3[3], const double c[3], double tq[3]) {
+  double E0[3], E1[3], D[3];
+  for (int k = 0; k < 3; ++k) {
+    E0[k] = TP2[k] - TP1[k];
+    E1[k] = TP3[k] - TP1[k];
+    D[k] = TP1[k] - c[k];
+  }
+  const double a = DOR_DOT(E0, E0), b = DOR_DOT(E0, E1), cc = DOR_DOT(E1, E1);
+  const double d = DOR_DOT(E0, D), e = DOR_DOT(E1, D), f = DOR_DOT(D, D);
+  const double det = a * cc - b * b;
+  double s = b * e - cc * d, t = b * d - a * e, sq = 0;
+  /* the seven regions of point.cpp:41-203 */
+  if ((s + t) <= det) {
+    if (s < 0) {
+      if (t < 0) { /* region 4 */
+        if (d < 0) {
+          t = 0;
+          if (-d >= a) { s = 1; sq = a + 2 * d + f; }
+          else { s = -d / a; sq = d * s + f; }
+        } else {
+          s = 0;
+          if (e >= 0) { t = 0; sq = f; }
+          else if (-e >= cc) { t = 1; sq = cc + 2 * e + f; }
+          else { t = -e / cc; sq = e * t + f; }
+        }
+      } else { /* region 3 */
+        s = 0;
+        if (e >= 0) { t = 0; sq = f; }
+        else if (-e >= cc) { t = 1; sq = cc + 2 * e + f; }
+        else { t = -e / cc; sq = e * t + f; }
+      }
+    } else if (t < 0) { /* region 5 */
+      t = 0;
+      if (d >= 0) { s = 0; sq = f; }
+      else if (-d >= a) { s = 1; sq = a + 2 * d + f; }
+      else { s = -d / a; sq = d * s + f; }
+    } else { /* region 0 */
+      const double inv = 1 / det;
+      s = s * inv;
+      t = t * inv;
+      sq = s * (a * s + b * t + 2 * d) + t * (b * s + cc * t + 2 * e) + f;
+    }
+  } else {
+    if (s < 0) { /* region 2 */
+      const double tmp0 = b + d, tmp1 = cc + e;
+      if (tmp1 > tmp0) {
+        const double numer = tmp1 - tmp0, denom = a - 2 * b + cc;
+        if (numer >= denom) { s = 1; t = 0; sq = a + 2 * d + f; }
+        else { s = numer / denom; t = 1 - s; sq = s * (a * s + b * t + 2 * d) + t * (b * s + cc * t + 2 * e) + f; }
+      } else {
+        s = 0;
+        if (tmp1 <= 0) { t = 1; sq = cc + 2 * e + f; }
+        else if (e >= 0) { t = 0; sq = f; }
+        else { t = -e / cc; sq = e * t + f; }
+      }
+    } else if (t < 0) { /* region 6 */
+      const double tmp0 = b + e, tmp1 = a + d;
+      if (tmp1 > tmp0) {
+        const double numer = tmp1 - tmp0, denom = a - 2 * b + cc;
+        if (numer >= denom) { t = 1; s = 0; sq = cc + 2 * e + f; }
+        else { t = numer / denom; s = 1 - t; sq = s * (a * s + b * t + 2 * d) + t * (b * s + cc * t + 2 * e) + f; }
+      } else {
+        t = 0;
+        if (tmp1 <= 0) { s = 1; sq = a + 2 * d + f; }
+        else if (d >= 0) { s = 0; sq = f; }
+        else { s = -d / a; sq = d * s + f; }
+      }
+    } else { /* region 1 */
+      const double numer = cc + e - b - d;
+      if (numer <= 0) { s = 0; t = 1; sq = cc + 2 * e + f; }
+      else {
+        const double denom = a - 2 * b + cc;
+        if (numer >= denom) { s = 1; t = 0; sq = a + 2 * d + f; }
+        else { s = numer / denom; t = 1 - s; sq = s * (a * s + b * t + 2 * d) + t * (b * s + cc * t + 2 * e) + f; }
+      }
+    }
+  }
+  if (sq < 0) sq = 0;
+  for (int k = 0; k < 3; ++k) tq[k] = TP1[k] + (E1[k] * t) + (E0[k] * s);
+  return sqrt(sq);
+}
+
+static double dor_contact_distance(const dor_contact *c) {
+  return sqrt(((c->Q[0] - c->P[0]) * (c->Q[0] - c->P[0])) + ((c->Q[1] - c->P[1]) * (c->Q[1] - c->P[1])) +
+              ((c->Q[2] - c->P[2]) * (c->Q[2] - c->P[2])));
+}
+
+int64_t dor_sphere(const double cA[3], double dA, double epsA, int32_t fricA, int32_t idA, const double cB[3],
+                   double dB, double epsB, int32_t fricB, int32_t idB, dor_contact *out) {
+  /* sphere.cpp:46-76 */
+  const double distance = sqrt(((cB[0] - cA[0]) * (cB[0] - cA[0])) + ((cB[1] - cA[1]) * (cB[1] - cA[1])) +
+                               ((cB[2] - cA[2]) * (cB[2] - cA[2])));
+  double n[3], PA[3], PB[3];
+  for (int k = 0; k < 3; ++k) n[k] = (1.0 / distance) * (cB[k] - cA[k]);
+  for (int k = 0; k < 3; ++k) {
+    PA[k] = cA[k] + ((dA / 2) * n[k]);
+    PB[k] = cB[k] - ((dB / 2) * n[k]);
+  }
+  dor_contact c;
+  dor_make_contact(PA[0], PA[1], PA[2], epsA, idA, PB[0], PB[1], PB[2], epsB, idB, (fricA & fricB) ? 1 : 0, &c);
+  if (dor_contact_distance(&c) <= (epsA + epsB)) {
+    if (out) *out = c;
+    return 1;
+  }
+  return 0;
+}
+
+int64_t dor_sphere_mesh(int32_t ba, const double c[3], double d, double epsS, int32_t fricS, int32_t idS,
+                        const double *x, const double *y, const double *z, int32_t nT, double epsM, int32_t fricM,
+                        int32_t idM, dor_contact *out, int64_t cap) {
+  int64_t n = 0;
+  for (int32_t i = 0; i < 3 * nT; i += 3) {
+    const double TP1[3] = {x[i], y[i], z[i]}, TP2[3] = {x[i + 1], y[i + 1], z[i + 1]},
+                 TP3[3] = {x[i + 2], y[i + 2], z[i + 2]};
+    double Q[3], S[3];
+    /* sphere.cpp:112-124 / 175-187 */
+    const double distance = dor_pt(TP1, TP2, TP3, c, Q) - (d / 2.0);
+    for (int k = 0; k < 3; ++k) {
+      const double nk = (Q[k] - c[k]) / (distance + (d / 2.0));
+      S[k] = c[k] + ((d / 2.0) * nk);
+    }
+    dor_contact ct;
+    const int32_t fr = (fricS & fricM) ? 1 : 0;
+    if (ba == 0)
+      dor_make_contact(S[0], S[1], S[2], epsS, idS, Q[0], Q[1], Q[2], epsM, idM, fr, &ct);
+    else /* sphere.cpp:189: the mesh point first, with the sphere's epsilon and id */
+      dor_make_contact(Q[0], Q[1], Q[2], epsS, idS, S[0], S[1], S[2], epsM, idM, fr, &ct);
+    if (dor_contact_distance(&ct) <= (epsS + epsM)) {
+      if (out && n < cap) {
+        out[n] = ct;
+        out[n].tri_b = i / 3;
+      }
+      ++n;
+    }
+  }
+  return n;
+}
+
+int32_t dor_sphere_overlay(const double cA[3], double rA, const double cB[3], double rB) {
+  const double distance = sqrt(pow(cB[0] - cA[0], 2) + pow(cB[1] - cA[1], 2) + pow(cB[2] - cA[2], 2));
+  return distance <= rA + rB ? 1 : 0;
+}

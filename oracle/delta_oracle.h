@@ -144,6 +144,20 @@ int64_t dor_sim_run(dor_sim *s, dor_scene *scene, const dor_step_params *prm, in
 /* Copies out the contacts currently held (sorted by (master, slave, tri_a, tri_b)). */
 int64_t dor_sim_contacts(const dor_sim *s, dor_contact *out, int64_t cap);
 
+/* Sphere model (sphere.cpp, point.cpp).  dor_pt: closest point tq of triangle
+ * (TP1,TP2,TP3) to c and its distance (point.cpp:11-210).  dor_sphere: sphere()
+ * (sphere.cpp:29-77), diameters; 0 or 1 contact.  dor_sphere_mesh: sphereWithBarrierAB
+ * (ba = 0: the sphere is A, the mesh B; sphere.cpp:79-140) or sphereWithBarrierBA (ba = 1;
+ * sphere.cpp:142-201); triangle order.  dor_sphere_overlay: isSphereOverlayInContact
+ * (sphere.cpp:203-218), radii. */
+double dor_pt(const double TP1[3], const double TP2[3], const double TP3[3], const double c[3], double tq[3]);
+int64_t dor_sphere(const double cA[3], double dA, double epsA, int32_t fricA, int32_t idA, const double cB[3],
+                   double dB, double epsB, int32_t fricB, int32_t idB, dor_contact *out);
+int64_t dor_sphere_mesh(int32_t ba, const double c[3], double d, double epsS, int32_t fricS, int32_t idS,
+                        const double *x, const double *y, const double *z, int32_t nT, double epsM, int32_t fricM,
+                        int32_t idM, dor_contact *out, int64_t cap);
+int32_t dor_sphere_overlay(const double cA[3], double rA, const double cB[3], double rB);
+
 /* Contact de-duplication (filter.cpp).  Contacts are given by their points x as 3 planes
  * of ld doubles and their (master, slave) ids; a segment is a maximal run of equal
  * (master, slave).  filterNewContacts (filter.cpp:80-101) within each segment, in order:

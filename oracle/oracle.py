@@ -98,6 +98,14 @@ class _Lib:
         getattr(L, pre + "gjk").argtypes = [vp, i32, vp, i32, vp, vp]
         getattr(L, pre + "gjk").restype = f8
         getattr(L, pre + "expmap").argtypes = [f8, f8, f8, vp]
+        getattr(L, pre + "pt").argtypes = [vp] * 5
+        getattr(L, pre + "pt").restype = f8
+        getattr(L, pre + "sphere").argtypes = [vp, f8, f8, i32, i32, vp, f8, f8, i32, i32, vp]
+        getattr(L, pre + "sphere").restype = i64
+        getattr(L, pre + "sphere_mesh").argtypes = [i32, vp, f8, f8, i32, i32, vp, vp, vp, i32, f8, i32, i32, vp, i64]
+        getattr(L, pre + "sphere_mesh").restype = i64
+        getattr(L, pre + "sphere_overlay").argtypes = [vp, f8, vp, f8]
+        getattr(L, pre + "sphere_overlay").restype = i32
 
     # ---- pair list -------------------------------------------------------------
     def pairs(self, method, a, b, max_error=0.0, nthreads=0, with_flags=True):
@@ -124,6 +132,36 @@ class _Lib:
             _p(B[0]), _p(B[1]), _p(B[2]), nB, epsB, int(fricB), idB,
             _p(out), cap, C.byref(st) if st is not None else None)
         return out[: min(n, cap)], st
+
+    # ---- sphere model ----------------------------------------------------------------
+    def pt(self, T1, T2, T3, c):
+        """point.cpp pt(): (distance, closest point)."""
+        a = [np.ascontiguousarray(v, np.float64) for v in (T1, T2, T3, c)]
+        tq = np.empty(3)
+        d = getattr(self.lib, self.prefix + "pt")(_p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), _p(tq))
+        return d, tq
+
+    def sphere(self, cA, dA, epsA, fA, idA, cB, dB, epsB, fB, idB):
+        """sphere(): the contact (array of 0 or 1 records)."""
+        out = np.zeros(1, CONTACT_DTYPE)
+        cA = np.ascontiguousarray(cA, np.float64); cB = np.ascontiguousarray(cB, np.float64)
+        n = getattr(self.lib, self.prefix + "sphere")(_p(cA), dA, epsA, int(fA), int(idA), _p(cB), dB, epsB,
+                                                      int(fB), int(idB), _p(out))
+        return out[:n]
+
+    def sphere_mesh(self, ba, c, d, epsS, fS, idS, M, nT, epsM, fM, idM):
+        """sphereWithBarrierAB (ba=0) / BA (ba=1) against the SoA-tri mesh M (3, 3*nT)."""
+        M = np.ascontiguousarray(M, np.float64)
+        c = np.ascontiguousarray(c, np.float64)
+        out = np.zeros(max(nT, 1), CONTACT_DTYPE)
+        n = getattr(self.lib, self.prefix + "sphere_mesh")(int(ba), _p(c), d, epsS, int(fS), int(idS), _p(M[0]),
+                                                           _p(M[1]), _p(M[2]), nT, epsM, int(fM), int(idM), _p(out),
+                                                           len(out))
+        return out[:n]
+
+    def sphere_overlay(self, cA, rA, cB, rB):
+        cA = np.ascontiguousarray(cA, np.float64); cB = np.ascontiguousarray(cB, np.float64)
+        return int(getattr(self.lib, self.prefix + "sphere_overlay")(_p(cA), rA, _p(cB), rB))
 
     def expmap(self, o):
         L = np.empty(9)

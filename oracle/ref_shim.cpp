@@ -10,6 +10,8 @@
 
 #include "contact/contactpoint.h"
 #include "contact/filter.h"
+#include "contact/detection/point.h"
+#include "contact/detection/sphere.h"
 #include "contact/detection/bf.h"
 #include "contact/detection/gjk.h"
 #include "contact/detection/hybrid.h"
@@ -217,6 +219,52 @@ void ref_update_angular(double ref_ang[3], double rot[9], double inertia[9], dou
 void ref_update_vertex(double *x, double *y, double *z, double *rx, double *ry, double *rz, double rot[9],
                        double pos[3], double ref_pos[3]) {
   delta::dynamics::updateVertices(x, y, z, rx, ry, rz, rot, pos, ref_pos);
+}
+
+static void to_ref(const delta::contact::contactpoint &c, ref_contact &o) {
+  std::memcpy(o.x, c.x, sizeof o.x);
+  std::memcpy(o.normal, c.normal, sizeof o.normal);
+  o.depth = c.depth;
+  std::memcpy(o.P, c.P, sizeof o.P);
+  std::memcpy(o.Q, c.Q, sizeof o.Q);
+  o.friction = c.friction ? 1 : 0;
+  o.eps_total = c.epsilonTotal;
+  o.master = c.master;
+  o.slave = c.slave;
+  o.penetration = c.penetration;
+  o.tri_a = -1;
+  o.tri_b = -1;
+}
+
+// point.cpp:11 pt(), sphere.cpp sphere / sphereWithBarrierAB / BA / isSphereOverlayInContact
+double ref_pt(const double *TP1, const double *TP2, const double *TP3, const double *c, double *tq) {
+  double a[3], b[3], d[3], p[3];
+  std::memcpy(a, TP1, sizeof a);
+  std::memcpy(b, TP2, sizeof b);
+  std::memcpy(d, TP3, sizeof d);
+  std::memcpy(p, c, sizeof p);
+  return det::pt(a, b, d, p, tq);
+}
+
+int64_t ref_sphere(const double *cA, double dA, double epsA, int32_t fA, int32_t idA, const double *cB, double dB,
+                   double epsB, int32_t fB, int32_t idB, ref_contact *out) {
+  auto r = det::sphere(cA[0], cA[1], cA[2], dA, epsA, fA != 0, idA, cB[0], cB[1], cB[2], dB, epsB, fB != 0, idB);
+  if (!r.empty() && out) to_ref(r[0], out[0]);
+  return (int64_t)r.size();
+}
+
+int64_t ref_sphere_mesh(int32_t ba, const double *c, double d, double epsS, int32_t fS, int32_t idS, const double *x,
+                        const double *y, const double *z, int32_t nT, double epsM, int32_t fM, int32_t idM,
+                        ref_contact *out, int64_t cap) {
+  std::vector<delta::contact::contactpoint> r =
+      ba == 0 ? det::sphereWithBarrierAB(c[0], c[1], c[2], d, epsS, fS != 0, idS, x, y, z, nT, epsM, fM != 0, idM)
+              : det::sphereWithBarrierBA(c[0], c[1], c[2], d, epsS, fS != 0, idS, x, y, z, nT, epsM, fM != 0, idM);
+  for (int64_t i = 0; i < (int64_t)r.size() && i < cap; ++i) to_ref(r[i], out[i]);
+  return (int64_t)r.size();
+}
+
+int32_t ref_sphere_overlay(const double *cA, double rA, const double *cB, double rB) {
+  return det::isSphereOverlayInContact(cA[0], cA[1], cA[2], rA, cB[0], cB[1], cB[2], rB) ? 1 : 0;
 }
 
 // filterNewContacts / filterOldContacts on one contact list each (x as 3 planes of ld
