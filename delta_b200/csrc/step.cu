@@ -1240,4 +1240,16 @@ delta_status delta_sim_destroy(delta_sim *s) {
   return DELTA_OK;
 }
 
+delta_status delta_sim_write_vtk(delta_sim *sim, const char *path, int32_t step) {
+  if (!sim || !path) return set_error(DELTA_ERR_INVALID, "delta_sim_write_vtk: bad argument");
+  // the vertices after the last step (graph replays run on the simulation's own stream)
+  if (sim->g.stream) {
+    const cudaError_t e = cudaStreamSynchronize(sim->g.stream);
+    if (e != cudaSuccess) return cuda_error(e, "delta_sim_write_vtk: graph stream");
+  }
+  delta_meshes m{sim->scene.n_bodies, sim->scene.tri_offset, sim->scene.x, sim->scene.y, sim->scene.z,
+                 sim->scene.eps, sim->scene.friction, sim->ids};
+  return delta_write_vtk(sim->ctx, path, step, &m);
+}
+
 }  // extern "C"

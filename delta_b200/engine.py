@@ -104,6 +104,15 @@ class Simulation:
         del st
         return out.to_numpy()
 
+    def write_vtk(self, path, step: int) -> str:
+        """Legacy VTK snapshot of the current vertices (writeGeometryToVTK's format)."""
+        import os
+
+        p = os.fspath(path)
+        p = p if p.endswith(os.sep) else p + os.sep
+        check(lib().delta_sim_write_vtk(self._h, p.encode(), int(step)))
+        return os.path.join(p, f"geometry_{int(step)}.vtk")
+
     def counters(self) -> dict:
         """steps, candidate body pairs, triangle pairs tested (sum nA*nB), triangle pairs solved."""
         out = np.zeros(4, np.int64)

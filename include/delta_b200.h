@@ -292,6 +292,31 @@ delta_status delta_sphere_mesh_contacts(delta_ctx *ctx, const delta_spheres *sph
 delta_status delta_sphere_overlap(delta_ctx *ctx, const double *centre, int64_t ld, const double *radius,
                                   const int32_t *pair_a, const int32_t *pair_b, int64_t n_pairs, uint8_t *overlap);
 
+/* ---- on-disk formats ------------------------------------------------------------------
+ * The legacy ASCII VTK snapshot of all triangles, as writeGeometryToVTK writes it
+ * (delta/core/io/write.cpp:226-306: file path + "geometry_<step>.vtk", POINTS at %.5f,
+ * one triangle cell per three points, CELL_TYPES 5).  _host takes host arrays; the device
+ * form copies the meshes back first (synchronises). */
+delta_status delta_write_vtk_host(const char *path, int32_t step, int32_t n_bodies, const int64_t *tri_offset,
+                                  const double *x, const double *y, const double *z);
+delta_status delta_write_vtk(delta_ctx *ctx, const char *path, int32_t step, const delta_meshes *meshes);
+/* The snapshot of a simulation's current vertices (obstacles included). */
+delta_status delta_sim_write_vtk(delta_sim *sim, const char *path, int32_t step);
+/* The .mbfcp scene reader (readmbfcp, delta/core/io/read.cpp:345-546): the material block's
+ * friction, spring, dashpot, density and gravity (parsed with std::stof at the reference's
+ * fixed offsets), the BODIES count, and every SPHERES body as (id, centre, radius) with the
+ * reference's fixed-offset fields.  Host memory; *n_out = the number of spheres, beyond
+ * capacity DELTA_ERR_CAPACITY; a malformed field gives DELTA_ERR_INVALID. */
+typedef struct {
+  int32_t *id;      /* [capacity] */
+  double *centre;   /* [capacity][3] */
+  double *radius;   /* [capacity] */
+  int32_t bodies;   /* the BODIES: count */
+  int32_t has_materials;
+  double friction, spring, dashpot, density, gravity[3];
+} delta_mbfcp;
+delta_status delta_read_mbfcp(const char *filename, delta_mbfcp *out, int64_t capacity, int64_t *n_out);
+
 /* ---- contact de-duplication ----------------------------------------------------------
  * filter.cpp (the reference defines these; its time step does not call them).  A run is a
  * maximal sequence of contacts with equal (master, slave), i.e. one particle pair's
