@@ -10,6 +10,8 @@
 // restores the serial order of the reference drivers, so the output is deterministic.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include "internal.h"
 #include "tri_cert.cuh"
 #include "tri_gjk.cuh"
@@ -32,6 +34,8 @@ struct RawContacts {
   uint64_t *sv;
   int64_t sv_cap;
   unsigned long long *sv_count;
+  // certified driver: per-body boxes (lo[3], hi[3]) for the row prefilter, or null
+  const double *bbox;
 };
 
 struct DevStats {
@@ -43,6 +47,7 @@ struct DevStats {
 
 struct RowCtx {
   int64_t k;       // pair index
+  int32_t bB;      // body B
   int32_t iA;      // triangle of A (within the body)
   int64_t tA, tB0; // global triangle indices
   int32_t nB;
@@ -183,6 +188,19 @@ __device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawCon
       ahi[k] = fmax(A[0][k], fmax(A[1][k], A[2][k]));
     }
     const double cull = mg * (1.0 + 1e-9) + 1e-12;
+    if (rc.bbox) {
+      // row prefilter: every B triangle box lies in B's body box, so when A's triangle box
+      // is farther than the cull distance from the body box no B triangle survives (the
+      // per-axis gaps and their squares are monotone in the boxes, so the skip is exact)
+      const double *bb = rc.bbox + 6 * (int64_t)r.bB;
+      double g2 = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double g = fmax(bb[k] - ahi[k], alo[k] - bb[3 + k]);
+        if (g > 0.0) g2 += g * g;
+      }
+      if (g2 > cull * cull) return;
+    }
     const int lane_ = lane;
     for (int32_t base = 0; base < r.nB; base += 32) {
       const int32_t tb = base + lane_;
@@ -297,6 +315,36 @@ __device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawCon
   }
 }
 
+// per-body bounding boxes of the current vertices: one warp per body
+__global__ void k_body_boxes(delta_meshes m, double *__restrict__ bbox) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b = warp; b < m.n_bodies; b += nwarps) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t v = 3 * m.tri_offset[b] + lane; v < 3 * m.tri_offset[b + 1]; v += 32) {
+      const double c[3] = {__ldg(m.x + v), __ldg(m.y + v), __ldg(m.z + v)};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = fmin(lo[k], c[k]);
+        hi[k] = fmax(hi[k], c[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      for (int o = 16; o > 0; o >>= 1) {
+        lo[k] = fmin(lo[k], __shfl_xor_sync(kFull, lo[k], o));
+        hi[k] = fmax(hi[k], __shfl_xor_sync(kFull, hi[k], o));
+      }
+    }
+    if (lane == 0)
+      for (int k = 0; k < 3; ++k) {
+        bbox[6 * b + k] = lo[k];
+        bbox[6 * b + 3 + k] = hi[k];
+      }
+  }
+}
+
 template <class R, int DRV>
 __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *__restrict__ pa,
                                                 const int32_t *__restrict__ pb,
@@ -307,10 +355,16 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
   const int64_t total_rows = *total_rows_p;
   __shared__ CertWarpSmem cert_sm[DRV == DELTA_DRV_BF_CERT ? 4 : 1];
   CertWarpSmem *csm = &cert_sm[DRV == DELTA_DRV_BF_CERT ? (threadIdx.x >> 5) : 0];
+  // rows are taken from the queue in batches (the certified driver's prefilter makes most
+  // rows cheap, so one atomic per row would make the queue the bottleneck)
+  constexpr unsigned long long kBatch = DRV == DELTA_DRV_BF_CERT ? 8 : 1;
+  unsigned long long row = 0, batch_end = 0;
   for (;;) {
-    unsigned long long row = 0;
-    if (lane == 0) row = atomicAdd(queue, 1ull);
-    row = __shfl_sync(kFull, row, 0);
+    if (row >= batch_end) {
+      if (lane == 0) row = atomicAdd(queue, kBatch);
+      row = __shfl_sync(kFull, row, 0);
+      batch_end = row + kBatch;
+    }
     if ((int64_t)row >= total_rows) return;
     // pair k: last k with row_offset[k] <= row
     int64_t lo = 0, hi = n_pairs;
@@ -322,6 +376,7 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
     RowCtx r;
     r.k = lo;
     const int32_t a = pa[lo], b = pb[lo];
+    r.bB = b;
     r.iA = (int32_t)((int64_t)row - row_offset[lo]);
     r.tA = m.tri_offset[a] + r.iA;
     r.tB0 = m.tri_offset[b];
@@ -336,6 +391,7 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
       if (DRV != DELTA_DRV_BF_CERT) atomicAdd(&st->evaluated, (unsigned long long)r.nB);
     }
     process_row<R, DRV>(m, r, rc, st, csm);
+    ++row;
   }
 }
 
@@ -568,6 +624,16 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   int64_t cap = out->capacity > 1024 ? out->capacity : 1024;
   unsigned long long hcount = 0;
   RawContacts rc{};
+  if (driver == DELTA_DRV_BF_CERT) {
+    // body boxes of the current vertices for the row prefilter
+    void *bb = nullptr;
+    if ((st = ctx_scratch(ctx, 23, 48 * (size_t)m.n_bodies + 64, &bb)) != DELTA_OK) return st;
+    const int64_t warps = std::min<int64_t>(m.n_bodies, (int64_t)kNumSMs * 64);
+    k_body_boxes<<<(unsigned)std::max<int64_t>(1, (warps * 32 + 127) / 128), 128, 0, s>>>(m, (double *)bb);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "body boxes");
+    ctx->launches += 1;
+    rc.bbox = (const double *)bb;
+  }
   for (int attempt = 0; attempt < 2; ++attempt) {
     void *raw = nullptr;
     const size_t per = 14 * sizeof(double) + 4 * sizeof(int32_t) + 1 + 2 * sizeof(uint64_t);
@@ -706,7 +772,7 @@ size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap) {
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
-                              void *temp, size_t temp_bytes) {
+                              void *temp, size_t temp_bytes, double *bbox) {
   cudaError_t e;
   const int64_t cap = out.capacity;
   char *p = (char *)state;
@@ -731,6 +797,12 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   rc.sv = (uint64_t *)p;
   rc.sv_cap = fixed_sv_cap(cap);
   rc.sv_count = queue + 2;
+  rc.bbox = bbox;
+  if (bbox && driver == DELTA_DRV_BF_CERT) {
+    const int64_t warps = std::min<int64_t>(m.n_bodies, (int64_t)kNumSMs * 64);
+    k_body_boxes<<<(unsigned)std::max<int64_t>(1, (warps * 32 + 127) / 128), 128, 0, s>>>(m, bbox);
+    ctx->launches += 1;
+  }
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
   if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");
   k_rows_fixed<<<(unsigned)((pair_cap + 256) / 256), 256, 0, s>>>(m.tri_offset, pa, pair_cap, rows);

@@ -48,7 +48,7 @@ size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap);
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
-                              void *temp, size_t temp_bytes);
+                              void *temp, size_t temp_bytes, double *bbox = nullptr);
 
 // Thread-local last-error text (capi.cu).
 delta_status set_error(delta_status st, const std::string &msg);

@@ -795,6 +795,7 @@ struct delta_sim {
     size_t temp_bytes = 0;
     delta_contacts c{};
     int64_t *d_nc = nullptr, *d_step = nullptr, *d_cnt = nullptr, *d_log = nullptr;
+    double *bbox = nullptr;  // per-body boxes for the certified driver's row prefilter
     int *d_ovf = nullptr, *d_snap = nullptr;
     int64_t log_len = 0;
     cudaStream_t stream = nullptr;
@@ -880,9 +881,10 @@ static void graph_release(delta_sim::Graph &g) {
   g.exec = nullptr;
   g.graph = nullptr;
   g.captured = false;
-  for (void *p : {(void *)g.pa, g.bp, g.fs, g.ds, g.temp, g.c_mem, g.dev})
+  for (void *p : {(void *)g.pa, g.bp, g.fs, g.ds, g.temp, g.c_mem, g.dev, (void *)g.bbox})
     if (p) cudaFree(p);
   g.pa = g.pb = nullptr;
+  g.bbox = nullptr;
   g.bp = g.fs = g.ds = g.temp = g.c_mem = g.dev = nullptr;
 }
 
@@ -905,7 +907,8 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
       (e = cudaMalloc(&g.fs, forces_fixed_state_bytes(contact_cap))) != cudaSuccess ||
       (e = cudaMalloc(&g.ds, detect_fixed_state_bytes(pair_cap, contact_cap))) != cudaSuccess ||
       (e = cudaMalloc(&g.temp, g.temp_bytes)) != cudaSuccess || (e = cudaMalloc(&g.c_mem, cbytes)) != cudaSuccess ||
-      (e = cudaMalloc(&g.dev, 256 + sizeof(int64_t) * (size_t)log_len)) != cudaSuccess)
+      (e = cudaMalloc(&g.dev, 256 + sizeof(int64_t) * (size_t)log_len)) != cudaSuccess ||
+      (e = cudaMalloc(&g.bbox, 48 * (size_t)n + 64)) != cudaSuccess)
     return cuda_error(e, "graph buffers");
   g.pb = g.pa + pair_cap;
   double *d = (double *)g.c_mem;
@@ -942,7 +945,7 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
                  s->scene.eps,      s->scene.friction,   s->ids};
   const int64_t before = s->ctx->launches;
   if ((ds = detect_run_fixed(s->ctx, st, s->driver, m, g.pa, g.pb, g.pair_cap, g.c, g.d_nc, g.d_ovf, 1, g.d_cnt,
-                             nullptr, g.ds, g.temp, g.temp_bytes)) != DELTA_OK)
+                             nullptr, g.ds, g.temp, g.temp_bytes, g.bbox)) != DELTA_OK)
     return ds;
   k += (int)(s->ctx->launches - before);
   s->ctx->launches = before;
