@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--timestep-steps", type=int, default=200)
     ap.add_argument("--hopper-steps", type=int, default=50)
+    ap.add_argument("--box-steps", type=int, default=0,
+                    help="time steps of the 200,000-particle box (off by default: its scene takes minutes to build)")
     return ap.parse_args()
 
 
@@ -446,7 +448,7 @@ def main():
                "h2d_bytes_per_step": int(ha.nbytes + hb.nbytes),
                "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes), "path": path}
 
-    ts = hop = None
+    ts = hop = box = None
     if args.timestep_steps > 0:
         from delta_b200.engine import StepParams
         from delta_b200.scenarios import hopper_scene, lattice_scene
@@ -456,6 +458,14 @@ def main():
             "256 perturbed icospheres (80 tri) on a 8x4x8 lattice over a 2-triangle floor, FP64, dt 1e-5, k 1e6, "
             "damping 0.1", args.timestep_steps, 3,
             StepParams.make(dt=1e-5, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0))
+        if args.box_steps > 0:
+            from delta_b200.scenarios import box_scene
+
+            box = timestep_section(
+                ctx, stream, box_scene(200000, seed=args.seed),
+                "200,000 perturbed spheres of {80,160,320,500} triangles (r 4-12 mm, 53 M triangles) poured from a "
+                "lattice into a 0.6 x 1.2 x 0.6 m box of 12 wall triangles, FP64, dt 2e-6", args.box_steps, 2,
+                StepParams.make(dt=2e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0))
         if args.hopper_steps > 0:
             hop = timestep_section(
                 ctx, stream, hopper_scene(10000, seed=args.seed),
@@ -502,6 +512,7 @@ def main():
             "cpu_baseline": cpu,
             "timestep": ts,
             "timestep_hopper": hop,
+            "timestep_box": box,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
