@@ -699,39 +699,75 @@ __global__ void k_penalty_warm(int64_t n, const double *a, const double *b, int6
   iters[i] = (uint8_t)it;
 }
 
-// Closest point of triangle (V0, V0+E0, V0+E1) to X: barycentric (s, t) by Eberly's region
-// classification (FP32; any feasible answer is acceptable here, the certificate decides).
-__device__ __forceinline__ void closest_on_tri(const float *V0, const float *E0, const float *E1, const float *X,
-                                               float &s, float &t) {
+// Closest point of triangle (V0, V0+E0, V0+E1) to X in FP32, branch-free: the interior
+// solution of the 2x2 normal equations when it lies inside, otherwise the nearest of the
+// three edges' clamped projections (all computed, one selected), so the lanes of a warp
+// never diverge.  Barycentric (s, t); returns the squared distance less |V0-X|^2.
+__device__ __forceinline__ float closest_on_tri(const float *V0, const float *E0, const float *E1, const float *X,
+                                                float &s, float &t) {
   float D[3];
+#pragma unroll
   for (int k = 0; k < 3; ++k) D[k] = V0[k] - X[k];
   const float a = dot3(E0, E0), b = dot3(E0, E1), c = dot3(E1, E1), d = dot3(E0, D), e = dot3(E1, D);
-  const float det = fmaxf(a * c - b * b, 1e-30f);
-  s = b * e - c * d;
-  t = b * d - a * e;
-  if (s + t <= det) {
-    if (s < 0.f) {
-      if (t < 0.f) {
-        if (d < 0.f) { t = 0.f; s = fminf(fmaxf(-d / a, 0.f), 1.f); }
-        else { s = 0.f; t = fminf(fmaxf(-e / c, 0.f), 1.f); }
-      } else { s = 0.f; t = fminf(fmaxf(-e / c, 0.f), 1.f); }
-    } else if (t < 0.f) { t = 0.f; s = fminf(fmaxf(-d / a, 0.f), 1.f); }
-    else { s /= det; t /= det; }
-  } else {
-    if (s < 0.f) {
-      const float tmp0 = b + d, tmp1 = c + e;
-      if (tmp1 > tmp0) { s = fminf((tmp1 - tmp0) / fmaxf(a - 2.f * b + c, 1e-30f), 1.f); t = 1.f - s; }
-      else { s = 0.f; t = fminf(fmaxf(-e / c, 0.f), 1.f); }
-    } else if (t < 0.f) {
-      const float tmp0 = b + e, tmp1 = a + d;
-      if (tmp1 > tmp0) { t = fminf((tmp1 - tmp0) / fmaxf(a - 2.f * b + c, 1e-30f), 1.f); s = 1.f - t; }
-      else { t = 0.f; s = fminf(fmaxf(-d / a, 0.f), 1.f); }
-    } else {
-      const float numer = c + e - b - d;
-      s = numer <= 0.f ? 0.f : fminf(numer / fmaxf(a - 2.f * b + c, 1e-30f), 1.f);
-      t = 1.f - s;
-    }
+  const float idet = __fdividef(1.f, fmaf(a, c, -b * b));
+  const float si = fmaf(b, e, -c * d) * idet, ti = fmaf(b, d, -a * e) * idet;
+  // squared distance at (s, t) minus |D|^2
+  auto q = [&](float u, float v) { return fmaf(u, fmaf(a, u, fmaf(2.f * b, v, 2.f * d)), v * fmaf(c, v, 2.f * e)); };
+  const float s0 = a > 0.f ? fminf(fmaxf(__fdividef(-d, a), 0.f), 1.f) : 0.f;  // edge t = 0
+  const float t1 = c > 0.f ? fminf(fmaxf(__fdividef(-e, c), 0.f), 1.f) : 0.f;  // edge s = 0
+  const float den = a - 2.f * b + c;
+  const float l2 = den > 0.f ? fminf(fmaxf(__fdividef(c + e - b - d, den), 0.f), 1.f) : 0.f;  // edge s + t = 1
+  float best = q(s0, 0.f);
+  s = s0;
+  t = 0.f;
+  const float q1 = q(0.f, t1), q2 = q(l2, 1.f - l2);
+  if (q1 < best) { best = q1; s = 0.f; t = t1; }
+  if (q2 < best) { best = q2; s = l2; t = 1.f - l2; }
+  if (si >= 0.f && ti >= 0.f && si + ti <= 1.f) { s = si; t = ti; best = q(si, ti); }
+  return best;
+}
+
+// FP32 distance of vertex-face pair (X, triangle V0 V1 V2), branch-free.
+__device__ __forceinline__ float pt_tri_dist32(const float *V0, const float *V1, const float *V2, const float *X) {
+  float E0[3], E1[3], s, t;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    E0[k] = V1[k] - V0[k];
+    E1[k] = V2[k] - V0[k];
   }
+  closest_on_tri(V0, E0, E1, X, s, t);
+  float r2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float r = fmaf(s, E0[k], fmaf(t, E1[k], V0[k] - X[k]));
+    r2 = fmaf(r, r, r2);
+  }
+  return sqrtf(r2);
+}
+
+// FP32 distance of edge pair (TA->HA, TB->HB): clamped closest parameters, branch-free.
+__device__ __forceinline__ float seg_seg_dist32(const float *HA, const float *TA, const float *HB, const float *TB) {
+  float u[3], v[3], w[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    u[k] = HA[k] - TA[k];
+    v[k] = HB[k] - TB[k];
+    w[k] = TA[k] - TB[k];
+  }
+  const float a = dot3(u, u), e = dot3(v, v), b = dot3(u, v), c = dot3(u, w), f = dot3(v, w);
+  const float den = fmaf(a, e, -b * b);
+  float s = den > 1e-12f * (a * e) ? fminf(fmaxf(__fdividef(fmaf(b, f, -c * e), den), 0.f), 1.f) : 0.f;
+  const float traw = e > 0.f ? __fdividef(fmaf(b, s, f), e) : 0.f;
+  const float t = fminf(fmaxf(traw, 0.f), 1.f);
+  const float s2 = a > 0.f ? fminf(fmaxf(__fdividef(fmaf(b, t, -c), a), 0.f), 1.f) : 0.f;
+  s = traw != t ? s2 : s;
+  float r2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float r = fmaf(s, u[k], fmaf(-t, v[k], w[k]));
+    r2 = fmaf(r, r, r2);
+  }
+  return sqrtf(r2);
 }
 
 // First index of the largest / smallest of three values.
@@ -829,7 +865,7 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
   // opposite vertex ea+2).  Operands are selected, not indexed, so all lanes run the
   // same code whichever features they picked.
   int ea = (kA + 1) % 3, eb = (kB + 1) % 3;
-  float HA[3], TA[3], HB[3], TB[3], f0, f1;
+  float HA[3], TA[3], HB[3], TB[3];
   bool faceB;  // chosen vertex-face feature: A's vertex vtx on face B, else B's vertex vtx on face A
   int vtx;
   float dpt, de;
@@ -837,8 +873,8 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
     float X1[3], X2[3];
     pick_vertex(Bf, jB, X1);
     pick_vertex(Af, iA, X2);
-    const float d1 = pt_tri_ref(Af[0], Af[1], Af[2], X1, f0, f1);
-    const float d2 = pt_tri_ref(Bf[0], Bf[1], Bf[2], X2, f0, f1);
+    const float d1 = pt_tri_dist32(Af[0], Af[1], Af[2], X1);
+    const float d2 = pt_tri_dist32(Bf[0], Bf[1], Bf[2], X2);
     faceB = d2 < d1;
     vtx = faceB ? iA : jB;
     dpt = faceB ? d2 : d1;
@@ -849,8 +885,7 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
     vtx = 0;
 #pragma unroll
     for (int j = 0; j < 6; ++j) {
-      const float dj = j < 3 ? pt_tri_ref(Af[0], Af[1], Af[2], Bf[j], f0, f1)
-                             : pt_tri_ref(Bf[0], Bf[1], Bf[2], Af[j - 3], f0, f1);
+      const float dj = j < 3 ? pt_tri_dist32(Af[0], Af[1], Af[2], Bf[j]) : pt_tri_dist32(Bf[0], Bf[1], Bf[2], Af[j - 3]);
       if (dj < dpt) { dpt = dj; faceB = j >= 3; vtx = j % 3; }
     }
   }
@@ -859,7 +894,7 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
     de = 1e30f;
 #pragma unroll
     for (int j = 0; j < 9; ++j) {
-      const float dj = seg_seg_ref(Af[j / 3], Af[(j / 3 + 1) % 3], Bf[j % 3], Bf[(j % 3 + 1) % 3], f0, f1);
+      const float dj = seg_seg_dist32(Af[j / 3], Af[(j / 3 + 1) % 3], Bf[j % 3], Bf[(j % 3 + 1) % 3]);
       if (dj < de) { de = dj; ea = j / 3; eb = j % 3; }
     }
   } else if constexpr (CAND == 11) {
@@ -874,7 +909,7 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
       pick_vertex(Af, (xa + 1) % 3, TA);
       pick_vertex(Bf, xb, HB);
       pick_vertex(Bf, (xb + 1) % 3, TB);
-      const float dj = seg_seg_ref(HA, TA, HB, TB, f0, f1);
+      const float dj = seg_seg_dist32(HA, TA, HB, TB);
       if (dj < de || (dj == de && 3 * xa + xb < 3 * ea + eb)) { de = dj; ea = xa; eb = xb; }
     }
   } else {
@@ -882,7 +917,7 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
     pick_vertex(Af, (ea + 1) % 3, TA);
     pick_vertex(Bf, eb, HB);
     pick_vertex(Bf, (eb + 1) % 3, TB);
-    de = seg_seg_ref(HA, TA, HB, TB, f0, f1);
+    de = seg_seg_dist32(HA, TA, HB, TB);
   }
   const bool edge = dpt > de;
   xf64 pq[6];
