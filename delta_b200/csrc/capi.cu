@@ -4,6 +4,8 @@
 #include <string>
 #include <vector>
 
+#include <algorithm>
+
 #include "internal.h"
 
 namespace delta {
@@ -38,6 +40,71 @@ delta_status ctx_scratch(delta_ctx *ctx, int slot, size_t bytes, void **out) {
   }
   *out = b.ptr;
   return DELTA_OK;
+}
+
+delta_status host_pipeline(
+    delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld, double *p, double *q, double *dist,
+    uint8_t *flags,
+    const std::function<delta_status(int64_t, int64_t, const double *, const double *, int64_t, double *, double *,
+                                     double *, uint8_t *)> &run,
+    const std::function<delta_status(int)> &after) {
+  // device layout: a(9n) b(9n) p(3n) q(3n) dist(n) | flags(n)
+  const size_t nd = (size_t)n;
+  void *buf = nullptr, *fbuf = nullptr;
+  delta_status st;
+  if ((st = ctx_scratch(ctx, 0, sizeof(double) * 25 * nd, &buf)) != DELTA_OK) return st;
+  if ((st = ctx_scratch(ctx, 1, nd, &fbuf)) != DELTA_OK) return st;
+  double *da = (double *)buf, *db = da + 9 * nd, *dp = db + 9 * nd, *dq = dp + 3 * nd, *dd = dq + 3 * nd;
+  uint8_t *df = (uint8_t *)fbuf;
+  cudaError_t e = cudaSuccess;
+  if (!ctx->copy_in && (e = cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_error(e, "copy stream");
+  if (!ctx->copy_out && (e = cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_error(e, "copy stream");
+  for (auto &ev : ctx->events)
+    if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_error(e, "copy events");
+  // up to 8 chunks of at least 2^18 pairs; event 0 starts the H2D after the context's
+  // earlier work, 1+3k and 2+3k mark the end of chunk k's H2D and compute, the last one
+  // the end of the copies
+  const int64_t min_chunk = 1 << 18;
+  int chunks = (int)std::min<int64_t>(8, std::max<int64_t>(1, n / min_chunk));
+  const int64_t chunk = (n + chunks - 1) / chunks;
+  chunks = (int)((n + chunk - 1) / chunk);
+  cudaEvent_t *ev = ctx->events;
+  if ((e = cudaEventRecord(ev[0], ctx->stream)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(ctx->copy_in, ev[0], 0)) != cudaSuccess)
+    return cuda_error(e, "pipeline start");
+  const size_t hp = sizeof(double) * (size_t)ld, dp_pitch = sizeof(double) * nd;
+  for (int k = 0; k < chunks; ++k) {
+    const int64_t c0 = k * chunk, nc = std::min<int64_t>(chunk, n - c0);
+    const size_t w = sizeof(double) * (size_t)nc;
+    e = cudaMemcpy2DAsync(da + c0, dp_pitch, a + c0, hp, w, 9, cudaMemcpyHostToDevice, ctx->copy_in);
+    if (e == cudaSuccess) e = cudaMemcpy2DAsync(db + c0, dp_pitch, b + c0, hp, w, 9, cudaMemcpyHostToDevice, ctx->copy_in);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1 + 3 * k], ctx->copy_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ev[1 + 3 * k], 0);
+    if (e != cudaSuccess) return cuda_error(e, "pipeline H2D");
+    if ((st = run(c0, nc, da + c0, db + c0, (int64_t)nd, dp + c0, dq + c0, dd + c0, flags ? df + c0 : nullptr)) !=
+        DELTA_OK)
+      return st;
+    if (after && (st = after(k)) != DELTA_OK) return st;
+    e = cudaEventRecord(ev[2 + 3 * k], ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_out, ev[2 + 3 * k], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(p + c0, hp, dp + c0, dp_pitch, w, 3, cudaMemcpyDeviceToHost, ctx->copy_out);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(q + c0, hp, dq + c0, dp_pitch, w, 3, cudaMemcpyDeviceToHost, ctx->copy_out);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dist + c0, dd + c0, w, cudaMemcpyDeviceToHost, ctx->copy_out);
+    if (e == cudaSuccess && flags)
+      e = cudaMemcpyAsync(flags + c0, df + c0, (size_t)nc, cudaMemcpyDeviceToHost, ctx->copy_out);
+    if (e != cudaSuccess) return cuda_error(e, "pipeline D2H");
+  }
+  // the context stream continues after the last copy
+  cudaEvent_t last = ev[sizeof(ctx->events) / sizeof(ctx->events[0]) - 1];
+  if ((e = cudaEventRecord(last, ctx->copy_out)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(ctx->stream, last, 0)) != cudaSuccess)
+    return cuda_error(e, "pipeline end");
+  return cuda_error(cudaStreamSynchronize(ctx->stream), "pipeline sync");
 }
 
 delta_status ctx_pinned(delta_ctx *ctx, size_t bytes, void **out) {
@@ -87,6 +154,10 @@ delta_status delta_destroy(delta_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto &b : ctx->scratch)
     if (b.ptr) cudaFree(b.ptr);
+  for (auto &ev : ctx->events)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+  if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   delete ctx;
   return DELTA_OK;
@@ -195,43 +266,15 @@ delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int
                                   uint8_t *flags) {
   delta_status st = check_pairs(ctx, method, precision, n, a, b, ld, p, q, dist);
   if (st != DELTA_OK || n == 0) return st;
-  // device layout: a(9n) b(9n) p(3n) q(3n) dist(n) | flags(n)
-  const size_t nd = (size_t)n;
-  void *buf = nullptr, *fbuf = nullptr;
-  if ((st = ctx_scratch(ctx, 0, sizeof(double) * 25 * nd, &buf)) != DELTA_OK) return st;
-  if ((st = ctx_scratch(ctx, 1, nd, &fbuf)) != DELTA_OK) return st;
-  double *da = (double *)buf, *db = da + 9 * nd, *dp = db + 9 * nd, *dq = dp + 3 * nd, *dd = dq + 3 * nd;
-  uint8_t *df = (uint8_t *)fbuf;
-  cudaError_t e = cudaSuccess;
-  if (ld == n) {
-    e = cudaMemcpyAsync(da, a, sizeof(double) * 9 * nd, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(db, b, sizeof(double) * 9 * nd, cudaMemcpyHostToDevice, ctx->stream);
-  } else {
-    e = cudaMemcpy2DAsync(da, sizeof(double) * nd, a, sizeof(double) * ld, sizeof(double) * nd, 9,
-                          cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpy2DAsync(db, sizeof(double) * nd, b, sizeof(double) * ld, sizeof(double) * nd, 9,
-                            cudaMemcpyHostToDevice, ctx->stream);
-  }
-  if (e != cudaSuccess) return cuda_error(e, "pairs H2D");
-  e = launch_pairs_cfg(method, precision, ctx->stream, n, da, db, n, max_error, dp, dq, dd, flags ? df : nullptr,
-                       ctx_pair_launch(ctx, method, precision));
-  if (e != cudaSuccess) return cuda_error(e, "pairs kernel launch");
-  ctx->launches += 1;
-  if (ld == n) {
-    e = cudaMemcpyAsync(p, dp, sizeof(double) * 3 * nd, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(q, dq, sizeof(double) * 3 * nd, cudaMemcpyDeviceToHost, ctx->stream);
-  } else {
-    e = cudaMemcpy2DAsync(p, sizeof(double) * ld, dp, sizeof(double) * nd, sizeof(double) * nd, 3,
-                          cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpy2DAsync(q, sizeof(double) * ld, dq, sizeof(double) * nd, sizeof(double) * nd, 3,
-                            cudaMemcpyDeviceToHost, ctx->stream);
-  }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dist, dd, sizeof(double) * nd, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess && flags) e = cudaMemcpyAsync(flags, df, nd, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e != cudaSuccess) return cuda_error(e, "pairs D2H");
-  return cuda_error(cudaStreamSynchronize(ctx->stream), "pairs sync");
+  const PairLaunch cfg = ctx_pair_launch(ctx, method, precision);
+  return host_pipeline(ctx, n, a, b, ld, p, q, dist, flags,
+                       [&](int64_t, int64_t nc, const double *da, const double *db, int64_t ldd, double *dp,
+                           double *dq, double *dd, uint8_t *df) -> delta_status {
+                         cudaError_t e = launch_pairs_cfg(method, precision, ctx->stream, nc, da, db, ldd, max_error,
+                                                          dp, dq, dd, df, cfg);
+                         ctx->launches += 1;
+                         return cuda_error(e, "pairs kernel launch");
+                       });
 }
 
 delta_status delta_detect(delta_ctx *ctx, int driver, int precision, const delta_meshes *meshes,

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 
 #include "delta_b200.h"
@@ -69,13 +70,28 @@ struct delta_ctx {
   // launch shapes of the pair kernels [method][precision], set by autotuning
   delta::PairLaunch pair_launch[6][2];
   bool pair_launch_set[6][2] = {};
-  delta_buffer scratch[24];
+  delta_buffer scratch[32];
+  // host-buffer entry points: copy streams and per-chunk events of the pipelined transfers
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t events[3 * 16] = {};
   int mlp_engine = DELTA_MLP_TCGEN05;  // network engine of the learned hybrid
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
 };
 
 namespace delta {
+// Host-buffer pipeline: stages the pair list (a, b: 9 planes of ld doubles) through the
+// device in chunks, H2D on one copy stream, `run` on the context stream, D2H of p, q, dist
+// (and flags when given) on another, so transfers of neighbouring chunks overlap the
+// compute.  `run(c0, nc, da, db, ldd, dp, dq, dd, df)` enqueues chunk [c0, c0+nc) on the
+// context stream (device planes of pitch ldd); `after(k)` (optional) enqueues per-chunk
+// bookkeeping after it.  Synchronises.
+delta_status host_pipeline(
+    delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld, double *p, double *q, double *dist,
+    uint8_t *flags,
+    const std::function<delta_status(int64_t, int64_t, const double *, const double *, int64_t, double *, double *,
+                                     double *, uint8_t *)> &run,
+    const std::function<delta_status(int)> &after = nullptr);
 // Returns a device buffer of at least `bytes` in slot `slot` of the context.
 delta_status ctx_scratch(delta_ctx *ctx, int slot, size_t bytes, void **out);
 delta_status ctx_pinned(delta_ctx *ctx, size_t bytes, void **out);

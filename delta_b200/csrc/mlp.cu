@@ -1041,6 +1041,14 @@ delta_status mlp_check_error(delta_ctx *ctx, const int *err) {
   return DELTA_OK;
 }
 
+// The learned pipeline enqueued on the context stream: network (when params are given),
+// refine with the device list of uncertified pairs, exact fallback over that list.
+// *count_out: device count of listed pairs; *err_out: the network's time-out flag or null.
+delta_status learned_enqueue(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                             const float *params, const void *params_bf16, int sweeps, int features, double rel_tol,
+                             double *p, double *q, double *dist, uint8_t *flags, uint32_t **count_out,
+                             int **err_out);
+
 void launch_refine(int features, cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld,
                    const float *x0, int sweeps, double rel_tol, double *p, double *q, double *dist, uint8_t *flags,
                    uint32_t *list, uint32_t *count) {
@@ -1049,6 +1057,40 @@ void launch_refine(int features, cudaStream_t s, int64_t n, const double *a, con
   else if (features == 15) k_learned_refine<15><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
   else if (features == 7) k_learned_refine<7><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
   else k_learned_refine<3><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+}
+
+delta_status learned_enqueue(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
+                             const float *params, const void *params_bf16, int sweeps, int features, double rel_tol,
+                             double *p, double *q, double *dist, uint8_t *flags, uint32_t **count_out,
+                             int **err_out) {
+  delta_status st;
+  float *x0 = nullptr;
+  *err_out = nullptr;
+  if (params) {
+    void *buf;
+    if ((st = ctx_scratch(ctx, 13, sizeof(float) * 4 * (size_t)n, &buf)) != DELTA_OK) return st;
+    x0 = static_cast<float *>(buf);
+    if ((reinterpret_cast<uintptr_t>(params_bf16) & 15))
+      return set_error(DELTA_ERR_INVALID, "learned pipeline: params_bf16 must be 16-byte aligned");
+    if ((st = mlp_infer_launch(ctx, ctx->mlp_engine, n, a, b, ld, params, params_bf16, x0, err_out)) != DELTA_OK)
+      return st;
+  }
+  void *lbuf;
+  if ((st = ctx_scratch(ctx, 14, 256 + sizeof(uint32_t) * (size_t)n, &lbuf)) != DELTA_OK) return st;
+  uint32_t *count = static_cast<uint32_t *>(lbuf);
+  uint32_t *list = reinterpret_cast<uint32_t *>(static_cast<char *>(lbuf) + 256);
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "learned pipeline: memset");
+  launch_refine(features, ctx->stream, n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+  ctx->launches += 1;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "learned pipeline: refine");
+  const PairLaunch cfg = ctx->pair_launch_set[DELTA_BF_CERT][0] ? ctx->pair_launch[DELTA_BF_CERT][0]
+                                                                : default_pair_launch(DELTA_BF_CERT);
+  e = launch_cert_indexed(ctx->stream, count, n, list, a, b, ld, p, q, dist, cfg);
+  ctx->launches += 1;
+  if (e != cudaSuccess) return cuda_error(e, "learned pipeline: exact fallback");
+  *count_out = count;
+  return DELTA_OK;
 }
 
 }  // namespace
@@ -1216,75 +1258,70 @@ delta_status delta_pairs_run_learned(delta_ctx *ctx, int64_t n, const double *a,
     return set_error(DELTA_ERR_INVALID, "delta_pairs_run_learned: bad argument");
   if (n_fallback) *n_fallback = 0;
   if (n == 0) return DELTA_OK;
-  delta_status st;
-  float *x0 = nullptr;
+  uint32_t *count = nullptr;
   int *mlp_err = nullptr;
-  if (params) {
-    void *buf;
-    if ((st = ctx_scratch(ctx, 13, sizeof(float) * 4 * (size_t)n, &buf)) != DELTA_OK) return st;
-    x0 = static_cast<float *>(buf);
-    if ((reinterpret_cast<uintptr_t>(params_bf16) & 15))
-      return set_error(DELTA_ERR_INVALID, "delta_pairs_run_learned: params_bf16 must be 16-byte aligned");
-    if ((st = mlp_infer_launch(ctx, ctx->mlp_engine, n, a, b, ld, params, params_bf16, x0, &mlp_err)) != DELTA_OK)
-      return st;
-  }
-  void *lbuf;
-  if ((st = ctx_scratch(ctx, 14, 256 + sizeof(uint32_t) * (size_t)n, &lbuf)) != DELTA_OK) return st;
-  uint32_t *count = static_cast<uint32_t *>(lbuf);
-  uint32_t *list = reinterpret_cast<uint32_t *>(static_cast<char *>(lbuf) + 256);
-  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), ctx->stream);
-  if (e != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: memset");
-  launch_refine(features, ctx->stream, n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
-  ctx->launches += 1;
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: refine");
-  const PairLaunch cfg = ctx->pair_launch_set[DELTA_BF_CERT][0] ? ctx->pair_launch[DELTA_BF_CERT][0]
-                                                                : default_pair_launch(DELTA_BF_CERT);
-  e = launch_cert_indexed(ctx->stream, count, n, list, a, b, ld, p, q, dist, cfg);
-  ctx->launches += 1;
-  if (e != cudaSuccess) return cuda_error(e, "delta_pairs_run_learned: exact fallback");
-  if (n_fallback) {
-    void *pin;
-    if ((st = ctx_pinned(ctx, sizeof(uint32_t), &pin)) != DELTA_OK) return st;
-    if ((e = cudaMemcpyAsync(pin, count, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
-      return cuda_error(e, "delta_pairs_run_learned: count");
-    *n_fallback = *static_cast<uint32_t *>(pin);
-    // the warm start only steers the search (every result is certified or exact), but a
-    // tensor-core time-out is still reported
-    return mlp_check_error(ctx, mlp_err);
-  }
-  return DELTA_OK;
+  delta_status st = learned_enqueue(ctx, n, a, b, ld, params, params_bf16, sweeps, features, rel_tol, p, q, dist,
+                                    flags, &count, &mlp_err);
+  if (st != DELTA_OK || !n_fallback) return st;
+  void *pin;
+  if ((st = ctx_pinned(ctx, sizeof(uint32_t), &pin)) != DELTA_OK) return st;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(pin, count, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_error(e, "delta_pairs_run_learned: count");
+  *n_fallback = *static_cast<uint32_t *>(pin);
+  // the warm start only steers the search (every result is certified or exact), but a
+  // tensor-core time-out is still reported
+  return mlp_check_error(ctx, mlp_err);
 }
 
 delta_status delta_pairs_run_learned_host(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                                           const float *params, const void *params_bf16, int32_t sweeps,
                                           int32_t features, double rel_tol, double *p, double *q, double *dist,
                                           uint8_t *flags, int64_t *n_fallback) {
-  if (!ctx || n < 0 || ld < n || (n > 0 && (!a || !b || !p || !q || !dist)))
+  if (!ctx || n < 0 || ld < n || sweeps < 0 || n > (int64_t)UINT32_MAX ||
+      (features != 3 && features != 7 && features != 11 && features != 15) ||
+      (n > 0 && (!a || !b || !p || !q || !dist)) || ((params == nullptr) != (params_bf16 == nullptr)))
     return set_error(DELTA_ERR_INVALID, "delta_pairs_run_learned_host: bad argument");
   if (n_fallback) *n_fallback = 0;
   if (n == 0) return DELTA_OK;
-  // device staging: a(9n) b(9n) p(3n) q(3n) dist(n) | flags(n)
-  const size_t nd = (size_t)n;
-  void *buf = nullptr, *fbuf = nullptr;
-  delta_status st;
-  if ((st = ctx_scratch(ctx, 0, sizeof(double) * 25 * nd, &buf)) != DELTA_OK) return st;
-  if ((st = ctx_scratch(ctx, 1, nd, &fbuf)) != DELTA_OK) return st;
-  double *da = (double *)buf, *db = da + 9 * nd, *dp = db + 9 * nd, *dq = dp + 3 * nd, *dd = dq + 3 * nd;
-  uint8_t *df = (uint8_t *)fbuf;
-  const size_t row = sizeof(double) * nd, pitch = sizeof(double) * (size_t)ld;
-  cudaError_t e = cudaMemcpy2DAsync(da, row, a, pitch, row, 9, cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpy2DAsync(db, row, b, pitch, row, 9, cudaMemcpyHostToDevice, ctx->stream);
-  if (e != cudaSuccess) return cuda_error(e, "learned H2D");
-  if ((st = delta_pairs_run_learned(ctx, n, da, db, n, params, params_bf16, sweeps, features, rel_tol, dp, dq, dd,
-                                    flags ? df : nullptr, n_fallback)) != DELTA_OK)
-    return st;
-  e = cudaMemcpy2DAsync(p, pitch, dp, row, row, 3, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpy2DAsync(q, pitch, dq, row, row, 3, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dist, dd, row, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess && flags) e = cudaMemcpyAsync(flags, df, nd, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e != cudaSuccess) return cuda_error(e, "learned D2H");
-  return cuda_error(cudaStreamSynchronize(ctx->stream), "learned sync");
+  // per chunk: fallback count and network time-out flag, gathered on the device
+  void *sbuf;
+  delta_status st = ctx_scratch(ctx, 24, 64 * sizeof(uint32_t), &sbuf);
+  if (st != DELTA_OK) return st;
+  uint32_t *tally = static_cast<uint32_t *>(sbuf);
+  cudaError_t e = cudaMemsetAsync(tally, 0, 64 * sizeof(uint32_t), ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "learned host: tally");
+  uint32_t *count = nullptr;
+  int *mlp_err = nullptr;
+  int chunks = 0;
+  st = host_pipeline(
+      ctx, n, a, b, ld, p, q, dist, flags,
+      [&](int64_t, int64_t nc, const double *da, const double *db, int64_t ldd, double *dp, double *dq, double *dd,
+          uint8_t *df) {
+        return learned_enqueue(ctx, nc, da, db, ldd, params, params_bf16, sweeps, features, rel_tol, dp, dq, dd, df,
+                               &count, &mlp_err);
+      },
+      [&](int k) {
+        cudaError_t ce = cudaMemcpyAsync(tally + 2 * k, count, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream);
+        if (ce == cudaSuccess && mlp_err)
+          ce = cudaMemcpyAsync(tally + 2 * k + 1, mlp_err, sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream);
+        chunks = k + 1;
+        return cuda_error(ce, "learned host: tally");
+      });
+  if (st != DELTA_OK) return st;
+  uint32_t h[64];
+  if ((e = cudaMemcpy(h, tally, sizeof(uint32_t) * 2 * chunks, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return cuda_error(e, "learned host: tally read");
+  int64_t total = 0;
+  bool timeout = false;
+  for (int k = 0; k < chunks; ++k) {
+    total += h[2 * k];
+    timeout |= h[2 * k + 1] != 0;
+  }
+  if (n_fallback) *n_fallback = total;
+  if (timeout) return set_error(DELTA_ERR_TIMEOUT, "tcgen05 inference: bounded wait for the tensor cores gave up");
+  return DELTA_OK;
 }
 
 }  // extern "C"

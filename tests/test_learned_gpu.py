@@ -275,3 +275,18 @@ def test_learned_rejects_bad_arguments(ctx, pairs):
         learned_pairs(ctx, None, a, b, sweeps=1, features=5)
     with pytest.raises(DeltaError):
         learned_pairs(ctx, None, a, b, sweeps=-1)
+
+
+def test_learned_host_pipeline_many_chunks(ctx, trained):
+    """The pipelined host entry (several chunks, pitched host arrays) equals the device entry."""
+    from delta_b200.learned import learned_pairs, learned_pairs_host
+    from delta_b200.scenarios import narrowphase_pairs
+
+    n = (1 << 20) + 12345
+    a, b, _, _ = narrowphase_pairs(n, seed=31)
+    model = trained[0]
+    p, q, d, fl, nf = learned_pairs(ctx, model, _dev(a), _dev(b), sweeps=1, count_fallback=True, features=3)
+    hp, hq, hd, hfl, hnf = learned_pairs_host(ctx, model, a, b, sweeps=1, features=3)
+    assert nf == hnf > 0
+    assert np.array_equal(d.cpu().numpy(), hd) and np.array_equal(fl.cpu().numpy(), hfl)
+    assert np.array_equal(p.cpu().numpy(), hp) and np.array_equal(q.cpu().numpy(), hq)

@@ -99,6 +99,29 @@ def test_host_path_equals_device_path(ctx, workload):
     assert np.array_equal(hp, gp) and np.array_equal(hq, gq) and np.array_equal(hd, gd)
 
 
+def test_host_pipeline_many_chunks_and_pitch(ctx):
+    """The host entry point streams several chunks (transfers overlapping compute); with a
+    host pitch ld > n the results equal the device path and entries past n stay untouched."""
+    import ctypes
+
+    from delta_b200._lib import check, lib
+    from delta_b200.narrowphase import pairs_device
+    from delta_b200.scenarios import narrowphase_pairs
+
+    n, ld = (1 << 20) + 777, (1 << 20) + 1000
+    a, b, _, _ = narrowphase_pairs(n, seed=8)
+    A = np.zeros((9, ld)); B = np.zeros((9, ld))
+    A[:, :n] = a; B[:, :n] = b
+    P = np.full((3, ld), 7.0); Q = P.copy(); D = np.full(ld, 7.0); F = np.full(ld, 9, np.uint8)
+    ptr = lambda x: x.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    check(lib().delta_pairs_run_host(ctx.handle, 5, 0, n, ptr(A), ptr(B), ld, 0.0, ptr(P), ptr(Q), ptr(D), ptr(F)))
+    gp, gq, gd, gf = pairs_device(ctx, 5, _dev(a), _dev(b))
+    ctx.synchronize()
+    assert np.array_equal(P[:, :n], gp.cpu().numpy()) and np.array_equal(Q[:, :n], gq.cpu().numpy())
+    assert np.array_equal(D[:n], gd.cpu().numpy()) and np.array_equal(F[:n], gf.cpu().numpy())
+    assert np.all(P[:, n:] == 7.0) and np.all(D[n:] == 7.0) and np.all(F[n:] == 9)
+
+
 def test_padded_leading_dimension(ctx, oracle, workload):
     """ld > n: the planes are strided; entries past n are untouched."""
     import ctypes
