@@ -699,6 +699,14 @@ __global__ void k_penalty_warm(int64_t n, const double *a, const double *b, int6
   iters[i] = (uint8_t)it;
 }
 
+// A second load of a value read before (an asm load, so the compiler does not keep the
+// first one alive in registers instead).
+__device__ __forceinline__ double ld_again(const double *p) {
+  double v;
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
 // Closest point of triangle (V0, V0+E0, V0+E1) to X in FP32, branch-free: the interior
 // solution of the 2x2 normal equations when it lies inside, otherwise the nearest of the
 // three edges' clamped projections (all computed, one selected), so the lanes of a warp
@@ -816,21 +824,22 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n;
   const int64_t ii = valid ? i : n - 1;
-  xf64 A[3][3], B[3][3];
+  // FP32 copies relative to A0 (the distance is translation invariant); the FP64 values
+  // are loaded again for the FP64 stage (from L1/L2), so they are not held in registers
+  // through the FP32 search
   float Af[3][3], Bf[3][3];
-  double scale = 0.0;
-  for (int v = 0; v < 3; ++v)
-    for (int k = 0; k < 3; ++k) {
-      A[v][k] = xf64(__ldg(a + (3 * v + k) * ld + ii));
-      B[v][k] = xf64(__ldg(b + (3 * v + k) * ld + ii));
-      scale = fmax(scale, fmax(fabs(A[v][k].v), fabs(B[v][k].v)));
-    }
-  // FP32 copies relative to A0 (the distance is translation invariant)
-  for (int v = 0; v < 3; ++v)
-    for (int k = 0; k < 3; ++k) {
-      Af[v][k] = (float)(A[v][k].v - A[0][k].v);
-      Bf[v][k] = (float)(B[v][k].v - A[0][k].v);
-    }
+  {
+    double A0[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) A0[k] = __ldg(a + k * ld + ii);
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        Af[v][k] = (float)(__ldg(a + (3 * v + k) * ld + ii) - A0[k]);
+        Bf[v][k] = (float)(__ldg(b + (3 * v + k) * ld + ii) - A0[k]);
+      }
+  }
   float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
   if (x0) {
     const float4 x = reinterpret_cast<const float4 *>(x0)[ii];
@@ -920,39 +929,55 @@ __global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double 
     de = seg_seg_dist32(HA, TA, HB, TB);
   }
   const bool edge = dpt > de;
+  // FP64 stage: only the chosen feature's vertices are loaded (again), then the six
+  // vertices stream through the certificate one at a time
+  auto vtx64 = [&](const double *T, int v, xf64 out[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = xf64(ld_again(T + (3 * v + k) * ld + ii));
+  };
   xf64 pq[6];
   if (edge) {
     xf64 HA[3], TA[3], HB[3], TB[3], sc, tc;
-    pick_vertex(A, ea, HA);
-    pick_vertex(A, (ea + 1) % 3, TA);
-    pick_vertex(B, eb, HB);
-    pick_vertex(B, (eb + 1) % 3, TB);
+    vtx64(a, ea, HA);
+    vtx64(a, (ea + 1) % 3, TA);
+    vtx64(b, eb, HB);
+    vtx64(b, (eb + 1) % 3, TB);
     seg_seg_ref(HA, TA, HB, TB, sc, tc);
+#pragma unroll
     for (int k = 0; k < 3; ++k) {  // bf.cpp:715-879 (seg_seg_points)
       pq[k] = TA[k] + ((HA[k] - TA[k]) * sc);
       pq[3 + k] = TB[k] + ((HB[k] - TB[k]) * tc);
     }
   } else {
-    xf64 T[3][3], X[3], sf, tf;
-    for (int v = 0; v < 3; ++v)
-      for (int k = 0; k < 3; ++k) T[v][k] = faceB ? B[v][k] : A[v][k];
-    if (faceB) pick_vertex(A, vtx, X);
-    else pick_vertex(B, vtx, X);
-    pt_tri_ref(T[0], T[1], T[2], X, sf, tf);
+    // face of A with B's vertex vtx, or face of B with A's vertex vtx
+    const double *face = faceB ? b : a, *pnt = faceB ? a : b;
+    xf64 T0[3], T1[3], T2[3], X[3], sf, tf;
+    vtx64(face, 0, T0);
+    vtx64(face, 1, T1);
+    vtx64(face, 2, T2);
+    vtx64(pnt, vtx, X);
+    pt_tri_ref(T0, T1, T2, X, sf, tf);
+#pragma unroll
     for (int k = 0; k < 3; ++k) {  // bf.cpp:1104-1177 (pt_tri_points)
-      const xf64 face = T[0][k] + ((T[2][k] - T[0][k]) * tf) + ((T[1][k] - T[0][k]) * sf);
-      pq[k] = faceB ? X[k] : face;
-      pq[3 + k] = faceB ? face : X[k];
+      const xf64 fp = T0[k] + ((T2[k] - T0[k]) * tf) + ((T1[k] - T0[k]) * sf);
+      pq[k] = faceB ? X[k] : fp;
+      pq[3 + k] = faceB ? fp : X[k];
     }
   }
   const double d = pq_distance(pq).v;
   bool ok = false;
   if (d > 0) {
     const double r[3] = {pq[0].v - pq[3].v, pq[1].v - pq[4].v, pq[2].v - pq[5].v};
-    double amin = 1e300, bmax = -1e300;
+    double amin = 1e300, bmax = -1e300, scale = 0.0;
+#pragma unroll
     for (int v = 0; v < 3; ++v) {
-      amin = fmin(amin, A[v][0].v * r[0] + A[v][1].v * r[1] + A[v][2].v * r[2]);
-      bmax = fmax(bmax, B[v][0].v * r[0] + B[v][1].v * r[1] + B[v][2].v * r[2]);
+      xf64 VA[3], VB[3];
+      vtx64(a, v, VA);
+      vtx64(b, v, VB);
+      amin = fmin(amin, VA[0].v * r[0] + VA[1].v * r[1] + VA[2].v * r[2]);
+      bmax = fmax(bmax, VB[0].v * r[0] + VB[1].v * r[1] + VB[2].v * r[2]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) scale = fmax(scale, fmax(fabs(VA[k].v), fabs(VB[k].v)));
     }
     const double d2r = d * d;
     ok = d2r - (amin - bmax) + 1e-14 * scale * d <= rel_tol * d2r;
