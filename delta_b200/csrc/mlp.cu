@@ -815,7 +815,7 @@ __device__ __forceinline__ void pick_vertex(const R T[3][3], int j, R out[3]) {
 // that reach the append together) and their
 // outputs left for the exact solver; flags then read 1 (certified) or 2 (listed).
 template <int CAND>
-__global__ void __launch_bounds__(128) k_learned_refine(int64_t n, const double *__restrict__ a,
+__global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const double *__restrict__ a,
                                                         const double *__restrict__ b, int64_t ld,
                                                         const float *__restrict__ x0, int sweeps, double rel_tol,
                                                         double *__restrict__ p, double *__restrict__ q,
