@@ -26,10 +26,11 @@ inline PairLaunch default_pair_launch(int method) {
   }
   return c;
 }
-// DELTA_BF_CERT over pairs idx[0 .. *count) (count read on the device, at most max_count).
+// DELTA_BF_CERT over pairs idx[0 .. *count) (count read on the device, at most max_count);
+// with `stage`, the coordinates of entry j come from stage's 18 planes of max_count.
 cudaError_t launch_cert_indexed(cudaStream_t s, const uint32_t *count, int64_t max_count, const uint32_t *idx,
                                 const double *a, const double *b, int64_t ld, double *p, double *q, double *dist,
-                                PairLaunch cfg);
+                                PairLaunch cfg, const double *stage = nullptr);
 cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
                              int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags,
                              PairLaunch cfg);

@@ -812,7 +812,8 @@ __device__ __forceinline__ void pick_vertex(const R T[3][3], int j, R out[3]) {
 // within rel_tol of the true one; slack = 1e-14 max|coordinate| covers the rounding of the
 // dot products.  Intersecting triangles have no separating plane and are never certified.
 // With `list`, uncertified pairs are appended to list[*count] (aggregated over the lanes
-// that reach the append together) and their
+// that reach the append together; with `stage`, their 18 coordinates too, as planes of n
+// at the list position) and their
 // outputs left for the exact solver; flags then read 1 (certified) or 2 (listed).
 template <int CAND>
 __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const double *__restrict__ a,
@@ -820,7 +821,8 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
                                                         const float *__restrict__ x0, int sweeps, double rel_tol,
                                                         double *__restrict__ p, double *__restrict__ q,
                                                         double *__restrict__ dist, uint8_t *__restrict__ flags,
-                                                        uint32_t *__restrict__ list, uint32_t *__restrict__ count) {
+                                                        uint32_t *__restrict__ list, uint32_t *__restrict__ count,
+                                                        double *__restrict__ stage) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n;
   const int64_t ii = valid ? i : n - 1;
@@ -991,7 +993,16 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
     unsigned base = 0;
     if (lane == leader) base = atomicAdd(count, (unsigned)__popc(grp));
     base = __shfl_sync(grp, base, leader);
-    list[base + __popc(grp & ((1u << lane) - 1u))] = (uint32_t)i;
+    const uint32_t slot = base + __popc(grp & ((1u << lane) - 1u));
+    list[slot] = (uint32_t)i;
+    if (stage) {
+      // the pair's coordinates, compact at its list position, for the exact solver
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        stage[c * (int64_t)n + slot] = ld_again(a + c * ld + i);
+        stage[(9 + c) * (int64_t)n + slot] = ld_again(b + c * ld + i);
+      }
+    }
   }
   if (ok || !list) {
     for (int k = 0; k < 3; ++k) {
@@ -1076,12 +1087,12 @@ delta_status learned_enqueue(delta_ctx *ctx, int64_t n, const double *a, const d
 
 void launch_refine(int features, cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld,
                    const float *x0, int sweeps, double rel_tol, double *p, double *q, double *dist, uint8_t *flags,
-                   uint32_t *list, uint32_t *count) {
+                   uint32_t *list, uint32_t *count, double *stage = nullptr) {
   const unsigned g = nblk(n, 128);
-  if (features == 11) k_learned_refine<11><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
-  else if (features == 15) k_learned_refine<15><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
-  else if (features == 7) k_learned_refine<7><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
-  else k_learned_refine<3><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+  if (features == 11) k_learned_refine<11><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count, stage);
+  else if (features == 15) k_learned_refine<15><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count, stage);
+  else if (features == 7) k_learned_refine<7><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count, stage);
+  else k_learned_refine<3><<<g, 128, 0, s>>>(n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count, stage);
 }
 
 delta_status learned_enqueue(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
@@ -1104,14 +1115,18 @@ delta_status learned_enqueue(delta_ctx *ctx, int64_t n, const double *a, const d
   if ((st = ctx_scratch(ctx, 14, 256 + sizeof(uint32_t) * (size_t)n, &lbuf)) != DELTA_OK) return st;
   uint32_t *count = static_cast<uint32_t *>(lbuf);
   uint32_t *list = reinterpret_cast<uint32_t *>(static_cast<char *>(lbuf) + 256);
+  // compact copies of the uncertified pairs (18 planes of n doubles) for the exact solver
+  void *sbuf;
+  if ((st = ctx_scratch(ctx, 25, sizeof(double) * 18 * (size_t)n, &sbuf)) != DELTA_OK) return st;
+  double *stage = static_cast<double *>(sbuf);
   cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), ctx->stream);
   if (e != cudaSuccess) return cuda_error(e, "learned pipeline: memset");
-  launch_refine(features, ctx->stream, n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count);
+  launch_refine(features, ctx->stream, n, a, b, ld, x0, sweeps, rel_tol, p, q, dist, flags, list, count, stage);
   ctx->launches += 1;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "learned pipeline: refine");
   const PairLaunch cfg = ctx->pair_launch_set[DELTA_BF_CERT][0] ? ctx->pair_launch[DELTA_BF_CERT][0]
                                                                 : default_pair_launch(DELTA_BF_CERT);
-  e = launch_cert_indexed(ctx->stream, count, n, list, a, b, ld, p, q, dist, cfg);
+  e = launch_cert_indexed(ctx->stream, count, n, list, a, b, ld, p, q, dist, cfg, stage);
   ctx->launches += 1;
   if (e != cudaSuccess) return cuda_error(e, "learned pipeline: exact fallback");
   *count_out = count;

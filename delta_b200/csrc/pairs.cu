@@ -95,12 +95,15 @@ __global__ void __launch_bounds__(32 * W) k_pairs_cert(int64_t n, const double *
 
 // The certified kernel over an index list: pairs idx[0 .. *count) of the pair list (the
 // count is read on the device, so the list can be built by an earlier kernel on the
-// stream without a host round trip).
+// stream without a host round trip).  With `stage`, entry j's coordinates are read from
+// stage (18 planes of sld doubles: a's 9 planes, then b's) at position j instead of being
+// gathered from a and b; results go to pair idx[j] of p, q, dist.
 template <int W>
 __global__ void __launch_bounds__(32 * W) k_pairs_cert_indexed(const uint32_t *__restrict__ count,
                                                                const uint32_t *__restrict__ idx,
                                                                const double *__restrict__ a,
                                                                const double *__restrict__ b, int64_t ld,
+                                                               const double *__restrict__ stage, int64_t sld,
                                                                double *__restrict__ p, double *__restrict__ q,
                                                                double *__restrict__ dist) {
   __shared__ CertWarpSmem sm[W];
@@ -109,14 +112,15 @@ __global__ void __launch_bounds__(32 * W) k_pairs_cert_indexed(const uint32_t *_
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += nwarps * 32) {
     const bool valid = base + lane < n;
-    const int64_t i = idx[valid ? base + lane : n - 1];
+    const int64_t j = valid ? base + lane : n - 1;
+    const int64_t i = idx[j];
     double A[3][3], B[3][3];
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        A[v][k] = __ldg(a + (3 * v + k) * ld + i);
-        B[v][k] = __ldg(b + (3 * v + k) * ld + i);
+        A[v][k] = stage ? __ldg(stage + (3 * v + k) * sld + j) : __ldg(a + (3 * v + k) * ld + i);
+        B[v][k] = stage ? __ldg(stage + (9 + 3 * v + k) * sld + j) : __ldg(b + (3 * v + k) * ld + i);
       }
     double out[6];
     bf_cert_warp(A, B, valid, out, sm[warp]);
@@ -186,7 +190,7 @@ cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t 
 
 cudaError_t launch_cert_indexed(cudaStream_t s, const uint32_t *count, int64_t max_count, const uint32_t *idx,
                                 const double *a, const double *b, int64_t ld, double *p, double *q, double *dist,
-                                PairLaunch cfg) {
+                                PairLaunch cfg, const double *stage) {
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_cert_indexed<4>, 128, 0);
   if (e != cudaSuccess) return e;
@@ -194,7 +198,8 @@ cudaError_t launch_cert_indexed(cudaStream_t s, const uint32_t *count, int64_t m
   const int64_t per = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 8;
   const int64_t cap = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1) * per;
   if (blocks > cap) blocks = cap;
-  k_pairs_cert_indexed<4><<<(unsigned)(blocks > 0 ? blocks : 1), 128, 0, s>>>(count, idx, a, b, ld, p, q, dist);
+  k_pairs_cert_indexed<4><<<(unsigned)(blocks > 0 ? blocks : 1), 128, 0, s>>>(count, idx, a, b, ld, stage, max_count,
+                                                                              p, q, dist);
   return cudaGetLastError();
 }
 
