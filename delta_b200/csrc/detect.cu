@@ -772,7 +772,7 @@ size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap) {
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
-                              void *temp, size_t temp_bytes, double *bbox) {
+                              void *temp, size_t temp_bytes, const double *bbox) {
   cudaError_t e;
   const int64_t cap = out.capacity;
   char *p = (char *)state;
@@ -797,12 +797,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   rc.sv = (uint64_t *)p;
   rc.sv_cap = fixed_sv_cap(cap);
   rc.sv_count = queue + 2;
-  rc.bbox = bbox;
-  if (bbox && driver == DELTA_DRV_BF_CERT) {
-    const int64_t warps = std::min<int64_t>(m.n_bodies, (int64_t)kNumSMs * 64);
-    k_body_boxes<<<(unsigned)std::max<int64_t>(1, (warps * 32 + 127) / 128), 128, 0, s>>>(m, bbox);
-    ctx->launches += 1;
-  }
+  rc.bbox = driver == DELTA_DRV_BF_CERT ? bbox : nullptr;  // the caller's boxes of the current vertices
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
   if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");
   k_rows_fixed<<<(unsigned)((pair_cap + 256) / 256), 256, 0, s>>>(m.tri_offset, pa, pair_cap, rows);
@@ -823,8 +818,12 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   }
   if (e != cudaSuccess) return cuda_error(e, "detect kernel");
   k_iota<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(perm_in, cap);
+  // keys (pair << 32 | A tri << 16 | B tri) of pairs below pair_cap: the bits above the pair
+  // index are zero (empty entries, ~0, still sort last: stable, and after every valid key)
+  int end_bit = 33;
+  while (end_bit < 64 && ((int64_t)1 << (end_bit - 32)) < pair_cap) ++end_bit;
   tb = temp_bytes;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, rc.key, key_out, perm_in, perm_out, cap, 0, 64, s)) !=
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, rc.key, key_out, perm_in, perm_out, cap, 0, end_bit, s)) !=
       cudaSuccess)
     return cuda_error(e, "contact sort");
   k_gather_fixed<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, perm_out, out, d_ncontacts, d_ovf, ovf_code,

@@ -228,10 +228,11 @@ __global__ void k_segment_heads(ContactView cv, int64_t n, uint8_t *head) {
   head[c] = (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]) ? 1 : 0;
 }
 
-// One thread per partner pair: both sides' sums, keyed (body << 32 | partner).
+// One thread per partner pair: both sides' sums, keyed (body << sh | partner), sh the bits
+// of a body index.
 __global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_start, const int64_t *n_seg_p,
-                              int64_t n_contacts_h, const int64_t *n_contacts_d, delta_step_params p, uint64_t *key,
-                              int64_t *val_idx, double *entry) {
+                              int64_t n_contacts_h, const int64_t *n_contacts_d, delta_step_params p, int sh,
+                              uint64_t *key, int64_t *val_idx, double *entry) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n_seg = *n_seg_p;
   int64_t n_contacts = n_contacts_d ? *n_contacts_d : n_contacts_h;
@@ -250,19 +251,19 @@ __global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_
     entry[(2 * g + 1) * 6 + k] = F[k].v;
     entry[(2 * g + 1) * 6 + 3 + k] = T[k].v;
   }
-  key[2 * g] = ((uint64_t)(uint32_t)i << 32) | (uint32_t)j;
-  key[2 * g + 1] = ((uint64_t)(uint32_t)j << 32) | (uint32_t)i;
+  key[2 * g] = ((uint64_t)(uint32_t)i << sh) | (uint32_t)j;
+  key[2 * g + 1] = ((uint64_t)(uint32_t)j << sh) | (uint32_t)i;
   val_idx[2 * g] = 2 * g;
   val_idx[2 * g + 1] = 2 * g + 1;
 }
 
 // One thread per body: partners in ascending order (entries sorted by key).
 // Entries past the valid ones carry the key ~0 and sort last; they match no body.
-__global__ void k_body_forces(int32_t n_bodies, const uint64_t *skey, const int64_t *sidx, const double *entry,
-                              int64_t ne, double *force, double *torque, uint8_t *has) {
+__global__ void k_body_forces(int32_t n_bodies, int sh, const uint64_t *skey, const int64_t *sidx,
+                              const double *entry, int64_t ne, double *force, double *torque, uint8_t *has) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_bodies) return;
-  const uint64_t lo_key = (uint64_t)(uint32_t)i << 32;
+  const uint64_t lo_key = (uint64_t)(uint32_t)i << sh;
   int64_t lo = 0, hi = ne;
   while (lo < hi) {
     const int64_t mid = (lo + hi) >> 1;
@@ -271,7 +272,7 @@ __global__ void k_body_forces(int32_t n_bodies, const uint64_t *skey, const int6
   }
   X F[3] = {X(0.0), X(0.0), X(0.0)}, T[3] = {X(0.0), X(0.0), X(0.0)};
   int64_t e = lo;
-  for (; e < ne && (skey[e] >> 32) == (uint64_t)(uint32_t)i; ++e) {
+  for (; e < ne && (skey[e] >> sh) == (uint64_t)(uint32_t)i; ++e) {
     const double *v = entry + sidx[e] * 6;
     for (int k = 0; k < 3; ++k) {
       F[k] += X(v[k]);
@@ -312,26 +313,97 @@ __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force
   update_rotation(s, b, dt);
 }
 
-// updateVertices, dynamics.cpp:215-242, one thread per vertex.
-__global__ void k_vertices(delta_scene s, int64_t n_vertices, const int *ovf) {
-  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n_vertices) return;
-  if (ovf && *ovf) return;
-  const int32_t i = s.tri_body[v / 3];
-  if (s.obstacle[i]) return;
+// updateVertices, dynamics.cpp:215-242, one warp per body: the body's 15 scalars (R, pos,
+// ref_pos) are loaded by lanes 0..14 and broadcast, the lanes then stride over the body's
+// vertices.  With `bbox` given the kernel also writes the box (lo[3], hi[3]) of every body's
+// current vertices, obstacles included, for the certified driver's row prefilter.  With the
+// overflow flag set no vertex moves (graph mode: the state is frozen) but the boxes are
+// still written, so they always describe the vertices in memory.
+__global__ void k_vertices(delta_scene s, const int *ovf, double *bbox) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const bool frozen = ovf && *ovf;
   const int32_t n = s.n_bodies;
-  X R[9], pos[3], rp[3];
+  for (int64_t i = warp; i < n; i += nwarps) {
+    const bool move = !frozen && !s.obstacle[i];
+    if (!move && !bbox) continue;
+    double q = 0.0;
+    if (move && lane < 15)
+      q = lane < 9 ? s.rot[(int64_t)lane * n + i]
+                   : (lane < 12 ? s.pos[(int64_t)(lane - 9) * n + i] : s.ref_pos[(int64_t)(lane - 12) * n + i]);
+    X R[9], pos[3], rp[3];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) R[k] = X(s.rot[(int64_t)k * n + i]);
+    for (int k = 0; k < 9; ++k) R[k] = X(__shfl_sync(0xffffffffu, q, k));
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    pos[k] = X(s.pos[(int64_t)k * n + i]);
-    rp[k] = X(s.ref_pos[(int64_t)k * n + i]);
+    for (int k = 0; k < 3; ++k) {
+      pos[k] = X(__shfl_sync(0xffffffffu, q, 9 + k));
+      rp[k] = X(__shfl_sync(0xffffffffu, q, 12 + k));
+    }
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int64_t v1 = 3 * s.tri_offset[i + 1];
+    // kU vertices per lane per pass, their loads issued together
+    constexpr int kU = 4;
+    for (int64_t base = 3 * s.tri_offset[i] + lane; base < v1; base += 32 * kU) {
+      double c[kU][3];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int64_t v = base + 32 * u;
+        if (v < v1) {
+          c[u][0] = move ? s.rx[v] : s.x[v];
+          c[u][1] = move ? s.ry[v] : s.y[v];
+          c[u][2] = move ? s.rz[v] : s.z[v];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int64_t v = base + 32 * u;
+        if (v < v1) {
+          if (move) {
+            const X C0 = X(c[u][0]) - rp[0], C1 = X(c[u][1]) - rp[1], C2 = X(c[u][2]) - rp[2];
+            c[u][0] = (pos[0] + (R[0] * C0 + R[3] * C1 + R[6] * C2)).v;
+            c[u][1] = (pos[1] + (R[1] * C0 + R[4] * C1 + R[7] * C2)).v;
+            c[u][2] = (pos[2] + (R[2] * C0 + R[5] * C1 + R[8] * C2)).v;
+            s.x[v] = c[u][0];
+            s.y[v] = c[u][1];
+            s.z[v] = c[u][2];
+          }
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            lo[k] = fmin(lo[k], c[u][k]);
+            hi[k] = fmax(hi[k], c[u][k]);
+          }
+        }
+      }
+    }
+    if (bbox) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+          lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+          hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+      }
+      if (lane == 0)
+        for (int k = 0; k < 3; ++k) {
+          bbox[6 * i + k] = lo[k];
+          bbox[6 * i + 3 + k] = hi[k];
+        }
+    }
   }
-  const X C0 = X(s.rx[v]) - rp[0], C1 = X(s.ry[v]) - rp[1], C2 = X(s.rz[v]) - rp[2];
-  s.x[v] = (pos[0] + (R[0] * C0 + R[3] * C1 + R[6] * C2)).v;
-  s.y[v] = (pos[1] + (R[1] * C0 + R[4] * C1 + R[7] * C2)).v;
-  s.z[v] = (pos[2] + (R[2] * C0 + R[5] * C1 + R[8] * C2)).v;
+}
+
+// bits of a value below 2^b with 2^b > v (at most 31): pair and force keys pack two body
+// indices in 2*bits_for(n_bodies) bits so that their radix sorts take fewer passes
+inline int bits_for(int64_t v) {
+  int b = 1;
+  while (b < 31 && ((int64_t)1 << b) <= v) ++b;
+  return b;
+}
+
+inline unsigned vertex_blocks(int32_t n_bodies) {
+  const int64_t b = ((int64_t)n_bodies + 7) / 8;  // 8 warps per 256-thread block
+  return (unsigned)(b < 1 ? 1 : (b > 8 * kNumSMs ? 8 * kNumSMs : b));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -377,37 +449,45 @@ __device__ __forceinline__ bool spheres_touch(const delta_scene &s, int32_t i, i
   return d2 <= reach * reach;
 }
 
-__device__ __forceinline__ void push_pair(int32_t a, int32_t b, uint64_t *out, unsigned long long *count, int64_t cap) {
+// pair key (min << sh | max), sh the bits of a body index, so pairs sort in 2*sh bits
+__device__ __forceinline__ void push_pair(int32_t a, int32_t b, int sh, uint64_t *out, unsigned long long *count,
+                                          int64_t cap) {
   const unsigned long long pos = atomicAdd(count, 1ull);
-  if ((int64_t)pos < cap) out[pos] = ((uint64_t)(uint32_t)(a < b ? a : b) << 32) | (uint32_t)(a < b ? b : a);
+  if ((int64_t)pos < cap) out[pos] = ((uint64_t)(uint32_t)(a < b ? a : b) << sh) | (uint32_t)(a < b ? b : a);
 }
 
+// One thread per (moving body, cell column (dx, dy)): the three cells (cx+dx, cy+dy,
+// cz-1 .. cz+1) have consecutive keys, so one binary search finds the column's bodies in the
+// sorted keys.  Columns outside the key range are skipped (every key is clamped into it, so
+// the clamped column is the body's own); pairs are pushed once, for j > i.
 __global__ void k_grid_pairs(delta_scene s, Grid g, const uint64_t *skey, const int32_t *sbody, int32_t n_moving,
-                             uint64_t *out, unsigned long long *count, int64_t cap) {
-  const int32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n_moving) return;
+                             int sh, uint64_t *out, unsigned long long *count, int64_t cap) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 9 * (int64_t)n_moving) return;
+  const int32_t p = (int32_t)(t / 9), col = (int32_t)(t % 9);
+  const int64_t M = (1 << 21) - 1;
   const int32_t i = sbody[p];
   int64_t c[3];
   cell_of(s, g, i, c);
-  for (int dx = -1; dx <= 1; ++dx)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dz = -1; dz <= 1; ++dz) {
-        const uint64_t k = cell_key(c[0] + dx, c[1] + dy, c[2] + dz);
-        int32_t lo = 0, hi = n_moving;
-        while (lo < hi) {
-          const int32_t mid = (lo + hi) >> 1;
-          if (skey[mid] < k) lo = mid + 1;
-          else hi = mid;
-        }
-        for (int32_t q = lo; q < n_moving && skey[q] == k; ++q) {
-          const int32_t j = sbody[q];
-          if (j > i && spheres_touch(s, i, j)) push_pair(i, j, out, count, cap);
-        }
-      }
+  for (int k = 0; k < 3; ++k) c[k] = c[k] < 0 ? 0 : (c[k] > M ? M : c[k]);
+  const int64_t cx = c[0] + col / 3 - 1, cy = c[1] + col % 3 - 1;
+  if (cx < 0 || cx > M || cy < 0 || cy > M) return;
+  const uint64_t k0 = cell_key(cx, cy, c[2] - 1 < 0 ? 0 : c[2] - 1);
+  const uint64_t k1 = cell_key(cx, cy, c[2] + 1 > M ? M : c[2] + 1);
+  int32_t lo = 0, hi = n_moving;
+  while (lo < hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (skey[mid] < k0) lo = mid + 1;
+    else hi = mid;
+  }
+  for (int32_t q = lo; q < n_moving && skey[q] <= k1; ++q) {
+    const int32_t j = sbody[q];
+    if (j > i && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
+  }
 }
 
 // obstacle L (box lo/hi) against every moving body j
-__global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const double *box, int32_t n_obst,
+__global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const double *box, int32_t n_obst, int sh,
                                  uint64_t *out, unsigned long long *count, int64_t cap) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)n_obst * s.n_bodies) return;
@@ -422,14 +502,17 @@ __global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const doubl
     d2 += d * d;
   }
   const double reach = (s.radius[j] + s.eps[j] + s.eps[L]) * (1.0 + 1e-9) + 1e-12;
-  if (d2 <= reach * reach) push_pair(L, j, out, count, cap);
+  if (d2 <= reach * reach) push_pair(L, j, sh, out, count, cap);
 }
 
-__global__ void k_unpack_pairs(const uint64_t *k, int64_t n, int32_t *a, int32_t *b) {
+// pair keys back to (a, b); the empty key ~0 gives (-1, -1)
+__global__ void k_unpack_pairs(const uint64_t *k, int64_t n, int sh, int32_t *a, int32_t *b) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  a[t] = (int32_t)(k[t] >> 32);
-  b[t] = (int32_t)(k[t] & 0xffffffffu);
+  const uint64_t v = k[t];
+  const bool empty = v == ~0ull;
+  a[t] = empty ? -1 : (int32_t)(v >> sh);
+  b[t] = empty ? -1 : (int32_t)(v & ((1ull << sh) - 1));
 }
 
 __global__ void k_iota32(int32_t *v, int32_t n) {
@@ -487,17 +570,18 @@ delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contac
   ctx->launches += 1;
   // entries for all potential segments (n_contacts bounds the count; unused keys sort last)
   if ((e = cudaMemsetAsync(key, 0xff, sizeof(uint64_t) * 2 * nc, st)) != cudaSuccess) return cuda_error(e, "memset");
-  k_pair_forces<<<blocks_for(n_contacts, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, n_contacts, nullptr, p, key, idx,
+  const int sh = bits_for(n);
+  k_pair_forces<<<blocks_for(n_contacts, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, n_contacts, nullptr, p, sh, key, idx,
                                                             entry);
   ctx->launches += 1;
   tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 64, st);
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 2 * sh, st);
   if ((ds = ctx_scratch(ctx, 8, tb, &temp)) != DELTA_OK) return ds;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 64, st)) !=
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 2 * sh, st)) !=
       cudaSuccess)
     return cuda_error(e, "entry sort");
   ctx->launches += 1;
-  k_body_forces<<<blocks_for(n), 256, 0, st>>>(n, skey, sidx, entry, (int64_t)(2 * nc), force, torque, has);
+  k_body_forces<<<blocks_for(n), 256, 0, st>>>(n, sh, skey, sidx, entry, (int64_t)(2 * nc), force, torque, has);
   ctx->launches += 1;
   return DELTA_OK;
 }
@@ -506,7 +590,8 @@ delta_status integrate_run(delta_ctx *ctx, const delta_scene &s, const delta_ste
                            const double *torque, const uint8_t *has, int64_t n_vertices) {
   cudaStream_t st = ctx->stream;
   k_bodies<<<blocks_for(s.n_bodies, 128), 128, 0, st>>>(s, p, force, torque, has, nullptr);
-  k_vertices<<<blocks_for(n_vertices), 256, 0, st>>>(s, n_vertices, nullptr);
+  (void)n_vertices;
+  k_vertices<<<vertex_blocks(s.n_bodies), 256, 0, st>>>(s, nullptr, nullptr);
   ctx->launches += 2;
   return cuda_error(cudaGetLastError(), "integrate launch");
 }
@@ -595,6 +680,7 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   cudaError_t e;
   delta_status ds;
   const int32_t n = s.n_bodies;
+  const int sh = bits_for(n);
   void *kb = nullptr;
   if ((ds = ctx_scratch(ctx, 10, (sizeof(uint64_t) * 2 + sizeof(int32_t) * 2) * (size_t)n + 64, &kb)) != DELTA_OK)
     return ds;
@@ -619,13 +705,13 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
     pk = (uint64_t *)pb + 8;
     if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess) return cuda_error(e, "memset");
     if (plan.n_moving > 0) {
-      k_grid_pairs<<<blocks_for(plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, pk, count,
+      k_grid_pairs<<<blocks_for(9 * (int64_t)plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, sh, pk, count,
                                                                    cap);
       ctx->launches += 1;
     }
     if (plan.n_obst > 0) {
       k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
-                                                                            pk, count, cap);
+                                                                            sh, pk, count, cap);
       ctx->launches += 1;
     }
     if ((e = cudaMemcpyAsync(&hcount, count, sizeof(hcount), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -639,14 +725,14 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   if (np == 0) return DELTA_OK;
   uint64_t *spk = pk + cap;
   tb = 0;
-  cub::DeviceRadixSort::SortKeys(nullptr, tb, pk, spk, np, 0, 64, st);
+  cub::DeviceRadixSort::SortKeys(nullptr, tb, pk, spk, np, 0, 2 * sh, st);
   if ((ds = ctx_scratch(ctx, 12, tb, &temp)) != DELTA_OK) return ds;
-  if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, np, 0, 64, st)) != cudaSuccess)
+  if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, np, 0, 2 * sh, st)) != cudaSuccess)
     return cuda_error(e, "pair sort");
   ctx->launches += 1;
   const int64_t wn = np < capacity ? np : capacity;
   if (wn > 0) {
-    k_unpack_pairs<<<blocks_for(wn), 256, 0, st>>>(spk, wn, pair_a, pair_b);
+    k_unpack_pairs<<<blocks_for(wn), 256, 0, st>>>(spk, wn, sh, pair_a, pair_b);
     ctx->launches += 1;
   }
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "broadphase");
@@ -654,12 +740,6 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   return DELTA_OK;
 }
 
-
-static int bits_for(int64_t v) {
-  int b = 1;
-  while (b < 31 && ((int64_t)1 << b) <= v) ++b;
-  return b;
-}
 
 // Forces from a fixed-capacity contact buffer with its count on the device.
 size_t forces_fixed_state_bytes(int64_t cap) { return (size_t)cap * (1 + 8 + 16 * 4 + 96) + 512; }
@@ -669,7 +749,7 @@ size_t forces_fixed_temp_bytes(int64_t cap, int32_t n_bodies) {
   cub::CountingInputIterator<int64_t> it(0);
   cub::DeviceSelect::Flagged(nullptr, a, it, (uint8_t *)nullptr, (int64_t *)nullptr, (int64_t *)nullptr, cap);
   cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, (int64_t *)nullptr,
-                                  (int64_t *)nullptr, 2 * cap, 0, 32 + bits_for(n_bodies));
+                                  (int64_t *)nullptr, 2 * cap, 0, 2 * bits_for(n_bodies));
   return a > b ? a : b;
 }
 
@@ -694,12 +774,14 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   if ((e = cub::DeviceSelect::Flagged(temp, tb, it, head, seg_start, n_seg, cap, st)) != cudaSuccess)
     return cuda_error(e, "segment select");
   if ((e = cudaMemsetAsync(key, 0xff, sizeof(uint64_t) * 2 * cap, st)) != cudaSuccess) return cuda_error(e, "memset");
-  k_pair_forces<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, 0, d_nc, p, key, idx, entry);
+  const int sh = bits_for(s.n_bodies);
+  k_pair_forces<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, 0, d_nc, p, sh, key, idx, entry);
   tb = temp_bytes;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, 2 * cap, 0, 32 + bits_for(s.n_bodies),
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, 2 * cap, 0, 2 * sh,
                                            st)) != cudaSuccess)
     return cuda_error(e, "entry sort");
-  k_body_forces<<<blocks_for(s.n_bodies), 256, 0, st>>>(s.n_bodies, skey, sidx, entry, 2 * cap, force, torque, has);
+  k_body_forces<<<blocks_for(s.n_bodies), 256, 0, st>>>(s.n_bodies, sh, skey, sidx, entry, 2 * cap, force, torque,
+                                                        has);
   kernels += 5;
   return cuda_error(cudaGetLastError(), "forces fixed");
 }
@@ -714,7 +796,7 @@ size_t broadphase_fixed_temp_bytes(int32_t n, int64_t pair_cap) {
   cub::DeviceRadixSort::SortPairs(nullptr, a, (uint64_t *)nullptr, (uint64_t *)nullptr, (int32_t *)nullptr,
                                   (int32_t *)nullptr, n, 0, 64);
   cub::DeviceRadixSort::SortKeys(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, pair_cap, 0,
-                                 32 + bits_for(n));
+                                 2 * bits_for(n));
   return a > b ? a : b;
 }
 
@@ -723,6 +805,7 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
                                   size_t temp_bytes, int &kernels) {
   cudaError_t e;
   const int32_t n = s.n_bodies;
+  const int sh = bits_for(n);
   char *b = (char *)state;
   uint64_t *key = (uint64_t *)b, *skey = key + n;
   int32_t *body = (int32_t *)(skey + n), *sbody = body + n;
@@ -739,19 +822,19 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
     return cuda_error(e, "memset");
   kernels += 2;
   if (plan.n_moving > 0) {
-    k_grid_pairs<<<blocks_for(plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, pk, count,
+    k_grid_pairs<<<blocks_for(9 * (int64_t)plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, sh, pk, count,
                                                                  pair_cap);
     kernels += 1;
   }
   if (plan.n_obst > 0) {
     k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
-                                                                          pk, count, pair_cap);
+                                                                          sh, pk, count, pair_cap);
     kernels += 1;
   }
   tb = temp_bytes;
-  if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, pair_cap, 0, 32 + bits_for(n), st)) != cudaSuccess)
+  if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, pair_cap, 0, 2 * sh, st)) != cudaSuccess)
     return cuda_error(e, "pair sort");
-  k_unpack_pairs<<<blocks_for(pair_cap), 256, 0, st>>>(spk, pair_cap, pair_a, pair_b);
+  k_unpack_pairs<<<blocks_for(pair_cap), 256, 0, st>>>(spk, pair_cap, sh, pair_a, pair_b);
   k_flag_overflow<<<1, 1, 0, st>>>(count, pair_cap, ovf);
   kernels += 3;
   return cuda_error(cudaGetLastError(), "broadphase fixed");
@@ -795,7 +878,7 @@ struct delta_sim {
     size_t temp_bytes = 0;
     delta_contacts c{};
     int64_t *d_nc = nullptr, *d_step = nullptr, *d_cnt = nullptr, *d_log = nullptr;
-    double *bbox = nullptr;  // per-body boxes for the certified driver's row prefilter
+    double *bbox = nullptr;  // body boxes (written by k_vertices) for the certified driver's row prefilter
     int *d_ovf = nullptr, *d_snap = nullptr;
     int64_t log_len = 0;
     cudaStream_t stream = nullptr;
@@ -937,7 +1020,8 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   delta_status ds = forces_run_fixed(st, s->scene, g.c, g.d_nc, p, s->F, s->T, s->has, g.fs, g.temp, g.temp_bytes, k);
   if (ds != DELTA_OK) return ds;
   k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf);
-  k_vertices<<<blocks_for(3 * s->n_tri), 256, 0, st>>>(s->scene, 3 * s->n_tri, g.d_ovf);
+  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, g.d_ovf,
+                                                               s->driver == DELTA_DRV_BF_CERT ? g.bbox : nullptr);
   if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.bp, g.temp, g.temp_bytes,
                                  k)) != DELTA_OK)
     return ds;
