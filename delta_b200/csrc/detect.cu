@@ -47,7 +47,6 @@ struct DevStats {
 
 struct RowCtx {
   int64_t k;       // pair index
-  int32_t bB;      // body B
   int32_t iA;      // triangle of A (within the body)
   int64_t tA, tB0; // global triangle indices
   int32_t nB;
@@ -167,63 +166,13 @@ __device__ __forceinline__ void for_row(int32_t nB, F &&fn) {
 }
 
 template <class R, int DRV>
-__device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawContacts &rc, DevStats *st,
-                            CertWarpSmem *csm) {
+__device__ void process_row(const delta_meshes &m, const RowCtx &r, const RawContacts &rc, DevStats *st) {
   const xf64 margin = xf64(r.epsA) + xf64(r.epsB);
   const double max_err = (margin / xf64(16.0)).v;  // (epsA+epsB)/16, hybrid.cpp:60
   const double mg = margin.v;
   double pq[6];
   int flag = 0;
-  if constexpr (DRV == DELTA_DRV_BF_CERT) {
-    // Exact culling: bf()'s distance is the length of a point pair on the two triangles,
-    // never below the gap between their bounding boxes, so a B triangle whose box is
-    // farther than epsA+epsB (with a relative margin for rounding) cannot give a
-    // contact (bf.cpp:125).  Survivors are packed into full 32-lane batches.
-    const int lane = threadIdx.x & 31;
-    double A[3][3], alo[3], ahi[3];
-    load_tri64(m, r.tA, A);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      alo[k] = fmin(A[0][k], fmin(A[1][k], A[2][k]));
-      ahi[k] = fmax(A[0][k], fmax(A[1][k], A[2][k]));
-    }
-    const double cull = mg * (1.0 + 1e-9) + 1e-12;
-    if (rc.bbox) {
-      // row prefilter: every B triangle box lies in B's body box, so when A's triangle box
-      // is farther than the cull distance from the body box no B triangle survives (the
-      // per-axis gaps and their squares are monotone in the boxes, so the skip is exact)
-      const double *bb = rc.bbox + 6 * (int64_t)r.bB;
-      double g2 = 0.0;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const double g = fmax(bb[k] - ahi[k], alo[k] - bb[3 + k]);
-        if (g > 0.0) g2 += g * g;
-      }
-      if (g2 > cull * cull) return;
-    }
-    const int lane_ = lane;
-    for (int32_t base = 0; base < r.nB; base += 32) {
-      const int32_t tb = base + lane_;
-      bool keep = false;
-      if (tb < r.nB) {
-        double B[3][3], g2 = 0.0;
-        load_tri64(m, r.tB0 + tb, B);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const double blo = fmin(B[0][k], fmin(B[1][k], B[2][k])), bhi = fmax(B[0][k], fmax(B[1][k], B[2][k]));
-          const double g = fmax(blo - ahi[k], alo[k] - bhi);
-          if (g > 0.0) g2 += g * g;
-        }
-        keep = g2 <= cull * cull;
-      }
-      if (keep) {
-        const int64_t pos = agg_slot(rc.sv_count);
-        if (pos < rc.sv_cap) rc.sv[pos] = ((uint64_t)r.k << 32) | ((uint64_t)r.iA << 16) | (uint64_t)tb;
-      }
-    }
-    (void)csm;
-    (void)pq;
-  } else if constexpr (DRV == DELTA_DRV_BF || DRV == DELTA_DRV_GJK) {
+  if constexpr (DRV == DELTA_DRV_BF || DRV == DELTA_DRV_GJK) {
     constexpr int S = DRV == DELTA_DRV_BF ? S_BF : S_GJK;
     for_row(r.nB, [&](int32_t tb, bool valid) {
       bool take = false;
@@ -353,18 +302,10 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
                                                 unsigned long long *queue) {
   const int lane = threadIdx.x & 31;
   const int64_t total_rows = *total_rows_p;
-  __shared__ CertWarpSmem cert_sm[DRV == DELTA_DRV_BF_CERT ? 4 : 1];
-  CertWarpSmem *csm = &cert_sm[DRV == DELTA_DRV_BF_CERT ? (threadIdx.x >> 5) : 0];
-  // rows are taken from the queue in batches (the certified driver's prefilter makes most
-  // rows cheap, so one atomic per row would make the queue the bottleneck)
-  constexpr unsigned long long kBatch = DRV == DELTA_DRV_BF_CERT ? 8 : 1;
-  unsigned long long row = 0, batch_end = 0;
   for (;;) {
-    if (row >= batch_end) {
-      if (lane == 0) row = atomicAdd(queue, kBatch);
-      row = __shfl_sync(kFull, row, 0);
-      batch_end = row + kBatch;
-    }
+    unsigned long long row = 0;
+    if (lane == 0) row = atomicAdd(queue, 1ull);
+    row = __shfl_sync(kFull, row, 0);
     if ((int64_t)row >= total_rows) return;
     // pair k: last k with row_offset[k] <= row
     int64_t lo = 0, hi = n_pairs;
@@ -376,7 +317,6 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
     RowCtx r;
     r.k = lo;
     const int32_t a = pa[lo], b = pb[lo];
-    r.bB = b;
     r.iA = (int32_t)((int64_t)row - row_offset[lo]);
     r.tA = m.tri_offset[a] + r.iA;
     r.tB0 = m.tri_offset[b];
@@ -388,11 +328,144 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
     r.fric = (m.friction[a] && m.friction[b]) ? 1 : 0;
     if (lane == 0) {
       atomicAdd(&st->tri_pairs, (unsigned long long)r.nB);
-      if (DRV != DELTA_DRV_BF_CERT) atomicAdd(&st->evaluated, (unsigned long long)r.nB);
+      atomicAdd(&st->evaluated, (unsigned long long)r.nB);
     }
-    process_row<R, DRV>(m, r, rc, st, csm);
-    ++row;
+    process_row<R, DRV>(m, r, rc, st);
   }
+}
+
+// ---- certified driver, phase 1: exact box culling, one warp per particle pair ----------
+// bf()'s distance is the length of a point pair on the two triangles, never below the gap
+// between their bounding boxes, so a triangle pair whose boxes are farther apart than
+// epsA+epsB (with a relative margin for rounding) cannot give a contact (bf.cpp:125).  A
+// warp stages in shared memory the A triangles whose box is within the cull distance of
+// B's body box and the B triangles within it of A's body box (at most kCullList each;
+// longer lists are taken in windows) and then tests the staged boxes pair by pair.  The
+// survivors are exactly the triangle pairs whose boxes pass the test: every triangle box
+// lies in its body box and the per-axis gaps, their squares and their sum are monotone in
+// the boxes, so a triangle dropped against a body box fails against every triangle of
+// that body too.
+constexpr int kCullList = 64;
+struct CullList {
+  double lo[3][kCullList], hi[3][kCullList];
+  uint16_t idx[kCullList];
+};
+
+// squared gap between the boxes (alo, ahi) and (blo, bhi): the sum of the squares of the
+// positive per-axis gaps
+__device__ __forceinline__ double box_gap2(const double alo[3], const double ahi[3], const double blo[3],
+                                           const double bhi[3]) {
+  double g2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double g = fmax(blo[k] - ahi[k], alo[k] - bhi[k]);
+    if (g > 0.0) g2 += g * g;
+  }
+  return g2;
+}
+
+// Stages the triangles cur, cur+1, ... of (t0, n) whose box lies within the cull distance
+// of the box (olo, ohi) into L, 32 at a time while L can take 32 more; returns the cursor.
+__device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, int64_t t0, int32_t n, int32_t cur,
+                                             const double olo[3], const double ohi[3], double cull2, CullList &L,
+                                             int &nL) {
+  const int lane = threadIdx.x & 31;
+  nL = 0;
+  while (cur < n && nL + 32 <= kCullList) {
+    const int32_t i = cur + lane;
+    double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {0.0, 0.0, 0.0};
+    bool keep = false;
+    if (i < n) {
+      double T[3][3];
+      load_tri64(m, t0 + i, T);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = fmin(T[0][k], fmin(T[1][k], T[2][k]));
+        hi[k] = fmax(T[0][k], fmax(T[1][k], T[2][k]));
+      }
+      keep = box_gap2(lo, hi, olo, ohi) <= cull2;
+    }
+    const unsigned bal = __ballot_sync(kFull, keep);
+    if (keep) {
+      const int s = nL + __popc(bal & ((1u << lane) - 1u));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        L.lo[k][s] = lo[k];
+        L.hi[k][s] = hi[k];
+      }
+      L.idx[s] = (uint16_t)i;
+    }
+    nL += __popc(bal);
+    cur += 32;
+  }
+  __syncwarp();
+  return cur;
+}
+
+// Pairs k = warp, warp + n_warps, ... (entries with a negative body are empty).  Survivor
+// keys (pair << 32 | A triangle << 16 | B triangle) go to rc.sv; their order is free (the
+// contacts are sorted by key afterwards).  rc.bbox holds the body boxes of the current
+// vertices (null: no body-box tests).
+__global__ void __launch_bounds__(128) k_cull_pairs(delta_meshes m, const int32_t *__restrict__ pa,
+                                                    const int32_t *__restrict__ pb, int64_t n_pairs, RawContacts rc,
+                                                    DevStats *st) {
+  __shared__ CullList lists[4][2];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  CullList &LA = lists[w][0], &LB = lists[w][1];
+  const int64_t n_warps = (int64_t)gridDim.x * 4;
+  for (int64_t k = (int64_t)blockIdx.x * 4 + w; k < n_pairs; k += n_warps) {
+    const int32_t a = pa[k], b = pb[k];
+    if (a < 0 || b < 0) continue;
+    const int64_t tA0 = m.tri_offset[a], tB0 = m.tri_offset[b];
+    const int32_t nA = (int32_t)(m.tri_offset[a + 1] - tA0), nB = (int32_t)(m.tri_offset[b + 1] - tB0);
+    if (lane == 0) atomicAdd(&st->tri_pairs, (unsigned long long)nA * (unsigned long long)nB);
+    const double mg = (xf64(m.eps[a]) + xf64(m.eps[b])).v;
+    const double cull = mg * (1.0 + 1e-9) + 1e-12, cull2 = cull * cull;
+    double Alo[3], Ahi[3], Blo[3], Bhi[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Alo[c] = rc.bbox ? rc.bbox[6 * (int64_t)a + c] : -INFINITY;
+      Ahi[c] = rc.bbox ? rc.bbox[6 * (int64_t)a + 3 + c] : INFINITY;
+      Blo[c] = rc.bbox ? rc.bbox[6 * (int64_t)b + c] : -INFINITY;
+      Bhi[c] = rc.bbox ? rc.bbox[6 * (int64_t)b + 3 + c] : INFINITY;
+    }
+    if (box_gap2(Alo, Ahi, Blo, Bhi) > cull2) continue;
+    for (int32_t cb = 0; cb < nB;) {
+      int nLB = 0;
+      cb = cull_fill(m, tB0, nB, cb, Alo, Ahi, cull2, LB, nLB);
+      if (nLB == 0) continue;
+      for (int32_t ca = 0; ca < nA;) {
+        int nLA = 0;
+        ca = cull_fill(m, tA0, nA, ca, Blo, Bhi, cull2, LA, nLA);
+        const int np = nLA * nLB;
+        for (int j = lane; j < np; j += 32) {
+          const int ia = j / nLB, ib = j - ia * nLB;
+          const double alo[3] = {LA.lo[0][ia], LA.lo[1][ia], LA.lo[2][ia]};
+          const double ahi[3] = {LA.hi[0][ia], LA.hi[1][ia], LA.hi[2][ia]};
+          const double blo[3] = {LB.lo[0][ib], LB.lo[1][ib], LB.lo[2][ib]};
+          const double bhi[3] = {LB.hi[0][ib], LB.hi[1][ib], LB.hi[2][ib]};
+          if (box_gap2(alo, ahi, blo, bhi) <= cull2) {
+            const int64_t pos = agg_slot(rc.sv_count);
+            if (pos < rc.sv_cap)
+              rc.sv[pos] = ((uint64_t)k << 32) | ((uint64_t)LA.idx[ia] << 16) | (uint64_t)LB.idx[ib];
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+}
+
+inline cudaError_t launch_cull(cudaStream_t s, const delta_meshes &m, const int32_t *pa, const int32_t *pb,
+                               int64_t n_pairs, const RawContacts &rc, DevStats *st) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cull_pairs, 128, 0);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
+  const int64_t need = (n_pairs + 3) / 4;
+  if (blocks > need) blocks = need > 0 ? need : 1;
+  k_cull_pairs<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, n_pairs, rc, st);
+  return cudaGetLastError();
 }
 
 // Certified bf over the survivors of the box test, 32 per warp (any mix of pairs).
@@ -660,9 +733,7 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
         rc.sv_cap = sv_cap;
         if ((e = cudaMemsetAsync(queue, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess)
           return cuda_error(e, "memset");
-        if ((e = launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats,
-                                                         queue)) != cudaSuccess)
-          return cuda_error(e, "cull kernel");
+        if ((e = launch_cull(s, m, pa, pb, n_pairs, rc, dstats)) != cudaSuccess) return cuda_error(e, "cull kernel");
         ctx->launches += 1;
         if ((e = cudaMemcpyAsync(&hsv, sv_count, sizeof(hsv), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
             (e = cudaStreamSynchronize(s)) != cudaSuccess)
@@ -684,11 +755,7 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
     } else {
       e = precision == DELTA_F32
             ? launch_detect_prec<float>(driver, s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats, queue)
-            : (driver == DELTA_DRV_BF_CERT
-                   ? launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, n_pairs, total_rows, rc,
-                                                             dstats, queue)
-                   : launch_detect_prec<xf64>(driver, s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats,
-                                              queue));
+            : launch_detect_prec<xf64>(driver, s, m, pa, pb, row_offset, n_pairs, total_rows, rc, dstats, queue);
       ctx->launches += 1;
     }
     if (e != cudaSuccess) return cuda_error(e, "detect kernel");
@@ -805,7 +872,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
     return cuda_error(e, "row scan");
   if (driver == DELTA_DRV_BF_CERT) {
-    e = launch_detect_t<xf64, DELTA_DRV_BF_CERT>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue);
+    e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats);
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0)) != cudaSuccess)
