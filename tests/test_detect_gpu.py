@@ -73,6 +73,46 @@ def test_bf_cert_driver_equals_bf(ctx):
             assert np.array_equal(a[f], b[f], equal_nan=True), f
 
 
+def _sheet(n, z0, tilt, shift, rng):
+    """Flat triangulated n x n quad grid (2*n*n triangles) over [0, 0.1]^2 at height z0,
+    tilted by `tilt` about x, vertices jittered slightly."""
+    g = np.linspace(0.0, 0.1, n + 1)
+    X, Y = np.meshgrid(g + shift, g + shift, indexing="ij")
+    Z = z0 + np.tan(tilt) * Y + 1e-5 * rng.random(X.shape)
+    tris = []
+    for i in range(n):
+        for j in range(n):
+            v00, v10 = (X[i, j], Y[i, j], Z[i, j]), (X[i + 1, j], Y[i + 1, j], Z[i + 1, j])
+            v01, v11 = (X[i, j + 1], Y[i, j + 1], Z[i, j + 1]), (X[i + 1, j + 1], Y[i + 1, j + 1], Z[i + 1, j + 1])
+            tris += [v00, v10, v11, v00, v11, v01]
+    return np.array(tris).T.copy()
+
+
+def test_bf_cert_driver_many_close_triangles(ctx, oracle):
+    """Two nearly parallel sheets of 288 triangles within the contact margin of each other
+    (and a sphere touching one): the certified driver's culling stages more than one
+    shared-memory window of triangles per side and must still give bf's contacts."""
+    from delta_b200.detection import DRV_BF, DRV_BF_CERT, Meshes, detect
+    from delta_b200.scenarios import sphere_mesh
+
+    rng = np.random.default_rng(7)
+    V, F = sphere_mesh(80, rng, 0.02, (0.9, 1.1))
+    sphere = (V[F].reshape(-1, 3) + np.array([0.05, 0.05, 0.0235])).T.copy()
+    bodies = [_sheet(12, 0.0, 0.0, 0.0, rng), _sheet(12, 0.0015, 0.01, 0.003, rng), sphere]
+    pa, pb = [0, 1, 2], [1, 2, 0]
+    eps_b = np.array([0.002, 0.002, 0.002])
+    fric = np.array([1, 0, 1], np.uint8)
+    ids = np.array([4, 9, 11])
+    m = Meshes.from_bodies(bodies, eps_b, fric, ids)
+    a = detect(ctx, DRV_BF, m, pa, pb)[0].to_numpy()
+    b = detect(ctx, DRV_BF_CERT, m, pa, pb)[0].to_numpy()
+    o, _, _ = _oracle_contacts(oracle, DRV_BF, bodies, pa, pb, eps_b, fric, ids)
+    assert len(a) > 500 and len(b) == len(a) == len(o)
+    for f in FIELDS:
+        assert np.array_equal(a[f], b[f], equal_nan=True), f
+        assert np.array_equal(b[f], o[f], equal_nan=True), f
+
+
 def test_golden_driver_fixture(ctx, golden):
     from delta_b200 import detection
 
