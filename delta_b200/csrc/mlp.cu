@@ -823,114 +823,154 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
                                                         double *__restrict__ dist, uint8_t *__restrict__ flags,
                                                         uint32_t *__restrict__ list, uint32_t *__restrict__ count,
                                                         double *__restrict__ stage) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < n;
-  const int64_t ii = valid ? i : n - 1;
-  // FP32 copies relative to A0 (the distance is translation invariant); the FP64 values
-  // are loaded again for the FP64 stage (from L1/L2), so they are not held in registers
-  // through the FP32 search
-  float Af[3][3], Bf[3][3];
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid0 = i0 < n;
+  bool edge0;      // the chosen feature is an edge pair
+  unsigned code0;  // edge pair: ea | eb << 2; vertex-face: vtx | faceB << 2
   {
-    double A0[3];
+    const int64_t ii = valid0 ? i0 : n - 1;
+    // FP32 copies relative to A0 (the distance is translation invariant); the FP64 values
+    // are loaded again for the FP64 stage (from L1/L2), so they are not held in registers
+    // through the FP32 search
+    float Af[3][3], Bf[3][3];
+    {
+      double A0[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) A0[k] = __ldg(a + k * ld + ii);
+      for (int k = 0; k < 3; ++k) A0[k] = __ldg(a + k * ld + ii);
 #pragma unroll
-    for (int v = 0; v < 3; ++v)
+      for (int v = 0; v < 3; ++v)
 #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          Af[v][k] = (float)(__ldg(a + (3 * v + k) * ld + ii) - A0[k]);
+          Bf[v][k] = (float)(__ldg(b + (3 * v + k) * ld + ii) - A0[k]);
+        }
+    }
+    float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
+    if (x0) {
+      const float4 x = reinterpret_cast<const float4 *>(x0)[ii];
+      // project the prediction into the parameter triangles
+      s = fmaxf(x.x, 0.f); t = fmaxf(x.y, 0.f); u = fmaxf(x.z, 0.f); w = fmaxf(x.w, 0.f);
+      const float st = s + t, uw = u + w;
+      if (st > 1.f) { s /= st; t /= st; }
+      if (uw > 1.f) { u /= uw; w /= uw; }
+    }
+    if (sweeps > 0) {
+      float EA0[3], EA1[3], EB0[3], EB1[3];
       for (int k = 0; k < 3; ++k) {
-        Af[v][k] = (float)(__ldg(a + (3 * v + k) * ld + ii) - A0[k]);
-        Bf[v][k] = (float)(__ldg(b + (3 * v + k) * ld + ii) - A0[k]);
+        EA0[k] = Af[1][k] - Af[0][k];
+        EA1[k] = Af[2][k] - Af[0][k];
+        EB0[k] = Bf[1][k] - Bf[0][k];
+        EB1[k] = Bf[2][k] - Bf[0][k];
       }
-  }
-  float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
-  if (x0) {
-    const float4 x = reinterpret_cast<const float4 *>(x0)[ii];
-    // project the prediction into the parameter triangles
-    s = fmaxf(x.x, 0.f); t = fmaxf(x.y, 0.f); u = fmaxf(x.z, 0.f); w = fmaxf(x.w, 0.f);
-    const float st = s + t, uw = u + w;
-    if (st > 1.f) { s /= st; t /= st; }
-    if (uw > 1.f) { u /= uw; w /= uw; }
-  }
-  if (sweeps > 0) {
-    float EA0[3], EA1[3], EB0[3], EB1[3];
-    for (int k = 0; k < 3; ++k) {
-      EA0[k] = Af[1][k] - Af[0][k];
-      EA1[k] = Af[2][k] - Af[0][k];
-      EB0[k] = Bf[1][k] - Bf[0][k];
-      EB1[k] = Bf[2][k] - Bf[0][k];
+      for (int it = 0; it < sweeps; ++it) {
+        float P[3];
+        for (int k = 0; k < 3; ++k) P[k] = Af[0][k] + s * EA0[k] + t * EA1[k];
+        closest_on_tri(Bf[0], EB0, EB1, P, u, w);
+        float Q[3];
+        for (int k = 0; k < 3; ++k) Q[k] = Bf[0][k] + u * EB0[k] + w * EB1[k];
+        closest_on_tri(Af[0], EA0, EA1, Q, s, t);
+      }
     }
-    for (int it = 0; it < sweeps; ++it) {
-      float P[3];
-      for (int k = 0; k < 3; ++k) P[k] = Af[0][k] + s * EA0[k] + t * EA1[k];
-      closest_on_tri(Bf[0], EB0, EB1, P, u, w);
-      float Q[3];
-      for (int k = 0; k < 3; ++k) Q[k] = Bf[0][k] + u * EB0[k] + w * EB1[k];
-      closest_on_tri(Af[0], EA0, EA1, Q, s, t);
-    }
-  }
-  // features read off the barycentric weights lA = (1-s-t, s, t), lB = (1-u-w, u, w)
-  const int iA = argmax3(1.f - s - t, s, t), jB = argmax3(1.f - u - w, u, w);
-  const int kA = argmin3(1.f - s - t, s, t), kB = argmin3(1.f - u - w, u, w);
-  // bf's vertex-face features: B's vertex jB on face A (feature 9 + jB), A's vertex iA
-  // on face B (12 + iA); edge-edge feature 3 ea + eb joins vertices ea, ea+1 (the edge
-  // opposite vertex ea+2).  Operands are selected, not indexed, so all lanes run the
-  // same code whichever features they picked.
-  int ea = (kA + 1) % 3, eb = (kB + 1) % 3;
-  float HA[3], TA[3], HB[3], TB[3];
-  bool faceB;  // chosen vertex-face feature: A's vertex vtx on face B, else B's vertex vtx on face A
-  int vtx;
-  float dpt, de;
-  if constexpr (CAND == 3) {
-    float X1[3], X2[3];
-    pick_vertex(Bf, jB, X1);
-    pick_vertex(Af, iA, X2);
-    const float d1 = pt_tri_dist32(Af[0], Af[1], Af[2], X1);
-    const float d2 = pt_tri_dist32(Bf[0], Bf[1], Bf[2], X2);
-    faceB = d2 < d1;
-    vtx = faceB ? iA : jB;
-    dpt = faceB ? d2 : d1;
-  } else {
-    // all six vertex-face features in bfSolver's order, first minimum kept
-    dpt = 1e30f;
-    faceB = false;
-    vtx = 0;
+    // features read off the barycentric weights lA = (1-s-t, s, t), lB = (1-u-w, u, w)
+    const int iA = argmax3(1.f - s - t, s, t), jB = argmax3(1.f - u - w, u, w);
+    const int kA = argmin3(1.f - s - t, s, t), kB = argmin3(1.f - u - w, u, w);
+    // bf's vertex-face features: B's vertex jB on face A (feature 9 + jB), A's vertex iA
+    // on face B (12 + iA); edge-edge feature 3 ea + eb joins vertices ea, ea+1 (the edge
+    // opposite vertex ea+2).  Operands are selected, not indexed, so all lanes run the
+    // same code whichever features they picked.
+    int ea = (kA + 1) % 3, eb = (kB + 1) % 3;
+    float HA[3], TA[3], HB[3], TB[3];
+    bool faceB;  // chosen vertex-face feature: A's vertex vtx on face B, else B's vertex vtx on face A
+    int vtx;
+    float dpt, de;
+    if constexpr (CAND == 3) {
+      float X1[3], X2[3];
+      pick_vertex(Bf, jB, X1);
+      pick_vertex(Af, iA, X2);
+      const float d1 = pt_tri_dist32(Af[0], Af[1], Af[2], X1);
+      const float d2 = pt_tri_dist32(Bf[0], Bf[1], Bf[2], X2);
+      faceB = d2 < d1;
+      vtx = faceB ? iA : jB;
+      dpt = faceB ? d2 : d1;
+    } else {
+      // all six vertex-face features in bfSolver's order, first minimum kept
+      dpt = 1e30f;
+      faceB = false;
+      vtx = 0;
 #pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      const float dj = j < 3 ? pt_tri_dist32(Af[0], Af[1], Af[2], Bf[j]) : pt_tri_dist32(Bf[0], Bf[1], Bf[2], Af[j - 3]);
-      if (dj < dpt) { dpt = dj; faceB = j >= 3; vtx = j % 3; }
+      for (int j = 0; j < 6; ++j) {
+        const float dj = j < 3 ? pt_tri_dist32(Af[0], Af[1], Af[2], Bf[j]) : pt_tri_dist32(Bf[0], Bf[1], Bf[2], Af[j - 3]);
+        if (dj < dpt) { dpt = dj; faceB = j >= 3; vtx = j % 3; }
+      }
     }
-  }
-  if constexpr (CAND == 15) {
-    // all nine edge pairs, first minimum kept
-    de = 1e30f;
+    if constexpr (CAND == 15) {
+      // all nine edge pairs, first minimum kept
+      de = 1e30f;
 #pragma unroll
-    for (int j = 0; j < 9; ++j) {
-      const float dj = seg_seg_dist32(Af[j / 3], Af[(j / 3 + 1) % 3], Bf[j % 3], Bf[(j % 3 + 1) % 3]);
-      if (dj < de) { de = dj; ea = j / 3; eb = j % 3; }
-    }
-  } else if constexpr (CAND == 11) {
-    // the edge pairs that contain A's nearest edge or B's nearest edge; the minimum in
-    // feature order (distance, then index 3 ea + eb)
-    const int ean = ea, ebn = eb;
-    de = 1e30f;
+      for (int j = 0; j < 9; ++j) {
+        const float dj = seg_seg_dist32(Af[j / 3], Af[(j / 3 + 1) % 3], Bf[j % 3], Bf[(j % 3 + 1) % 3]);
+        if (dj < de) { de = dj; ea = j / 3; eb = j % 3; }
+      }
+    } else if constexpr (CAND == 11) {
+      // the edge pairs that contain A's nearest edge or B's nearest edge; the minimum in
+      // feature order (distance, then index 3 ea + eb)
+      const int ean = ea, ebn = eb;
+      de = 1e30f;
 #pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      const int xa = j < 3 ? ean : j - 3, xb = j < 3 ? j : ebn;
-      pick_vertex(Af, xa, HA);
-      pick_vertex(Af, (xa + 1) % 3, TA);
-      pick_vertex(Bf, xb, HB);
-      pick_vertex(Bf, (xb + 1) % 3, TB);
-      const float dj = seg_seg_dist32(HA, TA, HB, TB);
-      if (dj < de || (dj == de && 3 * xa + xb < 3 * ea + eb)) { de = dj; ea = xa; eb = xb; }
+      for (int j = 0; j < 6; ++j) {
+        const int xa = j < 3 ? ean : j - 3, xb = j < 3 ? j : ebn;
+        pick_vertex(Af, xa, HA);
+        pick_vertex(Af, (xa + 1) % 3, TA);
+        pick_vertex(Bf, xb, HB);
+        pick_vertex(Bf, (xb + 1) % 3, TB);
+        const float dj = seg_seg_dist32(HA, TA, HB, TB);
+        if (dj < de || (dj == de && 3 * xa + xb < 3 * ea + eb)) { de = dj; ea = xa; eb = xb; }
+      }
+    } else {
+      pick_vertex(Af, ea, HA);
+      pick_vertex(Af, (ea + 1) % 3, TA);
+      pick_vertex(Bf, eb, HB);
+      pick_vertex(Bf, (eb + 1) % 3, TB);
+      de = seg_seg_dist32(HA, TA, HB, TB);
     }
-  } else {
-    pick_vertex(Af, ea, HA);
-    pick_vertex(Af, (ea + 1) % 3, TA);
-    pick_vertex(Bf, eb, HB);
-    pick_vertex(Bf, (eb + 1) % 3, TB);
-    de = seg_seg_dist32(HA, TA, HB, TB);
+    edge0 = dpt > de;
+    code0 = edge0 ? (unsigned)(ea | (eb << 2)) : (unsigned)(vtx | (faceB ? 4 : 0));
   }
-  const bool edge = dpt > de;
+  // Regroup the block's pairs by family before the FP64 stage: an edge pair and a
+  // vertex-face pair run different FP64 code, so edge pairs go first and vertex-face pairs
+  // after them (each family in pair order), and thread t continues with item t.  A warp
+  // then runs one family's code, except the warp whose items straddle the boundary.
+  __shared__ uint16_t s_item[128];
+  __shared__ int s_cnt[2][4];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned be = __ballot_sync(0xffffffffu, valid0 && edge0), bv = __ballot_sync(0xffffffffu, valid0 && !edge0);
+  if (lane == 0) {
+    s_cnt[0][wid] = __popc(be);
+    s_cnt[1][wid] = __popc(bv);
+  }
+  __syncthreads();
+  int nE = 0, nV = 0, preE = 0, preV = 0;
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const int ce = s_cnt[0][w], cv = s_cnt[1][w];
+    preE += w < wid ? ce : 0;
+    preV += w < wid ? cv : 0;
+    nE += ce;
+    nV += cv;
+  }
+  if (valid0) {
+    const int pos = edge0 ? preE + __popc(be & lt) : nE + preV + __popc(bv & lt);
+    s_item[pos] = (uint16_t)(tid | (edge0 ? 128u : 0u) | (code0 << 8));
+  }
+  __syncthreads();
+  // threads past the block's pairs (last block only) repeat item 0 and write nothing
+  const bool has = tid < nE + nV;
+  const unsigned item = s_item[has ? tid : 0];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + (item & 127), ii = i;
+  const bool edge = (item & 128u) != 0;
+  const int ea = (item >> 8) & 3, eb = (item >> 10) & 3, vtx = (item >> 8) & 3;
+  const bool faceB = ((item >> 10) & 1) != 0;
   // FP64 stage: only the chosen feature's vertices are loaded (again), then the six
   // vertices stream through the certificate one at a time
   auto vtx64 = [&](const double *T, int v, xf64 out[3]) {
@@ -984,34 +1024,38 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
     const double d2r = d * d;
     ok = d2r - (amin - bmax) + 1e-14 * scale * d <= rel_tol * d2r;
   }
-  if (!valid) return;
-  if (list && !ok) {
-    // append, aggregated over the lanes that arrive here together (whatever the warp's
-    // convergence after the data-dependent branches above)
-    const unsigned grp = __activemask();
-    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
-    unsigned base = 0;
-    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(grp));
-    base = __shfl_sync(grp, base, leader);
-    const uint32_t slot = base + __popc(grp & ((1u << lane) - 1u));
-    list[slot] = (uint32_t)i;
-    if (stage) {
-      // the pair's coordinates, compact at its list position, for the exact solver
-#pragma unroll
-      for (int c = 0; c < 9; ++c) {
-        stage[c * (int64_t)n + slot] = ld_again(a + c * ld + i);
-        stage[(9 + c) * (int64_t)n + slot] = ld_again(b + c * ld + i);
-      }
-    }
-  }
-  if (ok || !list) {
+  if (has && (ok || !list)) {
     for (int k = 0; k < 3; ++k) {
       p[k * ld + i] = pq[k].v;
       q[k * ld + i] = pq[3 + k].v;
     }
     dist[i] = d;
   }
-  if (flags) flags[i] = list ? (ok ? 1 : 2) : (ok ? 1 : 0);
+  if (has && flags) flags[i] = list ? (ok ? 1 : 2) : (ok ? 1 : 0);
+  if (!list) return;
+  // The uncertified pairs are appended by their own threads, in pair order, so the list
+  // (and the exact solver's reads and writes through it) keeps the pairs' order.
+  __shared__ uint8_t s_bad[128];
+  if (has) s_bad[item & 127] = ok ? 0 : 1;
+  __syncthreads();
+  if (valid0 && s_bad[tid]) {
+    // append, aggregated over the lanes that arrive here together
+    const unsigned grp = __activemask();
+    const int leader = __ffs(grp) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const uint32_t slot = base + __popc(grp & lt);
+    list[slot] = (uint32_t)i0;
+    if (stage) {
+      // the pair's coordinates, compact at its list position, for the exact solver
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        stage[c * (int64_t)n + slot] = ld_again(a + c * ld + i0);
+        stage[(9 + c) * (int64_t)n + slot] = ld_again(b + c * ld + i0);
+      }
+    }
+  }
 }
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
