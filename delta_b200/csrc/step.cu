@@ -415,12 +415,19 @@ struct Grid {
   double origin[3];
 };
 
+// Cell keys take each cell coordinate modulo 2^kCellBits.  Cells that far apart share a
+// key, so their bodies become extra candidates that spheres_touch rejects, but the 27
+// neighbours of a cell always have distinct keys, so no pair is missed.  Obstacles get
+// kObstacleKey, above every cell key, and sort after the moving bodies; the cell sort
+// runs over kCellKeyBits bits.
+constexpr int kCellBits = 10;
+constexpr int64_t kCellMask = (1 << kCellBits) - 1;
+constexpr uint64_t kObstacleKey = 1ull << (3 * kCellBits);
+constexpr int kCellKeyBits = 3 * kCellBits + 1;
+
 __device__ __forceinline__ uint64_t cell_key(int64_t cx, int64_t cy, int64_t cz) {
-  const int64_t M = (1 << 21) - 1;
-  cx = cx < 0 ? 0 : (cx > M ? M : cx);
-  cy = cy < 0 ? 0 : (cy > M ? M : cy);
-  cz = cz < 0 ? 0 : (cz > M ? M : cz);
-  return ((uint64_t)cx << 42) | ((uint64_t)cy << 21) | (uint64_t)cz;
+  return ((uint64_t)(cx & kCellMask) << (2 * kCellBits)) | ((uint64_t)(cy & kCellMask) << kCellBits) |
+         (uint64_t)(cz & kCellMask);
 }
 
 __device__ __forceinline__ void cell_of(const delta_scene &s, const Grid &g, int32_t i, int64_t c[3]) {
@@ -433,7 +440,7 @@ __global__ void k_cell_keys(delta_scene s, Grid g, uint64_t *key, int32_t *body)
   if (i >= s.n_bodies) return;
   int64_t c[3];
   cell_of(s, g, i, c);
-  key[i] = s.obstacle[i] ? ~0ull : cell_key(c[0], c[1], c[2]);
+  key[i] = s.obstacle[i] ? kObstacleKey : cell_key(c[0], c[1], c[2]);
   body[i] = i;
 }
 
@@ -456,33 +463,35 @@ __device__ __forceinline__ void push_pair(int32_t a, int32_t b, int sh, uint64_t
   if ((int64_t)pos < cap) out[pos] = ((uint64_t)(uint32_t)(a < b ? a : b) << sh) | (uint32_t)(a < b ? b : a);
 }
 
-// One thread per (moving body, cell column (dx, dy)): the three cells (cx+dx, cy+dy,
-// cz-1 .. cz+1) have consecutive keys, so one binary search finds the column's bodies in the
-// sorted keys.  Columns outside the key range are skipped (every key is clamped into it, so
-// the clamped column is the body's own); pairs are pushed once, for j > i.
+// One thread per (moving body, cell column (dx, dy)): the cells (cx+dx, cy+dy, cz-1 ..
+// cz+1) have consecutive keys (two runs when the z coordinate wraps), so one binary search
+// per run finds the column's bodies in the sorted keys.  Every body has one key and the
+// 27 neighbour cells have distinct keys, so each candidate is met once; pairs are pushed
+// for j > i.
 __global__ void k_grid_pairs(delta_scene s, Grid g, const uint64_t *skey, const int32_t *sbody, int32_t n_moving,
                              int sh, uint64_t *out, unsigned long long *count, int64_t cap) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 9 * (int64_t)n_moving) return;
   const int32_t p = (int32_t)(t / 9), col = (int32_t)(t % 9);
-  const int64_t M = (1 << 21) - 1;
   const int32_t i = sbody[p];
   int64_t c[3];
   cell_of(s, g, i, c);
-  for (int k = 0; k < 3; ++k) c[k] = c[k] < 0 ? 0 : (c[k] > M ? M : c[k]);
   const int64_t cx = c[0] + col / 3 - 1, cy = c[1] + col % 3 - 1;
-  if (cx < 0 || cx > M || cy < 0 || cy > M) return;
-  const uint64_t k0 = cell_key(cx, cy, c[2] - 1 < 0 ? 0 : c[2] - 1);
-  const uint64_t k1 = cell_key(cx, cy, c[2] + 1 > M ? M : c[2] + 1);
-  int32_t lo = 0, hi = n_moving;
-  while (lo < hi) {
-    const int32_t mid = (lo + hi) >> 1;
-    if (skey[mid] < k0) lo = mid + 1;
-    else hi = mid;
-  }
-  for (int32_t q = lo; q < n_moving && skey[q] <= k1; ++q) {
-    const int32_t j = sbody[q];
-    if (j > i && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
+  const int64_t z0 = (c[2] - 1) & kCellMask, z1 = (c[2] + 1) & kCellMask;
+  const int runs = z0 <= z1 ? 1 : 2;
+  for (int r = 0; r < runs; ++r) {
+    const uint64_t k0 = cell_key(cx, cy, r == 0 ? z0 : 0);
+    const uint64_t k1 = cell_key(cx, cy, runs == 1 || r == 1 ? z1 : kCellMask);
+    int32_t lo = 0, hi = n_moving;
+    while (lo < hi) {
+      const int32_t mid = (lo + hi) >> 1;
+      if (skey[mid] < k0) lo = mid + 1;
+      else hi = mid;
+    }
+    for (int32_t q = lo; q < n_moving && skey[q] <= k1; ++q) {
+      const int32_t j = sbody[q];
+      if (j > i && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
+    }
   }
 }
 
@@ -636,7 +645,8 @@ delta_status broadphase_plan(delta_ctx *ctx, const delta_scene &s, BroadphasePla
   }
   plan.release();
   plan.g.h = reach > 0 ? 2.0 * reach * (1.0 + 1e-6) : 1.0;
-  for (int k = 0; k < 3; ++k) plan.g.origin[k] = (lo[k] < 1e299 ? lo[k] : 0.0) - (double)(1 << 20) * plan.g.h;
+  // cell keys wrap (cell_key), so any origin works; the lowest moving centre is used
+  for (int k = 0; k < 3; ++k) plan.g.origin[k] = lo[k] < 1e299 ? lo[k] : 0.0;
   plan.n_obst = (int32_t)ob.size();
   plan.n_moving = n - plan.n_obst;
   if (plan.n_obst > 0) {
@@ -689,10 +699,10 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body);
   ctx->launches += 1;
   size_t tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, body, sbody, n, 0, 64, st);
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st);
   void *temp = nullptr;
   if ((ds = ctx_scratch(ctx, 12, tb, &temp)) != DELTA_OK) return ds;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, 64, st)) != cudaSuccess)
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st)) != cudaSuccess)
     return cuda_error(e, "cell sort");
   ctx->launches += 1;
   int64_t cap = capacity > 4096 ? capacity : 4096;
@@ -815,7 +825,7 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
   uint64_t *pk = (uint64_t *)(b + 256), *spk = pk + pair_cap;
   k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body);
   size_t tb = temp_bytes;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, 64, st)) != cudaSuccess)
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st)) != cudaSuccess)
     return cuda_error(e, "cell sort");
   if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(pk, 0xff, sizeof(uint64_t) * pair_cap, st)) != cudaSuccess)
