@@ -334,21 +334,23 @@ __global__ void __launch_bounds__(128) k_detect(delta_meshes m, const int32_t *_
   }
 }
 
-// ---- certified driver, phase 1: exact box culling, one warp per particle pair ----------
+// ---- certified driver, phase 1: exact box culling, one block per particle pair ---------
 // bf()'s distance is the length of a point pair on the two triangles, never below the gap
 // between their bounding boxes, so a triangle pair whose boxes are farther apart than
 // epsA+epsB (with a relative margin for rounding) cannot give a contact (bf.cpp:125).  A
-// warp stages in shared memory the A triangles whose box is within the cull distance of
+// block stages in shared memory the A triangles whose box is within the cull distance of
 // B's body box and the B triangles within it of A's body box (at most kCullList each;
 // longer lists are taken in windows) and then tests the staged boxes pair by pair.  The
 // survivors are exactly the triangle pairs whose boxes pass the test: every triangle box
 // lies in its body box and the per-axis gaps, their squares and their sum are monotone in
 // the boxes, so a triangle dropped against a body box fails against every triangle of
 // that body too.
-constexpr int kCullList = 64;
+constexpr int kCullThreads = 128;
+constexpr int kCullList = 256;
 struct CullList {
   double lo[3][kCullList], hi[3][kCullList];
   uint16_t idx[kCullList];
+  int n;
 };
 
 // squared gap between the boxes (alo, ahi) and (blo, bhi): the sum of the squares of the
@@ -365,14 +367,15 @@ __device__ __forceinline__ double box_gap2(const double alo[3], const double ahi
 }
 
 // Stages the triangles cur, cur+1, ... of (t0, n) whose box lies within the cull distance
-// of the box (olo, ohi) into L, 32 at a time while L can take 32 more; returns the cursor.
+// of the box (olo, ohi) into L (in any order), kCullThreads at a time while L can take
+// that many more; returns the cursor.  Called by the whole block.
 __device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, int64_t t0, int32_t n, int32_t cur,
-                                             const double olo[3], const double ohi[3], double cull2, CullList &L,
-                                             int &nL) {
-  const int lane = threadIdx.x & 31;
-  nL = 0;
-  while (cur < n && nL + 32 <= kCullList) {
-    const int32_t i = cur + lane;
+                                             const double olo[3], const double ohi[3], double cull2, CullList &L) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid == 0) L.n = 0;
+  __syncthreads();
+  while (cur < n && L.n + kCullThreads <= kCullList) {
+    const int32_t i = cur + tid;
     double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {0.0, 0.0, 0.0};
     bool keep = false;
     if (i < n) {
@@ -386,8 +389,11 @@ __device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, int64_t t0, 
       keep = box_gap2(lo, hi, olo, ohi) <= cull2;
     }
     const unsigned bal = __ballot_sync(kFull, keep);
+    int base = 0;
+    if (lane == 0 && bal) base = atomicAdd(&L.n, __popc(bal));
+    base = __shfl_sync(kFull, base, 0);
     if (keep) {
-      const int s = nL + __popc(bal & ((1u << lane) - 1u));
+      const int s = base + __popc(bal & ((1u << lane) - 1u));
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         L.lo[k][s] = lo[k];
@@ -395,30 +401,27 @@ __device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, int64_t t0, 
       }
       L.idx[s] = (uint16_t)i;
     }
-    nL += __popc(bal);
-    cur += 32;
+    cur += kCullThreads;
+    __syncthreads();
   }
-  __syncwarp();
   return cur;
 }
 
-// Pairs k = warp, warp + n_warps, ... (entries with a negative body are empty).  Survivor
-// keys (pair << 32 | A triangle << 16 | B triangle) go to rc.sv; their order is free (the
-// contacts are sorted by key afterwards).  rc.bbox holds the body boxes of the current
-// vertices (null: no body-box tests).
-__global__ void __launch_bounds__(128) k_cull_pairs(delta_meshes m, const int32_t *__restrict__ pa,
-                                                    const int32_t *__restrict__ pb, int64_t n_pairs, RawContacts rc,
-                                                    DevStats *st) {
-  __shared__ CullList lists[4][2];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  CullList &LA = lists[w][0], &LB = lists[w][1];
-  const int64_t n_warps = (int64_t)gridDim.x * 4;
-  for (int64_t k = (int64_t)blockIdx.x * 4 + w; k < n_pairs; k += n_warps) {
+// Pairs k = block, block + n_blocks, ... (entries with a negative body are empty).
+// Survivor keys (pair << 32 | A triangle << 16 | B triangle) go to rc.sv; their order is
+// free (the contacts are sorted by key afterwards).  rc.bbox holds the body boxes of the
+// current vertices (null: no body-box tests).
+__global__ void __launch_bounds__(kCullThreads) k_cull_pairs(delta_meshes m, const int32_t *__restrict__ pa,
+                                                             const int32_t *__restrict__ pb, int64_t n_pairs,
+                                                             RawContacts rc, DevStats *st) {
+  __shared__ CullList LA, LB;
+  const int tid = threadIdx.x;
+  for (int64_t k = blockIdx.x; k < n_pairs; k += gridDim.x) {
     const int32_t a = pa[k], b = pb[k];
     if (a < 0 || b < 0) continue;
     const int64_t tA0 = m.tri_offset[a], tB0 = m.tri_offset[b];
     const int32_t nA = (int32_t)(m.tri_offset[a + 1] - tA0), nB = (int32_t)(m.tri_offset[b + 1] - tB0);
-    if (lane == 0) atomicAdd(&st->tri_pairs, (unsigned long long)nA * (unsigned long long)nB);
+    if (tid == 0) atomicAdd(&st->tri_pairs, (unsigned long long)nA * (unsigned long long)nB);
     const double mg = (xf64(m.eps[a]) + xf64(m.eps[b])).v;
     const double cull = mg * (1.0 + 1e-9) + 1e-12, cull2 = cull * cull;
     double Alo[3], Ahi[3], Blo[3], Bhi[3];
@@ -431,14 +434,13 @@ __global__ void __launch_bounds__(128) k_cull_pairs(delta_meshes m, const int32_
     }
     if (box_gap2(Alo, Ahi, Blo, Bhi) > cull2) continue;
     for (int32_t cb = 0; cb < nB;) {
-      int nLB = 0;
-      cb = cull_fill(m, tB0, nB, cb, Alo, Ahi, cull2, LB, nLB);
+      cb = cull_fill(m, tB0, nB, cb, Alo, Ahi, cull2, LB);
+      const int nLB = LB.n;
       if (nLB == 0) continue;
       for (int32_t ca = 0; ca < nA;) {
-        int nLA = 0;
-        ca = cull_fill(m, tA0, nA, ca, Blo, Bhi, cull2, LA, nLA);
-        const int np = nLA * nLB;
-        for (int j = lane; j < np; j += 32) {
+        ca = cull_fill(m, tA0, nA, ca, Blo, Bhi, cull2, LA);
+        const int np = LA.n * nLB;
+        for (int j = tid; j < np; j += kCullThreads) {
           const int ia = j / nLB, ib = j - ia * nLB;
           const double alo[3] = {LA.lo[0][ia], LA.lo[1][ia], LA.lo[2][ia]};
           const double ahi[3] = {LA.hi[0][ia], LA.hi[1][ia], LA.hi[2][ia]};
@@ -450,7 +452,7 @@ __global__ void __launch_bounds__(128) k_cull_pairs(delta_meshes m, const int32_
               rc.sv[pos] = ((uint64_t)k << 32) | ((uint64_t)LA.idx[ia] << 16) | (uint64_t)LB.idx[ib];
           }
         }
-        __syncwarp();
+        __syncthreads();  // LA is refilled next
       }
     }
   }
@@ -459,12 +461,11 @@ __global__ void __launch_bounds__(128) k_cull_pairs(delta_meshes m, const int32_
 inline cudaError_t launch_cull(cudaStream_t s, const delta_meshes &m, const int32_t *pa, const int32_t *pb,
                                int64_t n_pairs, const RawContacts &rc, DevStats *st) {
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cull_pairs, 128, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cull_pairs, kCullThreads, 0);
   if (e != cudaSuccess) return e;
   int64_t blocks = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
-  const int64_t need = (n_pairs + 3) / 4;
-  if (blocks > need) blocks = need > 0 ? need : 1;
-  k_cull_pairs<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, n_pairs, rc, st);
+  if (blocks > n_pairs) blocks = n_pairs > 0 ? n_pairs : 1;
+  k_cull_pairs<<<(unsigned)blocks, kCullThreads, 0, s>>>(m, pa, pb, n_pairs, rc, st);
   return cudaGetLastError();
 }
 
