@@ -34,8 +34,10 @@ struct RawContacts {
   uint64_t *sv;
   int64_t sv_cap;
   unsigned long long *sv_count;
-  // certified driver: per-body boxes (lo[3], hi[3]) for the row prefilter, or null
+  // certified driver: per-body boxes (lo[3], hi[3]) for the culling, or null
   const double *bbox;
+  // sort key of a contact: pair << 2 tbits | A triangle << tbits | B triangle
+  int tbits;
 };
 
 struct DevStats {
@@ -124,7 +126,7 @@ __device__ __forceinline__ void write_contact(const RawContacts &rc, int64_t pos
   rc.i[2 * cap + pos] = r.iA;
   rc.i[3 * cap + pos] = tb;
   rc.fric[pos] = r.fric;
-  rc.key[pos] = ((uint64_t)r.k << 32) | ((uint64_t)r.iA << 16) | (uint64_t)tb;
+  rc.key[pos] = ((uint64_t)r.k << (2 * rc.tbits)) | ((uint64_t)r.iA << rc.tbits) | (uint64_t)tb;
 }
 
 // Slot for the calling lane in an append buffer: one atomic per group of lanes that
@@ -698,8 +700,9 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   int64_t cap = out->capacity > 1024 ? out->capacity : 1024;
   unsigned long long hcount = 0;
   RawContacts rc{};
+  rc.tbits = 16;
   if (driver == DELTA_DRV_BF_CERT) {
-    // body boxes of the current vertices for the row prefilter
+    // body boxes of the current vertices for the culling
     void *bb = nullptr;
     if ((st = ctx_scratch(ctx, 23, 48 * (size_t)m.n_bodies + 64, &bb)) != DELTA_OK) return st;
     const int64_t warps = std::min<int64_t>(m.n_bodies, (int64_t)kNumSMs * 64);
@@ -840,7 +843,7 @@ size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap) {
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
-                              void *temp, size_t temp_bytes, const double *bbox) {
+                              void *temp, size_t temp_bytes, const double *bbox, int tri_bits) {
   cudaError_t e;
   const int64_t cap = out.capacity;
   char *p = (char *)state;
@@ -850,6 +853,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   int64_t *rows = (int64_t *)p, *row_offset = rows + pair_cap + 1;
   p += sizeof(int64_t) * (size_t)(2 * pair_cap + 2);
   RawContacts rc{};
+  rc.tbits = tri_bits;
   rc.cap = cap;
   rc.f = (double *)p;
   rc.key = (uint64_t *)(rc.f + 14 * cap);
@@ -886,10 +890,11 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   }
   if (e != cudaSuccess) return cuda_error(e, "detect kernel");
   k_iota<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(perm_in, cap);
-  // keys (pair << 32 | A tri << 16 | B tri) of pairs below pair_cap: the bits above the pair
-  // index are zero (empty entries, ~0, still sort last: stable, and after every valid key)
-  int end_bit = 33;
-  while (end_bit < 64 && ((int64_t)1 << (end_bit - 32)) < pair_cap) ++end_bit;
+  // keys (pair << 2 tri_bits | A tri << tri_bits | B tri) of pairs below pair_cap: the bits
+  // above the pair index are zero (empty entries, ~0, still sort last: stable, and after
+  // every valid key)
+  int end_bit = 2 * rc.tbits + 1;
+  while (end_bit < 64 && ((int64_t)1 << (end_bit - 2 * rc.tbits)) < pair_cap) ++end_bit;
   tb = temp_bytes;
   if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, rc.key, key_out, perm_in, perm_out, cap, 0, end_bit, s)) !=
       cudaSuccess)

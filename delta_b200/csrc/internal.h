@@ -45,14 +45,15 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
                         delta_stats *stats, int64_t *counters = nullptr);
 
 // Fixed-capacity (graph-capturable) detection (detect.cu).  `bbox`: the boxes (lo[3], hi[3])
-// of every body's current vertices, written by the caller, for the certified driver's row
-// prefilter, or null.
+// of every body's current vertices, written by the caller, for the certified driver's
+// culling, or null.  `tri_bits`: bits of a triangle index within a body (every body has
+// fewer than 2^tri_bits triangles), used to pack the contact sort keys.
 size_t detect_fixed_temp_bytes(int64_t pair_cap, int64_t cap);
 size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap);
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
-                              void *temp, size_t temp_bytes, const double *bbox = nullptr);
+                              void *temp, size_t temp_bytes, const double *bbox = nullptr, int tri_bits = 16);
 
 // Thread-local last-error text (capi.cu).
 delta_status set_error(delta_status st, const std::string &msg);

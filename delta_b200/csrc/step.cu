@@ -316,7 +316,7 @@ __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force
 // updateVertices, dynamics.cpp:215-242, one warp per body: the body's 15 scalars (R, pos,
 // ref_pos) are loaded by lanes 0..14 and broadcast, the lanes then stride over the body's
 // vertices.  With `bbox` given the kernel also writes the box (lo[3], hi[3]) of every body's
-// current vertices, obstacles included, for the certified driver's row prefilter.  With the
+// current vertices, obstacles included, for the certified driver's culling.  With the
 // overflow flag set no vertex moves (graph mode: the state is frozen) but the boxes are
 // still written, so they always describe the vertices in memory.
 __global__ void k_vertices(delta_scene s, const int *ovf, double *bbox) {
@@ -867,6 +867,7 @@ struct delta_sim {
   int driver = DELTA_DRV_BF;
   delta::BroadphasePlan plan;
   int64_t n_tri = 0;
+  int tri_bits = 16;  // bits of a triangle index within a body (the graph's contact sort keys)
   int32_t *ids = nullptr;
   // contacts of the last detection
   delta_contacts c{};
@@ -888,7 +889,7 @@ struct delta_sim {
     size_t temp_bytes = 0;
     delta_contacts c{};
     int64_t *d_nc = nullptr, *d_step = nullptr, *d_cnt = nullptr, *d_log = nullptr;
-    double *bbox = nullptr;  // body boxes (written by k_vertices) for the certified driver's row prefilter
+    double *bbox = nullptr;  // body boxes (written by k_vertices) for the certified driver's culling
     int *d_ovf = nullptr, *d_snap = nullptr;
     int64_t log_len = 0;
     cudaStream_t stream = nullptr;
@@ -1039,7 +1040,7 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
                  s->scene.eps,      s->scene.friction,   s->ids};
   const int64_t before = s->ctx->launches;
   if ((ds = detect_run_fixed(s->ctx, st, s->driver, m, g.pa, g.pb, g.pair_cap, g.c, g.d_nc, g.d_ovf, 1, g.d_cnt,
-                             nullptr, g.ds, g.temp, g.temp_bytes, g.bbox)) != DELTA_OK)
+                             nullptr, g.ds, g.temp, g.temp_bytes, g.bbox, s->tri_bits)) != DELTA_OK)
     return ds;
   k += (int)(s->ctx->launches - before);
   s->ctx->launches = before;
@@ -1141,9 +1142,14 @@ delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driv
   s->scene = *scene;
   s->driver = driver;
   const int32_t n = scene->n_bodies;
-  cudaError_t e = cudaMemcpy(&s->n_tri, scene->tri_offset + n, sizeof(int64_t), cudaMemcpyDeviceToHost);
+  std::vector<int64_t> off((size_t)n + 1);
+  cudaError_t e = cudaMemcpy(off.data(), scene->tri_offset, sizeof(int64_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost);
   delta_status ds = DELTA_OK;
   if (e != cudaSuccess) ds = cuda_error(e, "sim create");
+  s->n_tri = off[n];
+  int64_t max_tri = 1;
+  for (int32_t i = 0; i < n; ++i) max_tri = std::max<int64_t>(max_tri, off[i + 1] - off[i]);
+  s->tri_bits = max_tri <= 65536 ? bits_for(max_tri - 1) : 16;
   if (ds == DELTA_OK && (e = cudaMalloc(&s->ids, sizeof(int32_t) * n)) != cudaSuccess) ds = cuda_error(e, "ids");
   if (ds == DELTA_OK && (e = cudaMalloc(&s->F, sizeof(double) * 6 * n + n)) != cudaSuccess) ds = cuda_error(e, "F");
   if (ds == DELTA_OK) {
