@@ -1230,16 +1230,21 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
     if ((ds = delta_sim_step(s, params, 1, contacts_per_step)) != DELTA_OK) return ds;
     done = 1;
   }
+  const bool requested = s->graph_pair_cap > 0 || s->graph_contact_cap > 0;
   int64_t want_pairs = std::max<int64_t>(1024, 2 * std::max<int64_t>(s->counters[1] / std::max<int64_t>(1, s->counters[0]), 1));
   int64_t want_contacts = std::max<int64_t>(2048, 4 * s->n_contacts);
   if (s->graph_pair_cap > 0) want_pairs = s->graph_pair_cap;
   if (s->graph_contact_cap > 0) want_contacts = s->graph_contact_cap;
   want_contacts = std::max<int64_t>(want_contacts, s->n_contacts);  // the current list must fit
   s->graph_pair_cap = s->graph_contact_cap = 0;
-  if (!g.pa || g.pair_cap < want_pairs || g.contact_cap < want_contacts || g.log_len < nsteps ||
-      g.pair_cap != want_pairs || g.contact_cap != want_contacts) {
-    if ((ds = graph_alloc(s, std::max(g.pair_cap, want_pairs), std::max(g.contact_cap, want_contacts),
-                          std::max<int64_t>(g.log_len, nsteps))) != DELTA_OK)
+  // The buffers (and the recorded graph) are kept from call to call while the current
+  // contacts and the step log fit; a replay that overflows grows them.  They are sized anew
+  // on the first call, on a capacity request, or when the contacts or the log outgrew them.
+  if (!g.pa || requested || g.contact_cap < s->n_contacts || g.log_len < nsteps) {
+    const bool fresh = !g.pa || requested;
+    if ((ds = graph_alloc(s, fresh ? want_pairs : std::max(g.pair_cap, want_pairs),
+                          fresh ? want_contacts : std::max(g.contact_cap, want_contacts),
+                          std::max<int64_t>({g.log_len, (int64_t)nsteps, 4096}))) != DELTA_OK)
       return ds;
   }
   if (memcmp(&g.params, params, sizeof(*params)) != 0) g.captured = false;
