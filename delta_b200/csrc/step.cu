@@ -208,8 +208,11 @@ __global__ void k_segment_heads_fixed(ContactView cv, int64_t cap, const int64_t
   head[c] = c < n && (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]) ? 1 : 0;
 }
 
-__global__ void k_flag_overflow(const unsigned long long *count, int64_t cap, int *ovf) {
+// Flags a pair-list overflow; adds the step's candidate body pairs to *total (graph mode's
+// body-pair counter).
+__global__ void k_flag_overflow(const unsigned long long *count, int64_t cap, int *ovf, int64_t *total) {
   if (*count > (unsigned long long)cap) atomicCAS(ovf, 0, 1);
+  if (total) *total += (int64_t)(*count < (unsigned long long)cap ? *count : (unsigned long long)cap);
 }
 
 __global__ void k_step_begin(const int *ovf, int *ovf_snap) { *ovf_snap = *ovf; }
@@ -811,8 +814,8 @@ size_t broadphase_fixed_temp_bytes(int32_t n, int64_t pair_cap) {
 }
 
 delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, int32_t *pair_a,
-                                  int32_t *pair_b, int64_t pair_cap, int *ovf, void *state, void *temp,
-                                  size_t temp_bytes, int &kernels) {
+                                  int32_t *pair_b, int64_t pair_cap, int *ovf, int64_t *pairs_total, void *state,
+                                  void *temp, size_t temp_bytes, int &kernels) {
   cudaError_t e;
   const int32_t n = s.n_bodies;
   const int sh = bits_for(n);
@@ -845,7 +848,7 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
   if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, pair_cap, 0, 2 * sh, st)) != cudaSuccess)
     return cuda_error(e, "pair sort");
   k_unpack_pairs<<<blocks_for(pair_cap), 256, 0, st>>>(spk, pair_cap, sh, pair_a, pair_b);
-  k_flag_overflow<<<1, 1, 0, st>>>(count, pair_cap, ovf);
+  k_flag_overflow<<<1, 1, 0, st>>>(count, pair_cap, ovf, pairs_total);
   kernels += 3;
   return cuda_error(cudaGetLastError(), "broadphase fixed");
 }
@@ -891,6 +894,7 @@ struct delta_sim {
     int64_t *d_nc = nullptr, *d_step = nullptr, *d_cnt = nullptr, *d_log = nullptr;
     double *bbox = nullptr;  // body boxes (written by k_vertices) for the certified driver's culling
     int *d_ovf = nullptr, *d_snap = nullptr;
+    int64_t *d_bp = nullptr;  // candidate body pairs summed over the replayed steps
     int64_t log_len = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
@@ -1017,6 +1021,7 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
   g.d_cnt = (int64_t *)(v + 16);
   g.d_ovf = (int *)(v + 32);
   g.d_snap = (int *)(v + 36);
+  g.d_bp = (int64_t *)(v + 40);
   g.d_log = (int64_t *)(v + 256);
   if ((e = cudaMemset(g.dev, 0, 256)) != cudaSuccess) return cuda_error(e, "graph memset");
   return DELTA_OK;
@@ -1033,7 +1038,8 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf);
   k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, g.d_ovf,
                                                                s->driver == DELTA_DRV_BF_CERT ? g.bbox : nullptr);
-  if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.bp, g.temp, g.temp_bytes,
+  if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_bp, g.bp, g.temp,
+                                 g.temp_bytes,
                                  k)) != DELTA_OK)
     return ds;
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
@@ -1257,6 +1263,7 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
   if ((e = cudaMemcpyAsync(g.d_nc, &hv[0], 8, cudaMemcpyHostToDevice, g.stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(g.d_step, 0, 8, g.stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(g.d_cnt, 0, 16, g.stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(g.d_bp, 0, 8, g.stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(g.d_ovf, 0, 8, g.stream)) != cudaSuccess || (e = cudaStreamSynchronize(g.stream)) != cudaSuccess)
     return cuda_error(e, "graph setup");
   int32_t base = done;  // steps completed before the current batch of launches
@@ -1290,8 +1297,11 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
     if ((e = cudaStreamSynchronize(s->ctx->stream)) != cudaSuccess) return cuda_error(e, "sync");
     if ((ds = sim_detect(s)) != DELTA_OK) return ds;  // non-graph detection of the current state
     if (contacts_per_step && done > 0) contacts_per_step[done - 1] = s->n_contacts;
-    int64_t saved_log = g.log_len, seg_cnt[2] = {0, 0};
-    if ((e = cudaMemcpy(seg_cnt, g.d_cnt, 16, cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_error(e, "counters");
+    int64_t saved_log = g.log_len, seg_cnt[2] = {0, 0}, seg_bp = 0;
+    if ((e = cudaMemcpy(seg_cnt, g.d_cnt, 16, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(&seg_bp, g.d_bp, 8, cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return cuda_error(e, "counters");
+    s->counters[1] += seg_bp;
     s->counters[2] += seg_cnt[0];
     s->counters[3] += seg_cnt[1];
     if ((ds = graph_alloc(s, std::max<int64_t>(2 * g.pair_cap, 2 * (int64_t)pc), std::max<int64_t>(2 * g.contact_cap,
@@ -1305,10 +1315,12 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
     base = done;
   }
   // counters and contacts back to the simulation object
-  int64_t cnt[2] = {0, 0}, nc = 0;
+  int64_t cnt[2] = {0, 0}, nc = 0, bp = 0;
   if ((e = cudaMemcpy(cnt, g.d_cnt, 16, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(&bp, g.d_bp, 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
       (e = cudaMemcpy(&nc, g.d_nc, 8, cudaMemcpyDeviceToHost)) != cudaSuccess)
     return cuda_error(e, "graph counters");
+  s->counters[1] += bp;
   s->counters[2] += cnt[0];
   s->counters[3] += cnt[1];
   if (nc > s->c.capacity && (ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;

@@ -120,3 +120,25 @@ def test_graph_replay_equals_stepping(ctx, oracle, scene, caps):
     assert len(c) == len(o_c)
     for f in FIELDS:
         assert np.array_equal(c[f], o_c[f]), f
+
+
+def test_graph_counters_and_repeated_calls_match_stepping(ctx, scene):
+    """Graph replays spread over several calls (1, 3, then 16 steps) give the stepped
+    trajectory and the same step, body-pair and triangle-pair counters."""
+    from delta_b200.engine import Simulation, StepParams
+
+    p = StepParams.make(**PARAMS)
+    ref = Simulation(ctx, scene, 8)
+    ref.step(20, p)
+    r_state, r_cnt = ref.state(), ref.counters()
+    ref.close()
+    sim = Simulation(ctx, scene, 8)
+    sim.set_graph_capacity(1 << 14, 1 << 16)
+    for n in (1, 3, 16):
+        sim.step(n, p, graph=True)
+    st, cnt = sim.state(), sim.counters()
+    sim.close()
+    for k in STATE:
+        assert np.array_equal(st[k], r_state[k]), k
+    for k in ("steps", "body_pairs", "triangle_pairs", "solved"):
+        assert cnt[k] == r_cnt[k], (k, cnt[k], r_cnt[k])
