@@ -215,7 +215,10 @@ __global__ void k_flag_overflow(const unsigned long long *count, int64_t cap, in
   if (total) *total += (int64_t)(*count < (unsigned long long)cap ? *count : (unsigned long long)cap);
 }
 
-__global__ void k_step_begin(const int *ovf, int *ovf_snap) { *ovf_snap = *ovf; }
+__global__ void k_step_begin(const int *ovf, int *ovf_snap, uint32_t *epoch) {
+  *ovf_snap = *ovf;
+  *epoch += 1u;  // the vertex stamps of this step (k_mark_pair_bodies)
+}
 
 __global__ void k_step_end(const int *ovf_snap, const int64_t *n_contacts, int64_t *log, int64_t log_len,
                            int64_t *step) {
@@ -322,13 +325,17 @@ __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force
 // current vertices, obstacles included, for the certified driver's culling.  With the
 // overflow flag set no vertex moves (graph mode: the state is frozen) but the boxes are
 // still written, so they always describe the vertices in memory.
-__global__ void k_vertices(delta_scene s, const int *ovf, double *bbox) {
+// With `stamp`, only the bodies whose stamp equals *epoch (the bodies of this step's
+// candidate pairs, k_mark_pair_bodies) are processed.
+__global__ void k_vertices(delta_scene s, const int *ovf, double *bbox, const uint32_t *stamp, const uint32_t *epoch) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const bool frozen = ovf && *ovf;
+  const uint32_t ep = stamp ? *epoch : 0u;
   const int32_t n = s.n_bodies;
   for (int64_t i = warp; i < n; i += nwarps) {
+    if (stamp && stamp[i] != ep) continue;
     const bool move = !frozen && !s.obstacle[i];
     if (!move && !bbox) continue;
     double q = 0.0;
@@ -402,6 +409,21 @@ inline int bits_for(int64_t v) {
   int b = 1;
   while (b < 31 && ((int64_t)1 << b) <= v) ++b;
   return b;
+}
+
+// Next epoch of the vertex stamps (one thread).
+__global__ void k_next_epoch(uint32_t *epoch) { *epoch += 1u; }
+
+// Stamps both bodies of every pair (entries with a negative body are empty) with the
+// current epoch: these are the bodies whose vertices the narrowphase reads this step.
+__global__ void k_mark_pair_bodies(const int32_t *pa, const int32_t *pb, int64_t n, const uint32_t *epoch,
+                                   uint32_t *stamp) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t e = *epoch;
+  const int32_t a = pa[t], b = pb[t];
+  if (a >= 0) stamp[a] = e;
+  if (b >= 0) stamp[b] = e;
 }
 
 inline unsigned vertex_blocks(int32_t n_bodies) {
@@ -603,7 +625,7 @@ delta_status integrate_run(delta_ctx *ctx, const delta_scene &s, const delta_ste
   cudaStream_t st = ctx->stream;
   k_bodies<<<blocks_for(s.n_bodies, 128), 128, 0, st>>>(s, p, force, torque, has, nullptr);
   (void)n_vertices;
-  k_vertices<<<vertex_blocks(s.n_bodies), 256, 0, st>>>(s, nullptr, nullptr);
+  k_vertices<<<vertex_blocks(s.n_bodies), 256, 0, st>>>(s, nullptr, nullptr, nullptr, nullptr);
   ctx->launches += 2;
   return cuda_error(cudaGetLastError(), "integrate launch");
 }
@@ -872,6 +894,10 @@ struct delta_sim {
   int64_t n_tri = 0;
   int tri_bits = 16;  // bits of a triangle index within a body (the graph's contact sort keys)
   int32_t *ids = nullptr;
+  // Vertex stamps: during a call of several steps only the bodies of each step's candidate
+  // pairs get their vertices updated (stamp[i] == *epoch); every vertex is brought up to
+  // date at the end of the call.  [n] stamps, then the epoch.
+  uint32_t *stamp = nullptr, *epoch = nullptr;
   // contacts of the last detection
   delta_contacts c{};
   void *c_mem = nullptr;
@@ -942,6 +968,15 @@ static delta_status alloc_pairs(delta_sim *s, int64_t cap) {
   return DELTA_OK;
 }
 
+// updateVertices for every body: the end of a call of delta_sim_step(_graph), after which
+// the vertices in memory describe the state (the steps in between update only the bodies of
+// their candidate pairs).
+static delta_status sim_all_vertices(delta_sim *s, cudaStream_t st) {
+  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, nullptr, nullptr, nullptr, nullptr);
+  s->ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "vertex update");
+}
+
 static delta_status sim_detect(delta_sim *s) {
   delta_status ds;
   int64_t np = 0;
@@ -952,6 +987,12 @@ static delta_status sim_detect(delta_sim *s) {
   }
   if (ds != DELTA_OK) return ds;
   s->counters[1] += np;
+  // vertices of the bodies the narrowphase reads
+  cudaStream_t st = s->ctx->stream;
+  k_next_epoch<<<1, 1, 0, st>>>(s->epoch);
+  if (np > 0) k_mark_pair_bodies<<<blocks_for(np), 256, 0, st>>>(s->pa, s->pb, np, s->epoch, s->stamp);
+  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, nullptr, nullptr, s->stamp, s->epoch);
+  s->ctx->launches += np > 0 ? 3 : 2;
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
                  s->scene.eps,      s->scene.friction,   s->ids};
   int64_t nc = 0;
@@ -1032,16 +1073,17 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   delta_sim::Graph &g = s->g;
   cudaStream_t st = g.stream;
   int k = 0;
-  k_step_begin<<<1, 1, 0, st>>>(g.d_ovf, g.d_snap);
+  k_step_begin<<<1, 1, 0, st>>>(g.d_ovf, g.d_snap, s->epoch);
   delta_status ds = forces_run_fixed(st, s->scene, g.c, g.d_nc, p, s->F, s->T, s->has, g.fs, g.temp, g.temp_bytes, k);
   if (ds != DELTA_OK) return ds;
   k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf);
-  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, g.d_ovf,
-                                                               s->driver == DELTA_DRV_BF_CERT ? g.bbox : nullptr);
   if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_bp, g.bp, g.temp,
-                                 g.temp_bytes,
-                                 k)) != DELTA_OK)
+                                 g.temp_bytes, k)) != DELTA_OK)
     return ds;
+  // vertices (and boxes) of the bodies the narrowphase reads this step
+  k_mark_pair_bodies<<<blocks_for(g.pair_cap), 256, 0, st>>>(g.pa, g.pb, g.pair_cap, s->epoch, s->stamp);
+  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(
+      s->scene, g.d_ovf, s->driver == DELTA_DRV_BF_CERT ? g.bbox : nullptr, s->stamp, s->epoch);
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
                  s->scene.eps,      s->scene.friction,   s->ids};
   const int64_t before = s->ctx->launches;
@@ -1051,7 +1093,7 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   k += (int)(s->ctx->launches - before);
   s->ctx->launches = before;
   k_step_end<<<1, 1, 0, st>>>(g.d_snap, g.d_nc, g.d_log, g.log_len, g.d_step);
-  g.kernels = k + 4;
+  g.kernels = k + 5;
   return cuda_error(cudaGetLastError(), "graph step");
 }
 
@@ -1157,6 +1199,10 @@ delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driv
   for (int32_t i = 0; i < n; ++i) max_tri = std::max<int64_t>(max_tri, off[i + 1] - off[i]);
   s->tri_bits = max_tri <= 65536 ? bits_for(max_tri - 1) : 16;
   if (ds == DELTA_OK && (e = cudaMalloc(&s->ids, sizeof(int32_t) * n)) != cudaSuccess) ds = cuda_error(e, "ids");
+  if (ds == DELTA_OK && ((e = cudaMalloc(&s->stamp, sizeof(uint32_t) * ((size_t)n + 1))) != cudaSuccess ||
+                         (e = cudaMemset(s->stamp, 0, sizeof(uint32_t) * ((size_t)n + 1))) != cudaSuccess))
+    ds = cuda_error(e, "vertex stamps");
+  if (ds == DELTA_OK) s->epoch = s->stamp + n;
   if (ds == DELTA_OK && (e = cudaMalloc(&s->F, sizeof(double) * 6 * n + n)) != cudaSuccess) ds = cuda_error(e, "F");
   if (ds == DELTA_OK) {
     s->T = s->F + 3 * n;
@@ -1181,12 +1227,14 @@ delta_status delta_sim_step(delta_sim *s, const delta_step_params *params, int32
   for (int32_t k = 0; k < nsteps; ++k) {
     delta_status ds = forces_run(s->ctx, s->scene, s->c, s->n_contacts, *params, s->F, s->T, s->has);
     if (ds != DELTA_OK) return ds;
-    if ((ds = integrate_run(s->ctx, s->scene, *params, s->F, s->T, s->has, 3 * s->n_tri)) != DELTA_OK) return ds;
+    k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, s->ctx->stream>>>(s->scene, *params, s->F, s->T, s->has,
+                                                                              nullptr);
+    s->ctx->launches += 1;
     if ((ds = sim_detect(s)) != DELTA_OK) return ds;
     s->counters[0] += 1;
     if (contacts_per_step) contacts_per_step[k] = s->n_contacts;
   }
-  return DELTA_OK;
+  return sim_all_vertices(s, s->ctx->stream);
 }
 
 delta_status delta_sim_contacts(delta_sim *s, const delta_contacts *out, int64_t *n_out) {
@@ -1325,6 +1373,7 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
   s->counters[3] += cnt[1];
   if (nc > s->c.capacity && (ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;
   if ((ds = copy_contacts(g.c, s->c, nc, g.stream)) != DELTA_OK) return ds;
+  if ((ds = sim_all_vertices(s, g.stream)) != DELTA_OK) return ds;
   if ((e = cudaStreamSynchronize(g.stream)) != cudaSuccess) return cuda_error(e, "graph end");
   s->n_contacts = nc;
   return DELTA_OK;
@@ -1353,6 +1402,7 @@ delta_status delta_sim_destroy(delta_sim *s) {
   if (s->g.stream) cudaStreamDestroy(s->g.stream);
   s->plan.release();
   if (s->ids) cudaFree(s->ids);
+  if (s->stamp) cudaFree(s->stamp);
   if (s->F) cudaFree(s->F);
   if (s->c_mem) cudaFree(s->c_mem);
   if (s->pa) cudaFree(s->pa);
