@@ -263,33 +263,58 @@ __global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_
   val_idx[2 * g + 1] = 2 * g + 1;
 }
 
-// One thread per body: partners in ascending order (entries sorted by key).
-// Entries past the valid ones carry the key ~0 and sort last; they match no body.
+// Per-body sums over the sorted entries: the thread at the first entry of a body's run
+// adds the run's entries in key order, i.e. over ascending partners, starting from 0.0.
+// Bodies without entries keep the zeros written before the launch.  Entries past the
+// valid ones carry the key ~0 and sort last.
 __global__ void k_body_forces(int32_t n_bodies, int sh, const uint64_t *skey, const int64_t *sidx,
                               const double *entry, int64_t ne, double *force, double *torque, uint8_t *has) {
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_bodies) return;
-  const uint64_t lo_key = (uint64_t)(uint32_t)i << sh;
-  int64_t lo = 0, hi = ne;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (skey[mid] < lo_key) lo = mid + 1;
-    else hi = mid;
-  }
+  const int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e0 >= ne) return;
+  const uint64_t key = skey[e0];
+  if (key == ~0ull) return;
+  const uint64_t body = key >> sh;
+  if (e0 > 0 && (skey[e0 - 1] >> sh) == body) return;  // not the first entry of the run
+  const int64_t i = (int64_t)body;
   X F[3] = {X(0.0), X(0.0), X(0.0)}, T[3] = {X(0.0), X(0.0), X(0.0)};
-  int64_t e = lo;
-  for (; e < ne && (skey[e] >> sh) == (uint64_t)(uint32_t)i; ++e) {
-    const double *v = entry + sidx[e] * 6;
-    for (int k = 0; k < 3; ++k) {
-      F[k] += X(v[k]);
-      T[k] += X(v[3 + k]);
+  // run end, then the run in groups of 4 entries whose loads are issued together (a body
+  // such as a floor can have thousands of partners); the additions stay in entry order
+  int64_t e1 = e0 + 1;
+  while (e1 < ne && skey[e1] != ~0ull && (skey[e1] >> sh) == body) ++e1;
+  for (int64_t e = e0; e < e1; e += 4) {
+    double v[4][6];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (e + u < e1) {
+        const double *src = entry + sidx[e + u] * 6;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[u][k] = src[k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (e + u < e1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          F[k] += X(v[u][k]);
+          T[k] += X(v[u][3 + k]);
+        }
+      }
     }
   }
   for (int k = 0; k < 3; ++k) {
     force[(int64_t)k * n_bodies + i] = F[k].v;
     torque[(int64_t)k * n_bodies + i] = T[k].v;
   }
-  has[i] = e > lo ? 1 : 0;
+  has[i] = 1;
+}
+
+// zeroes the per-body sums (bodies without contacts keep these)
+inline cudaError_t zero_body_sums(cudaStream_t st, int32_t n, double *force, double *torque, uint8_t *has) {
+  cudaError_t e = cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)n, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(torque, 0, sizeof(double) * 3 * (size_t)n, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(has, 0, (size_t)n, st);
+  return e;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -615,7 +640,9 @@ delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contac
       cudaSuccess)
     return cuda_error(e, "entry sort");
   ctx->launches += 1;
-  k_body_forces<<<blocks_for(n), 256, 0, st>>>(n, sh, skey, sidx, entry, (int64_t)(2 * nc), force, torque, has);
+  if ((e = zero_body_sums(st, n, force, torque, has)) != cudaSuccess) return cuda_error(e, "forces memset");
+  k_body_forces<<<blocks_for((int64_t)(2 * nc)), 256, 0, st>>>(n, sh, skey, sidx, entry, (int64_t)(2 * nc), force,
+                                                               torque, has);
   ctx->launches += 1;
   return DELTA_OK;
 }
@@ -815,8 +842,8 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, 2 * cap, 0, 2 * sh,
                                            st)) != cudaSuccess)
     return cuda_error(e, "entry sort");
-  k_body_forces<<<blocks_for(s.n_bodies), 256, 0, st>>>(s.n_bodies, sh, skey, sidx, entry, 2 * cap, force, torque,
-                                                        has);
+  if ((e = zero_body_sums(st, s.n_bodies, force, torque, has)) != cudaSuccess) return cuda_error(e, "forces memset");
+  k_body_forces<<<blocks_for(2 * cap), 256, 0, st>>>(s.n_bodies, sh, skey, sidx, entry, 2 * cap, force, torque, has);
   kernels += 5;
   return cuda_error(cudaGetLastError(), "forces fixed");
 }
