@@ -290,3 +290,21 @@ def test_learned_host_pipeline_many_chunks(ctx, trained):
     assert nf == hnf > 0
     assert np.array_equal(d.cpu().numpy(), hd) and np.array_equal(fl.cpu().numpy(), hfl)
     assert np.array_equal(p.cpu().numpy(), hp) and np.array_equal(q.cpu().numpy(), hq)
+
+
+@pytest.mark.parametrize("shift,scale", [(1e4, 1.0), (-3e2, 1.0), (0.0, 1e-5), (5.0, 1e3)])
+def test_learned_solver_translated_and_scaled(ctx, oracle, pairs, shift, scale):
+    """Pairs moved far from the origin or scaled: the certificate's rounding slack grows
+    with the coordinates, so pairs it cannot certify go to the exact solver; every result
+    stays within 1e-6 of FP64 bfSolver on the same (moved) inputs, fallback bit-exact."""
+    from delta_b200.learned import learned_pairs
+
+    a = pairs[0][:, :20000] * scale + shift
+    b = pairs[1][:, :20000] * scale + shift
+    p, q, d, fl, nf = learned_pairs(ctx, None, _dev(a), _dev(b), sweeps=2, count_fallback=True, features=3)
+    d, fl = d.cpu().numpy(), fl.cpu().numpy()
+    _, _, od, _ = oracle.pairs(0, a, b)
+    fin = np.isfinite(od)
+    assert np.all(np.abs(d - od)[fin] <= 1e-6 * od[fin])
+    assert np.array_equal(d[fl == 2], od[fl == 2], equal_nan=True)
+    assert nf == int((fl == 2).sum())
