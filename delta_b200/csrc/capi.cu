@@ -64,11 +64,12 @@ delta_status host_pipeline(
   for (auto &ev : ctx->events)
     if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
       return cuda_error(e, "copy events");
-  // up to 8 chunks of at least 2^18 pairs; event 0 starts the H2D after the context's
-  // earlier work, 1+3k and 2+3k mark the end of chunk k's H2D and compute, the last one
-  // the end of the copies
+  // up to 15 chunks of at least 2^18 pairs (the first H2D and the last D2H are not
+  // overlapped, so more chunks leave less of them exposed); event 0 starts the H2D after
+  // the context's earlier work, 1+3k and 2+3k mark the end of chunk k's H2D and compute,
+  // the last one the end of the copies
   const int64_t min_chunk = 1 << 18;
-  int chunks = (int)std::min<int64_t>(8, std::max<int64_t>(1, n / min_chunk));
+  int chunks = (int)std::min<int64_t>(15, std::max<int64_t>(1, n / min_chunk));
   const int64_t chunk = (n + chunks - 1) / chunks;
   chunks = (int)((n + chunk - 1) / chunk);
   cudaEvent_t *ev = ctx->events;
