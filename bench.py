@@ -444,9 +444,23 @@ def main():
             host_run()
         barrier()
         (el,) = max_ranks([time.perf_counter() - t0])
+        # the PCIe bound: a plain pinned host-to-device copy of the A planes, after the run
+        dev_a = torch.empty(ha.shape, dtype=torch.float64, device="cuda")
+        src_a = torch.from_numpy(ha)
+        for _ in range(2):
+            dev_a.copy_(src_a, non_blocking=True)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(3):
+            dev_a.copy_(src_a, non_blocking=True)
+        torch.cuda.synchronize()
+        h2d_gbs = 3 * ha.nbytes / (time.perf_counter() - t1) / 1e9
+        del dev_a
         e2e = {"value": world * n * args.e2e_steps / el, "unit": "pairs/s",
                "h2d_bytes_per_step": int(ha.nbytes + hb.nbytes),
-               "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes), "path": path}
+               "d2h_bytes_per_step": int(hp.nbytes + hq.nbytes + hd.nbytes + hf.nbytes), "path": path,
+               "pinned_h2d_gbs": h2d_gbs,
+               "h2d_bound_pairs_per_s": world * h2d_gbs * 1e9 / ((ha.nbytes + hb.nbytes) / n)}
 
     ts = hop = box = None
     if args.timestep_steps > 0:
