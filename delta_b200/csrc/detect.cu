@@ -569,6 +569,20 @@ __global__ void k_accumulate(const DevStats *st, int64_t *counters) {
   counters[1] += (int64_t)st->evaluated;
 }
 
+// End of a fixed-capacity certified detection, one thread: the survivors count as
+// evaluated pairs (a survivor-list overflow raises *ovf), then the step's statistics go
+// to the running counters.
+__global__ void k_cert_tail(const unsigned long long *sv_count, int64_t sv_cap, DevStats *st, int *ovf,
+                            int64_t *counters) {
+  const unsigned long long c = *sv_count;
+  st->evaluated += c;
+  if (ovf && c > (unsigned long long)sv_cap) atomicCAS(ovf, 0, 1);
+  if (counters) {
+    counters[0] += (int64_t)st->tri_pairs;
+    counters[1] += (int64_t)st->evaluated;
+  }
+}
+
 __global__ void k_check_pairs(const int64_t *tri_offset, const int32_t *pb, int64_t n_pairs, int32_t n_bodies,
                               int *bad) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -840,6 +854,15 @@ size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap) {
          sizeof(int64_t) * 2 * (size_t)cap + 256 + sizeof(uint64_t) * (size_t)fixed_sv_cap(cap) + 256;
 }
 
+// Once per allocation of the fixed-capacity state: the contact sort's identity permutation.
+delta_status detect_fixed_init(cudaStream_t s, void *state, int64_t pair_cap, int64_t cap) {
+  char *p = (char *)state + 512 + sizeof(DevStats) + sizeof(int64_t) * (size_t)(2 * pair_cap + 2);
+  p += (14 * sizeof(double) + 4 * sizeof(int32_t) + 1 + 2 * sizeof(uint64_t)) * (size_t)cap;
+  p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+  k_iota<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>((int64_t *)p, cap);
+  return cuda_error(cudaGetLastError(), "detect fixed init");
+}
+
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
@@ -872,24 +895,25 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   rc.bbox = driver == DELTA_DRV_BF_CERT ? bbox : nullptr;  // the caller's boxes of the current vertices
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
   if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");
-  k_rows_fixed<<<(unsigned)((pair_cap + 256) / 256), 256, 0, s>>>(m.tri_offset, pa, pair_cap, rows);
   size_t tb = temp_bytes;
-  if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
-    return cuda_error(e, "row scan");
   if (driver == DELTA_DRV_BF_CERT) {
+    // the culling takes body pairs directly: no rows
     e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats);
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0)) != cudaSuccess)
       return cuda_error(e, "occupancy");
     k_cert_survivors<<<(unsigned)(kNumSMs * (per_sm > 0 ? per_sm : 1)), 128, 0, s>>>(m, pa, pb, rc, dstats);
-    k_sv_evaluated<<<1, 1, 0, s>>>(rc.sv_count, rc.sv_cap, dstats, d_ovf);
     ctx->launches += 2;
   } else {
+    k_rows_fixed<<<(unsigned)((pair_cap + 256) / 256), 256, 0, s>>>(m.tri_offset, pa, pair_cap, rows);
+    if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
+      return cuda_error(e, "row scan");
     e = launch_detect_t<xf64, DELTA_DRV_BF>(s, m, pa, pb, row_offset, pair_cap, -1, rc, dstats, queue);
+    ctx->launches += 3;
   }
   if (e != cudaSuccess) return cuda_error(e, "detect kernel");
-  k_iota<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(perm_in, cap);
+  // perm_in holds 0 .. cap-1 from detect_fixed_init (the sort does not modify its inputs)
   // keys (pair << 2 tri_bits | A tri << tri_bits | B tri) of pairs below pair_cap: the bits
   // above the pair index are zero (empty entries, ~0, still sort last: stable, and after
   // every valid key)
@@ -901,8 +925,14 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
     return cuda_error(e, "contact sort");
   k_gather_fixed<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, perm_out, out, d_ncontacts, d_ovf, ovf_code,
                                                                d_count_log);
-  if (d_counters) k_accumulate<<<1, 1, 0, s>>>(dstats, d_counters);
-  ctx->launches += d_counters ? 6 : 5;
+  ctx->launches += 2;
+  if (driver == DELTA_DRV_BF_CERT) {
+    k_cert_tail<<<1, 1, 0, s>>>(rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters);
+    ctx->launches += 1;
+  } else if (d_counters) {
+    k_accumulate<<<1, 1, 0, s>>>(dstats, d_counters);
+    ctx->launches += 1;
+  }
   return cuda_error(cudaGetLastError(), "detect fixed");
 }
 

@@ -50,6 +50,8 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
 // fewer than 2^tri_bits triangles), used to pack the contact sort keys.
 size_t detect_fixed_temp_bytes(int64_t pair_cap, int64_t cap);
 size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap);
+// Fills the identity permutation of a freshly allocated fixed-capacity state (once).
+delta_status detect_fixed_init(cudaStream_t s, void *state, int64_t pair_cap, int64_t cap);
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,

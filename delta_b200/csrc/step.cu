@@ -208,18 +208,6 @@ __global__ void k_segment_heads_fixed(ContactView cv, int64_t cap, const int64_t
   head[c] = c < n && (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]) ? 1 : 0;
 }
 
-// Flags a pair-list overflow; adds the step's candidate body pairs to *total (graph mode's
-// body-pair counter).
-__global__ void k_flag_overflow(const unsigned long long *count, int64_t cap, int *ovf, int64_t *total) {
-  if (*count > (unsigned long long)cap) atomicCAS(ovf, 0, 1);
-  if (total) *total += (int64_t)(*count < (unsigned long long)cap ? *count : (unsigned long long)cap);
-}
-
-__global__ void k_step_begin(const int *ovf, int *ovf_snap, uint32_t *epoch) {
-  *ovf_snap = *ovf;
-  *epoch += 1u;  // the vertex stamps of this step (k_mark_pair_bodies)
-}
-
 __global__ void k_step_end(const int *ovf_snap, const int64_t *n_contacts, int64_t *log, int64_t log_len,
                            int64_t *step) {
   if (*ovf_snap) return;
@@ -311,6 +299,8 @@ __global__ void k_body_forces(int32_t n_bodies, int sh, const uint64_t *skey, co
 
 // zeroes the per-body sums (bodies without contacts keep these)
 inline cudaError_t zero_body_sums(cudaStream_t st, int32_t n, double *force, double *torque, uint8_t *has) {
+  if (torque == force + 3 * (size_t)n && has == reinterpret_cast<uint8_t *>(torque + 3 * (size_t)n))
+    return cudaMemsetAsync(force, 0, sizeof(double) * 6 * (size_t)n + (size_t)n, st);  // one buffer
   cudaError_t e = cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)n, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(torque, 0, sizeof(double) * 3 * (size_t)n, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(has, 0, (size_t)n, st);
@@ -323,9 +313,15 @@ inline cudaError_t zero_body_sums(cudaStream_t st, int32_t n, double *force, dou
 
 // Collision::touchVertexFirstTime velocity part (Collision.cpp:1105-1115) followed by
 // MoveParticles::moveAllParticlesAssociatedToVertex body part (MoveParticles.cpp:71-94).
+// With ovf_snap (graph mode) the first thread also opens the step: it snapshots the
+// overflow flag and advances the vertex-stamp epoch.
 __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force, const double *torque,
-                         const uint8_t *has, const int *ovf) {
+                         const uint8_t *has, const int *ovf, int *ovf_snap, uint32_t *epoch) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ovf_snap && i == 0) {
+    *ovf_snap = *ovf;
+    *epoch += 1u;
+  }
   if (i >= s.n_bodies || s.obstacle[i]) return;
   if (ovf && *ovf) return;  // graph mode: a capacity overflow froze the state
   const BodyRef b{s.n_bodies, i};
@@ -564,9 +560,17 @@ __global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const doubl
   if (d2 <= reach * reach) push_pair(L, j, sh, out, count, cap);
 }
 
-// pair keys back to (a, b); the empty key ~0 gives (-1, -1)
-__global__ void k_unpack_pairs(const uint64_t *k, int64_t n, int sh, int32_t *a, int32_t *b) {
+// pair keys back to (a, b); the empty key ~0 gives (-1, -1).  With `count` (fixed
+// capacity n), thread 0 also flags an overflow of the n entries and adds the step's
+// candidate body pairs to *total.
+__global__ void k_unpack_pairs(const uint64_t *k, int64_t n, int sh, int32_t *a, int32_t *b,
+                               const unsigned long long *count, int *ovf, int64_t *total) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (count && t == 0) {
+    const unsigned long long c = *count;
+    if (c > (unsigned long long)n) atomicCAS(ovf, 0, 1);
+    if (total) *total += (int64_t)(c < (unsigned long long)n ? c : (unsigned long long)n);
+  }
   if (t >= n) return;
   const uint64_t v = k[t];
   const bool empty = v == ~0ull;
@@ -650,7 +654,7 @@ delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contac
 delta_status integrate_run(delta_ctx *ctx, const delta_scene &s, const delta_step_params &p, const double *force,
                            const double *torque, const uint8_t *has, int64_t n_vertices) {
   cudaStream_t st = ctx->stream;
-  k_bodies<<<blocks_for(s.n_bodies, 128), 128, 0, st>>>(s, p, force, torque, has, nullptr);
+  k_bodies<<<blocks_for(s.n_bodies, 128), 128, 0, st>>>(s, p, force, torque, has, nullptr, nullptr, nullptr);
   (void)n_vertices;
   k_vertices<<<vertex_blocks(s.n_bodies), 256, 0, st>>>(s, nullptr, nullptr, nullptr, nullptr);
   ctx->launches += 2;
@@ -794,7 +798,7 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   ctx->launches += 1;
   const int64_t wn = np < capacity ? np : capacity;
   if (wn > 0) {
-    k_unpack_pairs<<<blocks_for(wn), 256, 0, st>>>(spk, wn, sh, pair_a, pair_b);
+    k_unpack_pairs<<<blocks_for(wn), 256, 0, st>>>(spk, wn, sh, pair_a, pair_b, nullptr, nullptr, nullptr);
     ctx->launches += 1;
   }
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "broadphase");
@@ -896,9 +900,8 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
   tb = temp_bytes;
   if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, pair_cap, 0, 2 * sh, st)) != cudaSuccess)
     return cuda_error(e, "pair sort");
-  k_unpack_pairs<<<blocks_for(pair_cap), 256, 0, st>>>(spk, pair_cap, sh, pair_a, pair_b);
-  k_flag_overflow<<<1, 1, 0, st>>>(count, pair_cap, ovf, pairs_total);
-  kernels += 3;
+  k_unpack_pairs<<<blocks_for(pair_cap), 256, 0, st>>>(spk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
+  kernels += 2;
   return cuda_error(cudaGetLastError(), "broadphase fixed");
 }
 
@@ -1092,6 +1095,9 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
   g.d_bp = (int64_t *)(v + 40);
   g.d_log = (int64_t *)(v + 256);
   if ((e = cudaMemset(g.dev, 0, 256)) != cudaSuccess) return cuda_error(e, "graph memset");
+  delta_status ds = detect_fixed_init(s->ctx->stream, g.ds, pair_cap, contact_cap);
+  if (ds != DELTA_OK) return ds;
+  if ((e = cudaStreamSynchronize(s->ctx->stream)) != cudaSuccess) return cuda_error(e, "graph init");
   return DELTA_OK;
 }
 
@@ -1100,10 +1106,10 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   delta_sim::Graph &g = s->g;
   cudaStream_t st = g.stream;
   int k = 0;
-  k_step_begin<<<1, 1, 0, st>>>(g.d_ovf, g.d_snap, s->epoch);
   delta_status ds = forces_run_fixed(st, s->scene, g.c, g.d_nc, p, s->F, s->T, s->has, g.fs, g.temp, g.temp_bytes, k);
   if (ds != DELTA_OK) return ds;
-  k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf);
+  k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf, g.d_snap,
+                                                               s->epoch);
   if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_bp, g.bp, g.temp,
                                  g.temp_bytes, k)) != DELTA_OK)
     return ds;
@@ -1120,7 +1126,7 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   k += (int)(s->ctx->launches - before);
   s->ctx->launches = before;
   k_step_end<<<1, 1, 0, st>>>(g.d_snap, g.d_nc, g.d_log, g.log_len, g.d_step);
-  g.kernels = k + 5;
+  g.kernels = k + 4;
   return cuda_error(cudaGetLastError(), "graph step");
 }
 
@@ -1255,7 +1261,7 @@ delta_status delta_sim_step(delta_sim *s, const delta_step_params *params, int32
     delta_status ds = forces_run(s->ctx, s->scene, s->c, s->n_contacts, *params, s->F, s->T, s->has);
     if (ds != DELTA_OK) return ds;
     k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, s->ctx->stream>>>(s->scene, *params, s->F, s->T, s->has,
-                                                                              nullptr);
+                                                                              nullptr, nullptr, nullptr);
     s->ctx->launches += 1;
     if ((ds = sim_detect(s)) != DELTA_OK) return ds;
     s->counters[0] += 1;
