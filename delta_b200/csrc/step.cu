@@ -201,13 +201,6 @@ __device__ void pair_forces(const delta_scene &s, const ContactView &cv, int64_t
   }
 }
 
-__global__ void k_segment_heads_fixed(ContactView cv, int64_t cap, const int64_t *n_d, uint8_t *head) {
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cap) return;
-  const int64_t n = *n_d < cap ? *n_d : cap;
-  head[c] = c < n && (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]) ? 1 : 0;
-}
-
 __global__ void k_step_end(const int *ovf_snap, const int64_t *n_contacts, int64_t *log, int64_t log_len,
                            int64_t *step) {
   if (*ovf_snap) return;
@@ -249,6 +242,40 @@ __global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_
   key[2 * g + 1] = ((uint64_t)(uint32_t)j << sh) | (uint32_t)i;
   val_idx[2 * g] = 2 * g;
   val_idx[2 * g + 1] = 2 * g + 1;
+}
+
+// Fixed-capacity variant, one thread per contact slot c < cap: the thread at the first
+// contact of a (master, slave) segment sums the segment (same sums as k_pair_forces) into
+// entries 2c and 2c+1; every other slot writes the empty key ~0, which sorts last.
+__global__ void k_pair_forces_heads(delta_scene s, ContactView cv, const int64_t *n_contacts_d,
+                                    delta_step_params p, int sh, uint64_t *key, int64_t *val_idx, double *entry) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cv.cap) return;
+  const int64_t n = *n_contacts_d < cv.cap ? *n_contacts_d : cv.cap;
+  val_idx[2 * c] = 2 * c;
+  val_idx[2 * c + 1] = 2 * c + 1;
+  const bool head = c < n && (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]);
+  if (!head) {
+    key[2 * c] = ~0ull;
+    key[2 * c + 1] = ~0ull;
+    return;
+  }
+  const int32_t i = cv.master[c], j = cv.slave[c];
+  int64_t c1 = c + 1;
+  while (c1 < n && cv.master[c1] == i && cv.slave[c1] == j) ++c1;
+  X F[3], T[3];
+  pair_forces(s, cv, c, c1, i, j, false, p, F, T);
+  for (int k = 0; k < 3; ++k) {
+    entry[(2 * c) * 6 + k] = F[k].v;
+    entry[(2 * c) * 6 + 3 + k] = T[k].v;
+  }
+  pair_forces(s, cv, c, c1, j, i, true, p, F, T);
+  for (int k = 0; k < 3; ++k) {
+    entry[(2 * c + 1) * 6 + k] = F[k].v;
+    entry[(2 * c + 1) * 6 + 3 + k] = T[k].v;
+  }
+  key[2 * c] = ((uint64_t)(uint32_t)i << sh) | (uint32_t)j;
+  key[2 * c + 1] = ((uint64_t)(uint32_t)j << sh) | (uint32_t)i;
 }
 
 // Per-body sums over the sorted entries: the thread at the first entry of a body's run
@@ -481,8 +508,15 @@ __device__ __forceinline__ void cell_of(const delta_scene &s, const Grid &g, int
   for (int k = 0; k < 3; ++k) c[k] = (int64_t)floor((s.pos[(int64_t)k * s.n_bodies + i] - g.origin[k]) / g.h);
 }
 
-__global__ void k_cell_keys(delta_scene s, Grid g, uint64_t *key, int32_t *body) {
+// With `pk` (fixed capacity), the grid's threads also empty the pair-key list (pk_cap
+// entries of ~0) and zero its counter before the pair search fills them.
+__global__ void k_cell_keys(delta_scene s, Grid g, uint64_t *key, int32_t *body, uint64_t *pk, int64_t pk_cap,
+                            unsigned long long *count) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pk) {
+    for (int64_t t = i; t < pk_cap; t += (int64_t)gridDim.x * blockDim.x) pk[t] = ~0ull;
+    if (i == 0) *count = 0ull;
+  }
   if (i >= s.n_bodies) return;
   int64_t c[3];
   cell_of(s, g, i, c);
@@ -752,7 +786,7 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
     return ds;
   uint64_t *key = (uint64_t *)kb, *skey = key + n;
   int32_t *body = (int32_t *)(skey + n), *sbody = body + n;
-  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body);
+  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body, nullptr, 0, nullptr);
   ctx->launches += 1;
   size_t tb = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st);
@@ -808,15 +842,13 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
 
 
 // Forces from a fixed-capacity contact buffer with its count on the device.
-size_t forces_fixed_state_bytes(int64_t cap) { return (size_t)cap * (1 + 8 + 16 * 4 + 96) + 512; }
+size_t forces_fixed_state_bytes(int64_t cap) { return (size_t)cap * (16 * 4 + 96) + 512; }
 
 size_t forces_fixed_temp_bytes(int64_t cap, int32_t n_bodies) {
-  size_t a = 0, b = 0;
-  cub::CountingInputIterator<int64_t> it(0);
-  cub::DeviceSelect::Flagged(nullptr, a, it, (uint8_t *)nullptr, (int64_t *)nullptr, (int64_t *)nullptr, cap);
+  size_t b = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, (int64_t *)nullptr,
                                   (int64_t *)nullptr, 2 * cap, 0, 2 * bits_for(n_bodies));
-  return a > b ? a : b;
+  return b;
 }
 
 delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta_contacts &c, const int64_t *d_nc,
@@ -825,30 +857,21 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   cudaError_t e;
   const int64_t cap = c.capacity;
   ContactView cv{c.x, c.normal, c.depth, c.master, c.slave, c.friction, cap};
-  char *b = (char *)state;
-  int64_t *n_seg = (int64_t *)b; b += 512;
-  int64_t *seg_start = (int64_t *)b; b += 8 * cap;
+  char *b = (char *)state + 512;
   uint64_t *key = (uint64_t *)b; b += 16 * cap;
   uint64_t *skey = (uint64_t *)b; b += 16 * cap;
   int64_t *idx = (int64_t *)b; b += 16 * cap;
   int64_t *sidx = (int64_t *)b; b += 16 * cap;
-  double *entry = (double *)b; b += 96 * cap;
-  uint8_t *head = (uint8_t *)b;
-  k_segment_heads_fixed<<<blocks_for(cap), 256, 0, st>>>(cv, cap, d_nc, head);
-  size_t tb = temp_bytes;
-  cub::CountingInputIterator<int64_t> it(0);
-  if ((e = cub::DeviceSelect::Flagged(temp, tb, it, head, seg_start, n_seg, cap, st)) != cudaSuccess)
-    return cuda_error(e, "segment select");
-  if ((e = cudaMemsetAsync(key, 0xff, sizeof(uint64_t) * 2 * cap, st)) != cudaSuccess) return cuda_error(e, "memset");
+  double *entry = (double *)b;
   const int sh = bits_for(s.n_bodies);
-  k_pair_forces<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, 0, d_nc, p, sh, key, idx, entry);
-  tb = temp_bytes;
+  k_pair_forces_heads<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, d_nc, p, sh, key, idx, entry);
+  size_t tb = temp_bytes;
   if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, 2 * cap, 0, 2 * sh,
                                            st)) != cudaSuccess)
     return cuda_error(e, "entry sort");
   if ((e = zero_body_sums(st, s.n_bodies, force, torque, has)) != cudaSuccess) return cuda_error(e, "forces memset");
   k_body_forces<<<blocks_for(2 * cap), 256, 0, st>>>(s.n_bodies, sh, skey, sidx, entry, 2 * cap, force, torque, has);
-  kernels += 5;
+  kernels += 3;
   return cuda_error(cudaGetLastError(), "forces fixed");
 }
 
@@ -879,13 +902,10 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
   b = (char *)(((uintptr_t)b + 255) & ~(uintptr_t)255);
   unsigned long long *count = (unsigned long long *)b;
   uint64_t *pk = (uint64_t *)(b + 256), *spk = pk + pair_cap;
-  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body);
+  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body, pk, pair_cap, count);
   size_t tb = temp_bytes;
   if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st)) != cudaSuccess)
     return cuda_error(e, "cell sort");
-  if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess ||
-      (e = cudaMemsetAsync(pk, 0xff, sizeof(uint64_t) * pair_cap, st)) != cudaSuccess)
-    return cuda_error(e, "memset");
   kernels += 2;
   if (plan.n_moving > 0) {
     k_grid_pairs<<<blocks_for(9 * (int64_t)plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, sh, pk, count,
