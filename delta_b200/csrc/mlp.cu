@@ -586,8 +586,8 @@ constexpr int kTcThreads = 2 * kTcRows;
 __global__ void __launch_bounds__(kTcThreads, 2)
     k_mlp_infer_tc(int64_t n, const __nv_bfloat16 *__restrict__ feat, const float *__restrict__ params,
                    const __nv_bfloat16 *__restrict__ wb, float *__restrict__ x0, int *__restrict__ err) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
+  extern __shared__ __align__(128) unsigned char tc_smem_raw[];
+  TcSmem &sm = *reinterpret_cast<TcSmem *>(tc_smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
   tc_stage(sm.w1, wb + kOffW1, kHid, kHid, kIn);
   tc_stage(sm.w2, wb + kOffW2, kHid, kHid, kHid);
