@@ -244,38 +244,98 @@ __global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_
   val_idx[2 * g + 1] = 2 * g + 1;
 }
 
-// Fixed-capacity variant, one thread per contact slot c < cap: the thread at the first
-// contact of a (master, slave) segment sums the segment (same sums as k_pair_forces) into
-// entries 2c and 2c+1; every other slot writes the empty key ~0, which sorts last.
+// Fixed-capacity force pass, one thread per contact slot: the thread at the first contact
+// of a (master, slave) segment sums the segment (the sums of k_pair_forces) into entry 2c
+// (on the master) and 2c+1 (on the slave) and counts the segment in its slave's list.
+// Sums on obstacles are not formed: nothing reads them.
 __global__ void k_pair_forces_heads(delta_scene s, ContactView cv, const int64_t *n_contacts_d,
-                                    delta_step_params p, int sh, uint64_t *key, int64_t *val_idx, double *entry) {
+                                    delta_step_params p, double *entry, uint32_t *slave_count) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cv.cap) return;
   const int64_t n = *n_contacts_d < cv.cap ? *n_contacts_d : cv.cap;
-  val_idx[2 * c] = 2 * c;
-  val_idx[2 * c + 1] = 2 * c + 1;
-  const bool head = c < n && (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]);
-  if (!head) {
-    key[2 * c] = ~0ull;
-    key[2 * c + 1] = ~0ull;
-    return;
-  }
+  if (c >= n) return;
+  if (c > 0 && cv.master[c] == cv.master[c - 1] && cv.slave[c] == cv.slave[c - 1]) return;
   const int32_t i = cv.master[c], j = cv.slave[c];
   int64_t c1 = c + 1;
   while (c1 < n && cv.master[c1] == i && cv.slave[c1] == j) ++c1;
   X F[3], T[3];
-  pair_forces(s, cv, c, c1, i, j, false, p, F, T);
-  for (int k = 0; k < 3; ++k) {
-    entry[(2 * c) * 6 + k] = F[k].v;
-    entry[(2 * c) * 6 + 3 + k] = T[k].v;
+  if (!s.obstacle[i]) {
+    pair_forces(s, cv, c, c1, i, j, false, p, F, T);
+    for (int k = 0; k < 3; ++k) {
+      entry[(2 * c) * 6 + k] = F[k].v;
+      entry[(2 * c) * 6 + 3 + k] = T[k].v;
+    }
   }
-  pair_forces(s, cv, c, c1, j, i, true, p, F, T);
-  for (int k = 0; k < 3; ++k) {
-    entry[(2 * c + 1) * 6 + k] = F[k].v;
-    entry[(2 * c + 1) * 6 + 3 + k] = T[k].v;
+  if (!s.obstacle[j]) {
+    pair_forces(s, cv, c, c1, j, i, true, p, F, T);
+    for (int k = 0; k < 3; ++k) {
+      entry[(2 * c + 1) * 6 + k] = F[k].v;
+      entry[(2 * c + 1) * 6 + 3 + k] = T[k].v;
+    }
+    atomicAdd(&slave_count[j], 1u);
   }
-  key[2 * c] = ((uint64_t)(uint32_t)i << sh) | (uint32_t)j;
-  key[2 * c + 1] = ((uint64_t)(uint32_t)j << sh) | (uint32_t)i;
+}
+
+// Each segment head c into its slave's list, at any position of the slave's range (the
+// sum kernel orders the range).
+__global__ void k_fill_slave_lists(delta_scene s, ContactView cv, const int64_t *n_contacts_d, const uint32_t *start,
+                                   uint32_t *fill, int32_t *list) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n = *n_contacts_d < cv.cap ? *n_contacts_d : cv.cap;
+  if (c >= n) return;
+  if (c > 0 && cv.master[c] == cv.master[c - 1] && cv.slave[c] == cv.slave[c - 1]) return;
+  const int32_t j = cv.slave[c];
+  if (s.obstacle[j]) return;
+  list[start[j] + atomicAdd(&fill[j], 1u)] = (int32_t)c;
+}
+
+// Per-body sums over ascending partners, one thread per body.  The pair list is ordered
+// (min, max), so a body's partners below it are the masters of the segments in which it is
+// the slave, and those above it the slaves of the segments in which it is the master.
+// The first come from the body's list, sorted by segment position (which orders them by
+// master); the second are the body's run of contacts as master, in contact order.  From
+// 0.0, these are the additions of the sorted-entry sums (k_body_forces), in that order.
+__global__ void k_body_forces_lists(delta_scene s, ContactView cv, const int64_t *n_contacts_d, const uint32_t *start,
+                                    int32_t *list, const double *entry, double *force, double *torque,
+                                    uint8_t *has) {
+  const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t nb = s.n_bodies;
+  if (b >= nb) return;
+  X F[3] = {X(0.0), X(0.0), X(0.0)}, T[3] = {X(0.0), X(0.0), X(0.0)};
+  bool any = false;
+  auto add = [&](const double *v) {
+    for (int k = 0; k < 3; ++k) {
+      F[k] += X(v[k]);
+      T[k] += X(v[3 + k]);
+    }
+    any = true;
+  };
+  if (!s.obstacle[b]) {
+    const uint32_t l0 = start[b], l1 = start[b + 1];
+    for (uint32_t u = l0 + 1; u < l1; ++u) {  // insertion sort of this body's short list
+      const int32_t v = list[u];
+      uint32_t w = u;
+      while (w > l0 && list[w - 1] > v) {
+        list[w] = list[w - 1];
+        --w;
+      }
+      list[w] = v;
+    }
+    for (uint32_t u = l0; u < l1; ++u) add(entry + (2 * (int64_t)list[u] + 1) * 6);
+    const int64_t n = *n_contacts_d < cv.cap ? *n_contacts_d : cv.cap;
+    int64_t lo = 0, hi = n;  // first contact with master >= b (masters ascend)
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (cv.master[mid] < b) lo = mid + 1;
+      else hi = mid;
+    }
+    for (int64_t c = lo; c < n && cv.master[c] == b; ++c)
+      if (c == lo || cv.slave[c] != cv.slave[c - 1]) add(entry + (2 * c) * 6);
+  }
+  for (int k = 0; k < 3; ++k) {
+    force[(int64_t)k * nb + b] = F[k].v;
+    torque[(int64_t)k * nb + b] = T[k].v;
+  }
+  has[b] = any ? 1 : 0;
 }
 
 // Per-body sums over the sorted entries: the thread at the first entry of a body's run
@@ -842,12 +902,14 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
 
 
 // Forces from a fixed-capacity contact buffer with its count on the device.
-size_t forces_fixed_state_bytes(int64_t cap) { return (size_t)cap * (16 * 4 + 96) + 512; }
+size_t forces_fixed_state_bytes(int64_t cap, int32_t n_bodies) {
+  return 4 * 256 + 96 * (size_t)cap + 4 * (size_t)cap + 4 * (2 * (size_t)n_bodies + 1) + 4 * ((size_t)n_bodies + 1);
+}
 
 size_t forces_fixed_temp_bytes(int64_t cap, int32_t n_bodies) {
+  (void)cap;
   size_t b = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, (int64_t *)nullptr,
-                                  (int64_t *)nullptr, 2 * cap, 0, 2 * bits_for(n_bodies));
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t *)nullptr, (uint32_t *)nullptr, (int64_t)n_bodies + 1);
   return b;
 }
 
@@ -856,22 +918,25 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
                               void *temp, size_t temp_bytes, int &kernels) {
   cudaError_t e;
   const int64_t cap = c.capacity;
+  const int32_t n = s.n_bodies;
   ContactView cv{c.x, c.normal, c.depth, c.master, c.slave, c.friction, cap};
-  char *b = (char *)state + 512;
-  uint64_t *key = (uint64_t *)b; b += 16 * cap;
-  uint64_t *skey = (uint64_t *)b; b += 16 * cap;
-  int64_t *idx = (int64_t *)b; b += 16 * cap;
-  int64_t *sidx = (int64_t *)b; b += 16 * cap;
+  auto align = [](char *q) { return (char *)(((uintptr_t)q + 255) & ~(uintptr_t)255); };
+  char *b = align((char *)state);
   double *entry = (double *)b;
-  const int sh = bits_for(s.n_bodies);
-  k_pair_forces_heads<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, d_nc, p, sh, key, idx, entry);
+  b = align(b + 96 * (size_t)cap);
+  int32_t *list = (int32_t *)b;
+  b = align(b + 4 * (size_t)cap);
+  uint32_t *cnt = (uint32_t *)b, *fill = cnt + n + 1;  // zeroed together
+  b = align(b + 4 * (2 * (size_t)n + 1));
+  uint32_t *start = (uint32_t *)b;
+  if ((e = cudaMemsetAsync(cnt, 0, 4 * (2 * (size_t)n + 1), st)) != cudaSuccess) return cuda_error(e, "forces memset");
+  k_pair_forces_heads<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, d_nc, p, entry, cnt);
   size_t tb = temp_bytes;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, idx, sidx, 2 * cap, 0, 2 * sh,
-                                           st)) != cudaSuccess)
-    return cuda_error(e, "entry sort");
-  if ((e = zero_body_sums(st, s.n_bodies, force, torque, has)) != cudaSuccess) return cuda_error(e, "forces memset");
-  k_body_forces<<<blocks_for(2 * cap), 256, 0, st>>>(s.n_bodies, sh, skey, sidx, entry, 2 * cap, force, torque, has);
-  kernels += 3;
+  if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, cnt, start, n + 1, st)) != cudaSuccess)
+    return cuda_error(e, "slave list scan");
+  k_fill_slave_lists<<<blocks_for(cap), 256, 0, st>>>(s, cv, d_nc, start, fill, list);
+  k_body_forces_lists<<<blocks_for(n), 256, 0, st>>>(s, cv, d_nc, start, list, entry, force, torque, has);
+  kernels += 4;
   return cuda_error(cudaGetLastError(), "forces fixed");
 }
 
@@ -1093,7 +1158,7 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
   const size_t cbytes = (14 * sizeof(double) + 5 * sizeof(int32_t) + 1) * (size_t)contact_cap + 256;
   if ((e = cudaMalloc(&g.pa, sizeof(int32_t) * 2 * (size_t)pair_cap)) != cudaSuccess ||
       (e = cudaMalloc(&g.bp, broadphase_fixed_state_bytes(n, pair_cap))) != cudaSuccess ||
-      (e = cudaMalloc(&g.fs, forces_fixed_state_bytes(contact_cap))) != cudaSuccess ||
+      (e = cudaMalloc(&g.fs, forces_fixed_state_bytes(contact_cap, n))) != cudaSuccess ||
       (e = cudaMalloc(&g.ds, detect_fixed_state_bytes(pair_cap, contact_cap))) != cudaSuccess ||
       (e = cudaMalloc(&g.temp, g.temp_bytes)) != cudaSuccess || (e = cudaMalloc(&g.c_mem, cbytes)) != cudaSuccess ||
       (e = cudaMalloc(&g.dev, 256 + sizeof(int64_t) * (size_t)log_len)) != cudaSuccess ||
