@@ -10,7 +10,7 @@ FP64 bfSolver closest points (bf.cpp:217-1178) of the same pairs.
 The learned solver (`learned_pairs`) starts from the prediction, identifies the
 closest features, evaluates them in FP64 with the reference arithmetic, certifies the
 distance with a separating plane, and sends every uncertified pair to DELTA_BF_CERT,
-which is exact; the brute force is both the fallback and the error judge.  There is no
+which is exact; the brute force is both the fallback and the reference for the error.  There is no
 counterpart of this module in the reference.
 """
 from __future__ import annotations

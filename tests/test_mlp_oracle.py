@@ -1,5 +1,5 @@
 """The learned warm start's CPU oracle (no GPU): its calculus, its rounding and its
-features, checked before it is used to judge the CUDA kernels."""
+features, checked before it is used to check the CUDA kernels."""
 import numpy as np
 import pytest
 
