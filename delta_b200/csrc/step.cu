@@ -548,19 +548,36 @@ struct Grid {
   double origin[3];
 };
 
-// Cell keys take each cell coordinate modulo 2^kCellBits.  Cells that far apart share a
-// key, so their bodies become extra candidates that spheres_touch rejects, but the 27
-// neighbours of a cell always have distinct keys, so no pair is missed.  Obstacles get
-// kObstacleKey, above every cell key, and sort after the moving bodies; the cell sort
-// runs over kCellKeyBits bits.
-constexpr int kCellBits = 10;
+// Hash grid of the moving bodies.  A cell is keyed by its coordinates modulo 2^21
+// (cells that far apart share a key; their bodies become extra candidates that
+// spheres_touch rejects) and lives in bucket hash(key) & (nb - 1), nb a power of two.
+// Buckets list their bodies in any order: the candidate pairs are sorted afterwards.
+constexpr int kCellBits = 21;
 constexpr int64_t kCellMask = (1 << kCellBits) - 1;
-constexpr uint64_t kObstacleKey = 1ull << (3 * kCellBits);
-constexpr int kCellKeyBits = 3 * kCellBits + 1;
 
 __device__ __forceinline__ uint64_t cell_key(int64_t cx, int64_t cy, int64_t cz) {
   return ((uint64_t)(cx & kCellMask) << (2 * kCellBits)) | ((uint64_t)(cy & kCellMask) << kCellBits) |
          (uint64_t)(cz & kCellMask);
+}
+
+__device__ __forceinline__ uint32_t cell_bucket(uint64_t key, int64_t nb) {
+  uint64_t h = key * 0x9E3779B97F4A7C15ull;  // multiplicative hashing (Knuth), high bits
+  return (uint32_t)(h >> 32) & (uint32_t)(nb - 1);
+}
+
+struct HashGrid {
+  int64_t nb;        // buckets, a power of two
+  uint32_t *count;   // [nb + 1], zero before the count pass (count[nb] stays 0)
+  uint32_t *fill;    // [nb], zero before the fill pass
+  uint32_t *start;   // [nb + 1], exclusive sum of count
+  int32_t *bodies;   // [n] bodies by bucket
+  uint64_t *cell;    // [n] cell key of each moving body
+};
+
+inline int64_t grid_buckets(int32_t n) {
+  int64_t nb = 1024;
+  while (nb < (int64_t)n) nb <<= 1;
+  return nb;
 }
 
 __device__ __forceinline__ void cell_of(const delta_scene &s, const Grid &g, int32_t i, int64_t c[3]) {
@@ -568,20 +585,30 @@ __device__ __forceinline__ void cell_of(const delta_scene &s, const Grid &g, int
   for (int k = 0; k < 3; ++k) c[k] = (int64_t)floor((s.pos[(int64_t)k * s.n_bodies + i] - g.origin[k]) / g.h);
 }
 
-// With `pk` (fixed capacity), the grid's threads also empty the pair-key list (pk_cap
-// entries of ~0) and zero its counter before the pair search fills them.
-__global__ void k_cell_keys(delta_scene s, Grid g, uint64_t *key, int32_t *body, uint64_t *pk, int64_t pk_cap,
-                            unsigned long long *count) {
+// Count pass: each moving body's cell key and bucket count.  With `pk` (fixed
+// capacity), the grid's threads also empty the pair-key list (pk_cap entries of ~0) and
+// zero its counter before the pair search fills them.
+__global__ void k_grid_count(delta_scene s, Grid g, HashGrid hg, uint64_t *pk, int64_t pk_cap,
+                             unsigned long long *count) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (pk) {
     for (int64_t t = i; t < pk_cap; t += (int64_t)gridDim.x * blockDim.x) pk[t] = ~0ull;
     if (i == 0) *count = 0ull;
   }
-  if (i >= s.n_bodies) return;
+  if (i >= s.n_bodies || s.obstacle[i]) return;
   int64_t c[3];
   cell_of(s, g, i, c);
-  key[i] = s.obstacle[i] ? kObstacleKey : cell_key(c[0], c[1], c[2]);
-  body[i] = i;
+  const uint64_t key = cell_key(c[0], c[1], c[2]);
+  hg.cell[i] = key;
+  atomicAdd(&hg.count[cell_bucket(key, hg.nb)], 1u);
+}
+
+// Fill pass: each moving body into its bucket.
+__global__ void k_grid_fill(delta_scene s, HashGrid hg) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_bodies || s.obstacle[i]) return;
+  const uint32_t b = cell_bucket(hg.cell[i], hg.nb);
+  hg.bodies[hg.start[b] + atomicAdd(&hg.fill[b], 1u)] = i;
 }
 
 __device__ __forceinline__ bool spheres_touch(const delta_scene &s, int32_t i, int32_t j) {
@@ -603,34 +630,25 @@ __device__ __forceinline__ void push_pair(int32_t a, int32_t b, int sh, uint64_t
   if ((int64_t)pos < cap) out[pos] = ((uint64_t)(uint32_t)(a < b ? a : b) << sh) | (uint32_t)(a < b ? b : a);
 }
 
-// One thread per (moving body, cell column (dx, dy)): the cells (cx+dx, cy+dy, cz-1 ..
-// cz+1) have consecutive keys (two runs when the z coordinate wraps), so one binary search
-// per run finds the column's bodies in the sorted keys.  Every body has one key and the
-// 27 neighbour cells have distinct keys, so each candidate is met once; pairs are pushed
-// for j > i.
-__global__ void k_grid_pairs(delta_scene s, Grid g, const uint64_t *skey, const int32_t *sbody, int32_t n_moving,
-                             int sh, uint64_t *out, unsigned long long *count, int64_t cap) {
+// One thread per (body, cell column (dx, dy)): the three cells (cx+dx, cy+dy, cz-1 ..
+// cz+1) are looked up in their buckets, and a body of a bucket counts only when its cell
+// key is the cell's.  The 27 neighbour cells have distinct keys and every body one key, so
+// each candidate is met once; pairs are pushed for j > i.
+__global__ void k_grid_pairs(delta_scene s, Grid g, HashGrid hg, int sh, uint64_t *out, unsigned long long *count,
+                             int64_t cap) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 9 * (int64_t)n_moving) return;
-  const int32_t p = (int32_t)(t / 9), col = (int32_t)(t % 9);
-  const int32_t i = sbody[p];
+  if (t >= 9 * (int64_t)s.n_bodies) return;
+  const int32_t i = (int32_t)(t / 9), col = (int32_t)(t % 9);
+  if (s.obstacle[i]) return;
   int64_t c[3];
   cell_of(s, g, i, c);
   const int64_t cx = c[0] + col / 3 - 1, cy = c[1] + col % 3 - 1;
-  const int64_t z0 = (c[2] - 1) & kCellMask, z1 = (c[2] + 1) & kCellMask;
-  const int runs = z0 <= z1 ? 1 : 2;
-  for (int r = 0; r < runs; ++r) {
-    const uint64_t k0 = cell_key(cx, cy, r == 0 ? z0 : 0);
-    const uint64_t k1 = cell_key(cx, cy, runs == 1 || r == 1 ? z1 : kCellMask);
-    int32_t lo = 0, hi = n_moving;
-    while (lo < hi) {
-      const int32_t mid = (lo + hi) >> 1;
-      if (skey[mid] < k0) lo = mid + 1;
-      else hi = mid;
-    }
-    for (int32_t q = lo; q < n_moving && skey[q] <= k1; ++q) {
-      const int32_t j = sbody[q];
-      if (j > i && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
+  for (int dz = -1; dz <= 1; ++dz) {
+    const uint64_t key = cell_key(cx, cy, c[2] + dz);
+    const uint32_t b = cell_bucket(key, hg.nb);
+    for (uint32_t q = hg.start[b]; q < hg.start[b + 1]; ++q) {
+      const int32_t j = hg.bodies[q];
+      if (j > i && hg.cell[j] == key && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
     }
   }
 }
@@ -834,6 +852,46 @@ delta_status broadphase_plan(delta_ctx *ctx, const delta_scene &s, BroadphasePla
 }
 
 // Scratch slots 10 (cell keys), 11 (pair keys), 12 (sort temp).
+// Hash grid arrays carved from `base` (256-byte aligned pieces); returns the end.
+static char *carve_grid(char *base, int32_t n, HashGrid &hg) {
+  auto align = [](char *q) { return (char *)(((uintptr_t)q + 255) & ~(uintptr_t)255); };
+  char *b = align(base);
+  hg.nb = grid_buckets(n);
+  hg.count = (uint32_t *)b;
+  hg.fill = hg.count + hg.nb + 1;  // zeroed together with count
+  b = align(b + 4 * (2 * (size_t)hg.nb + 1));
+  hg.start = (uint32_t *)b;
+  b = align(b + 4 * ((size_t)hg.nb + 1));
+  hg.bodies = (int32_t *)b;
+  b = align(b + 4 * (size_t)n);
+  hg.cell = (uint64_t *)b;
+  return align(b + 8 * (size_t)n);
+}
+
+static size_t grid_bytes(int32_t n) {
+  const size_t nb = (size_t)grid_buckets(n);
+  return 5 * 256 + 4 * (2 * nb + 1) + 4 * (nb + 1) + 12 * (size_t)n;
+}
+
+// count, scan, fill: the hash grid of the moving bodies (count and fill zeroed first)
+static cudaError_t build_grid(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, const HashGrid &hg,
+                              void *temp, size_t temp_bytes, uint64_t *pk, int64_t pk_cap, unsigned long long *pcount) {
+  const int32_t n = s.n_bodies;
+  cudaError_t e = cudaMemsetAsync(hg.count, 0, 4 * (2 * (size_t)hg.nb + 1), st);
+  if (e != cudaSuccess) return e;
+  k_grid_count<<<blocks_for(n), 256, 0, st>>>(s, plan.g, hg, pk, pk_cap, pcount);
+  size_t tb = temp_bytes;
+  if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, hg.count, hg.start, hg.nb + 1, st)) != cudaSuccess) return e;
+  k_grid_fill<<<blocks_for(n), 256, 0, st>>>(s, hg);
+  return cudaGetLastError();
+}
+
+static size_t grid_temp_bytes(int32_t n) {
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, (uint32_t *)nullptr, (uint32_t *)nullptr, grid_buckets(n) + 1);
+  return tb;
+}
+
 delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const BroadphasePlan &plan, int32_t *pair_a,
                             int32_t *pair_b, int64_t capacity, int64_t *n_out) {
   cudaStream_t st = ctx->stream;
@@ -842,19 +900,14 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   const int32_t n = s.n_bodies;
   const int sh = bits_for(n);
   void *kb = nullptr;
-  if ((ds = ctx_scratch(ctx, 10, (sizeof(uint64_t) * 2 + sizeof(int32_t) * 2) * (size_t)n + 64, &kb)) != DELTA_OK)
-    return ds;
-  uint64_t *key = (uint64_t *)kb, *skey = key + n;
-  int32_t *body = (int32_t *)(skey + n), *sbody = body + n;
-  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body, nullptr, 0, nullptr);
-  ctx->launches += 1;
-  size_t tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st);
+  if ((ds = ctx_scratch(ctx, 10, grid_bytes(n), &kb)) != DELTA_OK) return ds;
+  HashGrid hg{};
+  carve_grid((char *)kb, n, hg);
+  size_t tb = grid_temp_bytes(n);
   void *temp = nullptr;
   if ((ds = ctx_scratch(ctx, 12, tb, &temp)) != DELTA_OK) return ds;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st)) != cudaSuccess)
-    return cuda_error(e, "cell sort");
-  ctx->launches += 1;
+  if ((e = build_grid(st, s, plan, hg, temp, tb, nullptr, 0, nullptr)) != cudaSuccess) return cuda_error(e, "grid");
+  ctx->launches += 3;
   int64_t cap = capacity > 4096 ? capacity : 4096;
   unsigned long long hcount = 0;
   uint64_t *pk = nullptr;
@@ -865,8 +918,7 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
     pk = (uint64_t *)pb + 8;
     if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess) return cuda_error(e, "memset");
     if (plan.n_moving > 0) {
-      k_grid_pairs<<<blocks_for(9 * (int64_t)plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, sh, pk, count,
-                                                                   cap);
+      k_grid_pairs<<<blocks_for(9 * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, cap);
       ctx->launches += 1;
     }
     if (plan.n_obst > 0) {
@@ -942,13 +994,11 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
 
 // Broadphase into a fixed-capacity pair list (padded with -1), overflow flagged on the device.
 size_t broadphase_fixed_state_bytes(int32_t n, int64_t pair_cap) {
-  return (size_t)n * 24 + 512 + (size_t)pair_cap * 16 + 256;
+  return grid_bytes(n) + 512 + (size_t)pair_cap * 16 + 256;
 }
 
 size_t broadphase_fixed_temp_bytes(int32_t n, int64_t pair_cap) {
-  size_t a = 0, b = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, a, (uint64_t *)nullptr, (uint64_t *)nullptr, (int32_t *)nullptr,
-                                  (int32_t *)nullptr, n, 0, 64);
+  size_t a = grid_temp_bytes(n), b = 0;
   cub::DeviceRadixSort::SortKeys(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, pair_cap, 0,
                                  2 * bits_for(n));
   return a > b ? a : b;
@@ -960,21 +1010,16 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
   cudaError_t e;
   const int32_t n = s.n_bodies;
   const int sh = bits_for(n);
-  char *b = (char *)state;
-  uint64_t *key = (uint64_t *)b, *skey = key + n;
-  int32_t *body = (int32_t *)(skey + n), *sbody = body + n;
-  b += (size_t)n * 24;
-  b = (char *)(((uintptr_t)b + 255) & ~(uintptr_t)255);
+  HashGrid hg{};
+  char *b = carve_grid((char *)state, n, hg);
   unsigned long long *count = (unsigned long long *)b;
   uint64_t *pk = (uint64_t *)(b + 256), *spk = pk + pair_cap;
-  k_cell_keys<<<blocks_for(n), 256, 0, st>>>(s, plan.g, key, body, pk, pair_cap, count);
+  if ((e = build_grid(st, s, plan, hg, temp, temp_bytes, pk, pair_cap, count)) != cudaSuccess)
+    return cuda_error(e, "grid");
   size_t tb = temp_bytes;
-  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, key, skey, body, sbody, n, 0, kCellKeyBits, st)) != cudaSuccess)
-    return cuda_error(e, "cell sort");
-  kernels += 2;
+  kernels += 3;
   if (plan.n_moving > 0) {
-    k_grid_pairs<<<blocks_for(9 * (int64_t)plan.n_moving, 128), 128, 0, st>>>(s, plan.g, skey, sbody, plan.n_moving, sh, pk, count,
-                                                                 pair_cap);
+    k_grid_pairs<<<blocks_for(9 * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, pair_cap);
     kernels += 1;
   }
   if (plan.n_obst > 0) {
@@ -992,8 +1037,8 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
 
 // The raw pair count of the last fixed broadphase (for growing the capacity).
 static unsigned long long *broadphase_fixed_count(void *state, int32_t n) {
-  char *b = (char *)state + (size_t)n * 24;
-  return (unsigned long long *)(((uintptr_t)b + 255) & ~(uintptr_t)255);
+  HashGrid hg{};
+  return (unsigned long long *)carve_grid((char *)state, n, hg);
 }
 }  // namespace delta
 
