@@ -248,8 +248,9 @@ delta_status delta_sim_step(delta_sim *sim, const delta_step_params *params, int
  * host synchronisation.  The first call sizes the buffers from an observed detection.
  * A capacity overflow in a replayed step freezes the state after that step's
  * integration; the host then repeats that detection with larger buffers, records the
- * graph again and continues, so results equal delta_sim_step's bit for bit.  The graph is
- * recorded again whenever params change. */
+ * graph again and continues, so results equal delta_sim_step's bit for bit.  The buffers
+ * and the recorded graph are kept from call to call while the current contacts fit; the
+ * graph is recorded again whenever params change. */
 delta_status delta_sim_step_graph(delta_sim *sim, const delta_step_params *params, int32_t nsteps,
                                   int64_t *contacts_per_step /* host [nsteps] or NULL */);
 /* Capacities (candidate pairs, contacts) of the graph buffers for the next
