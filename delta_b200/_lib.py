@@ -56,6 +56,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_mlp_layout": ([vp], C.c_int),
     "delta_mlp_infer": ([vp, i64, vp, vp, i64, vp, vp, vp], C.c_int),
     "delta_mlp_infer_tcgen05": ([vp, i64, vp, vp, i64, vp, vp, vp], C.c_int),
+    "delta_mlp_infer_tcgen05_wait_test": ([vp, i64, vp, vp, i64, vp, vp, vp, C.c_uint32], C.c_int),
     "delta_mlp_set_engine": ([vp, C.c_int], C.c_int),
     "delta_mlp_features": ([vp, i64, vp, vp, i64, vp, vp, vp, vp, vp], C.c_int),
     "delta_gemm_bf16": ([vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int,

@@ -502,9 +502,9 @@ __device__ __forceinline__ void tc_commit(uint64_t *mbar) {
 }
 
 // bounded wait for the mbarrier phase with parity `phase`; false on time-out
-__device__ __forceinline__ bool tc_wait(uint64_t *mbar, uint32_t phase) {
+__device__ __forceinline__ bool tc_wait(uint64_t *mbar, uint32_t phase, uint32_t spin) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(mbar);
-  for (uint32_t it = 0; it < kTcSpin; ++it) {
+  for (uint32_t it = 0; it < spin; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
@@ -558,10 +558,12 @@ __device__ __forceinline__ void tc_stage(__nv_bfloat16 *dst, const __nv_bfloat16
   }
 }
 
-// one layer: the elected thread issues K/16 MMAs into TMEM and commits; everyone waits.
-// Returns false (and sets the CTA's abort flag) when the wait timed out.
+// one layer: the elected thread issues K/16 MMAs into TMEM and commits; everyone waits
+// (at most `spin` polls).  Returns false (and sets the CTA's abort flag) when the wait
+// timed out.  `withhold` (the time-out test only) issues neither the MMAs nor the commit,
+// so the barrier never completes and the wait runs out with nothing in flight.
 __device__ __forceinline__ bool tc_layer(TcSmem &sm, const __nv_bfloat16 *A, const __nv_bfloat16 *W, int K, int N,
-                                         uint32_t &phase) {
+                                         uint32_t &phase, uint32_t spin = kTcSpin, bool withhold = false) {
   // make the generic-proxy stores of A visible to the tensor cores, then synchronise
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -570,10 +572,12 @@ __device__ __forceinline__ bool tc_layer(TcSmem &sm, const __nv_bfloat16 *A, con
   if (threadIdx.x == 0) {
     const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(A), w0 = (uint32_t)__cvta_generic_to_shared(W);
     const uint32_t idesc = tc_idesc(kTcRows, N);
-    for (int s = 0; s < K / 16; ++s)
-      tc_mma(sm.tmem_base, tc_desc(a0 + 256u * s, 16u * K), tc_desc(w0 + 256u * s, 16u * K), idesc, s > 0 ? 1u : 0u);
-    tc_commit(&sm.mbar);
-    if (!tc_wait(&sm.mbar, phase)) sm.abort = 1;
+    if (!withhold) {
+      for (int s = 0; s < K / 16; ++s)
+        tc_mma(sm.tmem_base, tc_desc(a0 + 256u * s, 16u * K), tc_desc(w0 + 256u * s, 16u * K), idesc, s > 0 ? 1u : 0u);
+      tc_commit(&sm.mbar);
+    }
+    if (!tc_wait(&sm.mbar, phase, spin)) sm.abort = 1;
   }
   __syncthreads();
   phase ^= 1u;
@@ -585,7 +589,8 @@ constexpr int kTcThreads = 2 * kTcRows;
 
 __global__ void __launch_bounds__(kTcThreads, 2)
     k_mlp_infer_tc(int64_t n, const __nv_bfloat16 *__restrict__ feat, const float *__restrict__ params,
-                   const __nv_bfloat16 *__restrict__ wb, float *__restrict__ x0, int *__restrict__ err) {
+                   const __nv_bfloat16 *__restrict__ wb, float *__restrict__ x0, int *__restrict__ err,
+                   uint32_t spin, int withhold) {
   extern __shared__ __align__(128) unsigned char tc_smem_raw[];
   TcSmem &sm = *reinterpret_cast<TcSmem *>(tc_smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -634,7 +639,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     const __nv_bfloat16 *Ws[3] = {sm.w1, sm.w2, sm.w3};
     bool ok = true;
     for (int l = 0; l < 3; ++l) {
-      ok = tc_layer(sm, sm.ah, Ws[l], K, kHid, phase);
+      ok = tc_layer(sm, sm.ah, Ws[l], K, kHid, phase, spin, withhold != 0 && l == 0);
       if (!ok) break;
       // bias + GELU of this thread's 64 columns of its row, into the hidden A tile
 #pragma unroll 1
@@ -655,7 +660,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
       K = kHid;
     }
     if (!ok) break;
-    if (!tc_layer(sm, sm.ah, sm.w4, kHid, kTcW4Rows, phase)) break;
+    if (!tc_layer(sm, sm.ah, sm.w4, kHid, kTcW4Rows, phase, spin)) break;
     if (half == 0) {
       float v[16];
       tc_ld16(tlane, v);
@@ -1063,7 +1068,8 @@ inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t
 // Features into scratch, then the network on `engine`; with the tcgen05 engine *err_out
 // receives the device time-out flag (zeroed here, set by the kernel).
 delta_status mlp_infer_launch(delta_ctx *ctx, int engine, int64_t n, const double *a, const double *b, int64_t ld,
-                              const float *params, const void *params_bf16, float *x0, int **err_out) {
+                              const float *params, const void *params_bf16, float *x0, int **err_out,
+                              uint32_t spin = kTcSpin, int withhold = 0) {
   void *fbuf;
   delta_status st = ctx_scratch(ctx, 15, sizeof(__nv_bfloat16) * 32 * (size_t)n, &fbuf);
   if (st != DELTA_OK) return st;
@@ -1086,7 +1092,7 @@ delta_status mlp_infer_launch(delta_ctx *ctx, int engine, int64_t n, const doubl
     }
     const int64_t tiles = (n + kTcRows - 1) / kTcRows;
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, 2 * kNumSMs);
-    k_mlp_infer_tc<<<grid, kTcThreads, sizeof(TcSmem), ctx->stream>>>(n, feat, params, wb, x0, err);
+    k_mlp_infer_tc<<<grid, kTcThreads, sizeof(TcSmem), ctx->stream>>>(n, feat, params, wb, x0, err, spin, withhold);
     if (err_out) *err_out = err;
   } else {
     static thread_local int configured_device = -1;
@@ -1303,6 +1309,19 @@ delta_status delta_mlp_infer_tcgen05(delta_ctx *ctx, int64_t n, const double *a,
   if (n == 0) return DELTA_OK;
   int *err = nullptr;
   delta_status st = mlp_infer_launch(ctx, DELTA_MLP_TCGEN05, n, a, b, ld, params, params_bf16, x0, &err);
+  if (st != DELTA_OK) return st;
+  return mlp_check_error(ctx, err);
+}
+
+delta_status delta_mlp_infer_tcgen05_wait_test(delta_ctx *ctx, int64_t n, const double *a, const double *b,
+                                               int64_t ld, const float *params, const void *params_bf16, float *x0,
+                                               uint32_t polls) {
+  if (!ctx || n <= 0 || ld < n || !a || !b || !params || !params_bf16 || !x0 || polls < 1 || polls > kTcSpin)
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer_tcgen05_wait_test: bad argument");
+  if ((reinterpret_cast<uintptr_t>(params_bf16) & 15) || (reinterpret_cast<uintptr_t>(x0) & 15))
+    return set_error(DELTA_ERR_INVALID, "delta_mlp_infer_tcgen05_wait_test: params_bf16 and x0 must be 16-byte aligned");
+  int *err = nullptr;
+  delta_status st = mlp_infer_launch(ctx, DELTA_MLP_TCGEN05, n, a, b, ld, params, params_bf16, x0, &err, polls, 1);
   if (st != DELTA_OK) return st;
   return mlp_check_error(ctx, err);
 }

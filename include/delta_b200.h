@@ -368,6 +368,14 @@ delta_status delta_mlp_set_engine(delta_ctx *ctx, int engine);
  * cores gave up (x0 is then incomplete). */
 delta_status delta_mlp_infer_tcgen05(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                                      const float *params, const void *params_bf16, float *x0);
+/* Test of the failure path of delta_mlp_infer_tcgen05 (no counterpart in the reference):
+ * the kernel withholds the first layer's MMAs and commit, so its bounded wait for the
+ * tensor cores runs out after `polls` polls (1 .. 2^22) with nothing in flight; the kernel
+ * frees its TMEM and returns.  Expected result: DELTA_ERR_TIMEOUT, the context still
+ * usable; x0 is left unspecified.  Same arguments as delta_mlp_infer_tcgen05, n > 0. */
+delta_status delta_mlp_infer_tcgen05_wait_test(delta_ctx *ctx, int64_t n, const double *a, const double *b,
+                                               int64_t ld, const float *params, const void *params_bf16, float *x0,
+                                               uint32_t polls);
 /* Canonical features: triangle A's frame (origin at its centroid, x along A1-A0, z along
  * its normal, unit = its longest edge), the six vertices in that frame as 18 BF16 values
  * padded with zeros to rows of 32 (features_bf16 [n][32]).  With p, q (closest points,

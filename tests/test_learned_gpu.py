@@ -308,3 +308,27 @@ def test_learned_solver_translated_and_scaled(ctx, oracle, pairs, shift, scale):
     assert np.all(np.abs(d - od)[fin] <= 1e-6 * od[fin])
     assert np.array_equal(d[fl == 2], od[fl == 2], equal_nan=True)
     assert nf == int((fl == 2).sum())
+
+
+def test_tcgen05_bounded_wait_reports_timeout_and_context_stays_usable(ctx, pairs):
+    """The tcgen05 kernel's wait for the tensor cores is bounded: with the first layer's
+    commit withheld (nothing arrives on the barrier, nothing is in flight) the wait runs
+    out, the kernel frees its TMEM and the call reports DELTA_ERR_TIMEOUT.  The same
+    context then runs the network normally."""
+    import torch
+
+    from delta_b200._lib import DeltaError, check, lib
+    from delta_b200.learned import WarmStartMLP
+
+    a, b = pairs[0][:, :1000], pairs[1][:, :1000]
+    da, db = _dev(a), _dev(b)
+    model = WarmStartMLP.load(ctx)
+    x0 = torch.empty((1000, 4), dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        with pytest.raises(DeltaError, match="TIMEOUT"):
+            check(lib().delta_mlp_infer_tcgen05_wait_test(ctx.handle, 1000, da.data_ptr(), db.data_ptr(), 1000,
+                                                          model.params.data_ptr(), model.params_bf16.data_ptr(),
+                                                          x0.data_ptr(), 1 << 14))
+    x_tc = model.predict(da, db, engine="tcgen05").cpu().numpy()
+    x_mma = model.predict(da, db).cpu().numpy()
+    assert _rel(x_tc, x_mma) <= 1e-2
