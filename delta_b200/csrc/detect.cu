@@ -668,7 +668,7 @@ cudaError_t launch_detect_prec(int driver, cudaStream_t s, const delta_meshes &m
 // Scratch slots used here: 2 rows/row_offset, 3 raw contacts, 4 sort buffers, 5 small state.
 delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
-                        delta_stats *stats, int64_t *counters) {
+                        delta_stats *stats, int64_t *counters, const double *bbox) {
   cudaStream_t s = ctx->stream;
   delta_status st;
   cudaError_t e;
@@ -715,7 +715,9 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   unsigned long long hcount = 0;
   RawContacts rc{};
   rc.tbits = 16;
-  if (driver == DELTA_DRV_BF_CERT) {
+  if (driver == DELTA_DRV_BF_CERT && bbox) {
+    rc.bbox = bbox;  // the caller's boxes of every body in the pairs
+  } else if (driver == DELTA_DRV_BF_CERT) {
     // body boxes of the current vertices for the culling
     void *bb = nullptr;
     if ((st = ctx_scratch(ctx, 23, 48 * (size_t)m.n_bodies + 64, &bb)) != DELTA_OK) return st;

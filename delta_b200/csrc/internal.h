@@ -39,10 +39,12 @@ cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t 
 cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
                          int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags);
 
-// Particle-pair drivers (detect.cu).
+// Particle-pair drivers (detect.cu).  `bbox`: the certified driver's body boxes
+// (lo[3], hi[3]) of the current vertices of every body in the pairs, written by the
+// caller, or null (then computed here for all bodies).
 delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
-                        delta_stats *stats, int64_t *counters = nullptr);
+                        delta_stats *stats, int64_t *counters = nullptr, const double *bbox = nullptr);
 
 // Fixed-capacity (graph-capturable) detection (detect.cu).  `bbox`: the boxes (lo[3], hi[3])
 // of every body's current vertices, written by the caller, for the certified driver's

@@ -1058,6 +1058,7 @@ struct delta_sim {
   // pairs get their vertices updated (stamp[i] == *epoch); every vertex is brought up to
   // date at the end of the call.  [n] stamps, then the epoch.
   uint32_t *stamp = nullptr, *epoch = nullptr;
+  double *bbox = nullptr;  // body boxes of the stepped certified driver, from k_vertices
   // contacts of the last detection
   delta_contacts c{};
   void *c_mem = nullptr;
@@ -1151,7 +1152,8 @@ static delta_status sim_detect(delta_sim *s) {
   cudaStream_t st = s->ctx->stream;
   k_next_epoch<<<1, 1, 0, st>>>(s->epoch);
   if (np > 0) k_mark_pair_bodies<<<blocks_for(np), 256, 0, st>>>(s->pa, s->pb, np, s->epoch, s->stamp);
-  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, nullptr, nullptr, s->stamp, s->epoch);
+  double *bbox = s->driver == DELTA_DRV_BF_CERT ? s->bbox : nullptr;
+  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, nullptr, bbox, s->stamp, s->epoch);
   s->ctx->launches += np > 0 ? 3 : 2;
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
                  s->scene.eps,      s->scene.friction,   s->ids};
@@ -1161,11 +1163,11 @@ static delta_status sim_detect(delta_sim *s) {
     return DELTA_OK;
   }
   int64_t cnt[2] = {0, 0};
-  ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt);
+  ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt, bbox);
   if (ds == DELTA_ERR_CAPACITY) {
     if ((ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;
     cnt[0] = cnt[1] = 0;
-    ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt);
+    ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt, bbox);
   }
   s->counters[2] += cnt[0];
   s->counters[3] += cnt[1];
@@ -1366,6 +1368,7 @@ delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driv
                          (e = cudaMemset(s->stamp, 0, sizeof(uint32_t) * ((size_t)n + 1))) != cudaSuccess))
     ds = cuda_error(e, "vertex stamps");
   if (ds == DELTA_OK) s->epoch = s->stamp + n;
+  if (ds == DELTA_OK && (e = cudaMalloc(&s->bbox, 48 * (size_t)n + 64)) != cudaSuccess) ds = cuda_error(e, "boxes");
   if (ds == DELTA_OK && (e = cudaMalloc(&s->F, sizeof(double) * 6 * n + n)) != cudaSuccess) ds = cuda_error(e, "F");
   if (ds == DELTA_OK) {
     s->T = s->F + 3 * n;
@@ -1566,6 +1569,7 @@ delta_status delta_sim_destroy(delta_sim *s) {
   s->plan.release();
   if (s->ids) cudaFree(s->ids);
   if (s->stamp) cudaFree(s->stamp);
+  if (s->bbox) cudaFree(s->bbox);
   if (s->F) cudaFree(s->F);
   if (s->c_mem) cudaFree(s->c_mem);
   if (s->pa) cudaFree(s->pa);
