@@ -138,67 +138,69 @@ struct ContactView {
   int64_t cap;
 };
 
-// getContactsForces over contacts [c0, c1) of one partner pair, for body `a` (the
-// current particle) against `b`; sign = -1 applies the inverted normal stored for the
-// slave (Collision.cpp:176-184).  Sums into F, T from zero in list order.
-__device__ void pair_forces(const delta_scene &s, const ContactView &cv, int64_t c0, int64_t c1, int32_t a,
-                            int32_t b, bool negate, const delta_step_params &p, X F[3], X Tq[3]) {
+// State of one body as the contact forces read it.
+struct BodyKin {
+  X pos[3], ang[3], lin[3], mass;
+};
+
+__device__ __forceinline__ BodyKin body_kin(const delta_scene &s, int32_t a) {
   const int32_t n = s.n_bodies;
-  X posA[3], angA[3], linA[3], posB[3], angB[3], linB[3];
+  BodyKin k;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    posA[k] = X(s.pos[(int64_t)k * n + a]);
-    angA[k] = X(s.ang[(int64_t)k * n + a]);
-    linA[k] = X(s.vel[(int64_t)k * n + a]);
-    posB[k] = X(s.pos[(int64_t)k * n + b]);
-    angB[k] = X(s.ang[(int64_t)k * n + b]);
-    linB[k] = X(s.vel[(int64_t)k * n + b]);
+  for (int d = 0; d < 3; ++d) {
+    k.pos[d] = X(s.pos[(int64_t)d * n + a]);
+    k.ang[d] = X(s.ang[(int64_t)d * n + a]);
+    k.lin[d] = X(s.vel[(int64_t)d * n + a]);
   }
-  const X massA = X(s.mass[a]), massB = X(s.mass[b]);
+  k.mass = X(s.mass[a]);
+  return k;
+}
+
+// The terms of one contact c in getContactsForces (forces.cpp:23-396): the force term
+// (spring + damping + friction) and the torque term that the loop adds to its sums, for
+// body A against B; `negate` applies the inverted normal stored for the slave
+// (Collision.cpp:176-184).  Each term is formed in full before it is added, so a sum of
+// these terms in list order is the reference loop's sum bit for bit.
+__device__ __forceinline__ void contact_terms(const ContactView &cv, int64_t c, const BodyKin &A, const BodyKin &B,
+                                              bool negate, const delta_step_params &p, X Fc[3], X Tc[3]) {
   const X spring = X(p.spring), damper = X(p.damper), mu = X(p.friction);
-  for (int k = 0; k < 3; ++k) {
-    F[k] = X(0.0);
-    Tq[k] = X(0.0);
-  }
-  for (int64_t c = c0; c < c1; ++c) {
-    X x[3], nn[3];
+  X x[3], nn[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      x[k] = X(cv.x[k * cv.cap + c]);
-      const X nv = X(cv.normal[k * cv.cap + c]);
-      nn[k] = negate ? X(-1.0) * nv : nv;
-    }
-    const X depth = X(cv.depth[c]);
-    X z[3], vi[3], vj[3], vij[3];
-    for (int k = 0; k < 3; ++k) z[k] = x[k] - posA[k];
-    vi[0] = angA[1] * z[2] - angA[2] * z[1] + linA[0];
-    vi[1] = angA[2] * z[0] - angA[0] * z[2] + linA[1];
-    vi[2] = angA[0] * z[1] - angA[1] * z[0] + linA[2];
-    for (int k = 0; k < 3; ++k) z[k] = x[k] - posB[k];
-    vj[0] = angB[1] * z[2] - angB[2] * z[1] + linB[0];
-    vj[1] = angB[2] * z[0] - angB[0] * z[2] + linB[1];
-    vj[2] = angB[0] * z[1] - angB[1] * z[0] + linB[2];
-    for (int k = 0; k < 3; ++k) vij[k] = vj[k] - vi[k];
-    const X ma = X(1.0) / ((X(1.0) / massA) + (X(1.0) / massB));
-    const X velocity = (vij[0] * nn[0]) + (vij[1] * nn[1]) + (vij[2] * nn[2]);
-    const X damp = damper * X(2.0) * sqrt_(ma * spring) * velocity;
-    const X fmag = spring * depth + damp;
-    X f[3], fr[3] = {X(0.0), X(0.0), X(0.0)};
-    for (int k = 0; k < 3; ++k) f[k] = fmag * nn[k];
-    if (cv.friction[c]) {
-      const X vn = (vi[0] * nn[0]) + (vi[1] * nn[1]) + (vi[2] * nn[2]);
-      for (int k = 0; k < 3; ++k) {
-        const X vt = vi[k] - nn[k] * vn;
-        fr[k] = -vt * mu * fmag;
-      }
-    }
-    for (int k = 0; k < 3; ++k) F[k] += f[k] + fr[k];
-    X arm[3];
-    for (int k = 0; k < 3; ++k) arm[k] = x[k] - posA[k];
-    Tq[0] += arm[1] * (f[2]) - arm[2] * (f[1]);
-    Tq[1] += arm[2] * (f[0]) - arm[0] * (f[2]);
-    Tq[2] += arm[0] * (f[1]) - arm[1] * (f[0]);
+  for (int k = 0; k < 3; ++k) {
+    x[k] = X(cv.x[k * cv.cap + c]);
+    const X nv = X(cv.normal[k * cv.cap + c]);
+    nn[k] = negate ? X(-1.0) * nv : nv;
   }
+  const X depth = X(cv.depth[c]);
+  X z[3], vi[3], vj[3], vij[3];
+  for (int k = 0; k < 3; ++k) z[k] = x[k] - A.pos[k];
+  vi[0] = A.ang[1] * z[2] - A.ang[2] * z[1] + A.lin[0];
+  vi[1] = A.ang[2] * z[0] - A.ang[0] * z[2] + A.lin[1];
+  vi[2] = A.ang[0] * z[1] - A.ang[1] * z[0] + A.lin[2];
+  for (int k = 0; k < 3; ++k) z[k] = x[k] - B.pos[k];
+  vj[0] = B.ang[1] * z[2] - B.ang[2] * z[1] + B.lin[0];
+  vj[1] = B.ang[2] * z[0] - B.ang[0] * z[2] + B.lin[1];
+  vj[2] = B.ang[0] * z[1] - B.ang[1] * z[0] + B.lin[2];
+  for (int k = 0; k < 3; ++k) vij[k] = vj[k] - vi[k];
+  const X ma = X(1.0) / ((X(1.0) / A.mass) + (X(1.0) / B.mass));
+  const X velocity = (vij[0] * nn[0]) + (vij[1] * nn[1]) + (vij[2] * nn[2]);
+  const X damp = damper * X(2.0) * sqrt_(ma * spring) * velocity;
+  const X fmag = spring * depth + damp;
+  X f[3], fr[3] = {X(0.0), X(0.0), X(0.0)};
+  for (int k = 0; k < 3; ++k) f[k] = fmag * nn[k];
+  if (cv.friction[c]) {
+    const X vn = (vi[0] * nn[0]) + (vi[1] * nn[1]) + (vi[2] * nn[2]);
+    for (int k = 0; k < 3; ++k) {
+      const X vt = vi[k] - nn[k] * vn;
+      fr[k] = -vt * mu * fmag;
+    }
+  }
+  for (int k = 0; k < 3; ++k) Fc[k] = f[k] + fr[k];
+  X arm[3];
+  for (int k = 0; k < 3; ++k) arm[k] = x[k] - A.pos[k];
+  Tc[0] = arm[1] * (f[2]) - arm[2] * (f[1]);
+  Tc[1] = arm[2] * (f[0]) - arm[0] * (f[2]);
+  Tc[2] = arm[0] * (f[1]) - arm[1] * (f[0]);
 }
 
 __global__ void k_step_end(const int *ovf_snap, const int64_t *n_contacts, int64_t *log, int64_t log_len,
@@ -215,63 +217,104 @@ __global__ void k_segment_heads(ContactView cv, int64_t n, uint8_t *head) {
   head[c] = (c == 0 || cv.master[c] != cv.master[c - 1] || cv.slave[c] != cv.slave[c - 1]) ? 1 : 0;
 }
 
-// One thread per partner pair: both sides' sums, keyed (body << sh | partner), sh the bits
-// of a body index.
-__global__ void k_pair_forces(delta_scene s, ContactView cv, const int64_t *seg_start, const int64_t *n_seg_p,
-                              int64_t n_contacts_h, const int64_t *n_contacts_d, delta_step_params p, int sh,
-                              uint64_t *key, int64_t *val_idx, double *entry) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t n_seg = *n_seg_p;
-  int64_t n_contacts = n_contacts_d ? *n_contacts_d : n_contacts_h;
-  if (n_contacts > cv.cap) n_contacts = cv.cap;
-  if (g >= n_seg) return;
-  const int64_t c0 = seg_start[g], c1 = g + 1 < n_seg ? seg_start[g + 1] : n_contacts;
-  const int32_t i = cv.master[c0], j = cv.slave[c0];
-  X F[3], T[3];
-  pair_forces(s, cv, c0, c1, i, j, false, p, F, T);
-  for (int k = 0; k < 3; ++k) {
-    entry[(2 * g) * 6 + k] = F[k].v;
-    entry[(2 * g) * 6 + 3 + k] = T[k].v;
+// Partner-pair force sums, one thread per contact.  Every thread forms its contact's terms
+// for both sides (master: force and torque on the master; slave: with the inverted normal,
+// on the slave) in shared memory.  The thread at the first contact of a (master, slave)
+// segment then adds the segment's terms in contact order, forming itself the terms of
+// contacts past its block.  From 0.0 in contact order, these are the sums of the
+// getContactsForces loop over the pair's contacts (forces.cpp:23-396), bit for bit.
+//  - kFixed (graph path, count on the device): the sums go to entry 2c (on the master) and
+//    2c+1 (on the slave), c the segment's first contact, and the segment is counted in its
+//    slave's list.  Sums on obstacles are not formed: nothing reads them.
+//  - otherwise: segment g (seg_start[g] == c) gets entries 2g and 2g+1, keyed
+//    (body << sh | partner) for the entry sort, sh the bits of a body index.
+constexpr int kHeadThreads = 128;
+template <bool kFixed>
+__global__ void __launch_bounds__(kHeadThreads) k_pair_forces_heads(
+    delta_scene s, ContactView cv, const int64_t *n_contacts_d, int64_t n_contacts_h, const int64_t *seg_start,
+    const int64_t *n_seg_p, delta_step_params p, int sh, uint64_t *key, int64_t *val_idx, double *entry,
+    uint32_t *slave_count) {
+  __shared__ double term[12][kHeadThreads];  // master F, master T, slave F, slave T
+  const int64_t blk0 = (int64_t)blockIdx.x * kHeadThreads;
+  const int64_t c = blk0 + threadIdx.x;
+  int64_t n = n_contacts_d ? *n_contacts_d : n_contacts_h;
+  if (n > cv.cap) n = cv.cap;
+  if (blk0 >= n) return;  // the whole block is past the contacts
+  const int64_t blk1 = blk0 + kHeadThreads < n ? blk0 + kHeadThreads : n;
+  int32_t i = 0, j = 0;
+  bool oi = true, oj = true;
+  if (c < n) {
+    i = cv.master[c];
+    j = cv.slave[c];
+    oi = kFixed && s.obstacle[i] != 0;
+    oj = kFixed && s.obstacle[j] != 0;
+    const BodyKin Ki = body_kin(s, i), Kj = body_kin(s, j);
+    X Fc[3], Tc[3];
+    if (!oi) {
+      contact_terms(cv, c, Ki, Kj, false, p, Fc, Tc);
+      for (int k = 0; k < 3; ++k) {
+        term[k][threadIdx.x] = Fc[k].v;
+        term[3 + k][threadIdx.x] = Tc[k].v;
+      }
+    }
+    if (!oj) {
+      contact_terms(cv, c, Kj, Ki, true, p, Fc, Tc);
+      for (int k = 0; k < 3; ++k) {
+        term[6 + k][threadIdx.x] = Fc[k].v;
+        term[9 + k][threadIdx.x] = Tc[k].v;
+      }
+    }
   }
-  pair_forces(s, cv, c0, c1, j, i, true, p, F, T);
-  for (int k = 0; k < 3; ++k) {
-    entry[(2 * g + 1) * 6 + k] = F[k].v;
-    entry[(2 * g + 1) * 6 + 3 + k] = T[k].v;
-  }
-  key[2 * g] = ((uint64_t)(uint32_t)i << sh) | (uint32_t)j;
-  key[2 * g + 1] = ((uint64_t)(uint32_t)j << sh) | (uint32_t)i;
-  val_idx[2 * g] = 2 * g;
-  val_idx[2 * g + 1] = 2 * g + 1;
-}
-
-// Fixed-capacity force pass, one thread per contact slot: the thread at the first contact
-// of a (master, slave) segment sums the segment (the sums of k_pair_forces) into entry 2c
-// (on the master) and 2c+1 (on the slave) and counts the segment in its slave's list.
-// Sums on obstacles are not formed: nothing reads them.
-__global__ void k_pair_forces_heads(delta_scene s, ContactView cv, const int64_t *n_contacts_d,
-                                    delta_step_params p, double *entry, uint32_t *slave_count) {
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t n = *n_contacts_d < cv.cap ? *n_contacts_d : cv.cap;
+  __syncthreads();
   if (c >= n) return;
   if (c > 0 && cv.master[c] == cv.master[c - 1] && cv.slave[c] == cv.slave[c - 1]) return;
-  const int32_t i = cv.master[c], j = cv.slave[c];
   int64_t c1 = c + 1;
   while (c1 < n && cv.master[c1] == i && cv.slave[c1] == j) ++c1;
-  X F[3], T[3];
-  if (!s.obstacle[i]) {
-    pair_forces(s, cv, c, c1, i, j, false, p, F, T);
-    for (int k = 0; k < 3; ++k) {
-      entry[(2 * c) * 6 + k] = F[k].v;
-      entry[(2 * c) * 6 + 3 + k] = T[k].v;
+  int64_t e0 = 2 * c;
+  if constexpr (!kFixed) {
+    int64_t lo = 0, hi = *n_seg_p;  // the segment index: seg_start[g] == c
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (seg_start[mid] < c) lo = mid + 1;
+      else hi = mid;
     }
+    e0 = 2 * lo;
   }
-  if (!s.obstacle[j]) {
-    pair_forces(s, cv, c, c1, j, i, true, p, F, T);
-    for (int k = 0; k < 3; ++k) {
-      entry[(2 * c + 1) * 6 + k] = F[k].v;
-      entry[(2 * c + 1) * 6 + 3 + k] = T[k].v;
+  // the sums of one side: terms from shared memory within the block, formed here past it
+  auto side = [&](int o, int32_t a, int32_t b, bool negate, int64_t e) {
+    X F[3] = {X(0.0), X(0.0), X(0.0)}, T[3] = {X(0.0), X(0.0), X(0.0)};
+    for (int64_t u = c; u < c1 && u < blk1; ++u) {
+      const int t = (int)(u - blk0);
+      for (int k = 0; k < 3; ++k) {
+        F[k] += X(term[o + k][t]);
+        T[k] += X(term[o + 3 + k][t]);
+      }
     }
-    atomicAdd(&slave_count[j], 1u);
+    if (c1 > blk1) {
+      const BodyKin A = body_kin(s, a), B = body_kin(s, b);
+      for (int64_t u = blk1; u < c1; ++u) {
+        X Fc[3], Tc[3];
+        contact_terms(cv, u, A, B, negate, p, Fc, Tc);
+        for (int k = 0; k < 3; ++k) {
+          F[k] += Fc[k];
+          T[k] += Tc[k];
+        }
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      entry[e * 6 + k] = F[k].v;
+      entry[e * 6 + 3 + k] = T[k].v;
+    }
+  };
+  if (!oi) side(0, i, j, false, e0);
+  if (!oj) side(6, j, i, true, e0 + 1);
+  if constexpr (kFixed) {
+    if (!oj) atomicAdd(&slave_count[j], 1u);
+  } else {
+    key[e0] = ((uint64_t)(uint32_t)i << sh) | (uint32_t)j;
+    key[e0 + 1] = ((uint64_t)(uint32_t)j << sh) | (uint32_t)i;
+    val_idx[e0] = e0;
+    val_idx[e0 + 1] = e0 + 1;
   }
 }
 
@@ -746,8 +789,8 @@ delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contac
   // entries for all potential segments (n_contacts bounds the count; unused keys sort last)
   if ((e = cudaMemsetAsync(key, 0xff, sizeof(uint64_t) * 2 * nc, st)) != cudaSuccess) return cuda_error(e, "memset");
   const int sh = bits_for(n);
-  k_pair_forces<<<blocks_for(n_contacts, 128), 128, 0, st>>>(s, cv, seg_start, n_seg, n_contacts, nullptr, p, sh, key, idx,
-                                                            entry);
+  k_pair_forces_heads<false><<<blocks_for(n_contacts, kHeadThreads), kHeadThreads, 0, st>>>(
+      s, cv, nullptr, n_contacts, seg_start, n_seg, p, sh, key, idx, entry, nullptr);
   ctx->launches += 1;
   tb = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, idx, sidx, (int64_t)(2 * nc), 0, 2 * sh, st);
@@ -982,7 +1025,8 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   b = align(b + 4 * (2 * (size_t)n + 1));
   uint32_t *start = (uint32_t *)b;
   if ((e = cudaMemsetAsync(cnt, 0, 4 * (2 * (size_t)n + 1), st)) != cudaSuccess) return cuda_error(e, "forces memset");
-  k_pair_forces_heads<<<blocks_for(cap, 128), 128, 0, st>>>(s, cv, d_nc, p, entry, cnt);
+  k_pair_forces_heads<true><<<blocks_for(cap, kHeadThreads), kHeadThreads, 0, st>>>(
+      s, cv, d_nc, 0, nullptr, nullptr, p, 0, nullptr, nullptr, entry, cnt);
   size_t tb = temp_bytes;
   if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, cnt, start, n + 1, st)) != cudaSuccess)
     return cuda_error(e, "slave list scan");
