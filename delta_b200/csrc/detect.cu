@@ -38,6 +38,11 @@ struct RawContacts {
   const double *bbox;
   // sort key of a contact: pair << 2 tbits | A triangle << tbits | B triangle
   int tbits;
+  // fixed-capacity certified driver: contacts counted per pair (pcnt, zeroed by the culling)
+  // and each contact's rank of arrival within its pair (slot), for the sort-free ordering;
+  // null elsewhere
+  unsigned long long *pcnt;
+  uint32_t *slot;
 };
 
 struct DevStats {
@@ -146,7 +151,10 @@ __device__ __forceinline__ int64_t agg_slot(unsigned long long *count) {
 __device__ __forceinline__ void emit(const RawContacts &rc, bool take, const double pq[6], const RowCtx &r, int32_t tb) {
   if (!take) return;
   const int64_t pos = agg_slot(rc.count);
-  if (pos < rc.cap) write_contact(rc, pos, pq, r, tb);
+  if (pos < rc.cap) {
+    write_contact(rc, pos, pq, r, tb);
+    if (rc.pcnt) rc.slot[pos] = (uint32_t)atomicAdd(rc.pcnt + r.k, 1ull);
+  }
 }
 
 __device__ __forceinline__ int warp_sum(int v) { return __reduce_add_sync(kFull, v); }
@@ -418,7 +426,9 @@ __global__ void __launch_bounds__(kCullThreads) k_cull_pairs(delta_meshes m, con
                                                              RawContacts rc, DevStats *st) {
   __shared__ CullList LA, LB;
   const int tid = threadIdx.x;
+  if (rc.pcnt && blockIdx.x == 0 && tid == 0) rc.pcnt[n_pairs] = 0;
   for (int64_t k = blockIdx.x; k < n_pairs; k += gridDim.x) {
+    if (rc.pcnt && tid == 0) rc.pcnt[k] = 0;  // the pair's contact count (k_cert_survivors)
     const int32_t a = pa[k], b = pb[k];
     if (a < 0 || b < 0) continue;
     const int64_t tA0 = m.tri_offset[a], tB0 = m.tri_offset[b];
@@ -562,6 +572,67 @@ __global__ void k_gather_fixed(RawContacts rc, const int64_t *perm, delta_contac
   out.tri_b[j] = rc.i[3 * cap + s];
   out.penetration[j] = 1;
   out.friction[j] = rc.fric[s];
+}
+
+// Sort-free ordering of the fixed-capacity certified driver's contacts, step 1: contact c
+// of pair k goes to its pair's bucket, at poff[k] + its rank of arrival.
+__global__ void k_bucket_contacts(RawContacts rc, const int64_t *poff, int64_t *bidx) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long cnt = *rc.count;
+  const int64_t n = (int64_t)cnt < rc.cap ? (int64_t)cnt : rc.cap;
+  if (c >= n) return;
+  const int64_t k = (int64_t)(rc.key[c] >> (2 * rc.tbits));
+  bidx[poff[k] + rc.slot[c]] = c;
+}
+
+// Step 2, one warp per pair: the pair's contacts are ranked by key (A triangle, B
+// triangle; keys within a pair are distinct) and written to the pair's range of the
+// output, so the output is in (pair, A triangle, B triangle) order, the order of a stable
+// sort of all keys.  Thread 0 publishes the count and flags an overflow.
+__global__ void k_pair_gather(RawContacts rc, const int64_t *poff, const int64_t *bidx, int64_t n_pairs,
+                              delta_contacts out, int64_t *n_out, int *ovf, int ovf_code, int64_t *count_log) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned long long cnt = *rc.count;
+  if (warp == 0 && lane == 0) {
+    const int64_t n = (int64_t)cnt < out.capacity ? (int64_t)cnt : out.capacity;
+    *n_out = n;
+    if (count_log) *count_log = n;
+    if ((int64_t)cnt > out.capacity) atomicCAS(ovf, 0, ovf_code);
+  }
+  const int64_t cap = rc.cap, oc = out.capacity;
+  for (int64_t k = warp; k < n_pairs; k += nwarps) {
+    const int64_t base = poff[k], m = poff[k + 1] - base;
+    for (int64_t a0 = 0; a0 < m; a0 += 32) {
+      const bool valid = a0 + lane < m;
+      const int64_t s = valid ? bidx[base + a0 + lane] : 0;
+      const uint64_t key = valid ? rc.key[s] : ~0ull;
+      int64_t rank = 0;
+      for (int64_t b0 = 0; b0 < m; b0 += 32) {
+        const uint64_t kb = b0 + lane < m ? (b0 == a0 ? key : rc.key[bidx[base + b0 + lane]]) : ~0ull;
+#pragma unroll 8
+        for (int t = 0; t < 32; ++t) rank += __shfl_sync(kFull, kb, t) < key ? 1 : 0;
+      }
+      const int64_t j = base + rank;
+      if (!valid || j >= oc) continue;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        out.x[d * oc + j] = rc.f[(0 + d) * cap + s];
+        out.normal[d * oc + j] = rc.f[(3 + d) * cap + s];
+        out.P[d * oc + j] = rc.f[(7 + d) * cap + s];
+        out.Q[d * oc + j] = rc.f[(10 + d) * cap + s];
+      }
+      out.depth[j] = rc.f[6 * cap + s];
+      out.eps_total[j] = rc.f[13 * cap + s];
+      out.master[j] = rc.i[s];
+      out.slave[j] = rc.i[cap + s];
+      out.tri_a[j] = rc.i[2 * cap + s];
+      out.tri_b[j] = rc.i[3 * cap + s];
+      out.penetration[j] = 1;
+      out.friction[j] = rc.fric[s];
+    }
+  }
 }
 
 __global__ void k_accumulate(const DevStats *st, int64_t *counters) {
@@ -896,18 +967,31 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   rc.sv_count = queue + 2;
   rc.bbox = driver == DELTA_DRV_BF_CERT ? bbox : nullptr;  // the caller's boxes of the current vertices
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
-  if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");
   size_t tb = temp_bytes;
   if (driver == DELTA_DRV_BF_CERT) {
-    // the culling takes body pairs directly: no rows
+    // The culling takes body pairs directly (no rows).  The contacts are ordered without a
+    // sort: counted per pair (rows, zeroed by the culling), the counts scanned into pair
+    // offsets (row_offset), each contact put in its pair's bucket (perm_out), and each
+    // pair's bucket ranked by key.  The per-pair arrival ranks use the sort's key_out.
+    rc.pcnt = (unsigned long long *)rows;
+    rc.slot = (uint32_t *)key_out;
     e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats);
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0)) != cudaSuccess)
       return cuda_error(e, "occupancy");
     k_cert_survivors<<<(unsigned)(kNumSMs * (per_sm > 0 ? per_sm : 1)), 128, 0, s>>>(m, pa, pb, rc, dstats);
-    ctx->launches += 2;
+    if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
+      return cuda_error(e, "pair contact scan");
+    k_bucket_contacts<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out);
+    k_pair_gather<<<(unsigned)((pair_cap + 7) / 8), 256, 0, s>>>(rc, row_offset, perm_out, pair_cap, out, d_ncontacts,
+                                                                 d_ovf, ovf_code, d_count_log);
+    k_cert_tail<<<1, 1, 0, s>>>(rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters);
+    ctx->launches += 6;
+    return cuda_error(cudaGetLastError(), "detect fixed");
   } else {
+    // empty key entries sort last
+    if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");
     k_rows_fixed<<<(unsigned)((pair_cap + 256) / 256), 256, 0, s>>>(m.tri_offset, pa, pair_cap, rows);
     if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
       return cuda_error(e, "row scan");
@@ -928,10 +1012,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   k_gather_fixed<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, perm_out, out, d_ncontacts, d_ovf, ovf_code,
                                                                d_count_log);
   ctx->launches += 2;
-  if (driver == DELTA_DRV_BF_CERT) {
-    k_cert_tail<<<1, 1, 0, s>>>(rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters);
-    ctx->launches += 1;
-  } else if (d_counters) {
+  if (d_counters) {
     k_accumulate<<<1, 1, 0, s>>>(dstats, d_counters);
     ctx->launches += 1;
   }
