@@ -187,3 +187,66 @@ def test_obstacles_first_graph_equals_stepping_and_oracle(ctx, oracle, scene):
     for k in STATE:
         assert np.array_equal(r_state[k], o_state[k]), k
         assert np.array_equal(g_state[k], o_state[k]), k
+
+
+def _grid(n, x0, x1, z0, z1, y, up):
+    """n x n quads (2 n^2 triangles) over [x0, x1] x [z0, z1] at height y, normals +y
+    (`up`) or -y."""
+    xs, zs = np.linspace(x0, x1, n + 1), np.linspace(z0, z1, n + 1)
+    V = np.array([(x, y, z) for x in xs for z in zs])
+    F = []
+    for i in range(n):
+        for j in range(n):
+            a, b, c, d = i * (n + 1) + j, (i + 1) * (n + 1) + j, (i + 1) * (n + 1) + j + 1, i * (n + 1) + j + 1
+            F += [[a, c, b], [a, d, c]] if up else [[a, b, c], [a, c, d]]
+    return V, np.array(F)
+
+
+def _tile(n, x0, z0, w, h, y0):
+    """A closed w x h x w box whose bottom face (at y0) is an n x n grid of quads."""
+    from delta_b200.scenarios import _outward
+
+    Vb, Fb = _grid(n, x0, x0 + w, z0, z0 + w, y0, False)
+    c = [(x0, y0, z0), (x0 + w, y0, z0), (x0 + w, y0, z0 + w), (x0, y0, z0 + w)]
+    Vs = np.array(c + [(x, y0 + h, z) for x, _, z in c])
+    Fs = [[4, 5, 6], [4, 6, 7]]
+    for k in range(4):
+        a, b = k, (k + 1) % 4
+        Fs += [[a, b, b + 4], [a, b + 4, a + 4]]
+    V = np.concatenate([Vb, Vs])
+    return V, _outward(V, np.concatenate([Fb, np.array(Fs) + len(Vb)]))
+
+
+def test_graph_many_contacts_per_pair_equals_stepping_and_oracle(ctx, oracle):
+    """Two tiles resting face down on a finely meshed floor: 768 and 512 contacts per body
+    pair, far more than a warp, so the graph step's per-pair ordering of the contacts ranks
+    several chunks of keys.  Graph replays over several calls, stepping and the oracle give
+    the same trajectory and contact list bit for bit."""
+    from delta_b200.engine import Simulation, StepParams
+    from delta_b200.scenarios import build_scene
+
+    eps = 1e-4
+    sc = build_scene([_tile(8, -0.045, -0.02, 0.04, 0.01, 2 * eps - 6e-7),
+                      _tile(8, 0.0051, -0.02, 0.04, 0.01, 2 * eps - 4e-7)],
+                     obstacles=[_grid(12, -0.06, 0.06, -0.06, 0.06, 0.0, True)], eps=eps)
+    prm = dict(PARAMS, spring=1e3)  # a softer spring: hundreds of contacts act on each tile
+    o_state, o_cps, o_c = oracle.simulate(sc, prm["dt"], prm["gravity"], prm["spring"], prm["damper"],
+                                          prm["friction"], 20)
+    p = StepParams.make(**prm)
+    ref = Simulation(ctx, sc, 8)
+    r_cps = ref.step(20, p)
+    r_state = ref.state()
+    ref.close()
+    sim = Simulation(ctx, sc, 8)
+    g_cps = np.concatenate([sim.step(n, p, graph=True) for n in (1, 4, 15)])
+    g_state, g_c = sim.state(), sim.contacts()
+    sim.close()
+    per_pair = np.unique(np.stack([g_c["master"], g_c["slave"]]), axis=1, return_counts=True)[1]
+    assert per_pair.max() > 256, per_pair
+    assert list(r_cps) == list(o_cps) and list(g_cps) == list(o_cps)
+    for k in STATE:
+        assert np.array_equal(r_state[k], o_state[k]), k
+        assert np.array_equal(g_state[k], o_state[k]), k
+    assert len(g_c) == len(o_c)
+    for f in FIELDS:
+        assert np.array_equal(g_c[f], o_c[f]), f
