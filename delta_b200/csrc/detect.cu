@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "internal.h"
+#include "pose.cuh"
 #include "tri_cert.cuh"
 #include "tri_gjk.cuh"
 #include "tri_ref.cuh"
@@ -36,6 +37,9 @@ struct RawContacts {
   unsigned long long *sv_count;
   // certified driver: per-body boxes (lo[3], hi[3]) for the culling, or null
   const double *bbox;
+  // certified driver: with pose.rx set, the vertices are formed from the bodies' poses (the
+  // mesh arrays are not current) and the body boxes come from pose_box
+  Pose pose;
   // sort key of a contact: pair << 2 tbits | A triangle << tbits | B triangle
   int tbits;
   // fixed-capacity certified driver: contacts counted per pair (pcnt, zeroed by the culling)
@@ -79,6 +83,14 @@ __device__ __forceinline__ void load_tri64(const delta_meshes &m, int64_t t, dou
     T[v][1] = __ldg(m.y + 3 * t + v);
     T[v][2] = __ldg(m.z + 3 * t + v);
   }
+}
+
+// Triangle t of body `body`, current vertices: formed from the pose when one is given and
+// the body moves, read from the meshes otherwise.
+__device__ __forceinline__ void load_tri_cur(const delta_meshes &m, const Pose &P, int32_t body, int64_t t,
+                                             double T[3][3]) {
+  if (P.rx && !P.obstacle[body]) posed_tri(P, body_pose(P, body), t, T);
+  else load_tri64(m, t, T);
 }
 
 // The per-triangle-pair solver of each driver.  Returns closest points (FP64 values).
@@ -378,9 +390,11 @@ __device__ __forceinline__ double box_gap2(const double alo[3], const double ahi
 
 // Stages the triangles cur, cur+1, ... of (t0, n) whose box lies within the cull distance
 // of the box (olo, ohi) into L (in any order), kCullThreads at a time while L can take
-// that many more; returns the cursor.  Called by the whole block.
-__device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, int64_t t0, int32_t n, int32_t cur,
-                                             const double olo[3], const double ohi[3], double cull2, CullList &L) {
+// that many more; returns the cursor.  Called by the whole block.  With `q` (the body's
+// pose, in shared memory) the vertices are formed from the reference vertices.
+__device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, const Pose &P, const BodyPose *q, int64_t t0,
+                                             int32_t n, int32_t cur, const double olo[3], const double ohi[3],
+                                             double cull2, CullList &L) {
   const int tid = threadIdx.x, lane = tid & 31;
   if (tid == 0) L.n = 0;
   __syncthreads();
@@ -390,7 +404,8 @@ __device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, int64_t t0, 
     bool keep = false;
     if (i < n) {
       double T[3][3];
-      load_tri64(m, t0 + i, T);
+      if (q) posed_tri(P, *q, t0 + i, T);
+      else load_tri64(m, t0 + i, T);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         lo[k] = fmin(T[0][k], fmin(T[1][k], T[2][k]));
@@ -419,12 +434,14 @@ __device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, int64_t t0, 
 
 // Pairs k = block, block + n_blocks, ... (entries with a negative body are empty).
 // Survivor keys (pair << 32 | A triangle << 16 | B triangle) go to rc.sv; their order is
-// free (the contacts are sorted by key afterwards).  rc.bbox holds the body boxes of the
-// current vertices (null: no body-box tests).
+// free (the contacts are ordered by key afterwards).  With rc.pose the vertices are formed
+// from the bodies' poses and the body boxes come from pose_box; otherwise rc.bbox holds
+// the body boxes of the current vertices (null: no body-box tests).
 __global__ void __launch_bounds__(kCullThreads) k_cull_pairs(delta_meshes m, const int32_t *__restrict__ pa,
                                                              const int32_t *__restrict__ pb, int64_t n_pairs,
                                                              RawContacts rc, DevStats *st) {
   __shared__ CullList LA, LB;
+  __shared__ BodyPose QA, QB;
   const int tid = threadIdx.x;
   if (rc.pcnt && blockIdx.x == 0 && tid == 0) rc.pcnt[n_pairs] = 0;
   for (int64_t k = blockIdx.x; k < n_pairs; k += gridDim.x) {
@@ -437,20 +454,30 @@ __global__ void __launch_bounds__(kCullThreads) k_cull_pairs(delta_meshes m, con
     const double mg = (xf64(m.eps[a]) + xf64(m.eps[b])).v;
     const double cull = mg * (1.0 + 1e-9) + 1e-12, cull2 = cull * cull;
     double Alo[3], Ahi[3], Blo[3], Bhi[3];
+    const Pose &P = rc.pose;
+    if (P.rx) {
+      pose_box(P, a, Alo, Ahi);
+      pose_box(P, b, Blo, Bhi);
+    } else {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      Alo[c] = rc.bbox ? rc.bbox[6 * (int64_t)a + c] : -INFINITY;
-      Ahi[c] = rc.bbox ? rc.bbox[6 * (int64_t)a + 3 + c] : INFINITY;
-      Blo[c] = rc.bbox ? rc.bbox[6 * (int64_t)b + c] : -INFINITY;
-      Bhi[c] = rc.bbox ? rc.bbox[6 * (int64_t)b + 3 + c] : INFINITY;
+      for (int c = 0; c < 3; ++c) {
+        Alo[c] = rc.bbox ? rc.bbox[6 * (int64_t)a + c] : -INFINITY;
+        Ahi[c] = rc.bbox ? rc.bbox[6 * (int64_t)a + 3 + c] : INFINITY;
+        Blo[c] = rc.bbox ? rc.bbox[6 * (int64_t)b + c] : -INFINITY;
+        Bhi[c] = rc.bbox ? rc.bbox[6 * (int64_t)b + 3 + c] : INFINITY;
+      }
     }
     if (box_gap2(Alo, Ahi, Blo, Bhi) > cull2) continue;
+    const bool moveA = P.rx && !P.obstacle[a], moveB = P.rx && !P.obstacle[b];
+    if (tid == 0 && moveA) QA = body_pose(P, a);
+    if (tid == 1 && moveB) QB = body_pose(P, b);
+    __syncthreads();  // the poses are read by cull_fill (which synchronises before refilling)
     for (int32_t cb = 0; cb < nB;) {
-      cb = cull_fill(m, tB0, nB, cb, Alo, Ahi, cull2, LB);
+      cb = cull_fill(m, P, moveB ? &QB : nullptr, tB0, nB, cb, Alo, Ahi, cull2, LB);
       const int nLB = LB.n;
       if (nLB == 0) continue;
       for (int32_t ca = 0; ca < nA;) {
-        ca = cull_fill(m, tA0, nA, ca, Blo, Bhi, cull2, LA);
+        ca = cull_fill(m, P, moveA ? &QA : nullptr, tA0, nA, ca, Blo, Bhi, cull2, LA);
         const int np = LA.n * nLB;
         for (int j = tid; j < np; j += kCullThreads) {
           const int ia = j / nLB, ib = j - ia * nLB;
@@ -508,8 +535,8 @@ __global__ void __launch_bounds__(128) k_cert_survivors(delta_meshes m, const in
     r.idB = m.id[b];
     r.fric = (m.friction[a] && m.friction[b]) ? 1 : 0;
     double A[3][3], B[3][3], pq[6];
-    load_tri64(m, r.tA, A);
-    load_tri64(m, r.tB0 + tb, B);
+    load_tri_cur(m, rc.pose, a, r.tA, A);
+    load_tri_cur(m, rc.pose, b, r.tB0 + tb, B);
     bf_cert_warp(A, B, valid, pq, sm[warp]);
     const double mg = (xf64(r.epsA) + xf64(r.epsB)).v;
     const bool take = valid && pq_dist64(pq) <= mg;  // bf.cpp:125
@@ -739,7 +766,7 @@ cudaError_t launch_detect_prec(int driver, cudaStream_t s, const delta_meshes &m
 // Scratch slots used here: 2 rows/row_offset, 3 raw contacts, 4 sort buffers, 5 small state.
 delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
-                        delta_stats *stats, int64_t *counters, const double *bbox) {
+                        delta_stats *stats, int64_t *counters, const Pose *pose) {
   cudaStream_t s = ctx->stream;
   delta_status st;
   cudaError_t e;
@@ -786,8 +813,8 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   unsigned long long hcount = 0;
   RawContacts rc{};
   rc.tbits = 16;
-  if (driver == DELTA_DRV_BF_CERT && bbox) {
-    rc.bbox = bbox;  // the caller's boxes of every body in the pairs
+  if (driver == DELTA_DRV_BF_CERT && pose) {
+    rc.pose = *pose;  // current vertices and body boxes from the bodies' poses
   } else if (driver == DELTA_DRV_BF_CERT) {
     // body boxes of the current vertices for the culling
     void *bb = nullptr;
@@ -939,7 +966,7 @@ delta_status detect_fixed_init(cudaStream_t s, void *state, int64_t pair_cap, in
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
-                              void *temp, size_t temp_bytes, const double *bbox, int tri_bits) {
+                              void *temp, size_t temp_bytes, const Pose *pose, int tri_bits) {
   cudaError_t e;
   const int64_t cap = out.capacity;
   char *p = (char *)state;
@@ -965,7 +992,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   rc.sv = (uint64_t *)p;
   rc.sv_cap = fixed_sv_cap(cap);
   rc.sv_count = queue + 2;
-  rc.bbox = driver == DELTA_DRV_BF_CERT ? bbox : nullptr;  // the caller's boxes of the current vertices
+  if (driver == DELTA_DRV_BF_CERT && pose) rc.pose = *pose;  // vertices and body boxes from the poses
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
   size_t tb = temp_bytes;
   if (driver == DELTA_DRV_BF_CERT) {

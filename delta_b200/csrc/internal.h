@@ -39,16 +39,19 @@ cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t 
 cudaError_t launch_pairs(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,
                          int64_t ld, double max_error, double *p, double *q, double *dist, uint8_t *flags);
 
-// Particle-pair drivers (detect.cu).  `bbox`: the certified driver's body boxes
-// (lo[3], hi[3]) of the current vertices of every body in the pairs, written by the
-// caller, or null (then computed here for all bodies).
+struct Pose;  // pose.cuh
+
+// Particle-pair drivers (detect.cu).  `pose`: for the certified driver, the bodies' poses
+// from which the current vertices and the body boxes are formed (the meshes' vertex arrays
+// need not be current), or null (then the meshes' vertices are read and the body boxes
+// computed from them).
 delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
-                        delta_stats *stats, int64_t *counters = nullptr, const double *bbox = nullptr);
+                        delta_stats *stats, int64_t *counters = nullptr, const Pose *pose = nullptr);
 
-// Fixed-capacity (graph-capturable) detection (detect.cu).  `bbox`: the boxes (lo[3], hi[3])
-// of every body's current vertices, written by the caller, for the certified driver's
-// culling, or null.  `tri_bits`: bits of a triangle index within a body (every body has
+// Fixed-capacity (graph-capturable) detection (detect.cu).  `pose`: as for detect_run
+// (null: the certified driver reads the meshes' vertices and culls without body boxes).
+// `tri_bits`: bits of a triangle index within a body (every body has
 // fewer than 2^tri_bits triangles), used to pack the contact sort keys.
 size_t detect_fixed_temp_bytes(int64_t pair_cap, int64_t cap);
 size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap);
@@ -57,7 +60,7 @@ delta_status detect_fixed_init(cudaStream_t s, void *state, int64_t pair_cap, in
 delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const delta_meshes &m, const int32_t *pa,
                               const int32_t *pb, int64_t pair_cap, const delta_contacts &out, int64_t *d_ncontacts,
                               int *d_ovf, int ovf_code, int64_t *d_counters, int64_t *d_count_log, void *state,
-                              void *temp, size_t temp_bytes, const double *bbox = nullptr, int tri_bits = 16);
+                              void *temp, size_t temp_bytes, const Pose *pose = nullptr, int tri_bits = 16);
 
 // Thread-local last-error text (capi.cu).
 delta_status set_error(delta_status st, const std::string &msg);

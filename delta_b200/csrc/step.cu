@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "pose.cuh"
 #include "real.cuh"
 
 namespace delta {
@@ -521,10 +522,7 @@ __global__ void k_vertices(delta_scene s, const int *ovf, double *bbox, const ui
         const int64_t v = base + 32 * u;
         if (v < v1) {
           if (move) {
-            const X C0 = X(c[u][0]) - rp[0], C1 = X(c[u][1]) - rp[1], C2 = X(c[u][2]) - rp[2];
-            c[u][0] = (pos[0] + (R[0] * C0 + R[3] * C1 + R[6] * C2)).v;
-            c[u][1] = (pos[1] + (R[1] * C0 + R[4] * C1 + R[7] * C2)).v;
-            c[u][2] = (pos[2] + (R[2] * C0 + R[5] * C1 + R[8] * C2)).v;
+            posed_point(R, pos, rp, c[u][0], c[u][1], c[u][2], c[u]);
             s.x[v] = c[u][0];
             s.y[v] = c[u][1];
             s.z[v] = c[u][2];
@@ -575,6 +573,47 @@ __global__ void k_mark_pair_bodies(const int32_t *pa, const int32_t *pb, int64_t
   const int32_t a = pa[t], b = pb[t];
   if (a >= 0) stamp[a] = e;
   if (b >= 0) stamp[b] = e;
+}
+
+// Once per simulation, one warp per body: a moving body's reach, the largest |r - ref_pos|
+// over its reference vertices (each difference rounded as the vertex update rounds it),
+// and an obstacle's box (lo[3], hi[3]) of its vertices, which never move.
+__global__ void k_reach_boxes(delta_scene s, double *reach, double *obox) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int32_t n = s.n_bodies;
+  for (int64_t i = warp; i < n; i += nwarps) {
+    const bool obst = s.obstacle[i] != 0;
+    double rp[3], r2 = 0.0, lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int k = 0; k < 3; ++k) rp[k] = s.ref_pos[(int64_t)k * n + i];
+    for (int64_t v = 3 * s.tri_offset[i] + lane; v < 3 * s.tri_offset[i + 1]; v += 32) {
+      if (obst) {
+        const double c[3] = {s.x[v], s.y[v], s.z[v]};
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = fmin(lo[k], c[k]);
+          hi[k] = fmax(hi[k], c[k]);
+        }
+      } else {
+        const double d0 = (X(s.rx[v]) - X(rp[0])).v, d1 = (X(s.ry[v]) - X(rp[1])).v, d2 = (X(s.rz[v]) - X(rp[2])).v;
+        r2 = fmax(r2, d0 * d0 + d1 * d1 + d2 * d2);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+        hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+      }
+    }
+    if (lane == 0) {
+      reach[i] = sqrt(r2) * (1.0 + 1e-12);
+      for (int k = 0; k < 3; ++k) {
+        obox[6 * i + k] = lo[k];
+        obox[6 * i + 3 + k] = hi[k];
+      }
+    }
+  }
 }
 
 inline unsigned vertex_blocks(int32_t n_bodies) {
@@ -1102,7 +1141,10 @@ struct delta_sim {
   // pairs get their vertices updated (stamp[i] == *epoch); every vertex is brought up to
   // date at the end of the call.  [n] stamps, then the epoch.
   uint32_t *stamp = nullptr, *epoch = nullptr;
-  double *bbox = nullptr;  // body boxes of the stepped certified driver, from k_vertices
+  // The certified driver reads no vertex array during a call: it forms the vertices from
+  // the bodies' poses (pose.cuh).  reach: per body, the bound on |r - ref_pos|; obox: the
+  // boxes of the obstacles (static), by body.
+  double *reach = nullptr, *obox = nullptr;
   // contacts of the last detection
   delta_contacts c{};
   void *c_mem = nullptr;
@@ -1123,7 +1165,6 @@ struct delta_sim {
     size_t temp_bytes = 0;
     delta_contacts c{};
     int64_t *d_nc = nullptr, *d_step = nullptr, *d_cnt = nullptr, *d_log = nullptr;
-    double *bbox = nullptr;  // body boxes (written by k_vertices) for the certified driver's culling
     int *d_ovf = nullptr, *d_snap = nullptr;
     int64_t *d_bp = nullptr;  // candidate body pairs summed over the replayed steps
     int64_t log_len = 0;
@@ -1182,6 +1223,12 @@ static delta_status sim_all_vertices(delta_sim *s, cudaStream_t st) {
   return cuda_error(cudaGetLastError(), "vertex update");
 }
 
+// The poses of the simulation's bodies, for the certified driver.
+static Pose sim_pose(const delta_sim *s) {
+  const delta_scene &c = s->scene;
+  return Pose{c.rx, c.ry, c.rz, c.rot, c.pos, c.ref_pos, c.obstacle, s->reach, s->obox, c.n_bodies};
+}
+
 static delta_status sim_detect(delta_sim *s) {
   delta_status ds;
   int64_t np = 0;
@@ -1192,13 +1239,17 @@ static delta_status sim_detect(delta_sim *s) {
   }
   if (ds != DELTA_OK) return ds;
   s->counters[1] += np;
-  // vertices of the bodies the narrowphase reads
-  cudaStream_t st = s->ctx->stream;
-  k_next_epoch<<<1, 1, 0, st>>>(s->epoch);
-  if (np > 0) k_mark_pair_bodies<<<blocks_for(np), 256, 0, st>>>(s->pa, s->pb, np, s->epoch, s->stamp);
-  double *bbox = s->driver == DELTA_DRV_BF_CERT ? s->bbox : nullptr;
-  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, nullptr, bbox, s->stamp, s->epoch);
-  s->ctx->launches += np > 0 ? 3 : 2;
+  // vertices of the bodies the narrowphase reads: formed from the poses by the certified
+  // driver, updated here for the others
+  const bool posed = s->driver == DELTA_DRV_BF_CERT;
+  const Pose pose = sim_pose(s);
+  if (!posed) {
+    cudaStream_t st = s->ctx->stream;
+    k_next_epoch<<<1, 1, 0, st>>>(s->epoch);
+    if (np > 0) k_mark_pair_bodies<<<blocks_for(np), 256, 0, st>>>(s->pa, s->pb, np, s->epoch, s->stamp);
+    k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, nullptr, nullptr, s->stamp, s->epoch);
+    s->ctx->launches += np > 0 ? 3 : 2;
+  }
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
                  s->scene.eps,      s->scene.friction,   s->ids};
   int64_t nc = 0;
@@ -1207,11 +1258,13 @@ static delta_status sim_detect(delta_sim *s) {
     return DELTA_OK;
   }
   int64_t cnt[2] = {0, 0};
-  ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt, bbox);
+  ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt,
+                    posed ? &pose : nullptr);
   if (ds == DELTA_ERR_CAPACITY) {
     if ((ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;
     cnt[0] = cnt[1] = 0;
-    ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt, bbox);
+    ds = detect_run(s->ctx, s->driver, DELTA_F64, m, s->pa, s->pb, np, &s->c, &nc, nullptr, cnt,
+                    posed ? &pose : nullptr);
   }
   s->counters[2] += cnt[0];
   s->counters[3] += cnt[1];
@@ -1226,10 +1279,9 @@ static void graph_release(delta_sim::Graph &g) {
   g.exec = nullptr;
   g.graph = nullptr;
   g.captured = false;
-  for (void *p : {(void *)g.pa, g.bp, g.fs, g.ds, g.temp, g.c_mem, g.dev, (void *)g.bbox})
+  for (void *p : {(void *)g.pa, g.bp, g.fs, g.ds, g.temp, g.c_mem, g.dev})
     if (p) cudaFree(p);
   g.pa = g.pb = nullptr;
-  g.bbox = nullptr;
   g.bp = g.fs = g.ds = g.temp = g.c_mem = g.dev = nullptr;
 }
 
@@ -1252,8 +1304,7 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
       (e = cudaMalloc(&g.fs, forces_fixed_state_bytes(contact_cap, n))) != cudaSuccess ||
       (e = cudaMalloc(&g.ds, detect_fixed_state_bytes(pair_cap, contact_cap))) != cudaSuccess ||
       (e = cudaMalloc(&g.temp, g.temp_bytes)) != cudaSuccess || (e = cudaMalloc(&g.c_mem, cbytes)) != cudaSuccess ||
-      (e = cudaMalloc(&g.dev, 256 + sizeof(int64_t) * (size_t)log_len)) != cudaSuccess ||
-      (e = cudaMalloc(&g.bbox, 48 * (size_t)n + 64)) != cudaSuccess)
+      (e = cudaMalloc(&g.dev, 256 + sizeof(int64_t) * (size_t)log_len)) != cudaSuccess)
     return cuda_error(e, "graph buffers");
   g.pb = g.pa + pair_cap;
   double *d = (double *)g.c_mem;
@@ -1289,20 +1340,25 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_bp, g.bp, g.temp,
                                  g.temp_bytes, k)) != DELTA_OK)
     return ds;
-  // vertices (and boxes) of the bodies the narrowphase reads this step
-  k_mark_pair_bodies<<<blocks_for(g.pair_cap), 256, 0, st>>>(g.pa, g.pb, g.pair_cap, s->epoch, s->stamp);
-  k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(
-      s->scene, g.d_ovf, s->driver == DELTA_DRV_BF_CERT ? g.bbox : nullptr, s->stamp, s->epoch);
+  // vertices of the bodies the narrowphase reads this step: formed from the poses by the
+  // certified driver, updated here for the others
+  const bool posed = s->driver == DELTA_DRV_BF_CERT;
+  const Pose pose = sim_pose(s);
+  if (!posed) {
+    k_mark_pair_bodies<<<blocks_for(g.pair_cap), 256, 0, st>>>(g.pa, g.pb, g.pair_cap, s->epoch, s->stamp);
+    k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, g.d_ovf, nullptr, s->stamp, s->epoch);
+    k += 2;
+  }
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
                  s->scene.eps,      s->scene.friction,   s->ids};
   const int64_t before = s->ctx->launches;
   if ((ds = detect_run_fixed(s->ctx, st, s->driver, m, g.pa, g.pb, g.pair_cap, g.c, g.d_nc, g.d_ovf, 1, g.d_cnt,
-                             nullptr, g.ds, g.temp, g.temp_bytes, g.bbox, s->tri_bits)) != DELTA_OK)
+                             nullptr, g.ds, g.temp, g.temp_bytes, posed ? &pose : nullptr, s->tri_bits)) != DELTA_OK)
     return ds;
   k += (int)(s->ctx->launches - before);
   s->ctx->launches = before;
   k_step_end<<<1, 1, 0, st>>>(g.d_snap, g.d_nc, g.d_log, g.log_len, g.d_step);
-  g.kernels = k + 4;
+  g.kernels = k + 2;
   return cuda_error(cudaGetLastError(), "graph step");
 }
 
@@ -1412,7 +1468,12 @@ delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driv
                          (e = cudaMemset(s->stamp, 0, sizeof(uint32_t) * ((size_t)n + 1))) != cudaSuccess))
     ds = cuda_error(e, "vertex stamps");
   if (ds == DELTA_OK) s->epoch = s->stamp + n;
-  if (ds == DELTA_OK && (e = cudaMalloc(&s->bbox, 48 * (size_t)n + 64)) != cudaSuccess) ds = cuda_error(e, "boxes");
+  if (ds == DELTA_OK && (e = cudaMalloc(&s->reach, 56 * (size_t)n + 64)) != cudaSuccess) ds = cuda_error(e, "reach");
+  if (ds == DELTA_OK) {
+    s->obox = s->reach + n;
+    k_reach_boxes<<<vertex_blocks(n), 256, 0, ctx->stream>>>(*scene, s->reach, s->obox);
+    ctx->launches += 1;
+  }
   if (ds == DELTA_OK && (e = cudaMalloc(&s->F, sizeof(double) * 6 * n + n)) != cudaSuccess) ds = cuda_error(e, "F");
   if (ds == DELTA_OK) {
     s->T = s->F + 3 * n;
@@ -1613,7 +1674,7 @@ delta_status delta_sim_destroy(delta_sim *s) {
   s->plan.release();
   if (s->ids) cudaFree(s->ids);
   if (s->stamp) cudaFree(s->stamp);
-  if (s->bbox) cudaFree(s->bbox);
+  if (s->reach) cudaFree(s->reach);
   if (s->F) cudaFree(s->F);
   if (s->c_mem) cudaFree(s->c_mem);
   if (s->pa) cudaFree(s->pa);

@@ -236,9 +236,10 @@ delta_status delta_broadphase(delta_ctx *ctx, const delta_scene *scene, int32_t 
  * the multiscale order: forces from the previous detection's contacts, velocity and
  * angular update, move, then broadphase and narrowphase with `driver`.  Within a call,
  * a step updates the vertices (updateVertices) of only the bodies of its candidate pairs,
- * the only vertices the narrowphase reads; all vertices are updated at the end of the
- * call, so the scene's vertex arrays equal those of a per-step full update whenever a
- * call returns. */
+ * the only vertices the narrowphase reads (the certified driver updates none: it forms
+ * the vertices it reads from the bodies' poses with the same arithmetic); all vertices
+ * are updated at the end of the call, so the scene's vertex arrays equal those of a
+ * per-step full update whenever a call returns. */
 typedef struct delta_sim delta_sim;
 delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driver, delta_sim **out);
 delta_status delta_sim_step(delta_sim *sim, const delta_step_params *params, int32_t nsteps,
