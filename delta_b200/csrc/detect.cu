@@ -437,7 +437,7 @@ __device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, const Pose &
 // free (the contacts are ordered by key afterwards).  With rc.pose the vertices are formed
 // from the bodies' poses and the body boxes come from pose_box; otherwise rc.bbox holds
 // the body boxes of the current vertices (null: no body-box tests).
-__global__ void __launch_bounds__(kCullThreads) k_cull_pairs(delta_meshes m, const int32_t *__restrict__ pa,
+__global__ void __launch_bounds__(kCullThreads, 8) k_cull_pairs(delta_meshes m, const int32_t *__restrict__ pa,
                                                              const int32_t *__restrict__ pb, int64_t n_pairs,
                                                              RawContacts rc, DevStats *st) {
   __shared__ CullList LA, LB;
@@ -509,7 +509,7 @@ inline cudaError_t launch_cull(cudaStream_t s, const delta_meshes &m, const int3
 }
 
 // Certified bf over the survivors of the box test, 32 per warp (any mix of pairs).
-__global__ void __launch_bounds__(128) k_cert_survivors(delta_meshes m, const int32_t *__restrict__ pa,
+__global__ void __launch_bounds__(128, 5) k_cert_survivors(delta_meshes m, const int32_t *__restrict__ pa,
                                                         const int32_t *__restrict__ pb, RawContacts rc,
                                                         DevStats *st) {
   __shared__ CertWarpSmem sm[4];
