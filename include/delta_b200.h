@@ -239,7 +239,10 @@ delta_status delta_broadphase(delta_ctx *ctx, const delta_scene *scene, int32_t 
  * the only vertices the narrowphase reads (the certified driver updates none: it forms
  * the vertices it reads from the bodies' poses with the same arithmetic); all vertices
  * are updated at the end of the call, so the scene's vertex arrays equal those of a
- * per-step full update whenever a call returns. */
+ * per-step full update whenever a call returns.  The scene's buffers stay the caller's;
+ * the simulation reads the obstacles' vertices (their boxes) and the reference vertices
+ * and centres (each body's reach) once, at creation, so those must not change while it
+ * exists (in the reference they never do). */
 typedef struct delta_sim delta_sim;
 delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driver, delta_sim **out);
 delta_status delta_sim_step(delta_sim *sim, const delta_step_params *params, int32_t nsteps,
