@@ -602,64 +602,62 @@ __global__ void k_gather_fixed(RawContacts rc, const int64_t *perm, delta_contac
 }
 
 // Sort-free ordering of the fixed-capacity certified driver's contacts, step 1: contact c
-// of pair k goes to its pair's bucket, at poff[k] + its rank of arrival.
-__global__ void k_bucket_contacts(RawContacts rc, const int64_t *poff, int64_t *bidx) {
+// of pair k goes to its pair's bucket, at poff[k] + its rank of arrival, with its key.
+__global__ void k_bucket_contacts(RawContacts rc, const int64_t *poff, int64_t *bidx, uint64_t *bkey) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long cnt = *rc.count;
   const int64_t n = (int64_t)cnt < rc.cap ? (int64_t)cnt : rc.cap;
   if (c >= n) return;
-  const int64_t k = (int64_t)(rc.key[c] >> (2 * rc.tbits));
-  bidx[poff[k] + rc.slot[c]] = c;
+  const uint64_t key = rc.key[c];
+  const int64_t j = poff[(int64_t)(key >> (2 * rc.tbits))] + rc.slot[c];
+  bidx[j] = c;
+  bkey[j] = key;
 }
 
-// Step 2, one warp per pair: the pair's contacts are ranked by key (A triangle, B
-// triangle; keys within a pair are distinct) and written to the pair's range of the
-// output, so the output is in (pair, A triangle, B triangle) order, the order of a stable
-// sort of all keys.  Thread 0 publishes the count and flags an overflow.
-__global__ void k_pair_gather(RawContacts rc, const int64_t *poff, const int64_t *bidx, int64_t n_pairs,
-                              delta_contacts out, int64_t *n_out, int *ovf, int ovf_code, int64_t *count_log) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+// Step 2, one thread per bucket entry j: its pair k is the last with poff[k] <= j, its
+// rank the number of smaller keys in the pair's bucket (keys within a pair are distinct),
+// and the contact is written at poff[k] + rank, so the output is in (pair, A triangle,
+// B triangle) order, the order of a stable sort of all keys.  Thread 0 publishes the
+// count and flags an overflow.
+__global__ void k_pair_gather(RawContacts rc, const int64_t *poff, const int64_t *bidx, const uint64_t *bkey,
+                              int64_t n_pairs, delta_contacts out, int64_t *n_out, int *ovf, int ovf_code,
+                              int64_t *count_log) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long cnt = *rc.count;
-  if (warp == 0 && lane == 0) {
+  if (j == 0) {
     const int64_t n = (int64_t)cnt < out.capacity ? (int64_t)cnt : out.capacity;
     *n_out = n;
     if (count_log) *count_log = n;
     if ((int64_t)cnt > out.capacity) atomicCAS(ovf, 0, ovf_code);
   }
-  const int64_t cap = rc.cap, oc = out.capacity;
-  for (int64_t k = warp; k < n_pairs; k += nwarps) {
-    const int64_t base = poff[k], m = poff[k + 1] - base;
-    for (int64_t a0 = 0; a0 < m; a0 += 32) {
-      const bool valid = a0 + lane < m;
-      const int64_t s = valid ? bidx[base + a0 + lane] : 0;
-      const uint64_t key = valid ? rc.key[s] : ~0ull;
-      int64_t rank = 0;
-      for (int64_t b0 = 0; b0 < m; b0 += 32) {
-        const uint64_t kb = b0 + lane < m ? (b0 == a0 ? key : rc.key[bidx[base + b0 + lane]]) : ~0ull;
-#pragma unroll 8
-        for (int t = 0; t < 32; ++t) rank += __shfl_sync(kFull, kb, t) < key ? 1 : 0;
-      }
-      const int64_t j = base + rank;
-      if (!valid || j >= oc) continue;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        out.x[d * oc + j] = rc.f[(0 + d) * cap + s];
-        out.normal[d * oc + j] = rc.f[(3 + d) * cap + s];
-        out.P[d * oc + j] = rc.f[(7 + d) * cap + s];
-        out.Q[d * oc + j] = rc.f[(10 + d) * cap + s];
-      }
-      out.depth[j] = rc.f[6 * cap + s];
-      out.eps_total[j] = rc.f[13 * cap + s];
-      out.master[j] = rc.i[s];
-      out.slave[j] = rc.i[cap + s];
-      out.tri_a[j] = rc.i[2 * cap + s];
-      out.tri_b[j] = rc.i[3 * cap + s];
-      out.penetration[j] = 1;
-      out.friction[j] = rc.fric[s];
-    }
+  if (j >= poff[n_pairs]) return;
+  int64_t lo = 0, hi = n_pairs;  // poff[0] = 0 <= j < poff[n_pairs]
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if (poff[mid] <= j) lo = mid;
+    else hi = mid - 1;
   }
+  const int64_t base = poff[lo], m = poff[lo + 1] - base;
+  const uint64_t key = bkey[j];
+  int64_t rank = 0;
+  for (int64_t i = 0; i < m; ++i) rank += bkey[base + i] < key ? 1 : 0;
+  const int64_t d = base + rank, s = bidx[j], cap = rc.cap, oc = out.capacity;
+  if (d >= oc) return;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    out.x[k * oc + d] = rc.f[(0 + k) * cap + s];
+    out.normal[k * oc + d] = rc.f[(3 + k) * cap + s];
+    out.P[k * oc + d] = rc.f[(7 + k) * cap + s];
+    out.Q[k * oc + d] = rc.f[(10 + k) * cap + s];
+  }
+  out.depth[d] = rc.f[6 * cap + s];
+  out.eps_total[d] = rc.f[13 * cap + s];
+  out.master[d] = rc.i[s];
+  out.slave[d] = rc.i[cap + s];
+  out.tri_a[d] = rc.i[2 * cap + s];
+  out.tri_b[d] = rc.i[3 * cap + s];
+  out.penetration[d] = 1;
+  out.friction[d] = rc.fric[s];
 }
 
 __global__ void k_accumulate(const DevStats *st, int64_t *counters) {
@@ -998,7 +996,8 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   if (driver == DELTA_DRV_BF_CERT) {
     // The culling takes body pairs directly (no rows).  The contacts are ordered without a
     // sort: counted per pair (rows, zeroed by the culling), the counts scanned into pair
-    // offsets (row_offset), each contact put in its pair's bucket (perm_out), and each
+    // offsets (row_offset), each contact put in its pair's bucket (indices in perm_out,
+    // keys in perm_in, whose identity permutation serves only the other driver), and each
     // pair's bucket ranked by key.  The per-pair arrival ranks use the sort's key_out.
     rc.pcnt = (unsigned long long *)rows;
     rc.slot = (uint32_t *)key_out;
@@ -1010,9 +1009,10 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
     k_cert_survivors<<<(unsigned)(kNumSMs * (per_sm > 0 ? per_sm : 1)), 128, 0, s>>>(m, pa, pb, rc, dstats);
     if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
       return cuda_error(e, "pair contact scan");
-    k_bucket_contacts<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out);
-    k_pair_gather<<<(unsigned)((pair_cap + 7) / 8), 256, 0, s>>>(rc, row_offset, perm_out, pair_cap, out, d_ncontacts,
-                                                                 d_ovf, ovf_code, d_count_log);
+    k_bucket_contacts<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out, (uint64_t *)perm_in);
+    k_pair_gather<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out, (const uint64_t *)perm_in,
+                                                                pair_cap, out, d_ncontacts, d_ovf, ovf_code,
+                                                                d_count_log);
     k_cert_tail<<<1, 1, 0, s>>>(rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters);
     ctx->launches += 6;
     return cuda_error(cudaGetLastError(), "detect fixed");
