@@ -90,6 +90,14 @@ def header_functions() -> list[str]:
     return sorted(set(re.findall(r"\b(delta_\w+)\s*\(", text)))
 
 
+def header_define(name: str) -> int:
+    """Integer value of a ``#define`` in include/delta_b200.h."""
+    m = re.search(rf"#define\s+{name}\s+(\d+)", HEADER.read_text())
+    if not m:
+        raise KeyError(name)
+    return int(m.group(1))
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is not None:

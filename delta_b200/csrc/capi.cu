@@ -177,10 +177,6 @@ delta_status delta_synchronize(delta_ctx *ctx) {
 
 int64_t delta_launch_count(const delta_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
-static PairLaunch ctx_pair_launch(const delta_ctx *ctx, int method, int precision) {
-  return ctx->pair_launch_set[method][precision] ? ctx->pair_launch[method][precision] : default_pair_launch(method);
-}
-
 static delta_status check_pairs(delta_ctx *ctx, int method, int precision, int64_t n, const void *a, const void *b,
                                 int64_t ld, const void *p, const void *q, const void *dist) {
   if (!ctx) return set_error(DELTA_ERR_INVALID, "null context");

@@ -91,6 +91,11 @@ struct delta_ctx {
 };
 
 namespace delta {
+// Launch shape of the pair kernel of (method, precision) on this context: the one set by
+// delta_set_pair_launch / delta_autotune_pairs, else the default.
+inline PairLaunch ctx_pair_launch(const delta_ctx *ctx, int method, int precision) {
+  return ctx->pair_launch_set[method][precision] ? ctx->pair_launch[method][precision] : default_pair_launch(method);
+}
 // Host-buffer pipeline: stages the pair list (a, b: 9 planes of ld doubles) through the
 // device in chunks, H2D on one copy stream, `run` on the context stream, D2H of p, q, dist
 // (and flags when given) on another, so transfers of neighbouring chunks overlap the

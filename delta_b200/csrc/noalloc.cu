@@ -2,21 +2,23 @@
 // without any device allocation.
 //
 // Some callers cannot let a library call cudaMalloc: a host that hands all device memory
-// to its own pooling allocator (a raw cudaMalloc either fails for lack of memory or
-// fragments the pool), code that records work into a CUDA graph by stream capture (a
-// blocking allocation there breaks or invalidates the capture), and latency-bound loops
-// that must not pay for an allocation.  For them this entry point stages inputs and
-// outputs in one fixed device array that is part of the library image: the CUDA driver
-// reserves it on each GPU when it loads the library's module there, and every GPU that
-// loads the library holds it until the process exits.
+// to its own pooling allocator (a raw cudaMalloc there either fails for lack of memory or
+// fragments the pool), and latency-bound loops that must not pay for an allocation or
+// for the implicit device synchronisation that cudaMalloc/cudaFree can bring.  For them
+// this entry point stages inputs and outputs in one fixed device array that is part of
+// the library image: the CUDA driver reserves it (62.8 MiB) on each GPU when it loads the
+// library's module there, and every GPU that loads the library holds it until the
+// process exits.
 //
-// The array's address is looked up once per device with cudaGetSymbolAddress (host code
-// may not use the array's name as a device address).  That lookup happens on the first
-// call on a device, which may also make the driver load the module; make that first call
-// outside any stream capture.  Every call on a device shares the one array and the array
-// keeps the previous call's contents: each call overwrites the entries it uses before
-// reading them, so nothing has to start at zero, but calls that overlap on the GPU (other
-// streams, other threads, other contexts on the same device) race for the array.
+// Host code may not use the array's name as a device address: on the host it names a
+// stand-in object.  So the first call on a device, with that device current, looks the
+// array's device address up with cudaGetSymbolAddress (which may also make the driver
+// load the module there) and keeps it for that device.  That address stays valid for the
+// life of the device's primary context; do not use this entry point across a
+// cudaDeviceReset of the device.  Every call on a device shares the one array and the
+// array keeps the previous call's contents: each call overwrites the entries it uses
+// before reading them, so nothing has to start at zero, but calls that overlap on the GPU
+// (other streams, other threads, other contexts on the same device) race for the array.
 #include <mutex>
 
 #include "internal.h"
@@ -81,7 +83,8 @@ extern "C" delta_status delta_pairs_run_host_noalloc(delta_ctx *ctx, int method,
     e = cudaMemcpy2DAsync(db, sizeof(double) * nd, b, sizeof(double) * ld, sizeof(double) * nd, 9,
                           cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_error(e, "noalloc H2D");
-  e = launch_pairs(method, precision, s, n, da, db, n, max_error, dp, dq, dd, flags ? df : nullptr);
+  e = launch_pairs_cfg(method, precision, s, n, da, db, n, max_error, dp, dq, dd, flags ? df : nullptr,
+                       ctx_pair_launch(ctx, method, precision));
   if (e != cudaSuccess) return cuda_error(e, "noalloc pairs kernel launch");
   ctx->launches += 1;
   e = cudaMemcpy2DAsync(p, sizeof(double) * ld, dp, sizeof(double) * nd, sizeof(double) * nd, 3,

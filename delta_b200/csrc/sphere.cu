@@ -14,94 +14,19 @@
 
 #include "internal.h"
 #include "real.cuh"
+#include "tri_ref.cuh"
 
 namespace delta {
 namespace {
 
-// point.cpp:11-210: closest point tq of triangle (T1,T2,T3) to c; returns the distance
+// point.cpp:11-210: closest point tq of triangle (T1,T2,T3) to c; returns the distance.
+// Eberly's regions are tri_ref.cuh's, with point.cpp's `< 0` clamp.
 __device__ xf64 pt_point(const xf64 T1[3], const xf64 T2[3], const xf64 T3[3], const xf64 c[3], xf64 tq[3]) {
-  xf64 E0[3], E1[3], D[3];
+  xf64 s, t;
+  const xf64 dist = pt_tri_ref<xf64, false>(T1, T2, T3, c, s, t);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    E0[k] = T2[k] - T1[k];
-    E1[k] = T3[k] - T1[k];
-    D[k] = T1[k] - c[k];
-  }
-  const xf64 a = dot3(E0, E0), b = dot3(E0, E1), cc = dot3(E1, E1), d = dot3(E0, D), e = dot3(E1, D),
-             f = dot3(D, D);
-  const xf64 zero(0.0), one(1.0), two(2.0);
-  const xf64 det = a * cc - b * b;
-  xf64 s = b * e - cc * d, t = b * d - a * e, sq = zero;
-  auto full = [&]() { return s * (a * s + b * t + two * d) + t * (b * s + cc * t + two * e) + f; };
-  if ((s + t) <= det) {
-    if (s < zero) {
-      if (t < zero) {  // region 4
-        if (d < zero) {
-          t = zero;
-          if (-d >= a) { s = one; sq = a + two * d + f; }
-          else { s = -d / a; sq = d * s + f; }
-        } else {
-          s = zero;
-          if (e >= zero) { t = zero; sq = f; }
-          else if (-e >= cc) { t = one; sq = cc + two * e + f; }
-          else { t = -e / cc; sq = e * t + f; }
-        }
-      } else {  // region 3
-        s = zero;
-        if (e >= zero) { t = zero; sq = f; }
-        else if (-e >= cc) { t = one; sq = cc + two * e + f; }
-        else { t = -e / cc; sq = e * t + f; }
-      }
-    } else if (t < zero) {  // region 5
-      t = zero;
-      if (d >= zero) { s = zero; sq = f; }
-      else if (-d >= a) { s = one; sq = a + two * d + f; }
-      else { s = -d / a; sq = d * s + f; }
-    } else {  // region 0
-      const xf64 inv = one / det;
-      s = s * inv;
-      t = t * inv;
-      sq = full();
-    }
-  } else {
-    if (s < zero) {  // region 2
-      const xf64 tmp0 = b + d, tmp1 = cc + e;
-      if (tmp1 > tmp0) {
-        const xf64 numer = tmp1 - tmp0, denom = a - two * b + cc;
-        if (numer >= denom) { s = one; t = zero; sq = a + two * d + f; }
-        else { s = numer / denom; t = one - s; sq = full(); }
-      } else {
-        s = zero;
-        if (tmp1 <= zero) { t = one; sq = cc + two * e + f; }
-        else if (e >= zero) { t = zero; sq = f; }
-        else { t = -e / cc; sq = e * t + f; }
-      }
-    } else if (t < zero) {  // region 6
-      const xf64 tmp0 = b + e, tmp1 = a + d;
-      if (tmp1 > tmp0) {
-        const xf64 numer = tmp1 - tmp0, denom = a - two * b + cc;
-        if (numer >= denom) { t = one; s = zero; sq = cc + two * e + f; }
-        else { t = numer / denom; s = one - t; sq = full(); }
-      } else {
-        t = zero;
-        if (tmp1 <= zero) { s = one; sq = a + two * d + f; }
-        else if (d >= zero) { s = zero; sq = f; }
-        else { s = -d / a; sq = d * s + f; }
-      }
-    } else {  // region 1
-      const xf64 numer = cc + e - b - d;
-      if (numer <= zero) { s = zero; t = one; sq = cc + two * e + f; }
-      else {
-        const xf64 denom = a - two * b + cc;
-        if (numer >= denom) { s = one; t = zero; sq = a + two * d + f; }
-        else { s = numer / denom; t = one - s; sq = full(); }
-      }
-    }
-  }
-  if (sq < zero) sq = zero;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) tq[k] = T1[k] + (E1[k] * t) + (E0[k] * s);
-  return sqrt_(sq);
+  for (int k = 0; k < 3; ++k) tq[k] = T1[k] + ((T3[k] - T1[k]) * t) + ((T2[k] - T1[k]) * s);
+  return dist;
 }
 
 struct Rec {

@@ -55,8 +55,10 @@ __device__ __forceinline__ R seg_seg_ref(const R *HA, const R *TA, const R *HB, 
 }
 
 // Point X against triangle (V0,V1,V2): Eberly's seven regions as written in
-// bf.cpp:920-1090.  s runs along V1-V0, t along V2-V0.  Returns the distance.
-template <class R>
+// bf.cpp:920-1090.  s runs along V1-V0, t along V2-V0.  Returns the distance.  The final
+// clamp of the squared distance is bf.cpp:1090's `<= 0` (kClampLE) or point.cpp:199's and
+// zoltan/hybrid.cpp's `< 0`; they differ only for -0.0, which `<` keeps.
+template <class R, bool kClampLE = true>
 __device__ __forceinline__ R pt_tri_ref(const R *V0, const R *V1, const R *V2, const R *X, R &s_out, R &t_out) {
   R E0[3], E1[3], Dv[3];
 #pragma unroll
@@ -140,7 +142,7 @@ __device__ __forceinline__ R pt_tri_ref(const R *V0, const R *V1, const R *V2, c
     }
   }
 #undef DELTA_FULLQ
-  if (sq <= zero) sq = zero;
+  if (kClampLE ? (sq <= zero) : (sq < zero)) sq = zero;
   s_out = s;
   t_out = t;
   return sqrt_(sq);

@@ -115,15 +115,17 @@ delta_status delta_autotune_pairs(delta_ctx *ctx, int method, int precision, int
                                   float *ms_out);
 
 /* No counterpart in the reference.  delta_pairs_run_host for callers that must not let
- * the library allocate device memory (a host whose own pool owns the GPU memory, work
- * recorded by stream capture, allocation-free loops).  Inputs and outputs are staged in
- * one fixed device array built into the library (DELTA_NOALLOC_MAX_PAIRS pairs,
- * 64 MiB, held on every GPU that loads the library until the process exits); no
- * cudaMalloc, cudaFree or allocating library routine is called.  n above the maximum
- * returns DELTA_ERR_CAPACITY.  The first call on a device looks the array up (and may
- * make the driver load the library module there): make it outside any stream capture.
- * All calls on a device share the array and leave their data in it; calls that overlap
- * on the GPU race.  Synchronises the context's stream. */
+ * the library allocate device memory: a host whose own pooling allocator owns the GPU
+ * memory, or an allocation-free latency-bound loop.  Inputs and outputs are staged in one
+ * fixed device array built into the library (DELTA_NOALLOC_MAX_PAIRS pairs, 201 bytes
+ * each: 65,863,680 bytes = 62.8 MiB, held on every GPU that loads the library until the
+ * process exits); no cudaMalloc, cudaFree or allocating library routine is called.  n
+ * above the maximum returns DELTA_ERR_CAPACITY.  The launch shape is the context's, as
+ * for delta_pairs_run_host.  The first call on a device looks the array's device address
+ * up (and may make the driver load the library module there); the address is kept for
+ * the device, so do not use this entry point across a cudaDeviceReset.  All calls on a
+ * device share the array and leave their data in it; calls that overlap on the GPU race.
+ * Synchronises the context's stream. */
 #define DELTA_NOALLOC_MAX_PAIRS 327680
 delta_status delta_pairs_run_host_noalloc(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
                                           const double *b, int64_t ld, double max_error, double *p, double *q,

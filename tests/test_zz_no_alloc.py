@@ -1,49 +1,73 @@
 """The allocation-free host entry point, delta_pairs_run_host_noalloc.
 
-Callers that cannot let the library allocate device memory (their own pool owns it,
-they record work by stream capture, or they run allocation-free loops) use this entry
-point; it stages through a fixed device array built into the library.  This file is
-collected last so that a failure here stops a -x run only after every other test ran.
-The test checks the new entry point against delta_pairs_run_host (bit for bit, the
-tolerance these pair tests use) on two different inputs in a row, and that sizes above
-the stated maximum are refused.
-"""
-import ctypes as C
+Some callers cannot let this library allocate device memory: a host whose own pooling
+allocator owns the GPU's memory (a raw cudaMalloc there fails or fragments its pool), or
+a loop that must not pay for an allocation.  They use this entry point, which stages
+inputs and outputs in a fixed device array built into the library.
 
+This file is collected last, so that a failure here stops a -x run only after every
+other test ran.  It checks, through the C ABI:
+- the results equal delta_pairs_run_host's bit for bit (the tolerance of these pair
+  tests), for FP64 and FP32 and four methods, on two different inputs in a row (the
+  second one smaller, so stale entries of the shared array would show);
+- the calls allocate no device memory (free device memory is unchanged across them);
+- n equal to DELTA_NOALLOC_MAX_PAIRS runs and n one above it is refused.
+It passes alone in a fresh process and after the other tests.
+"""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
+CASES = [(m, prec) for m in (0, 1, 3, 5) for prec in (0, 1) if not (m == 5 and prec == 1)]
 
-def _call(ctx, fn, method, a, b, max_error=1e-3):
+
+def _call(ctx, fn, method, precision, a, b, max_error=1e-3):
     from delta_b200._lib import check
 
     n = a.shape[1]
     p = np.empty((3, n)); q = np.empty((3, n)); d = np.empty(n); fl = np.empty(n, np.uint8)
-    check(fn(ctx.handle, method, 0, n, a.ctypes.data, b.ctypes.data, n, max_error, p.ctypes.data, q.ctypes.data,
-             d.ctypes.data, fl.ctypes.data))
+    check(fn(ctx.handle, method, precision, n, a.ctypes.data, b.ctypes.data, n, max_error, p.ctypes.data,
+             q.ctypes.data, d.ctypes.data, fl.ctypes.data))
     return p, q, d, fl
 
 
-@pytest.mark.parametrize("method", [0, 1, 5])
-def test_noalloc_matches_allocating_entry_point_twice(ctx, method):
+def _free_bytes():
+    import torch
+
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info(0)[0]
+
+
+def test_noalloc_matches_allocating_entry_point_twice_without_allocating(ctx):
     from delta_b200._lib import lib
     from delta_b200.scenarios import narrowphase_pairs
 
     L = lib()
-    for seed, n in ((71, 40000), (72, 25000)):  # the second call is smaller: stale data must not leak
-        a, b, _, _ = narrowphase_pairs(n, seed=seed)
-        ref = _call(ctx, L.delta_pairs_run_host, method, a, b)
-        new = _call(ctx, L.delta_pairs_run_host_noalloc, method, a, b)
-        for x, y in zip(ref, new):
-            assert np.array_equal(x, y, equal_nan=True)
+    inputs = [narrowphase_pairs(n, seed=seed)[:2] for seed, n in ((71, 40000), (72, 25000))]
+    refs = {(c, k): _call(ctx, L.delta_pairs_run_host, *c, a, b) for c in CASES for k, (a, b) in enumerate(inputs)}
+    for c in CASES:  # first calls: the array's address lookup and the module/kernel loads
+        _call(ctx, L.delta_pairs_run_host_noalloc, *c, *inputs[1])
+    free0 = _free_bytes()
+    for c in CASES:
+        for k, (a, b) in enumerate(inputs):  # two calls in a row, the second smaller
+            new = _call(ctx, L.delta_pairs_run_host_noalloc, *c, a, b)
+            for x, y in zip(refs[(c, k)], new):
+                assert np.array_equal(x, y, equal_nan=True), (c, k)
+    assert _free_bytes() == free0, "a no-alloc call changed the free device memory"
 
 
-def test_noalloc_rejects_sizes_above_the_maximum(ctx):
-    from delta_b200._lib import DeltaError, check, lib
+def test_noalloc_maximum_size_runs_and_one_more_is_refused(ctx):
+    from delta_b200._lib import DeltaError, check, header_define, lib
+    from delta_b200.scenarios import narrowphase_pairs
 
-    n = 327680 + 1
+    nmax = header_define("DELTA_NOALLOC_MAX_PAIRS")
+    a, b = narrowphase_pairs(nmax, seed=73)[:2]
+    ref = _call(ctx, lib().delta_pairs_run_host, 5, 0, a, b)
+    new = _call(ctx, lib().delta_pairs_run_host_noalloc, 5, 0, a, b)
+    for x, y in zip(ref, new):
+        assert np.array_equal(x, y, equal_nan=True)
+    n = nmax + 1
     dummy = np.zeros(1)
     with pytest.raises(DeltaError, match="CAPACITY"):
         check(lib().delta_pairs_run_host_noalloc(ctx.handle, 0, 0, n, dummy.ctypes.data, dummy.ctypes.data, n, 0.0,
