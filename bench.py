@@ -53,9 +53,14 @@ def parse():
                     help="auto (autotuned) or network:sweeps:features, e.g. off:1:3, to pin the learned hybrid's "
                          "setting (no tuning, no comparison arms)")
     ap.add_argument("--pairs-log2", type=int, default=24)
+    ap.add_argument("--passes", type=int, default=32,
+                    help="passes over the resident pair batch per timed step (32 x 2^24 pairs: the timed region "
+                         "of the default 20-step run lasts about a second, long enough for the clock record)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--method-table", type=int, default=1,
+                    help="1: time every pair method in FP64 and FP32 and state each result's error per class")
     ap.add_argument("--timestep-steps", type=int, default=200)
     ap.add_argument("--hopper-steps", type=int, default=50)
     ap.add_argument("--box-steps", type=int, default=-1,
@@ -184,7 +189,9 @@ def _time_sim(ctx, stream, sim, steps, params, graph):
     t = wall if graph else e0.elapsed_time(e1) / 1e3
     c1 = sim.counters()
     tri = c1["triangle_pairs"] - c0["triangle_pairs"]
+    solved = c1["solved"] - c0["solved"]
     return {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps, "triangle_pair_tests_per_s": tri / t,
+            "solved_pairs_per_s": solved / t,
             "triangle_pairs_per_step": tri / steps, "solved_pairs_per_step": (c1["solved"] - c0["solved"]) / steps,
             "body_pairs_per_step": (c1["body_pairs"] - c0["body_pairs"]) / steps,
             "gpu_launches": ctx.launches - l0, "timer": "wall clock around synchronised replays" if graph else
@@ -196,22 +203,37 @@ def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, para
     candidate body pair, as the reference) and with the certified FP32 driver (exact box
     culling + bf_cert), stepped and replayed as a CUDA graph.  All three must give the same
     trajectory bit for bit."""
-    from delta_b200.detection import DRV_BF, DRV_BF_CERT
+    from delta_b200.detection import DRV_BF, DRV_BF_CERT, DRV_BF_CULLED, DRV_LEARNED
     from delta_b200.engine import Simulation
 
     out, states = {}, {}
-    for name, drv, graph in (("fp64_bf", DRV_BF, False), ("bf_cert_culled", DRV_BF_CERT, False),
-                             ("bf_cert_culled_graph", DRV_BF_CERT, True)):
+    arms = [("fp64_bf", DRV_BF, False, steps), ("fp64_bf_culled", DRV_BF_CULLED, False, steps),
+            ("fp64_bf_culled_graph", DRV_BF_CULLED, True, steps), ("bf_cert_culled", DRV_BF_CERT, False, steps),
+            ("bf_cert_culled_graph", DRV_BF_CERT, True, steps), ("learned_culled_graph", DRV_LEARNED, True, steps)]
+    for name, drv, graph, k in arms:
         sim = Simulation(ctx, scene, drv)
         sim.step(warmup, params, graph=graph)
-        out[name] = _time_sim(ctx, stream, sim, steps, params, graph)
+        out[name] = _time_sim(ctx, stream, sim, k, params, graph)
         states[name] = sim.state()
         sim.close()
     ref = states["fp64_bf"]
-    same = all(np.array_equal(ref[k], st[k]) for st in states.values() for k in ("pos", "vel", "rot", "x"))
+    exact = [n for n in states if n != "learned_culled_graph"]
+    same = all(np.array_equal(ref[k], states[n][k]) for n in exact for k in ("pos", "vel", "rot", "x"))
+    lrn = states["learned_culled_graph"]
+    out["learned_culled_graph"]["vs_fp64_bf"] = {
+        "max_abs_pos_m": float(np.max(np.abs(lrn["pos"] - ref["pos"]))),
+        "max_abs_vel_m_per_s": float(np.max(np.abs(lrn["vel"] - ref["vel"]))),
+        "bit_identical": bool(all(np.array_equal(ref[k], lrn[k]) for k in ("pos", "vel", "rot", "x")))}
+    sps = {k: v["steps_per_s"] for k, v in out.items()}
     return {"workload": workload, "steps": steps, "warmup": warmup, **out,
-            "speedup": out["bf_cert_culled_graph"]["steps_per_s"] / out["fp64_bf"]["steps_per_s"],
-            "trajectories_bit_identical": bool(same)}
+            "speedup": sps["bf_cert_culled_graph"] / sps["fp64_bf"],
+            "speedup_learned": sps["learned_culled_graph"] / sps["fp64_bf"],
+            "speedup_from_culling": sps["fp64_bf_culled"] / sps["fp64_bf"],
+            "speedup_from_precision": sps["bf_cert_culled_graph"] / sps["fp64_bf_culled_graph"],
+            "speedup_note": "culling: culled FP64 bf vs plain FP64 bf (both stepped); precision: certified "
+                            "FP32+FP64 vs FP64 bfSolver on the same survivors (both graph-replayed)",
+            "trajectories_bit_identical": bool(same),
+            "bit_identical_arms": exact}
 
 
 def run_reference(args, rank, world):
@@ -260,7 +282,7 @@ def main():
     # host-side generation first (spawned pool, before any CUDA initialisation)
     from delta_b200.scenarios import narrowphase_pairs_chunked
 
-    a_np, b_np, _, _ = narrowphase_pairs_chunked(n, seed=args.seed + 7919 * rank)
+    a_np, b_np, _, cls_np = narrowphase_pairs_chunked(n, seed=args.seed + 7919 * rank)
 
     import torch
     import torch.distributed as dist
@@ -312,6 +334,13 @@ def main():
     def pair_run(m):
         return lambda outs: pairs_device(ctx, m, a, b, out=outs)
 
+    def per_step(run):
+        """One timed step: args.passes passes of `run` over the resident batch."""
+        def step(outs):
+            for _ in range(args.passes):
+                run(outs)
+        return step
+
     # launch shapes of the pair kernels chosen by the autotuner on this rank's pairs
     tuned = {"bf_cert": autotune(ctx, METHODS["bf_cert"], a, b, out=out),
              "bf": autotune(ctx, METHODS["bf"], a, b, out=out64)}
@@ -338,12 +367,12 @@ def main():
 
     peak, peak_kind = measured_peak_hbm()
     with ClockSampler(local) as clk:
-        total_ms, per_ms, launches = timed(headline, out, args.steps, args.warmup)
+        total_ms, per_ms, launches = timed(per_step(headline), out, args.steps, args.warmup)
     # the plain FP64 bf kernel on the same pairs (comparison arm, not the headline)
     steps64 = max(3, args.steps // 2)
     total64_ms, per64_ms, _ = timed(pair_run(METHODS["bf"]), out64, steps64, 2)
     total_ms, total64_ms = max_ranks([total_ms, total64_ms])
-    value = world * n * args.steps / (total_ms / 1e3)
+    value = world * n * args.passes * args.steps / (total_ms / 1e3)
     value64 = world * n * steps64 / (total64_ms / 1e3)
 
     # parity of the headline against plain FP64 bf on this rank's pairs
@@ -401,7 +430,7 @@ def main():
 
         refine_ms = ev_time(lambda: refine(ctx, a, b, x0, sweeps, out=ref_out, features=feats))
         infer_ms = ev_time(lambda: model.predict(a, b, out=x0)) if use_model is not None else 0.0
-        head_ms = total_ms / args.steps
+        head_ms = total_ms / (args.steps * args.passes)
         ckpt = json.loads(default_weights().with_suffix(".json").read_text()) if args.weights is None else None
         learned_info = {
             "config": {"network": bool(best["network"]), "sweeps": sweeps, "features": feats,
@@ -422,6 +451,48 @@ def main():
                 "lr": ckpt["lr"], "train_samples_per_second": ckpt["train_samples_per_second"],
                 "eval_loss": ckpt["evaluation"]["loss"], "device": ckpt["device"]},
         }
+
+    # the method x precision table of the microbenchmark: every pair method in FP64 and FP32
+    # on the same pairs, throughput (CUDA events) and the error of each result per class
+    methods_table = None
+    if args.method_table:
+        from delta_b200.scenarios import CLASS_NAMES
+
+        cls = torch.from_numpy(cls_np).cuda()
+        d_bf = out64[2].clone()
+        tab_out = new_out()
+        methods_table = {}
+        for mname in ("bf", "penalty", "penalty_iter", "gjk", "hybrid"):
+            row = {}
+            d_prec = {}
+            for prec, pname in ((0, "f64"), (1, "f32")):
+                def run(o, m=METHODS[mname], pr=prec):
+                    pairs_device(ctx, m, a, b, precision=pr, max_error=1e-3, out=o)
+                t_ms, _, _ = timed(run, tab_out, 3, 1)
+                (t_ms,) = max_ranks([t_ms])
+                d_prec[pname] = tab_out[2].clone()
+                row[pname] = {"value": world * n * 3 / (t_ms / 1e3), "unit": "pairs/s", "ms_per_step": t_ms / 3}
+
+            def err_stats(x, ref):
+                per = {}
+                for c, cname in enumerate(CLASS_NAMES):
+                    sel = (cls == c) & torch.isfinite(ref) & (ref > 0)
+                    e = (x[sel] - ref[sel]).abs()
+                    r = (e / ref[sel]).double()
+                    fin = torch.isfinite(r)
+                    r, ea = r[fin], e[fin]
+                    per[cname] = {"pairs": int(sel.sum().item()),
+                                  "nonfinite": int((~fin).sum().item()),
+                                  "rel_p50": float(torch.quantile(r[:1 << 24].float(), 0.5).item()) if r.numel() else None,
+                                  "rel_p99": float(torch.quantile(r[:1 << 24].float(), 0.99).item()) if r.numel() else None,
+                                  "rel_max": float(r.max().item()) if r.numel() else None,
+                                  "abs_max": float(ea.max().item()) if ea.numel() else None}
+                return per
+            row["f32_vs_f64_same_method"] = err_stats(d_prec["f32"], d_prec["f64"])
+            row["f64_vs_fp64_bf"] = err_stats(d_prec["f64"], d_bf)
+            row["f32_vs_fp64_bf"] = err_stats(d_prec["f32"], d_bf)
+            methods_table[mname] = row
+        del tab_out, d_prec, d_bf
 
     # end to end through the C ABI with pinned host buffers
     e2e = None
@@ -506,14 +577,15 @@ def main():
         else:
             kname = f"k_pairs<{args.method}>"
             bpp = BYTES_PER_PAIR
-            kern_ms = float(np.mean(per_ms))
+            kern_ms = float(np.mean(per_ms)) / args.passes
             traffic = profiled_traffic(args.method, n)
         achieved = bpp * n / (kern_ms / 1e3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {**workload_config(n), "method": args.method,
+            "config": {**workload_config(n), "method": args.method, "passes_per_step": args.passes,
+                       "step": f"{args.passes} passes of the narrowphase over the resident {n}-pair batch",
                        "comparison": "plain FP64 bf kernel on the same pairs"},
             "fp64_bf": {"value": value64, "unit": "pairs/s", "ms_per_step": total64_ms / steps64},
             "autotuned_launch": tuned,
@@ -526,6 +598,7 @@ def main():
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "e2e": e2e,
+            "methods_fp64_fp32": methods_table,
             "cpu_baseline": cpu,
             "timestep": ts,
             "timestep_hopper": hop,

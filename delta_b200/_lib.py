@@ -71,6 +71,17 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_learned_refine": ([vp, i64, vp, vp, i64, vp, i32, i32, f8, vp, vp, vp, vp], C.c_int),
     "delta_pairs_run_learned": ([vp, i64, vp, vp, i64, vp, vp, i32, i32, f8, vp, vp, vp, vp, vp], C.c_int),
     "delta_pairs_run_learned_host": ([vp, i64, vp, vp, i64, vp, vp, i32, i32, f8, vp, vp, vp, vp, vp], C.c_int),
+    "delta_contact_forces": ([vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "delta_update_angular": ([vp, i32, vp, vp, vp, vp, vp, f8], C.c_int),
+    "delta_update_rotation": ([vp, i32, vp, vp, vp, f8], C.c_int),
+    "delta_update_vertices": ([vp, i64, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "delta_zoltan_bf": ([vp, C.c_uint32, C.c_uint32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "delta_zoltan_penalty": ([vp, C.c_uint32, C.c_uint32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "delta_zoltan_hybrid": ([vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "delta_zoltan_update": ([vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, f8], C.c_int),
+    "delta_zoltan_euler": ([vp, i32, vp, vp, vp, vp, f8], C.c_int),
+    "delta_zoltan_integrate": ([vp, f8, vp, vp, i32, vp, vp], C.c_int),
+    "delta_zoltan_force": ([vp, i32, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, f8, f8], C.c_int),
 }
 
 

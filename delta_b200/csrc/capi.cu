@@ -278,7 +278,7 @@ delta_status delta_detect(delta_ctx *ctx, int driver, int precision, const delta
                           const int32_t *pair_a, const int32_t *pair_b, int64_t n_pairs,
                           const delta_contacts *out, int64_t *n_out, delta_stats *stats) {
   if (!ctx || !meshes || !out || !n_out) return set_error(DELTA_ERR_INVALID, "delta_detect: null argument");
-  if (driver < DELTA_DRV_BF || driver > DELTA_DRV_BF_CERT) return set_error(DELTA_ERR_INVALID, "unknown driver");
+  if (driver < DELTA_DRV_BF || driver > DELTA_DRV_LEARNED) return set_error(DELTA_ERR_INVALID, "unknown driver");
   if (precision != DELTA_F64 && precision != DELTA_F32) return set_error(DELTA_ERR_INVALID, "unknown precision");
   if (n_pairs < 0 || out->capacity < 0) return set_error(DELTA_ERR_INVALID, "negative size");
   *n_out = 0;

@@ -15,6 +15,7 @@
 #include "internal.h"
 #include "pose.cuh"
 #include "tri_cert.cuh"
+#include "tri_learned.cuh"
 #include "tri_gjk.cuh"
 #include "tri_ref.cuh"
 
@@ -544,6 +545,121 @@ __global__ void __launch_bounds__(128, 5) k_cert_survivors(delta_meshes m, const
   }
 }
 
+// The reference's FP64 bfSolver (bf.cpp:217-1178, xf64) over the survivors of the box
+// test, one per thread: the culled driver without the FP32 filter (DELTA_DRV_BF_CULLED),
+// which separates what the culling gains from what the certified FP32 solver gains.
+__global__ void __launch_bounds__(128) k_bf64_survivors(delta_meshes m, const int32_t *__restrict__ pa,
+                                                        const int32_t *__restrict__ pb, RawContacts rc) {
+  const unsigned long long cnt = *rc.sv_count;
+  const int64_t n = (int64_t)cnt < rc.sv_cap ? (int64_t)cnt : rc.sv_cap;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t key = rc.sv[i];
+    RowCtx r;
+    r.k = (int64_t)(key >> 32);
+    r.iA = (int32_t)((key >> 16) & 0xffff);
+    const int32_t tb = (int32_t)(key & 0xffff);
+    const int32_t a = pa[r.k], b = pb[r.k];
+    r.tA = m.tri_offset[a] + r.iA;
+    r.tB0 = m.tri_offset[b];
+    r.epsA = m.eps[a];
+    r.epsB = m.eps[b];
+    r.idA = m.id[a];
+    r.idB = m.id[b];
+    r.fric = (m.friction[a] && m.friction[b]) ? 1 : 0;
+    double A[3][3], B[3][3], pq[6];
+    load_tri_cur(m, rc.pose, a, r.tA, A);
+    load_tri_cur(m, rc.pose, b, r.tB0 + tb, B);
+    xf64 A64[3][3], B64[3][3], out[6];
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        A64[v][k] = xf64(A[v][k]);
+        B64[v][k] = xf64(B[v][k]);
+      }
+    bf_solve_ref(A64, B64, out);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) pq[k] = out[k].v;
+    const double mg = (xf64(r.epsA) + xf64(r.epsB)).v;
+    emit(rc, pq_dist64(pq) <= mg, pq, r, tb);  // bf.cpp:125
+  }
+}
+
+// The learned FP32 hybrid over the survivors of the box test (DELTA_DRV_LEARNED), 32 per
+// warp: each lane runs learned_pair_solve (2 FP32 projection sweeps from the centroids,
+// the named bfSolver feature in FP64, the separating-plane certificate at 1e-6); the lanes
+// whose result is not certified then take the exact certified solver together.  The
+// contact rule is bf()'s (bf.cpp:125) on the FP64 distance.
+constexpr int kLearnedSweeps = 2;
+constexpr double kLearnedRelTol = 1e-6;
+__global__ void __launch_bounds__(128, 4) k_learned_survivors(delta_meshes m, const int32_t *__restrict__ pa,
+                                                           const int32_t *__restrict__ pb, RawContacts rc,
+                                                           DevStats *st) {
+  __shared__ CertWarpSmem sm[4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned long long cnt = *rc.sv_count;
+  const int64_t n = (int64_t)cnt < rc.sv_cap ? (int64_t)cnt : rc.sv_cap;
+  if (n == 0) return;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  unsigned exact = 0;
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += nwarps * 32) {
+    const int64_t i = base + lane;
+    const bool valid = i < n;
+    const uint64_t key = rc.sv[valid ? i : n - 1];
+    RowCtx r;
+    r.k = (int64_t)(key >> 32);
+    r.iA = (int32_t)((key >> 16) & 0xffff);
+    const int32_t tb = (int32_t)(key & 0xffff);
+    const int32_t a = pa[r.k], b = pb[r.k];
+    r.tA = m.tri_offset[a] + r.iA;
+    r.tB0 = m.tri_offset[b];
+    r.epsA = m.eps[a];
+    r.epsB = m.eps[b];
+    r.idA = m.id[a];
+    r.idB = m.id[b];
+    r.fric = (m.friction[a] && m.friction[b]) ? 1 : 0;
+    double A[3][3], B[3][3], pq[6];
+    load_tri_cur(m, rc.pose, a, r.tA, A);
+    load_tri_cur(m, rc.pose, b, r.tB0 + tb, B);
+    const bool ok = learned_pair_solve(A, B, kLearnedSweeps, kLearnedRelTol, pq);
+    const bool need = valid && !ok;
+    if (__any_sync(kFull, need)) {
+      double px[6];
+      bf_cert_warp(A, B, need, px, sm[warp]);
+      if (need) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) pq[k] = px[k];
+      }
+      exact += need ? 1u : 0u;
+    }
+    const double mg = (xf64(r.epsA) + xf64(r.epsB)).v;
+    emit(rc, valid && pq_dist64(pq) <= mg, pq, r, tb);  // bf.cpp:125
+  }
+  const unsigned tot = __reduce_add_sync(kFull, exact);
+  if (lane == 0 && tot) atomicAdd(&st->penalty_fails, (unsigned long long)tot);  // pairs solved exactly
+}
+
+// The survivors' solver of a culled driver: certified FP32 + FP64 (DELTA_DRV_BF_CERT), FP64
+// bfSolver (DELTA_DRV_BF_CULLED) or the learned FP32 hybrid (DELTA_DRV_LEARNED).
+inline cudaError_t launch_survivors(int driver, cudaStream_t s, const delta_meshes &m, const int32_t *pa,
+                                    const int32_t *pb, const RawContacts &rc, DevStats *st, int64_t n_hint) {
+  int per_sm = 0;
+  cudaError_t e = driver == DELTA_DRV_BF_CULLED
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bf64_survivors, 128, 0)
+                  : driver == DELTA_DRV_LEARNED
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_learned_survivors, 128, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = n_hint >= 0 ? (n_hint + 127) / 128 : INT64_MAX;
+  const int64_t mx = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
+  if (blocks > mx) blocks = mx;
+  if (blocks < 1) blocks = 1;
+  if (driver == DELTA_DRV_BF_CULLED) k_bf64_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc);
+  else if (driver == DELTA_DRV_LEARNED) k_learned_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc, st);
+  else k_cert_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc, st);
+  return cudaGetLastError();
+}
+
 __global__ void k_sv_evaluated(const unsigned long long *sv_count, int64_t sv_cap, DevStats *st, int *ovf) {
   const unsigned long long c = *sv_count;
   st->evaluated += c;
@@ -811,9 +927,10 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   unsigned long long hcount = 0;
   RawContacts rc{};
   rc.tbits = 16;
-  if (driver == DELTA_DRV_BF_CERT && pose) {
+  const bool culled = driver == DELTA_DRV_BF_CERT || driver == DELTA_DRV_BF_CULLED || driver == DELTA_DRV_LEARNED;
+  if (culled && pose) {
     rc.pose = *pose;  // current vertices and body boxes from the bodies' poses
-  } else if (driver == DELTA_DRV_BF_CERT) {
+  } else if (culled) {
     // body boxes of the current vertices for the culling
     void *bb = nullptr;
     if ((st = ctx_scratch(ctx, 23, 48 * (size_t)m.n_bodies + 64, &bb)) != DELTA_OK) return st;
@@ -837,9 +954,9 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
     if ((e = cudaMemsetAsync(queue, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess)
       return cuda_error(e, "memset");
     if ((e = cudaMemsetAsync(dstats, 0, sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
-    if (driver == DELTA_DRV_BF_CERT) {
+    if (culled) {
       // phase 1: box culling into the survivor list (grown and repeated on overflow);
-      // phase 2: certified bf over the survivors, full warps across pairs
+      // phase 2: the survivors' solver (certified bf, full warps across pairs; or FP64 bf)
       int64_t sv_cap = 8 * cap > (1 << 16) ? 8 * cap : (1 << 16);
       unsigned long long hsv = 0;
       for (int sv_attempt = 0; sv_attempt < 2; ++sv_attempt) {
@@ -857,14 +974,8 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
         if ((int64_t)hsv <= sv_cap) break;
         sv_cap = (int64_t)hsv + hsv / 4;
       }
-      int per_sm = 0;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0)) != cudaSuccess)
-        return cuda_error(e, "occupancy");
-      int64_t blocks = ((int64_t)hsv + 127) / 128;
-      const int64_t mx = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
-      if (blocks > mx) blocks = mx;
-      if (blocks < 1) blocks = 1;
-      k_cert_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc, dstats);
+      if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, (int64_t)hsv)) != cudaSuccess)
+        return cuda_error(e, "survivor kernel");
       k_sv_evaluated<<<1, 1, 0, s>>>(sv_count, rc.sv_cap, dstats, nullptr);
       ctx->launches += 2;
       e = cudaGetLastError();
@@ -990,10 +1101,11 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   rc.sv = (uint64_t *)p;
   rc.sv_cap = fixed_sv_cap(cap);
   rc.sv_count = queue + 2;
-  if (driver == DELTA_DRV_BF_CERT && pose) rc.pose = *pose;  // vertices and body boxes from the poses
+  const bool culled = driver == DELTA_DRV_BF_CERT || driver == DELTA_DRV_BF_CULLED || driver == DELTA_DRV_LEARNED;
+  if (culled && pose) rc.pose = *pose;  // vertices and body boxes from the poses
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
   size_t tb = temp_bytes;
-  if (driver == DELTA_DRV_BF_CERT) {
+  if (culled) {
     // The culling takes body pairs directly (no rows).  The contacts are ordered without a
     // sort: counted per pair (rows, zeroed by the culling), the counts scanned into pair
     // offsets (row_offset), each contact put in its pair's bucket (indices in perm_out,
@@ -1003,10 +1115,8 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
     rc.slot = (uint32_t *)key_out;
     e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats);
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
-    int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0)) != cudaSuccess)
-      return cuda_error(e, "occupancy");
-    k_cert_survivors<<<(unsigned)(kNumSMs * (per_sm > 0 ? per_sm : 1)), 128, 0, s>>>(m, pa, pb, rc, dstats);
+    if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, -1)) != cudaSuccess)
+      return cuda_error(e, "survivor kernel");
     if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
       return cuda_error(e, "pair contact scan");
     k_bucket_contacts<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out, (uint64_t *)perm_in);

@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "internal.h"
+#include "tri_learned.cuh"
 #include "tri_ref.cuh"
 
 namespace delta {
@@ -710,94 +711,6 @@ __device__ __forceinline__ double ld_again(const double *p) {
   double v;
   asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
   return v;
-}
-
-// Closest point of triangle (V0, V0+E0, V0+E1) to X in FP32, branch-free: the interior
-// solution of the 2x2 normal equations when it lies inside, otherwise the nearest of the
-// three edges' clamped projections (all computed, one selected), so the lanes of a warp
-// never diverge.  Barycentric (s, t); returns the squared distance less |V0-X|^2.
-__device__ __forceinline__ float closest_on_tri(const float *V0, const float *E0, const float *E1, const float *X,
-                                                float &s, float &t) {
-  float D[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) D[k] = V0[k] - X[k];
-  const float a = dot3(E0, E0), b = dot3(E0, E1), c = dot3(E1, E1), d = dot3(E0, D), e = dot3(E1, D);
-  const float idet = __fdividef(1.f, fmaf(a, c, -b * b));
-  const float si = fmaf(b, e, -c * d) * idet, ti = fmaf(b, d, -a * e) * idet;
-  // squared distance at (s, t) minus |D|^2
-  auto q = [&](float u, float v) { return fmaf(u, fmaf(a, u, fmaf(2.f * b, v, 2.f * d)), v * fmaf(c, v, 2.f * e)); };
-  const float s0 = a > 0.f ? fminf(fmaxf(__fdividef(-d, a), 0.f), 1.f) : 0.f;  // edge t = 0
-  const float t1 = c > 0.f ? fminf(fmaxf(__fdividef(-e, c), 0.f), 1.f) : 0.f;  // edge s = 0
-  const float den = a - 2.f * b + c;
-  const float l2 = den > 0.f ? fminf(fmaxf(__fdividef(c + e - b - d, den), 0.f), 1.f) : 0.f;  // edge s + t = 1
-  float best = q(s0, 0.f);
-  s = s0;
-  t = 0.f;
-  const float q1 = q(0.f, t1), q2 = q(l2, 1.f - l2);
-  if (q1 < best) { best = q1; s = 0.f; t = t1; }
-  if (q2 < best) { best = q2; s = l2; t = 1.f - l2; }
-  if (si >= 0.f && ti >= 0.f && si + ti <= 1.f) { s = si; t = ti; best = q(si, ti); }
-  return best;
-}
-
-// FP32 distance of vertex-face pair (X, triangle V0 V1 V2), branch-free.
-__device__ __forceinline__ float pt_tri_dist32(const float *V0, const float *V1, const float *V2, const float *X) {
-  float E0[3], E1[3], s, t;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    E0[k] = V1[k] - V0[k];
-    E1[k] = V2[k] - V0[k];
-  }
-  closest_on_tri(V0, E0, E1, X, s, t);
-  float r2 = 0.f;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float r = fmaf(s, E0[k], fmaf(t, E1[k], V0[k] - X[k]));
-    r2 = fmaf(r, r, r2);
-  }
-  return sqrtf(r2);
-}
-
-// FP32 distance of edge pair (TA->HA, TB->HB): clamped closest parameters, branch-free.
-__device__ __forceinline__ float seg_seg_dist32(const float *HA, const float *TA, const float *HB, const float *TB) {
-  float u[3], v[3], w[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    u[k] = HA[k] - TA[k];
-    v[k] = HB[k] - TB[k];
-    w[k] = TA[k] - TB[k];
-  }
-  const float a = dot3(u, u), e = dot3(v, v), b = dot3(u, v), c = dot3(u, w), f = dot3(v, w);
-  const float den = fmaf(a, e, -b * b);
-  float s = den > 1e-12f * (a * e) ? fminf(fmaxf(__fdividef(fmaf(b, f, -c * e), den), 0.f), 1.f) : 0.f;
-  const float traw = e > 0.f ? __fdividef(fmaf(b, s, f), e) : 0.f;
-  const float t = fminf(fmaxf(traw, 0.f), 1.f);
-  const float s2 = a > 0.f ? fminf(fmaxf(__fdividef(fmaf(b, t, -c), a), 0.f), 1.f) : 0.f;
-  s = traw != t ? s2 : s;
-  float r2 = 0.f;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float r = fmaf(s, u[k], fmaf(-t, v[k], w[k]));
-    r2 = fmaf(r, r, r2);
-  }
-  return sqrtf(r2);
-}
-
-// First index of the largest / smallest of three values.
-__device__ __forceinline__ int argmax3(float x0, float x1, float x2) {
-  const int i = x1 > x0 ? 1 : 0;
-  return x2 > (i ? x1 : x0) ? 2 : i;
-}
-__device__ __forceinline__ int argmin3(float x0, float x1, float x2) {
-  const int i = x1 < x0 ? 1 : 0;
-  return x2 < (i ? x1 : x0) ? 2 : i;
-}
-
-// Vertex j (0..2) of T, by selects (no dynamically indexed register array).
-template <class R>
-__device__ __forceinline__ void pick_vertex(const R T[3][3], int j, R out[3]) {
-#pragma unroll
-  for (int k = 0; k < 3; ++k) out[k] = j == 0 ? T[0][k] : (j == 1 ? T[1][k] : T[2][k]);
 }
 
 // Learned hybrid solver, one pair per thread.  From the warm start x0 (barycentric

@@ -12,6 +12,49 @@
 
 namespace delta {
 
+// expmap, dynamics.cpp:26-102 (Taylor branch below 10 degrees; the off-diagonal term
+// v02 = Omega2*Omega3 of dynamics.cpp:78 is kept as written).
+__device__ __forceinline__ void expmap(xf64 O1, xf64 O2, xf64 O3, xf64 L[9]) {
+  using X = xf64;
+  const X v0 = O1 * O1, v1 = O2 * O2, v2 = O3 * O3;
+  X angsq = v0 + v1 + v2, sx, cx;
+  if (angsq < X(3.0461741978671E-02)) {
+    sx = X(1.0) + (X(-1.666666666666667E-1) + (X(8.333333333333333E-3) + (X(-1.984126984126984E-4) +
+         (X(2.755731922398589E-6) + (X(-2.505210838544172E-8) + X(1.605904383682161E-10) * angsq) * angsq) *
+         angsq) * angsq) * angsq) * angsq;
+    cx = X(0.5) + (X(-4.166666666666667E-2) + (X(1.388888888888889E-3) + (X(-2.480158730158730E-5) +
+         (X(2.755731922398589E-7) + (X(-2.087675698786810E-9) + X(1.147074559772972E-11) * angsq) * angsq) *
+         angsq) * angsq) * angsq) * angsq;
+  } else {
+    const X t = angsq;
+    angsq = sqrt_(angsq);
+    const X s = X(sin(angsq.v)), c = X(cos(angsq.v));
+    sx = s / angsq;
+    cx = (X(1.0) - c) / t;
+  }
+  const X v01 = O1 * O2, v02 = O2 * O3, v12 = O2 * O3;
+  const X s0 = sx * O1, s1 = sx * O2, s2 = sx * O3;
+  L[0] = -cx * (v2 + v1);
+  L[1] = cx * v01;
+  L[2] = cx * v02;
+  L[3] = L[1];
+  L[4] = -cx * (v2 + v0);
+  L[5] = cx * v12;
+  L[6] = L[2];
+  L[7] = L[5];
+  L[8] = -cx * (v1 + v0);
+  L[0] += X(1.0);
+  L[1] += s2;
+  L[2] -= s1;
+  L[3] -= s2;
+  L[4] += X(1.0);
+  L[5] += s0;
+  L[6] += s1;
+  L[7] -= s0;
+  L[8] += X(1.0);
+}
+
+
 __device__ __forceinline__ void posed_point(const xf64 R[9], const xf64 pos[3], const xf64 rp[3], double r0,
                                             double r1, double r2, double out[3]) {
   const xf64 C0 = xf64(r0) - rp[0], C1 = xf64(r1) - rp[1], C2 = xf64(r2) - rp[2];

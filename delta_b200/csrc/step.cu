@@ -26,47 +26,6 @@ using X = xf64;
 // dynamics.cpp
 // ---------------------------------------------------------------------------------------
 
-// expmap, dynamics.cpp:26-102 (Taylor branch below 10 degrees; the off-diagonal term
-// v02 = Omega2*Omega3 of dynamics.cpp:78 is kept as written).
-__device__ __forceinline__ void expmap(X O1, X O2, X O3, X L[9]) {
-  const X v0 = O1 * O1, v1 = O2 * O2, v2 = O3 * O3;
-  X angsq = v0 + v1 + v2, sx, cx;
-  if (angsq < X(3.0461741978671E-02)) {
-    sx = X(1.0) + (X(-1.666666666666667E-1) + (X(8.333333333333333E-3) + (X(-1.984126984126984E-4) +
-         (X(2.755731922398589E-6) + (X(-2.505210838544172E-8) + X(1.605904383682161E-10) * angsq) * angsq) *
-         angsq) * angsq) * angsq) * angsq;
-    cx = X(0.5) + (X(-4.166666666666667E-2) + (X(1.388888888888889E-3) + (X(-2.480158730158730E-5) +
-         (X(2.755731922398589E-7) + (X(-2.087675698786810E-9) + X(1.147074559772972E-11) * angsq) * angsq) *
-         angsq) * angsq) * angsq) * angsq;
-  } else {
-    const X t = angsq;
-    angsq = sqrt_(angsq);
-    const X s = X(sin(angsq.v)), c = X(cos(angsq.v));
-    sx = s / angsq;
-    cx = (X(1.0) - c) / t;
-  }
-  const X v01 = O1 * O2, v02 = O2 * O3, v12 = O2 * O3;
-  const X s0 = sx * O1, s1 = sx * O2, s2 = sx * O3;
-  L[0] = -cx * (v2 + v1);
-  L[1] = cx * v01;
-  L[2] = cx * v02;
-  L[3] = L[1];
-  L[4] = -cx * (v2 + v0);
-  L[5] = cx * v12;
-  L[6] = L[2];
-  L[7] = L[5];
-  L[8] = -cx * (v1 + v0);
-  L[0] += X(1.0);
-  L[1] += s2;
-  L[2] -= s1;
-  L[3] -= s2;
-  L[4] += X(1.0);
-  L[5] += s0;
-  L[6] += s1;
-  L[7] -= s0;
-  L[8] += X(1.0);
-}
-
 struct BodyRef {
   int32_t n, i;
   __device__ __forceinline__ int64_t at(int c) const { return (int64_t)c * n + i; }
@@ -772,6 +731,92 @@ __global__ void k_unpack_pairs(const uint64_t *k, int64_t n, int sh, int32_t *a,
   b[t] = empty ? -1 : (int32_t)(v & ((1ull << sh) - 1));
 }
 
+// ---- the reference's per-call forces and dynamics, batched --------------------------
+// getContactsForces (forces.cpp:291-396) for group g: the contacts [off[g], off[g+1]) of
+// body A against body B, added in list order onto force[g], torque[g] (3 planes of n).
+struct GroupKin {
+  const double *pos_a, *ang_a, *lin_a, *mass_a, *pos_b, *ang_b, *lin_b, *mass_b;
+};
+__global__ void k_contact_forces_groups(int64_t n, const int64_t *off, ContactView cv, GroupKin g,
+                                        delta_step_params p, double *force, double *torque) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BodyKin A, B;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    A.pos[d] = X(g.pos_a[d * n + i]);
+    A.ang[d] = X(g.ang_a[d * n + i]);
+    A.lin[d] = X(g.lin_a[d * n + i]);
+    B.pos[d] = X(g.pos_b[d * n + i]);
+    B.ang[d] = X(g.ang_b[d * n + i]);
+    B.lin[d] = X(g.lin_b[d * n + i]);
+  }
+  A.mass = X(g.mass_a[i]);
+  B.mass = X(g.mass_b[i]);
+  X F[3], T[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    F[d] = X(force[d * n + i]);
+    T[d] = X(torque[d * n + i]);
+  }
+  const int64_t c0 = max((int64_t)0, off[i]), c1 = min(cv.cap, off[i + 1]);
+  for (int64_t c = c0; c < c1; ++c) {
+    X Fc[3], Tc[3];
+    contact_terms(cv, c, A, B, false, p, Fc, Tc);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      F[d] += Fc[d];
+      T[d] += Tc[d];
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    force[d * n + i] = F[d].v;
+    torque[d * n + i] = T[d].v;
+  }
+}
+
+// updateAngular (dynamics.cpp:140-213) of every body of s with its torque (3 planes).
+__global__ void k_update_angular_only(delta_scene s, const double *torque, double step) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_bodies) return;
+  const BodyRef b{s.n_bodies, i};
+  X tq[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) tq[k] = X(torque[b.at(k)]);
+  update_angular(s, b, tq, X(step));
+}
+
+// updateRotationMatrix (dynamics.cpp:104-138) of every body of s.
+__global__ void k_update_rotation_only(delta_scene s, double step) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_bodies) return;
+  update_rotation(s, BodyRef{s.n_bodies, i}, X(step));
+}
+
+// updateVertices (dynamics.cpp:215-242) of vertex v, owned by body[v] of n bodies.
+__global__ void k_update_vertices_only(int64_t nv, const int32_t *body, int32_t n, double *x, double *y, double *z,
+                                       const double *rx, const double *ry, const double *rz, const double *rot,
+                                       const double *pos, const double *ref_pos) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int32_t i = body ? body[v] : 0;
+  if (i < 0 || i >= n) return;
+  xf64 R[9], P[3], RP[3];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) R[k] = xf64(rot[(int64_t)k * n + i]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    P[k] = xf64(pos[(int64_t)k * n + i]);
+    RP[k] = xf64(ref_pos[(int64_t)k * n + i]);
+  }
+  double out[3];
+  posed_point(R, P, RP, rx[v], ry[v], rz[v], out);
+  x[v] = out[0];
+  y[v] = out[1];
+  z[v] = out[2];
+}
+
 __global__ void k_iota32(int32_t *v, int32_t n) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) v[i] = i;
@@ -1241,7 +1286,7 @@ static delta_status sim_detect(delta_sim *s) {
   s->counters[1] += np;
   // vertices of the bodies the narrowphase reads: formed from the poses by the certified
   // driver, updated here for the others
-  const bool posed = s->driver == DELTA_DRV_BF_CERT;
+  const bool posed = s->driver == DELTA_DRV_BF_CERT || s->driver == DELTA_DRV_BF_CULLED || s->driver == DELTA_DRV_LEARNED;
   const Pose pose = sim_pose(s);
   if (!posed) {
     cudaStream_t st = s->ctx->stream;
@@ -1342,7 +1387,7 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
     return ds;
   // vertices of the bodies the narrowphase reads this step: formed from the poses by the
   // certified driver, updated here for the others
-  const bool posed = s->driver == DELTA_DRV_BF_CERT;
+  const bool posed = s->driver == DELTA_DRV_BF_CERT || s->driver == DELTA_DRV_BF_CULLED || s->driver == DELTA_DRV_LEARNED;
   const Pose pose = sim_pose(s);
   if (!posed) {
     k_mark_pair_bodies<<<blocks_for(g.pair_cap), 256, 0, st>>>(g.pa, g.pb, g.pair_cap, s->epoch, s->stamp);
@@ -1422,6 +1467,72 @@ delta_status delta_forces(delta_ctx *ctx, const delta_scene *scene, const delta_
   return forces_run(ctx, *scene, contacts ? *contacts : empty, n_contacts, *params, force, torque, has_contact);
 }
 
+delta_status delta_contact_forces(delta_ctx *ctx, int64_t n_groups, const int64_t *offset,
+                                  const delta_contacts *contacts, const double *pos_a, const double *ang_a,
+                                  const double *lin_a, const double *mass_a, const double *pos_b,
+                                  const double *ang_b, const double *lin_b, const double *mass_b,
+                                  const delta_step_params *params, double *force, double *torque) {
+  if (!ctx || !params) return set_error(DELTA_ERR_INVALID, "delta_contact_forces: null argument");
+  if (n_groups < 0) return set_error(DELTA_ERR_INVALID, "delta_contact_forces: negative size");
+  if (n_groups == 0) return DELTA_OK;
+  if (!offset || !contacts || !pos_a || !ang_a || !lin_a || !mass_a || !pos_b || !ang_b || !lin_b || !mass_b ||
+      !force || !torque || (contacts->capacity > 0 && (!contacts->x || !contacts->normal || !contacts->depth ||
+                                                       !contacts->friction)))
+    return set_error(DELTA_ERR_INVALID, "delta_contact_forces: null argument");
+  ContactView cv{contacts->x, contacts->normal, contacts->depth, contacts->master, contacts->slave,
+                 contacts->friction, contacts->capacity};
+  GroupKin g{pos_a, ang_a, lin_a, mass_a, pos_b, ang_b, lin_b, mass_b};
+  k_contact_forces_groups<<<(unsigned)((n_groups + 127) / 128), 128, 0, ctx->stream>>>(n_groups, offset, cv, g,
+                                                                                      *params, force, torque);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_contact_forces launch");
+}
+
+delta_status delta_update_angular(delta_ctx *ctx, int32_t n, double *ref_ang, const double *rot,
+                                  const double *inertia, const double *inverse, const double *torque, double step) {
+  if (!ctx || n < 0) return set_error(DELTA_ERR_INVALID, "delta_update_angular: bad argument");
+  if (n == 0) return DELTA_OK;
+  if (!ref_ang || !rot || !inertia || !inverse || !torque)
+    return set_error(DELTA_ERR_INVALID, "delta_update_angular: null argument");
+  delta_scene s{};
+  s.n_bodies = n;
+  s.ref_ang = ref_ang;
+  s.rot = const_cast<double *>(rot);
+  s.inertia = inertia;
+  s.inverse = inverse;
+  k_update_angular_only<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(s, torque, step);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_update_angular launch");
+}
+
+delta_status delta_update_rotation(delta_ctx *ctx, int32_t n, double *ang, const double *ref_ang, double *rot,
+                                   double step) {
+  if (!ctx || n < 0) return set_error(DELTA_ERR_INVALID, "delta_update_rotation: bad argument");
+  if (n == 0) return DELTA_OK;
+  if (!ang || !ref_ang || !rot) return set_error(DELTA_ERR_INVALID, "delta_update_rotation: null argument");
+  delta_scene s{};
+  s.n_bodies = n;
+  s.ang = ang;
+  s.ref_ang = const_cast<double *>(ref_ang);
+  s.rot = rot;
+  k_update_rotation_only<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(s, step);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_update_rotation launch");
+}
+
+delta_status delta_update_vertices(delta_ctx *ctx, int64_t n_vertices, const int32_t *body, int32_t n_bodies,
+                                   double *x, double *y, double *z, const double *rx, const double *ry,
+                                   const double *rz, const double *rot, const double *pos, const double *ref_pos) {
+  if (!ctx || n_vertices < 0 || n_bodies < 0) return set_error(DELTA_ERR_INVALID, "delta_update_vertices: bad size");
+  if (n_vertices == 0) return DELTA_OK;
+  if (n_bodies == 0 || !x || !y || !z || !rx || !ry || !rz || !rot || !pos || !ref_pos || (!body && n_bodies != 1))
+    return set_error(DELTA_ERR_INVALID, "delta_update_vertices: null argument");
+  k_update_vertices_only<<<(unsigned)((n_vertices + 127) / 128), 128, 0, ctx->stream>>>(
+      n_vertices, body, n_bodies, x, y, z, rx, ry, rz, rot, pos, ref_pos);
+  ctx->launches += 1;
+  return cuda_error(cudaGetLastError(), "delta_update_vertices launch");
+}
+
 delta_status delta_integrate(delta_ctx *ctx, const delta_scene *scene, const delta_step_params *params,
                              const double *force, const double *torque, const uint8_t *has_contact) {
   if (!ctx || !scene || !params || !force || !torque || !has_contact)
@@ -1448,8 +1559,10 @@ delta_status delta_broadphase(delta_ctx *ctx, const delta_scene *scene, int32_t 
 
 delta_status delta_sim_create(delta_ctx *ctx, const delta_scene *scene, int driver, delta_sim **out) {
   if (!ctx || !scene || !out) return set_error(DELTA_ERR_INVALID, "delta_sim_create: null argument");
-  if (driver != DELTA_DRV_BF && driver != DELTA_DRV_BF_CERT)
-    return set_error(DELTA_ERR_UNSUPPORTED, "delta_sim_create: the time step runs DELTA_DRV_BF or DELTA_DRV_BF_CERT");
+  if (driver != DELTA_DRV_BF && driver != DELTA_DRV_BF_CERT && driver != DELTA_DRV_BF_CULLED &&
+      driver != DELTA_DRV_LEARNED)
+    return set_error(DELTA_ERR_UNSUPPORTED, "delta_sim_create: the time step runs DELTA_DRV_BF, DELTA_DRV_BF_CERT, "
+                                            "DELTA_DRV_BF_CULLED or DELTA_DRV_LEARNED");
   delta_sim *s = new delta_sim();
   s->ctx = ctx;
   s->scene = *scene;

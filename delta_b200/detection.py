@@ -18,7 +18,7 @@ from ._lib import DeltaError, ERR_CAPACITY, check, lib
 from .narrowphase import F64, Context
 
 (DRV_BF, DRV_PENALTY, DRV_PENALTY_STAT, DRV_HYBRID_BATCH, DRV_HYBRID_TRIANGLE, DRV_HYBRID_BATCH_STAT,
- DRV_HYBRID_TRI_STAT, DRV_GJK, DRV_BF_CERT) = range(9)
+ DRV_HYBRID_TRI_STAT, DRV_GJK, DRV_BF_CERT, DRV_BF_CULLED, DRV_LEARNED) = range(11)
 
 CONTACT_DTYPE = np.dtype(
     [("x", "<f8", 3), ("normal", "<f8", 3), ("depth", "<f8"), ("P", "<f8", 3), ("Q", "<f8", 3),

@@ -17,6 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 GENERAL, NEAR_PARALLEL, INTERSECTING = 0, 1, 2
+CLASS_NAMES = ("general", "near_parallel", "intersecting")
 
 
 def _unit(v):

@@ -63,7 +63,16 @@ typedef enum {
   DELTA_DRV_HYBRID_BATCH_STAT = 5, /* hybridBatchStat(),             hybrid.cpp:489-628  */
   DELTA_DRV_HYBRID_TRI_STAT = 6,   /* hybridTriangleStat(),          hybrid.cpp:202-336  */
   DELTA_DRV_GJK = 7,               /* gjk per triangle pair with bf()'s contact rule     */
-  DELTA_DRV_BF_CERT = 8            /* bf() contact set computed with DELTA_BF_CERT        */
+  DELTA_DRV_BF_CERT = 8,           /* bf() contact set computed with DELTA_BF_CERT        */
+  DELTA_DRV_BF_CULLED = 9,         /* bf() contact set: the certified driver's exact box
+                                      culling, then FP64 bfSolver on the survivors        */
+  DELTA_DRV_LEARNED = 10           /* the learned FP32 hybrid: the same culling, then per
+                                      survivor 2 FP32 projection sweeps, the bfSolver
+                                      feature they name in FP64, a separating-plane
+                                      certificate at 1e-6 relative, and DELTA_BF_CERT for
+                                      the pairs it does not certify; bf()'s contact rule on
+                                      the FP64 distance, so the contact set is bf()'s
+                                      except for pairs within 1e-6 of the threshold       */
 } delta_driver;
 
 typedef struct delta_ctx delta_ctx;
@@ -226,6 +235,35 @@ delta_status delta_forces(delta_ctx *ctx, const delta_scene *scene, const delta_
 delta_status delta_integrate(delta_ctx *ctx, const delta_scene *scene, const delta_step_params *params,
                              const double *force, const double *torque, const uint8_t *has_contact);
 
+/* getContactsForces (forces.cpp:291-396) for n_groups calls at once.  Group g is one call:
+ * the contacts [offset[g], offset[g+1]) of `contacts` (x, normal, depth and friction are
+ * read; the normal as stored for body A), body A's and body B's centre, spatial angular
+ * velocity and linear velocity (pos_a, ang_a, lin_a, ... : 3 planes of n_groups) and
+ * masses (mass_a, mass_b: n_groups).  force and torque (3 planes of n_groups) accumulate
+ * onto their inputs contact by contact, as the reference adds into its force[3] and
+ * torque[3].  params: spring, damper, friction (SPRING, DAMPER, FRICTION, forces.cpp:11-21;
+ * a sphere contact, isSphere, is springSphere's formula with SSPRING, SDAMPER and
+ * SFRICTIONGOLD, forces.cpp:227-289); dt and gravity are not used. */
+delta_status delta_contact_forces(delta_ctx *ctx, int64_t n_groups, const int64_t *offset,
+                                  const delta_contacts *contacts, const double *pos_a, const double *ang_a,
+                                  const double *lin_a, const double *mass_a, const double *pos_b,
+                                  const double *ang_b, const double *lin_b, const double *mass_b,
+                                  const delta_step_params *params, double *force, double *torque);
+/* updateAngular (dynamics.cpp:140-213) of n bodies: ref_ang [3n] in/out, rot [9n],
+ * inertia [9n], inverse [9n], torque [3n]. */
+delta_status delta_update_angular(delta_ctx *ctx, int32_t n, double *ref_ang, const double *rot,
+                                  const double *inertia, const double *inverse, const double *torque, double step);
+/* updateRotationMatrix (dynamics.cpp:104-138) of n bodies: rot [9n] in/out, the spatial
+ * angular velocity ang [3n] out, from ref_ang [3n]. */
+delta_status delta_update_rotation(delta_ctx *ctx, int32_t n, double *ang, const double *ref_ang, double *rot,
+                                   double step);
+/* updateVertices (dynamics.cpp:215-242) of n_vertices vertices: vertex v gets
+ * pos + R (r - ref_pos) of its body body[v] (body may be NULL when n_bodies == 1);
+ * rot [9 n_bodies], pos, ref_pos [3 n_bodies]. */
+delta_status delta_update_vertices(delta_ctx *ctx, int64_t n_vertices, const int32_t *body, int32_t n_bodies,
+                                   double *x, double *y, double *z, const double *rx, const double *ry,
+                                   const double *rz, const double *rot, const double *pos, const double *ref_pos);
+
 /* Candidate body pairs (a < b, not both obstacles) whose bounding spheres, grown by the
  * two epsilons, overlap; sorted by (a, b).  A superset of the pairs that can hold a
  * contact (replaces the Peano grid traversal + isSphereOverlayInContact precheck,
@@ -302,6 +340,74 @@ delta_status delta_sphere_mesh_contacts(delta_ctx *ctx, const delta_spheres *sph
  * (the values the caller passes as radii); overlap [n_pairs] = 1 when |cA - cB| <= rA + rB. */
 delta_status delta_sphere_overlap(delta_ctx *ctx, const double *centre, int64_t ld, const double *radius,
                                   const int32_t *pair_a, const int32_t *pair_b, int64_t n_pairs, uint8_t *overlap);
+
+/* ---- the zoltan/ code path -------------------------------------------------------------
+ * The reference's second front end (zoltan/) keeps the system as structure-of-arrays and
+ * calls the narrowphase with one triangle against a list.  These entry points keep those
+ * argument lists: the reference's pointer arrays become arrays of device pointers
+ * (d[k] = coordinate k of every list entry; t[v][k] = coordinate k of vertex v of every
+ * triangle, v = 0..2 spatial and 3..5 referential); a, b, c, lo, hi and gravity are host
+ * arrays of 3 doubles.  FP64 in the reference's operation order; the penalty weights use
+ * pow/log/log10 (CUDA's, which can differ from the host C library's in the last bit).
+ * Asynchronous on the context's stream. */
+
+/* bf(it, nt, A, B, C, D, E, F, P, Q), declared at zoltan/bf.h:61-64 (the reference defines
+ * only the per-pair form, zoltan/bf.cpp:26-952): for i in [it, nt), the closest points of
+ * triangle ABC and triangle (D[i], E[i], F[i]) with zoltan/bf.cpp's arithmetic and its
+ * differences from delta's bfSolver (early return on a zero cross product, leaving P[i],
+ * Q[i] untouched; no break after case 1 of either switch). */
+delta_status delta_zoltan_bf(delta_ctx *ctx, uint32_t it, uint32_t nt, const double a[3], const double b[3],
+                             const double c[3], const double *const d[3], const double *const e[3],
+                             const double *const f[3], double *const p[3], double *const q[3]);
+/* penalty(it, nt, ...), zoltan/penalty.cpp:27-209: 5 quasi-Newton steps per entry, delta
+ * = 0.1 tr(H) (multiplied by r before every step for entries i >= 4, as the reference's
+ * test `i < 4` reads the list index), r = lambda 10^(ln lambda + 14). */
+delta_status delta_zoltan_penalty(delta_ctx *ctx, uint32_t it, uint32_t nt, const double a[3], const double b[3],
+                                  const double c[3], const double *const d[3], const double *const e[3],
+                                  const double *const f[3], double *const p[3], double *const q[3]);
+/* hybrid(it, nt, ...), zoltan/hybrid.cpp:37-131: batches k in [it, nt/4) of entries
+ * 4k..4k+3 (it counts batches; entries past the last full batch are not visited); 7
+ * penalty steps per entry; when the batch's mean error exceeds 1e-8, every entry of the
+ * batch gets the points of the segment-triangle / vertex-face / edge-edge bf of
+ * hybrid.cpp:646-886 applied to the batch's last entry (the reference's serial loop reuses
+ * the last D, E, F), with that bf's own quirks (SMALL_NUM 1e-8; Q's y and z of an
+ * edge-edge point start from p4's x, hybrid.cpp:436-437). */
+delta_status delta_zoltan_hybrid(delta_ctx *ctx, int32_t it, int32_t nt, const double a[3], const double b[3],
+                                 const double c[3], const double *const d[3], const double *const e[3],
+                                 const double *const f[3], double *const p[3], double *const q[3]);
+/* dynamics::update, zoltan/dynamics.cpp:66-250 (loba and rank unused on one GPU): per body,
+ * the half-step angular update with expmap, v += (step/m) force, rotation *= expmap(step
+ * O), x += step v, and force and torque zeroed; then every triangle's spatial vertices
+ * t[0..2] from its referential ones t[3..5] and its body pid[i].  angular[0..2] is the
+ * referential angular velocity, angular[3..5] the spatial one; position[0..2] the centre,
+ * position[3..5] the referential centre. */
+delta_status delta_zoltan_update(delta_ctx *ctx, int32_t nt, int32_t nb, double *const t[6][3], const int32_t *pid,
+                                 double *const angular[6], double *const linear[3], double *const rotation[9],
+                                 double *const position[6], const double *const inertia[9],
+                                 const double *const inverse[9], const double *mass, double *const force[3],
+                                 double *const torque[3], double step);
+/* dynamics::euler, zoltan/dynamics.cpp:252-297 */
+delta_status delta_zoltan_euler(delta_ctx *ctx, int32_t nb, double *const angular[6], const double *const linear[3],
+                                double *const rotation[9], double *const position[6], double step);
+/* dynamics::integrate, zoltan/dynamics.cpp:299-335: t[0..2] += step v per triangle; a
+ * velocity component flips for every vertex coordinate outside [lo, hi]. */
+delta_status delta_zoltan_integrate(delta_ctx *ctx, double step, const double lo[3], const double hi[3], int32_t nt,
+                                    double *const t[3][3], double *const v[3]);
+/* forces::force, zoltan/forces.cpp:48-205, on one GPU (every body is this rank's, nothing
+ * to migrate): the reference's std::vector<contactpoint> conpnt[nb] becomes contacts
+ * grouped by master body, body i's at [offset[i], offset[i+1]) of n_contacts, with the
+ * slave id (contactpoint pid[1]), point, normal and depth.  force and torque accumulate
+ * onto their inputs in the serial loop's order: per master i, each contact adds granular's
+ * f = (spring depth + damper sqrt(spring m_red) (v_ij . n)) n to i and -f to the slave,
+ * with their torques about each body's centre, then i gets mass_i gravity.  spring and
+ * damper are material::iparam[SPRING/DAMPER][GRANULAR] (zoltan/delta.cpp:69-70 sets 1e2,
+ * 1).  Contacts whose slave is not in [0, nb) add nothing.  Uses context scratch. */
+delta_status delta_zoltan_force(delta_ctx *ctx, int32_t nb, const int64_t *offset, const int32_t *slave,
+                                int64_t n_contacts, const double *const point[3], const double *const normal[3],
+                                const double *depth, const double *const position[6],
+                                const double *const angular[6], const double *const linear[3], const double *mass,
+                                double *const force[3], double *const torque[3], const double gravity[3],
+                                double spring, double damper);
 
 /* ---- on-disk formats ------------------------------------------------------------------
  * The legacy ASCII VTK snapshot of all triangles, as writeGeometryToVTK writes it

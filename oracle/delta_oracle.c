@@ -7,6 +7,7 @@
  * compiled without FMA contraction.  Reference paths are relative to the project root.
  */
 #include "delta_oracle.h"
+#include "oracle_internal.h"
 
 #include <float.h>
 #include <math.h>
@@ -33,7 +34,7 @@ static inline double dot3(const double *a, const double *b) {
 
 /* One edge-edge feature: clamped closest parameters (Sunday's method as written
  * in bf.cpp:586-697) and the distance of the resulting point pair. */
-static double seg_seg_feature(const double *HA, const double *TA, const double *HB,
+double dor_seg_seg_feature(const double *HA, const double *TA, const double *HB,
                               const double *TB, double *sc_out, double *tc_out) {
   double u[3], v[3], w[3];
   for (int k = 0; k < 3; ++k) {
@@ -87,7 +88,7 @@ static double seg_seg_feature(const double *HA, const double *TA, const double *
 /* One vertex-face feature: point X against triangle (V0,V1,V2), Eberly's region
  * classification as written in bf.cpp:920-1090.  Returns the distance, and the
  * parameters s (along V1-V0) and t (along V2-V0). */
-static double pt_tri_feature(const double *V0, const double *V1, const double *V2,
+double dor_pt_tri_feature(const double *V0, const double *V1, const double *V2,
                              const double *X, double *s_out, double *t_out) {
   double E0[3], E1[3], Dv[3];
   for (int k = 0; k < 3; ++k) {
@@ -187,7 +188,7 @@ void dor_bf_solver(const double *xA, const double *yA, const double *zA,
   for (int ea = 0; ea < 3; ++ea)
     for (int eb = 0; eb < 3; ++eb) {
       double sc, tc;
-      const double dist = seg_seg_feature(A[ea], A[(ea + 1) % 3], B[eb], B[(eb + 1) % 3], &sc, &tc);
+      const double dist = dor_seg_seg_feature(A[ea], A[(ea + 1) % 3], B[eb], B[(eb + 1) % 3], &sc, &tc);
       if (dist < ssmin) { ssmin = dist; ttc = tc; ssc = sc; ssid = 3 * ea + eb; }
     }
   /* vertex-face minimum: B's vertices against A (j=0..2), A's against B (j=3..5) */
@@ -195,8 +196,8 @@ void dor_bf_solver(const double *xA, const double *yA, const double *zA,
   int id = 0;
   for (int j = 0; j < 6; ++j) {
     double s, t, dist;
-    if (j < 3) dist = pt_tri_feature(A[0], A[1], A[2], B[j], &s, &t);
-    else dist = pt_tri_feature(B[0], B[1], B[2], A[j - 3], &s, &t);
+    if (j < 3) dist = dor_pt_tri_feature(A[0], A[1], A[2], B[j], &s, &t);
+    else dist = dor_pt_tri_feature(B[0], B[1], B[2], A[j - 3], &s, &t);
     if (dist < ptmin) { ptmin = dist; ss = s; tt = t; id = j; }
   }
   if (ptmin > ssmin) { /* bf.cpp:1102 */

@@ -170,6 +170,36 @@ void dor_filter_old(int64_t ns, const double *xs, int64_t lds, const int32_t *ms
                     const double *xn, int64_t ldn, const int32_t *mn, const int32_t *sn, double eps,
                     uint8_t *keep);
 
+/* ---- the zoltan/ code path (zoltan_oracle.c) ------------------------------------------
+ * Planar layouts: d, e, f, p, q hold 3 planes of ld doubles (plane k = coordinate k);
+ * per-body vectors plane k of nb; triangles t: plane 3*v + k of ldt (v = 0..2 spatial,
+ * 3..5 referential vertices). */
+/* zoltan/bf.cpp:26-952 for one pair; returns 1 on its early return (pq untouched). */
+int dzo_bf(const double *xA, const double *yA, const double *zA, const double *xB, const double *yB,
+           const double *zB, double pq[6]);
+/* bf(it, nt, ...) (declared at zoltan/bf.h:61-64): dzo_bf for i in [it, nt) */
+void dzo_bf_soa(uint32_t it, uint32_t nt, const double a[3], const double b[3], const double c[3], const double *d,
+                const double *e, const double *f, int64_t ld, double *p, double *q);
+/* penalty(it, nt, ...), zoltan/penalty.cpp:27-209 */
+void dzo_penalty(uint32_t it, uint32_t nt, const double a[3], const double b[3], const double c[3],
+                 const double *d, const double *e, const double *f, int64_t ld, double *p, double *q);
+/* hybrid(it, nt, ...), zoltan/hybrid.cpp:37-131 (it counts batches of 4) */
+void dzo_hybrid(int32_t it, int32_t nt, const double a[3], const double b[3], const double c[3], const double *d,
+                const double *e, const double *f, int64_t ld, double *p, double *q);
+/* dynamics::update, euler, integrate (zoltan/dynamics.cpp:66-335) */
+void dzo_update(int32_t nt, int32_t nb, double *t, int64_t ldt, const int32_t *pid, double *angular,
+                double *linear, double *rotation, double *position, const double *inertia, const double *inverse,
+                const double *mass, double *force, double *torque, double step);
+void dzo_euler(int32_t nb, double *angular, const double *linear, double *rotation, double *position, double step);
+void dzo_integrate(double step, const double lo[3], const double hi[3], int32_t nt, double *t, int64_t ldt,
+                   double *v);
+/* forces::force (zoltan/forces.cpp:48-205) on one process; contacts grouped by master:
+ * [offset[i], offset[i+1]), fields as 3 planes (point, normal) or one (depth) of ldc. */
+void dzo_force(int32_t nb, const int64_t *offset, const int32_t *slave, const double *point, const double *normal,
+               const double *depth, int64_t ldc, const double *position, const double *angular, const double *linear,
+               const double *mass, double *force, double *torque, const double gravity[3], double spring,
+               double damper);
+
 #ifdef __cplusplus
 }
 #endif

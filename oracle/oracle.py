@@ -169,17 +169,70 @@ class _Lib:
         return L
 
 
-class Oracle(_Lib):
+class _Zoltan:
+    """The zoltan/ narrowphase functions (SoA "one triangle against a list" shape)."""
+
+    zprefix = ""
+
+    def _zsig(self):
+        L, pre = self.zlib, self.zprefix
+        vp, i32, i64, u32 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32
+        getattr(L, pre + "bf").argtypes = [vp] * 7
+        getattr(L, pre + "penalty").argtypes = [u32, u32, vp, vp, vp, vp, vp, vp, i64, vp, vp]
+        getattr(L, pre + "hybrid").argtypes = [i32, i32, vp, vp, vp, vp, vp, vp, i64, vp, vp]
+
+    def zoltan_bf_pairs(self, a, b, p0=None, q0=None):
+        """zoltan/bf.cpp's per-pair bf over pair-list planes a, b (9, n); p0/q0 (3, n) are
+        the values left where it returns early (default NaN)."""
+        a = np.ascontiguousarray(a, np.float64); b = np.ascontiguousarray(b, np.float64)
+        n = a.shape[1]
+        p = np.full((3, n), np.nan) if p0 is None else np.array(p0, np.float64)
+        q = np.full((3, n), np.nan) if q0 is None else np.array(q0, np.float64)
+        f = getattr(self.zlib, self.zprefix + "bf")
+        pq = np.empty(6)
+        for i in range(n):
+            xa, ya, za = (np.ascontiguousarray(a[[k, 3 + k, 6 + k], i]) for k in range(3))
+            xb, yb, zb = (np.ascontiguousarray(b[[k, 3 + k, 6 + k], i]) for k in range(3))
+            pq[:3] = p[:, i]; pq[3:] = q[:, i]
+            f(_p(xa), _p(ya), _p(za), _p(xb), _p(yb), _p(zb), _p(pq))
+            p[:, i] = pq[:3]; q[:, i] = pq[3:]
+        return p, q
+
+    def zoltan_soa(self, method, it, nt, abc, d, e, f, p0=None, q0=None):
+        """method "penalty" or "hybrid" (and "bf" for the oracle): triangle abc (3, 3) rows
+        a, b, c against the list d, e, f (3, n); returns p, q (3, n) starting from p0, q0."""
+        abc = np.ascontiguousarray(abc, np.float64)
+        d, e, f = (np.ascontiguousarray(x, np.float64) for x in (d, e, f))
+        n = d.shape[1]
+        p = np.full((3, n), np.nan) if p0 is None else np.array(p0, np.float64)
+        q = np.full((3, n), np.nan) if q0 is None else np.array(q0, np.float64)
+        fn = getattr(self.zlib, self.zprefix + method)
+        fn(it, nt, _p(abc[0]), _p(abc[1]), _p(abc[2]), _p(d), _p(e), _p(f), n, _p(p), _p(q))
+        return p, q
+
+
+class Oracle(_Lib, _Zoltan):
     """The C restatement (liboracle.so)."""
 
     prefix = "dor_"
+    zprefix = "dzo_"
 
     def __init__(self, path: str | os.PathLike | None = None):
         path = Path(path) if path else HERE / "liboracle.so"
         if not _build_if_missing(path):
             raise RuntimeError(f"oracle library missing: {path}")
         self.lib = C.CDLL(str(path))
+        self.zlib = self.lib
         self._sig()
+        self._zsig()
+        vp0, i32_, i64_, u32_, f8_ = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32, C.c_double
+        self.lib.dzo_bf_soa.argtypes = [u32_, u32_, vp0, vp0, vp0, vp0, vp0, vp0, i64_, vp0, vp0]
+        self.lib.dzo_update.argtypes = [i32_, i32_, vp0, i64_, vp0, vp0, vp0, vp0, vp0, vp0, vp0, vp0, vp0, vp0,
+                                        f8_]
+        self.lib.dzo_euler.argtypes = [i32_, vp0, vp0, vp0, vp0, f8_]
+        self.lib.dzo_integrate.argtypes = [f8_, vp0, vp0, i32_, vp0, i64_, vp0]
+        self.lib.dzo_force.argtypes = [i32_, vp0, vp0, vp0, vp0, vp0, i64_, vp0, vp0, vp0, vp0, vp0, vp0, vp0,
+                                       f8_, f8_]
         L = self.lib
         vp, i32, i64, f8 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
         L.dor_contacts_forces.argtypes = [vp, i64, f8, vp, vp, vp, f8, vp, vp, vp, f8, vp, vp, vp]
@@ -193,6 +246,46 @@ class Oracle(_Lib):
         L.dor_sim_contacts.restype = i64
         L.dor_filter_new.argtypes = [i64, vp, i64, vp, vp, f8, vp]
         L.dor_filter_old.argtypes = [i64, vp, i64, vp, vp, i64, vp, i64, vp, vp, f8, vp]
+
+    # ---- zoltan dynamics and forces (zoltan_oracle.c) ------------------------------------
+    def zoltan_update(self, t, pid, angular, linear, rotation, position, inertia, inverse, mass, force, torque, step):
+        """dynamics::update on copies; t (6, 3, nt), per-body arrays (k, nb).  Returns the
+        updated (t, angular, linear, rotation, position, force, torque)."""
+        t = np.array(t, np.float64, copy=True).reshape(18, -1)
+        nt = t.shape[1]
+        out = [np.array(x, np.float64, copy=True) for x in (angular, linear, rotation, position, force, torque)]
+        inertia = np.ascontiguousarray(inertia, np.float64); inverse = np.ascontiguousarray(inverse, np.float64)
+        mass = np.ascontiguousarray(mass, np.float64); pid = np.ascontiguousarray(pid, np.int32)
+        self.lib.dzo_update(nt, len(mass), _p(t), nt, _p(pid), _p(out[0]), _p(out[1]), _p(out[2]), _p(out[3]),
+                            _p(inertia), _p(inverse), _p(mass), _p(out[4]), _p(out[5]), step)
+        return (t.reshape(6, 3, nt), *out)
+
+    def zoltan_euler(self, angular, linear, rotation, position, step):
+        out = [np.array(x, np.float64, copy=True) for x in (angular, rotation, position)]
+        linear = np.ascontiguousarray(linear, np.float64)
+        self.lib.dzo_euler(linear.shape[1], _p(out[0]), _p(linear), _p(out[1]), _p(out[2]), step)
+        return tuple(out)
+
+    def zoltan_integrate(self, step, lo, hi, t, v):
+        t = np.array(t, np.float64, copy=True).reshape(9, -1)
+        v = np.array(v, np.float64, copy=True)
+        lo = np.ascontiguousarray(lo, np.float64); hi = np.ascontiguousarray(hi, np.float64)
+        nt = t.shape[1]
+        self.lib.dzo_integrate(step, _p(lo), _p(hi), nt, _p(t), nt, _p(v))
+        return t.reshape(3, 3, nt), v
+
+    def zoltan_force(self, offset, slave, point, normal, depth, position, angular, linear, mass, force, torque,
+                     gravity, spring=1e2, damper=1.0):
+        """forces::force; returns the accumulated (force, torque) copies."""
+        F = np.array(force, np.float64, copy=True); T = np.array(torque, np.float64, copy=True)
+        offset = np.ascontiguousarray(offset, np.int64); slave = np.ascontiguousarray(slave, np.int32)
+        point, normal, position, angular, linear = (np.ascontiguousarray(x, np.float64)
+                                                    for x in (point, normal, position, angular, linear))
+        depth = np.ascontiguousarray(depth, np.float64); mass = np.ascontiguousarray(mass, np.float64)
+        g = np.ascontiguousarray(gravity, np.float64)
+        self.lib.dzo_force(len(mass), _p(offset), _p(slave), _p(point), _p(normal), _p(depth), len(slave),
+                           _p(position), _p(angular), _p(linear), _p(mass), _p(F), _p(T), _p(g), spring, damper)
+        return F, T
 
     def filter_new(self, x, master, slave, eps=1e-4):
         """keep flags of filterNewContacts per (master, slave) segment; x is (3, n)."""
@@ -242,6 +335,23 @@ class Oracle(_Lib):
         return s, cps[:nsteps], out[:n]
 
 
+class ZoltanReference(_Zoltan):
+    """The reference's zoltan/{bf,penalty,hybrid}.cpp (oracle/_ref/libzoltan_ref.so)."""
+
+    zprefix = "zref_"
+
+    def __init__(self):
+        path = HERE / "_ref" / "libzoltan_ref.so"
+        if not path.exists():
+            raise FileNotFoundError(path)
+        self.zlib = C.CDLL(str(path))
+        self._zsig()
+
+    @staticmethod
+    def available() -> bool:
+        return (HERE / "_ref" / "libzoltan_ref.so").exists()
+
+
 class Reference(_Lib):
     """The reference's own functions (oracle/_ref), built by oracle/Makefile."""
 
@@ -277,6 +387,29 @@ class Reference(_Lib):
         keep = np.zeros(xn.shape[1], np.uint8)
         self.lib.ref_filter_old(xs.shape[1], _p(xs), xs.shape[1], xn.shape[1], _p(xn), xn.shape[1], _p(keep))
         return keep
+
+    def simulate(self, scene: dict, dt, gravity, nsteps):
+        """Runs nsteps of the reference-driven time step (ref_sim.cpp) on a copy of `scene`
+        (force constants: those compiled into forces.cpp).  Returns (new_scene, contacts_per_step)."""
+        s = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in scene.items()}
+        sc = Scene()
+        sc.n_bodies = s["n_bodies"]
+        for name in ("tri_offset", "x", "y", "z", "rx", "ry", "rz", "pos", "ref_pos", "vel", "ang", "ref_ang",
+                     "rot", "inertia", "inverse", "mass", "eps", "radius", "friction", "obstacle"):
+            setattr(sc, name, s[name].ctypes.data)
+        L = self.lib
+        L.ref_sim_create.restype = C.c_void_p
+        L.ref_sim_destroy.argtypes = [C.c_void_p]
+        L.ref_sim_run.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int32, C.c_void_p]
+        L.ref_sim_run.restype = C.c_int64
+        cps = np.zeros(max(nsteps, 1), np.int64)
+        g = np.ascontiguousarray(gravity, np.float64)
+        sim = L.ref_sim_create()
+        try:
+            L.ref_sim_run(sim, C.byref(sc), dt, _p(g), nsteps, _p(cps))
+        finally:
+            L.ref_sim_destroy(sim)
+        return s, cps[:nsteps]
 
     @staticmethod
     def available(flavour: str = "par") -> bool:

@@ -47,12 +47,31 @@ def test_trajectory_bit_exact(ctx, oracle, scene, steps):
         assert np.array_equal(g_state[k], o_state[k]), k
 
 
-def test_certified_driver_gives_the_same_trajectory(ctx, scene):
+@pytest.mark.parametrize("driver", [8, 9])
+def test_culled_drivers_give_the_same_trajectory(ctx, scene, driver):
+    """The certified driver (box culling + certified FP32/FP64 solver) and the culled FP64
+    driver (box culling + FP64 bfSolver) give FP64 bf's trajectory and contacts bit for bit."""
     a_state, a_cps, a_c = _gpu(ctx, scene, 20, driver=0)
-    b_state, b_cps, b_c = _gpu(ctx, scene, 20, driver=8)
+    b_state, b_cps, b_c = _gpu(ctx, scene, 20, driver=driver)
     assert list(a_cps) == list(b_cps)
     for k in STATE:
         assert np.array_equal(a_state[k], b_state[k]), k
+    for f in FIELDS:
+        assert np.array_equal(a_c[f], b_c[f]), f
+
+
+def test_culled_fp64_driver_graph_equals_stepping(ctx, scene):
+    from delta_b200.engine import Simulation, StepParams
+
+    p = StepParams.make(**PARAMS)
+    a_state, a_cps, _ = _gpu(ctx, scene, 25, driver=9)
+    sim = Simulation(ctx, scene, 9)
+    cps = sim.step(25, p, graph=True)
+    st = sim.state()
+    sim.close()
+    assert list(cps) == list(a_cps)
+    for k in STATE:
+        assert np.array_equal(st[k], a_state[k]), k
 
 
 def test_friction_trajectory_bit_exact(ctx, oracle):

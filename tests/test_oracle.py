@@ -114,3 +114,22 @@ def test_forces_match_reference_build(oracle):
     F1, T1 = oracle.contacts_forces(c, 1.0, *st, 1e4, 0.5, 0.5)
     F2, T2 = ref.contacts_forces(c, *st)
     assert np.array_equal(F1, F2) and np.array_equal(T1, T2)
+
+
+def test_time_step_equals_the_reference_driven_step(oracle):
+    """The oracle's time step (dor_sim_run) against a time step driven by the reference's
+    own bf(), getContactsForces, updateAngular, updateRotationMatrix and updateVertices
+    (oracle/ref_sim.cpp), with forces.cpp's compiled constants: bit for bit."""
+    from oracle.oracle import Reference
+
+    if not Reference.available("par"):
+        pytest.skip("oracle/_ref not built (the reference sources are absent)")
+    from delta_b200.scenarios import lattice_scene
+
+    sc = lattice_scene(seed=7, nx=4, ny=2, nz=4, friction=True)
+    dt, g = 1e-5, (0.0, -9.81, 0.0)
+    o_state, o_cps, _ = oracle.simulate(sc, dt, g, 1e4, 0.5, 0.5, 4)
+    r_state, r_cps = Reference("par").simulate(sc, dt, g, 4)
+    assert list(o_cps) == list(r_cps) and o_cps[-1] > 0
+    for k in ("pos", "vel", "ang", "ref_ang", "rot", "x", "y", "z"):
+        assert np.array_equal(o_state[k], r_state[k]), k
