@@ -198,7 +198,29 @@ def _time_sim(ctx, stream, sim, steps, params, graph):
             "CUDA events"}
 
 
-def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, params):
+def cpu_timestep_rate(scene, params, steps: int):
+    """Timesteps/s of the reference-driven time step (oracle/_ref, ref_sim.cpp: the reference's
+    bf() on every triangle pair of every candidate body pair, getContactsForces,
+    updateAngular, updateRotationMatrix, updateVertices) on all host threads."""
+    from oracle.oracle import Reference
+
+    if not Reference.available("omp"):
+        return None
+    ref = Reference("omp")
+    dt = float(params.dt)
+    g = [float(params.gravity[k]) for k in range(3)]
+    warm, _ = ref.simulate(scene, dt, g, 1)  # the first detection (contacts for the next step)
+    t0 = time.perf_counter()
+    _, cps = ref.simulate(warm, dt, g, steps)
+    el = time.perf_counter() - t0
+    return {"value": steps / el, "unit": "timesteps/s", "cores": os.cpu_count() or 1, "kind": "reference",
+            "sample": f"{steps} time steps after one warm-up step; the reference's bf() over all triangle pairs "
+                      "of the candidate body pairs, getContactsForces with forces.cpp's compiled constants, "
+                      "dynamics.cpp's updates; OpenMP over candidate pairs and bodies",
+            "contacts_last_step": int(cps[-1]) if len(cps) else 0}
+
+
+def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, params, cpu_steps: int = 0):
     """Timesteps/s of a scene with the plain FP64 bf driver (every triangle pair of every
     candidate body pair, as the reference) and with the certified FP32 driver (exact box
     culling + bf_cert), stepped and replayed as a CUDA graph.  All three must give the same
@@ -225,7 +247,8 @@ def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, para
         "max_abs_vel_m_per_s": float(np.max(np.abs(lrn["vel"] - ref["vel"]))),
         "bit_identical": bool(all(np.array_equal(ref[k], lrn[k]) for k in ("pos", "vel", "rot", "x")))}
     sps = {k: v["steps_per_s"] for k, v in out.items()}
-    return {"workload": workload, "steps": steps, "warmup": warmup, **out,
+    cpu = cpu_timestep_rate(scene, params, cpu_steps) if cpu_steps > 0 else None
+    return {"workload": workload, "steps": steps, "warmup": warmup, **out, "cpu_baseline": cpu,
             "speedup": sps["bf_cert_culled_graph"] / sps["fp64_bf"],
             "speedup_learned": sps["learned_culled_graph"] / sps["fp64_bf"],
             "speedup_from_culling": sps["fp64_bf_culled"] / sps["fp64_bf"],
@@ -545,7 +568,8 @@ def main():
             ctx, stream, lattice_scene(args.seed),
             "256 perturbed icospheres (80 tri) on a 8x4x8 lattice over a 2-triangle floor, FP64, dt 1e-5, k 1e6, "
             "damping 0.1", args.timestep_steps, 3,
-            StepParams.make(dt=1e-5, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0))
+            StepParams.make(dt=1e-5, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0),
+            cpu_steps=3 if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0)
         if args.box_steps > 0:
             from delta_b200.scenarios import box_scene
 
@@ -559,7 +583,8 @@ def main():
                 ctx, stream, hopper_scene(10000, seed=args.seed),
                 "10,000 perturbed spheres of {40,80,160,320} triangles (r 5-15 mm) over a conical hopper of 2,048 "
                 "wall triangles (30 deg, 8 cm outlet), FP64, dt 5e-6", args.hopper_steps, 3,
-                StepParams.make(dt=5e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0))
+                StepParams.make(dt=5e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0),
+                cpu_steps=2 if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -50,6 +50,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_write_vtk_host": ([C.c_char_p, i32, i32, vp, vp, vp, vp], C.c_int),
     "delta_write_vtk": ([vp, C.c_char_p, i32, vp], C.c_int),
     "delta_sim_write_vtk": ([vp, C.c_char_p, i32], C.c_int),
+    "delta_write_vtu_host": ([C.c_char_p, i32, i64, vp, vp, vp], C.c_int),
+    "delta_sim_write_vtu": ([vp, C.c_char_p, i32], C.c_int),
     "delta_read_mbfcp": ([C.c_char_p, vp, i64, vp], C.c_int),
     "delta_filter_new_contacts": ([vp, vp, i64, f8, vp], C.c_int),
     "delta_filter_old_contacts": ([vp, vp, i64, vp, i64, f8, vp], C.c_int),

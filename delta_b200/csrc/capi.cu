@@ -160,6 +160,7 @@ delta_status delta_destroy(delta_ctx *ctx) {
   if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
   if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->gemm_err) cudaFree(ctx->gemm_err);
   delete ctx;
   return DELTA_OK;
 }
@@ -172,7 +173,15 @@ delta_status delta_set_stream(delta_ctx *ctx, void *stream) {
 
 delta_status delta_synchronize(delta_ctx *ctx) {
   if (!ctx) return set_error(DELTA_ERR_INVALID, "null context");
-  return cuda_error(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess || !ctx->gemm_err) return cuda_error(e, "cudaStreamSynchronize");
+  // a tcgen05 GEMM whose bounded wait gave up (its output was set to NaN) since the last check
+  int flag = 0;
+  if ((e = cudaMemcpy(&flag, ctx->gemm_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return cuda_error(e, "gemm flag");
+  if (!flag) return DELTA_OK;
+  cudaMemset(ctx->gemm_err, 0, sizeof(int));
+  return set_error(DELTA_ERR_TIMEOUT, "tcgen05 GEMM: bounded wait for the tensor cores gave up");
 }
 
 int64_t delta_launch_count(const delta_ctx *ctx) { return ctx ? ctx->launches : 0; }

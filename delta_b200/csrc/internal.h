@@ -85,7 +85,8 @@ struct delta_ctx {
   // host-buffer entry points: copy streams and per-chunk events of the pipelined transfers
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t events[3 * 16] = {};
-  int mlp_engine = DELTA_MLP_TCGEN05;  // network engine of the learned hybrid
+  int mlp_engine = DELTA_MLP_TCGEN05;  // network engine of the learned hybrid and its training GEMM
+  int *gemm_err = nullptr;             // device flag: a tcgen05 GEMM's bounded wait gave up
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
 };

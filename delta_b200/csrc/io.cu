@@ -41,6 +41,58 @@ delta_status write_vtk(const std::string &path, int32_t step, int32_t n_bodies, 
   return ok ? DELTA_OK : set_error(DELTA_ERR_INVALID, "delta_write_vtk: write failed: " + filename);
 }
 
+// writeGeometryToVTKVTK (delta/core/io/write.cpp:10-70) without the VTK library: the same
+// unstructured grid of particle centres, written as ASCII VTK XML.  The reference inserts
+// the centres into a vtkPoints (float by default, so Float32), the linear velocity as the
+// "direction" vectors and then calls SetScalars twice, radius and then epsilon; the second
+// call replaces the first attribute, so the file holds "direction" and "epsilon" (Float64)
+// and no cells.  The reference's writer encodes the arrays in binary; the arrays and their
+// values are the same.
+delta_status write_vtu(const std::string &path, int32_t step, int64_t n, const double *centre,
+                       const double *velocity, const double *eps) {
+  const std::string filename = path + "geometry_" + std::to_string(step) + ".vtu";
+  FILE *fp = std::fopen(filename.c_str(), "w");
+  if (!fp) return set_error(DELTA_ERR_INVALID, "delta_write_vtu: cannot open " + filename + ": " + std::strerror(errno));
+  std::fprintf(fp,
+               "<?xml version=\"1.0\"?>\n"
+               "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
+               "  <UnstructuredGrid>\n"
+               "    <Piece NumberOfPoints=\"%lld\" NumberOfCells=\"0\">\n"
+               "      <PointData Scalars=\"epsilon\" Vectors=\"direction\">\n"
+               "        <DataArray type=\"Float64\" Name=\"direction\" NumberOfComponents=\"3\" format=\"ascii\">\n",
+               (long long)n);
+  for (int64_t i = 0; i < n; ++i)
+    std::fprintf(fp, "%.17g %.17g %.17g\n", velocity[i], velocity[n + i], velocity[2 * n + i]);
+  std::fputs("        </DataArray>\n"
+             "        <DataArray type=\"Float64\" Name=\"epsilon\" format=\"ascii\">\n", fp);
+  for (int64_t i = 0; i < n; ++i) std::fprintf(fp, "%.17g\n", eps[i]);
+  std::fputs("        </DataArray>\n"
+             "      </PointData>\n"
+             "      <CellData>\n"
+             "      </CellData>\n"
+             "      <Points>\n"
+             "        <DataArray type=\"Float32\" Name=\"Points\" NumberOfComponents=\"3\" format=\"ascii\">\n", fp);
+  for (int64_t i = 0; i < n; ++i)
+    std::fprintf(fp, "%.9g %.9g %.9g\n", (double)(float)centre[i], (double)(float)centre[n + i],
+                 (double)(float)centre[2 * n + i]);
+  std::fputs("        </DataArray>\n"
+             "      </Points>\n"
+             "      <Cells>\n"
+             "        <DataArray type=\"Int64\" Name=\"connectivity\" format=\"ascii\">\n"
+             "        </DataArray>\n"
+             "        <DataArray type=\"Int64\" Name=\"offsets\" format=\"ascii\">\n"
+             "        </DataArray>\n"
+             "        <DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\">\n"
+             "        </DataArray>\n"
+             "      </Cells>\n"
+             "    </Piece>\n"
+             "  </UnstructuredGrid>\n"
+             "</VTKFile>\n", fp);
+  const bool ok = std::ferror(fp) == 0;
+  std::fclose(fp);
+  return ok ? DELTA_OK : set_error(DELTA_ERR_INVALID, "delta_write_vtu: write failed: " + filename);
+}
+
 // std::stoi / std::stof / std::stod on a substring as read.cpp does; false on a parse error
 template <class F>
 bool parse_at(const std::string &line, size_t pos, size_t len, F conv) {
@@ -65,6 +117,13 @@ delta_status delta_write_vtk_host(const char *path, int32_t step, int32_t n_bodi
   if (!path || n_bodies < 0 || !tri_offset || (tri_offset[n_bodies] > tri_offset[0] && (!x || !y || !z)))
     return set_error(DELTA_ERR_INVALID, "delta_write_vtk_host: bad argument");
   return write_vtk(path, step, n_bodies, tri_offset, x, y, z);
+}
+
+delta_status delta_write_vtu_host(const char *path, int32_t step, int64_t n, const double *centre,
+                                  const double *velocity, const double *eps) {
+  if (!path || n < 0 || (n > 0 && (!centre || !velocity || !eps)))
+    return set_error(DELTA_ERR_INVALID, "delta_write_vtu_host: bad argument");
+  return write_vtu(path, step, n, centre, velocity, eps);
 }
 
 delta_status delta_write_vtk(delta_ctx *ctx, const char *path, int32_t step, const delta_meshes *meshes) {

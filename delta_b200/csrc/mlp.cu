@@ -681,6 +681,168 @@ __global__ void __launch_bounds__(kTcThreads, 2)
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// the training GEMM on the 5th-generation tensor cores: C[M,N] (+)= op(A)[M,K] op(B)[K,N]
+// with BF16 operands and an FP32 TMEM accumulator.  A CTA of 128 threads owns a 128 x 128
+// output tile (M rows = TMEM lanes, N columns) and a K range; its K range is taken in
+// chunks of 64: the threads stage the chunk's A and B tiles into shared memory in the
+// canonical K-major layout (transposing while they stage when the operand is stored the
+// other way), one thread issues the chunk's K/16 MMAs and commits them to an mbarrier
+// (bounded wait), and the TMEM accumulator carries the sum over the CTA's whole K range.
+// With split-K each CTA writes its partial tile to a workspace and k_gemm_reduce adds the
+// partials in split order, so the result does not depend on scheduling (no atomics).
+// ---------------------------------------------------------------------------------------
+constexpr int kGtRows = 128, kGtK = 64, kGtThreads = 128;
+
+struct GemmTcSmem {
+  __nv_bfloat16 a[kGtRows * kGtK];  // 16 KB: A chunk, canonical K-major [128][64]
+  __nv_bfloat16 b[kGtRows * kGtK];  // 16 KB: B chunk, canonical K-major [N tile][64]
+  uint64_t mbar;
+  uint32_t tmem_base;
+  int abort;
+};
+
+// Stages rows [r0, r0+128) x k [k0, k0+64) of X into the canonical K-major tile dst, where
+// element (r, k) is X[r*ld + k] (trans = 0) or X[k*ld + r] (trans = 1); rows >= rmax and
+// k >= kend are zero.
+__device__ __forceinline__ void gt_stage(__nv_bfloat16 *dst, const __nv_bfloat16 *__restrict__ X, int ld, int trans,
+                                         int r0, int rmax, int k0, int kend) {
+  const int tid = threadIdx.x;
+  char *d = reinterpret_cast<char *>(dst);
+  const bool vec = !trans && (ld % 8 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+  if (vec) {
+    // 16-byte chunks along k: 128 rows x 8 chunks
+    for (int e = tid; e < kGtRows * (kGtK / 8); e += kGtThreads) {
+      const int r = e >> 3, kc = e & 7, gr = r0 + r, gk = k0 + 8 * kc;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gr < rmax && gk < kend) {
+        if (gk + 8 <= kend) {
+          v = __ldg(reinterpret_cast<const uint4 *>(X + (int64_t)gr * ld + gk));
+        } else {
+          __nv_bfloat16 t[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) t[j] = gk + j < kend ? X[(int64_t)gr * ld + gk + j] : __float2bfloat16(0.f);
+          v = *reinterpret_cast<const uint4 *>(t);
+        }
+      }
+      *reinterpret_cast<uint4 *>(d + tc_chunk(r, kc, kGtK)) = v;
+    }
+  } else {
+    // pairs (k, k+1) of one row per thread, 4-byte stores; consecutive threads take
+    // consecutive rows, so the transposed loads are coalesced
+    for (int e = tid; e < kGtRows * (kGtK / 2); e += kGtThreads) {
+      const int r = e & (kGtRows - 1), k = 2 * (e >> 7), gr = r0 + r;
+      __nv_bfloat16 v0 = __float2bfloat16(0.f), v1 = v0;
+      if (gr < rmax) {
+        const int g0 = k0 + k, g1 = g0 + 1;
+        if (g0 < kend) v0 = trans ? X[(int64_t)g0 * ld + gr] : X[(int64_t)gr * ld + g0];
+        if (g1 < kend) v1 = trans ? X[(int64_t)g1 * ld + gr] : X[(int64_t)gr * ld + g1];
+      }
+      __nv_bfloat162 pr;
+      pr.x = v0;
+      pr.y = v1;
+      *reinterpret_cast<__nv_bfloat162 *>(d + tc_chunk(r, k >> 3, kGtK) + (k & 7) * 2) = pr;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kGtThreads) k_gemm_tc(int M, int N, int K, const __nv_bfloat16 *__restrict__ A,
+                                                        int lda, int trans_a, const __nv_bfloat16 *__restrict__ B,
+                                                        int ldb, int trans_b, float *__restrict__ Cm, int ldc,
+                                                        int accumulate, int k_per_split, float *__restrict__ part,
+                                                        int *__restrict__ err, uint32_t spin) {
+  __shared__ __align__(128) GemmTcSmem sm;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int n0 = blockIdx.x * kGtRows, m0 = blockIdx.y * kGtRows;
+  const int kb = blockIdx.z * k_per_split, ke = min(K, kb + k_per_split);
+  const int nvalid = min(kGtRows, N - n0), ntile = (nvalid + 15) / 16 * 16;
+  if (tid == 0) {
+    sm.abort = 0;
+    const unsigned a = (unsigned)__cvta_generic_to_shared(&sm.mbar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(&sm.tmem_base);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  uint32_t phase = 0;
+  bool issued = false;
+  for (int k0 = kb; k0 < ke && !sm.abort; k0 += kGtK) {
+    gt_stage(sm.a, A, lda, trans_a, m0, M, k0, ke);
+    gt_stage(sm.b, B, ldb, !trans_b, n0, N, k0, ke);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sm.a), b0 = (uint32_t)__cvta_generic_to_shared(sm.b);
+      const uint32_t idesc = tc_idesc(kGtRows, ntile);
+      const int steps = (min(kGtK, ke - k0) + 15) / 16;
+      for (int s = 0; s < steps; ++s)
+        tc_mma(sm.tmem_base, tc_desc(a0 + 256u * s, 16u * kGtK), tc_desc(b0 + 256u * s, 16u * kGtK), idesc,
+               (issued || s > 0) ? 1u : 0u);
+      tc_commit(&sm.mbar);
+      if (!tc_wait(&sm.mbar, phase, spin)) sm.abort = 1;
+    }
+    issued = true;
+    __syncthreads();
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  // epilogue: thread t owns row m0 + t (TMEM lane t)
+  const int m = m0 + tid;
+  const uint32_t tlane = sm.tmem_base + ((uint32_t)(warp * 32) << 16);
+  const bool ok = !sm.abort;
+  for (int c = 0; c < ntile; c += 16) {
+    float v[16];
+    if (issued && ok) {
+      tc_ld16(tlane + (uint32_t)c, v);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = ok ? 0.f : __int_as_float(0x7fc00000);
+    }
+    if (m < M) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + c + j;
+        if (c + j < nvalid) {
+          if (part) {
+            part[((int64_t)blockIdx.z * M + m) * N + n] = v[j];
+          } else {
+            float *dst = Cm + (int64_t)m * ldc + n;
+            *dst = accumulate ? *dst + v[j] : v[j];
+          }
+        }
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem_base), "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// C[m][n] = (accumulate ? C[m][n] : 0) + sum over s in split order of part[s][m][n]
+__global__ void k_gemm_reduce(int M, int N, int splits, const float *__restrict__ part, float *__restrict__ Cm,
+                              int ldc, int accumulate) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)M * N) return;
+  const int m = (int)(e / N), n = (int)(e % N);
+  float acc = accumulate ? Cm[(int64_t)m * ldc + n] : 0.f;
+  for (int s = 0; s < splits; ++s) acc += part[(int64_t)s * M * N + e];
+  Cm[(int64_t)m * ldc + n] = acc;
+}
+
 // penaltySolver (penalty.cpp:434-582, adaptive, FP64 reference arithmetic) started from
 // x0 (4 floats per pair) instead of 0.33; iterations written to iters.
 __global__ void k_penalty_warm(int64_t n, const double *a, const double *b, int64_t ld, const float *x0,
@@ -1124,6 +1286,34 @@ delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A,
     return set_error(DELTA_ERR_INVALID, "delta_gemm_bf16: bad argument");
   if (M == 0 || N == 0) return DELTA_OK;
   cudaError_t e = cudaSuccess;
+  if (ctx->mlp_engine == DELTA_MLP_TCGEN05) {
+    if (!ctx->gemm_err) {
+      if ((e = cudaMalloc(&ctx->gemm_err, sizeof(int))) != cudaSuccess) return cuda_error(e, "gemm flag");
+      if ((e = cudaMemsetAsync(ctx->gemm_err, 0, sizeof(int), ctx->stream)) != cudaSuccess)
+        return cuda_error(e, "gemm flag");
+    }
+    int per = (K + split_k - 1) / split_k;
+    per = (per + kGtK - 1) / kGtK * kGtK;
+    if (per <= 0) per = kGtK;
+    const int splits = K > 0 ? (K + per - 1) / per : 1;
+    float *part = nullptr;
+    if (splits > 1) {
+      void *buf;
+      delta_status st = ctx_scratch(ctx, 28, sizeof(float) * (size_t)splits * M * N, &buf);
+      if (st != DELTA_OK) return st;
+      part = static_cast<float *>(buf);
+    }
+    dim3 grid((N + kGtRows - 1) / kGtRows, (M + kGtRows - 1) / kGtRows, splits);
+    k_gemm_tc<<<grid, kGtThreads, 0, ctx->stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, trans_a,
+                                                    (const __nv_bfloat16 *)B, ldb, trans_b, C, ldc, accumulate, per,
+                                                    part, ctx->gemm_err, kTcSpin);
+    ctx->launches += 1;
+    if (splits > 1) {
+      k_gemm_reduce<<<nblk((int64_t)M * N), 256, 0, ctx->stream>>>(M, N, splits, part, C, ldc, accumulate);
+      ctx->launches += 1;
+    }
+    return cuda_error(cudaGetLastError(), "delta_gemm_bf16 (tcgen05)");
+  }
   if (!accumulate && (split_k > 1)) e = cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * ldc, ctx->stream);
   if (e != cudaSuccess) return cuda_error(e, "gemm memset");
   int per = (K + split_k - 1) / split_k;

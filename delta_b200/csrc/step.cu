@@ -1807,4 +1807,19 @@ delta_status delta_sim_write_vtk(delta_sim *sim, const char *path, int32_t step)
   return delta_write_vtk(sim->ctx, path, step, &m);
 }
 
+delta_status delta_sim_write_vtu(delta_sim *sim, const char *path, int32_t step) {
+  if (!sim || !path) return set_error(DELTA_ERR_INVALID, "delta_sim_write_vtu: bad argument");
+  cudaError_t e = cudaSuccess;
+  if (sim->g.stream) e = cudaStreamSynchronize(sim->g.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sim->ctx->stream);
+  if (e != cudaSuccess) return cuda_error(e, "delta_sim_write_vtu: sync");
+  const int64_t n = sim->scene.n_bodies;
+  std::vector<double> pos(3 * n), vel(3 * n), eps(n);
+  if ((e = cudaMemcpy(pos.data(), sim->scene.pos, 8 * 3 * n, cudaMemcpyDeviceToHost)) == cudaSuccess &&
+      (e = cudaMemcpy(vel.data(), sim->scene.vel, 8 * 3 * n, cudaMemcpyDeviceToHost)) == cudaSuccess)
+    e = cudaMemcpy(eps.data(), sim->scene.eps, 8 * n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_error(e, "delta_sim_write_vtu: copy");
+  return delta_write_vtu_host(path, step, n, pos.data(), vel.data(), eps.data());
+}
+
 }  // extern "C"

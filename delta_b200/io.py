@@ -40,6 +40,38 @@ def write_vtk(ctx, path, step: int, meshes) -> str:
     return os.path.join(os.fspath(path), f"geometry_{int(step)}.vtk")
 
 
+def write_vtu_host(path, step: int, centre, velocity, eps) -> str:
+    """writeGeometryToVTKVTK (write.cpp:10-70): <path>/geometry_<step>.vtu for n particles
+    (centre, velocity: (3, n); eps: (n,)); returns the file name."""
+    c = np.ascontiguousarray(centre, np.float64); v = np.ascontiguousarray(velocity, np.float64)
+    e = np.ascontiguousarray(eps, np.float64)
+    check(lib().delta_write_vtu_host(_dir(path), int(step), e.shape[0], c.ctypes.data, v.ctypes.data,
+                                     e.ctypes.data))
+    return os.path.join(os.fspath(path), f"geometry_{int(step)}.vtu")
+
+
+def read_vtu(filename) -> dict:
+    """The arrays of a .vtu written by write_vtu_host (ASCII VTK XML): 'points' (n, 3) and
+    every point-data array by name ((n, k) or (n,))."""
+    import xml.etree.ElementTree as ET
+
+    root = ET.parse(os.fspath(filename)).getroot()
+    piece = root.find("UnstructuredGrid/Piece")
+    n = int(piece.get("NumberOfPoints"))
+
+    def arr(da):
+        k = int(da.get("NumberOfComponents", "1"))
+        dt = np.float32 if da.get("type") == "Float32" else np.float64
+        v = np.array((da.text or "").split(), dtype=dt)
+        return v.reshape(n, k) if k > 1 else v
+    out = {"points": arr(piece.find("Points/DataArray")), "cells": int(piece.get("NumberOfCells"))}
+    for da in piece.find("PointData"):
+        out[da.get("Name")] = arr(da)
+    out["active_scalars"] = piece.find("PointData").get("Scalars")
+    out["active_vectors"] = piece.find("PointData").get("Vectors")
+    return out
+
+
 def read_mbfcp(filename, capacity: int = 1024) -> dict:
     """{'bodies', 'materials' (or None), 'id', 'centre' (n, 3), 'radius'} of a .mbfcp file."""
     while True:

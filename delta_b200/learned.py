@@ -155,7 +155,12 @@ class WarmStartMLP:
     def backward(self, X, T, valid, n_valid: int):
         """Gradients of the MSE over valid rows into self.grads (after forward(X))."""
         M = X.shape[0]
-        split = max(1, min(128, M // 1024))
+        # split-K of the weight gradients (K = the batch): the tcgen05 GEMM adds the partial
+        # tiles in a second kernel, so more splits fill the SMs at no atomics cost
+        if getattr(self.ctx, "mlp_engine", "tcgen05") == "tcgen05":
+            split = max(1, min(256, M // 256))
+        else:
+            split = max(1, min(128, M // 1024))
         self.grads.zero_()
         self.loss.zero_()
         h = lib()
@@ -210,6 +215,7 @@ ENGINES = {"tcgen05": 0, "mma": 1}
 def set_engine(ctx: Context, engine: str):
     """Network engine of the learned hybrid on this context: "tcgen05" (default) or "mma"."""
     check(lib().delta_mlp_set_engine(ctx.handle, ENGINES[engine]))
+    ctx.mlp_engine = engine
 
 
 def features(ctx: Context, a, b, p=None, q=None):

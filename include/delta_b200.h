@@ -83,6 +83,8 @@ typedef struct delta_ctx delta_ctx;
 delta_status delta_create(delta_ctx **ctx, int device, void *stream);
 delta_status delta_destroy(delta_ctx *ctx);
 delta_status delta_set_stream(delta_ctx *ctx, void *stream);
+/* Waits for the context's stream; DELTA_ERR_TIMEOUT when a tcgen05 GEMM's bounded wait
+ * gave up since the last call. */
 delta_status delta_synchronize(delta_ctx *ctx);
 const char *delta_last_error(void);
 const char *delta_version(void);
@@ -417,6 +419,15 @@ delta_status delta_zoltan_force(delta_ctx *ctx, int32_t nb, const int64_t *offse
 delta_status delta_write_vtk_host(const char *path, int32_t step, int32_t n_bodies, const int64_t *tri_offset,
                                   const double *x, const double *y, const double *z);
 delta_status delta_write_vtk(delta_ctx *ctx, const char *path, int32_t step, const delta_meshes *meshes);
+/* writeGeometryToVTKVTK (delta/core/io/write.cpp:10-70) without the VTK library:
+ * path + "geometry_<step>.vtu", an ASCII VTK XML unstructured grid of the n particle
+ * centres (centre: 3 planes of n; Float32 points, as vtkPoints stores them), point data
+ * "direction" = the linear velocity (3 planes of n) and "epsilon" (the reference's second
+ * SetScalars call replaces its "radius"), no cells.  Host arrays. */
+delta_status delta_write_vtu_host(const char *path, int32_t step, int64_t n, const double *centre,
+                                  const double *velocity, const double *eps);
+/* The same for a simulation's bodies (centre, velocity, epsilon). */
+delta_status delta_sim_write_vtu(delta_sim *sim, const char *path, int32_t step);
 /* The snapshot of a simulation's current vertices (obstacles included). */
 delta_status delta_sim_write_vtk(delta_sim *sim, const char *path, int32_t step);
 /* The .mbfcp scene reader (readmbfcp, delta/core/io/read.cpp:345-546): the material block's
@@ -467,9 +478,9 @@ delta_status delta_mlp_layout(int64_t offsets[9]);
  * for bit to delta_mlp_features + delta_gemm_bf16 + delta_mlp_bias_act layer by layer. */
 delta_status delta_mlp_infer(delta_ctx *ctx, int64_t n, const double *a, const double *b, int64_t ld,
                              const float *params, const void *params_bf16, float *x0);
-/* Network engines of the learned hybrid (delta_pairs_run_learned): the 5th-generation
- * tensor cores (tcgen05 MMAs, TMEM accumulators; the default) or the warp-level
- * mma.sync path. */
+/* Network engines of the learned hybrid (delta_pairs_run_learned) and of the training
+ * GEMM (delta_gemm_bf16): the 5th-generation tensor cores (tcgen05 MMAs, TMEM
+ * accumulators; the default) or the warp-level mma.sync path. */
 #define DELTA_MLP_TCGEN05 0
 #define DELTA_MLP_MMA_SYNC 1
 delta_status delta_mlp_set_engine(delta_ctx *ctx, int engine);
@@ -498,8 +509,12 @@ delta_status delta_mlp_features(delta_ctx *ctx, int64_t n, const double *a, cons
                                 const double *p, const double *q, void *features_bf16, float *targets,
                                 uint8_t *valid);
 /* C[M][N] (+)= op(A) op(B): A is [M][K] (trans_a 0) or [K][M]; B is [K][N] (trans_b 0)
- * or [N][K]; BF16 operands on the tensor cores, FP32 C.  split_k > 1 splits K across
- * CTAs and accumulates with atomics (C is zeroed first unless accumulate). */
+ * or [N][K]; BF16 operands on the tensor cores, FP32 C.  On the context's engine: tcgen05
+ * (the default: 128 x 128 output tiles, M=128 MMAs from shared memory into a TMEM
+ * accumulator that sums the CTA's whole K range; with split_k > 1 the K splits write
+ * partial tiles that one more kernel adds in split order, without atomics; a bounded wait
+ * that gives up sets the output to NaN and makes the next delta_synchronize return
+ * DELTA_ERR_TIMEOUT) or mma.sync (split_k > 1 accumulates with atomics). */
 delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A, int lda, int trans_a,
                              const void *B, int ldb, int trans_b, float *C, int ldc, int accumulate, int split_k);
 /* Z[M][N] += bias; H_bf16 (optional) = bf16(GELU(Z)) (tanh form) or bf16(Z) when gelu_on is 0. */

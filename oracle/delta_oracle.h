@@ -186,6 +186,15 @@ void dzo_penalty(uint32_t it, uint32_t nt, const double a[3], const double b[3],
 /* hybrid(it, nt, ...), zoltan/hybrid.cpp:37-131 (it counts batches of 4) */
 void dzo_hybrid(int32_t it, int32_t nt, const double a[3], const double b[3], const double c[3], const double *d,
                 const double *e, const double *f, int64_t ld, double *p, double *q);
+/* The same two with the penalty weight r moved by r_ulps units in the last place (test
+ * hook: which results depend on the last bit of pow/log/log10); hybrid's mode 0 keeps the
+ * reference's fallback decision, 1 never falls back, 2 always falls back. */
+void dzo_penalty_shifted(uint32_t it, uint32_t nt, const double a[3], const double b[3], const double c[3],
+                         const double *d, const double *e, const double *f, int64_t ld, double *p, double *q,
+                         int32_t r_ulps);
+void dzo_hybrid_shifted(int32_t it, int32_t nt, const double a[3], const double b[3], const double c[3],
+                        const double *d, const double *e, const double *f, int64_t ld, double *p, double *q,
+                        int32_t r_ulps, int32_t mode);
 /* dynamics::update, euler, integrate (zoltan/dynamics.cpp:66-335) */
 void dzo_update(int32_t nt, int32_t nb, double *t, int64_t ldt, const int32_t *pid, double *angular,
                 double *linear, double *rotation, double *position, const double *inertia, const double *inverse,

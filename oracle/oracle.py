@@ -227,6 +227,9 @@ class Oracle(_Lib, _Zoltan):
         self._zsig()
         vp0, i32_, i64_, u32_, f8_ = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32, C.c_double
         self.lib.dzo_bf_soa.argtypes = [u32_, u32_, vp0, vp0, vp0, vp0, vp0, vp0, i64_, vp0, vp0]
+        self.lib.dzo_penalty_shifted.argtypes = [u32_, u32_, vp0, vp0, vp0, vp0, vp0, vp0, i64_, vp0, vp0, i32_]
+        self.lib.dzo_hybrid_shifted.argtypes = [i32_, i32_, vp0, vp0, vp0, vp0, vp0, vp0, i64_, vp0, vp0, i32_,
+                                                i32_]
         self.lib.dzo_update.argtypes = [i32_, i32_, vp0, i64_, vp0, vp0, vp0, vp0, vp0, vp0, vp0, vp0, vp0, vp0,
                                         f8_]
         self.lib.dzo_euler.argtypes = [i32_, vp0, vp0, vp0, vp0, f8_]
@@ -246,6 +249,30 @@ class Oracle(_Lib, _Zoltan):
         L.dor_sim_contacts.restype = i64
         L.dor_filter_new.argtypes = [i64, vp, i64, vp, vp, f8, vp]
         L.dor_filter_old.argtypes = [i64, vp, i64, vp, vp, i64, vp, i64, vp, vp, f8, vp]
+
+    def zoltan_r_shifted(self, method, it, nt, abc, d, e, f, p0=None, q0=None, shifts=range(-12, 13)):
+        """The results penalty / hybrid can give when the penalty weight r (formed with pow
+        and log/log10, whose last bit depends on the math library) moves by each of `shifts`
+        units in the last place: array (k, 6, n) of (p, q) planes.  For hybrid: the 7-step
+        penalty points for every shift (no fallback), and the fallback points of every batch
+        (bf, which does not depend on r)."""
+        abc = np.ascontiguousarray(abc, np.float64)
+        d, e, f = (np.ascontiguousarray(x, np.float64) for x in (d, e, f))
+        n = d.shape[1]
+
+        def run(u, mode):
+            p = np.full((3, n), np.nan) if p0 is None else np.array(p0, np.float64)
+            q = np.full((3, n), np.nan) if q0 is None else np.array(q0, np.float64)
+            args = [it, nt, _p(abc[0]), _p(abc[1]), _p(abc[2]), _p(d), _p(e), _p(f), n, _p(p), _p(q), int(u)]
+            if method == "hybrid":
+                self.lib.dzo_hybrid_shifted(*args, mode)
+            else:
+                self.lib.dzo_penalty_shifted(*args)
+            return np.concatenate([p, q])
+        out = [run(u, 1) for u in shifts]
+        if method == "hybrid":
+            out.append(run(0, 2))
+        return np.stack(out)
 
     # ---- zoltan dynamics and forces (zoltan_oracle.c) ------------------------------------
     def zoltan_update(self, t, pid, angular, linear, rotation, position, inertia, inverse, mass, force, torque, step):

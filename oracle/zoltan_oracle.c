@@ -22,6 +22,25 @@
 
 static inline double dot3z(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
+/* The penalty weight r of list entry i moved by `ulps` units in the last place (0: as
+ * computed; 1000 and above: a seeded pseudo-random shift in [-3, 3] per entry).  The
+ * reference forms r with pow and log/log10, whose last bit depends on the math library;
+ * the shifted variants let a test tell which results depend on that bit. */
+static double shift_ulps_at(double r, int32_t ulps, uint32_t i) {
+  if (ulps >= 1000) { /* a pseudo-random shift in [-3, 3] per list entry, seeded by ulps */
+    uint32_t h = (i + 0x9e3779b9u * (uint32_t)ulps) ^ 0x85ebca6bu;
+    h ^= h >> 15;
+    h *= 0x2c1b3c6du;
+    h ^= h >> 12;
+    h *= 0x297a2d39u;
+    h ^= h >> 15;
+    ulps = (int32_t)(h % 7u) - 3;
+  }
+  for (; ulps > 0; --ulps) r = nextafter(r, INFINITY);
+  for (; ulps < 0; ++ulps) r = nextafter(r, -INFINITY);
+  return r;
+}
+
 /* ============================================================================
  * zoltan/bf.cpp:26-952, bf(xA,yA,zA, xB,yB,zB, xPA,...,zPB) for one triangle pair.
  *
@@ -188,8 +207,9 @@ static void zoltan_hessian(const double BA[3], const double CA[3], const double 
  * triangle index i is 4 or more (the test `i < 4` at zoltan/penalty.cpp:137 reads the
  * list index, not the step index).
  * ========================================================================== */
-void dzo_penalty(uint32_t it, uint32_t nt, const double a[3], const double b[3], const double c[3],
-                 const double *d, const double *e, const double *f, int64_t ld, double *p, double *q) {
+void dzo_penalty_shifted(uint32_t it, uint32_t nt, const double a[3], const double b[3], const double c[3],
+                         const double *d, const double *e, const double *f, int64_t ld, double *p, double *q,
+                         int32_t r_ulps) {
   for (uint32_t i = it; i < nt; ++i) {
     double A[3], D[3], BA[3], CA[3], ED[3], FD[3], h[16], x[4] = {0.33, 0.33, 0.33, 0.33}, dx[4];
     for (int k = 0; k < 3; ++k) {
@@ -204,7 +224,7 @@ void dzo_penalty(uint32_t it, uint32_t nt, const double a[3], const double b[3],
     const double eps = 0.1;
     double delta = (h[0] + h[5] + h[10] + h[15]) * eps;
     const double lambda = sqrt(0.0125 * (h[0] + h[5] + h[10] + h[15]));
-    const double r = lambda * pow(10, log(lambda) + 14);
+    const double r = shift_ulps_at(lambda * pow(10, log(lambda) + 14), r_ulps, i);
     for (int j = 0; j < 5; ++j) {
       delta = i < 4 ? delta : r * delta;
       zoltan_newton_step(A, D, BA, CA, ED, FD, h, r, delta, x, dx);
@@ -220,7 +240,8 @@ void dzo_penalty(uint32_t it, uint32_t nt, const double a[3], const double b[3],
 /* zoltan/hybrid.cpp:134-278: 7 steps with delta = 1e-16 tr(H), r = lambda 10^(log10
  * lambda + 8); error = sqrt(|dx|^2 / |x|^2) of the last step. */
 static void zoltan_hybrid_penalty(const double A[3], const double B[3], const double C[3], const double D[3],
-                                  const double E[3], const double F[3], double P[3], double Q[3], double *error) {
+                                  const double E[3], const double F[3], double P[3], double Q[3], double *error,
+                                  int32_t r_ulps, uint32_t i) {
   double BA[3], CA[3], ED[3], FD[3], h[16], x[4] = {0.33, 0.33, 0.33, 0.33}, dx[4] = {0, 0, 0, 0};
   for (int k = 0; k < 3; ++k) {
     BA[k] = B[k] - A[k];
@@ -232,7 +253,7 @@ static void zoltan_hybrid_penalty(const double A[3], const double B[3], const do
   const double eps = 1E-16;
   const double delta = (h[0] + h[5] + h[10] + h[15]) * eps; /* `i < 7 ? delta : 2000*delta` never changes it */
   const double lambda = sqrt(0.0125 * (h[0] + h[5] + h[10] + h[15]));
-  const double r = lambda * pow(10, log10(lambda) + 8);
+  const double r = shift_ulps_at(lambda * pow(10, log10(lambda) + 8), r_ulps, i);
   for (int i = 0; i < 7; ++i) {
     zoltan_newton_step(A, D, BA, CA, ED, FD, h, r, delta, x, dx);
     for (int k = 0; k < 4; ++k) x[k] = x[k] - dx[k];
@@ -392,8 +413,9 @@ static void zoltan_hybrid_bf(const double A[3], const double B[3], const double 
  * batch gets the points of bf with the batch's last triangle (the loop at
  * hybrid.cpp:115-128 reuses the A..F left by the penalty loop).
  * ========================================================================== */
-void dzo_hybrid(int32_t it, int32_t nt, const double a[3], const double b[3], const double c[3], const double *d,
-                const double *e, const double *f, int64_t ld, double *p, double *q) {
+void dzo_hybrid_shifted(int32_t it, int32_t nt, const double a[3], const double b[3], const double c[3],
+                        const double *d, const double *e, const double *f, int64_t ld, double *p, double *q,
+                        int32_t r_ulps, int32_t mode) {
   const unsigned batchSize = 4;
   double D[3] = {0, 0, 0}, E[3] = {0, 0, 0}, F[3] = {0, 0, 0}, P[3] = {0, 0, 0}, Q[3] = {0, 0, 0};
   for (unsigned k = (unsigned)it; k < (unsigned)nt / batchSize; k++) {
@@ -405,7 +427,7 @@ void dzo_hybrid(int32_t it, int32_t nt, const double a[3], const double b[3], co
         E[x] = e[x * ld + i];
         F[x] = f[x * ld + i];
       }
-      zoltan_hybrid_penalty(a, b, c, D, E, F, P, Q, &error[l]);
+      zoltan_hybrid_penalty(a, b, c, D, E, F, P, Q, &error[l], r_ulps, i);
       for (int x = 0; x < 3; ++x) {
         p[x * ld + i] = P[x];
         q[x * ld + i] = Q[x];
@@ -413,7 +435,8 @@ void dzo_hybrid(int32_t it, int32_t nt, const double a[3], const double b[3], co
     }
     double batchError = 0.0;
     for (unsigned l = 0; l < batchSize; l++) batchError += error[l];
-    if (batchError / batchSize > 1E-8) {
+    /* mode 0: the reference's decision; 1: never fall back; 2: always fall back */
+    if (mode == 2 || (mode == 0 && batchError / batchSize > 1E-8)) {
       for (unsigned l = 0; l < batchSize; l++) {
         const unsigned i = k * batchSize + l;
         zoltan_hybrid_bf(a, b, c, D, E, F, P, Q);
@@ -612,4 +635,14 @@ void dzo_force(int32_t nb, const int64_t *offset, const int32_t *slave, const do
     }
     for (int k = 0; k < 3; ++k) force[k * nb + i] += mass[i] * gravity[k];
   }
+}
+
+void dzo_penalty(uint32_t it, uint32_t nt, const double a[3], const double b[3], const double c[3],
+                 const double *d, const double *e, const double *f, int64_t ld, double *p, double *q) {
+  dzo_penalty_shifted(it, nt, a, b, c, d, e, f, ld, p, q, 0);
+}
+
+void dzo_hybrid(int32_t it, int32_t nt, const double a[3], const double b[3], const double c[3], const double *d,
+                const double *e, const double *f, int64_t ld, double *p, double *q) {
+  dzo_hybrid_shifted(it, nt, a, b, c, d, e, f, ld, p, q, 0, 0);
 }

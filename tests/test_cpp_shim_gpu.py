@@ -146,10 +146,15 @@ def test_cpp_zoltan_narrowphase_matches_oracle(calls_exe, oracle, tmp_path):
     for m, method in enumerate(("bf_soa", "penalty", "hybrid")):
         p, q = oracle.zoltan_soa(method, it, nt, abc, b[0:3], b[3:6], b[6:9], fill, fill)
         want = np.concatenate([p, q])
-        if method == "bf_soa":
-            assert np.array_equal(got[m], want, equal_nan=True)
-        else:  # pow/log of the penalty weight: see tests/test_zoltan_gpu.py
-            assert np.allclose(got[m], want, rtol=0, atol=1e-9, equal_nan=True)
+        exact = ((got[m] == want) | (np.isnan(got[m]) & np.isnan(want))).all(0)
+        if method in ("bf_soa", "penalty"):
+            assert exact.all()
+        else:  # the oracle for a penalty weight within 12 ulps: see tests/test_zoltan_gpu.py
+            shifted = oracle.zoltan_r_shifted(method, it, nt, abc, b[0:3], b[3:6], b[6:9], fill, fill)
+            match = np.zeros(n, bool)
+            for x in shifted:
+                match |= ((got[m] == x) | (np.isnan(got[m]) & np.isnan(x))).all(0)
+            assert match.all()
 
 
 def test_cpp_zoltan_system_matches_oracle(calls_exe, oracle, tmp_path):

@@ -77,3 +77,24 @@ def test_read_mbfcp_without_materials_and_errors(tmp_path):
     bad.write_text("ID:\tx\n")
     with pytest.raises(DeltaError):
         read_mbfcp(bad)
+
+
+@pytest.mark.parametrize("n", [0, 1, 257])
+def test_write_vtu_holds_the_reference_arrays(tmp_path, n):
+    """writeGeometryToVTKVTK's grid (write.cpp:10-70) written without VTK: Float32 centres,
+    "direction" = linear velocity, "epsilon" (the active scalars; the reference's second
+    SetScalars call replaces "radius"), no cells; values round-trip exactly."""
+    from delta_b200.io import read_vtu, write_vtu_host
+
+    rng = np.random.default_rng(n)
+    centre = rng.normal(size=(3, n))
+    vel = rng.normal(size=(3, n)) * 1e-3
+    eps = rng.uniform(1e-5, 1e-3, n)
+    fn = write_vtu_host(tmp_path, 12, centre, vel, eps)
+    assert fn.endswith("geometry_12.vtu")
+    v = read_vtu(fn)
+    assert v["cells"] == 0 and v["active_scalars"] == "epsilon" and v["active_vectors"] == "direction"
+    assert "radius" not in v
+    assert np.array_equal(v["points"].reshape(n, 3), centre.T.astype(np.float32))
+    assert np.array_equal(v["direction"].reshape(n, 3), vel.T)
+    assert np.array_equal(v["epsilon"].reshape(n), eps)

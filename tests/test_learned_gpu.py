@@ -46,15 +46,22 @@ def test_layout_matches_oracle():
     assert layout() == mo.layout()
 
 
+@pytest.mark.parametrize("engine", ["tcgen05", "mma"])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("split,acc", [(1, 0), (4, 0), (1, 1), (3, 1)])
-def test_gemm_bf16_vs_torch(ctx, ta, tb, split, acc):
+@pytest.mark.parametrize("shape", [(200, 72, 300), (130, 4, 37), (4, 128, 1000), (300, 136, 4)])
+def test_gemm_bf16_vs_torch(ctx, engine, ta, tb, split, acc, shape):
+    """The training GEMM on both engines against torch's FP32 matmul of the same BF16
+    operands, for the shapes training uses (N or M of 4: the output layer; K of 4: its
+    backward) and ragged ones."""
     import torch
 
     from delta_b200._lib import check, lib
+    from delta_b200.learned import set_engine
 
+    set_engine(ctx, engine)
     g = torch.Generator(device="cuda").manual_seed(ta * 7 + tb * 3 + split)
-    M, N, K = 200, 72, 300
+    M, N, K = shape
     A = torch.randn((K, M) if ta else (M, K), generator=g, device="cuda").to(torch.bfloat16)
     B = torch.randn((N, K) if tb else (K, N), generator=g, device="cuda").to(torch.bfloat16)
     C0 = torch.randn((M, N), generator=g, device="cuda")
@@ -62,6 +69,8 @@ def test_gemm_bf16_vs_torch(ctx, ta, tb, split, acc):
     check(lib().delta_gemm_bf16(ctx.handle, M, N, K, A.data_ptr(), A.shape[1], ta, B.data_ptr(), B.shape[1], tb,
                                 Cm.data_ptr(), N, acc, split))
     ctx.synchronize()
+    ctx.synchronize()
+    set_engine(ctx, "tcgen05")
     Af = A.float().T if ta else A.float()
     Bf = B.float().T if tb else B.float()
     ref = Af @ Bf + (C0 if acc else 0)
