@@ -150,6 +150,18 @@ def profiled_traffic(kernel: str, n: int):
         return None
 
 
+def profiled_flops(kernel: str):
+    """(FP32, FP64) FLOP per pair of `kernel` counted by ncu (committed summary), or None."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        t = json.loads(p.read_text())[kernel]
+        return float(t["fp32_flop_per_pair"]), float(t["fp64_flop_per_pair"]), t["flop_source"]
+    except (KeyError, ValueError):
+        return None
+
+
 def cpu_reference_rate(a, b, sample: int, min_seconds: float):
     """The reference's bfSolver (oracle/_ref, or the oracle port when absent) over `sample`
     pairs on all host threads; repeated until min_seconds.  Returns (pairs/s, cores, kind)."""
@@ -605,6 +617,22 @@ def main():
             kern_ms = float(np.mean(per_ms)) / args.passes
             traffic = profiled_traffic(args.method, n)
         achieved = bpp * n / (kern_ms / 1e3) / 1e9
+        # compute side: FP32/FP64 operations per pair (ncu counts of the same kernel) at the
+        # measured rate, against CUDA-core peaks derived from 148 SMs x max SM clock x lanes
+        # x 2 (FMA): 128 FP32 and 64 FP64 lanes per SM
+        compute = None
+        fl = profiled_flops("learned_refine") if args.method == "learned" else None
+        if fl is not None:
+            clk_ghz = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("sm_max_mhz", 1965.0)) / 1e3 \
+                if (ROOT / "MEASURED_PEAKS.json").exists() else 1.965
+            rate = n / (kern_ms / 1e3)
+            p32, p64 = 148 * clk_ghz * 128 * 2 / 1e3, 148 * clk_ghz * 64 * 2 / 1e3
+            compute = {"fp32_flop_per_pair": fl[0], "fp64_flop_per_pair": fl[1], "source": fl[2],
+                       "fp32_tflops": fl[0] * rate / 1e12, "fp32_peak_tflops_derived": p32,
+                       "fp32_frac": fl[0] * rate / 1e12 / p32,
+                       "fp64_tflops": fl[1] * rate / 1e12, "fp64_peak_tflops_derived": p64,
+                       "fp64_frac": fl[1] * rate / 1e12 / p64,
+                       "note": "issue-bound: ~76% of scheduler cycles issue (ncu); the FP pipes are not the limit"}
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -619,7 +647,7 @@ def main():
             "learned": learned_info,
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": bpp * n, "kernel_ms": kern_ms},
+                         "algorithmic_bytes_per_launch": bpp * n, "kernel_ms": kern_ms, "compute": compute},
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "e2e": e2e,

@@ -11,6 +11,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "internal.h"
 #include "pose.cuh"
@@ -48,6 +49,9 @@ struct RawContacts {
   // null elsewhere
   unsigned long long *pcnt;
   uint32_t *slot;
+  // culled drivers: the body-pair work queue of the culling kernel (zeroed before it runs);
+  // null: blocks take the pairs by a fixed stride
+  unsigned long long *pair_queue;
 };
 
 struct DevStats {
@@ -443,9 +447,20 @@ __global__ void __launch_bounds__(kCullThreads, 8) k_cull_pairs(delta_meshes m, 
                                                              RawContacts rc, DevStats *st) {
   __shared__ CullList LA, LB;
   __shared__ BodyPose QA, QB;
+  __shared__ int64_t s_next;
   const int tid = threadIdx.x;
   if (rc.pcnt && blockIdx.x == 0 && tid == 0) rc.pcnt[n_pairs] = 0;
-  for (int64_t k = blockIdx.x; k < n_pairs; k += gridDim.x) {
+  // a persistent work queue of body pairs: each block takes the next pair when it is done
+  // with its last, so uneven pairs (a wall of thousands of triangles next to small meshes)
+  // do not leave the other blocks idle; without a queue, a fixed stride
+  int64_t k = blockIdx.x;
+  if (rc.pair_queue) {
+    if (tid == 0) s_next = (int64_t)atomicAdd(rc.pair_queue, 1ull);
+    __syncthreads();
+    k = s_next;
+  }
+  while (k < n_pairs) {
+    do {  // one body pair; `continue` ends it
     if (rc.pcnt && tid == 0) rc.pcnt[k] = 0;  // the pair's contact count (k_cert_survivors)
     const int32_t a = pa[k], b = pb[k];
     if (a < 0 || b < 0) continue;
@@ -495,7 +510,26 @@ __global__ void __launch_bounds__(kCullThreads, 8) k_cull_pairs(delta_meshes m, 
         __syncthreads();  // LA is refilled next
       }
     }
+    } while (0);
+    if (rc.pair_queue) {
+      __syncthreads();  // every thread has read s_next for this pair
+      if (tid == 0) s_next = (int64_t)atomicAdd(rc.pair_queue, 1ull);
+      __syncthreads();
+      k = s_next;
+    } else {
+      k += gridDim.x;
+    }
   }
+}
+
+// DELTA_CULL_STRIDE=1 in the environment: the culling kernel's blocks take the body pairs
+// by a fixed stride instead of the work queue (for comparison).
+inline bool cull_stride() {
+  static const bool v = [] {
+    const char *e = std::getenv("DELTA_CULL_STRIDE");
+    return e && e[0] == '1';
+  }();
+  return v;
 }
 
 inline cudaError_t launch_cull(cudaStream_t s, const delta_meshes &m, const int32_t *pa, const int32_t *pb,
@@ -928,6 +962,7 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
   RawContacts rc{};
   rc.tbits = 16;
   const bool culled = driver == DELTA_DRV_BF_CERT || driver == DELTA_DRV_BF_CULLED || driver == DELTA_DRV_LEARNED;
+  if (culled && !cull_stride()) rc.pair_queue = queue;  // zeroed below before every culling launch
   if (culled && pose) {
     rc.pose = *pose;  // current vertices and body boxes from the bodies' poses
   } else if (culled) {
@@ -1103,6 +1138,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   rc.sv_count = queue + 2;
   const bool culled = driver == DELTA_DRV_BF_CERT || driver == DELTA_DRV_BF_CULLED || driver == DELTA_DRV_LEARNED;
   if (culled && pose) rc.pose = *pose;  // vertices and body boxes from the poses
+  if (culled && !cull_stride()) rc.pair_queue = queue;  // queue[0], zeroed with the state below
   if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
   size_t tb = temp_bytes;
   if (culled) {

@@ -269,3 +269,25 @@ def test_graph_many_contacts_per_pair_equals_stepping_and_oracle(ctx, oracle):
     assert len(g_c) == len(o_c)
     for f in FIELDS:
         assert np.array_equal(g_c[f], o_c[f]), f
+
+
+@pytest.mark.skipif(not __import__("os").environ.get("DELTA_LONG_TESTS"),
+                    reason="opt-in (DELTA_LONG_TESTS=1): the lattice's 1000 steps against the oracle")
+@pytest.mark.parametrize("driver,graph", [(0, False), (8, True)])
+def test_lattice_1000_steps_bit_exact(ctx, oracle, driver, graph):
+    """The small plain configuration in full: 256 icospheres, FP64, dt 1e-5, 1000 steps;
+    the GPU trajectory (FP64 bf stepped, or the certified driver as a CUDA graph) equals the
+    oracle's bit for bit."""
+    from delta_b200.engine import Simulation, StepParams
+    from delta_b200.scenarios import lattice_scene
+
+    scene = lattice_scene(seed=2024)
+    p = PARAMS
+    o_state, o_cps, _ = oracle.simulate(scene, p["dt"], p["gravity"], p["spring"], p["damper"], p["friction"], 1000)
+    sim = Simulation(ctx, scene, driver)
+    cps = sim.step(1000, StepParams.make(**p), graph=graph)
+    st = sim.state()
+    sim.close()
+    assert list(cps) == list(o_cps)
+    for k in STATE:
+        assert np.array_equal(st[k], o_state[k]), k
