@@ -250,6 +250,23 @@ def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, para
         out[name] = _time_sim(ctx, stream, sim, k, params, graph)
         states[name] = sim.state()
         sim.close()
+    # the certified driver after delta_sim_autotune (its own context: the launch shapes are
+    # the context's), with the same number of steps before the timed region
+    from delta_b200.narrowphase import Context
+
+    tctx = Context(0, stream=stream.cuda_stream)
+    try:
+        sim = Simulation(tctx, scene, DRV_BF_CERT)
+        if warmup > 1:
+            sim.step(warmup - 1, params, graph=True)
+        tune = sim.autotune(reps=3)
+        sim.step(1, params, graph=True)  # records the graph with the chosen shapes
+        out["bf_cert_culled_graph_tuned"] = dict(_time_sim(tctx, stream, sim, steps, params, True),
+                                                 launch_shape=tune)
+        states["bf_cert_culled_graph_tuned"] = sim.state()
+        sim.close()
+    finally:
+        tctx.close()
     ref = states["fp64_bf"]
     exact = [n for n in states if n != "learned_culled_graph"]
     same = all(np.array_equal(ref[k], states[n][k]) for n in exact for k in ("pos", "vel", "rot", "x"))
@@ -263,6 +280,7 @@ def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, para
     return {"workload": workload, "steps": steps, "warmup": warmup, **out, "cpu_baseline": cpu,
             "speedup": sps["bf_cert_culled_graph"] / sps["fp64_bf"],
             "speedup_learned": sps["learned_culled_graph"] / sps["fp64_bf"],
+            "speedup_tuned": sps["bf_cert_culled_graph_tuned"] / sps["fp64_bf"],
             "speedup_from_culling": sps["fp64_bf_culled"] / sps["fp64_bf"],
             "speedup_from_precision": sps["bf_cert_culled_graph"] / sps["fp64_bf_culled_graph"],
             "speedup_note": "culling: culled FP64 bf vs plain FP64 bf (both stepped); precision: certified "

@@ -43,6 +43,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_sim_set_graph_capacity": ([vp, i64, i64], C.c_int),
     "delta_sim_contacts": ([vp, vp, vp], C.c_int),
     "delta_sim_counters": ([vp, vp], C.c_int),
+    "delta_set_cull_launch": ([vp, i32, i32], C.c_int),
+    "delta_sim_autotune": ([vp, i32, vp, vp], C.c_int),
     "delta_sim_destroy": ([vp], C.c_int),
     "delta_sphere_contacts": ([vp, vp, vp, vp, i64, vp, vp], C.c_int),
     "delta_sphere_mesh_contacts": ([vp, vp, vp, vp, vp, i64, C.c_int, vp, vp], C.c_int),

@@ -220,6 +220,15 @@ delta_status delta_set_pair_launch(delta_ctx *ctx, int method, int precision, in
   return DELTA_OK;
 }
 
+delta_status delta_set_cull_launch(delta_ctx *ctx, int32_t cull_blocks_per_sm, int32_t survivor_blocks_per_sm) {
+  if (!ctx || cull_blocks_per_sm < 0 || survivor_blocks_per_sm < 0)
+    return set_error(DELTA_ERR_INVALID, "delta_set_cull_launch: bad argument");
+  ctx->cull_blocks_per_sm = cull_blocks_per_sm;
+  ctx->surv_blocks_per_sm = survivor_blocks_per_sm;
+  ctx->launch_epoch += 1;
+  return DELTA_OK;
+}
+
 delta_status delta_autotune_pairs(delta_ctx *ctx, int method, int precision, int64_t n, const double *a,
                                   const double *b, int64_t ld, double max_error, double *p, double *q, double *dist,
                                   uint8_t *flags, int32_t *threads_out, int32_t *blocks_per_sm_out, float *ms_out) {

@@ -532,11 +532,13 @@ inline bool cull_stride() {
   return v;
 }
 
+// cap: blocks per SM (the time-step autotuner's choice), 0 = as many as fit
 inline cudaError_t launch_cull(cudaStream_t s, const delta_meshes &m, const int32_t *pa, const int32_t *pb,
-                               int64_t n_pairs, const RawContacts &rc, DevStats *st) {
+                               int64_t n_pairs, const RawContacts &rc, DevStats *st, int cap = 0) {
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cull_pairs, kCullThreads, 0);
   if (e != cudaSuccess) return e;
+  if (cap > 0 && cap < per_sm) per_sm = cap;
   int64_t blocks = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
   if (blocks > n_pairs) blocks = n_pairs > 0 ? n_pairs : 1;
   k_cull_pairs<<<(unsigned)blocks, kCullThreads, 0, s>>>(m, pa, pb, n_pairs, rc, st);
@@ -676,7 +678,8 @@ __global__ void __launch_bounds__(128, 4) k_learned_survivors(delta_meshes m, co
 // The survivors' solver of a culled driver: certified FP32 + FP64 (DELTA_DRV_BF_CERT), FP64
 // bfSolver (DELTA_DRV_BF_CULLED) or the learned FP32 hybrid (DELTA_DRV_LEARNED).
 inline cudaError_t launch_survivors(int driver, cudaStream_t s, const delta_meshes &m, const int32_t *pa,
-                                    const int32_t *pb, const RawContacts &rc, DevStats *st, int64_t n_hint) {
+                                    const int32_t *pb, const RawContacts &rc, DevStats *st, int64_t n_hint,
+                                    int cap = 0) {
   int per_sm = 0;
   cudaError_t e = driver == DELTA_DRV_BF_CULLED
                       ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bf64_survivors, 128, 0)
@@ -684,6 +687,7 @@ inline cudaError_t launch_survivors(int driver, cudaStream_t s, const delta_mesh
                       ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_learned_survivors, 128, 0)
                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cert_survivors, 128, 0);
   if (e != cudaSuccess) return e;
+  if (cap > 0 && cap < per_sm) per_sm = cap;
   int64_t blocks = n_hint >= 0 ? (n_hint + 127) / 128 : INT64_MAX;
   const int64_t mx = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
   if (blocks > mx) blocks = mx;
@@ -911,6 +915,16 @@ cudaError_t launch_detect_prec(int driver, cudaStream_t s, const delta_meshes &m
 
 }  // namespace
 
+cudaError_t detect_launch_limits(int driver, int *cull_per_sm, int *surv_per_sm) {
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(cull_per_sm, k_cull_pairs, kCullThreads, 0);
+  if (e != cudaSuccess) return e;
+  return driver == DELTA_DRV_BF_CULLED
+             ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(surv_per_sm, k_bf64_survivors, 128, 0)
+         : driver == DELTA_DRV_LEARNED
+             ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(surv_per_sm, k_learned_survivors, 128, 0)
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(surv_per_sm, k_cert_survivors, 128, 0);
+}
+
 // Scratch slots used here: 2 rows/row_offset, 3 raw contacts, 4 sort buffers, 5 small state.
 delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_meshes &m, const int32_t *pa,
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
@@ -1001,7 +1015,8 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
         rc.sv_cap = sv_cap;
         if ((e = cudaMemsetAsync(queue, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess)
           return cuda_error(e, "memset");
-        if ((e = launch_cull(s, m, pa, pb, n_pairs, rc, dstats)) != cudaSuccess) return cuda_error(e, "cull kernel");
+        if ((e = launch_cull(s, m, pa, pb, n_pairs, rc, dstats, ctx->cull_blocks_per_sm)) != cudaSuccess)
+          return cuda_error(e, "cull kernel");
         ctx->launches += 1;
         if ((e = cudaMemcpyAsync(&hsv, sv_count, sizeof(hsv), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
             (e = cudaStreamSynchronize(s)) != cudaSuccess)
@@ -1009,7 +1024,8 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
         if ((int64_t)hsv <= sv_cap) break;
         sv_cap = (int64_t)hsv + hsv / 4;
       }
-      if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, (int64_t)hsv)) != cudaSuccess)
+      if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, (int64_t)hsv, ctx->surv_blocks_per_sm)) !=
+          cudaSuccess)
         return cuda_error(e, "survivor kernel");
       k_sv_evaluated<<<1, 1, 0, s>>>(sv_count, rc.sv_cap, dstats, nullptr);
       ctx->launches += 2;
@@ -1149,9 +1165,9 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
     // pair's bucket ranked by key.  The per-pair arrival ranks use the sort's key_out.
     rc.pcnt = (unsigned long long *)rows;
     rc.slot = (uint32_t *)key_out;
-    e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats);
+    e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats, ctx->cull_blocks_per_sm);
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
-    if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, -1)) != cudaSuccess)
+    if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, -1, ctx->surv_blocks_per_sm)) != cudaSuccess)
       return cuda_error(e, "survivor kernel");
     if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
       return cuda_error(e, "pair contact scan");

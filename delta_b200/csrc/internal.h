@@ -49,6 +49,11 @@ delta_status detect_run(delta_ctx *ctx, int driver, int precision, const delta_m
                         const int32_t *pb, int64_t n_pairs, const delta_contacts *out, int64_t *n_out,
                         delta_stats *stats, int64_t *counters = nullptr, const Pose *pose = nullptr);
 
+// Resident blocks per SM of a culled driver's two kernels (the culling kernel and the
+// survivors' solver): the largest caps delta_ctx::cull_blocks_per_sm / surv_blocks_per_sm
+// can take (detect.cu).
+cudaError_t detect_launch_limits(int driver, int *cull_per_sm, int *surv_per_sm);
+
 // Fixed-capacity (graph-capturable) detection (detect.cu).  `pose`: as for detect_run
 // (null: the certified driver reads the meshes' vertices and culls without body boxes).
 // `tri_bits`: bits of a triangle index within a body (every body has
@@ -87,6 +92,10 @@ struct delta_ctx {
   cudaEvent_t events[3 * 16] = {};
   int mlp_engine = DELTA_MLP_TCGEN05;  // network engine of the learned hybrid and its training GEMM
   int *gemm_err = nullptr;             // device flag: a tcgen05 GEMM's bounded wait gave up
+  // launch shapes of the culled drivers' kernels (blocks per SM; 0 = as many as fit), set
+  // by delta_sim_autotune
+  int cull_blocks_per_sm = 0, surv_blocks_per_sm = 0;
+  int64_t launch_epoch = 0;  // bumped when they change: recorded graphs are recorded again
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
 };

@@ -1202,6 +1202,7 @@ struct delta_sim {
   // steps, candidate body pairs, triangle pairs of the candidates, triangle pairs solved
   int64_t counters[4] = {0, 0, 0, 0};
   int64_t graph_pair_cap = 0, graph_contact_cap = 0;  // requested by delta_sim_set_graph_capacity
+  int64_t last_pairs = 0;                            // candidate body pairs of the last detection
   // graph mode: fixed-capacity buffers, device-side counts, the captured step
   struct Graph {
     int64_t pair_cap = 0, contact_cap = 0;
@@ -1219,6 +1220,7 @@ struct delta_sim {
     cudaGraphExec_t exec = nullptr;
     delta_step_params params{};
     int kernels = 0;
+    int64_t launch_epoch = 0;  // the context's launch shapes the graph was recorded with
     bool captured = false;
   } g;
 };
@@ -1284,6 +1286,7 @@ static delta_status sim_detect(delta_sim *s) {
   }
   if (ds != DELTA_OK) return ds;
   s->counters[1] += np;
+  s->last_pairs = np;
   // vertices of the bodies the narrowphase reads: formed from the poses by the certified
   // driver, updated here for the others
   const bool posed = s->driver == DELTA_DRV_BF_CERT || s->driver == DELTA_DRV_BF_CULLED || s->driver == DELTA_DRV_LEARNED;
@@ -1426,6 +1429,7 @@ static delta_status graph_capture(delta_sim *s, const delta_step_params &p) {
   g.graph = graph;
   if ((e = cudaGraphInstantiate(&g.exec, g.graph, 0)) != cudaSuccess) return cuda_error(e, "graph instantiate");
   g.params = p;
+  g.launch_epoch = s->ctx->launch_epoch;
   g.captured = true;
   return DELTA_OK;
 }
@@ -1621,6 +1625,86 @@ delta_status delta_sim_step(delta_sim *s, const delta_step_params *params, int32
   return sim_all_vertices(s, s->ctx->stream);
 }
 
+delta_status delta_sim_autotune(delta_sim *s, int32_t reps, int32_t *choice, float *ms_out) {
+  if (!s || reps < 1 || !choice) return set_error(DELTA_ERR_INVALID, "delta_sim_autotune: bad argument");
+  delta_ctx *ctx = s->ctx;
+  if (s->driver != DELTA_DRV_BF_CERT && s->driver != DELTA_DRV_BF_CULLED && s->driver != DELTA_DRV_LEARNED) {
+    choice[0] = choice[1] = 0;  // nothing to tune: the pair kernels take delta_set_pair_launch
+    if (ms_out) *ms_out = 0.f;
+    return DELTA_OK;
+  }
+  int cull_max = 0, surv_max = 0;
+  cudaError_t e = detect_launch_limits(s->driver, &cull_max, &surv_max);
+  if (e != cudaSuccess) return cuda_error(e, "delta_sim_autotune: occupancy");
+  // one detection of the current state (grows the pair and contact buffers to fit), then
+  // every launch shape on the same pairs; detection changes no state but the contacts,
+  // which each run writes alike
+  const int64_t saved[4] = {s->counters[0], s->counters[1], s->counters[2], s->counters[3]};
+  const int saved_shape[2] = {ctx->cull_blocks_per_sm, ctx->surv_blocks_per_sm};
+  delta_status ds = sim_detect(s);
+  std::copy(saved, saved + 4, s->counters);
+  if (ds != DELTA_OK) return ds;
+  std::vector<int> cull_c, surv_c;
+  for (int c = 1; c <= cull_max; c = c < 2 ? c + 1 : c + 2) cull_c.push_back(c);
+  for (int c = 1; c <= surv_max; ++c) surv_c.push_back(c);
+  if (cull_c.empty()) cull_c.push_back(0);
+  if (surv_c.empty()) surv_c.push_back(0);
+  const Pose pose = sim_pose(s);
+  delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
+                 s->scene.eps,      s->scene.friction,   s->ids};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if ((e = cudaEventCreate(&ev[0])) != cudaSuccess || (e = cudaEventCreate(&ev[1])) != cudaSuccess) {
+    for (cudaEvent_t x : ev)
+      if (x) cudaEventDestroy(x);
+    return cuda_error(e, "delta_sim_autotune: events");
+  }
+  float best = -1.f;
+  int best_c = 0, best_s = 0;
+  for (int cc : cull_c) {
+    for (int sc : surv_c) {
+      ctx->cull_blocks_per_sm = cc;
+      ctx->surv_blocks_per_sm = sc;
+      std::vector<float> t;
+      for (int r = 0; r <= reps && ds == DELTA_OK; ++r) {  // r == 0: warm-up
+        int64_t nc = 0;
+        if ((e = cudaEventRecord(ev[0], ctx->stream)) != cudaSuccess) break;
+        if (s->last_pairs > 0)
+          ds = detect_run(ctx, s->driver, DELTA_F64, m, s->pa, s->pb, s->last_pairs, &s->c, &nc, nullptr, nullptr,
+                          &pose);
+        if (ds != DELTA_OK) break;
+        if ((e = cudaEventRecord(ev[1], ctx->stream)) != cudaSuccess || (e = cudaEventSynchronize(ev[1])) != cudaSuccess)
+          break;
+        float ms = 0.f;
+        if ((e = cudaEventElapsedTime(&ms, ev[0], ev[1])) != cudaSuccess) break;
+        if (r > 0) t.push_back(ms);
+      }
+      if (ds != DELTA_OK || e != cudaSuccess) break;
+      std::sort(t.begin(), t.end());
+      const float med = t[t.size() / 2];
+      if (best < 0.f || med < best) {
+        best = med;
+        best_c = cc;
+        best_s = sc;
+      }
+    }
+    if (ds != DELTA_OK || e != cudaSuccess) break;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (ds == DELTA_OK && e != cudaSuccess) ds = cuda_error(e, "delta_sim_autotune");
+  if (ds != DELTA_OK) {
+    ctx->cull_blocks_per_sm = saved_shape[0];
+    ctx->surv_blocks_per_sm = saved_shape[1];
+    ctx->launch_epoch += 1;
+    return ds;
+  }
+  ctx->cull_blocks_per_sm = choice[0] = best_c;
+  ctx->surv_blocks_per_sm = choice[1] = best_s;
+  ctx->launch_epoch += 1;  // recorded steps hold the old launch shapes
+  if (ms_out) *ms_out = best;
+  return DELTA_OK;
+}
+
 delta_status delta_sim_contacts(delta_sim *s, const delta_contacts *out, int64_t *n_out) {
   if (!s || !out || !n_out) return set_error(DELTA_ERR_INVALID, "delta_sim_contacts: null argument");
   *n_out = s->n_contacts;
@@ -1685,7 +1769,7 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
                           std::max<int64_t>({g.log_len, (int64_t)nsteps, 4096}))) != DELTA_OK)
       return ds;
   }
-  if (memcmp(&g.params, params, sizeof(*params)) != 0) g.captured = false;
+  if (memcmp(&g.params, params, sizeof(*params)) != 0 || g.launch_epoch != s->ctx->launch_epoch) g.captured = false;
   // hand the current contacts to the graph buffers; ctx stream work must be done first
   if ((e = cudaEventRecord(g.ev, s->ctx->stream)) != cudaSuccess ||
       (e = cudaStreamWaitEvent(g.stream, g.ev, 0)) != cudaSuccess)

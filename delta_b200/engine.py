@@ -78,6 +78,7 @@ class Simulation:
 
     def __init__(self, ctx: Context, scene: dict, driver: int = DRV_BF):
         self.ctx = ctx
+        self.driver = int(driver)
         self.dev = DeviceScene(scene)
         self._s = self.dev.struct()
         self._h = C.c_void_p()
@@ -93,6 +94,45 @@ class Simulation:
 
     def set_graph_capacity(self, pairs: int, contacts: int):
         check(lib().delta_sim_set_graph_capacity(self._h, int(pairs), int(contacts)))
+
+    def autotune(self, reps: int = 5, cache=None) -> dict:
+        """delta_sim_autotune: times the culled driver's detection of the current state under
+        every launch shape of its culling and survivor kernels and keeps the fastest on the
+        context.  Returns {"cull_blocks_per_sm", "survivor_blocks_per_sm", "ms", "cached"}.
+
+        cache: a JSON file of earlier choices keyed by device, driver, bodies and triangles;
+        a hit sets the stored shape (delta_set_cull_launch) without timing, a miss tunes and
+        adds the result."""
+        import json
+        import os
+
+        key = None
+        if cache is not None:
+            import torch
+
+            dev = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+            ntri = int(self.dev.t["tri_offset"][-1].item())
+            key = f"{dev}|driver={self.driver}|bodies={self.dev.n_bodies}|triangles={ntri}"
+            table = {}
+            if os.path.exists(cache):
+                with open(cache) as f:
+                    table = json.load(f)
+            if key in table:
+                e = table[key]
+                check(lib().delta_set_cull_launch(self.ctx.handle, int(e["cull_blocks_per_sm"]),
+                                                  int(e["survivor_blocks_per_sm"])))
+                return dict(e, cached=True)
+        choice = np.zeros(2, np.int32)
+        ms = C.c_float(0)
+        check(lib().delta_sim_autotune(self._h, int(reps), choice.ctypes.data, C.byref(ms)))
+        e = {"cull_blocks_per_sm": int(choice[0]), "survivor_blocks_per_sm": int(choice[1]), "ms": float(ms.value)}
+        if key is not None:
+            table[key] = e
+            tmp = os.fspath(cache) + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(table, f, indent=1, sort_keys=True)
+            os.replace(tmp, cache)
+        return dict(e, cached=False)
 
     def contacts(self) -> np.ndarray:
         n = C.c_int64(0)

@@ -46,6 +46,10 @@ class Context:
     def synchronize(self):
         check(lib().delta_synchronize(self._h))
 
+    def set_cull_launch(self, cull_blocks_per_sm: int, survivor_blocks_per_sm: int):
+        """Blocks per SM of the culled drivers' culling and survivor kernels (0 = all that fit)."""
+        check(lib().delta_set_cull_launch(self._h, int(cull_blocks_per_sm), int(survivor_blocks_per_sm)))
+
     @property
     def launches(self) -> int:
         return int(lib().delta_launch_count(self._h))

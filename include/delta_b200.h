@@ -303,6 +303,19 @@ delta_status delta_sim_step_graph(delta_sim *sim, const delta_step_params *param
  * delta_sim_step_graph call instead of the observed-size default; overflows still
  * recover as described above. */
 delta_status delta_sim_set_graph_capacity(delta_sim *sim, int64_t pair_capacity, int64_t contact_capacity);
+/* Launch shapes of the culled drivers' two kernels (DELTA_DRV_BF_CERT, DELTA_DRV_BF_CULLED,
+ * DELTA_DRV_LEARNED): the culling kernel's and the survivors' solver's resident blocks per
+ * SM (0 = as many as fit; larger values are clamped to what fits).  They belong to the
+ * context and apply to every detection it runs; a simulation's recorded graph is recorded
+ * again with them on its next delta_sim_step_graph call. */
+delta_status delta_set_cull_launch(delta_ctx *ctx, int32_t cull_blocks_per_sm, int32_t survivor_blocks_per_sm);
+/* Times the detection of the simulation's current state (the same candidate pairs, reps
+ * runs after one warm-up, median) under every launch shape of the culled driver's two
+ * kernels that fits, keeps the fastest in the context (delta_set_cull_launch) and writes
+ * it to choice[0..1], its median time in ms to *ms_out (may be NULL).  The state is not
+ * changed (the current contacts are detected again, alike); the counters are kept.  For
+ * the other drivers nothing is tuned: choice = {0, 0}. */
+delta_status delta_sim_autotune(delta_sim *sim, int32_t reps, int32_t choice[2], float *ms_out);
 /* Copies the current contacts into out (device); *n_out gets their number. */
 delta_status delta_sim_contacts(delta_sim *sim, const delta_contacts *out, int64_t *n_out);
 /* Totals since creation: [0] steps, [1] candidate body pairs, [2] triangle pairs of the

@@ -74,6 +74,64 @@ def test_culled_fp64_driver_graph_equals_stepping(ctx, scene):
         assert np.array_equal(st[k], a_state[k]), k
 
 
+@pytest.mark.parametrize("driver", [8, 9, 10])
+def test_autotuned_time_step_keeps_the_trajectory(ctx, scene, driver, tmp_path):
+    """delta_sim_autotune picks launch shapes of the culling and survivor kernels; the
+    trajectory and contacts after tuning (stepped and replayed in a graph) equal those of an
+    untuned simulation bit for bit, and a cache hit sets the same shape without timing."""
+    from delta_b200.engine import Simulation, StepParams
+    from delta_b200.narrowphase import Context
+
+    p = StepParams.make(**PARAMS)
+    ref = Simulation(ctx, scene, driver)
+    r_cps = list(ref.step(10, p)) + list(ref.step(10, p, graph=True))
+    r_state, r_c = ref.state(), ref.contacts()
+    ref.close()
+    tctx = Context(0)
+    try:
+        sim = Simulation(tctx, scene, driver)
+        cps = list(sim.step(10, p))
+        cache = tmp_path / "tune.json"
+        t = sim.autotune(reps=2, cache=cache)
+        assert not t["cached"] and t["ms"] > 0
+        assert t["cull_blocks_per_sm"] >= 1 and t["survivor_blocks_per_sm"] >= 1
+        assert sim.counters()["steps"] == 10
+        cps += list(sim.step(10, p, graph=True))
+        st, c = sim.state(), sim.contacts()
+        assert sim.autotune(cache=cache) == dict(t, cached=True)
+        sim.close()
+    finally:
+        tctx.close()
+    assert cps == r_cps
+    for k in STATE:
+        assert np.array_equal(st[k], r_state[k]), k
+    for f in FIELDS:
+        assert np.array_equal(c[f], r_c[f]), f
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (2, 3), (0, 0)])
+def test_every_cull_launch_shape_gives_the_same_contacts(ctx, scene, shape):
+    from delta_b200.engine import Simulation, StepParams
+    from delta_b200.narrowphase import Context
+
+    p = StepParams.make(**PARAMS)
+    a_state, a_cps, a_c = _gpu(ctx, scene, 15, driver=8)
+    tctx = Context(0)
+    try:
+        tctx.set_cull_launch(*shape)
+        sim = Simulation(tctx, scene, 8)
+        cps = sim.step(15, p, graph=True)
+        st, c = sim.state(), sim.contacts()
+        sim.close()
+    finally:
+        tctx.close()
+    assert list(cps) == list(a_cps)
+    for k in STATE:
+        assert np.array_equal(st[k], a_state[k]), k
+    for f in FIELDS:
+        assert np.array_equal(c[f], a_c[f]), f
+
+
 def test_friction_trajectory_bit_exact(ctx, oracle):
     from delta_b200.scenarios import lattice_scene
 
