@@ -108,7 +108,7 @@ __device__ __forceinline__ void solve(const delta_meshes &m, int64_t tA, int64_t
     R A[3][3], B[3][3], out[6];
     load_tri<R>(m, tA, A);
     load_tri<R>(m, tB, B);
-    if constexpr (S == S_BF) bf_solve_ref(A, B, out);
+    if constexpr (S == S_BF) bf_solve_lean(A, B, out);
     else if constexpr (S == S_PENALTY) penalty_ref(A, B, from_f64<R>(max_err), false, out, flag);
     else if constexpr (S == S_PENALTY_ITER) penalty_ref(A, B, from_f64<R>(max_err), true, out, flag);
     else gjk_ref(A, B, out);
@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(128) k_bf64_survivors(delta_meshes m, const in
         A64[v][k] = xf64(A[v][k]);
         B64[v][k] = xf64(B[v][k]);
       }
-    bf_solve_ref(A64, B64, out);
+    bf_solve_lean(A64, B64, out);
 #pragma unroll
     for (int k = 0; k < 6; ++k) pq[k] = out[k].v;
     const double mg = (xf64(r.epsA) + xf64(r.epsB)).v;

@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restri
     int flag = 0;
     const R me = from_f64<R>(max_error);
     if constexpr (M == M_BF) {
-      bf_solve_ref(A, B, pq);
+      bf_solve_lean(A, B, pq);
     } else if constexpr (M == M_PENALTY) {
       penalty_ref(A, B, me, false, pq, flag);
     } else if constexpr (M == M_PENALTY_ITER) {
@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restri
       gjk_ref(A, B, pq);
     } else {  // per-pair hybrid: penalty, bf when the pair reports failure
       penalty_ref(A, B, me, false, pq, flag);
-      if (flag) bf_solve_ref(A, B, pq);
+      if (flag) bf_solve_lean(A, B, pq);
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {

@@ -6,10 +6,12 @@ their penalty weight r with pow and log/log10, whose last bit differs between CU
 the host C library.  hybrid's 7-step penalty is so ill-conditioned (delta = 1e-16 tr H)
 that moving r by one unit in the last place changes the points of about a quarter of the
 entries, by up to the triangle size (measured with the oracle).  A tolerance cannot state
-parity there.  The statement is exact instead: every GPU entry of hybrid equals either the
-oracle's 7-step penalty point for a penalty weight within 12 units in the last place of the
-host's, or its batch's fallback point (bf, which does not depend on r); penalty's entries
-equal the oracle bit for bit."""
+parity there.  The statement is exact instead: every GPU entry of penalty and hybrid equals
+the oracle's point for a penalty weight within 40 units in the last place of the host's (a
+last-bit difference of log/log10 moves pow's argument by one of its own units, which is up
+to ~20 units of r), or, for hybrid, its batch's fallback point (bf, which does not depend on
+r).  The 5-step penalty is nearly insensitive (at most one entry in 16k moves over the
+window); hybrid's 7-step penalty is not."""
 import numpy as np
 import pytest
 
@@ -68,15 +70,15 @@ def test_zoltan_penalty_and_hybrid_vs_oracle(ctx, oracle, method):
         po, qo = oracle.zoltan_soa(method, it, n - cut, abc, b[0:3], b[3:6], b[6:9], fill, fill)
         g, o = np.concatenate([p, q]), np.concatenate([po, qo])
         same = lambda x, y: ((x == y) | (np.isnan(x) & np.isnan(y))).all(0)  # noqa: E731
-        if method == "penalty":
-            assert same(g, o).all()
-        else:
-            shifted = oracle.zoltan_r_shifted(method, it, n - cut, abc, b[0:3], b[3:6], b[6:9], fill, fill)
-            match = np.zeros(n, bool)
-            for x in shifted:
-                match |= same(g, x)
-            assert match.all(), np.flatnonzero(~match)[:10]
-            print(f"hybrid: {same(g, o).mean():.3f} of the entries equal the unshifted oracle")
+        # r = lambda * pow(10, log(lambda) + c): a last-bit difference of log/log10 moves pow's
+        # argument (about 5-16) by one of its ulps, which moves r by up to ~20 of its ulps
+        shifted = oracle.zoltan_r_shifted(method, it, n - cut, abc, b[0:3], b[3:6], b[6:9], fill, fill,
+                                          shifts=range(-40, 41))
+        match = np.zeros(n, bool)
+        for x in shifted:
+            match |= same(g, x)
+        assert match.all(), np.flatnonzero(~match)[:10]
+        print(f"{method}: {same(g, o).mean():.3f} of the entries equal the unshifted oracle")
         if method == "hybrid":  # entries outside the visited batches stay untouched
             k1 = (n - cut) // 4
             assert np.all(p[:, :4 * it] == 7.0) and np.all(p[:, 4 * k1:] == 7.0)
