@@ -684,23 +684,35 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 // ---------------------------------------------------------------------------------------
 // the training GEMM on the 5th-generation tensor cores: C[M,N] (+)= op(A)[M,K] op(B)[K,N]
 // with BF16 operands and an FP32 TMEM accumulator.  A CTA of 128 threads owns a 128 x 128
-// output tile (M rows = TMEM lanes, N columns) and a K range; its K range is taken in
-// chunks of 64: the threads stage the chunk's A and B tiles into shared memory in the
-// canonical K-major layout (transposing while they stage when the operand is stored the
-// other way), one thread issues the chunk's K/16 MMAs and commits them to an mbarrier
-// (bounded wait), and the TMEM accumulator carries the sum over the CTA's whole K range.
-// With split-K each CTA writes its partial tile to a workspace and k_gemm_reduce adds the
-// partials in split order, so the result does not depend on scheduling (no atomics).
+// output tile (M rows = TMEM lanes, N columns) and a K range, taken in chunks of 64 through
+// two shared-memory buffers: the threads stage chunk i+1 (16-byte loads; an operand stored
+// the other way is loaded as 8 x 8 blocks and transposed in registers) while the tensor
+// core runs chunk i's K/16 MMAs, issued by one thread and committed to the buffer's
+// mbarrier (bounded waits).  The TMEM accumulator carries the sum over the CTA's K range.
+// The epilogue goes through shared memory so that every warp store writes 128 contiguous
+// bytes of one output row.  With split-K each CTA writes its partial tile to a workspace
+// and k_gemm_reduce adds the partials in split order, so the result does not depend on
+// scheduling (no atomics).
 // ---------------------------------------------------------------------------------------
 constexpr int kGtRows = 128, kGtK = 64, kGtThreads = 128;
+constexpr int kGtTile = kGtRows * kGtK;             // elements of one operand chunk (16 KB)
+constexpr int kGtSmem = 2 * 2 * kGtTile * 2;        // two buffers of (A, B): 64 KB
+constexpr int kGtEpi = 33;                          // floats per staged output row (no bank conflicts)
+static_assert(kGtRows * kGtEpi * 4 <= kGtSmem, "epilogue staging fits in the operand buffers");
 
-struct GemmTcSmem {
-  __nv_bfloat16 a[kGtRows * kGtK];  // 16 KB: A chunk, canonical K-major [128][64]
-  __nv_bfloat16 b[kGtRows * kGtK];  // 16 KB: B chunk, canonical K-major [N tile][64]
-  uint64_t mbar;
-  uint32_t tmem_base;
-  int abort;
-};
+// 8 x 8 transpose of 16-bit elements: in[i] holds row i (8 elements), out[j] column j
+__device__ __forceinline__ void gt_transpose8(const uint4 in[8], uint4 out[8]) {
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(in);  // w[4*i + q] = (in[i][2q], in[i][2q+1])
+  uint32_t *o = reinterpret_cast<uint32_t *>(out);              // o[4*j + p] = (in[2p][j], in[2p+1][j])
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t lo = w[4 * (2 * p) + q], hi = w[4 * (2 * p + 1) + q];
+      o[4 * (2 * q) + p] = __byte_perm(lo, hi, 0x5410);
+      o[4 * (2 * q + 1) + p] = __byte_perm(lo, hi, 0x7632);
+    }
+}
 
 // Stages rows [r0, r0+128) x k [k0, k0+64) of X into the canonical K-major tile dst, where
 // element (r, k) is X[r*ld + k] (trans = 0) or X[k*ld + r] (trans = 1); rows >= rmax and
@@ -709,8 +721,9 @@ __device__ __forceinline__ void gt_stage(__nv_bfloat16 *dst, const __nv_bfloat16
                                          int r0, int rmax, int k0, int kend) {
   const int tid = threadIdx.x;
   char *d = reinterpret_cast<char *>(dst);
-  const bool vec = !trans && (ld % 8 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
-  if (vec) {
+  const bool aligned = (ld % 8 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+  const __nv_bfloat16 zero = __float2bfloat16(0.f);
+  if (!trans && aligned) {
     // 16-byte chunks along k: 128 rows x 8 chunks
     for (int e = tid; e < kGtRows * (kGtK / 8); e += kGtThreads) {
       const int r = e >> 3, kc = e & 7, gr = r0 + r, gk = k0 + 8 * kc;
@@ -721,18 +734,41 @@ __device__ __forceinline__ void gt_stage(__nv_bfloat16 *dst, const __nv_bfloat16
         } else {
           __nv_bfloat16 t[8];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) t[j] = gk + j < kend ? X[(int64_t)gr * ld + gk + j] : __float2bfloat16(0.f);
+          for (int j = 0; j < 8; ++j) t[j] = gk + j < kend ? X[(int64_t)gr * ld + gk + j] : zero;
           v = *reinterpret_cast<const uint4 *>(t);
         }
       }
       *reinterpret_cast<uint4 *>(d + tc_chunk(r, kc, kGtK)) = v;
     }
+  } else if (aligned) {
+    // one 8 (k) x 8 (r) block per thread: 8 loads of 8 consecutive r, transposed in
+    // registers into 8 chunks of 8 consecutive k; 16 threads read 256 contiguous bytes
+    const int rb = tid & 15, kb = tid >> 4, gr = r0 + 8 * rb;
+    uint4 in[8], out[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int gk = k0 + 8 * kb + i;
+      in[i] = make_uint4(0u, 0u, 0u, 0u);
+      if (gk < kend && gr < rmax) {
+        const __nv_bfloat16 *src = X + (int64_t)gk * ld + gr;
+        if (gr + 8 <= rmax) {
+          in[i] = __ldg(reinterpret_cast<const uint4 *>(src));
+        } else {
+          __nv_bfloat16 t[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) t[j] = gr + j < rmax ? src[j] : zero;
+          in[i] = *reinterpret_cast<const uint4 *>(t);
+        }
+      }
+    }
+    gt_transpose8(in, out);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) *reinterpret_cast<uint4 *>(d + tc_chunk(8 * rb + j, kb, kGtK)) = out[j];
   } else {
-    // pairs (k, k+1) of one row per thread, 4-byte stores; consecutive threads take
-    // consecutive rows, so the transposed loads are coalesced
+    // unaligned operand: pairs (k, k+1) of one row per thread, 4-byte stores
     for (int e = tid; e < kGtRows * (kGtK / 2); e += kGtThreads) {
       const int r = e & (kGtRows - 1), k = 2 * (e >> 7), gr = r0 + r;
-      __nv_bfloat16 v0 = __float2bfloat16(0.f), v1 = v0;
+      __nv_bfloat16 v0 = zero, v1 = zero;
       if (gr < rmax) {
         const int g0 = k0 + k, g1 = g0 + 1;
         if (g0 < kend) v0 = trans ? X[(int64_t)g0 * ld + gr] : X[(int64_t)gr * ld + g0];
@@ -751,19 +787,25 @@ __global__ void __launch_bounds__(kGtThreads) k_gemm_tc(int M, int N, int K, con
                                                         int ldb, int trans_b, float *__restrict__ Cm, int ldc,
                                                         int accumulate, int k_per_split, float *__restrict__ part,
                                                         int *__restrict__ err, uint32_t spin) {
-  __shared__ __align__(128) GemmTcSmem sm;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  extern __shared__ __align__(1024) unsigned char gsm[];
+  __shared__ uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  __nv_bfloat16 *bufs = reinterpret_cast<__nv_bfloat16 *>(gsm);  // [2 buffers][A, B][kGtTile]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n0 = blockIdx.x * kGtRows, m0 = blockIdx.y * kGtRows;
   const int kb = blockIdx.z * k_per_split, ke = min(K, kb + k_per_split);
   const int nvalid = min(kGtRows, N - n0), ntile = (nvalid + 15) / 16 * 16;
   if (tid == 0) {
-    sm.abort = 0;
-    const unsigned a = (unsigned)__cvta_generic_to_shared(&sm.mbar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    abort_flag = 0;
+    for (int b = 0; b < 2; ++b) {
+      const unsigned a = (unsigned)__cvta_generic_to_shared(&mbar[b]);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
-    const unsigned dst = (unsigned)__cvta_generic_to_shared(&sm.tmem_base);
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(&tmem_base);
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -771,63 +813,84 @@ __global__ void __launch_bounds__(kGtThreads) k_gemm_tc(int M, int N, int K, con
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  uint32_t phase = 0;
-  bool issued = false;
-  for (int k0 = kb; k0 < ke && !sm.abort; k0 += kGtK) {
-    gt_stage(sm.a, A, lda, trans_a, m0, M, k0, ke);
-    gt_stage(sm.b, B, ldb, !trans_b, n0, N, k0, ke);
+  uint32_t ph[2] = {0u, 0u};  // parity of the next phase of each buffer's mbarrier (thread 0)
+  int pending = -1;           // buffer whose last commit has not been waited for (thread 0)
+  int chunks = 0;
+  for (int k0 = kb; k0 < ke; k0 += kGtK, ++chunks) {
+    if (abort_flag) break;  // set by thread 0 before the last barrier: the same for all
+    const int s = chunks & 1;
+    __nv_bfloat16 *sa = bufs + (2 * s) * kGtTile, *sb = sa + kGtTile;
+    // buffer s was last read by chunk i-2's MMAs, waited for at the end of chunk i-1
+    gt_stage(sa, A, lda, trans_a, m0, M, k0, ke);
+    gt_stage(sb, B, ldb, !trans_b, n0, N, k0, ke);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (tid == 0) {
-      const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sm.a), b0 = (uint32_t)__cvta_generic_to_shared(sm.b);
+      const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sa), b0 = (uint32_t)__cvta_generic_to_shared(sb);
       const uint32_t idesc = tc_idesc(kGtRows, ntile);
       const int steps = (min(kGtK, ke - k0) + 15) / 16;
-      for (int s = 0; s < steps; ++s)
-        tc_mma(sm.tmem_base, tc_desc(a0 + 256u * s, 16u * kGtK), tc_desc(b0 + 256u * s, 16u * kGtK), idesc,
-               (issued || s > 0) ? 1u : 0u);
-      tc_commit(&sm.mbar);
-      if (!tc_wait(&sm.mbar, phase, spin)) sm.abort = 1;
+      for (int st = 0; st < steps; ++st)
+        tc_mma(tmem_base, tc_desc(a0 + 256u * st, 16u * kGtK), tc_desc(b0 + 256u * st, 16u * kGtK), idesc,
+               (chunks > 0 || st > 0) ? 1u : 0u);
+      tc_commit(&mbar[s]);
+      // the previous chunk's MMAs (buffer s^1) must be done before the next chunk is staged
+      if (pending >= 0) {
+        if (!tc_wait(&mbar[pending], ph[pending], spin)) abort_flag = 1;
+        ph[pending] ^= 1u;
+      }
+      pending = s;
     }
-    issued = true;
     __syncthreads();
-    phase ^= 1u;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
-  // epilogue: thread t owns row m0 + t (TMEM lane t)
-  const int m = m0 + tid;
-  const uint32_t tlane = sm.tmem_base + ((uint32_t)(warp * 32) << 16);
-  const bool ok = !sm.abort;
-  for (int c = 0; c < ntile; c += 16) {
-    float v[16];
+  // the last commit (it tracks every earlier MMA of this thread too): also after a
+  // time-out, bounded, so that no MMA is left in flight when the TMEM is freed
+  if (tid == 0 && pending >= 0) {
+    if (!tc_wait(&mbar[pending], ph[pending], spin)) abort_flag = 1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // epilogue: warp w reads TMEM lanes 32w.. (its rows) 32 columns at a time, stages them
+  // in shared memory row by row, and writes each row's 32 columns with one store
+  const bool ok = !abort_flag;
+  const bool issued = chunks > 0;
+  float *stg = reinterpret_cast<float *>(gsm);
+  const uint32_t tlane = tmem_base + ((uint32_t)(warp * 32) << 16);
+  for (int c = 0; c < ntile; c += 32) {
+    float v[32];
     if (issued && ok) {
-      tc_ld16(tlane + (uint32_t)c, v);
+      tc_ld32(tlane + (uint32_t)c, v);
     } else {
 #pragma unroll
-      for (int j = 0; j < 16; ++j) v[j] = ok ? 0.f : __int_as_float(0x7fc00000);
+      for (int j = 0; j < 32; ++j) v[j] = ok ? 0.f : __int_as_float(0x7fc00000);
     }
-    if (m < M) {
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int n = n0 + c + j;
-        if (c + j < nvalid) {
-          if (part) {
-            part[((int64_t)blockIdx.z * M + m) * N + n] = v[j];
-          } else {
-            float *dst = Cm + (int64_t)m * ldc + n;
-            *dst = accumulate ? *dst + v[j] : v[j];
-          }
+    for (int j = 0; j < 32; ++j) stg[tid * kGtEpi + j] = v[j];
+    __syncwarp();
+    const int n = n0 + c + lane;
+    const bool col_ok = c + lane < nvalid;
+    for (int rr = 0; rr < 32; ++rr) {
+      const int row = warp * 32 + rr, m = m0 + row;
+      if (m < M && col_ok) {
+        const float x = stg[row * kGtEpi + lane];
+        if (part) {
+          part[((int64_t)blockIdx.z * M + m) * N + n] = x;
+        } else {
+          float *dst = Cm + (int64_t)m * ldc + n;
+          *dst = accumulate ? *dst + x : x;
         }
       }
     }
+    __syncwarp();
   }
   if (!ok && tid == 0) atomicExch(err, 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem_base), "r"(kTmemCols)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols)
                  : "memory");
   }
 }
@@ -1303,8 +1366,10 @@ delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A,
       if (st != DELTA_OK) return st;
       part = static_cast<float *>(buf);
     }
+    if ((e = cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem)) != cudaSuccess)
+      return cuda_error(e, "gemm shared memory");
     dim3 grid((N + kGtRows - 1) / kGtRows, (M + kGtRows - 1) / kGtRows, splits);
-    k_gemm_tc<<<grid, kGtThreads, 0, ctx->stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, trans_a,
+    k_gemm_tc<<<grid, kGtThreads, kGtSmem, ctx->stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, trans_a,
                                                     (const __nv_bfloat16 *)B, ldb, trans_b, C, ldc, accumulate, per,
                                                     part, ctx->gemm_err, kTcSpin);
     ctx->launches += 1;

@@ -11,9 +11,9 @@ namespace delta {
 
 // Closest points of edge (HA<-TA) and edge (HB<-TB): Sunday's clamped parameters as
 // written in bf.cpp:586-697.  The edge runs from its tail T (parameter 0) to its head H
-// (parameter 1).  Returns |dP|.
+// (parameter 1).  Returns |dP|^2 (seg_seg_ref: |dP|).
 template <class R>
-__device__ __forceinline__ R seg_seg_ref(const R *HA, const R *TA, const R *HB, const R *TB, R &sc, R &tc) {
+__device__ __forceinline__ R seg_seg_sq_ref(const R *HA, const R *TA, const R *HB, const R *TB, R &sc, R &tc) {
   R u[3], v[3], w[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -51,15 +51,21 @@ __device__ __forceinline__ R seg_seg_ref(const R *HA, const R *TA, const R *HB, 
   R dP[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) dP[k] = (TA[k] - TB[k]) + (sc * (HA[k] - TA[k])) - (tc * (HB[k] - TB[k]));
-  return sqrt_(dP[0] * dP[0] + dP[1] * dP[1] + dP[2] * dP[2]);
+  return dP[0] * dP[0] + dP[1] * dP[1] + dP[2] * dP[2];
+}
+
+template <class R>
+__device__ __forceinline__ R seg_seg_ref(const R *HA, const R *TA, const R *HB, const R *TB, R &sc, R &tc) {
+  return sqrt_(seg_seg_sq_ref(HA, TA, HB, TB, sc, tc));
 }
 
 // Point X against triangle (V0,V1,V2): Eberly's seven regions as written in
-// bf.cpp:920-1090.  s runs along V1-V0, t along V2-V0.  Returns the distance.  The final
-// clamp of the squared distance is bf.cpp:1090's `<= 0` (kClampLE) or point.cpp:199's and
-// zoltan/hybrid.cpp's `< 0`; they differ only for -0.0, which `<` keeps.
+// bf.cpp:920-1090.  s runs along V1-V0, t along V2-V0.  Returns the clamped squared
+// distance (pt_tri_ref: the distance).  The final clamp of the squared distance is
+// bf.cpp:1090's `<= 0` (kClampLE) or point.cpp:199's and zoltan/hybrid.cpp's `< 0`; they
+// differ only for -0.0, which `<` keeps.
 template <class R, bool kClampLE = true>
-__device__ __forceinline__ R pt_tri_ref(const R *V0, const R *V1, const R *V2, const R *X, R &s_out, R &t_out) {
+__device__ __forceinline__ R pt_tri_sq_ref(const R *V0, const R *V1, const R *V2, const R *X, R &s_out, R &t_out) {
   R E0[3], E1[3], Dv[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -145,16 +151,22 @@ __device__ __forceinline__ R pt_tri_ref(const R *V0, const R *V1, const R *V2, c
   if (kClampLE ? (sq <= zero) : (sq < zero)) sq = zero;
   s_out = s;
   t_out = t;
-  return sqrt_(sq);
+  return sq;
 }
 
-// pt_tri_ref with one division per call and no divergent arithmetic: the region and its
+template <class R, bool kClampLE = true>
+__device__ __forceinline__ R pt_tri_ref(const R *V0, const R *V1, const R *V2, const R *X, R &s_out, R &t_out) {
+  return sqrt_(pt_tri_sq_ref<R, kClampLE>(V0, V1, V2, X, s_out, t_out));
+}
+
+// pt_tri_sq_ref with one division per call and no divergent arithmetic: the region and its
 // sub-case are classified first from the same comparisons, in the same order, on the same
 // rounded quantities; then the one quotient the case needs (-d/a, -e/c, 1/det or
 // numer/denom) is formed, and s, t and the squared distance follow from it with the
-// case's own expression.  Results equal pt_tri_ref's bit for bit.
+// case's own expression.  Results equal pt_tri_sq_ref's bit for bit.
 template <class R, bool kClampLE = true>
-__device__ __forceinline__ R pt_tri_lean(const R *V0, const R *V1, const R *V2, const R *X, R &s_out, R &t_out) {
+__device__ __forceinline__ R pt_tri_sq_lean(const R *V0, const R *V1, const R *V2, const R *X, R &s_out,
+                                            R &t_out) {
   R E0[3], E1[3], Dv[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -212,7 +224,7 @@ __device__ __forceinline__ R pt_tri_lean(const R *V0, const R *V1, const R *V2, 
   if (kClampLE ? (sq <= zero) : (sq < zero)) sq = zero;
   s_out = s;
   t_out = t;
-  return sqrt_(sq);
+  return sq;
 }
 
 // Closest point on edge pair j = 3*ea + eb for parameters (sc, tc); bf.cpp:715-879.

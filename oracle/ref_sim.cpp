@@ -29,8 +29,9 @@ extern "C" {
 // each run through the reference's bf() over all of its triangle pairs.  The body and
 // triangle arrays are dor_scene's (delta_oracle.h).  getContactsForces uses the constants
 // compiled into forces.cpp (SPRING 1e4, DAMPER 0.5, FRICTION 0.5).  Candidate pairs and
-// bodies are spread over the threads with OpenMP when this file is compiled with it (the
-// timed baseline build); each bf() call then runs serially inside (OpenMP does not nest).
+// bodies are spread over the threads with OpenMP (both builds); each bf() call and each
+// body's sum over its partners runs serially, so the result does not depend on the
+// threads.
 struct ref_scene {
   int32_t n_bodies;
   const int64_t *tri_offset;

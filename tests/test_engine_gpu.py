@@ -329,23 +329,79 @@ def test_graph_many_contacts_per_pair_equals_stepping_and_oracle(ctx, oracle):
         assert np.array_equal(g_c[f], o_c[f]), f
 
 
-@pytest.mark.skipif(not __import__("os").environ.get("DELTA_LONG_TESTS"),
-                    reason="opt-in (DELTA_LONG_TESTS=1): the lattice's 1000 steps against the oracle")
-@pytest.mark.parametrize("driver,graph", [(0, False), (8, True)])
-def test_lattice_1000_steps_bit_exact(ctx, oracle, driver, graph):
-    """The small plain configuration in full: 256 icospheres, FP64, dt 1e-5, 1000 steps;
-    the GPU trajectory (FP64 bf stepped, or the certified driver as a CUDA graph) equals the
-    oracle's bit for bit."""
-    from delta_b200.engine import Simulation, StepParams
-    from delta_b200.scenarios import lattice_scene
+@pytest.fixture(scope="module")
+def hopper():
+    from delta_b200.scenarios import hopper_scene
 
-    scene = lattice_scene(seed=2024)
+    return hopper_scene(10000, seed=7)
+
+
+@pytest.fixture(scope="module")
+def hopper_oracle(oracle, hopper):
     p = PARAMS
-    o_state, o_cps, _ = oracle.simulate(scene, p["dt"], p["gravity"], p["spring"], p["damper"], p["friction"], 1000)
-    sim = Simulation(ctx, scene, driver)
-    cps = sim.step(1000, StepParams.make(**p), graph=graph)
-    st = sim.state()
+    return oracle.simulate(hopper, 5e-6, p["gravity"], p["spring"], p["damper"], p["friction"], 4)
+
+
+@pytest.mark.parametrize("driver,graph", [(0, False), (8, True), (9, True)])
+def test_hopper_steps_bit_exact(ctx, hopper, hopper_oracle, driver, graph):
+    """The uneven hopper (10,000 particles of 40-320 triangles over a 2,048-triangle cone,
+    ~3,700 contacts per step): 4 steps of the plain FP64 driver (stepped) and of the culled
+    drivers (graph-replayed) equal the oracle's bit for bit, trajectory and contacts."""
+    from delta_b200.engine import Simulation, StepParams
+
+    o_state, o_cps, o_c = hopper_oracle
+    assert min(o_cps) > 1000
+    prm = dict(PARAMS, dt=5e-6)
+    sim = Simulation(ctx, hopper, driver)
+    cps = sim.step(4, StepParams.make(**prm), graph=graph)
+    st, c = sim.state(), sim.contacts()
     sim.close()
     assert list(cps) == list(o_cps)
     for k in STATE:
         assert np.array_equal(st[k], o_state[k]), k
+    assert len(c) == len(o_c)
+    for f in FIELDS:
+        assert np.array_equal(c[f], o_c[f]), f
+
+
+def _digests(state):
+    import hashlib
+
+    return {k: hashlib.sha256(np.ascontiguousarray(state[k], np.float64).tobytes()).hexdigest() for k in STATE}
+
+
+def _fixture(name):
+    import json
+    from pathlib import Path
+
+    return json.loads((Path(__file__).resolve().parent / "golden" / name).read_text())
+
+
+@pytest.mark.parametrize("case,driver,graph", [("lattice", 0, False), ("lattice", 8, True), ("hopper", 0, False),
+                                               ("hopper", 8, True), ("hopper", 9, True), ("hopper", 10, True)])
+def test_full_length_runs_equal_the_reference(ctx, hopper, case, driver, graph):
+    """Two configurations at their full length against the reference's own time step
+    (tests/golden/make_timestep_golden.py: the reference's bf(), getContactsForces with
+    forces.cpp's compiled constants, and dynamics.cpp's updates, run on the host): the
+    256-icosphere lattice for 1000 steps and the 10,000-particle hopper for 2000.  The
+    contacts of every step and every state array after the last step (SHA-256 of the
+    bytes) equal the reference's, for the plain FP64 driver and for the culled drivers
+    replayed as a CUDA graph.  The learned driver (FP32 hybrid) matches the contact
+    counts but is not bit-exact: its trajectory stays within 1e-9 m of the reference's."""
+    from delta_b200.engine import Simulation, StepParams
+    from delta_b200.scenarios import lattice_scene
+
+    fx = _fixture("timestep_lattice_1000.json" if case == "lattice" else "timestep_hopper_2000.json")
+    scene = lattice_scene(seed=2024) if case == "lattice" else hopper
+    m = fx["material"]
+    prm = StepParams.make(dt=fx["dt"], gravity=tuple(fx["gravity"]), spring=m["spring"], damper=m["damper"],
+                          friction=m["friction"])
+    sim = Simulation(ctx, scene, driver)
+    cps = sim.step(fx["steps"], prm, graph=graph)
+    st = sim.state()
+    sim.close()
+    if driver == 10:
+        assert np.abs(np.asarray(st["pos"][:24]) - np.asarray(fx["pos_first_bodies"])).max() < 1e-9
+        return
+    assert [int(x) for x in cps] == fx["contacts_per_step"]
+    assert _digests(st) == fx["sha256"]

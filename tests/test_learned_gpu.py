@@ -77,6 +77,29 @@ def test_gemm_bf16_vs_torch(ctx, engine, ta, tb, split, acc, shape):
     assert _rel(Cm.cpu(), ref.cpu()) <= 1e-5
 
 
+@pytest.mark.parametrize("split", [1, 32])
+def test_gemm_bf16_weight_gradient_shape(ctx, split):
+    """A weight-gradient GEMM as training runs it (dW = d^T prev: both operands transposed,
+    K = the batch, split-K, accumulate) on the tcgen05 engine against torch."""
+    import torch
+
+    from delta_b200._lib import check, lib
+    from delta_b200.learned import set_engine
+
+    set_engine(ctx, "tcgen05")
+    g = torch.Generator(device="cuda").manual_seed(split)
+    M, N, K = 128, 128, 16384
+    A = torch.randn((K, M), generator=g, device="cuda").to(torch.bfloat16)
+    B = torch.randn((K, N), generator=g, device="cuda").to(torch.bfloat16)
+    C0 = torch.randn((M, N), generator=g, device="cuda")
+    Cm = C0.clone()
+    check(lib().delta_gemm_bf16(ctx.handle, M, N, K, A.data_ptr(), M, 1, B.data_ptr(), N, 0, Cm.data_ptr(), N, 1,
+                                split))
+    ctx.synchronize()
+    ref = A.float().T @ B.float() + C0
+    assert _rel(Cm.cpu(), ref.cpu()) <= 1e-5
+
+
 def test_features_bit_exact_vs_oracle(ctx, pairs):
     from delta_b200.learned import features
     from delta_b200.narrowphase import pairs_device
