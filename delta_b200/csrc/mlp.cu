@@ -698,7 +698,7 @@ constexpr int kGtRows = 128, kGtK = 64, kGtThreads = 128;
 constexpr int kGtTile = kGtRows * kGtK;             // elements of one operand chunk (16 KB)
 constexpr int kGtSmem = 2 * 2 * kGtTile * 2;        // two buffers of (A, B): 64 KB
 constexpr int kGtEpi = 33;                          // floats per staged output row (no bank conflicts)
-static_assert(kGtRows * kGtEpi * 4 <= kGtSmem, "epilogue staging fits in the operand buffers");
+static_assert(kGtRows * kGtEpi * 4 <= kGtSmem / 2, "epilogue staging fits in one operand buffer");
 
 // 8 x 8 transpose of 16-bit elements: in[i] holds row i (8 elements), out[j] column j
 __device__ __forceinline__ void gt_transpose8(const uint4 in[8], uint4 out[8]) {
@@ -1368,8 +1368,10 @@ delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A,
     }
     if ((e = cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem)) != cudaSuccess)
       return cuda_error(e, "gemm shared memory");
+    // a CTA with one K chunk uses one buffer: half the shared memory, twice the CTAs per SM
+    const int smem = per <= kGtK ? kGtSmem / 2 : kGtSmem;
     dim3 grid((N + kGtRows - 1) / kGtRows, (M + kGtRows - 1) / kGtRows, splits);
-    k_gemm_tc<<<grid, kGtThreads, kGtSmem, ctx->stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, trans_a,
+    k_gemm_tc<<<grid, kGtThreads, smem, ctx->stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, trans_a,
                                                     (const __nv_bfloat16 *)B, ldb, trans_b, C, ldc, accumulate, per,
                                                     part, ctx->gemm_err, kTcSpin);
     ctx->launches += 1;

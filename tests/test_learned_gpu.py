@@ -96,8 +96,10 @@ def test_gemm_bf16_weight_gradient_shape(ctx, split):
     check(lib().delta_gemm_bf16(ctx.handle, M, N, K, A.data_ptr(), M, 1, B.data_ptr(), N, 0, Cm.data_ptr(), N, 1,
                                 split))
     ctx.synchronize()
-    ref = A.float().T @ B.float() + C0
-    assert _rel(Cm.cpu(), ref.cpu()) <= 1e-5
+    # FP64 reference: with K = 16384 one FP32 accumulation chain (split 1) carries a relative
+    # rounding error of order sqrt(K) * 2^-24 ~ 1e-5, as torch's own FP32 matmul does
+    ref = A.double().T @ B.double() + C0.double()
+    assert _rel(Cm.cpu(), ref.cpu()) <= 4e-5
 
 
 def test_features_bit_exact_vs_oracle(ctx, pairs):
