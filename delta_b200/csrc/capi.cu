@@ -212,8 +212,8 @@ delta_status delta_set_pair_launch(delta_ctx *ctx, int method, int precision, in
                                    int32_t blocks_per_sm) {
   if (!ctx || method < DELTA_BF || method > DELTA_BF_CERT || (precision != 0 && precision != 1))
     return set_error(DELTA_ERR_INVALID, "delta_set_pair_launch: bad method/precision");
-  if (!(threads == 64 || threads == 128 || threads == 256) || blocks_per_sm < 1 ||
-      (method == DELTA_BF_CERT && threads == 256))
+  if (!(threads == 64 || threads == 128 || threads == 256) || blocks_per_sm < 0 ||
+      threads > pair_max_threads(method, precision))
     return set_error(DELTA_ERR_INVALID, "delta_set_pair_launch: unsupported launch shape");
   ctx->pair_launch[method][precision] = PairLaunch{threads, blocks_per_sm};
   ctx->pair_launch_set[method][precision] = true;
@@ -241,7 +241,8 @@ delta_status delta_autotune_pairs(delta_ctx *ctx, int method, int precision, int
       for (int b : {2, 4, 8, 16}) cand.push_back(PairLaunch{t, b});
   } else {
     for (int t : {64, 128, 256})
-      for (int b : {4, 8, 16, 32}) cand.push_back(PairLaunch{t, b});
+      for (int b : {4, 8, 16, 32, 0})  // 0: one thread per pair
+        if (t <= pair_max_threads(method, precision)) cand.push_back(PairLaunch{t, b});
   }
   cudaEvent_t e0, e1;
   cudaError_t e = cudaEventCreate(&e0);

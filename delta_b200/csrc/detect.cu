@@ -584,11 +584,20 @@ __global__ void __launch_bounds__(128, 5) k_cert_survivors(delta_meshes m, const
 // The reference's FP64 bfSolver (bf.cpp:217-1178, xf64) over the survivors of the box
 // test, one per thread: the culled driver without the FP32 filter (DELTA_DRV_BF_CULLED),
 // which separates what the culling gains from what the certified FP32 solver gains.
-__global__ void __launch_bounds__(128) k_bf64_survivors(delta_meshes m, const int32_t *__restrict__ pa,
-                                                        const int32_t *__restrict__ pb, RawContacts rc) {
+__global__ void __launch_bounds__(128, 5) k_bf64_survivors(delta_meshes m, const int32_t *__restrict__ pa,
+                                                           const int32_t *__restrict__ pb, RawContacts rc) {
   const unsigned long long cnt = *rc.sv_count;
   const int64_t n = (int64_t)cnt < rc.sv_cap ? (int64_t)cnt : rc.sv_cap;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  // a warp takes 32 survivors at a time and meets at __syncwarp after them, so that its
+  // lanes do not drift apart over the grid-stride loop (see k_pairs)
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = base + lane;
+    if (i >= n) {
+      __syncwarp();
+      continue;
+    }
     const uint64_t key = rc.sv[i];
     RowCtx r;
     r.k = (int64_t)(key >> 32);
@@ -618,6 +627,7 @@ __global__ void __launch_bounds__(128) k_bf64_survivors(delta_meshes m, const in
     for (int k = 0; k < 6; ++k) pq[k] = out[k].v;
     const double mg = (xf64(r.epsA) + xf64(r.epsB)).v;
     emit(rc, pq_dist64(pq) <= mg, pq, r, tb);  // bf.cpp:125
+    __syncwarp();
   }
 }
 

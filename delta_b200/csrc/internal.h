@@ -14,6 +14,8 @@ constexpr int kNumSMs = 148;  // B200
 
 // Launch shape of a pair-list kernel: threads per block (64, 128, 256) and the grid
 // cap in blocks per SM (cert: in units of the occupancy limit).
+// Launch shape of a pair kernel: threads per block and the grid cap in blocks per SM
+// (0: no cap, one thread per pair).
 struct PairLaunch {
   int threads = 256;
   int blocks_per_sm = 32;
@@ -23,9 +25,14 @@ inline PairLaunch default_pair_launch(int method) {
   if (method == 5) {
     c.threads = 128;
     c.blocks_per_sm = 8;
+  } else if (method == 0) {
+    c.threads = 128;
+    c.blocks_per_sm = 0;
   }
   return c;
 }
+// The largest threads per block the pair kernel of (method, precision) takes (pairs.cu).
+int pair_max_threads(int method, int precision);
 // DELTA_BF_CERT over pairs idx[0 .. *count) (count read on the device, at most max_count);
 // with `stage`, the coordinates of entry j come from stage's 18 planes of max_count.
 cudaError_t launch_cert_indexed(cudaStream_t s, const uint32_t *count, int64_t max_count, const uint32_t *idx,

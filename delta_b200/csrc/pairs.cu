@@ -14,13 +14,34 @@ namespace delta {
 
 enum { M_BF = 0, M_PENALTY = 1, M_PENALTY_ITER = 2, M_GJK = 3, M_HYBRID_PAIR = 4, M_BF_CERT = 5 };
 
+// Launch bounds of the pair kernel: the FP64 bfSolver kernel is held to 96 registers (5
+// blocks of 128 per SM; 109 unbounded, with one 256-thread block fewer per SM), the
+// others keep their registers.
 template <class R, int M>
-__global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
-                                               int64_t ld, double max_error, double *__restrict__ p,
-                                               double *__restrict__ q, double *__restrict__ dist,
-                                               uint8_t *__restrict__ flags) {
+struct PairBounds {
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+};
+template <>
+struct PairBounds<xf64, M_BF> {
+  static constexpr int kThreads = 128, kMinBlocks = 5;
+};
+
+// A warp walks the list 32 pairs at a time and meets at __syncwarp after each group: the
+// lanes of a divergent solver would otherwise drift apart over the iterations of a
+// grid-stride loop and run as several partial warps (measured: 4x slower when each
+// thread takes ~50 pairs).
+template <class R, int M>
+__global__ void __launch_bounds__(PairBounds<R, M>::kThreads, PairBounds<R, M>::kMinBlocks)
+    k_pairs(int64_t n, const double *__restrict__ a, const double *__restrict__ b, int64_t ld, double max_error,
+            double *__restrict__ p, double *__restrict__ q, double *__restrict__ dist, uint8_t *__restrict__ flags) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+    const int64_t i = base + lane;
+    if (i >= n) {
+      __syncwarp();
+      continue;
+    }
     R A[3][3], B[3][3];
 #pragma unroll
     for (int v = 0; v < 3; ++v)
@@ -51,6 +72,7 @@ __global__ void __launch_bounds__(256) k_pairs(int64_t n, const double *__restri
     }
     dist[i] = to_f64(pq_distance(pq));
     if (flags) flags[i] = (uint8_t)flag;
+    __syncwarp();
   }
 }
 
@@ -138,13 +160,16 @@ __global__ void __launch_bounds__(32 * W) k_pairs_cert_indexed(const uint32_t *_
   }
 }
 
+// cfg.blocks_per_sm > 0 caps the grid at that many blocks per SM (a grid-stride loop);
+// 0 launches one thread per pair
 template <class R, int M>
 static cudaError_t launch_one(cudaStream_t s, int64_t n, const double *a, const double *b, int64_t ld, double me,
                               double *p, double *q, double *dist, uint8_t *flags, PairLaunch cfg) {
-  const int threads = cfg.threads == 64 || cfg.threads == 128 ? cfg.threads : 256;
+  int threads = cfg.threads == 64 || cfg.threads == 128 ? cfg.threads : 256;
+  if (threads > PairBounds<R, M>::kThreads) threads = PairBounds<R, M>::kThreads;
   int64_t blocks = (n + threads - 1) / threads;
-  const int64_t cap = (int64_t)kNumSMs * (cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 32);
-  if (blocks > cap) blocks = cap;
+  if (cfg.blocks_per_sm > 0 && blocks > (int64_t)kNumSMs * cfg.blocks_per_sm) blocks = (int64_t)kNumSMs * cfg.blocks_per_sm;
+  if (blocks > 0x7fffffffLL) blocks = 0x7fffffffLL;
   if (blocks < 1) blocks = 1;
   k_pairs<R, M><<<(unsigned)blocks, threads, 0, s>>>(n, a, b, ld, me, p, q, dist, flags);
   return cudaGetLastError();
@@ -175,6 +200,11 @@ static cudaError_t launch_cert(cudaStream_t s, int64_t n, const double *a, const
   if (blocks > cap) blocks = cap;
   k_pairs_cert<W><<<(unsigned)(blocks > 0 ? blocks : 1), 32 * W, 0, s>>>(n, a, b, ld, p, q, dist, flags);
   return cudaGetLastError();
+}
+
+int pair_max_threads(int method, int precision) {
+  if (method == M_BF_CERT) return 128;
+  return (method == M_BF && precision == 0) ? PairBounds<xf64, M_BF>::kThreads : 256;
 }
 
 cudaError_t launch_pairs_cfg(int method, int precision, cudaStream_t s, int64_t n, const double *a, const double *b,

@@ -109,9 +109,9 @@ delta_status delta_pairs_run_host(delta_ctx *ctx, int method, int precision, int
                                   double *dist, uint8_t *flags);
 
 /* Launch shape of the pair kernel of (method, precision) on this context: threads per
- * block (64, 128 or 256; the certified kernel takes 64 or 128) and the grid cap in
- * blocks per SM.  No counterpart in the reference (its SIMD width and OpenMP schedule are
- * compile-time, bf.cpp:93-102). */
+ * block (64, 128 or 256; the certified kernel and the FP64 bf kernel take 64 or 128) and
+ * the grid cap in blocks per SM (0: no cap, one thread per pair).  No counterpart in the
+ * reference (its SIMD width and OpenMP schedule are compile-time, bf.cpp:93-102). */
 delta_status delta_set_pair_launch(delta_ctx *ctx, int method, int precision, int32_t threads,
                                    int32_t blocks_per_sm);
 
