@@ -251,6 +251,67 @@ __global__ void k_act_grad(int64_t M, int N, const float *dH, const float *Z, __
   dZ[e] = __float2bfloat16(dH[e] * gelu_grad(Z[e]));
 }
 
+// Row-tiled forms of the three element-wise kernels for N dividing 4 * 256 (N a power of
+// two, at most 1024): thread t of a block owns 4 consecutive columns (N4 = N / 4 groups of
+// them per row) of rows t / N4, t / N4 + 256 / N4, ..., so a warp moves whole row segments
+// with 16-byte loads and the column needs no 64-bit division.  Same arithmetic as the
+// scalar kernels above.
+__global__ void k_bias_act4(int64_t M, int N4, float *__restrict__ Z, const float *__restrict__ bias,
+                            __nv_bfloat16 *__restrict__ H, int act) {
+  const int c4 = threadIdx.x % N4, rows = blockDim.x / N4;
+  const float b0 = bias[4 * c4], b1 = bias[4 * c4 + 1], b2 = bias[4 * c4 + 2], b3 = bias[4 * c4 + 3];
+  for (int64_t m = (int64_t)blockIdx.x * rows + threadIdx.x / N4; m < M; m += (int64_t)gridDim.x * rows) {
+    float4 *zp = reinterpret_cast<float4 *>(Z + m * 4 * N4) + c4;
+    float4 z = *zp;
+    z.x += b0;
+    z.y += b1;
+    z.z += b2;
+    z.w += b3;
+    *zp = z;
+    if (H) {
+      const __nv_bfloat162 h0 = act ? __floats2bfloat162_rn(gelu(z.x), gelu(z.y)) : __floats2bfloat162_rn(z.x, z.y);
+      const __nv_bfloat162 h1 = act ? __floats2bfloat162_rn(gelu(z.z), gelu(z.w)) : __floats2bfloat162_rn(z.z, z.w);
+      uint2 v;
+      v.x = *reinterpret_cast<const uint32_t *>(&h0);
+      v.y = *reinterpret_cast<const uint32_t *>(&h1);
+      reinterpret_cast<uint2 *>(H + m * 4 * N4)[c4] = v;
+    }
+  }
+}
+
+__global__ void k_act_grad4(int64_t M, int N4, const float *__restrict__ dH, const float *__restrict__ Z,
+                            __nv_bfloat16 *__restrict__ dZ) {
+  const int c4 = threadIdx.x % N4, rows = blockDim.x / N4;
+  for (int64_t m = (int64_t)blockIdx.x * rows + threadIdx.x / N4; m < M; m += (int64_t)gridDim.x * rows) {
+    const float4 d = reinterpret_cast<const float4 *>(dH + m * 4 * N4)[c4];
+    const float4 z = reinterpret_cast<const float4 *>(Z + m * 4 * N4)[c4];
+    const __nv_bfloat162 h0 = __floats2bfloat162_rn(d.x * gelu_grad(z.x), d.y * gelu_grad(z.y));
+    const __nv_bfloat162 h1 = __floats2bfloat162_rn(d.z * gelu_grad(z.z), d.w * gelu_grad(z.w));
+    uint2 v;
+    v.x = *reinterpret_cast<const uint32_t *>(&h0);
+    v.y = *reinterpret_cast<const uint32_t *>(&h1);
+    reinterpret_cast<uint2 *>(dZ + m * 4 * N4)[c4] = v;
+  }
+}
+
+// db[n] += column sums of dZ: thread t sums column t % N over rows t / N, t / N + 256 / N,
+// ... (a warp reads whole row segments), the block combines its row partials per column
+// in shared memory and adds them to db.
+__global__ void k_colsum_rows(int64_t M, int N, const __nv_bfloat16 *__restrict__ dZ, float *db) {
+  __shared__ float part[256];
+  const int c = threadIdx.x % N, rows = blockDim.x / N;
+  float s = 0.f;
+  for (int64_t m = (int64_t)blockIdx.x * rows + threadIdx.x / N; m < M; m += (int64_t)gridDim.x * rows)
+    s += __bfloat162float(dZ[m * N + c]);
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x < N) {
+    float t = 0.f;
+    for (int r = 0; r < rows; ++r) t += part[r * N + threadIdx.x];
+    atomicAdd(&db[threadIdx.x], t);
+  }
+}
+
 // db[n] += sum over rows of dZ[:, n]
 __global__ void k_colsum(int64_t M, int N, const __nv_bfloat16 *dZ, float *db) {
   const int n = blockIdx.x;
@@ -895,15 +956,28 @@ __global__ void __launch_bounds__(kGtThreads) k_gemm_tc(int M, int N, int K, con
   }
 }
 
-// C[m][n] = (accumulate ? C[m][n] : 0) + sum over s in split order of part[s][m][n]
-__global__ void k_gemm_reduce(int M, int N, int splits, const float *__restrict__ part, float *__restrict__ Cm,
-                              int ldc, int accumulate) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (int64_t)M * N) return;
-  const int m = (int)(e / N), n = (int)(e % N);
-  float acc = accumulate ? Cm[(int64_t)m * ldc + n] : 0.f;
-  for (int s = 0; s < splits; ++s) acc += part[(int64_t)s * M * N + e];
-  Cm[(int64_t)m * ldc + n] = acc;
+// C[m][n] = (accumulate ? C[m][n] : 0) + the sum of the split partials part[s][m][n], in a
+// fixed order: a block of 8 warps takes 32 consecutive elements, warp w adds splits w,
+// w + 8, ... in order, and warp 0 adds the 8 warp sums in order (deterministic, and every
+// load is 128 contiguous bytes).
+__global__ void __launch_bounds__(256) k_gemm_reduce(int M, int N, int splits, const float *__restrict__ part,
+                                                     float *__restrict__ Cm, int ldc, int accumulate) {
+  __shared__ float ws[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t e = (int64_t)blockIdx.x * 32 + lane, mn = (int64_t)M * N;
+  float s = 0.f;
+  if (e < mn)
+    for (int j = w; j < splits; j += 8) s += part[(int64_t)j * mn + e];
+  ws[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && e < mn) {
+    float t = ws[0][lane];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) t += ws[k][lane];
+    const int m = (int)(e / N), n = (int)(e % N);
+    float *dst = Cm + (int64_t)m * ldc + n;
+    *dst = accumulate ? *dst + t : t;
+  }
 }
 
 // penaltySolver (penalty.cpp:434-582, adaptive, FP64 reference arithmetic) started from
@@ -1376,7 +1450,8 @@ delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A,
                                                     part, ctx->gemm_err, kTcSpin);
     ctx->launches += 1;
     if (splits > 1) {
-      k_gemm_reduce<<<nblk((int64_t)M * N), 256, 0, ctx->stream>>>(M, N, splits, part, C, ldc, accumulate);
+      k_gemm_reduce<<<(unsigned)(((int64_t)M * N + 31) / 32), 256, 0, ctx->stream>>>(M, N, splits, part, C, ldc,
+                                                                                     accumulate);
       ctx->launches += 1;
     }
     return cuda_error(cudaGetLastError(), "delta_gemm_bf16 (tcgen05)");
@@ -1393,11 +1468,27 @@ delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A,
   return cuda_error(cudaGetLastError(), "delta_gemm_bf16");
 }
 
+// The row-tiled element-wise kernels take N a power of two from 4 to 1024 and 16-byte
+// aligned FP32 rows (8-byte aligned BF16 rows follow).
+static bool rows_tiled(int N, const void *f32, const void *bf16) {
+  return N >= 4 && N <= 1024 && (N & (N - 1)) == 0 && (reinterpret_cast<uintptr_t>(f32) & 15) == 0 &&
+         (reinterpret_cast<uintptr_t>(bf16) & 7) == 0;
+}
+static unsigned tiled_blocks(int64_t M, int rows) {
+  const int64_t b = (M + rows - 1) / rows, cap = (int64_t)kNumSMs * 8;
+  return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
 delta_status delta_mlp_bias_act(delta_ctx *ctx, int64_t M, int N, float *Z, const float *bias, void *H_bf16,
                                 int gelu_on) {
   if (!ctx || !Z || !bias || M < 0 || N <= 0) return set_error(DELTA_ERR_INVALID, "delta_mlp_bias_act");
   if (M == 0) return DELTA_OK;
-  k_bias_act<<<nblk(M * N), 256, 0, ctx->stream>>>(M, N, Z, bias, (__nv_bfloat16 *)H_bf16, gelu_on);
+  if (rows_tiled(N, Z, H_bf16)) {
+    const int rows = 256 / (N / 4);
+    k_bias_act4<<<tiled_blocks(M, rows), 256, 0, ctx->stream>>>(M, N / 4, Z, bias, (__nv_bfloat16 *)H_bf16, gelu_on);
+  } else {
+    k_bias_act<<<nblk(M * N), 256, 0, ctx->stream>>>(M, N, Z, bias, (__nv_bfloat16 *)H_bf16, gelu_on);
+  }
   ctx->launches += 1;
   return cuda_error(cudaGetLastError(), "delta_mlp_bias_act");
 }
@@ -1414,7 +1505,12 @@ delta_status delta_mlp_mse(delta_ctx *ctx, int64_t M, const float *Y, const floa
 delta_status delta_mlp_act_grad(delta_ctx *ctx, int64_t M, int N, const float *dH, const float *Z, void *dZ_bf16) {
   if (!ctx || !dH || !Z || !dZ_bf16) return set_error(DELTA_ERR_INVALID, "delta_mlp_act_grad");
   if (M == 0) return DELTA_OK;
-  k_act_grad<<<nblk(M * N), 256, 0, ctx->stream>>>(M, N, dH, Z, (__nv_bfloat16 *)dZ_bf16);
+  if (rows_tiled(N, dH, dZ_bf16) && (reinterpret_cast<uintptr_t>(Z) & 15) == 0) {
+    const int rows = 256 / (N / 4);
+    k_act_grad4<<<tiled_blocks(M, rows), 256, 0, ctx->stream>>>(M, N / 4, dH, Z, (__nv_bfloat16 *)dZ_bf16);
+  } else {
+    k_act_grad<<<nblk(M * N), 256, 0, ctx->stream>>>(M, N, dH, Z, (__nv_bfloat16 *)dZ_bf16);
+  }
   ctx->launches += 1;
   return cuda_error(cudaGetLastError(), "delta_mlp_act_grad");
 }
@@ -1422,8 +1518,12 @@ delta_status delta_mlp_act_grad(delta_ctx *ctx, int64_t M, int N, const float *d
 delta_status delta_mlp_colsum(delta_ctx *ctx, int64_t M, int N, const void *dZ_bf16, float *db) {
   if (!ctx || !dZ_bf16 || !db) return set_error(DELTA_ERR_INVALID, "delta_mlp_colsum");
   if (M == 0) return DELTA_OK;
-  const int ys = (int)std::min<int64_t>(64, (M + 255) / 256);
-  k_colsum<<<dim3(N, ys > 0 ? ys : 1), 256, 0, ctx->stream>>>(M, N, (const __nv_bfloat16 *)dZ_bf16, db);
+  if (N <= 256 && (N & (N - 1)) == 0) {
+    k_colsum_rows<<<tiled_blocks(M, 256 / N), 256, 0, ctx->stream>>>(M, N, (const __nv_bfloat16 *)dZ_bf16, db);
+  } else {
+    const int ys = (int)std::min<int64_t>(64, (M + 255) / 256);
+    k_colsum<<<dim3(N, ys > 0 ? ys : 1), 256, 0, ctx->stream>>>(M, N, (const __nv_bfloat16 *)dZ_bf16, db);
+  }
   ctx->launches += 1;
   return cuda_error(cudaGetLastError(), "delta_mlp_colsum");
 }

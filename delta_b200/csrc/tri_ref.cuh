@@ -159,74 +159,6 @@ __device__ __forceinline__ R pt_tri_ref(const R *V0, const R *V1, const R *V2, c
   return sqrt_(pt_tri_sq_ref<R, kClampLE>(V0, V1, V2, X, s_out, t_out));
 }
 
-// pt_tri_sq_ref with one division per call and no divergent arithmetic: the region and its
-// sub-case are classified first from the same comparisons, in the same order, on the same
-// rounded quantities; then the one quotient the case needs (-d/a, -e/c, 1/det or
-// numer/denom) is formed, and s, t and the squared distance follow from it with the
-// case's own expression.  Results equal pt_tri_sq_ref's bit for bit.
-template <class R, bool kClampLE = true>
-__device__ __forceinline__ R pt_tri_sq_lean(const R *V0, const R *V1, const R *V2, const R *X, R &s_out,
-                                            R &t_out) {
-  R E0[3], E1[3], Dv[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    E0[k] = V1[k] - V0[k];
-    E1[k] = V2[k] - V0[k];
-    Dv[k] = V0[k] - X[k];
-  }
-  const R a = dot3(E0, E0), b = dot3(E0, E1), c = dot3(E1, E1);
-  const R d = dot3(E0, Dv), e = dot3(E1, Dv), f = dot3(Dv, Dv);
-  const R det = a * c - b * b;
-  const R s0 = b * e - c * d;
-  const R t0 = b * d - a * e;
-  const R zero = R(0), one = R(1), two = R(2);
-  const R md = -d, me = -e;
-  const R bd = b + d, ce = c + e, be = b + e, ad = a + d;  // region 2's and 6's tmp0, tmp1
-  const R denom = a - two * b + c;
-  // cases: f only; s = 1 (a + 2d + f); t = 1 (c + 2e + f); s = -d/a; t = -e/c; interior;
-  // s = numer/denom, t = 1 - s; t = numer/denom, s = 1 - t
-  enum { kF, kA, kC, kDS, kET, kR0, kS1, kT1 };
-  int kind;
-  R numer = one;
-  if ((s0 + t0) <= det) {
-    if (s0 < zero) {
-      if (t0 < zero && d < zero) kind = (md >= a) ? kA : kDS;  // region 4, d < 0
-      else kind = (e >= zero) ? kF : (me >= c) ? kC : kET;     // region 4 (d >= 0) and 3
-    } else if (t0 < zero) {                                    // region 5
-      kind = (d >= zero) ? kF : (md >= a) ? kA : kDS;
-    } else {
-      kind = kR0;
-    }
-  } else if (s0 < zero) {  // region 2
-    numer = ce - bd;
-    if (ce > bd) kind = (numer >= denom) ? kA : kS1;
-    else kind = (ce <= zero) ? kC : (e >= zero) ? kF : kET;
-  } else if (t0 < zero) {  // region 6
-    numer = ad - be;
-    if (ad > be) kind = (numer >= denom) ? kC : kT1;
-    else kind = (ad <= zero) ? kA : (d >= zero) ? kF : kDS;
-  } else {  // region 1
-    numer = c + e - b - d;
-    kind = (numer <= zero) ? kC : (numer >= denom) ? kA : kS1;
-  }
-  const R num = kind == kDS ? md : kind == kET ? me : kind == kR0 ? one : numer;
-  const R den = kind == kDS ? a : kind == kET ? c : kind == kR0 ? det : (kind == kS1 || kind == kT1) ? denom : one;
-  const R q = num / den;
-  R s = (kind == kA) ? one : (kind == kDS || kind == kS1) ? q : (kind == kT1) ? one - q : (kind == kR0) ? s0 * q : zero;
-  R t = (kind == kC) ? one : (kind == kET || kind == kT1) ? q : (kind == kS1) ? one - q : (kind == kR0) ? t0 * q : zero;
-  R sq;
-  if (kind >= kR0) sq = s * (a * s + b * t + two * d) + t * (b * s + c * t + two * e) + f;
-  else if (kind == kDS) sq = d * s + f;
-  else if (kind == kET) sq = e * t + f;
-  else if (kind == kA) sq = a + two * d + f;
-  else if (kind == kC) sq = c + two * e + f;
-  else sq = f;
-  if (kClampLE ? (sq <= zero) : (sq < zero)) sq = zero;
-  s_out = s;
-  t_out = t;
-  return sq;
-}
-
 // Closest point on edge pair j = 3*ea + eb for parameters (sc, tc); bf.cpp:715-879.
 template <class R>
 __device__ __forceinline__ void seg_seg_points(const R A[3][3], const R B[3][3], int j, R sc, R tc, R pq[6]) {

@@ -252,14 +252,17 @@ def train(model: WarmStartMLP, X, T, valid, epochs: int = 1, batch: int = 65536,
     if nb == 0:
         raise ValueError("fewer rows than one batch")
     for ep in range(epochs):
-        perm = torch.randperm(n, device=X.device, generator=gen)[: nb * batch].view(nb, batch)
-        vb = valid[perm].view(nb, batch)
+        # one gather per epoch into shuffled copies; the mini-batches are contiguous slices
+        perm = torch.randperm(n, device=X.device, generator=gen)[: nb * batch]
+        Xs, Ts, vb = X[perm], T[perm], valid[perm].view(nb, batch)
+        del perm
         counts = vb.sum(1, dtype=torch.int64).cpu().tolist()
         total = torch.zeros(1, dtype=torch.float32, device=X.device)
         for k in range(nb):
-            idx = perm[k]
-            model.train_step(X[idx], T[idx], vb[k].contiguous(), counts[k], lr)
+            rows = slice(k * batch, (k + 1) * batch)
+            model.train_step(Xs[rows], Ts[rows], vb[k], counts[k], lr)
             total += model.loss
+        del Xs, Ts
         losses.append(float(total.item()) / nb)
         if log:
             log(f"epoch {ep}: loss {losses[-1]:.6g}")
