@@ -126,6 +126,7 @@ def main(argv=None):
         "train_samples_per_second": samples / train_s, "data_seconds": t_data,
         "evaluation": ev,
         "device": torch.cuda.get_device_name(0),
+        "gemm_engine": getattr(ctx, "mlp_engine", "tcgen05"),
     }
     out.with_suffix(".json").write_text(json.dumps(summary, indent=1) + "\n")
     print(json.dumps(summary, indent=1))
