@@ -755,23 +755,26 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 // and k_gemm_reduce adds the partials in split order, so the result does not depend on
 // scheduling (no atomics).
 // ---------------------------------------------------------------------------------------
-constexpr int kGtRows = 128, kGtK = 64, kGtThreads = 128;
+constexpr int kGtRows = 128, kGtK = 64, kGtThreads = 256;
 constexpr int kGtTile = kGtRows * kGtK;             // elements of one operand chunk (16 KB)
 constexpr int kGtSmem = 2 * 2 * kGtTile * 2;        // two buffers of (A, B): 64 KB
 constexpr int kGtEpi = 33;                          // floats per staged output row (no bank conflicts)
-static_assert(kGtRows * kGtEpi * 4 <= kGtSmem / 2, "epilogue staging fits in one operand buffer");
+constexpr int kGtEpiBytes = (kGtThreads / 32) * 32 * kGtEpi * 4;  // one 32 x 32 tile per warp
+constexpr int kGtSmem1 = kGtSmem / 2 > kGtEpiBytes ? kGtSmem / 2 : kGtEpiBytes;  // one-chunk CTAs
+static_assert(kGtEpiBytes <= kGtSmem, "epilogue staging fits in the operand buffers");
 
-// 8 x 8 transpose of 16-bit elements: in[i] holds row i (8 elements), out[j] column j
-__device__ __forceinline__ void gt_transpose8(const uint4 in[8], uint4 out[8]) {
+// 4 x 8 transpose of 16-bit elements: in[i] holds row i (8 elements), out[j] column j
+// (4 elements)
+__device__ __forceinline__ void gt_transpose4x8(const uint4 in[4], uint2 out[8]) {
   const uint32_t *w = reinterpret_cast<const uint32_t *>(in);  // w[4*i + q] = (in[i][2q], in[i][2q+1])
-  uint32_t *o = reinterpret_cast<uint32_t *>(out);              // o[4*j + p] = (in[2p][j], in[2p+1][j])
+  uint32_t *o = reinterpret_cast<uint32_t *>(out);              // o[2*j + p] = (in[2p][j], in[2p+1][j])
 #pragma unroll
-  for (int p = 0; p < 4; ++p)
+  for (int p = 0; p < 2; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const uint32_t lo = w[4 * (2 * p) + q], hi = w[4 * (2 * p + 1) + q];
-      o[4 * (2 * q) + p] = __byte_perm(lo, hi, 0x5410);
-      o[4 * (2 * q + 1) + p] = __byte_perm(lo, hi, 0x7632);
+      o[2 * (2 * q) + p] = __byte_perm(lo, hi, 0x5410);
+      o[2 * (2 * q + 1) + p] = __byte_perm(lo, hi, 0x7632);
     }
 }
 
@@ -785,9 +788,12 @@ __device__ __forceinline__ void gt_stage(__nv_bfloat16 *dst, const __nv_bfloat16
   const bool aligned = (ld % 8 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
   const __nv_bfloat16 zero = __float2bfloat16(0.f);
   if (!trans && aligned) {
-    // 16-byte chunks along k: 128 rows x 8 chunks
+    // 16-byte chunks along k: 128 rows x 8 chunks.  A warp takes 8 rows (one 8-row group)
+    // x 4 chunks: its loads are 8 runs of 64 contiguous bytes, and its stores fall in the
+    // 8 bank groups of the 8 rows, 4 threads each (the 4 wavefronts that 512 bytes take)
     for (int e = tid; e < kGtRows * (kGtK / 8); e += kGtThreads) {
-      const int r = e >> 3, kc = e & 7, gr = r0 + r, gk = k0 + 8 * kc;
+      const int w = e >> 5, l = e & 31;
+      const int r = 8 * (w >> 1) + (l & 7), kc = (l >> 3) + 4 * (w & 1), gr = r0 + r, gk = k0 + 8 * kc;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
       if (gr < rmax && gk < kend) {
         if (gk + 8 <= kend) {
@@ -802,13 +808,19 @@ __device__ __forceinline__ void gt_stage(__nv_bfloat16 *dst, const __nv_bfloat16
       *reinterpret_cast<uint4 *>(d + tc_chunk(r, kc, kGtK)) = v;
     }
   } else if (aligned) {
-    // one 8 (k) x 8 (r) block per thread: 8 loads of 8 consecutive r, transposed in
-    // registers into 8 chunks of 8 consecutive k; 16 threads read 256 contiguous bytes
-    const int rb = tid & 15, kb = tid >> 4, gr = r0 + 8 * rb;
-    uint4 in[8], out[8];
+    // half of an 8 (k) x 8 (r) block per thread: 4 loads of 8 consecutive r (k rows
+    // 4h .. 4h+3 of the block), transposed in registers into the 8-byte halves h of 8
+    // chunks of 8 consecutive k.  A warp holds one k block (kb): 16 r blocks x 2 halves;
+    // 16 threads read 256 contiguous bytes per load.  Each thread stores its 8 chunks
+    // starting at row (rb mod 8) of the 8-row group, so that the 32 stores of a warp fall
+    // in 16 different 16-byte bank groups and halves (2 wavefronts for 256 bytes)
+    static_assert(kGtThreads == 256, "the transposed staging maps 256 threads onto 16 x 8 x 2 half blocks");
+    const int h = tid & 1, rb = (tid >> 1) & 15, kb = tid >> 5, gr = r0 + 8 * rb;
+    uint4 in[4];
+    uint2 out[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int gk = k0 + 8 * kb + i;
+    for (int i = 0; i < 4; ++i) {
+      const int gk = k0 + 8 * kb + 4 * h + i;
       in[i] = make_uint4(0u, 0u, 0u, 0u);
       if (gk < kend && gr < rmax) {
         const __nv_bfloat16 *src = X + (int64_t)gk * ld + gr;
@@ -822,9 +834,22 @@ __device__ __forceinline__ void gt_stage(__nv_bfloat16 *dst, const __nv_bfloat16
         }
       }
     }
-    gt_transpose8(in, out);
+    gt_transpose4x8(in, out);
+    // rotate out[] left by rot = rb mod 8 (three conditional stages of register moves)
+    const int rot = rb & 7;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) *reinterpret_cast<uint4 *>(d + tc_chunk(8 * rb + j, kb, kGtK)) = out[j];
+    for (int b = 1; b < 8; b <<= 1) {
+      uint2 t[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) t[j] = out[(j + b) & 7];
+      if (rot & b) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) out[j] = t[j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      *reinterpret_cast<uint2 *>(d + tc_chunk(8 * rb + ((j + rot) & 7), kb, kGtK) + 8 * h) = out[j];
   } else {
     // unaligned operand: pairs (k, k+1) of one row per thread, 4-byte stores
     for (int e = tid; e < kGtRows * (kGtK / 2); e += kGtThreads) {
@@ -913,13 +938,15 @@ __global__ void __launch_bounds__(kGtThreads) k_gemm_tc(int M, int N, int K, con
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  // epilogue: warp w reads TMEM lanes 32w.. (its rows) 32 columns at a time, stages them
-  // in shared memory row by row, and writes each row's 32 columns with one store
+  // epilogue: warps w and w+4 read TMEM lanes 32(w%4).. (their rows), the first the
+  // column chunks 0, 64, the second 32, 96, 32 columns at a time; each stages its 32 x 32
+  // tile in shared memory row by row and writes each row's 32 columns with one store
   const bool ok = !abort_flag;
   const bool issued = chunks > 0;
-  float *stg = reinterpret_cast<float *>(gsm);
-  const uint32_t tlane = tmem_base + ((uint32_t)(warp * 32) << 16);
-  for (int c = 0; c < ntile; c += 32) {
+  const int quad = warp & 3;
+  float *stg = reinterpret_cast<float *>(gsm) + warp * 32 * kGtEpi;
+  const uint32_t tlane = tmem_base + ((uint32_t)(quad * 32) << 16);
+  for (int c = (warp >> 2) * 32; c < ntile; c += 64) {
     float v[32];
     if (issued && ok) {
       tc_ld32(tlane + (uint32_t)c, v);
@@ -928,14 +955,14 @@ __global__ void __launch_bounds__(kGtThreads) k_gemm_tc(int M, int N, int K, con
       for (int j = 0; j < 32; ++j) v[j] = ok ? 0.f : __int_as_float(0x7fc00000);
     }
 #pragma unroll
-    for (int j = 0; j < 32; ++j) stg[tid * kGtEpi + j] = v[j];
+    for (int j = 0; j < 32; ++j) stg[lane * kGtEpi + j] = v[j];
     __syncwarp();
     const int n = n0 + c + lane;
     const bool col_ok = c + lane < nvalid;
     for (int rr = 0; rr < 32; ++rr) {
-      const int row = warp * 32 + rr, m = m0 + row;
+      const int row = quad * 32 + rr, m = m0 + row;
       if (m < M && col_ok) {
-        const float x = stg[row * kGtEpi + lane];
+        const float x = stg[rr * kGtEpi + lane];
         if (part) {
           part[((int64_t)blockIdx.z * M + m) * N + n] = x;
         } else {
@@ -1443,7 +1470,7 @@ delta_status delta_gemm_bf16(delta_ctx *ctx, int M, int N, int K, const void *A,
     if ((e = cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem)) != cudaSuccess)
       return cuda_error(e, "gemm shared memory");
     // a CTA with one K chunk uses one buffer: half the shared memory, twice the CTAs per SM
-    const int smem = per <= kGtK ? kGtSmem / 2 : kGtSmem;
+    const int smem = per <= kGtK ? kGtSmem1 : kGtSmem;
     dim3 grid((N + kGtRows - 1) / kGtRows, (M + kGtRows - 1) / kGtRows, splits);
     k_gemm_tc<<<grid, kGtThreads, smem, ctx->stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, trans_a,
                                                     (const __nv_bfloat16 *)B, ldb, trans_b, C, ldc, accumulate, per,
