@@ -713,6 +713,44 @@ __global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const doubl
   if (d2 <= reach * reach) push_pair(L, j, sh, out, count, cap);
 }
 
+// The fixed-capacity pair list of a scene with at most 2^16 bodies and at most
+// kBlockSortCap entries, sorted and unpacked by one CTA (cub's block radix sort of 32-bit
+// keys over the 2 sh key bits) instead of a device-wide radix sort (a histogram and one
+// launch per 8-bit digit) and an unpacking kernel: one graph node instead of six.  The
+// result, the overflow flag and the pair total are k_unpack_pairs's.
+constexpr int kBlockSortThreads = 512, kBlockSortItems = 16;
+constexpr int64_t kBlockSortCap = (int64_t)kBlockSortThreads * kBlockSortItems;
+
+__global__ void __launch_bounds__(kBlockSortThreads) k_sort_unpack_pairs_block(
+    const uint64_t *__restrict__ keys, int64_t n, int sh, int32_t *__restrict__ a, int32_t *__restrict__ b,
+    const unsigned long long *count, int *ovf, int64_t *total) {
+  using Sort = cub::BlockRadixSort<uint32_t, kBlockSortThreads, kBlockSortItems>;
+  __shared__ typename Sort::TempStorage tmp;
+  const int t = threadIdx.x;
+  if (t == 0) {
+    const unsigned long long c = *count;
+    if (c > (unsigned long long)n) atomicCAS(ovf, 0, 1);
+    if (total) *total += (int64_t)(c < (unsigned long long)n ? c : (unsigned long long)n);
+  }
+  uint32_t k[kBlockSortItems];
+#pragma unroll
+  for (int j = 0; j < kBlockSortItems; ++j) {
+    const int64_t i = (int64_t)t * kBlockSortItems + j;
+    // a valid key has a < b < 2^sh, so it is never 0xffffffff, the empty key's low half
+    k[j] = i < n ? (uint32_t)keys[i] : 0xffffffffu;
+  }
+  Sort(tmp).Sort(k, 0, 2 * sh);
+#pragma unroll
+  for (int j = 0; j < kBlockSortItems; ++j) {
+    const int64_t i = (int64_t)t * kBlockSortItems + j;
+    if (i < n) {
+      const bool empty = k[j] == 0xffffffffu;
+      a[i] = empty ? -1 : (int32_t)(k[j] >> sh);
+      b[i] = empty ? -1 : (int32_t)(k[j] & ((1u << sh) - 1u));
+    }
+  }
+}
+
 // pair keys back to (a, b); the empty key ~0 gives (-1, -1).  With `count` (fixed
 // capacity n), thread 0 also flags an overflow of the n entries and adds the step's
 // candidate body pairs to *total.
@@ -1154,6 +1192,12 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
     k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
                                                                           sh, pk, count, pair_cap);
     kernels += 1;
+  }
+  if (2 * sh <= 32 && pair_cap <= kBlockSortCap) {
+    k_sort_unpack_pairs_block<<<1, kBlockSortThreads, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf,
+                                                                pairs_total);
+    kernels += 1;
+    return cuda_error(cudaGetLastError(), "broadphase fixed");
   }
   tb = temp_bytes;
   if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, pk, spk, pair_cap, 0, 2 * sh, st)) != cudaSuccess)
