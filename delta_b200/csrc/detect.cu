@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdlib>
 
+#include "blockscan.cuh"
 #include "internal.h"
 #include "pose.cuh"
 #include "tri_cert.cuh"
@@ -1191,7 +1192,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
     if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, -1, ctx->surv_blocks_per_sm)) != cudaSuccess)
       return cuda_error(e, "survivor kernel");
-    if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
+    if ((e = exclusive_sum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
       return cuda_error(e, "pair contact scan");
     k_bucket_contacts<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out, (uint64_t *)perm_in);
     k_pair_gather<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out, (const uint64_t *)perm_in,

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <vector>
 
+#include "blockscan.cuh"
 #include "internal.h"
 #include "pose.cuh"
 #include "real.cuh"
@@ -1046,7 +1047,7 @@ static cudaError_t build_grid(cudaStream_t st, const delta_scene &s, const Broad
   if (e != cudaSuccess) return e;
   k_grid_count<<<blocks_for(n), 256, 0, st>>>(s, plan.g, hg, pk, pk_cap, pcount);
   size_t tb = temp_bytes;
-  if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, hg.count, hg.start, hg.nb + 1, st)) != cudaSuccess) return e;
+  if ((e = exclusive_sum(temp, tb, hg.count, hg.start, hg.nb + 1, st)) != cudaSuccess) return e;
   k_grid_fill<<<blocks_for(n), 256, 0, st>>>(s, hg);
   return cudaGetLastError();
 }
@@ -1150,7 +1151,7 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   k_pair_forces_heads<true><<<blocks_for(cap, kHeadThreads), kHeadThreads, 0, st>>>(
       s, cv, d_nc, 0, nullptr, nullptr, p, 0, nullptr, nullptr, entry, cnt);
   size_t tb = temp_bytes;
-  if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, cnt, start, n + 1, st)) != cudaSuccess)
+  if ((e = exclusive_sum(temp, tb, cnt, start, (int64_t)n + 1, st)) != cudaSuccess)
     return cuda_error(e, "slave list scan");
   k_fill_slave_lists<<<blocks_for(cap), 256, 0, st>>>(s, cv, d_nc, start, fill, list);
   k_body_forces_lists<<<blocks_for(n), 256, 0, st>>>(s, cv, d_nc, start, list, entry, force, torque, has);
