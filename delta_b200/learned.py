@@ -156,10 +156,11 @@ class WarmStartMLP:
         """Gradients of the MSE over valid rows into self.grads (after forward(X))."""
         M = X.shape[0]
         # split-K of the weight gradients (K = the batch): the tcgen05 GEMM adds the partial
-        # tiles in a second kernel; about one CTA per SM, each with K/split >= 512 rows so
-        # that its two-buffer pipeline runs several chunks
+        # tiles in a second kernel; about two CTAs per SM (one left the SM's loads
+        # latency-bound), each with K/split >= 256 rows so that its two-buffer pipeline
+        # runs several chunks
         if getattr(self.ctx, "mlp_engine", "tcgen05") == "tcgen05":
-            split = max(1, min(148, M // 512))
+            split = max(1, min(296, M // 256))
         else:
             split = max(1, min(128, M // 1024))
         self.grads.zero_()
