@@ -405,3 +405,32 @@ def test_full_length_runs_equal_the_reference(ctx, hopper, case, driver, graph):
         return
     assert [int(x) for x in cps] == fx["contacts_per_step"]
     assert _digests(st) == fx["sha256"]
+
+
+def test_graph_sort_and_scan_paths_agree(ctx):
+    """The graph step sorts a candidate list of at most 8,192 entries in one CTA and
+    prefix-sums count arrays of at most 32,768 entries in one CTA; longer ones go to cub's
+    device-wide sort and scan.  A 40,000-particle box (its body and bucket arrays are
+    longer than 32,768) replayed with the default pair capacity and with one above 8,192
+    gives the stepped trajectory and contacts bit for bit."""
+    from delta_b200.engine import Simulation, StepParams
+    from delta_b200.scenarios import box_scene
+
+    scene = box_scene(40000, seed=11)
+    prm = StepParams.make(dt=2e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0)
+    runs = []
+    for graph, cap in ((False, None), (True, None), (True, 9000)):
+        sim = Simulation(ctx, scene, 8)
+        if cap:
+            sim.set_graph_capacity(cap, 1 << 16)
+        cps = sim.step(6, prm, graph=graph)
+        runs.append((list(cps), sim.state(), sim.contacts()))
+        assert sim.counters()["body_pairs"] > 0  # candidate pairs to sort every step
+        sim.close()
+    (c0, s0, k0) = runs[0]
+    for cps, st, c in runs[1:]:
+        assert cps == c0
+        for k in STATE:
+            assert np.array_equal(st[k], s0[k]), k
+        for f in FIELDS:
+            assert np.array_equal(c[f], k0[f]), f
