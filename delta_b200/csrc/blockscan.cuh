@@ -10,7 +10,9 @@
 namespace delta {
 
 constexpr int kBlockScanThreads = 1024, kBlockScanItems = 8;
-constexpr int64_t kBlockScanMax = 4LL * kBlockScanThreads * kBlockScanItems;  // 4 tiles
+// one tile: a CTA that loops over two or more tiles was slower than cub's two kernels (the
+// hopper's 10,001-entry slave lists: 8% of its replayed step)
+constexpr int64_t kBlockScanMax = (int64_t)kBlockScanThreads * kBlockScanItems;
 
 // out[i] = in[0] + ... + in[i-1] over tiles of 8192 entries, the running total carried
 // from tile to tile (integer sums: exact in any order).

@@ -722,9 +722,14 @@ __global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const doubl
 constexpr int kBlockSortThreads = 512, kBlockSortItems = 16;
 constexpr int64_t kBlockSortCap = (int64_t)kBlockSortThreads * kBlockSortItems;
 
+// ITEMS keys per thread: the smallest of 2, 4, 8, 16 whose 512 * ITEMS covers the list
+// (a block sort of a short list pays for every padded key: one sized to 8,192 keys made
+// the 256-body lattice's step 6% slower than cub's device sort)
+template <int ITEMS>
 __global__ void __launch_bounds__(kBlockSortThreads) k_sort_unpack_pairs_block(
     const uint64_t *__restrict__ keys, int64_t n, int sh, int32_t *__restrict__ a, int32_t *__restrict__ b,
     const unsigned long long *count, int *ovf, int64_t *total) {
+  constexpr int kBlockSortItems = ITEMS;
   using Sort = cub::BlockRadixSort<uint32_t, kBlockSortThreads, kBlockSortItems>;
   __shared__ typename Sort::TempStorage tmp;
   const int t = threadIdx.x;
@@ -1195,8 +1200,15 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
     kernels += 1;
   }
   if (2 * sh <= 32 && pair_cap <= kBlockSortCap) {
-    k_sort_unpack_pairs_block<<<1, kBlockSortThreads, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf,
-                                                                pairs_total);
+    const int64_t T = kBlockSortThreads;
+    if (pair_cap <= 2 * T)
+      k_sort_unpack_pairs_block<2><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
+    else if (pair_cap <= 4 * T)
+      k_sort_unpack_pairs_block<4><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
+    else if (pair_cap <= 8 * T)
+      k_sort_unpack_pairs_block<8><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
+    else
+      k_sort_unpack_pairs_block<16><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
     kernels += 1;
     return cuda_error(cudaGetLastError(), "broadphase fixed");
   }

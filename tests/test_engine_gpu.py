@@ -409,9 +409,9 @@ def test_full_length_runs_equal_the_reference(ctx, hopper, case, driver, graph):
 
 def test_graph_sort_and_scan_paths_agree(ctx):
     """The graph step sorts a candidate list of at most 8,192 entries in one CTA and
-    prefix-sums count arrays of at most 32,768 entries in one CTA; longer ones go to cub's
+    prefix-sums count arrays of at most 8,192 entries in one CTA; longer ones go to cub's
     device-wide sort and scan.  A 40,000-particle box (its body and bucket arrays are
-    longer than 32,768) replayed with the default pair capacity and with one above 8,192
+    longer than 8,192) replayed with the default pair capacity and with one above 8,192
     gives the stepped trajectory and contacts bit for bit."""
     from delta_b200.engine import Simulation, StepParams
     from delta_b200.scenarios import box_scene
