@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--method-table", type=int, default=1,
                     help="1: time every pair method in FP64 and FP32 and state each result's error per class")
+    ap.add_argument("--min-timed-s", type=float, default=1.0,
+                    help="a time-step arm whose steps take less runs again from the same initial state until its "
+                         "timed total reaches this (0: one run, e.g. under a profiler)")
     ap.add_argument("--timestep-steps", type=int, default=1000,
                     help="time steps of the 256-icosphere lattice (its configuration's full length)")
     ap.add_argument("--hopper-steps", type=int, default=2000,
@@ -186,7 +189,7 @@ def cpu_reference_rate(a, b, sample: int, min_seconds: float):
     return done / el, cores, kind
 
 
-MIN_TIMED_S = 1.0  # the least timed total of a time-step arm (repeated runs of the same steps)
+MIN_TIMED_S = 1.0  # the least timed total of a time-step arm (repeated runs of the same steps); --min-timed-s
 
 
 def _time_sim(ctx, stream, sim, steps, params, graph):
@@ -348,7 +351,9 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global MIN_TIMED_S
     args = parse()
+    MIN_TIMED_S = args.min_timed_s
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.box_steps < 0:
