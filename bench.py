@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--method-table", type=int, default=1,
                     help="1: time every pair method in FP64 and FP32 and state each result's error per class")
+    ap.add_argument("--timestep-arms", default="",
+                    help="comma-separated subset of the time-step arms to run (e.g. bf_cert_culled_graph under a "
+                         "profiler); default all, with their comparisons")
     ap.add_argument("--min-timed-s", type=float, default=1.0,
                     help="a time-step arm whose steps take less runs again from the same initial state until its "
                          "timed total reaches this (0: one run, e.g. under a profiler)")
@@ -240,7 +243,8 @@ def cpu_timestep_rate(scene, params, steps: int):
             "contacts_last_step": int(cps[-1]) if len(cps) else 0}
 
 
-def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, params, cpu_steps: int = 0):
+def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, params, cpu_steps: int = 0,
+                     arm_filter=None):
     """Timesteps/s of a scene with the plain FP64 bf driver (every triangle pair of every
     candidate body pair, as the reference) and with the certified FP32 driver (exact box
     culling + bf_cert), stepped and replayed as a CUDA graph.  All three must give the same
@@ -287,16 +291,22 @@ def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, para
             res["launch_shape"] = shape
         return res, state
 
+    only = set(arm_filter) if arm_filter else None
     for name, drv, graph, k in arms:
-        out[name], states[name] = timed_arm(ctx, drv, graph, k)
-    from delta_b200.narrowphase import Context
+        if only is None or name in only:
+            out[name], states[name] = timed_arm(ctx, drv, graph, k)
+    if only is None or "bf_cert_culled_graph_tuned" in only:
+        from delta_b200.narrowphase import Context
 
-    tctx = Context(0, stream=stream.cuda_stream)
-    try:
-        out["bf_cert_culled_graph_tuned"], states["bf_cert_culled_graph_tuned"] = timed_arm(
-            tctx, DRV_BF_CERT, True, steps, tune=True)
-    finally:
-        tctx.close()
+        tctx = Context(0, stream=stream.cuda_stream)
+        try:
+            out["bf_cert_culled_graph_tuned"], states["bf_cert_culled_graph_tuned"] = timed_arm(
+                tctx, DRV_BF_CERT, True, steps, tune=True)
+        finally:
+            tctx.close()
+    res = {"workload": workload, "steps": steps, "warmup": warmup, **out}
+    if only is not None:  # a subset of the arms (e.g. under a profiler): no comparisons
+        return res
     ref = states["fp64_bf"]
     exact = [n for n in states if n != "learned_culled_graph"]
     same = all(np.array_equal(ref[k], states[n][k]) for n in exact for k in ("pos", "vel", "rot", "x"))
@@ -307,7 +317,7 @@ def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, para
         "bit_identical": bool(all(np.array_equal(ref[k], lrn[k]) for k in ("pos", "vel", "rot", "x")))}
     sps = {k: v["steps_per_s"] for k, v in out.items()}
     cpu = cpu_timestep_rate(scene, params, cpu_steps) if cpu_steps > 0 else None
-    return {"workload": workload, "steps": steps, "warmup": warmup, **out, "cpu_baseline": cpu,
+    return {**res, "cpu_baseline": cpu,
             "speedup": sps["bf_cert_culled_graph"] / sps["fp64_bf"],
             "speedup_learned": sps["learned_culled_graph"] / sps["fp64_bf"],
             "speedup_tuned": sps["bf_cert_culled_graph_tuned"] / sps["fp64_bf"],
@@ -622,6 +632,7 @@ def main():
                "h2d_bound_pairs_per_s": world * h2d_gbs * 1e9 / ((ha.nbytes + hb.nbytes) / n)}
 
     ts = hop = box = None
+    arm_filter = [a for a in args.timestep_arms.split(",") if a]
     if args.timestep_steps > 0:
         from delta_b200.engine import StepParams
         from delta_b200.scenarios import hopper_scene, lattice_scene
@@ -631,7 +642,7 @@ def main():
             "256 perturbed icospheres (80 tri) on a 8x4x8 lattice over a 2-triangle floor, FP64, dt 1e-5, k 1e6, "
             "damping 0.1", args.timestep_steps, 3,
             StepParams.make(dt=1e-5, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0),
-            cpu_steps=3 if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0)
+            cpu_steps=3 if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0, arm_filter=arm_filter)
         if args.box_steps > 0:
             from delta_b200.scenarios import box_scene
 
@@ -639,14 +650,15 @@ def main():
                 ctx, stream, box_scene(200000, seed=args.seed),
                 "200,000 perturbed spheres of {80,160,320,500} triangles (r 4-12 mm, 53 M triangles) poured from a "
                 "lattice into a 0.6 x 1.2 x 0.6 m box of 12 wall triangles, FP64, dt 2e-6", args.box_steps, 2,
-                StepParams.make(dt=2e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0))
+                StepParams.make(dt=2e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0),
+                arm_filter=arm_filter)
         if args.hopper_steps > 0:
             hop = timestep_section(
                 ctx, stream, hopper_scene(10000, seed=args.seed),
                 "10,000 perturbed spheres of {40,80,160,320} triangles (r 5-15 mm) over a conical hopper of 2,048 "
                 "wall triangles (30 deg, 8 cm outlet), FP64, dt 5e-6", args.hopper_steps, 3,
                 StepParams.make(dt=5e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0),
-                cpu_steps=2 if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0)
+                cpu_steps=2 if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0, arm_filter=arm_filter)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
