@@ -744,14 +744,14 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 
 // ---------------------------------------------------------------------------------------
 // the training GEMM on the 5th-generation tensor cores: C[M,N] (+)= op(A)[M,K] op(B)[K,N]
-// with BF16 operands and an FP32 TMEM accumulator.  A CTA of 128 threads owns a 128 x 128
+// with BF16 operands and an FP32 TMEM accumulator.  A CTA of 256 threads owns a 128 x 128
 // output tile (M rows = TMEM lanes, N columns) and a K range, taken in chunks of 64 through
-// two shared-memory buffers: the threads stage chunk i+1 (16-byte loads; an operand stored
-// the other way is loaded as 8 x 8 blocks and transposed in registers) while the tensor
-// core runs chunk i's K/16 MMAs, issued by one thread and committed to the buffer's
-// mbarrier (bounded waits).  The TMEM accumulator carries the sum over the CTA's K range.
-// The epilogue goes through shared memory so that every warp store writes 128 contiguous
-// bytes of one output row.  With split-K each CTA writes its partial tile to a workspace
+// two shared-memory buffers: the threads stage chunk i+1 (16-byte loads spread over the
+// shared-memory banks; an operand stored the other way is loaded as half 8 x 8 blocks and
+// transposed in registers) while the tensor core runs chunk i's K/16 MMAs, issued by one
+// thread and committed to the buffer's mbarrier (bounded waits).  The TMEM accumulator
+// carries the sum over the CTA's K range.  The epilogue goes through shared memory so that
+// every warp store writes 128 contiguous bytes of one output row.  With split-K each CTA writes its partial tile to a workspace
 // and k_gemm_reduce adds the partials in split order, so the result does not depend on
 // scheduling (no atomics).
 // ---------------------------------------------------------------------------------------
