@@ -682,8 +682,11 @@ __global__ void k_grid_pairs(delta_scene s, Grid g, HashGrid hg, int sh, uint64_
   if (t >= 9 * (int64_t)s.n_bodies) return;
   const int32_t i = (int32_t)(t / 9), col = (int32_t)(t % 9);
   if (s.obstacle[i]) return;
-  int64_t c[3];
-  cell_of(s, g, i, c);
+  // the body's cell from the key the count pass stored (coordinates modulo 2^kCellBits,
+  // which is all cell_key keeps), instead of three FP64 divisions per thread
+  const uint64_t own = hg.cell[i];
+  const int64_t c[3] = {(int64_t)((own >> (2 * kCellBits)) & kCellMask), (int64_t)((own >> kCellBits) & kCellMask),
+                        (int64_t)(own & kCellMask)};
   const int64_t cx = c[0] + col / 3 - 1, cy = c[1] + col % 3 - 1;
   for (int dz = -1; dz <= 1; ++dz) {
     const uint64_t key = cell_key(cx, cy, c[2] + dz);
