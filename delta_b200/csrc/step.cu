@@ -672,28 +672,38 @@ __device__ __forceinline__ void push_pair(int32_t a, int32_t b, int sh, uint64_t
   if ((int64_t)pos < cap) out[pos] = ((uint64_t)(uint32_t)(a < b ? a : b) << sh) | (uint32_t)(a < b ? b : a);
 }
 
-// One thread per (body, cell column (dx, dy)): the three cells (cx+dx, cy+dy, cz-1 ..
-// cz+1) are looked up in their buckets, and a body of a bucket counts only when its cell
-// key is the cell's.  The 27 neighbour cells have distinct keys and every body one key, so
-// each candidate is met once; pairs are pushed for j > i.
+// Each unordered pair is searched from one side only: body i looks at its own cell (for
+// bodies j > i) and at the 13 neighbour cells whose offset (dx, dy, dz) is positive in
+// lexicographic order (for any body j); a pair in two different cells is met from the body
+// whose neighbour offset is positive, exactly once.  Five threads per body, one per cell
+// column: (1, -1), (1, 0), (1, 1) and (0, 1) take dz = -1, 0, 1; (0, 0) takes dz = 0 (j > i)
+// and 1.  In a cell's bucket a body counts only when its cell key is the cell's; the 27
+// neighbour cells have distinct keys and every body one key.  (Cells 2^kCellBits apart
+// share keys; their bodies become extra candidates that the sphere test rejects.)  The
+// pairs pushed, as (min, max) keys, are those of a search of all 27 cells for j > i.
+constexpr int kGridColumns = 5;
+
 __global__ void k_grid_pairs(delta_scene s, Grid g, HashGrid hg, int sh, uint64_t *out, unsigned long long *count,
                              int64_t cap) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 9 * (int64_t)s.n_bodies) return;
-  const int32_t i = (int32_t)(t / 9), col = (int32_t)(t % 9);
+  if (t >= kGridColumns * (int64_t)s.n_bodies) return;
+  const int32_t i = (int32_t)(t / kGridColumns), col = (int32_t)(t % kGridColumns);
   if (s.obstacle[i]) return;
   // the body's cell from the key the count pass stored (coordinates modulo 2^kCellBits,
   // which is all cell_key keeps), instead of three FP64 divisions per thread
   const uint64_t own = hg.cell[i];
   const int64_t c[3] = {(int64_t)((own >> (2 * kCellBits)) & kCellMask), (int64_t)((own >> kCellBits) & kCellMask),
                         (int64_t)(own & kCellMask)};
-  const int64_t cx = c[0] + col / 3 - 1, cy = c[1] + col % 3 - 1;
-  for (int dz = -1; dz <= 1; ++dz) {
+  const int dx = col < 3 ? 1 : 0, dy = col < 3 ? col - 1 : (col == 3 ? 1 : 0);
+  const int dz0 = col == 4 ? 0 : -1;
+  const int64_t cx = c[0] + dx, cy = c[1] + dy;
+  for (int dz = dz0; dz <= 1; ++dz) {
+    const bool same = col == 4 && dz == 0;  // the body's own cell: only j > i
     const uint64_t key = cell_key(cx, cy, c[2] + dz);
     const uint32_t b = cell_bucket(key, hg.nb);
     for (uint32_t q = hg.start[b]; q < hg.start[b + 1]; ++q) {
       const int32_t j = hg.bodies[q];
-      if (j > i && hg.cell[j] == key && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
+      if ((same ? j > i : j != i) && hg.cell[j] == key && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
     }
   }
 }
@@ -1092,7 +1102,7 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
     pk = (uint64_t *)pb + 8;
     if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess) return cuda_error(e, "memset");
     if (plan.n_moving > 0) {
-      k_grid_pairs<<<blocks_for(9 * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, cap);
+      k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, cap);
       ctx->launches += 1;
     }
     if (plan.n_obst > 0) {
@@ -1194,7 +1204,7 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
   size_t tb = temp_bytes;
   kernels += 3;
   if (plan.n_moving > 0) {
-    k_grid_pairs<<<blocks_for(9 * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, pair_cap);
+    k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, pair_cap);
     kernels += 1;
   }
   if (plan.n_obst > 0) {
