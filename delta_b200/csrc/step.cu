@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_sort_unpack_pairs_block(
     const uint64_t *__restrict__ keys, int64_t n, int sh, int32_t *__restrict__ a, int32_t *__restrict__ b,
     const unsigned long long *count, int *ovf, int64_t *total) {
   constexpr int kBlockSortItems = ITEMS;
-  using Sort = cub::BlockRadixSort<uint32_t, kBlockSortThreads, kBlockSortItems>;
+  using Sort = cub::BlockRadixSort<uint32_t, kBlockSortThreads, kBlockSortItems, cub::NullType, 5>;
   __shared__ typename Sort::TempStorage tmp;
   const int t = threadIdx.x;
   if (t == 0) {
