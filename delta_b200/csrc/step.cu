@@ -614,7 +614,6 @@ struct HashGrid {
   uint32_t *start;   // [nb + 1], exclusive sum of count
   int32_t *bodies;   // [n] bodies by bucket
   uint64_t *cell;    // [n] cell key of each moving body
-  uint64_t *ekey;    // [n] cell key of each bucket entry (bodies[q]'s), read beside it
 };
 
 inline int64_t grid_buckets(int32_t n) {
@@ -650,11 +649,8 @@ __global__ void k_grid_count(delta_scene s, Grid g, HashGrid hg, uint64_t *pk, i
 __global__ void k_grid_fill(delta_scene s, HashGrid hg) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n_bodies || s.obstacle[i]) return;
-  const uint64_t key = hg.cell[i];
-  const uint32_t b = cell_bucket(key, hg.nb);
-  const uint32_t q = hg.start[b] + atomicAdd(&hg.fill[b], 1u);
-  hg.bodies[q] = i;
-  hg.ekey[q] = key;
+  const uint32_t b = cell_bucket(hg.cell[i], hg.nb);
+  hg.bodies[hg.start[b] + atomicAdd(&hg.fill[b], 1u)] = i;
 }
 
 __device__ __forceinline__ bool spheres_touch(const delta_scene &s, int32_t i, int32_t j) {
@@ -701,25 +697,13 @@ __global__ void k_grid_pairs(delta_scene s, Grid g, HashGrid hg, int sh, uint64_
   const int dx = col < 3 ? 1 : 0, dy = col < 3 ? col - 1 : (col == 3 ? 1 : 0);
   const int dz0 = col == 4 ? 0 : -1;
   const int64_t cx = c[0] + dx, cy = c[1] + dy;
-  // the column's bucket ranges first (independent loads), then their entries; an entry's
-  // cell key sits beside its body, so neither waits on the other
-  uint64_t key[3];
-  uint32_t q0[3], q1[3];
-#pragma unroll
-  for (int z = 0; z < 3; ++z) {
-    key[z] = cell_key(cx, cy, c[2] + dz0 + z);
-    const uint32_t b = cell_bucket(key[z], hg.nb);
-    const bool live = dz0 + z <= 1;
-    q0[z] = live ? hg.start[b] : 0u;
-    q1[z] = live ? hg.start[b + 1] : 0u;
-  }
-#pragma unroll
-  for (int z = 0; z < 3; ++z) {
-    const bool same = col == 4 && dz0 + z == 0;  // the body's own cell: only j > i
-    for (uint32_t q = q0[z]; q < q1[z]; ++q) {
+  for (int dz = dz0; dz <= 1; ++dz) {
+    const bool same = col == 4 && dz == 0;  // the body's own cell: only j > i
+    const uint64_t key = cell_key(cx, cy, c[2] + dz);
+    const uint32_t b = cell_bucket(key, hg.nb);
+    for (uint32_t q = hg.start[b]; q < hg.start[b + 1]; ++q) {
       const int32_t j = hg.bodies[q];
-      if (hg.ekey[q] == key[z] && (same ? j > i : j != i) && spheres_touch(s, i, j))
-        push_pair(i, j, sh, out, count, cap);
+      if ((same ? j > i : j != i) && hg.cell[j] == key && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
     }
   }
 }
@@ -1065,14 +1049,12 @@ static char *carve_grid(char *base, int32_t n, HashGrid &hg) {
   hg.bodies = (int32_t *)b;
   b = align(b + 4 * (size_t)n);
   hg.cell = (uint64_t *)b;
-  b = align(b + 8 * (size_t)n);
-  hg.ekey = (uint64_t *)b;
   return align(b + 8 * (size_t)n);
 }
 
 static size_t grid_bytes(int32_t n) {
   const size_t nb = (size_t)grid_buckets(n);
-  return 6 * 256 + 4 * (2 * nb + 1) + 4 * (nb + 1) + 20 * (size_t)n;
+  return 5 * 256 + 4 * (2 * nb + 1) + 4 * (nb + 1) + 12 * (size_t)n;
 }
 
 // count, scan, fill: the hash grid of the moving bodies (count and fill zeroed first)
