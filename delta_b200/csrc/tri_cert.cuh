@@ -30,7 +30,9 @@ namespace delta {
 constexpr float kU32 = 5.9604644775390625e-08f;  // 2^-24
 constexpr double kU64 = 1.1102230246251565e-16;  // 2^-53
 
-__device__ __forceinline__ float clamp01(float x) { return fminf(fmaxf(x, 0.f), 1.f); }
+// Clamp to [0, 1] in the producing instruction (.sat), NaN to 0: a clamped parameter only
+// has to be a feasible point of its segment or triangle for the bounds below to hold.
+__device__ __forceinline__ float clamp01(float x) { return __saturatef(x); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
 // FP32 edge-edge: clamped closest parameters (segment P(s)=TA+s*u, Q(t)=TB+t*v), the
@@ -49,7 +51,7 @@ __device__ __forceinline__ float seg_seg_lb(const float *HA, const float *TA, co
   float s = den > 1e-12f * (a * e) ? clamp01(fdiv(fmaf(b, f, -c * e), den)) : 0.f;
   const float traw = e > 0.f ? fdiv(fmaf(b, s, f), e) : 0.f;
   const float t = clamp01(traw);
-  const float s2 = a > 0.f ? clamp01(fdiv(fmaf(b, t, -c), a)) : 0.f;
+  const float s2 = clamp01(fdiv(fmaf(b, t, -c), a));  // a = 0: u = 0, c = 0, 0/0 -> 0
   s = (traw != t) ? s2 : s;
   float r[3];
 #pragma unroll
@@ -84,10 +86,11 @@ __device__ __forceinline__ float pt_tri_lb(const float *V0, const float *V1, con
   auto q = [&](float s, float t) {
     return fmaf(s, fmaf(a, s, fmaf(2.f * b, t, 2.f * d)), fmaf(t, fmaf(c, t, 2.f * e), f));
   };
-  const float s0 = a > 0.f ? clamp01(fdiv(-d, a)) : 0.f;  // edge t = 0
-  const float t1 = c > 0.f ? clamp01(fdiv(-e, c)) : 0.f;  // edge s = 0
+  // degenerate edges give 0/0, which clamp01 sends to 0; any value in [0, 1] is feasible
+  const float s0 = clamp01(fdiv(-d, a));  // edge t = 0
+  const float t1 = clamp01(fdiv(-e, c));  // edge s = 0
   const float den2 = a - 2.f * b + c;
-  const float l2 = den2 > 0.f ? clamp01(fdiv(c + e - b - d, den2)) : 0.f;  // edge s + t = 1: s = l2
+  const float l2 = clamp01(fdiv(c + e - b - d, den2));  // edge s + t = 1: s = l2
   float s = s0, t = 0.f, best = q(s0, 0.f);
   const float q1 = q(0.f, t1), q2 = q(l2, 1.f - l2);
   if (q1 < best) { best = q1; s = 0.f; t = t1; }

@@ -24,10 +24,13 @@ __device__ __forceinline__ float closest_on_tri(const float *V0, const float *E0
   const float si = fmaf(b, e, -c * d) * idet, ti = fmaf(b, d, -a * e) * idet;
   // squared distance at (s, t) minus |D|^2
   auto q = [&](float u, float v) { return fmaf(u, fmaf(a, u, fmaf(2.f * b, v, 2.f * d)), v * fmaf(c, v, 2.f * e)); };
-  const float s0 = a > 0.f ? fminf(fmaxf(__fdividef(-d, a), 0.f), 1.f) : 0.f;  // edge t = 0
-  const float t1 = c > 0.f ? fminf(fmaxf(__fdividef(-e, c), 0.f), 1.f) : 0.f;  // edge s = 0
+  // clamped edge parameters: __saturatef clamps to [0, 1] in the multiply itself and sends
+  // NaN to 0, which is the degenerate edge's 0/0 (a = 0 forces d = 0, and so on), so no
+  // guard is needed
+  const float s0 = __saturatef(__fdividef(-d, a));  // edge t = 0
+  const float t1 = __saturatef(__fdividef(-e, c));  // edge s = 0
   const float den = a - 2.f * b + c;
-  const float l2 = den > 0.f ? fminf(fmaxf(__fdividef(c + e - b - d, den), 0.f), 1.f) : 0.f;  // edge s + t = 1
+  const float l2 = __saturatef(__fdividef(c + e - b - d, den));  // edge s + t = 1
   float best = q(s0, 0.f);
   s = s0;
   t = 0.f;
@@ -67,10 +70,10 @@ __device__ __forceinline__ float seg_seg_dist32(const float *HA, const float *TA
   }
   const float a = dot3(u, u), e = dot3(v, v), b = dot3(u, v), c = dot3(u, w), f = dot3(v, w);
   const float den = fmaf(a, e, -b * b);
-  float s = den > 1e-12f * (a * e) ? fminf(fmaxf(__fdividef(fmaf(b, f, -c * e), den), 0.f), 1.f) : 0.f;
+  float s = den > 1e-12f * (a * e) ? __saturatef(__fdividef(fmaf(b, f, -c * e), den)) : 0.f;
   const float traw = e > 0.f ? __fdividef(fmaf(b, s, f), e) : 0.f;
-  const float t = fminf(fmaxf(traw, 0.f), 1.f);
-  const float s2 = a > 0.f ? fminf(fmaxf(__fdividef(fmaf(b, t, -c), a), 0.f), 1.f) : 0.f;
+  const float t = __saturatef(traw);
+  const float s2 = __saturatef(__fdividef(fmaf(b, t, -c), a));  // a = 0: 0/0 -> 0
   s = traw != t ? s2 : s;
   float r2 = 0.f;
 #pragma unroll
