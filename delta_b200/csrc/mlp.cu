@@ -1171,10 +1171,8 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
         if (dj < de || (dj == de && 3 * xa + xb < 3 * ea + eb)) { de = dj; ea = xa; eb = xb; }
       }
     } else {
-      pick_vertex(Af, ea, HA);
-      pick_vertex(Af, (ea + 1) % 3, TA);
-      pick_vertex(Bf, eb, HB);
-      pick_vertex(Bf, (eb + 1) % 3, TB);
+      other_two(Af, kA, HA, TA);  // edge ea of A
+      other_two(Bf, kB, HB, TB);  // edge eb of B
       de = seg_seg_dist32(HA, TA, HB, TB);
     }
     edge0 = dpt > de;

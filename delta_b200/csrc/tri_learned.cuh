@@ -31,10 +31,11 @@ __device__ __forceinline__ float closest_on_tri(const float *V0, const float *E0
   const float t1 = __saturatef(__fdividef(-e, c));  // edge s = 0
   const float den = a - 2.f * b + c;
   const float l2 = __saturatef(__fdividef(c + e - b - d, den));  // edge s + t = 1
-  float best = q(s0, 0.f);
+  // q on the edges t = 0 and s = 0 without the vanishing terms
+  float best = s0 * fmaf(a, s0, 2.f * d);
   s = s0;
   t = 0.f;
-  const float q1 = q(0.f, t1), q2 = q(l2, 1.f - l2);
+  const float q1 = t1 * fmaf(c, t1, 2.f * e), q2 = q(l2, 1.f - l2);
   if (q1 < best) { best = q1; s = 0.f; t = t1; }
   if (q2 < best) { best = q2; s = l2; t = 1.f - l2; }
   if (si >= 0.f && ti >= 0.f && si + ti <= 1.f) { s = si; t = ti; best = q(si, ti); }
@@ -82,6 +83,17 @@ __device__ __forceinline__ float seg_seg_dist32(const float *HA, const float *TA
     r2 = fmaf(r, r, r2);
   }
   return sqrtf(r2);
+}
+
+// The two vertices of T other than vertex k (the edge opposite it, joining k+1 and k+2),
+// in an order of no consequence to the FP32 edge-edge distance, with one select per
+// coordinate each.
+__device__ __forceinline__ void other_two(const float T[3][3], int k, float P[3], float Q[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    P[c] = k == 0 ? T[1][c] : T[0][c];
+    Q[c] = k == 2 ? T[1][c] : T[2][c];
+  }
 }
 
 // First index of the largest / smallest of three values.
@@ -140,10 +152,8 @@ __device__ __forceinline__ bool learned_pair_solve(const double A[3][3], const d
   const bool faceB = d2 < d1;
   const int vtx = faceB ? iA : jB;
   const float dpt = faceB ? d2 : d1;
-  pick_vertex(Af, ea, HA);
-  pick_vertex(Af, (ea + 1) % 3, TA);
-  pick_vertex(Bf, eb, HB);
-  pick_vertex(Bf, (eb + 1) % 3, TB);
+  other_two(Af, kA, HA, TA);  // edge ea of A
+  other_two(Bf, kB, HB, TB);  // edge eb of B
   const float de = seg_seg_dist32(HA, TA, HB, TB);
   xf64 A64[3][3], B64[3][3], pq[6];
 #pragma unroll
