@@ -82,17 +82,16 @@ __device__ __forceinline__ float pt_tri_lb(const float *V0, const float *V1, con
   const float idet = fdiv(1.f, det);
   const float si = fmaf(b, e, -c * d) * idet, ti = fmaf(b, d, -a * e) * idet;
   const bool inside = si >= 0.f && ti >= 0.f && si + ti <= 1.f;
-  // squared distance of parameter (s,t): |D + s E0 + t E1|^2 = f + 2(s d + t e) + s^2 a + 2 s t b + t^2 c
-  auto q = [&](float s, float t) {
-    return fmaf(s, fmaf(a, s, fmaf(2.f * b, t, 2.f * d)), fmaf(t, fmaf(c, t, 2.f * e), f));
-  };
+  // squared distance of parameter (s,t) less f: |D + s E0 + t E1|^2 - f
+  //   = 2(s d + t e) + s^2 a + 2 s t b + t^2 c (it only ranks the three edge points)
+  auto q = [&](float s, float t) { return fmaf(s, fmaf(a, s, fmaf(2.f * b, t, 2.f * d)), t * fmaf(c, t, 2.f * e)); };
   // degenerate edges give 0/0, which clamp01 sends to 0; any value in [0, 1] is feasible
   const float s0 = clamp01(fdiv(-d, a));  // edge t = 0
   const float t1 = clamp01(fdiv(-e, c));  // edge s = 0
   const float den2 = a - 2.f * b + c;
   const float l2 = clamp01(fdiv(c + e - b - d, den2));  // edge s + t = 1: s = l2
-  float s = s0, t = 0.f, best = q(s0, 0.f);
-  const float q1 = q(0.f, t1), q2 = q(l2, 1.f - l2);
+  float s = s0, t = 0.f, best = s0 * fmaf(a, s0, 2.f * d);  // q(s0, 0)
+  const float q1 = t1 * fmaf(c, t1, 2.f * e), q2 = q(l2, 1.f - l2);  // q(0, t1), q(l2, 1 - l2)
   if (q1 < best) { best = q1; s = 0.f; t = t1; }
   if (q2 < best) { best = q2; s = l2; t = 1.f - l2; }
   if (inside) { s = si; t = ti; }
