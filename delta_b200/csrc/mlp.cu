@@ -1098,22 +1098,15 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
       if (st > 1.f) { s /= st; t /= st; }
       if (uw > 1.f) { u /= uw; w /= uw; }
     }
-    if (sweeps > 0) {
-      float EA0[3], EA1[3], EB0[3], EB1[3];
-      for (int k = 0; k < 3; ++k) {
-        EA0[k] = Af[1][k] - Af[0][k];
-        EA1[k] = Af[2][k] - Af[0][k];
-        EB0[k] = Bf[1][k] - Bf[0][k];
-        EB1[k] = Bf[2][k] - Bf[0][k];
-      }
-      for (int it = 0; it < sweeps; ++it) {
-        float P[3];
-        for (int k = 0; k < 3; ++k) P[k] = Af[0][k] + s * EA0[k] + t * EA1[k];
-        closest_on_tri(Bf[0], EB0, EB1, P, u, w);
-        float Q[3];
-        for (int k = 0; k < 3; ++k) Q[k] = Bf[0][k] + u * EB0[k] + w * EB1[k];
-        closest_on_tri(Af[0], EA0, EA1, Q, s, t);
-      }
+    // each triangle's constants once, for the sweeps and the vertex-face distances
+    const TriFrame FA = tri_frame(Af), FB = tri_frame(Bf);
+    for (int it = 0; it < sweeps; ++it) {
+      float P[3];
+      for (int k = 0; k < 3; ++k) P[k] = Af[0][k] + s * FA.e0[k] + t * FA.e1[k];
+      closest_on_frame(Bf[0], FB, P, u, w);
+      float Q[3];
+      for (int k = 0; k < 3; ++k) Q[k] = Bf[0][k] + u * FB.e0[k] + w * FB.e1[k];
+      closest_on_frame(Af[0], FA, Q, s, t);
     }
     // features read off the barycentric weights lA = (1-s-t, s, t), lB = (1-u-w, u, w)
     const int iA = argmax3(1.f - s - t, s, t), jB = argmax3(1.f - u - w, u, w);
@@ -1131,8 +1124,8 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
       float X1[3], X2[3];
       pick_vertex(Bf, jB, X1);
       pick_vertex(Af, iA, X2);
-      const float d1 = pt_tri_dist32(Af[0], Af[1], Af[2], X1);
-      const float d2 = pt_tri_dist32(Bf[0], Bf[1], Bf[2], X2);
+      const float d1 = pt_dist_frame(Af[0], FA, X1);
+      const float d2 = pt_dist_frame(Bf[0], FB, X2);
       faceB = d2 < d1;
       vtx = faceB ? iA : jB;
       dpt = faceB ? d2 : d1;
@@ -1143,7 +1136,7 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
       vtx = 0;
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
-        const float dj = j < 3 ? pt_tri_dist32(Af[0], Af[1], Af[2], Bf[j]) : pt_tri_dist32(Bf[0], Bf[1], Bf[2], Af[j - 3]);
+        const float dj = j < 3 ? pt_dist_frame(Af[0], FA, Bf[j]) : pt_dist_frame(Bf[0], FB, Af[j - 3]);
         if (dj < dpt) { dpt = dj; faceB = j >= 3; vtx = j % 3; }
       }
     }

@@ -10,51 +10,66 @@
 
 namespace delta {
 
-// Closest point of triangle (V0, V0+E0, V0+E1) to X in FP32, branch-free: the interior
-// solution of the 2x2 normal equations when it lies inside, otherwise the nearest of the
-// three edges' clamped projections (all computed, one selected), so the lanes of a warp
-// never diverge.  Barycentric (s, t); returns the squared distance less |V0-X|^2.
-__device__ __forceinline__ float closest_on_tri(const float *V0, const float *E0, const float *E1, const float *X,
-                                                float &s, float &t) {
+// The per-triangle constants of closest_on_frame (edges, Gram entries and the reciprocals of
+// the four divisions), formed once for the sweeps and the vertex-face distances that
+// project onto the same triangle.
+struct TriFrame {
+  float e0[3], e1[3];
+  float a, b, c, idet, ra, rc, rden;
+};
+
+__device__ __forceinline__ TriFrame tri_frame(const float V[3][3]) {
+  TriFrame F;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    F.e0[k] = V[1][k] - V[0][k];
+    F.e1[k] = V[2][k] - V[0][k];
+  }
+  F.a = dot3(F.e0, F.e0);
+  F.b = dot3(F.e0, F.e1);
+  F.c = dot3(F.e1, F.e1);
+  F.idet = __fdividef(1.f, fmaf(F.a, F.c, -F.b * F.b));
+  F.ra = __fdividef(1.f, F.a);
+  F.rc = __fdividef(1.f, F.c);
+  F.rden = __fdividef(1.f, F.a - 2.f * F.b + F.c);
+  return F;
+}
+
+// Closest point of the triangle of frame F (first vertex V0; edges e0, e1) to X in FP32,
+// branch-free: the interior solution of the 2x2 normal equations when it lies inside,
+// otherwise the nearest of the three edges' clamped projections (all computed, one
+// selected), so the lanes of a warp never diverge.  Barycentric (s, t).  The clamps are
+// saturations, which send a degenerate edge's 0 * inf = NaN to 0 (a = 0 forces d = 0, and
+// so on), so no guard is needed; the edge points are ranked by the squared distance less
+// |V0 - X|^2.
+__device__ __forceinline__ void closest_on_frame(const float *V0, const TriFrame &F, const float *X, float &s,
+                                                 float &t) {
   float D[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) D[k] = V0[k] - X[k];
-  const float a = dot3(E0, E0), b = dot3(E0, E1), c = dot3(E1, E1), d = dot3(E0, D), e = dot3(E1, D);
-  const float idet = __fdividef(1.f, fmaf(a, c, -b * b));
-  const float si = fmaf(b, e, -c * d) * idet, ti = fmaf(b, d, -a * e) * idet;
-  // squared distance at (s, t) minus |D|^2
+  const float a = F.a, b = F.b, c = F.c, d = dot3(F.e0, D), e = dot3(F.e1, D);
+  const float si = fmaf(b, e, -c * d) * F.idet, ti = fmaf(b, d, -a * e) * F.idet;
   auto q = [&](float u, float v) { return fmaf(u, fmaf(a, u, fmaf(2.f * b, v, 2.f * d)), v * fmaf(c, v, 2.f * e)); };
-  // clamped edge parameters: __saturatef clamps to [0, 1] in the multiply itself and sends
-  // NaN to 0, which is the degenerate edge's 0/0 (a = 0 forces d = 0, and so on), so no
-  // guard is needed
-  const float s0 = __saturatef(__fdividef(-d, a));  // edge t = 0
-  const float t1 = __saturatef(__fdividef(-e, c));  // edge s = 0
-  const float den = a - 2.f * b + c;
-  const float l2 = __saturatef(__fdividef(c + e - b - d, den));  // edge s + t = 1
-  // q on the edges t = 0 and s = 0 without the vanishing terms
+  const float s0 = __saturatef(-d * F.ra);               // edge t = 0
+  const float t1 = __saturatef(-e * F.rc);               // edge s = 0
+  const float l2 = __saturatef((c + e - b - d) * F.rden);  // edge s + t = 1
   float best = s0 * fmaf(a, s0, 2.f * d);
   s = s0;
   t = 0.f;
   const float q1 = t1 * fmaf(c, t1, 2.f * e), q2 = q(l2, 1.f - l2);
   if (q1 < best) { best = q1; s = 0.f; t = t1; }
-  if (q2 < best) { best = q2; s = l2; t = 1.f - l2; }
-  if (si >= 0.f && ti >= 0.f && si + ti <= 1.f) { s = si; t = ti; best = q(si, ti); }
-  return best;
+  if (q2 < best) { s = l2; t = 1.f - l2; }
+  if (si >= 0.f && ti >= 0.f && si + ti <= 1.f) { s = si; t = ti; }
 }
 
-// FP32 distance of vertex-face pair (X, triangle V0 V1 V2), branch-free.
-__device__ __forceinline__ float pt_tri_dist32(const float *V0, const float *V1, const float *V2, const float *X) {
-  float E0[3], E1[3], s, t;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    E0[k] = V1[k] - V0[k];
-    E1[k] = V2[k] - V0[k];
-  }
-  closest_on_tri(V0, E0, E1, X, s, t);
+// FP32 distance of vertex-face pair (X, the triangle of frame F with first vertex V0).
+__device__ __forceinline__ float pt_dist_frame(const float *V0, const TriFrame &F, const float *X) {
+  float s, t;
+  closest_on_frame(V0, F, X, s, t);
   float r2 = 0.f;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    const float r = fmaf(s, E0[k], fmaf(t, E1[k], V0[k] - X[k]));
+    const float r = fmaf(s, F.e0[k], fmaf(t, F.e1[k], V0[k] - X[k]));
     r2 = fmaf(r, r, r2);
   }
   return sqrtf(r2);
@@ -122,24 +137,15 @@ __device__ __forceinline__ bool learned_pair_solve(const double A[3][3], const d
       Bf[v][k] = (float)(B[v][k] - A[0][k]);
     }
   float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
-  if (sweeps > 0) {
-    float EA0[3], EA1[3], EB0[3], EB1[3];
+  const TriFrame FA = tri_frame(Af), FB = tri_frame(Bf);
+  for (int it = 0; it < sweeps; ++it) {
+    float P[3], Q[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      EA0[k] = Af[1][k] - Af[0][k];
-      EA1[k] = Af[2][k] - Af[0][k];
-      EB0[k] = Bf[1][k] - Bf[0][k];
-      EB1[k] = Bf[2][k] - Bf[0][k];
-    }
-    for (int it = 0; it < sweeps; ++it) {
-      float P[3], Q[3];
+    for (int k = 0; k < 3; ++k) P[k] = Af[0][k] + s * FA.e0[k] + t * FA.e1[k];
+    closest_on_frame(Bf[0], FB, P, u, w);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) P[k] = Af[0][k] + s * EA0[k] + t * EA1[k];
-      closest_on_tri(Bf[0], EB0, EB1, P, u, w);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) Q[k] = Bf[0][k] + u * EB0[k] + w * EB1[k];
-      closest_on_tri(Af[0], EA0, EA1, Q, s, t);
-    }
+    for (int k = 0; k < 3; ++k) Q[k] = Bf[0][k] + u * FB.e0[k] + w * FB.e1[k];
+    closest_on_frame(Af[0], FA, Q, s, t);
   }
   const int iA = argmax3(1.f - s - t, s, t), jB = argmax3(1.f - u - w, u, w);
   const int kA = argmin3(1.f - s - t, s, t), kB = argmin3(1.f - u - w, u, w);
@@ -147,8 +153,8 @@ __device__ __forceinline__ bool learned_pair_solve(const double A[3][3], const d
   float X1[3], X2[3], HA[3], TA[3], HB[3], TB[3];
   pick_vertex(Bf, jB, X1);
   pick_vertex(Af, iA, X2);
-  const float d1 = pt_tri_dist32(Af[0], Af[1], Af[2], X1);
-  const float d2 = pt_tri_dist32(Bf[0], Bf[1], Bf[2], X2);
+  const float d1 = pt_dist_frame(Af[0], FA, X1);
+  const float d2 = pt_dist_frame(Bf[0], FB, X2);
   const bool faceB = d2 < d1;
   const int vtx = faceB ? iA : jB;
   const float dpt = faceB ? d2 : d1;
