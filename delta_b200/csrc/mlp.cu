@@ -1085,7 +1085,8 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
       for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          Af[v][k] = (float)(__ldg(a + (3 * v + k) * ld + ii) - A0[k]);
+          // A0 is the origin (a non-finite A0 fails the FP64 certificate all the same)
+          Af[v][k] = v == 0 ? 0.f : (float)(__ldg(a + (3 * v + k) * ld + ii) - A0[k]);
           Bf[v][k] = (float)(__ldg(b + (3 * v + k) * ld + ii) - A0[k]);
         }
     }
@@ -1119,13 +1120,13 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
     float HA[3], TA[3], HB[3], TB[3];
     bool faceB;  // chosen vertex-face feature: A's vertex vtx on face B, else B's vertex vtx on face A
     int vtx;
-    float dpt, de;
+    float dpt, de;  // squared FP32 distances of the picked vertex-face and edge features
     if constexpr (CAND == 3) {
       float X1[3], X2[3];
       pick_vertex(Bf, jB, X1);
       pick_vertex(Af, iA, X2);
-      const float d1 = pt_dist_frame(Af[0], FA, X1);
-      const float d2 = pt_dist_frame(Bf[0], FB, X2);
+      const float d1 = pt_dist2_frame(Af[0], FA, X1);
+      const float d2 = pt_dist2_frame(Bf[0], FB, X2);
       faceB = d2 < d1;
       vtx = faceB ? iA : jB;
       dpt = faceB ? d2 : d1;
@@ -1136,7 +1137,7 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
       vtx = 0;
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
-        const float dj = j < 3 ? pt_dist_frame(Af[0], FA, Bf[j]) : pt_dist_frame(Bf[0], FB, Af[j - 3]);
+        const float dj = j < 3 ? pt_dist2_frame(Af[0], FA, Bf[j]) : pt_dist2_frame(Bf[0], FB, Af[j - 3]);
         if (dj < dpt) { dpt = dj; faceB = j >= 3; vtx = j % 3; }
       }
     }
@@ -1145,7 +1146,7 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
       de = 1e30f;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
-        const float dj = seg_seg_dist32(Af[j / 3], Af[(j / 3 + 1) % 3], Bf[j % 3], Bf[(j % 3 + 1) % 3]);
+        const float dj = seg_seg_dist2_32(Af[j / 3], Af[(j / 3 + 1) % 3], Bf[j % 3], Bf[(j % 3 + 1) % 3]);
         if (dj < de) { de = dj; ea = j / 3; eb = j % 3; }
       }
     } else if constexpr (CAND == 11) {
@@ -1160,13 +1161,13 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
         pick_vertex(Af, (xa + 1) % 3, TA);
         pick_vertex(Bf, xb, HB);
         pick_vertex(Bf, (xb + 1) % 3, TB);
-        const float dj = seg_seg_dist32(HA, TA, HB, TB);
+        const float dj = seg_seg_dist2_32(HA, TA, HB, TB);
         if (dj < de || (dj == de && 3 * xa + xb < 3 * ea + eb)) { de = dj; ea = xa; eb = xb; }
       }
     } else {
       other_two(Af, kA, HA, TA);  // edge ea of A
       other_two(Bf, kB, HB, TB);  // edge eb of B
-      de = seg_seg_dist32(HA, TA, HB, TB);
+      de = seg_seg_dist2_32(HA, TA, HB, TB);
     }
     edge0 = dpt > de;
     code0 = edge0 ? (unsigned)(ea | (eb << 2)) : (unsigned)(vtx | (faceB ? 4 : 0));

@@ -62,8 +62,9 @@ __device__ __forceinline__ void closest_on_frame(const float *V0, const TriFrame
   if (si >= 0.f && ti >= 0.f && si + ti <= 1.f) { s = si; t = ti; }
 }
 
-// FP32 distance of vertex-face pair (X, the triangle of frame F with first vertex V0).
-__device__ __forceinline__ float pt_dist_frame(const float *V0, const TriFrame &F, const float *X) {
+// FP32 squared distance of vertex-face pair (X, the triangle of frame F with first vertex
+// V0); the callers only rank distances, and the square ranks them alike.
+__device__ __forceinline__ float pt_dist2_frame(const float *V0, const TriFrame &F, const float *X) {
   float s, t;
   closest_on_frame(V0, F, X, s, t);
   float r2 = 0.f;
@@ -72,11 +73,13 @@ __device__ __forceinline__ float pt_dist_frame(const float *V0, const TriFrame &
     const float r = fmaf(s, F.e0[k], fmaf(t, F.e1[k], V0[k] - X[k]));
     r2 = fmaf(r, r, r2);
   }
-  return sqrtf(r2);
+  return r2;
 }
 
-// FP32 distance of edge pair (TA->HA, TB->HB): clamped closest parameters, branch-free.
-__device__ __forceinline__ float seg_seg_dist32(const float *HA, const float *TA, const float *HB, const float *TB) {
+// FP32 squared distance of edge pair (TA->HA, TB->HB): clamped closest parameters,
+// branch-free.
+__device__ __forceinline__ float seg_seg_dist2_32(const float *HA, const float *TA, const float *HB,
+                                                  const float *TB) {
   float u[3], v[3], w[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -97,7 +100,7 @@ __device__ __forceinline__ float seg_seg_dist32(const float *HA, const float *TA
     const float r = fmaf(s, u[k], fmaf(-t, v[k], w[k]));
     r2 = fmaf(r, r, r2);
   }
-  return sqrtf(r2);
+  return r2;
 }
 
 // The two vertices of T other than vertex k (the edge opposite it, joining k+1 and k+2),
@@ -133,7 +136,7 @@ __device__ __forceinline__ bool learned_pair_solve(const double A[3][3], const d
   for (int v = 0; v < 3; ++v)
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      Af[v][k] = (float)(A[v][k] - A[0][k]);
+      Af[v][k] = v == 0 ? 0.f : (float)(A[v][k] - A[0][k]);  // A0 is the origin
       Bf[v][k] = (float)(B[v][k] - A[0][k]);
     }
   float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
@@ -153,14 +156,14 @@ __device__ __forceinline__ bool learned_pair_solve(const double A[3][3], const d
   float X1[3], X2[3], HA[3], TA[3], HB[3], TB[3];
   pick_vertex(Bf, jB, X1);
   pick_vertex(Af, iA, X2);
-  const float d1 = pt_dist_frame(Af[0], FA, X1);
-  const float d2 = pt_dist_frame(Bf[0], FB, X2);
+  const float d1 = pt_dist2_frame(Af[0], FA, X1);
+  const float d2 = pt_dist2_frame(Bf[0], FB, X2);
   const bool faceB = d2 < d1;
   const int vtx = faceB ? iA : jB;
   const float dpt = faceB ? d2 : d1;
   other_two(Af, kA, HA, TA);  // edge ea of A
   other_two(Bf, kB, HB, TB);  // edge eb of B
-  const float de = seg_seg_dist32(HA, TA, HB, TB);
+  const float de = seg_seg_dist2_32(HA, TA, HB, TB);
   xf64 A64[3][3], B64[3][3], pq[6];
 #pragma unroll
   for (int v = 0; v < 3; ++v)
