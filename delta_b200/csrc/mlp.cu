@@ -1031,14 +1031,6 @@ __global__ void k_penalty_warm(int64_t n, const double *a, const double *b, int6
   iters[i] = (uint8_t)it;
 }
 
-// A second load of a value read before (an asm load, so the compiler does not keep the
-// first one alive in registers instead).
-__device__ __forceinline__ double ld_again(const double *p) {
-  double v;
-  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
-  return v;
-}
-
 // Learned hybrid solver, one pair per thread.  From the warm start x0 (barycentric
 // weights of P on A and Q on B; centroids when x0 is null), `sweeps` FP32 alternating
 // projections (Q <- closest point of B to P, P <- closest point of A to Q) locate the
@@ -1071,23 +1063,27 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
   const bool valid0 = i0 < n;
   bool edge0;      // the chosen feature is an edge pair
   unsigned code0;  // edge pair: ea | eb << 2; vertex-face: vtx | faceB << 2
+  // the block's FP64 coordinates, kept in shared memory for the FP64 stage (which takes
+  // the block's pairs in another order) instead of in registers through the FP32 search:
+  // [plane 3 * vertex + coordinate][pair of the block]
+  __shared__ double s_a[9][128], s_b[9][128];
   {
     const int64_t ii = valid0 ? i0 : n - 1;
-    // FP32 copies relative to A0 (the distance is translation invariant); the FP64 values
-    // are loaded again for the FP64 stage (from L1/L2), so they are not held in registers
-    // through the FP32 search
+    // FP32 copies relative to A0 (the distance is translation invariant)
     float Af[3][3], Bf[3][3];
     {
       double A0[3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) A0[k] = __ldg(a + k * ld + ii);
-#pragma unroll
       for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
+          const double xa = __ldg(a + (3 * v + k) * ld + ii), xb = __ldg(b + (3 * v + k) * ld + ii);
+          s_a[3 * v + k][threadIdx.x] = xa;
+          s_b[3 * v + k][threadIdx.x] = xb;
+          if (v == 0) A0[k] = xa;
           // A0 is the origin (a non-finite A0 fails the FP64 certificate all the same)
-          Af[v][k] = v == 0 ? 0.f : (float)(__ldg(a + (3 * v + k) * ld + ii) - A0[k]);
-          Bf[v][k] = (float)(__ldg(b + (3 * v + k) * ld + ii) - A0[k]);
+          Af[v][k] = v == 0 ? 0.f : (float)(xa - A0[k]);
+          Bf[v][k] = (float)(xb - A0[k]);
         }
     }
     float s = 1.f / 3.f, t = 1.f / 3.f, u = 1.f / 3.f, w = 1.f / 3.f;
@@ -1203,23 +1199,24 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
   // threads past the block's pairs (last block only) repeat item 0 and write nothing
   const bool has = tid < nE + nV;
   const unsigned item = s_item[has ? tid : 0];
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + (item & 127), ii = i;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + (item & 127);
   const bool edge = (item & 128u) != 0;
   const int ea = (item >> 8) & 3, eb = (item >> 10) & 3, vtx = (item >> 8) & 3;
   const bool faceB = ((item >> 10) & 1) != 0;
-  // FP64 stage: only the chosen feature's vertices are loaded (again), then the six
-  // vertices stream through the certificate one at a time
-  auto vtx64 = [&](const double *T, int v, xf64 out[3]) {
+  // FP64 stage: only the chosen feature's vertices are read (from the block's shared
+  // copies), then the six vertices stream through the certificate one at a time
+  const int it = (int)(item & 127);  // the pair's slot in the block's shared copies
+  auto vtx64 = [&](const double (*T)[128], int v, xf64 out[3]) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) out[k] = xf64(ld_again(T + (3 * v + k) * ld + ii));
+    for (int k = 0; k < 3; ++k) out[k] = xf64(T[3 * v + k][it]);
   };
   xf64 pq[6];
   if (edge) {
     xf64 HA[3], TA[3], HB[3], TB[3], sc, tc;
-    vtx64(a, ea, HA);
-    vtx64(a, (ea + 1) % 3, TA);
-    vtx64(b, eb, HB);
-    vtx64(b, (eb + 1) % 3, TB);
+    vtx64(s_a, ea, HA);
+    vtx64(s_a, (ea + 1) % 3, TA);
+    vtx64(s_b, eb, HB);
+    vtx64(s_b, (eb + 1) % 3, TB);
     seg_seg_ref(HA, TA, HB, TB, sc, tc);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {  // bf.cpp:715-879 (seg_seg_points)
@@ -1228,7 +1225,8 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
     }
   } else {
     // face of A with B's vertex vtx, or face of B with A's vertex vtx
-    const double *face = faceB ? b : a, *pnt = faceB ? a : b;
+    const double(*face)[128] = faceB ? s_b : s_a;
+    const double(*pnt)[128] = faceB ? s_a : s_b;
     xf64 T0[3], T1[3], T2[3], X[3], sf, tf;
     vtx64(face, 0, T0);
     vtx64(face, 1, T1);
@@ -1250,8 +1248,8 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
       xf64 VA[3], VB[3];
-      vtx64(a, v, VA);
-      vtx64(b, v, VB);
+      vtx64(s_a, v, VA);
+      vtx64(s_b, v, VB);
       amin = fmin(amin, VA[0].v * r[0] + VA[1].v * r[1] + VA[2].v * r[2]);
       bmax = fmax(bmax, VB[0].v * r[0] + VB[1].v * r[1] + VB[2].v * r[2]);
 #pragma unroll
@@ -1287,8 +1285,8 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
       // the pair's coordinates, compact at its list position, for the exact solver
 #pragma unroll
       for (int c = 0; c < 9; ++c) {
-        stage[c * (int64_t)n + slot] = ld_again(a + c * ld + i0);
-        stage[(9 + c) * (int64_t)n + slot] = ld_again(b + c * ld + i0);
+        stage[c * (int64_t)n + slot] = s_a[c][tid];
+        stage[(9 + c) * (int64_t)n + slot] = s_b[c][tid];
       }
     }
   }
