@@ -35,23 +35,63 @@ constexpr double kU64 = 1.1102230246251565e-16;  // 2^-53
 __device__ __forceinline__ float clamp01(float x) { return __saturatef(x); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
-// FP32 edge-edge: clamped closest parameters (segment P(s)=TA+s*u, Q(t)=TB+t*v), the
-// distance of that point pair and its Frank-Wolfe lower bound.  Returns d, writes lb.
-__device__ __forceinline__ float seg_seg_lb(const float *HA, const float *TA, const float *HB, const float *TB,
-                                            float &lb) {
-  float u[3], v[3], w[3];
+// The per-triangle constants of an FP32 point-triangle projection (edges from vertex 0,
+// Gram entries, the reciprocals of the four divisions), formed once per triangle for all
+// the points projected onto it.
+struct TriFrame {
+  float e0[3], e1[3];
+  float a, b, c, idet, ra, rc, rden;
+};
+
+__device__ __forceinline__ TriFrame tri_frame(const float V[3][3]) {
+  TriFrame F;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    u[k] = HA[k] - TA[k];
-    v[k] = HB[k] - TB[k];
-    w[k] = TA[k] - TB[k];
+    F.e0[k] = V[1][k] - V[0][k];
+    F.e1[k] = V[2][k] - V[0][k];
   }
-  const float a = dot3(u, u), e = dot3(v, v), b = dot3(u, v), c = dot3(u, w), f = dot3(v, w);
+  F.a = dot3(F.e0, F.e0);
+  F.b = dot3(F.e0, F.e1);
+  F.c = dot3(F.e1, F.e1);
+  F.idet = __fdividef(1.f, fmaf(F.a, F.c, -F.b * F.b));
+  F.ra = __fdividef(1.f, F.a);
+  F.rc = __fdividef(1.f, F.c);
+  F.rden = __fdividef(1.f, F.a - 2.f * F.b + F.c);
+  return F;
+}
+
+// The per-edge constants of the FP32 edge-edge bound: the edge from its tail to its head,
+// its squared length and the reciprocal of that, formed once per edge for the three edge
+// pairs it is in.
+struct EdgeFrame {
+  float u[3];
+  float a, ra;
+};
+
+__device__ __forceinline__ EdgeFrame edge_frame(const float *H, const float *T) {
+  EdgeFrame E;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) E.u[k] = H[k] - T[k];
+  E.a = dot3(E.u, E.u);
+  E.ra = fdiv(1.f, E.a);
+  return E;
+}
+
+// FP32 edge-edge: clamped closest parameters (segment P(s)=TA+s*u, Q(t)=TB+t*v, with u and
+// v the edges of U and V), the distance of that point pair and its Frank-Wolfe lower bound.
+// Returns d, writes lb.
+__device__ __forceinline__ float seg_seg_lb(const float *TA, const EdgeFrame &U, const float *TB,
+                                            const EdgeFrame &V, float &lb) {
+  const float *u = U.u, *v = V.u;
+  float w[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) w[k] = TA[k] - TB[k];
+  const float a = U.a, e = V.a, b = dot3(u, v), c = dot3(u, w), f = dot3(v, w);
   const float den = fmaf(a, e, -b * b);
   float s = den > 1e-12f * (a * e) ? clamp01(fdiv(fmaf(b, f, -c * e), den)) : 0.f;
-  const float traw = e > 0.f ? fdiv(fmaf(b, s, f), e) : 0.f;
+  const float traw = e > 0.f ? fmaf(b, s, f) * V.ra : 0.f;
   const float t = clamp01(traw);
-  const float s2 = clamp01(fdiv(fmaf(b, t, -c), a));  // a = 0: u = 0, c = 0, 0/0 -> 0
+  const float s2 = clamp01(fmaf(b, t, -c) * U.ra);  // a = 0: u = 0, c = 0, 0 * inf -> 0
   s = (traw != t) ? s2 : s;
   float r[3];
 #pragma unroll
@@ -68,28 +108,21 @@ __device__ __forceinline__ float seg_seg_lb(const float *HA, const float *TA, co
 // FP32 vertex-face: closest point of triangle (V0,V1,V2) to X chosen among the interior
 // projection (when inside) and the three edges, its distance, and the Frank-Wolfe lower
 // bound with the reference's quadratic-form error removed.  Returns d, writes lb.
-__device__ __forceinline__ float pt_tri_lb(const float *V0, const float *V1, const float *V2, const float *X, float eps,
-                                           float &lb) {
-  float E0[3], E1[3], D[3];
+__device__ __forceinline__ float pt_tri_lb(const float *V0, const TriFrame &F, const float *X, float eps, float &lb) {
+  const float *E0 = F.e0, *E1 = F.e1;
+  float D[3];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    E0[k] = V1[k] - V0[k];
-    E1[k] = V2[k] - V0[k];
-    D[k] = V0[k] - X[k];
-  }
-  const float a = dot3(E0, E0), b = dot3(E0, E1), c = dot3(E1, E1), d = dot3(E0, D), e = dot3(E1, D), f = dot3(D, D);
-  const float det = fmaf(a, c, -b * b);
-  const float idet = fdiv(1.f, det);
-  const float si = fmaf(b, e, -c * d) * idet, ti = fmaf(b, d, -a * e) * idet;
+  for (int k = 0; k < 3; ++k) D[k] = V0[k] - X[k];
+  const float a = F.a, b = F.b, c = F.c, d = dot3(E0, D), e = dot3(E1, D), f = dot3(D, D);
+  const float si = fmaf(b, e, -c * d) * F.idet, ti = fmaf(b, d, -a * e) * F.idet;
   const bool inside = si >= 0.f && ti >= 0.f && si + ti <= 1.f;
   // squared distance of parameter (s,t) less f: |D + s E0 + t E1|^2 - f
   //   = 2(s d + t e) + s^2 a + 2 s t b + t^2 c (it only ranks the three edge points)
   auto q = [&](float s, float t) { return fmaf(s, fmaf(a, s, fmaf(2.f * b, t, 2.f * d)), t * fmaf(c, t, 2.f * e)); };
   // degenerate edges give 0/0, which clamp01 sends to 0; any value in [0, 1] is feasible
-  const float s0 = clamp01(fdiv(-d, a));  // edge t = 0
-  const float t1 = clamp01(fdiv(-e, c));  // edge s = 0
-  const float den2 = a - 2.f * b + c;
-  const float l2 = clamp01(fdiv(c + e - b - d, den2));  // edge s + t = 1: s = l2
+  const float s0 = clamp01(-d * F.ra);  // edge t = 0
+  const float t1 = clamp01(-e * F.rc);  // edge s = 0
+  const float l2 = clamp01((c + e - b - d) * F.rden);  // edge s + t = 1: s = l2
   float s = s0, t = 0.f, best = s0 * fmaf(a, s0, 2.f * d);  // q(s0, 0)
   const float q1 = t1 * fmaf(c, t1, 2.f * e), q2 = q(l2, 1.f - l2);  // q(0, t1), q(l2, 1 - l2)
   if (q1 < best) { best = q1; s = 0.f; t = t1; }
@@ -296,7 +329,7 @@ __device__ __forceinline__ int bf_cert_warp(const double A64[3][3], const double
     double lo = A64[0][k], hi = A64[0][k];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-      A[v][k] = (float)(A64[v][k] - A64[0][k]);
+      A[v][k] = v == 0 ? 0.f : (float)(A64[v][k] - A64[0][k]);  // A's vertex 0 is the origin
       B[v][k] = (float)(B64[v][k] - A64[0][k]);
       lo = fmin(lo, fmin(A64[v][k], B64[v][k]));
       hi = fmax(hi, fmax(A64[v][k], B64[v][k]));
@@ -307,19 +340,32 @@ __device__ __forceinline__ int bf_cert_warp(const double A64[3][3], const double
   float lb[15];
   int sbest = 0, pbest = 0;
   float sd = 3.0e38f, pd = 3.0e38f;
+  {
+    // edge j of a triangle runs from vertex j+1 (tail) to vertex j (head); each edge is
+    // in three edge pairs
+    EdgeFrame EA[3], EB[3];
 #pragma unroll
-  for (int j = 0; j < 9; ++j) {
-    float l;
-    const float d = seg_seg_lb(A[j / 3], A[(j / 3 + 1) % 3], B[j % 3], B[(j % 3 + 1) % 3], l);
-    lb[j] = l - eps;
-    if (d < sd) { sd = d; sbest = j; }
+    for (int j = 0; j < 3; ++j) {
+      EA[j] = edge_frame(A[j], A[(j + 1) % 3]);
+      EB[j] = edge_frame(B[j], B[(j + 1) % 3]);
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      float l;
+      const float d = seg_seg_lb(A[(j / 3 + 1) % 3], EA[j / 3], B[(j % 3 + 1) % 3], EB[j % 3], l);
+      lb[j] = l - eps;
+      if (d < sd) { sd = d; sbest = j; }
+    }
   }
+  {
+    const TriFrame FA = tri_frame(A), FB = tri_frame(B);
 #pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    float d = pt_tri_lb(A[0], A[1], A[2], B[j], eps, lb[9 + j]);
-    if (d < pd) { pd = d; pbest = j; }
-    d = pt_tri_lb(B[0], B[1], B[2], A[j], eps, lb[12 + j]);
-    if (d < pd) { pd = d; pbest = 3 + j; }
+    for (int j = 0; j < 3; ++j) {
+      float d = pt_tri_lb(A[0], FA, B[j], eps, lb[9 + j]);
+      if (d < pd) { pd = d; pbest = j; }
+      d = pt_tri_lb(B[0], FB, A[j], eps, lb[12 + j]);
+      if (d < pd) { pd = d; pbest = 3 + j; }
+    }
   }
   __syncwarp();
   // ---- 2. FP64 values of each family's FP32 argmin (every lane runs both paths) --------

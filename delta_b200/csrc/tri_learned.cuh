@@ -10,31 +10,6 @@
 
 namespace delta {
 
-// The per-triangle constants of closest_on_frame (edges, Gram entries and the reciprocals of
-// the four divisions), formed once for the sweeps and the vertex-face distances that
-// project onto the same triangle.
-struct TriFrame {
-  float e0[3], e1[3];
-  float a, b, c, idet, ra, rc, rden;
-};
-
-__device__ __forceinline__ TriFrame tri_frame(const float V[3][3]) {
-  TriFrame F;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    F.e0[k] = V[1][k] - V[0][k];
-    F.e1[k] = V[2][k] - V[0][k];
-  }
-  F.a = dot3(F.e0, F.e0);
-  F.b = dot3(F.e0, F.e1);
-  F.c = dot3(F.e1, F.e1);
-  F.idet = __fdividef(1.f, fmaf(F.a, F.c, -F.b * F.b));
-  F.ra = __fdividef(1.f, F.a);
-  F.rc = __fdividef(1.f, F.c);
-  F.rden = __fdividef(1.f, F.a - 2.f * F.b + F.c);
-  return F;
-}
-
 // Closest point of the triangle of frame F (first vertex V0; edges e0, e1) to X in FP32,
 // branch-free: the interior solution of the 2x2 normal equations when it lies inside,
 // otherwise the nearest of the three edges' clamped projections (all computed, one
