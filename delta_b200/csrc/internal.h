@@ -33,8 +33,17 @@ inline PairLaunch default_pair_launch(int method) {
 }
 // The largest threads per block the pair kernel of (method, precision) takes (pairs.cu).
 int pair_max_threads(int method, int precision);
+// Position of coordinate c (0..17: a's 9, then b's 9) of list entry j in the exact
+// solver's staging buffer: tiles of 32 entries, each tile 18 rows of 32 doubles, so one
+// warp's 32 consecutive entries read one contiguous 4.6 KB tile (rather than 18 planes a
+// power-of-two stride apart). A buffer for m entries holds kStageCoords * round_up(m, 32).
+constexpr int kStageCoords = 18;
+__host__ __device__ __forceinline__ int64_t stage_at(int64_t j, int c) {
+  return ((j >> 5) * kStageCoords + c) * 32 + (j & 31);
+}
+inline size_t stage_doubles(int64_t m) { return (size_t)kStageCoords * (size_t)((m + 31) & ~(int64_t)31); }
 // DELTA_BF_CERT over pairs idx[0 .. *count) (count read on the device, at most max_count);
-// with `stage`, the coordinates of entry j come from stage's 18 planes of max_count.
+// with `stage`, the coordinates of entry j come from stage[stage_at(j, c)].
 cudaError_t launch_cert_indexed(cudaStream_t s, const uint32_t *count, int64_t max_count, const uint32_t *idx,
                                 const double *a, const double *b, int64_t ld, double *p, double *q, double *dist,
                                 PairLaunch cfg, const double *stage = nullptr);

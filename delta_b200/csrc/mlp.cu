@@ -1047,9 +1047,9 @@ __global__ void k_penalty_warm(int64_t n, const double *a, const double *b, int6
 // |r|^2 - (min_i r.A_i - max_j r.B_j) + slack |r| <= rel_tol |r|^2, i.e. the distance is
 // within rel_tol of the true one; slack = 1e-14 max|coordinate| covers the rounding of the
 // dot products.  Intersecting triangles have no separating plane and are never certified.
-// With `list`, uncertified pairs are appended to list[*count] (aggregated over the lanes
-// that reach the append together; with `stage`, their 18 coordinates too, as planes of n
-// at the list position) and their
+// With `list`, uncertified pairs are appended to list[*count] (one atomicAdd per block,
+// in pair order within the block; with `stage`, their 18 coordinates too, at
+// stage_at(list position, c)) and their
 // outputs left for the exact solver; flags then read 1 (certified) or 2 (listed).
 template <int CAND>
 __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const double *__restrict__ a,
@@ -1267,26 +1267,34 @@ __global__ void __launch_bounds__(128, 8) k_learned_refine(int64_t n, const doub
   }
   if (has && flags) flags[i] = list ? (ok ? 1 : 2) : (ok ? 1 : 0);
   if (!list) return;
-  // The uncertified pairs are appended by their own threads, in pair order, so the list
-  // (and the exact solver's reads and writes through it) keeps the pairs' order.
+  // The uncertified pairs are appended by their own threads, in pair order within the
+  // block, so the list (and the exact solver's reads and writes through it) keeps the
+  // pairs' order block by block. One atomicAdd per block on the shared counter: appends
+  // from every warp to one address serialise in L2 (the counter's slice may sit on the
+  // other die), which cost up to a fifth of the pipeline's time.
   __shared__ uint8_t s_bad[128];
+  __shared__ uint32_t s_wcount[4], s_base;
   if (has) s_bad[item & 127] = ok ? 0 : 1;
   __syncthreads();
-  if (valid0 && s_bad[tid]) {
-    // append, aggregated over the lanes that arrive here together
-    const unsigned grp = __activemask();
-    const int leader = __ffs(grp) - 1;
-    unsigned base = 0;
-    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(grp));
-    base = __shfl_sync(grp, base, leader);
-    const uint32_t slot = base + __popc(grp & lt);
+  const bool bad = valid0 && s_bad[tid];
+  const unsigned bad_mask = __ballot_sync(0xffffffffu, bad);
+  if (lane == 0) s_wcount[wid] = __popc(bad_mask);
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t total = s_wcount[0] + s_wcount[1] + s_wcount[2] + s_wcount[3];
+    s_base = total ? atomicAdd(count, total) : 0u;
+  }
+  __syncthreads();
+  if (bad) {
+    uint32_t slot = s_base + __popc(bad_mask & lt);
+    for (int w = 0; w < wid; ++w) slot += s_wcount[w];
     list[slot] = (uint32_t)i0;
     if (stage) {
       // the pair's coordinates, compact at its list position, for the exact solver
 #pragma unroll
       for (int c = 0; c < 9; ++c) {
-        stage[c * (int64_t)n + slot] = s_a[c][tid];
-        stage[(9 + c) * (int64_t)n + slot] = s_b[c][tid];
+        stage[stage_at(slot, c)] = s_a[c][tid];
+        stage[stage_at(slot, 9 + c)] = s_b[c][tid];
       }
     }
   }
@@ -1394,9 +1402,9 @@ delta_status learned_enqueue(delta_ctx *ctx, int64_t n, const double *a, const d
   if ((st = ctx_scratch(ctx, 14, 256 + sizeof(uint32_t) * (size_t)n, &lbuf)) != DELTA_OK) return st;
   uint32_t *count = static_cast<uint32_t *>(lbuf);
   uint32_t *list = reinterpret_cast<uint32_t *>(static_cast<char *>(lbuf) + 256);
-  // compact copies of the uncertified pairs (18 planes of n doubles) for the exact solver
+  // compact copies of the uncertified pairs' coordinates (tiles of 32) for the exact solver
   void *sbuf;
-  if ((st = ctx_scratch(ctx, 25, sizeof(double) * 18 * (size_t)n, &sbuf)) != DELTA_OK) return st;
+  if ((st = ctx_scratch(ctx, 25, sizeof(double) * stage_doubles(n), &sbuf)) != DELTA_OK) return st;
   double *stage = static_cast<double *>(sbuf);
   cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), ctx->stream);
   if (e != cudaSuccess) return cuda_error(e, "learned pipeline: memset");

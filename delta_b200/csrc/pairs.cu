@@ -118,14 +118,14 @@ __global__ void __launch_bounds__(32 * W) k_pairs_cert(int64_t n, const double *
 // The certified kernel over an index list: pairs idx[0 .. *count) of the pair list (the
 // count is read on the device, so the list can be built by an earlier kernel on the
 // stream without a host round trip).  With `stage`, entry j's coordinates are read from
-// stage (18 planes of sld doubles: a's 9 planes, then b's) at position j instead of being
+// stage[stage_at(j, c)] (a's 9, then b's; one contiguous tile per warp) instead of being
 // gathered from a and b; results go to pair idx[j] of p, q, dist.
 template <int W>
 __global__ void __launch_bounds__(32 * W) k_pairs_cert_indexed(const uint32_t *__restrict__ count,
                                                                const uint32_t *__restrict__ idx,
                                                                const double *__restrict__ a,
                                                                const double *__restrict__ b, int64_t ld,
-                                                               const double *__restrict__ stage, int64_t sld,
+                                                               const double *__restrict__ stage,
                                                                double *__restrict__ p, double *__restrict__ q,
                                                                double *__restrict__ dist) {
   __shared__ CertWarpSmem sm[W];
@@ -141,8 +141,8 @@ __global__ void __launch_bounds__(32 * W) k_pairs_cert_indexed(const uint32_t *_
     for (int v = 0; v < 3; ++v)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        A[v][k] = stage ? __ldg(stage + (3 * v + k) * sld + j) : __ldg(a + (3 * v + k) * ld + i);
-        B[v][k] = stage ? __ldg(stage + (9 + 3 * v + k) * sld + j) : __ldg(b + (3 * v + k) * ld + i);
+        A[v][k] = stage ? __ldg(stage + stage_at(j, 3 * v + k)) : __ldg(a + (3 * v + k) * ld + i);
+        B[v][k] = stage ? __ldg(stage + stage_at(j, 9 + 3 * v + k)) : __ldg(b + (3 * v + k) * ld + i);
       }
     double out[6];
     bf_cert_warp(A, B, valid, out, sm[warp]);
@@ -228,8 +228,7 @@ cudaError_t launch_cert_indexed(cudaStream_t s, const uint32_t *count, int64_t m
   const int64_t per = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 8;
   const int64_t cap = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1) * per;
   if (blocks > cap) blocks = cap;
-  k_pairs_cert_indexed<4><<<(unsigned)(blocks > 0 ? blocks : 1), 128, 0, s>>>(count, idx, a, b, ld, stage, max_count,
-                                                                              p, q, dist);
+  k_pairs_cert_indexed<4><<<(unsigned)(blocks > 0 ? blocks : 1), 128, 0, s>>>(count, idx, a, b, ld, stage, p, q, dist);
   return cudaGetLastError();
 }
 
