@@ -727,47 +727,102 @@ __global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const doubl
   if (d2 <= reach * reach) push_pair(L, j, sh, out, count, cap);
 }
 
-// The fixed-capacity pair list of a scene with at most 2^16 bodies and at most
-// kBlockSortCap entries, sorted and unpacked by one CTA (cub's block radix sort of 32-bit
-// keys over the 2 sh key bits) instead of a device-wide radix sort (a histogram and one
-// launch per 8-bit digit) and an unpacking kernel: one graph node instead of six.  The
-// result, the overflow flag and the pair total are k_unpack_pairs's.
+// The fixed-capacity pair list of at most kBlockSortCap entries, sorted and unpacked by
+// one CTA (cub's block radix sort over the 2 sh key bits: 32-bit keys up to 2^16 bodies,
+// 64-bit keys above) instead of a device-wide radix sort (a histogram and one launch per
+// digit) and an unpacking kernel: one graph node instead of six.  The result, the
+// overflow flag and the pair total are k_unpack_pairs's.
 constexpr int kBlockSortThreads = 512, kBlockSortItems = 16;
 constexpr int64_t kBlockSortCap = (int64_t)kBlockSortThreads * kBlockSortItems;
 
-// ITEMS keys per thread: the smallest of 2, 4, 8, 16 whose 512 * ITEMS covers the list
-// (a block sort of a short list pays for every padded key: one sized to 8,192 keys made
-// the 256-body lattice's step 6% slower than cub's device sort)
-template <int ITEMS>
-__global__ void __launch_bounds__(kBlockSortThreads) k_sort_unpack_pairs_block(
-    const uint64_t *__restrict__ keys, int64_t n, int sh, int32_t *__restrict__ a, int32_t *__restrict__ b,
-    const unsigned long long *count, int *ovf, int64_t *total) {
-  constexpr int kBlockSortItems = ITEMS;
-  using Sort = cub::BlockRadixSort<uint32_t, kBlockSortThreads, kBlockSortItems, cub::NullType, 5>;
-  __shared__ typename Sort::TempStorage tmp;
+template <class K, int ITEMS>
+using PairBlockSort = cub::BlockRadixSort<K, kBlockSortThreads, ITEMS, cub::NullType, 5>;
+
+// Shared memory of the block sort of up to MAXI keys per thread (the largest variant's).
+template <class K, int MAXI>
+constexpr size_t block_sort_smem() {
+  return sizeof(typename PairBlockSort<K, MAXI>::TempStorage) > sizeof(typename PairBlockSort<K, 2>::TempStorage)
+             ? sizeof(typename PairBlockSort<K, MAXI>::TempStorage)
+             : sizeof(typename PairBlockSort<K, 2>::TempStorage);
+}
+
+// Sorts keys[0 .. m) (m <= 512 * ITEMS) and unpacks them to a, b; entries [m, cap) are
+// empty (-1, -1), as the padding keys of a sort over the whole capacity would leave them.
+template <class K, int ITEMS>
+__device__ __forceinline__ void sort_unpack_items(unsigned char *smem, const uint64_t *__restrict__ keys, int64_t m,
+                                                  int64_t cap, int sh, int32_t *__restrict__ a,
+                                                  int32_t *__restrict__ b) {
+  auto &tmp = *reinterpret_cast<typename PairBlockSort<K, ITEMS>::TempStorage *>(smem);
   const int t = threadIdx.x;
-  if (t == 0) {
-    const unsigned long long c = *count;
-    if (c > (unsigned long long)n) atomicCAS(ovf, 0, 1);
-    if (total) *total += (int64_t)(c < (unsigned long long)n ? c : (unsigned long long)n);
-  }
-  uint32_t k[kBlockSortItems];
+  K k[ITEMS];
 #pragma unroll
-  for (int j = 0; j < kBlockSortItems; ++j) {
-    const int64_t i = (int64_t)t * kBlockSortItems + j;
-    // a valid key has a < b < 2^sh, so it is never 0xffffffff, the empty key's low half
-    k[j] = i < n ? (uint32_t)keys[i] : 0xffffffffu;
+  for (int j = 0; j < ITEMS; ++j) {
+    const int64_t i = (int64_t)t * ITEMS + j;
+    // a valid key has a < b < 2^sh, so its 2 sh bits are never all set: the padding
+    // key ~0 sorts last
+    k[j] = i < m ? (K)keys[i] : ~(K)0;
   }
-  Sort(tmp).Sort(k, 0, 2 * sh);
+  PairBlockSort<K, ITEMS>(tmp).Sort(k, 0, 2 * sh);
+  const K low = ((K)1 << sh) - (K)1;
 #pragma unroll
-  for (int j = 0; j < kBlockSortItems; ++j) {
-    const int64_t i = (int64_t)t * kBlockSortItems + j;
-    if (i < n) {
-      const bool empty = k[j] == 0xffffffffu;
-      a[i] = empty ? -1 : (int32_t)(k[j] >> sh);
-      b[i] = empty ? -1 : (int32_t)(k[j] & ((1u << sh) - 1u));
+  for (int j = 0; j < ITEMS; ++j) {
+    const int64_t i = (int64_t)t * ITEMS + j;
+    if (i < m) {
+      a[i] = (int32_t)(k[j] >> sh);
+      b[i] = (int32_t)(k[j] & low);
     }
   }
+  for (int64_t i = m + t; i < cap; i += kBlockSortThreads) a[i] = b[i] = -1;
+}
+
+// The pair list's block sort, sized at run time to the step's pair count (the smallest
+// of 2, 4, 8, 16 keys per thread that holds it, at most MAXI): a sort sized to the
+// capacity pays for every padded key (8,192 keys for the hopper's 2,860 pairs).
+template <class K, int MAXI>
+__global__ void __launch_bounds__(kBlockSortThreads) k_sort_unpack_pairs_block(
+    const uint64_t *__restrict__ keys, int64_t cap, int sh, int32_t *__restrict__ a, int32_t *__restrict__ b,
+    const unsigned long long *count, int *ovf, int64_t *total) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const unsigned long long c = *count;
+  if (threadIdx.x == 0) {
+    if (c > (unsigned long long)cap) atomicCAS(ovf, 0, 1);
+    if (total) *total += (int64_t)(c < (unsigned long long)cap ? c : (unsigned long long)cap);
+  }
+  const int64_t m = c < (unsigned long long)cap ? (int64_t)c : cap;
+  constexpr int T = kBlockSortThreads;
+  if (m <= 2 * T) sort_unpack_items<K, 2>(smem, keys, m, cap, sh, a, b);
+  else if (m <= 4 * T) sort_unpack_items<K, (MAXI < 4 ? MAXI : 4)>(smem, keys, m, cap, sh, a, b);
+  else if (m <= 8 * T) sort_unpack_items<K, (MAXI < 8 ? MAXI : 8)>(smem, keys, m, cap, sh, a, b);
+  else sort_unpack_items<K, MAXI>(smem, keys, m, cap, sh, a, b);
+}
+
+template <class K, int MAXI>
+static cudaError_t block_sort_attr() {
+  return cudaFuncSetAttribute(k_sort_unpack_pairs_block<K, MAXI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)block_sort_smem<K, MAXI>());
+}
+
+// Raises the dynamic shared memory limit of the block sorts that need more than the
+// default 48 KB (called before a capture, outside it).
+static cudaError_t block_sort_prepare() {
+  cudaError_t e;
+  if ((e = block_sort_attr<uint32_t, 16>()) != cudaSuccess) return e;
+  if ((e = block_sort_attr<uint64_t, 8>()) != cudaSuccess) return e;
+  return block_sort_attr<uint64_t, 16>();
+}
+
+template <class K>
+static void launch_block_sort(cudaStream_t st, const uint64_t *pk, int64_t cap, int sh, int32_t *pa, int32_t *pb,
+                              const unsigned long long *count, int *ovf, int64_t *total) {
+  constexpr int64_t T = kBlockSortThreads;
+  if (cap <= 2 * T)
+    k_sort_unpack_pairs_block<K, 2><<<1, T, block_sort_smem<K, 2>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
+  else if (cap <= 4 * T)
+    k_sort_unpack_pairs_block<K, 4><<<1, T, block_sort_smem<K, 4>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
+  else if (cap <= 8 * T)
+    k_sort_unpack_pairs_block<K, 8><<<1, T, block_sort_smem<K, 8>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
+  else
+    k_sort_unpack_pairs_block<K, 16><<<1, T, block_sort_smem<K, 16>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
 }
 
 // pair keys back to (a, b); the empty key ~0 gives (-1, -1).  With `count` (fixed
@@ -902,20 +957,24 @@ delta_status forces_run(delta_ctx *ctx, const delta_scene &s, const delta_contac
     return DELTA_OK;
   }
   ContactView cv{c.x, c.normal, c.depth, c.master, c.slave, c.friction, c.capacity};
-  // scratch: head flags, segment starts, segment count, entries (2 per segment)
+  // scratch: segment count, segment starts (nc), entry keys and sorted keys, entry
+  // indices and sorted indices (2 nc each: two entries per segment), entries (2 nc x 6
+  // doubles), head flags (nc bytes); the size is the sum of the same terms
   const size_t nc = (size_t)n_contacts;
+  const size_t off_seg = 64, off_key = off_seg + 8 * nc, off_skey = off_key + 16 * nc, off_idx = off_skey + 16 * nc,
+               off_sidx = off_idx + 16 * nc, off_entry = off_sidx + 16 * nc, off_head = off_entry + 96 * nc,
+               bytes = off_head + nc;
   void *buf = nullptr;
-  const size_t bytes = nc * (1 + 8 + 8 * 2 + 8 * 2 + 8 * 2 + 6 * 8 * 2) + 64;
   if ((ds = ctx_scratch(ctx, 7, bytes, &buf)) != DELTA_OK) return ds;
   char *b = (char *)buf;
-  int64_t *n_seg = (int64_t *)b; b += 64;
-  int64_t *seg_start = (int64_t *)b; b += 8 * nc;
-  uint64_t *key = (uint64_t *)b; b += 8 * 2 * nc;
-  uint64_t *skey = (uint64_t *)b; b += 8 * 2 * nc;
-  int64_t *idx = (int64_t *)b; b += 8 * 2 * nc;
-  int64_t *sidx = (int64_t *)b; b += 8 * 2 * nc;  // (fits: bytes above counts 8*2 for idx and sidx each)
-  double *entry = (double *)b; b += 6 * 8 * 2 * nc;
-  uint8_t *head = (uint8_t *)b;
+  int64_t *n_seg = (int64_t *)b;
+  int64_t *seg_start = (int64_t *)(b + off_seg);
+  uint64_t *key = (uint64_t *)(b + off_key);
+  uint64_t *skey = (uint64_t *)(b + off_skey);
+  int64_t *idx = (int64_t *)(b + off_idx);
+  int64_t *sidx = (int64_t *)(b + off_sidx);
+  double *entry = (double *)(b + off_entry);
+  uint8_t *head = (uint8_t *)(b + off_head);
   k_segment_heads<<<blocks_for(n_contacts), 256, 0, st>>>(cv, n_contacts, head);
   ctx->launches += 1;
   // segment starts: indices where head == 1
@@ -1212,16 +1271,9 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
                                                                           sh, pk, count, pair_cap);
     kernels += 1;
   }
-  if (2 * sh <= 32 && pair_cap <= kBlockSortCap) {
-    const int64_t T = kBlockSortThreads;
-    if (pair_cap <= 2 * T)
-      k_sort_unpack_pairs_block<2><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
-    else if (pair_cap <= 4 * T)
-      k_sort_unpack_pairs_block<4><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
-    else if (pair_cap <= 8 * T)
-      k_sort_unpack_pairs_block<8><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
-    else
-      k_sort_unpack_pairs_block<16><<<1, T, 0, st>>>(pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
+  if (pair_cap <= kBlockSortCap) {
+    if (2 * sh <= 32) launch_block_sort<uint32_t>(st, pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
+    else launch_block_sort<uint64_t>(st, pk, pair_cap, sh, pair_a, pair_b, count, ovf, pairs_total);
     kernels += 1;
     return cuda_error(cudaGetLastError(), "broadphase fixed");
   }
@@ -1440,6 +1492,7 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
   g.d_bp = (int64_t *)(v + 40);
   g.d_log = (int64_t *)(v + 256);
   if ((e = cudaMemset(g.dev, 0, 256)) != cudaSuccess) return cuda_error(e, "graph memset");
+  if ((e = block_sort_prepare()) != cudaSuccess) return cuda_error(e, "pair sort attributes");
   delta_status ds = detect_fixed_init(s->ctx->stream, g.ds, pair_cap, contact_cap);
   if (ds != DELTA_OK) return ds;
   if ((e = cudaStreamSynchronize(s->ctx->stream)) != cudaSuccess) return cuda_error(e, "graph init");

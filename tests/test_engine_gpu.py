@@ -379,7 +379,7 @@ def _fixture(name):
 
 @pytest.mark.parametrize("case,driver,graph", [("lattice", 0, False), ("lattice", 8, True), ("hopper", 0, False),
                                                ("hopper", 8, True), ("hopper", 9, True), ("hopper", 10, True)])
-def test_full_length_runs_equal_the_reference(ctx, hopper, case, driver, graph):
+def test_full_length_runs_equal_the_reference(hopper, case, driver, graph):
     """Two configurations at their full length against the reference's own time step
     (tests/golden/make_timestep_golden.py: the reference's bf(), getContactsForces with
     forces.cpp's compiled constants, and dynamics.cpp's updates, run on the host): the
@@ -387,8 +387,12 @@ def test_full_length_runs_equal_the_reference(ctx, hopper, case, driver, graph):
     contacts of every step and every state array after the last step (SHA-256 of the
     bytes) equal the reference's, for the plain FP64 driver and for the culled drivers
     replayed as a CUDA graph.  The learned driver (FP32 hybrid) matches the contact
-    counts but is not bit-exact: its trajectory stays within 1e-9 m of the reference's."""
+    counts but is not bit-exact: its trajectory stays within 1e-9 m of the reference's.
+    Each run has a context of its own, as a user's first simulation does: its scratch
+    buffers grow with the contact count during the run (a context whose buffers earlier
+    tests had grown once hid a scratch layout larger than its allocation)."""
     from delta_b200.engine import Simulation, StepParams
+    from delta_b200.narrowphase import Context
     from delta_b200.scenarios import lattice_scene
 
     fx = _fixture("timestep_lattice_1000.json" if case == "lattice" else "timestep_hopper_2000.json")
@@ -396,10 +400,14 @@ def test_full_length_runs_equal_the_reference(ctx, hopper, case, driver, graph):
     m = fx["material"]
     prm = StepParams.make(dt=fx["dt"], gravity=tuple(fx["gravity"]), spring=m["spring"], damper=m["damper"],
                           friction=m["friction"])
-    sim = Simulation(ctx, scene, driver)
-    cps = sim.step(fx["steps"], prm, graph=graph)
-    st = sim.state()
-    sim.close()
+    own = Context(0)
+    try:
+        sim = Simulation(own, scene, driver)
+        cps = sim.step(fx["steps"], prm, graph=graph)
+        st = sim.state()
+        sim.close()
+    finally:
+        own.close()
     if driver == 10:
         assert np.abs(np.asarray(st["pos"][:24]) - np.asarray(fx["pos_first_bodies"])).max() < 1e-9
         return
@@ -407,19 +415,22 @@ def test_full_length_runs_equal_the_reference(ctx, hopper, case, driver, graph):
     assert _digests(st) == fx["sha256"]
 
 
-def test_graph_sort_and_scan_paths_agree(ctx):
-    """The graph step sorts a candidate list of at most 8,192 entries in one CTA and
-    prefix-sums count arrays of at most 8,192 entries in one CTA; longer ones go to cub's
-    device-wide sort and scan.  A 40,000-particle box (its body and bucket arrays are
-    longer than 8,192) replayed with the default pair capacity and with one above 8,192
-    gives the stepped trajectory and contacts bit for bit."""
+@pytest.mark.parametrize("bodies", [40000, 70000])
+def test_graph_sort_and_scan_paths_agree(ctx, bodies):
+    """The graph step sorts a candidate list of at most 8,192 entries in one CTA (32-bit
+    keys up to 2^16 bodies, 64-bit keys above; sized at run time to the step's pair
+    count) and prefix-sums count arrays of at most 8,192 entries in one CTA; longer ones
+    go to cub's device-wide sort and scan.  A box of 40,000 or 70,000 particles (its body
+    and bucket arrays are longer than 8,192) replayed with the default pair capacity, with
+    8,000 (the largest block sort, mostly padding) and with one above 8,192 gives the
+    stepped trajectory and contacts bit for bit."""
     from delta_b200.engine import Simulation, StepParams
     from delta_b200.scenarios import box_scene
 
-    scene = box_scene(40000, seed=11)
+    scene = box_scene(bodies, seed=11)
     prm = StepParams.make(dt=2e-6, gravity=(0.0, -9.81, 0.0), spring=1e6, damper=0.1, friction=0.0)
     runs = []
-    for graph, cap in ((False, None), (True, None), (True, 9000)):
+    for graph, cap in ((False, None), (True, None), (True, 8000), (True, 9000)):
         sim = Simulation(ctx, scene, 8)
         if cap:
             sim.set_graph_capacity(cap, 1 << 16)
