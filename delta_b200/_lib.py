@@ -41,6 +41,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "delta_sim_step": ([vp, vp, i32, vp], C.c_int),
     "delta_sim_step_graph": ([vp, vp, i32, vp], C.c_int),
     "delta_sim_set_graph_capacity": ([vp, i64, i64], C.c_int),
+    "delta_sim_skin_stats": ([vp, vp, vp, vp], C.c_int),
     "delta_sim_contacts": ([vp, vp, vp], C.c_int),
     "delta_sim_counters": ([vp, vp], C.c_int),
     "delta_set_cull_launch": ([vp, i32, i32], C.c_int),

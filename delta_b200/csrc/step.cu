@@ -164,12 +164,24 @@ __device__ __forceinline__ void contact_terms(const ContactView &cv, int64_t c, 
   Tc[2] = arm[0] * (f[1]) - arm[1] * (f[0]);
 }
 
-__global__ void k_step_end(const int *ovf_snap, const int64_t *n_contacts, int64_t *log, int64_t log_len,
-                           int64_t *step) {
-  if (*ovf_snap) return;
-  const int64_t k = *step;
-  if (k < log_len) log[k] = *n_contacts;
-  *step = k + 1;
+// Last kernel of a graph step.  A step that integrated (no overflow before it) is counted
+// and logged; its counters (pend: candidate pairs, triangle pairs, solved pairs, summed
+// during the step) go to the running totals only if no overflow arose in it either: the
+// host repeats an overflowing step's detection, with its counters, outside the graph, and
+// the replays queued after it are frozen.  pend is cleared for the next step.
+__global__ void k_step_end(const int *ovf_snap, const int *ovf, const int64_t *n_contacts, int64_t *log,
+                           int64_t log_len, int64_t *step, int64_t *pend, int64_t *pairs_total, int64_t *counters) {
+  if (!*ovf_snap) {
+    const int64_t k = *step;
+    if (k < log_len) log[k] = *n_contacts;
+    *step = k + 1;
+    if (!*ovf) {
+      *pairs_total += pend[0];
+      counters[0] += pend[1];
+      counters[1] += pend[2];
+    }
+  }
+  pend[0] = pend[1] = pend[2] = 0;
 }
 
 __global__ void k_segment_heads(ContactView cv, int64_t n, uint8_t *head) {
@@ -590,6 +602,9 @@ struct Grid {
   double origin[3];
 };
 
+// The skin list's margin as a fraction of a grid cell (skin = cell / kSkinPerCell).
+constexpr double kSkinPerCell = 32.0;
+
 // Hash grid of the moving bodies.  A cell is keyed by its coordinates modulo 2^21
 // (cells that far apart share a key; their bodies become extra candidates that
 // spheres_touch rejects) and lives in bucket hash(key) & (nb - 1), nb a power of two.
@@ -653,15 +668,41 @@ __global__ void k_grid_fill(delta_scene s, HashGrid hg) {
   hg.bodies[hg.start[b] + atomicAdd(&hg.fill[b], 1u)] = i;
 }
 
-__device__ __forceinline__ bool spheres_touch(const delta_scene &s, int32_t i, int32_t j) {
+// The candidate test of two moving bodies: their bounding spheres, grown by both eps,
+// overlap.  With skin > 0 the reach is widened by skin (the skin list's build test); with
+// skin 0 it is the step's test exactly.  The pair is taken in index order, so the
+// rounding of the sums is the same whichever body the search starts from.
+__device__ __forceinline__ bool spheres_within(const delta_scene &s, int32_t i0, int32_t j0, double skin) {
   const int32_t n = s.n_bodies;
+  const int32_t i = i0 < j0 ? i0 : j0, j = i0 < j0 ? j0 : i0;
   double d2 = 0.0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const double d = s.pos[(int64_t)k * n + j] - s.pos[(int64_t)k * n + i];
     d2 += d * d;
   }
-  const double reach = (s.radius[i] + s.radius[j] + s.eps[i] + s.eps[j]) * (1.0 + 1e-9) + 1e-12;
+  double reach = (s.radius[i] + s.radius[j] + s.eps[i] + s.eps[j]) * (1.0 + 1e-9) + 1e-12;
+  if (skin > 0.0) reach = (reach + skin) * (1.0 + 1e-9) + 1e-12;
+  return d2 <= reach * reach;
+}
+
+__device__ __forceinline__ bool spheres_touch(const delta_scene &s, int32_t i, int32_t j) {
+  return spheres_within(s, i, j, 0.0);
+}
+
+// The candidate test of obstacle L (box lo[3], hi[3]) and moving body j: the body's centre
+// within its radius and both eps of the box; skin as in spheres_within.
+__device__ __forceinline__ bool obstacle_within(const delta_scene &s, const double *box, int32_t L, int32_t j,
+                                                double skin) {
+  double d2 = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    const double c = s.pos[(int64_t)k * s.n_bodies + j];
+    const double lo = box[k], hi = box[3 + k];
+    const double d = c < lo ? lo - c : (c > hi ? c - hi : 0.0);
+    d2 += d * d;
+  }
+  double reach = (s.radius[j] + s.eps[j] + s.eps[L]) * (1.0 + 1e-9) + 1e-12;
+  if (skin > 0.0) reach = (reach + skin) * (1.0 + 1e-9) + 1e-12;
   return d2 <= reach * reach;
 }
 
@@ -684,7 +725,7 @@ __device__ __forceinline__ void push_pair(int32_t a, int32_t b, int sh, uint64_t
 constexpr int kGridColumns = 5;
 
 __global__ void k_grid_pairs(delta_scene s, Grid g, HashGrid hg, int sh, uint64_t *out, unsigned long long *count,
-                             int64_t cap) {
+                             int64_t cap, double skin) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= kGridColumns * (int64_t)s.n_bodies) return;
   const int32_t i = (int32_t)(t / kGridColumns), col = (int32_t)(t % kGridColumns);
@@ -703,28 +744,21 @@ __global__ void k_grid_pairs(delta_scene s, Grid g, HashGrid hg, int sh, uint64_
     const uint32_t b = cell_bucket(key, hg.nb);
     for (uint32_t q = hg.start[b]; q < hg.start[b + 1]; ++q) {
       const int32_t j = hg.bodies[q];
-      if ((same ? j > i : j != i) && hg.cell[j] == key && spheres_touch(s, i, j)) push_pair(i, j, sh, out, count, cap);
+      if ((same ? j > i : j != i) && hg.cell[j] == key && spheres_within(s, i, j, skin))
+        push_pair(i, j, sh, out, count, cap);
     }
   }
 }
 
 // obstacle L (box lo/hi) against every moving body j
 __global__ void k_obstacle_pairs(delta_scene s, const int32_t *obst, const double *box, int32_t n_obst, int sh,
-                                 uint64_t *out, unsigned long long *count, int64_t cap) {
+                                 uint64_t *out, unsigned long long *count, int64_t cap, double skin) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)n_obst * s.n_bodies) return;
   const int32_t o = (int32_t)(t / s.n_bodies), j = (int32_t)(t % s.n_bodies);
   const int32_t L = obst[o];
   if (s.obstacle[j]) return;
-  double d2 = 0.0;
-  for (int k = 0; k < 3; ++k) {
-    const double c = s.pos[(int64_t)k * s.n_bodies + j];
-    const double lo = box[6 * o + k], hi = box[6 * o + 3 + k];
-    const double d = c < lo ? lo - c : (c > hi ? c - hi : 0.0);
-    d2 += d * d;
-  }
-  const double reach = (s.radius[j] + s.eps[j] + s.eps[L]) * (1.0 + 1e-9) + 1e-12;
-  if (d2 <= reach * reach) push_pair(L, j, sh, out, count, cap);
+  if (obstacle_within(s, box + 6 * o, L, j, skin)) push_pair(L, j, sh, out, count, cap);
 }
 
 // The fixed-capacity pair list of at most kBlockSortCap entries, sorted and unpacked by
@@ -748,10 +782,11 @@ constexpr size_t block_sort_smem() {
 
 // Sorts keys[0 .. m) (m <= 512 * ITEMS) and unpacks them to a, b; entries [m, cap) are
 // empty (-1, -1), as the padding keys of a sort over the whole capacity would leave them.
+// With kout, the sorted keys go to kout instead ([m, cap) the empty key ~0).
 template <class K, int ITEMS>
 __device__ __forceinline__ void sort_unpack_items(unsigned char *smem, const uint64_t *__restrict__ keys, int64_t m,
                                                   int64_t cap, int sh, int32_t *__restrict__ a,
-                                                  int32_t *__restrict__ b) {
+                                                  int32_t *__restrict__ b, uint64_t *__restrict__ kout) {
   auto &tmp = *reinterpret_cast<typename PairBlockSort<K, ITEMS>::TempStorage *>(smem);
   const int t = threadIdx.x;
   K k[ITEMS];
@@ -763,6 +798,15 @@ __device__ __forceinline__ void sort_unpack_items(unsigned char *smem, const uin
     k[j] = i < m ? (K)keys[i] : ~(K)0;
   }
   PairBlockSort<K, ITEMS>(tmp).Sort(k, 0, 2 * sh);
+  if (kout) {
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const int64_t i = (int64_t)t * ITEMS + j;
+      if (i < m) kout[i] = (uint64_t)k[j];
+    }
+    for (int64_t i = m + t; i < cap; i += kBlockSortThreads) kout[i] = ~0ull;
+    return;
+  }
   const K low = ((K)1 << sh) - (K)1;
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
@@ -781,7 +825,7 @@ __device__ __forceinline__ void sort_unpack_items(unsigned char *smem, const uin
 template <class K, int MAXI>
 __global__ void __launch_bounds__(kBlockSortThreads) k_sort_unpack_pairs_block(
     const uint64_t *__restrict__ keys, int64_t cap, int sh, int32_t *__restrict__ a, int32_t *__restrict__ b,
-    const unsigned long long *count, int *ovf, int64_t *total) {
+    const unsigned long long *count, int *ovf, int64_t *total, uint64_t *__restrict__ kout) {
   extern __shared__ __align__(16) unsigned char smem[];
   const unsigned long long c = *count;
   if (threadIdx.x == 0) {
@@ -790,10 +834,10 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_sort_unpack_pairs_block(
   }
   const int64_t m = c < (unsigned long long)cap ? (int64_t)c : cap;
   constexpr int T = kBlockSortThreads;
-  if (m <= 2 * T) sort_unpack_items<K, 2>(smem, keys, m, cap, sh, a, b);
-  else if (m <= 4 * T) sort_unpack_items<K, (MAXI < 4 ? MAXI : 4)>(smem, keys, m, cap, sh, a, b);
-  else if (m <= 8 * T) sort_unpack_items<K, (MAXI < 8 ? MAXI : 8)>(smem, keys, m, cap, sh, a, b);
-  else sort_unpack_items<K, MAXI>(smem, keys, m, cap, sh, a, b);
+  if (m <= 2 * T) sort_unpack_items<K, 2>(smem, keys, m, cap, sh, a, b, kout);
+  else if (m <= 4 * T) sort_unpack_items<K, (MAXI < 4 ? MAXI : 4)>(smem, keys, m, cap, sh, a, b, kout);
+  else if (m <= 8 * T) sort_unpack_items<K, (MAXI < 8 ? MAXI : 8)>(smem, keys, m, cap, sh, a, b, kout);
+  else sort_unpack_items<K, MAXI>(smem, keys, m, cap, sh, a, b, kout);
 }
 
 template <class K, int MAXI>
@@ -813,16 +857,20 @@ static cudaError_t block_sort_prepare() {
 
 template <class K>
 static void launch_block_sort(cudaStream_t st, const uint64_t *pk, int64_t cap, int sh, int32_t *pa, int32_t *pb,
-                              const unsigned long long *count, int *ovf, int64_t *total) {
+                              const unsigned long long *count, int *ovf, int64_t *total, uint64_t *kout = nullptr) {
   constexpr int64_t T = kBlockSortThreads;
   if (cap <= 2 * T)
-    k_sort_unpack_pairs_block<K, 2><<<1, T, block_sort_smem<K, 2>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
+    k_sort_unpack_pairs_block<K, 2><<<1, T, block_sort_smem<K, 2>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total,
+                                                                          kout);
   else if (cap <= 4 * T)
-    k_sort_unpack_pairs_block<K, 4><<<1, T, block_sort_smem<K, 4>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
+    k_sort_unpack_pairs_block<K, 4><<<1, T, block_sort_smem<K, 4>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total,
+                                                                          kout);
   else if (cap <= 8 * T)
-    k_sort_unpack_pairs_block<K, 8><<<1, T, block_sort_smem<K, 8>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
+    k_sort_unpack_pairs_block<K, 8><<<1, T, block_sort_smem<K, 8>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total,
+                                                                          kout);
   else
-    k_sort_unpack_pairs_block<K, 16><<<1, T, block_sort_smem<K, 16>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total);
+    k_sort_unpack_pairs_block<K, 16><<<1, T, block_sort_smem<K, 16>(), st>>>(pk, cap, sh, pa, pb, count, ovf, total,
+                                                                            kout);
 }
 
 // pair keys back to (a, b); the empty key ~0 gives (-1, -1).  With `count` (fixed
@@ -1020,14 +1068,21 @@ delta_status integrate_run(delta_ctx *ctx, const delta_scene &s, const delta_ste
 // once from their current vertices.
 struct BroadphasePlan {
   Grid g{};
+  // the graph step's skin list: pairs within reach + skin, searched on the grid gs whose
+  // cells hold that reach (0: no skin list)
+  double skin = 0.0;
+  Grid gs{};
   int32_t n_obst = 0, n_moving = 0;
   int32_t *d_obst = nullptr;  // obstacle body indices
   double *d_box = nullptr;    // [6*n_obst] lo(3) hi(3)
+  int32_t *d_slot = nullptr;  // [n] each body's obstacle index o (its box at d_box + 6 o), -1 if moving
   void release() {
     if (d_obst) cudaFree(d_obst);
     if (d_box) cudaFree(d_box);
+    if (d_slot) cudaFree(d_slot);
     d_obst = nullptr;
     d_box = nullptr;
+    d_slot = nullptr;
   }
 };
 
@@ -1058,6 +1113,11 @@ delta_status broadphase_plan(delta_ctx *ctx, const delta_scene &s, BroadphasePla
   plan.g.h = reach > 0 ? 2.0 * reach * (1.0 + 1e-6) : 1.0;
   // cell keys wrap (cell_key), so any origin works; the lowest moving centre is used
   for (int k = 0; k < 3; ++k) plan.g.origin[k] = lo[k] < 1e299 ? lo[k] : 0.0;
+  // skin: 1/32 of a cell (a body moves it in far more steps than a call takes in these
+  // scenes); its grid's cells hold the widened reach
+  plan.skin = reach > 0 ? plan.g.h / kSkinPerCell : 0.0;
+  plan.gs = plan.g;
+  plan.gs.h = reach > 0 ? (2.0 * reach + plan.skin) * (1.0 + 1e-6) + 1e-9 : 1.0;
   plan.n_obst = (int32_t)ob.size();
   plan.n_moving = n - plan.n_obst;
   if (plan.n_obst > 0) {
@@ -1084,11 +1144,15 @@ delta_status broadphase_plan(delta_ctx *ctx, const delta_scene &s, BroadphasePla
         box[6 * o + 3 + k] = bh[k];
       }
     }
+    std::vector<int32_t> slot(n, -1);
+    for (size_t o = 0; o < ob.size(); ++o) slot[ob[o]] = (int32_t)o;
     if ((e = cudaMalloc(&plan.d_obst, sizeof(int32_t) * ob.size())) != cudaSuccess ||
         (e = cudaMalloc(&plan.d_box, sizeof(double) * box.size())) != cudaSuccess ||
+        (e = cudaMalloc(&plan.d_slot, sizeof(int32_t) * (size_t)n)) != cudaSuccess ||
         (e = cudaMemcpy(plan.d_obst, ob.data(), sizeof(int32_t) * ob.size(), cudaMemcpyHostToDevice)) !=
             cudaSuccess ||
-        (e = cudaMemcpy(plan.d_box, box.data(), sizeof(double) * box.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        (e = cudaMemcpy(plan.d_box, box.data(), sizeof(double) * box.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(plan.d_slot, slot.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice)) != cudaSuccess)
       return cuda_error(e, "obstacle upload");
   }
   return DELTA_OK;
@@ -1117,12 +1181,12 @@ static size_t grid_bytes(int32_t n) {
 }
 
 // count, scan, fill: the hash grid of the moving bodies (count and fill zeroed first)
-static cudaError_t build_grid(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, const HashGrid &hg,
+static cudaError_t build_grid(cudaStream_t st, const delta_scene &s, const Grid &grid, const HashGrid &hg,
                               void *temp, size_t temp_bytes, uint64_t *pk, int64_t pk_cap, unsigned long long *pcount) {
   const int32_t n = s.n_bodies;
   cudaError_t e = cudaMemsetAsync(hg.count, 0, 4 * (2 * (size_t)hg.nb + 1), st);
   if (e != cudaSuccess) return e;
-  k_grid_count<<<blocks_for(n), 256, 0, st>>>(s, plan.g, hg, pk, pk_cap, pcount);
+  k_grid_count<<<blocks_for(n), 256, 0, st>>>(s, grid, hg, pk, pk_cap, pcount);
   size_t tb = temp_bytes;
   if ((e = exclusive_sum(temp, tb, hg.count, hg.start, hg.nb + 1, st)) != cudaSuccess) return e;
   k_grid_fill<<<blocks_for(n), 256, 0, st>>>(s, hg);
@@ -1149,7 +1213,7 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
   size_t tb = grid_temp_bytes(n);
   void *temp = nullptr;
   if ((ds = ctx_scratch(ctx, 12, tb, &temp)) != DELTA_OK) return ds;
-  if ((e = build_grid(st, s, plan, hg, temp, tb, nullptr, 0, nullptr)) != cudaSuccess) return cuda_error(e, "grid");
+  if ((e = build_grid(st, s, plan.g, hg, temp, tb, nullptr, 0, nullptr)) != cudaSuccess) return cuda_error(e, "grid");
   ctx->launches += 3;
   int64_t cap = capacity > 4096 ? capacity : 4096;
   unsigned long long hcount = 0;
@@ -1161,12 +1225,13 @@ delta_status broadphase_run(delta_ctx *ctx, const delta_scene &s, const Broadpha
     pk = (uint64_t *)pb + 8;
     if ((e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess) return cuda_error(e, "memset");
     if (plan.n_moving > 0) {
-      k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, cap);
+      k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, cap,
+                                                                                0.0);
       ctx->launches += 1;
     }
     if (plan.n_obst > 0) {
       k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
-                                                                            sh, pk, count, cap);
+                                                                            sh, pk, count, cap, 0.0);
       ctx->launches += 1;
     }
     if ((e = cudaMemcpyAsync(&hcount, count, sizeof(hcount), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -1258,17 +1323,18 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
   char *b = carve_grid((char *)state, n, hg);
   unsigned long long *count = (unsigned long long *)b;
   uint64_t *pk = (uint64_t *)(b + 256), *spk = pk + pair_cap;
-  if ((e = build_grid(st, s, plan, hg, temp, temp_bytes, pk, pair_cap, count)) != cudaSuccess)
+  if ((e = build_grid(st, s, plan.g, hg, temp, temp_bytes, pk, pair_cap, count)) != cudaSuccess)
     return cuda_error(e, "grid");
   size_t tb = temp_bytes;
   kernels += 3;
   if (plan.n_moving > 0) {
-    k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, pair_cap);
+    k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.g, hg, sh, pk, count, pair_cap,
+                                                                                0.0);
     kernels += 1;
   }
   if (plan.n_obst > 0) {
     k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
-                                                                          sh, pk, count, pair_cap);
+                                                                          sh, pk, count, pair_cap, 0.0);
     kernels += 1;
   }
   if (pair_cap <= kBlockSortCap) {
@@ -1289,6 +1355,267 @@ delta_status broadphase_run_fixed(cudaStream_t st, const delta_scene &s, const B
 static unsigned long long *broadphase_fixed_count(void *state, int32_t n) {
   HashGrid hg{};
   return (unsigned long long *)carve_grid((char *)state, n, hg);
+}
+
+// ---- skin list (graph step) ------------------------------------------------------------
+// The candidate pairs of a step are those within reach (spheres_touch, obstacle_within).
+// The graph step keeps the sorted list of pairs within reach + skin, built at anchor
+// positions, and filters it with the exact tests each step, in key order: the same pairs,
+// in the same order, as a grid search of that step.  A pair within reach now was within
+// reach + skin at the build if neither body has moved more than skin/2 since (triangle
+// inequality; the build test's relative and absolute margins cover the rounding), so the
+// list is rebuilt, inside the graph through a conditional node, in any step where some
+// moving body has moved further.  Obstacles do not move.
+struct SkinList {
+  int64_t cap = 0;                          // entries of keys, raw, sel
+  unsigned long long *raw_count = nullptr;  // pairs found by the last build (may exceed cap)
+  int64_t *sel_count = nullptr;             // this step's pairs (multi-CTA filter)
+  int *need = nullptr;                      // nonzero: rebuild before this step's filter
+  unsigned long long *rebuilds = nullptr;   // builds run inside the graph
+  uint64_t *keys = nullptr;                 // [cap] sorted keys of the last build, ~0 after them
+  uint64_t *raw = nullptr;                  // [cap] a build's keys as found
+  uint64_t *sel = nullptr;                  // [cap] this step's keys (multi-CTA filter)
+  double *anchor = nullptr;                 // [3n] positions at the last build
+};
+
+static size_t skin_bytes(int32_t n, int64_t cap) { return 256 + 24 * (size_t)cap + 24 * (size_t)n; }
+
+static SkinList carve_skin(void *mem, int32_t n, int64_t cap) {
+  SkinList k;
+  char *b = (char *)mem;
+  k.cap = cap;
+  k.raw_count = (unsigned long long *)b;
+  k.sel_count = (int64_t *)(b + 8);
+  k.rebuilds = (unsigned long long *)(b + 16);
+  k.need = (int *)(b + 24);
+  k.keys = (uint64_t *)(b + 256);
+  k.raw = k.keys + cap;
+  k.sel = k.raw + cap;
+  k.anchor = (double *)(k.sel + cap);
+  (void)n;
+  return k;
+}
+
+// A pair key of the list (~0: empty) within reach at the current positions.
+struct SkinTouch {
+  delta_scene s;
+  int sh;
+  const int32_t *slot;
+  const double *box;
+  __device__ __forceinline__ bool operator()(uint64_t key) const {
+    if (key == ~0ull) return false;
+    const int32_t a = (int32_t)(key >> sh), b = (int32_t)(key & ((1ull << sh) - 1ull));
+    if (s.obstacle[a]) return obstacle_within(s, box + 6 * slot[a], a, b, 0.0);
+    if (s.obstacle[b]) return obstacle_within(s, box + 6 * slot[b], b, a, 0.0);
+    return spheres_touch(s, a, b);
+  }
+};
+
+// Sets *need when a moving body has moved more than `limit` from its anchor (or its
+// position is not finite).
+__global__ void k_skin_check(delta_scene s, const double *__restrict__ anchor, double limit2, int *need) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_bodies || s.obstacle[i]) return;
+  const int64_t n = s.n_bodies;
+  double d2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double d = s.pos[k * n + i] - anchor[k * n + i];
+    d2 += d * d;
+  }
+  if (!(d2 <= limit2)) *need = 1;
+}
+
+__global__ void k_skin_cond(cudaGraphConditionalHandle h, const int *need) {
+  cudaGraphSetConditional(h, *need != 0 ? 1u : 0u);
+}
+
+// End of a build: no rebuild pending, one more build counted.
+__global__ void k_skin_done(int *need, unsigned long long *rebuilds) {
+  *need = 0;
+  *rebuilds += 1ull;
+}
+
+__global__ void k_skin_overflow(const unsigned long long *raw_count, int64_t cap, int *ovf) {
+  if (*raw_count > (unsigned long long)cap) atomicCAS(ovf, 0, 1);
+}
+
+// One CTA: the list's keys (at most 512 * ITEMS) filtered by the exact tests, in order,
+// into the step's pair list (-1 after the pairs); *count_out receives the pairs found,
+// an overflow of pair_cap sets *ovf, *total adds the pairs kept.
+template <int ITEMS>
+__global__ void __launch_bounds__(kBlockSortThreads) k_skin_filter_block(const uint64_t *__restrict__ keys, int64_t cap,
+                                                                       SkinTouch touch, int32_t *__restrict__ pa,
+                                                                       int32_t *__restrict__ pb, int64_t pair_cap,
+                                                                       unsigned long long *count_out, int *ovf,
+                                                                       int64_t *total) {
+  using Scan = cub::BlockScan<int, kBlockSortThreads>;
+  __shared__ typename Scan::TempStorage tmp;
+  const int t = threadIdx.x;
+  uint64_t k[ITEMS];
+  int f[ITEMS], pos[ITEMS];
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const int64_t i = (int64_t)t * ITEMS + j;
+    k[j] = i < cap ? keys[i] : ~0ull;
+    f[j] = touch(k[j]) ? 1 : 0;
+  }
+  int found = 0;
+  Scan(tmp).ExclusiveSum(f, pos, found);
+  const uint64_t low = (1ull << touch.sh) - 1ull;
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j)
+    if (f[j] && pos[j] < pair_cap) {
+      pa[pos[j]] = (int32_t)(k[j] >> touch.sh);
+      pb[pos[j]] = (int32_t)(k[j] & low);
+    }
+  for (int64_t i = found + t; i < pair_cap; i += kBlockSortThreads) pa[i] = pb[i] = -1;
+  if (t == 0) {
+    *count_out = (unsigned long long)found;
+    if (found > pair_cap) atomicCAS(ovf, 0, 1);
+    if (total) *total += found < pair_cap ? found : pair_cap;
+  }
+}
+
+// The multi-CTA filter's output (cub's select, in order) into the step's pair list.
+__global__ void k_unpack_selected(const uint64_t *__restrict__ sel, const int64_t *sel_count, int64_t pair_cap, int sh,
+                                  int32_t *__restrict__ pa, int32_t *__restrict__ pb, unsigned long long *count_out,
+                                  int *ovf, int64_t *total) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t c = *sel_count;
+  if (t == 0) {
+    *count_out = (unsigned long long)c;
+    if (c > pair_cap) atomicCAS(ovf, 0, 1);
+    if (total) *total += c < pair_cap ? c : pair_cap;
+  }
+  if (t >= pair_cap) return;
+  if (t < c) {
+    const uint64_t k = sel[t];
+    pa[t] = (int32_t)(k >> sh);
+    pb[t] = (int32_t)(k & ((1ull << sh) - 1ull));
+  } else {
+    pa[t] = pb[t] = -1;
+  }
+}
+
+static SkinTouch skin_touch(const delta_scene &s, const BroadphasePlan &plan) {
+  return SkinTouch{s, bits_for(s.n_bodies), plan.d_slot, plan.d_box};
+}
+
+// cub's temporary storage for a build's sort and a step's selection over cap entries.
+static size_t skin_temp_bytes(const delta_scene &s, const BroadphasePlan &plan, int64_t cap) {
+  size_t a = grid_temp_bytes(s.n_bodies), b = 0, c = 0;
+  cub::DeviceRadixSort::SortKeys(nullptr, b, (uint64_t *)nullptr, (uint64_t *)nullptr, cap, 0,
+                                 2 * bits_for(s.n_bodies));
+  cub::DeviceSelect::If(nullptr, c, (const uint64_t *)nullptr, (uint64_t *)nullptr, (int64_t *)nullptr, cap,
+                        skin_touch(s, plan));
+  return std::max(a, std::max(b, c));
+}
+
+// The pairs within reach + skin at the current positions, counted (synchronous; the
+// grid part of the fixed broadphase state and its temporary storage are used).
+static delta_status skin_count(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, void *state,
+                               void *temp, size_t temp_bytes, int64_t *found) {
+  const int32_t n = s.n_bodies;
+  const int sh = bits_for(n);
+  HashGrid hg{};
+  unsigned long long *count = (unsigned long long *)carve_grid((char *)state, n, hg);
+  cudaError_t e;
+  if ((e = build_grid(st, s, plan.gs, hg, temp, temp_bytes, nullptr, 0, nullptr)) != cudaSuccess ||
+      (e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st)) != cudaSuccess)
+    return cuda_error(e, "skin count");
+  if (plan.n_moving > 0)
+    k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.gs, hg, sh, nullptr, count, 0,
+                                                                            plan.skin);
+  if (plan.n_obst > 0)
+    k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
+                                                                          sh, nullptr, count, 0, plan.skin);
+  unsigned long long h = 0;
+  if ((e = cudaGetLastError()) != cudaSuccess ||
+      (e = cudaMemcpyAsync(&h, count, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_error(e, "skin count");
+  *found = (int64_t)h;
+  return DELTA_OK;
+}
+
+// A build of the list at the current positions (the body of the graph's conditional
+// node): grid on gs, search with the widened reach, sort, anchors; an overflow of the
+// capacity sets *ovf.
+static cudaError_t skin_build(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, const SkinList &k,
+                              void *state, void *temp, size_t temp_bytes, int *ovf, int &kernels) {
+  const int32_t n = s.n_bodies;
+  const int sh = bits_for(n);
+  HashGrid hg{};
+  carve_grid((char *)state, n, hg);
+  cudaError_t e;
+  if ((e = build_grid(st, s, plan.gs, hg, temp, temp_bytes, k.raw, k.cap, k.raw_count)) != cudaSuccess) return e;
+  kernels += 3;
+  if (plan.n_moving > 0) {
+    k_grid_pairs<<<blocks_for(kGridColumns * (int64_t)n, 128), 128, 0, st>>>(s, plan.gs, hg, sh, k.raw, k.raw_count,
+                                                                            k.cap, plan.skin);
+    kernels += 1;
+  }
+  if (plan.n_obst > 0) {
+    k_obstacle_pairs<<<blocks_for((int64_t)plan.n_obst * n), 256, 0, st>>>(s, plan.d_obst, plan.d_box, plan.n_obst,
+                                                                          sh, k.raw, k.raw_count, k.cap, plan.skin);
+    kernels += 1;
+  }
+  if (k.cap <= kBlockSortCap) {
+    if (2 * sh <= 32) launch_block_sort<uint32_t>(st, k.raw, k.cap, sh, nullptr, nullptr, k.raw_count, ovf, nullptr, k.keys);
+    else launch_block_sort<uint64_t>(st, k.raw, k.cap, sh, nullptr, nullptr, k.raw_count, ovf, nullptr, k.keys);
+    kernels += 1;
+  } else {
+    size_t tb = temp_bytes;
+    if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, k.raw, k.keys, k.cap, 0, 2 * sh, st)) != cudaSuccess) return e;
+    k_skin_overflow<<<1, 1, 0, st>>>(k.raw_count, k.cap, ovf);
+    kernels += 2;
+  }
+  if ((e = cudaMemcpyAsync(k.anchor, s.pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st)) !=
+      cudaSuccess)
+    return e;
+  k_skin_done<<<1, 1, 0, st>>>(k.need, k.rebuilds);
+  kernels += 1;
+  return cudaGetLastError();
+}
+
+// A step's check: sets the rebuild condition of the graph's conditional node.
+static cudaError_t skin_check(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, const SkinList &k,
+                              cudaGraphConditionalHandle h, int &kernels) {
+  const double limit = 0.5 * plan.skin * (1.0 - 1e-9);
+  k_skin_check<<<blocks_for(s.n_bodies, 256), 256, 0, st>>>(s, k.anchor, limit * limit, k.need);
+  k_skin_cond<<<1, 1, 0, st>>>(h, k.need);
+  kernels += 2;
+  return cudaGetLastError();
+}
+
+// A step's candidate pairs from the list: one CTA for lists of at most kBlockSortCap
+// entries, else cub's select and an unpacking kernel.
+static cudaError_t skin_filter(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, const SkinList &k,
+                               int32_t *pa, int32_t *pb, int64_t pair_cap, int *ovf, int64_t *pairs_total, void *state,
+                               void *temp, size_t temp_bytes, int &kernels) {
+  const SkinTouch touch = skin_touch(s, plan);
+  unsigned long long *count_out = broadphase_fixed_count(state, s.n_bodies);
+  constexpr int64_t T = kBlockSortThreads;
+  if (k.cap <= 2 * T)
+    k_skin_filter_block<2><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
+  else if (k.cap <= 4 * T)
+    k_skin_filter_block<4><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
+  else if (k.cap <= 8 * T)
+    k_skin_filter_block<8><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
+  else if (k.cap <= 16 * T)
+    k_skin_filter_block<16><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
+  else {
+    size_t tb = temp_bytes;
+    cudaError_t e = cub::DeviceSelect::If(temp, tb, k.keys, k.sel, k.sel_count, k.cap, touch, st);
+    if (e != cudaSuccess) return e;
+    k_unpack_selected<<<blocks_for(pair_cap), 256, 0, st>>>(k.sel, k.sel_count, pair_cap, touch.sh, pa, pb, count_out,
+                                                           ovf, pairs_total);
+    kernels += 2;
+    return cudaGetLastError();
+  }
+  kernels += 1;
+  return cudaGetLastError();
 }
 }  // namespace delta
 
@@ -1325,6 +1652,7 @@ struct delta_sim {
   int64_t counters[4] = {0, 0, 0, 0};
   int64_t graph_pair_cap = 0, graph_contact_cap = 0;  // requested by delta_sim_set_graph_capacity
   int64_t last_pairs = 0;                            // candidate body pairs of the last detection
+  int64_t skin_rebuilds = 0;                         // skin list builds inside graph replays
   // graph mode: fixed-capacity buffers, device-side counts, the captured step
   struct Graph {
     int64_t pair_cap = 0, contact_cap = 0;
@@ -1335,7 +1663,15 @@ struct delta_sim {
     int64_t *d_nc = nullptr, *d_step = nullptr, *d_cnt = nullptr, *d_log = nullptr;
     int *d_ovf = nullptr, *d_snap = nullptr;
     int64_t *d_bp = nullptr;  // candidate body pairs summed over the replayed steps
+    int64_t *d_pend = nullptr;  // the step in flight's pairs, triangle pairs, solved pairs
     int64_t log_len = 0;
+    // the skin list (its buffer sk), its rebuilds' kernels, and the stream its conditional
+    // body is captured from
+    void *sk = nullptr;
+    delta::SkinList skin{};
+    int rebuild_kernels = 0;
+    unsigned long long rebuilds_seen = 0;
+    cudaStream_t stream2 = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
     cudaGraph_t graph = nullptr;
@@ -1449,10 +1785,12 @@ static void graph_release(delta_sim::Graph &g) {
   g.exec = nullptr;
   g.graph = nullptr;
   g.captured = false;
-  for (void *p : {(void *)g.pa, g.bp, g.fs, g.ds, g.temp, g.c_mem, g.dev})
+  for (void *p : {(void *)g.pa, g.bp, g.fs, g.ds, g.temp, g.c_mem, g.dev, g.sk})
     if (p) cudaFree(p);
   g.pa = g.pb = nullptr;
-  g.bp = g.fs = g.ds = g.temp = g.c_mem = g.dev = nullptr;
+  g.bp = g.fs = g.ds = g.temp = g.c_mem = g.dev = g.sk = nullptr;
+  g.skin = delta::SkinList{};
+  g.rebuilds_seen = 0;
 }
 
 // (Re)allocates the fixed buffers for the given capacities (no capture in progress).
@@ -1490,12 +1828,92 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
   g.d_ovf = (int *)(v + 32);
   g.d_snap = (int *)(v + 36);
   g.d_bp = (int64_t *)(v + 40);
+  g.d_pend = (int64_t *)(v + 48);  // 3 counters of the step in flight
   g.d_log = (int64_t *)(v + 256);
   if ((e = cudaMemset(g.dev, 0, 256)) != cudaSuccess) return cuda_error(e, "graph memset");
   if ((e = block_sort_prepare()) != cudaSuccess) return cuda_error(e, "pair sort attributes");
   delta_status ds = detect_fixed_init(s->ctx->stream, g.ds, pair_cap, contact_cap);
   if (ds != DELTA_OK) return ds;
+  if (s->plan.skin > 0.0) {
+    // the skin list, sized from the pairs within reach + skin now (half again, and more)
+    int64_t found = 0;
+    if ((ds = skin_count(s->ctx->stream, s->scene, s->plan, g.bp, g.temp, g.temp_bytes, &found)) != DELTA_OK)
+      return ds;
+    const int64_t cap = std::max<int64_t>(1024, found + found / 2 + 1024);
+    const size_t tb = skin_temp_bytes(s->scene, s->plan, cap) + 256;
+    if (tb > g.temp_bytes) {
+      cudaFree(g.temp);
+      g.temp = nullptr;
+      if ((e = cudaMalloc(&g.temp, tb)) != cudaSuccess) return cuda_error(e, "skin temp");
+      g.temp_bytes = tb;
+    }
+    if ((e = cudaMalloc(&g.sk, skin_bytes(n, cap))) != cudaSuccess) return cuda_error(e, "skin list");
+    g.skin = carve_skin(g.sk, n, cap);
+    if ((e = cudaMemset(g.sk, 0, 256)) != cudaSuccess || (e = cudaMemset(g.skin.need, 0xff, sizeof(int))) != cudaSuccess)
+      return cuda_error(e, "skin init");
+  }
   if ((e = cudaStreamSynchronize(s->ctx->stream)) != cudaSuccess) return cuda_error(e, "graph init");
+  return DELTA_OK;
+}
+
+// The step's broadphase from the skin list, under capture on g.stream: the check sets
+// the condition of an IF node whose body (captured from stream2) rebuilds the list; the
+// filter then forms the step's pairs.  k counts the kernels of every step; the body's
+// kernels go to g.rebuild_kernels.
+static delta_status graph_skin_broadphase(delta_sim *s, int &k) {
+  delta_sim::Graph &g = s->g;
+  cudaStream_t st = g.stream;
+  cudaError_t e;
+  if (!g.stream2 && (e = cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_error(e, "skin stream");
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, nullptr, nullptr)) != cudaSuccess)
+    return cuda_error(e, "skin capture info");
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, cg, 0, 0)) != cudaSuccess) return cuda_error(e, "skin condition");
+  if ((e = skin_check(st, s->scene, s->plan, g.skin, h, k)) != cudaSuccess) return cuda_error(e, "skin check");
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd)) != cudaSuccess)
+    return cuda_error(e, "skin capture info");
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeIf;
+  np.conditional.size = 1;
+  cudaGraphNode_t cn;
+  if ((e = cudaGraphAddNode(&cn, cg, deps, nd, &np)) != cudaSuccess) return cuda_error(e, "skin conditional node");
+  if ((e = cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+    return cuda_error(e, "skin capture dependencies");
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(g.stream2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return cuda_error(e, "skin body capture");
+  int rk = 0;
+  const cudaError_t eb = skin_build(g.stream2, s->scene, s->plan, g.skin, g.bp, g.temp, g.temp_bytes, g.d_ovf, rk);
+  cudaGraph_t out = nullptr;
+  e = cudaStreamEndCapture(g.stream2, &out);
+  if (eb != cudaSuccess) return cuda_error(eb, "skin build");
+  if (e != cudaSuccess) return cuda_error(e, "skin body capture");
+  g.rebuild_kernels = rk;
+  if ((e = skin_filter(st, s->scene, s->plan, g.skin, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_pend, g.bp, g.temp,
+                       g.temp_bytes, k)) != cudaSuccess)
+    return cuda_error(e, "skin filter");
+  return DELTA_OK;
+}
+
+// The skin list's rebuilds inside the graph since the last count: their kernels go to the
+// context's launch count, the builds to the simulation's total.
+static delta_status graph_count_rebuilds(delta_sim *s) {
+  delta_sim::Graph &g = s->g;
+  if (g.skin.cap <= 0) return DELTA_OK;
+  unsigned long long rb = 0;
+  cudaError_t e = cudaMemcpy(&rb, g.skin.rebuilds, 8, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_error(e, "skin rebuilds");
+  s->ctx->launches += (int64_t)(rb - g.rebuilds_seen) * g.rebuild_kernels;
+  s->skin_rebuilds += (int64_t)(rb - g.rebuilds_seen);
+  g.rebuilds_seen = rb;
   return DELTA_OK;
 }
 
@@ -1508,9 +1926,12 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   if (ds != DELTA_OK) return ds;
   k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf, g.d_snap,
                                                                s->epoch);
-  if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_bp, g.bp, g.temp,
-                                 g.temp_bytes, k)) != DELTA_OK)
+  if (g.skin.cap > 0) {
+    if ((ds = graph_skin_broadphase(s, k)) != DELTA_OK) return ds;
+  } else if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_pend, g.bp,
+                                        g.temp, g.temp_bytes, k)) != DELTA_OK) {
     return ds;
+  }
   // vertices of the bodies the narrowphase reads this step: formed from the poses by the
   // certified driver, updated here for the others
   const bool posed = s->driver == DELTA_DRV_BF_CERT || s->driver == DELTA_DRV_BF_CULLED || s->driver == DELTA_DRV_LEARNED;
@@ -1523,12 +1944,12 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
                  s->scene.eps,      s->scene.friction,   s->ids};
   const int64_t before = s->ctx->launches;
-  if ((ds = detect_run_fixed(s->ctx, st, s->driver, m, g.pa, g.pb, g.pair_cap, g.c, g.d_nc, g.d_ovf, 1, g.d_cnt,
+  if ((ds = detect_run_fixed(s->ctx, st, s->driver, m, g.pa, g.pb, g.pair_cap, g.c, g.d_nc, g.d_ovf, 1, g.d_pend + 1,
                              nullptr, g.ds, g.temp, g.temp_bytes, posed ? &pose : nullptr, s->tri_bits)) != DELTA_OK)
     return ds;
   k += (int)(s->ctx->launches - before);
   s->ctx->launches = before;
-  k_step_end<<<1, 1, 0, st>>>(g.d_snap, g.d_nc, g.d_log, g.log_len, g.d_step);
+  k_step_end<<<1, 1, 0, st>>>(g.d_snap, g.d_ovf, g.d_nc, g.d_log, g.log_len, g.d_step, g.d_pend, g.d_bp, g.d_cnt);
   g.kernels = k + 2;
   return cuda_error(cudaGetLastError(), "graph step");
 }
@@ -1903,7 +2324,10 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
       (e = cudaMemsetAsync(g.d_step, 0, 8, g.stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(g.d_cnt, 0, 16, g.stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(g.d_bp, 0, 8, g.stream)) != cudaSuccess ||
-      (e = cudaMemsetAsync(g.d_ovf, 0, 8, g.stream)) != cudaSuccess || (e = cudaStreamSynchronize(g.stream)) != cudaSuccess)
+      (e = cudaMemsetAsync(g.d_pend, 0, 24, g.stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(g.d_ovf, 0, 8, g.stream)) != cudaSuccess ||
+      (g.skin.cap > 0 && (e = cudaMemsetAsync(g.skin.need, 0xff, sizeof(int), g.stream)) != cudaSuccess) ||
+      (e = cudaStreamSynchronize(g.stream)) != cudaSuccess)
     return cuda_error(e, "graph setup");
   int32_t base = done;  // steps completed before the current batch of launches
   while (done < nsteps) {
@@ -1943,6 +2367,7 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
     s->counters[1] += seg_bp;
     s->counters[2] += seg_cnt[0];
     s->counters[3] += seg_cnt[1];
+    if ((ds = graph_count_rebuilds(s)) != DELTA_OK) return ds;
     if ((ds = graph_alloc(s, std::max<int64_t>(2 * g.pair_cap, 2 * (int64_t)pc), std::max<int64_t>(2 * g.contact_cap,
                           4 * s->n_contacts), saved_log)) != DELTA_OK)
       return ds;
@@ -1962,11 +2387,20 @@ delta_status delta_sim_step_graph(delta_sim *s, const delta_step_params *params,
   s->counters[1] += bp;
   s->counters[2] += cnt[0];
   s->counters[3] += cnt[1];
+  if ((ds = graph_count_rebuilds(s)) != DELTA_OK) return ds;
   if (nc > s->c.capacity && (ds = alloc_contacts(s, nc + nc / 2 + 1024)) != DELTA_OK) return ds;
   if ((ds = copy_contacts(g.c, s->c, nc, g.stream)) != DELTA_OK) return ds;
   if ((ds = sim_all_vertices(s, g.stream)) != DELTA_OK) return ds;
   if ((e = cudaStreamSynchronize(g.stream)) != cudaSuccess) return cuda_error(e, "graph end");
   s->n_contacts = nc;
+  return DELTA_OK;
+}
+
+delta_status delta_sim_skin_stats(delta_sim *s, double *skin, int64_t *capacity, int64_t *rebuilds) {
+  if (!s || !skin || !capacity || !rebuilds) return set_error(DELTA_ERR_INVALID, "delta_sim_skin_stats: bad argument");
+  *skin = s->plan.skin;
+  *capacity = s->g.skin.cap;
+  *rebuilds = s->skin_rebuilds;
   return DELTA_OK;
 }
 
@@ -1991,6 +2425,7 @@ delta_status delta_sim_destroy(delta_sim *s) {
   graph_release(s->g);
   if (s->g.ev) cudaEventDestroy(s->g.ev);
   if (s->g.stream) cudaStreamDestroy(s->g.stream);
+  if (s->g.stream2) cudaStreamDestroy(s->g.stream2);
   s->plan.release();
   if (s->ids) cudaFree(s->ids);
   if (s->stamp) cudaFree(s->stamp);

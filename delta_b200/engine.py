@@ -95,6 +95,12 @@ class Simulation:
     def set_graph_capacity(self, pairs: int, contacts: int):
         check(lib().delta_sim_set_graph_capacity(self._h, int(pairs), int(contacts)))
 
+    def skin_stats(self) -> dict:
+        """The graph step's skin list: skin distance, capacity, builds inside graph replays."""
+        skin, cap, rb = C.c_double(0), C.c_int64(0), C.c_int64(0)
+        check(lib().delta_sim_skin_stats(self._h, C.byref(skin), C.byref(cap), C.byref(rb)))
+        return {"skin": skin.value, "capacity": cap.value, "rebuilds": rb.value}
+
     def autotune(self, reps: int = 5, cache=None) -> dict:
         """delta_sim_autotune: times the culled driver's detection of the current state under
         every launch shape of its culling and survivor kernels and keeps the fastest on the

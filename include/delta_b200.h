@@ -292,6 +292,11 @@ delta_status delta_sim_step(delta_sim *sim, const delta_step_params *params, int
 /* Same steps as delta_sim_step, recorded once as a CUDA graph (every kernel of a step,
  * fixed-capacity buffers, counts kept on the device) and replayed nsteps times without
  * host synchronisation.  The first call sizes the buffers from an observed detection.
+ * The replayed step takes its candidate pairs from a skin list: the sorted pairs within
+ * reach + skin (skin = 1/32 of a broadphase cell), filtered each step with the exact
+ * candidate test; a conditional node of the graph rebuilds the list at the start of each
+ * call and in any step where a moving body has moved more than skin/2 since the last
+ * build, so the candidates, and their order, are those of delta_sim_step's search.
  * A capacity overflow in a replayed step freezes the state after that step's
  * integration; the host then repeats that detection with larger buffers, records the
  * graph again and continues, so results equal delta_sim_step's bit for bit.  The buffers
@@ -303,6 +308,10 @@ delta_status delta_sim_step_graph(delta_sim *sim, const delta_step_params *param
  * delta_sim_step_graph call instead of the observed-size default; overflows still
  * recover as described above. */
 delta_status delta_sim_set_graph_capacity(delta_sim *sim, int64_t pair_capacity, int64_t contact_capacity);
+/* The graph step's skin list: the skin distance (0: no list, the step searches the grid),
+ * the list's capacity (0 before the first graph call) and the builds run inside graph
+ * replays so far. */
+delta_status delta_sim_skin_stats(delta_sim *sim, double *skin, int64_t *capacity, int64_t *rebuilds);
 /* Launch shapes of the culled drivers' two kernels (DELTA_DRV_BF_CERT, DELTA_DRV_BF_CULLED,
  * DELTA_DRV_LEARNED): the culling kernel's and the survivors' solver's resident blocks per
  * SM (0 = as many as fit; larger values are clamped to what fits).  They belong to the

@@ -445,3 +445,72 @@ def test_graph_sort_and_scan_paths_agree(ctx, bodies):
             assert np.array_equal(st[k], s0[k]), k
         for f in FIELDS:
             assert np.array_equal(c[f], k0[f]), f
+
+
+def _graph_and_stepped(ctx, scene, driver, steps, prm):
+    """Runs `steps` with delta_sim_step and with the graph (one call); returns both
+    (contacts per step, state, counters) and the graph run's skin list statistics."""
+    from delta_b200.engine import Simulation
+
+    out = []
+    for graph in (False, True):
+        sim = Simulation(ctx, scene, driver)
+        cps = sim.step(steps, prm, graph=graph)
+        out.append((list(cps), sim.state(), sim.counters()))
+        skin = sim.skin_stats()
+        sim.close()
+    return out[0], out[1], skin
+
+
+def _assert_same_run(a, b):
+    (c0, s0, n0), (c1, s1, n1) = a, b
+    assert c1 == c0
+    for k in STATE:
+        assert np.array_equal(s1[k], s0[k]), k
+    for k in ("steps", "body_pairs", "triangle_pairs", "solved"):
+        assert n1[k] == n0[k], (k, n1[k], n0[k])
+
+
+@pytest.mark.parametrize("driver", [0, 8])
+def test_graph_skin_list_rebuilds_inside_the_graph(ctx, driver):
+    """The graph step takes its candidates from a skin list (pairs within reach + skin,
+    filtered each step) that a conditional node rebuilds whenever a body has moved more
+    than skin/2.  A lattice whose bodies move at up to 3 m/s crosses the skin many times in
+    300 steps: the graph run, with its rebuilds inside the replays, equals delta_sim_step
+    bit for bit, counters included."""
+    from delta_b200.engine import StepParams
+    from delta_b200.scenarios import lattice_scene
+
+    scene = lattice_scene(seed=5)
+    rng = np.random.default_rng(5)
+    n = scene["n_bodies"]
+    vel = rng.uniform(-3.0, 3.0, (n, 3))
+    vel[scene["obstacle"] != 0] = 0.0
+    scene["vel"] = vel.reshape(-1).copy()
+    prm = StepParams.make(**PARAMS)
+    stepped, graph, skin = _graph_and_stepped(ctx, scene, driver, 300, prm)
+    assert skin["skin"] > 0 and skin["capacity"] > 0
+    assert skin["rebuilds"] > 10, skin
+    assert sum(stepped[0]) > 0  # the moving bodies touch
+    _assert_same_run(stepped, graph)
+
+
+def test_graph_skin_list_overflow_recovers(ctx):
+    """An 8 x 8 x 8 lattice just wider than the skin list's reach, squeezed towards its
+    centre: the pairs within reach + skin grow past the list's capacity (sized from the
+    first, empty search), the replay freezes at the overflowing step and the host
+    re-sizes the list and records the graph again; the run equals delta_sim_step's."""
+    from delta_b200.engine import StepParams
+    from delta_b200.scenarios import particle_cloud_scene
+
+    sp, k = 0.027, 8
+    g = (np.arange(k) - (k - 1) / 2) * sp
+    cen = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    n = cen.shape[0]
+    scene = particle_cloud_scene(cen, np.full(n, 0.0095), np.full(n, 80), [], seed=9)
+    scene["vel"] = (-30.0 * cen).reshape(-1).copy()  # neighbours close at 0.81 m/s: spacing 0.022 m after 6 ms
+    prm = StepParams.make(dt=1e-5, gravity=(0.0, 0.0, 0.0), spring=1e6, damper=0.1, friction=0.0)
+    stepped, graph, skin = _graph_and_stepped(ctx, scene, 0, 600, prm)
+    assert skin["capacity"] > 1024 + 1024 // 2, skin  # grown past the first list
+    assert sum(stepped[0]) > 0
+    _assert_same_run(stepped, graph)
