@@ -276,6 +276,8 @@ def timestep_section(ctx, stream, scene, workload, steps: int, warmup: int, para
             r = _time_sim(c, stream, sim, k, params, graph)
             if reps == 0:
                 first, state = r, sim.state()
+                if graph:  # the graph step's skin list: its capacity and the builds inside the replays
+                    first = dict(first, skin_list=sim.skin_stats())
             sim.close()
             total_t += k / r["steps_per_s"]
             total_steps += k

@@ -1440,15 +1440,24 @@ __global__ void k_skin_overflow(const unsigned long long *raw_count, int64_t cap
   if (*raw_count > (unsigned long long)cap) atomicCAS(ovf, 0, 1);
 }
 
-// One CTA: the list's keys (at most 512 * ITEMS) filtered by the exact tests, in order,
-// into the step's pair list (-1 after the pairs); *count_out receives the pairs found,
-// an overflow of pair_cap sets *ovf, *total adds the pairs kept.
+// The exact test of every list entry, one thread per entry (the tests' dependent loads
+// spread over the GPU): flags[i] = 1 where keys[i] is a pair within reach.
+__global__ void k_skin_flags(const uint64_t *__restrict__ keys, int64_t cap, SkinTouch touch,
+                             uint8_t *__restrict__ flags) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < cap) flags[i] = touch(keys[i]) ? 1 : 0;
+}
+
+// One CTA: the flagged keys of a list of at most 512 * ITEMS entries, in order, into the
+// step's pair list (-1 after the pairs); *count_out receives the pairs found, an overflow
+// of pair_cap sets *ovf, *total adds the pairs kept.
 template <int ITEMS>
-__global__ void __launch_bounds__(kBlockSortThreads) k_skin_filter_block(const uint64_t *__restrict__ keys, int64_t cap,
-                                                                       SkinTouch touch, int32_t *__restrict__ pa,
-                                                                       int32_t *__restrict__ pb, int64_t pair_cap,
-                                                                       unsigned long long *count_out, int *ovf,
-                                                                       int64_t *total) {
+__global__ void __launch_bounds__(kBlockSortThreads) k_skin_compact_block(const uint64_t *__restrict__ keys,
+                                                                        const uint8_t *__restrict__ flags, int64_t cap,
+                                                                        int sh, int32_t *__restrict__ pa,
+                                                                        int32_t *__restrict__ pb, int64_t pair_cap,
+                                                                        unsigned long long *count_out, int *ovf,
+                                                                        int64_t *total) {
   using Scan = cub::BlockScan<int, kBlockSortThreads>;
   __shared__ typename Scan::TempStorage tmp;
   const int t = threadIdx.x;
@@ -1457,16 +1466,16 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_skin_filter_block(const u
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
     const int64_t i = (int64_t)t * ITEMS + j;
-    k[j] = i < cap ? keys[i] : ~0ull;
-    f[j] = touch(k[j]) ? 1 : 0;
+    f[j] = i < cap ? flags[i] : 0;
+    k[j] = f[j] ? keys[i] : 0ull;
   }
   int found = 0;
   Scan(tmp).ExclusiveSum(f, pos, found);
-  const uint64_t low = (1ull << touch.sh) - 1ull;
+  const uint64_t low = (1ull << sh) - 1ull;
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j)
     if (f[j] && pos[j] < pair_cap) {
-      pa[pos[j]] = (int32_t)(k[j] >> touch.sh);
+      pa[pos[j]] = (int32_t)(k[j] >> sh);
       pb[pos[j]] = (int32_t)(k[j] & low);
     }
   for (int64_t i = found + t; i < pair_cap; i += kBlockSortThreads) pa[i] = pb[i] = -1;
@@ -1589,23 +1598,34 @@ static cudaError_t skin_check(cudaStream_t st, const delta_scene &s, const Broad
   return cudaGetLastError();
 }
 
-// A step's candidate pairs from the list: one CTA for lists of at most kBlockSortCap
-// entries, else cub's select and an unpacking kernel.
+// A step's candidate pairs from the list: the tests one thread per entry and an ordered
+// compaction in one CTA for lists of at most kBlockSortCap entries, else cub's select and
+// an unpacking kernel.
 static cudaError_t skin_filter(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, const SkinList &k,
                                int32_t *pa, int32_t *pb, int64_t pair_cap, int *ovf, int64_t *pairs_total, void *state,
                                void *temp, size_t temp_bytes, int &kernels) {
   const SkinTouch touch = skin_touch(s, plan);
   unsigned long long *count_out = broadphase_fixed_count(state, s.n_bodies);
   constexpr int64_t T = kBlockSortThreads;
-  if (k.cap <= 2 * T)
-    k_skin_filter_block<2><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
-  else if (k.cap <= 4 * T)
-    k_skin_filter_block<4><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
-  else if (k.cap <= 8 * T)
-    k_skin_filter_block<8><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
-  else if (k.cap <= 16 * T)
-    k_skin_filter_block<16><<<1, T, 0, st>>>(k.keys, k.cap, touch, pa, pb, pair_cap, count_out, ovf, pairs_total);
-  else {
+  if (k.cap <= kBlockSortCap) {
+    // the tests on the whole GPU, the ordered compaction in one CTA (the flags in sel)
+    uint8_t *flags = reinterpret_cast<uint8_t *>(k.sel);
+    k_skin_flags<<<blocks_for(k.cap, 128), 128, 0, st>>>(k.keys, k.cap, touch, flags);
+    if (k.cap <= 2 * T)
+      k_skin_compact_block<2><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
+                                                pairs_total);
+    else if (k.cap <= 4 * T)
+      k_skin_compact_block<4><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
+                                                pairs_total);
+    else if (k.cap <= 8 * T)
+      k_skin_compact_block<8><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
+                                                pairs_total);
+    else
+      k_skin_compact_block<16><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
+                                                 pairs_total);
+    kernels += 2;
+    return cudaGetLastError();
+  } else {
     size_t tb = temp_bytes;
     cudaError_t e = cub::DeviceSelect::If(temp, tb, k.keys, k.sel, k.sel_count, k.cap, touch, st);
     if (e != cudaSuccess) return e;
@@ -1614,8 +1634,6 @@ static cudaError_t skin_filter(cudaStream_t st, const delta_scene &s, const Broa
     kernels += 2;
     return cudaGetLastError();
   }
-  kernels += 1;
-  return cudaGetLastError();
 }
 }  // namespace delta
 
