@@ -5,6 +5,8 @@
 #pragma once
 #include <cub/cub.cuh>
 
+#include "pdl.cuh"
+
 #include <cstdint>
 
 namespace delta {
@@ -19,6 +21,7 @@ constexpr int64_t kBlockScanMax = (int64_t)kBlockScanThreads * kBlockScanItems;
 template <class T>
 __global__ void __launch_bounds__(kBlockScanThreads) k_block_exclusive_scan(const T *__restrict__ in,
                                                                             T *__restrict__ out, int64_t n) {
+  dep_sync();
   using Scan = cub::BlockScan<T, kBlockScanThreads>;
   __shared__ typename Scan::TempStorage tmp;
   __shared__ T carry;
@@ -48,11 +51,9 @@ __global__ void __launch_bounds__(kBlockScanThreads) k_block_exclusive_scan(cons
 // Exclusive sum of n entries: one CTA for n <= kBlockScanMax, else cub's device scan with
 // the given temporary storage (sized by cub for n).
 template <class T>
-inline cudaError_t exclusive_sum(void *temp, size_t &temp_bytes, const T *in, T *out, int64_t n, cudaStream_t s) {
-  if (n <= kBlockScanMax) {
-    k_block_exclusive_scan<T><<<1, kBlockScanThreads, 0, s>>>(in, out, n);
-    return cudaGetLastError();
-  }
+inline cudaError_t exclusive_sum(void *temp, size_t &temp_bytes, const T *in, T *out, int64_t n, cudaStream_t s,
+                                 bool dep = false) {
+  if (n <= kBlockScanMax) return launch_dep(dep, k_block_exclusive_scan<T>, 1, kBlockScanThreads, 0, s, in, out, n);
   return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, in, out, n, s);
 }
 

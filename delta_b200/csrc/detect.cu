@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdlib>
 
+#include "pdl.cuh"
 #include "blockscan.cuh"
 #include "internal.h"
 #include "pose.cuh"
@@ -458,6 +459,7 @@ __device__ __forceinline__ int32_t cull_fill(const delta_meshes &m, const Pose &
 __global__ void __launch_bounds__(kCullThreads, 8) k_cull_pairs(delta_meshes m, const int32_t *__restrict__ pa,
                                                              const int32_t *__restrict__ pb, int64_t n_pairs,
                                                              RawContacts rc, DevStats *st) {
+  dep_sync();
   __shared__ CullList LA, LB;
   __shared__ BodyPose QA, QB;
   __shared__ int64_t s_next;
@@ -562,6 +564,7 @@ inline cudaError_t launch_cull(cudaStream_t s, const delta_meshes &m, const int3
 __global__ void __launch_bounds__(128, 5) k_cert_survivors(delta_meshes m, const int32_t *__restrict__ pa,
                                                         const int32_t *__restrict__ pb, RawContacts rc,
                                                         DevStats *st) {
+  dep_sync();
   __shared__ CertWarpSmem sm[4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned long long cnt = *rc.sv_count;
@@ -599,6 +602,7 @@ __global__ void __launch_bounds__(128, 5) k_cert_survivors(delta_meshes m, const
 // which separates what the culling gains from what the certified FP32 solver gains.
 __global__ void __launch_bounds__(128, 5) k_bf64_survivors(delta_meshes m, const int32_t *__restrict__ pa,
                                                            const int32_t *__restrict__ pb, RawContacts rc) {
+  dep_sync();
   const unsigned long long cnt = *rc.sv_count;
   const int64_t n = (int64_t)cnt < rc.sv_cap ? (int64_t)cnt : rc.sv_cap;
   // a warp takes 32 survivors at a time and meets at __syncwarp after them, so that its
@@ -654,6 +658,7 @@ constexpr double kLearnedRelTol = 1e-6;
 __global__ void __launch_bounds__(128, 4) k_learned_survivors(delta_meshes m, const int32_t *__restrict__ pa,
                                                            const int32_t *__restrict__ pb, RawContacts rc,
                                                            DevStats *st) {
+  dep_sync();
   __shared__ CertWarpSmem sm[4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned long long cnt = *rc.sv_count;
@@ -702,7 +707,7 @@ __global__ void __launch_bounds__(128, 4) k_learned_survivors(delta_meshes m, co
 // bfSolver (DELTA_DRV_BF_CULLED) or the learned FP32 hybrid (DELTA_DRV_LEARNED).
 inline cudaError_t launch_survivors(int driver, cudaStream_t s, const delta_meshes &m, const int32_t *pa,
                                     const int32_t *pb, const RawContacts &rc, DevStats *st, int64_t n_hint,
-                                    int cap = 0) {
+                                    int cap = 0, bool dep = false) {
   int per_sm = 0;
   cudaError_t e = driver == DELTA_DRV_BF_CULLED
                       ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bf64_survivors, 128, 0)
@@ -715,10 +720,10 @@ inline cudaError_t launch_survivors(int driver, cudaStream_t s, const delta_mesh
   const int64_t mx = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
   if (blocks > mx) blocks = mx;
   if (blocks < 1) blocks = 1;
-  if (driver == DELTA_DRV_BF_CULLED) k_bf64_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc);
-  else if (driver == DELTA_DRV_LEARNED) k_learned_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc, st);
-  else k_cert_survivors<<<(unsigned)blocks, 128, 0, s>>>(m, pa, pb, rc, st);
-  return cudaGetLastError();
+  if (driver == DELTA_DRV_BF_CULLED) return launch_dep(dep, k_bf64_survivors, (unsigned)blocks, 128, 0, s, m, pa, pb, rc);
+  if (driver == DELTA_DRV_LEARNED)
+    return launch_dep(dep, k_learned_survivors, (unsigned)blocks, 128, 0, s, m, pa, pb, rc, st);
+  return launch_dep(dep, k_cert_survivors, (unsigned)blocks, 128, 0, s, m, pa, pb, rc, st);
 }
 
 __global__ void k_sv_evaluated(const unsigned long long *sv_count, int64_t sv_cap, DevStats *st, int *ovf) {
@@ -781,6 +786,7 @@ __global__ void k_gather_fixed(RawContacts rc, const int64_t *perm, delta_contac
 // Sort-free ordering of the fixed-capacity certified driver's contacts, step 1: contact c
 // of pair k goes to its pair's bucket, at poff[k] + its rank of arrival, with its key.
 __global__ void k_bucket_contacts(RawContacts rc, const int64_t *poff, int64_t *bidx, uint64_t *bkey) {
+  dep_sync();
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long cnt = *rc.count;
   const int64_t n = (int64_t)cnt < rc.cap ? (int64_t)cnt : rc.cap;
@@ -799,6 +805,7 @@ __global__ void k_bucket_contacts(RawContacts rc, const int64_t *poff, int64_t *
 __global__ void k_pair_gather(RawContacts rc, const int64_t *poff, const int64_t *bidx, const uint64_t *bkey,
                               int64_t n_pairs, delta_contacts out, int64_t *n_out, int *ovf, int ovf_code,
                               int64_t *count_log) {
+  dep_sync();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long cnt = *rc.count;
   if (j == 0) {
@@ -847,6 +854,7 @@ __global__ void k_accumulate(const DevStats *st, int64_t *counters) {
 // to the running counters.
 __global__ void k_cert_tail(const unsigned long long *sv_count, int64_t sv_cap, DevStats *st, int *ovf,
                             int64_t *counters) {
+  dep_sync();
   const unsigned long long c = *sv_count;
   st->evaluated += c;
   if (ovf && c > (unsigned long long)sv_cap) atomicCAS(ovf, 0, 1);
@@ -1190,17 +1198,21 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
     rc.slot = (uint32_t *)key_out;
     e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats, ctx->cull_blocks_per_sm);
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
-    if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, -1, ctx->surv_blocks_per_sm)) != cudaSuccess)
+    // after the culling (which follows a memset), programmatic dependent launches (pdl.cuh)
+    if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, -1, ctx->surv_blocks_per_sm, true)) != cudaSuccess)
       return cuda_error(e, "survivor kernel");
-    if ((e = exclusive_sum(temp, tb, rows, row_offset, pair_cap + 1, s)) != cudaSuccess)
+    if ((e = exclusive_sum(temp, tb, rows, row_offset, pair_cap + 1, s, true)) != cudaSuccess)
       return cuda_error(e, "pair contact scan");
-    k_bucket_contacts<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out, (uint64_t *)perm_in);
-    k_pair_gather<<<(unsigned)((cap + 255) / 256), 256, 0, s>>>(rc, row_offset, perm_out, (const uint64_t *)perm_in,
-                                                                pair_cap, out, d_ncontacts, d_ovf, ovf_code,
-                                                                d_count_log);
-    k_cert_tail<<<1, 1, 0, s>>>(rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters);
+    const unsigned cb = (unsigned)((cap + 255) / 256);
+    if ((e = launch_dep(true, k_bucket_contacts, cb, 256, 0, s, rc, row_offset, perm_out, (uint64_t *)perm_in)) !=
+            cudaSuccess ||
+        (e = launch_dep(true, k_pair_gather, cb, 256, 0, s, rc, row_offset, perm_out, (const uint64_t *)perm_in,
+                        pair_cap, out, d_ncontacts, d_ovf, ovf_code, d_count_log)) != cudaSuccess ||
+        (e = launch_dep(true, k_cert_tail, 1, 1, 0, s, rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters)) !=
+            cudaSuccess)
+      return cuda_error(e, "detect fixed");
     ctx->launches += 6;
-    return cuda_error(cudaGetLastError(), "detect fixed");
+    return DELTA_OK;
   } else {
     // empty key entries sort last
     if ((e = cudaMemsetAsync(rc.key, 0xff, sizeof(uint64_t) * cap, s)) != cudaSuccess) return cuda_error(e, "memset");

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <vector>
 
+#include "pdl.cuh"
 #include "blockscan.cuh"
 #include "internal.h"
 #include "pose.cuh"
@@ -171,6 +172,7 @@ __device__ __forceinline__ void contact_terms(const ContactView &cv, int64_t c, 
 // the replays queued after it are frozen.  pend is cleared for the next step.
 __global__ void k_step_end(const int *ovf_snap, const int *ovf, const int64_t *n_contacts, int64_t *log,
                            int64_t log_len, int64_t *step, int64_t *pend, int64_t *pairs_total, int64_t *counters) {
+  dep_sync();
   if (!*ovf_snap) {
     const int64_t k = *step;
     if (k < log_len) log[k] = *n_contacts;
@@ -207,6 +209,7 @@ __global__ void __launch_bounds__(kHeadThreads) k_pair_forces_heads(
     delta_scene s, ContactView cv, const int64_t *n_contacts_d, int64_t n_contacts_h, const int64_t *seg_start,
     const int64_t *n_seg_p, delta_step_params p, int sh, uint64_t *key, int64_t *val_idx, double *entry,
     uint32_t *slave_count) {
+  dep_sync();
   __shared__ double term[12][kHeadThreads];  // master F, master T, slave F, slave T
   const int64_t blk0 = (int64_t)blockIdx.x * kHeadThreads;
   const int64_t c = blk0 + threadIdx.x;
@@ -295,6 +298,7 @@ __global__ void __launch_bounds__(kHeadThreads) k_pair_forces_heads(
 // sum kernel orders the range).
 __global__ void k_fill_slave_lists(delta_scene s, ContactView cv, const int64_t *n_contacts_d, const uint32_t *start,
                                    uint32_t *fill, int32_t *list) {
+  dep_sync();
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = *n_contacts_d < cv.cap ? *n_contacts_d : cv.cap;
   if (c >= n) return;
@@ -313,6 +317,7 @@ __global__ void k_fill_slave_lists(delta_scene s, ContactView cv, const int64_t 
 __global__ void k_body_forces_lists(delta_scene s, ContactView cv, const int64_t *n_contacts_d, const uint32_t *start,
                                     int32_t *list, const double *entry, double *force, double *torque,
                                     uint8_t *has) {
+  dep_sync();
   const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   const int32_t nb = s.n_bodies;
   if (b >= nb) return;
@@ -420,6 +425,7 @@ inline cudaError_t zero_body_sums(cudaStream_t st, int32_t n, double *force, dou
 // overflow flag and advances the vertex-stamp epoch.
 __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force, const double *torque,
                          const uint8_t *has, const int *ovf, int *ovf_snap, uint32_t *epoch) {
+  dep_sync();
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (ovf_snap && i == 0) {
     *ovf_snap = *ovf;
@@ -452,6 +458,7 @@ __global__ void k_bodies(delta_scene s, delta_step_params p, const double *force
 // With `stamp`, only the bodies whose stamp equals *epoch (the bodies of this step's
 // candidate pairs, k_mark_pair_bodies) are processed.
 __global__ void k_vertices(delta_scene s, const int *ovf, double *bbox, const uint32_t *stamp, const uint32_t *epoch) {
+  dep_sync();
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -539,6 +546,7 @@ __global__ void k_next_epoch(uint32_t *epoch) { *epoch += 1u; }
 // current epoch: these are the bodies whose vertices the narrowphase reads this step.
 __global__ void k_mark_pair_bodies(const int32_t *pa, const int32_t *pb, int64_t n, const uint32_t *epoch,
                                    uint32_t *stamp) {
+  dep_sync();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const uint32_t e = *epoch;
@@ -1293,10 +1301,14 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   k_pair_forces_heads<true><<<blocks_for(cap, kHeadThreads), kHeadThreads, 0, st>>>(
       s, cv, d_nc, 0, nullptr, nullptr, p, 0, nullptr, nullptr, entry, cnt);
   size_t tb = temp_bytes;
-  if ((e = exclusive_sum(temp, tb, cnt, start, (int64_t)n + 1, st)) != cudaSuccess)
+  // the kernels after the first start as programmatic dependent launches (pdl.cuh)
+  if ((e = exclusive_sum(temp, tb, cnt, start, (int64_t)n + 1, st, true)) != cudaSuccess)
     return cuda_error(e, "slave list scan");
-  k_fill_slave_lists<<<blocks_for(cap), 256, 0, st>>>(s, cv, d_nc, start, fill, list);
-  k_body_forces_lists<<<blocks_for(n), 256, 0, st>>>(s, cv, d_nc, start, list, entry, force, torque, has);
+  if ((e = launch_dep(true, k_fill_slave_lists, blocks_for(cap), 256, 0, st, s, cv, d_nc, start, fill, list)) !=
+          cudaSuccess ||
+      (e = launch_dep(true, k_body_forces_lists, blocks_for(n), 256, 0, st, s, cv, d_nc, start, list, entry, force,
+                      torque, has)) != cudaSuccess)
+    return cuda_error(e, "forces fixed");
   kernels += 4;
   return cuda_error(cudaGetLastError(), "forces fixed");
 }
@@ -1414,6 +1426,7 @@ struct SkinTouch {
 // Sets *need when a moving body has moved more than `limit` from its anchor (or its
 // position is not finite).
 __global__ void k_skin_check(delta_scene s, const double *__restrict__ anchor, double limit2, int *need) {
+  dep_sync();
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n_bodies || s.obstacle[i]) return;
   const int64_t n = s.n_bodies;
@@ -1427,6 +1440,7 @@ __global__ void k_skin_check(delta_scene s, const double *__restrict__ anchor, d
 }
 
 __global__ void k_skin_cond(cudaGraphConditionalHandle h, const int *need) {
+  dep_sync();
   cudaGraphSetConditional(h, *need != 0 ? 1u : 0u);
 }
 
@@ -1444,6 +1458,7 @@ __global__ void k_skin_overflow(const unsigned long long *raw_count, int64_t cap
 // spread over the GPU): flags[i] = 1 where keys[i] is a pair within reach.
 __global__ void k_skin_flags(const uint64_t *__restrict__ keys, int64_t cap, SkinTouch touch,
                              uint8_t *__restrict__ flags) {
+  dep_sync();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < cap) flags[i] = touch(keys[i]) ? 1 : 0;
 }
@@ -1458,6 +1473,7 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_skin_compact_block(const 
                                                                         int32_t *__restrict__ pb, int64_t pair_cap,
                                                                         unsigned long long *count_out, int *ovf,
                                                                         int64_t *total) {
+  dep_sync();
   using Scan = cub::BlockScan<int, kBlockSortThreads>;
   __shared__ typename Scan::TempStorage tmp;
   const int t = threadIdx.x;
@@ -1490,6 +1506,7 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_skin_compact_block(const 
 __global__ void k_unpack_selected(const uint64_t *__restrict__ sel, const int64_t *sel_count, int64_t pair_cap, int sh,
                                   int32_t *__restrict__ pa, int32_t *__restrict__ pb, unsigned long long *count_out,
                                   int *ovf, int64_t *total) {
+  dep_sync();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t c = *sel_count;
   if (t == 0) {
@@ -1592,10 +1609,11 @@ static cudaError_t skin_build(cudaStream_t st, const delta_scene &s, const Broad
 static cudaError_t skin_check(cudaStream_t st, const delta_scene &s, const BroadphasePlan &plan, const SkinList &k,
                               cudaGraphConditionalHandle h, int &kernels) {
   const double limit = 0.5 * plan.skin * (1.0 - 1e-9);
-  k_skin_check<<<blocks_for(s.n_bodies, 256), 256, 0, st>>>(s, k.anchor, limit * limit, k.need);
-  k_skin_cond<<<1, 1, 0, st>>>(h, k.need);
+  cudaError_t e = launch_dep(true, k_skin_check, blocks_for(s.n_bodies, 256), 256, 0, st, s, k.anchor, limit * limit,
+                             k.need);
+  if (e == cudaSuccess) e = launch_dep(true, k_skin_cond, 1, 1, 0, st, h, k.need);
   kernels += 2;
-  return cudaGetLastError();
+  return e;
 }
 
 // A step's candidate pairs from the list: the tests one thread per entry and an ordered
@@ -1610,29 +1628,24 @@ static cudaError_t skin_filter(cudaStream_t st, const delta_scene &s, const Broa
   if (k.cap <= kBlockSortCap) {
     // the tests on the whole GPU, the ordered compaction in one CTA (the flags in sel)
     uint8_t *flags = reinterpret_cast<uint8_t *>(k.sel);
+    // (the flags kernel follows the conditional node: a plain launch)
     k_skin_flags<<<blocks_for(k.cap, 128), 128, 0, st>>>(k.keys, k.cap, touch, flags);
-    if (k.cap <= 2 * T)
-      k_skin_compact_block<2><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
-                                                pairs_total);
-    else if (k.cap <= 4 * T)
-      k_skin_compact_block<4><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
-                                                pairs_total);
-    else if (k.cap <= 8 * T)
-      k_skin_compact_block<8><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
-                                                pairs_total);
-    else
-      k_skin_compact_block<16><<<1, T, 0, st>>>(k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out, ovf,
-                                                 pairs_total);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    auto compact = k.cap <= 2 * T   ? k_skin_compact_block<2>
+                   : k.cap <= 4 * T ? k_skin_compact_block<4>
+                   : k.cap <= 8 * T ? k_skin_compact_block<8>
+                                    : k_skin_compact_block<16>;
     kernels += 2;
-    return cudaGetLastError();
+    return launch_dep(true, compact, 1, (unsigned)T, 0, st, k.keys, flags, k.cap, touch.sh, pa, pb, pair_cap, count_out,
+                      ovf, pairs_total);
   } else {
     size_t tb = temp_bytes;
     cudaError_t e = cub::DeviceSelect::If(temp, tb, k.keys, k.sel, k.sel_count, k.cap, touch, st);
     if (e != cudaSuccess) return e;
-    k_unpack_selected<<<blocks_for(pair_cap), 256, 0, st>>>(k.sel, k.sel_count, pair_cap, touch.sh, pa, pb, count_out,
-                                                           ovf, pairs_total);
     kernels += 2;
-    return cudaGetLastError();
+    return launch_dep(true, k_unpack_selected, blocks_for(pair_cap), 256, 0, st, k.sel, k.sel_count, pair_cap, touch.sh,
+                      pa, pb, count_out, ovf, pairs_total);
   }
 }
 }  // namespace delta
@@ -1942,8 +1955,9 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   int k = 0;
   delta_status ds = forces_run_fixed(st, s->scene, g.c, g.d_nc, p, s->F, s->T, s->has, g.fs, g.temp, g.temp_bytes, k);
   if (ds != DELTA_OK) return ds;
-  k_bodies<<<blocks_for(s->scene.n_bodies, 128), 128, 0, st>>>(s->scene, p, s->F, s->T, s->has, g.d_ovf, g.d_snap,
-                                                               s->epoch);
+  cudaError_t le = launch_dep(true, k_bodies, blocks_for(s->scene.n_bodies, 128), 128, 0, st, s->scene, p, s->F, s->T,
+                              s->has, g.d_ovf, g.d_snap, s->epoch);
+  if (le != cudaSuccess) return cuda_error(le, "body update");
   if (g.skin.cap > 0) {
     if ((ds = graph_skin_broadphase(s, k)) != DELTA_OK) return ds;
   } else if ((ds = broadphase_run_fixed(st, s->scene, s->plan, g.pa, g.pb, g.pair_cap, g.d_ovf, g.d_pend, g.bp,
@@ -1955,8 +1969,12 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
   const bool posed = s->driver == DELTA_DRV_BF_CERT || s->driver == DELTA_DRV_BF_CULLED || s->driver == DELTA_DRV_LEARNED;
   const Pose pose = sim_pose(s);
   if (!posed) {
-    k_mark_pair_bodies<<<blocks_for(g.pair_cap), 256, 0, st>>>(g.pa, g.pb, g.pair_cap, s->epoch, s->stamp);
-    k_vertices<<<vertex_blocks(s->scene.n_bodies), 256, 0, st>>>(s->scene, g.d_ovf, nullptr, s->stamp, s->epoch);
+    cudaError_t ve = launch_dep(true, k_mark_pair_bodies, blocks_for(g.pair_cap), 256, 0, st, g.pa, g.pb, g.pair_cap,
+                                s->epoch, s->stamp);
+    if (ve == cudaSuccess)
+      ve = launch_dep(true, k_vertices, vertex_blocks(s->scene.n_bodies), 256, 0, st, s->scene, g.d_ovf, nullptr,
+                      s->stamp, s->epoch);
+    if (ve != cudaSuccess) return cuda_error(ve, "step vertices");
     k += 2;
   }
   delta_meshes m{s->scene.n_bodies, s->scene.tri_offset, s->scene.x, s->scene.y, s->scene.z,
@@ -1967,7 +1985,9 @@ static delta_status graph_enqueue_step(delta_sim *s, const delta_step_params &p)
     return ds;
   k += (int)(s->ctx->launches - before);
   s->ctx->launches = before;
-  k_step_end<<<1, 1, 0, st>>>(g.d_snap, g.d_ovf, g.d_nc, g.d_log, g.log_len, g.d_step, g.d_pend, g.d_bp, g.d_cnt);
+  const cudaError_t ee = launch_dep(true, k_step_end, 1, 1, 0, st, g.d_snap, g.d_ovf, g.d_nc, g.d_log, g.log_len,
+                                    g.d_step, g.d_pend, g.d_bp, g.d_cnt);
+  if (ee != cudaSuccess) return cuda_error(ee, "step end");
   g.kernels = k + 2;
   return cuda_error(cudaGetLastError(), "graph step");
 }
