@@ -549,15 +549,14 @@ inline bool cull_stride() {
 
 // cap: blocks per SM (the time-step autotuner's choice), 0 = as many as fit
 inline cudaError_t launch_cull(cudaStream_t s, const delta_meshes &m, const int32_t *pa, const int32_t *pb,
-                               int64_t n_pairs, const RawContacts &rc, DevStats *st, int cap = 0) {
+                               int64_t n_pairs, const RawContacts &rc, DevStats *st, int cap = 0, bool dep = false) {
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cull_pairs, kCullThreads, 0);
   if (e != cudaSuccess) return e;
   if (cap > 0 && cap < per_sm) per_sm = cap;
   int64_t blocks = (int64_t)kNumSMs * (per_sm > 0 ? per_sm : 1);
   if (blocks > n_pairs) blocks = n_pairs > 0 ? n_pairs : 1;
-  k_cull_pairs<<<(unsigned)blocks, kCullThreads, 0, s>>>(m, pa, pb, n_pairs, rc, st);
-  return cudaGetLastError();
+  return launch_dep(dep, k_cull_pairs, (unsigned)blocks, kCullThreads, 0, s, m, pa, pb, n_pairs, rc, st);
 }
 
 // Certified bf over the survivors of the box test, 32 per warp (any mix of pairs).
@@ -853,7 +852,7 @@ __global__ void k_accumulate(const DevStats *st, int64_t *counters) {
 // evaluated pairs (a survivor-list overflow raises *ovf), then the step's statistics go
 // to the running counters.
 __global__ void k_cert_tail(const unsigned long long *sv_count, int64_t sv_cap, DevStats *st, int *ovf,
-                            int64_t *counters) {
+                            int64_t *counters, unsigned long long *queue) {
   dep_sync();
   const unsigned long long c = *sv_count;
   st->evaluated += c;
@@ -861,6 +860,10 @@ __global__ void k_cert_tail(const unsigned long long *sv_count, int64_t sv_cap, 
   if (counters) {
     counters[0] += (int64_t)st->tri_pairs;
     counters[1] += (int64_t)st->evaluated;
+  }
+  if (queue) {  // fixed-capacity state: cleared for the next step (the step's last reader)
+    queue[0] = queue[1] = queue[2] = 0ull;
+    *st = DevStats{};
   }
 }
 
@@ -1147,6 +1150,10 @@ size_t detect_fixed_state_bytes(int64_t pair_cap, int64_t cap) {
 
 // Once per allocation of the fixed-capacity state: the contact sort's identity permutation.
 delta_status detect_fixed_init(cudaStream_t s, void *state, int64_t pair_cap, int64_t cap) {
+  // the queue, counts and statistics start at zero; the culled drivers' tail kernel clears
+  // them after each step, the other drivers' steps before
+  cudaError_t e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s);
+  if (e != cudaSuccess) return cuda_error(e, "detect fixed init");
   char *p = (char *)state + 512 + sizeof(DevStats) + sizeof(int64_t) * (size_t)(2 * pair_cap + 2);
   p += (14 * sizeof(double) + 4 * sizeof(int32_t) + 1 + 2 * sizeof(uint64_t)) * (size_t)cap;
   p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
@@ -1186,7 +1193,11 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
   const bool culled = driver == DELTA_DRV_BF_CERT || driver == DELTA_DRV_BF_CULLED || driver == DELTA_DRV_LEARNED;
   if (culled && pose) rc.pose = *pose;  // vertices and body boxes from the poses
   if (culled && !cull_stride()) rc.pair_queue = queue;  // queue[0], zeroed with the state below
-  if ((e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess) return cuda_error(e, "memset");
+  // the culled drivers find the queue, counts and statistics cleared by the previous step's
+  // tail kernel (or at allocation), so the culling follows the broadphase's last kernel
+  // directly; the other drivers clear them here
+  if (!culled && (e = cudaMemsetAsync(state, 0, 512 + sizeof(DevStats), s)) != cudaSuccess)
+    return cuda_error(e, "memset");
   size_t tb = temp_bytes;
   if (culled) {
     // The culling takes body pairs directly (no rows).  The contacts are ordered without a
@@ -1196,9 +1207,9 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
     // pair's bucket ranked by key.  The per-pair arrival ranks use the sort's key_out.
     rc.pcnt = (unsigned long long *)rows;
     rc.slot = (uint32_t *)key_out;
-    e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats, ctx->cull_blocks_per_sm);
+    // programmatic dependent launches (pdl.cuh)
+    e = launch_cull(s, m, pa, pb, pair_cap, rc, dstats, ctx->cull_blocks_per_sm, true);
     if (e != cudaSuccess) return cuda_error(e, "cull kernel");
-    // after the culling (which follows a memset), programmatic dependent launches (pdl.cuh)
     if ((e = launch_survivors(driver, s, m, pa, pb, rc, dstats, -1, ctx->surv_blocks_per_sm, true)) != cudaSuccess)
       return cuda_error(e, "survivor kernel");
     if ((e = exclusive_sum(temp, tb, rows, row_offset, pair_cap + 1, s, true)) != cudaSuccess)
@@ -1208,7 +1219,7 @@ delta_status detect_run_fixed(delta_ctx *ctx, cudaStream_t s, int driver, const 
             cudaSuccess ||
         (e = launch_dep(true, k_pair_gather, cb, 256, 0, s, rc, row_offset, perm_out, (const uint64_t *)perm_in,
                         pair_cap, out, d_ncontacts, d_ovf, ovf_code, d_count_log)) != cudaSuccess ||
-        (e = launch_dep(true, k_cert_tail, 1, 1, 0, s, rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters)) !=
+        (e = launch_dep(true, k_cert_tail, 1, 1, 0, s, rc.sv_count, rc.sv_cap, dstats, d_ovf, d_counters, queue)) !=
             cudaSuccess)
       return cuda_error(e, "detect fixed");
     ctx->launches += 6;

@@ -315,12 +315,16 @@ __global__ void k_fill_slave_lists(delta_scene s, ContactView cv, const int64_t 
 // master); the second are the body's run of contacts as master, in contact order.  From
 // 0.0, these are the additions of the sorted-entry sums (k_body_forces), in that order.
 __global__ void k_body_forces_lists(delta_scene s, ContactView cv, const int64_t *n_contacts_d, const uint32_t *start,
-                                    int32_t *list, const double *entry, double *force, double *torque,
-                                    uint8_t *has) {
+                                    int32_t *list, const double *entry, double *force, double *torque, uint8_t *has,
+                                    uint32_t *slave_count, uint32_t *fill) {
   dep_sync();
   const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   const int32_t nb = s.n_bodies;
   if (b >= nb) return;
+  // the body's slave count and fill position, read by the kernels before this one, are
+  // cleared for the next step (slave_count[nb] is never counted)
+  slave_count[b] = 0u;
+  fill[b] = 0u;
   X F[3] = {X(0.0), X(0.0), X(0.0)}, T[3] = {X(0.0), X(0.0), X(0.0)};
   bool any = false;
   auto add = [&](const double *v) {
@@ -1281,6 +1285,31 @@ size_t forces_fixed_temp_bytes(int64_t cap, int32_t n_bodies) {
   return b;
 }
 
+// The fixed-capacity force state: entries (2 per segment, 6 doubles), slave lists, slave
+// counts [n + 1] and fill positions [n] (adjacent), list starts [n + 1].
+static void forces_fixed_layout(void *state, int64_t cap, int32_t n, double *&entry, int32_t *&list, uint32_t *&cnt,
+                                uint32_t *&fill, uint32_t *&start) {
+  auto align = [](char *q) { return (char *)(((uintptr_t)q + 255) & ~(uintptr_t)255); };
+  char *b = align((char *)state);
+  entry = (double *)b;
+  b = align(b + 96 * (size_t)cap);
+  list = (int32_t *)b;
+  b = align(b + 4 * (size_t)cap);
+  cnt = (uint32_t *)b;
+  fill = cnt + n + 1;
+  b = align(b + 4 * (2 * (size_t)n + 1));
+  start = (uint32_t *)b;
+}
+
+// Once per allocation of the force state: slave counts and fill positions at zero.
+static cudaError_t forces_fixed_init(cudaStream_t st, void *state, int64_t cap, int32_t n) {
+  double *entry;
+  int32_t *list;
+  uint32_t *cnt, *fill, *start;
+  forces_fixed_layout(state, cap, n, entry, list, cnt, fill, start);
+  return cudaMemsetAsync(cnt, 0, 4 * (2 * (size_t)n + 1), st);
+}
+
 delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta_contacts &c, const int64_t *d_nc,
                               const delta_step_params &p, double *force, double *torque, uint8_t *has, void *state,
                               void *temp, size_t temp_bytes, int &kernels) {
@@ -1288,16 +1317,12 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   const int64_t cap = c.capacity;
   const int32_t n = s.n_bodies;
   ContactView cv{c.x, c.normal, c.depth, c.master, c.slave, c.friction, cap};
-  auto align = [](char *q) { return (char *)(((uintptr_t)q + 255) & ~(uintptr_t)255); };
-  char *b = align((char *)state);
-  double *entry = (double *)b;
-  b = align(b + 96 * (size_t)cap);
-  int32_t *list = (int32_t *)b;
-  b = align(b + 4 * (size_t)cap);
-  uint32_t *cnt = (uint32_t *)b, *fill = cnt + n + 1;  // zeroed together
-  b = align(b + 4 * (2 * (size_t)n + 1));
-  uint32_t *start = (uint32_t *)b;
-  if ((e = cudaMemsetAsync(cnt, 0, 4 * (2 * (size_t)n + 1), st)) != cudaSuccess) return cuda_error(e, "forces memset");
+  double *entry;
+  int32_t *list;
+  uint32_t *cnt, *fill, *start;
+  forces_fixed_layout(state, cap, n, entry, list, cnt, fill, start);
+  // cnt and fill are zero: cleared at allocation (forces_fixed_init) and by the per-body
+  // sums of the step before
   k_pair_forces_heads<true><<<blocks_for(cap, kHeadThreads), kHeadThreads, 0, st>>>(
       s, cv, d_nc, 0, nullptr, nullptr, p, 0, nullptr, nullptr, entry, cnt);
   size_t tb = temp_bytes;
@@ -1307,7 +1332,7 @@ delta_status forces_run_fixed(cudaStream_t st, const delta_scene &s, const delta
   if ((e = launch_dep(true, k_fill_slave_lists, blocks_for(cap), 256, 0, st, s, cv, d_nc, start, fill, list)) !=
           cudaSuccess ||
       (e = launch_dep(true, k_body_forces_lists, blocks_for(n), 256, 0, st, s, cv, d_nc, start, list, entry, force,
-                      torque, has)) != cudaSuccess)
+                      torque, has, cnt, fill)) != cudaSuccess)
     return cuda_error(e, "forces fixed");
   kernels += 4;
   return cuda_error(cudaGetLastError(), "forces fixed");
@@ -1863,6 +1888,7 @@ static delta_status graph_alloc(delta_sim *s, int64_t pair_cap, int64_t contact_
   g.d_log = (int64_t *)(v + 256);
   if ((e = cudaMemset(g.dev, 0, 256)) != cudaSuccess) return cuda_error(e, "graph memset");
   if ((e = block_sort_prepare()) != cudaSuccess) return cuda_error(e, "pair sort attributes");
+  if ((e = forces_fixed_init(s->ctx->stream, g.fs, contact_cap, n)) != cudaSuccess) return cuda_error(e, "forces init");
   delta_status ds = detect_fixed_init(s->ctx->stream, g.ds, pair_cap, contact_cap);
   if (ds != DELTA_OK) return ds;
   if (s->plan.skin > 0.0) {
